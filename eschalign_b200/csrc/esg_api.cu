@@ -1,0 +1,943 @@
+// esg_api.cu -- host side of the B200 panel scorer: the C ABI of
+// include/eschalign_b200.h.
+//
+// Mirrors eschalign's GpuScorer (crates/eschalign/src/cuda/mod.rs:328-709):
+// a panel laid out once on one device under one scoring and mode, batches
+// prepared on the host (prepare), queued (submit) and collected (finish).
+// What differs is what the device does with a batch (esg_kernels.cuh): every
+// query is scored on the GPU -- nothing is left unscored for a CPU path --
+// and the per-read best / XS / tie reduction runs there too.
+#include "../../include/eschalign_b200.h"
+#include "esg_kernels.cuh"
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace esg;
+
+namespace {
+
+thread_local std::string g_err;
+
+esg_status fail(esg_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return st;
+}
+
+esg_status cuda_fail(cudaError_t e, const char* what) {
+  const esg_status st = (e == cudaErrorMemoryAllocation) ? ESG_ERR_OUT_OF_MEMORY
+                        : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+                            ? ESG_ERR_UNAVAILABLE
+                            : ESG_ERR_DRIVER;
+  return fail(st, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define ESG_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+constexpr uint32_t kMaxRefLen = 32768;
+constexpr int kPad = 5;     // selector / table index of a padding column or row
+constexpr int kWild = 4;
+
+inline uint32_t code_of(uint8_t c) { return c > 4 ? 4u : c; }
+
+// Pinned host memory, reused across batches of one scorer.
+struct PinnedPool {
+  std::mutex mu;
+  std::vector<std::pair<void*, size_t>> free_;
+  void* get(size_t bytes, size_t* got) {
+    bytes = std::max<size_t>(bytes, 64);
+    std::lock_guard<std::mutex> lk(mu);
+    size_t best = (size_t)-1;
+    for (size_t k = 0; k < free_.size(); ++k)
+      if (free_[k].second >= bytes && (best == (size_t)-1 || free_[k].second < free_[best].second))
+        best = k;
+    if (best != (size_t)-1) {
+      auto p = free_[best];
+      free_.erase(free_.begin() + best);
+      *got = p.second;
+      return p.first;
+    }
+    void* p = nullptr;
+    const size_t sz = bytes + bytes / 8;
+    if (cudaHostAlloc(&p, sz, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+    *got = sz;
+    return p;
+  }
+  void put(void* p, size_t sz) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(mu);
+    free_.push_back({p, sz});
+  }
+  ~PinnedPool() {
+    for (auto& b : free_) cudaFreeHost(b.first);
+  }
+};
+
+struct Pinned {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace
+
+struct esg_scorer {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  esg_scoring scoring{};
+  int mode = ESG_MODE_LOCAL;
+  int kernel = ESG_KERNEL_AUTO;
+  uint32_t cap = 8;
+  uint32_t n_refs = 0;
+  uint32_t max_ref_len = 0;
+  uint64_t panel_bases = 0;
+  bool panel_w = false;
+  bool batched_ok = false;
+  // k2 panel
+  uint32_t n_pairs = 0;
+  uint32_t blob_bytes = 0;
+  uint32_t sel_base = 0;
+  bool smem_panel = false;
+  void* d_blob = nullptr;
+  uint32_t tab_a[6]{}, tab_b[6]{};
+  int sat = 0;
+  int k2_blocks = 0;
+  size_t k2_smem = 0;
+  const void* k2_fn = nullptr;
+  // k3 panel (longest first)
+  uint8_t* d_rcodes = nullptr;
+  uint32_t* d_roff = nullptr;
+  uint32_t* d_rlen = nullptr;
+  uint32_t* d_ridx = nullptr;
+  int2* d_scratch = nullptr;
+  int k3_blocks = 0;
+  const void* k3_fn = nullptr;
+  PinnedPool pinned;
+  esg_info info{};
+};
+
+struct esg_batch {
+  uint32_t n_reads = 0;
+  uint32_t flags = 0;
+  uint32_t n_q = 0;
+  int kernel = ESG_KERNEL_AUTO;
+  uint64_t total_bases = 0;
+  // host plan
+  uint32_t n_tasks = 0;
+  uint32_t n_order = 0;
+  uint32_t host_list = 0;
+  uint32_t redo_cap = 0;
+  // pinned staging (inputs, then outputs)
+  Pinned in_buf, out_buf;
+  uint8_t* h_codes = nullptr;
+  uint64_t* h_off = nullptr;
+  uint32_t* h_len = nullptr;
+  uint32_t* h_order = nullptr;
+  uint2* h_tasks = nullptr;
+  uint32_t* h_list = nullptr;
+  size_t in_bytes = 0;
+  int4* h_results = nullptr;
+  uint32_t* h_ties = nullptr;
+  int32_t* h_rows = nullptr;
+  uint32_t* h_counters = nullptr;
+  // device
+  void* d_mem = nullptr;
+  size_t d_bytes = 0;
+  uint8_t* d_codes = nullptr;
+  uint64_t* d_off = nullptr;
+  uint32_t* d_len = nullptr;
+  uint32_t* d_order = nullptr;
+  uint2* d_tasks = nullptr;
+  uint32_t* d_list = nullptr;
+  uint32_t* d_counters = nullptr;
+  int4* d_qhead = nullptr;
+  uint32_t* d_qties = nullptr;
+  int32_t* d_k3out = nullptr;
+  int4* d_results = nullptr;
+  uint32_t* d_ties = nullptr;
+  int32_t* d_rows = nullptr;
+  cudaEvent_t done = nullptr;
+  bool submitted = false;
+  esg_scorer* owner = nullptr;
+  esg_batch_stats stats{};
+};
+
+namespace {
+
+// Static bound on every cell of a query of n rows (simd/mod.rs:59-69 argues
+// the same bound for its i16 lanes): |H| <= min(n, L) * max(|ma|, |mi|).
+int64_t value_bound(uint64_t n, uint32_t max_ref_len, const esg_scoring& s) {
+  const int64_t k = (int64_t)std::min<uint64_t>(n, max_ref_len);
+  const int64_t mm = std::max(std::abs(s.match_score), std::abs(s.mismatch));
+  return k * mm + std::abs(s.gap_open) + std::abs(s.gap_extend);
+}
+
+bool k2_takes(const esg_scorer* sc, uint64_t n) {
+  if (!sc->batched_ok || n == 0) return false;
+  if ((n + kRows - 1) / kRows > (uint64_t)kMaxStripes) return false;
+  if (sc->mode == ESG_MODE_SEMIGLOBAL) {
+    // semi-global cells go negative: both sides must stay inside int16
+    const int64_t mm = std::max(std::abs(sc->scoring.match_score), std::abs(sc->scoring.mismatch));
+    return value_bound(n, sc->max_ref_len, sc->scoring) + mm < 28000;
+  }
+  return true;  // local: a wrap is detected by the kernel (K2Params::sat)
+}
+
+bool k2_may_flag(const esg_scorer* sc, uint64_t n) {
+  if (sc->mode != ESG_MODE_LOCAL) return false;
+  const int64_t hmax = (int64_t)std::min<uint64_t>(n, sc->max_ref_len) * sc->scoring.match_score;
+  return hmax >= sc->sat;
+}
+
+template <typename T>
+T* carve(char*& at, size_t count) {
+  T* p = reinterpret_cast<T*>(at);
+  at += ((count * sizeof(T)) + 255) / 256 * 256;
+  return p;
+}
+
+size_t carve_size(size_t count, size_t elem) { return (count * elem + 255) / 256 * 256; }
+
+void set_k2_fn(esg_scorer* sc) {
+  const bool local = sc->mode == ESG_MODE_LOCAL;
+  if (local) {
+    if (sc->panel_w)
+      sc->k2_fn = sc->smem_panel ? (const void*)k2_batched<true, true, true>
+                                 : (const void*)k2_batched<true, true, false>;
+    else
+      sc->k2_fn = sc->smem_panel ? (const void*)k2_batched<true, false, true>
+                                 : (const void*)k2_batched<true, false, false>;
+  } else {
+    if (sc->panel_w)
+      sc->k2_fn = sc->smem_panel ? (const void*)k2_batched<false, true, true>
+                                 : (const void*)k2_batched<false, true, false>;
+    else
+      sc->k2_fn = sc->smem_panel ? (const void*)k2_batched<false, false, true>
+                                 : (const void*)k2_batched<false, false, false>;
+  }
+  sc->k3_fn = local ? (const void*)k3_plain<true> : (const void*)k3_plain<false>;
+}
+
+}  // namespace
+
+// ===================================================================== API
+
+extern "C" {
+
+int esg_abi_version(void) { return ESG_ABI_VERSION; }
+
+const char* esg_status_string(esg_status st) {
+  switch (st) {
+    case ESG_OK: return "ok";
+    case ESG_ERR_UNAVAILABLE: return "CUDA unavailable";
+    case ESG_ERR_DRIVER: return "CUDA driver error";
+    case ESG_ERR_REFERENCE_TOO_LONG: return "reference too long";
+    case ESG_ERR_SCORING_INVALID: return "invalid scoring";
+    case ESG_ERR_EMPTY_PANEL: return "empty panel";
+    case ESG_ERR_EMPTY_REFERENCE: return "empty reference";
+    case ESG_ERR_BAD_ARGUMENT: return "bad argument";
+    case ESG_ERR_OUT_OF_MEMORY: return "out of memory";
+    case ESG_ERR_TIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+const char* esg_last_error(void) { return g_err.c_str(); }
+
+esg_status esg_device_count(int32_t* out) {
+  if (!out) return fail(ESG_ERR_BAD_ARGUMENT, "out is NULL");
+  int n = 0;
+  const cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *out = 0;
+    return ESG_OK;
+  }
+  *out = n;
+  return ESG_OK;
+}
+
+int32_t esg_fits_i16(uint64_t len, uint64_t max_ref_len, const esg_scoring* s) {
+  if (!s) return 0;
+  const int64_t k = (int64_t)std::min(len, max_ref_len);
+  const int64_t mm = std::max(std::abs(s->match_score), std::abs(s->mismatch));
+  const int64_t bound = k * mm + std::abs(s->gap_open) + std::abs(s->gap_extend);
+  return bound < 15000 && max_ref_len < 15000;
+}
+
+esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64_t* ref_off,
+                          const uint32_t* ref_len, uint32_t n_refs, const esg_scoring* scoring,
+                          int32_t mode, const esg_options* options, esg_scorer** out) {
+  g_err.clear();
+  if (!out || !scoring) return fail(ESG_ERR_BAD_ARGUMENT, "out and scoring must not be NULL");
+  *out = nullptr;
+  if (mode != ESG_MODE_LOCAL && mode != ESG_MODE_SEMIGLOBAL)
+    return fail(ESG_ERR_BAD_ARGUMENT, "mode %d is not local (0) or semiglobal (1)", mode);
+  // scoring.rs:70-100
+  const esg_scoring s = *scoring;
+  if (s.match_score <= 0)
+    return fail(ESG_ERR_SCORING_INVALID, "match must be positive, got %d", s.match_score);
+  if (s.mismatch >= s.match_score)
+    return fail(ESG_ERR_SCORING_INVALID, "mismatch (%d) must score below match (%d)", s.mismatch,
+                s.match_score);
+  if (s.gap_open > 0 || s.gap_extend > 0)
+    return fail(ESG_ERR_SCORING_INVALID,
+                "gap scores are penalties and must be zero or negative, got open %d extend %d",
+                s.gap_open, s.gap_extend);
+  for (int32_t v : {s.match_score, s.mismatch, s.gap_open, s.gap_extend})
+    if (std::abs(v) > 1000)
+      return fail(ESG_ERR_SCORING_INVALID, "|%d| exceeds the supported magnitude 1000", v);
+  // panel.rs:34-55
+  if (n_refs == 0) return fail(ESG_ERR_EMPTY_PANEL, "the reference panel is empty");
+  if (!ref_codes || !ref_off || !ref_len)
+    return fail(ESG_ERR_BAD_ARGUMENT, "reference arrays must not be NULL");
+  uint32_t max_len = 0;
+  uint64_t bases = 0;
+  for (uint32_t r = 0; r < n_refs; ++r) {
+    if (ref_len[r] == 0) return fail(ESG_ERR_EMPTY_REFERENCE, "reference %u has no bases", r);
+    max_len = std::max(max_len, ref_len[r]);
+    bases += ref_len[r];
+  }
+  if (max_len > kMaxRefLen)
+    return fail(ESG_ERR_REFERENCE_TOO_LONG,
+                "the panel's longest reference (%u nt) exceeds the GPU kernel's %u nt", max_len,
+                kMaxRefLen);
+  uint32_t cap = 8;
+  int kernel = ESG_KERNEL_AUTO;
+  void* ext_stream = nullptr;
+  if (options) {
+    if (options->tie_capacity) cap = options->tie_capacity;
+    kernel = options->kernel;
+    ext_stream = options->stream;
+  }
+  if (cap < 1 || cap > ESG_MAX_TIE_CAPACITY)
+    return fail(ESG_ERR_BAD_ARGUMENT, "tie_capacity %u outside 1..%d", cap, ESG_MAX_TIE_CAPACITY);
+  if (kernel != ESG_KERNEL_AUTO && kernel != ESG_KERNEL_PLAIN32)
+    return fail(ESG_ERR_BAD_ARGUMENT, "unknown kernel %d", kernel);
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(ESG_ERR_UNAVAILABLE, "no CUDA device is visible");
+  }
+  if (device < 0 || device >= ndev)
+    return fail(ESG_ERR_UNAVAILABLE, "device %d not present (%d visible)", device, ndev);
+  ESG_CUDA(cudaSetDevice(device));
+
+  auto* sc = new esg_scorer();
+  sc->device = device;
+  sc->scoring = s;
+  sc->mode = mode;
+  sc->kernel = kernel;
+  sc->cap = cap;
+  sc->n_refs = n_refs;
+  sc->max_ref_len = max_len;
+  sc->panel_bases = bases;
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+    delete sc;
+    return cuda_fail(cudaGetLastError(), "cudaGetDeviceProperties");
+  }
+  sc->sm_count = prop.multiProcessorCount;
+  if (prop.major < 10) {
+    delete sc;
+    return fail(ESG_ERR_UNAVAILABLE,
+                "device %d (%s, sm_%d%d) is not a Blackwell sm_100 part this library is built for",
+                device, prop.name, prop.major, prop.minor);
+  }
+  if (ext_stream) {
+    sc->stream = (cudaStream_t)ext_stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete sc;
+      return cuda_fail(cudaGetLastError(), "cudaStreamCreate");
+    }
+    sc->own_stream = true;
+  }
+
+  // Longest first, stable (cuda/mod.rs:379-380; simd/mod.rs:294-296).
+  std::vector<uint32_t> order(n_refs);
+  for (uint32_t r = 0; r < n_refs; ++r) order[r] = r;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return ref_len[a] > ref_len[b]; });
+  for (uint32_t r = 0; r < n_refs; ++r)
+    for (uint32_t j = 0; j < ref_len[r]; ++j)
+      if (code_of(ref_codes[ref_off[r] + j]) == kWild) sc->panel_w = true;
+
+  // --- scoring tables of the batched kernel: s - o as int8 per byte
+  const int ma = s.match_score, mi = s.mismatch, o = s.gap_open;
+  auto fits8 = [](int v) { return v >= -128 && v <= 127; };
+  sc->batched_ok = fits8(ma - o) && fits8(mi - o) && fits8(-o);
+  if (sc->batched_ok) {
+    for (int c = 0; c < 6; ++c) {
+      uint32_t a = 0, b = 0;
+      for (int x = 0; x < 4; ++x) {
+        int v;
+        if (c == kPad) v = -o;
+        else if (c == kWild) v = ma - o;
+        else v = (c == x ? ma : mi) - o;
+        a |= (uint32_t)(uint8_t)(int8_t)v << (8 * x);
+      }
+      const int w = (c == kPad) ? -o : ma - o;  // against a wildcard reference base
+      b = (uint32_t)(uint8_t)(int8_t)w | (0x80u << 8);  // byte 5: a padding column, -128
+      sc->tab_a[c] = a;
+      sc->tab_b[c] = b;
+    }
+    sc->sat = 32767 - ma;
+  }
+
+  // --- reference pairs and their selectors
+  sc->n_pairs = (n_refs + 1) / 2;
+  std::vector<uint4> pairs(sc->n_pairs);
+  std::vector<uint16_t> sels;
+  for (uint32_t p = 0; p < sc->n_pairs; ++p) {
+    const uint32_t ra = order[2 * p];
+    const bool hasb = 2 * p + 1 < n_refs;
+    const uint32_t rb = hasb ? order[2 * p + 1] : kNoRef;
+    const uint32_t ma_ = ref_len[ra], mb_ = hasb ? ref_len[rb] : 0;
+    const uint32_t m = std::max(ma_, mb_);
+    pairs[p] = make_uint4((uint32_t)sels.size(), (ma_ & 0xffffu) | (mb_ << 16), ra, rb);
+    for (uint32_t j = 0; j < m; ++j) {
+      const uint32_t x = j < ma_ ? code_of(ref_codes[ref_off[ra] + j]) : kPad;
+      const uint32_t y = (hasb && j < mb_) ? code_of(ref_codes[ref_off[rb] + j]) : kPad;
+      sels.push_back((uint16_t)(x | ((x | 8u) << 4) | (y << 8) | ((y | 8u) << 12)));
+    }
+  }
+  // m is stored in 16 bits: lengths up to kMaxRefLen (32768) fit.
+  sc->sel_base = sc->n_pairs * 8;  // uint16 units after the pair table
+  const size_t raw = (size_t)sc->n_pairs * 16 + sels.size() * 2;
+  sc->blob_bytes = (uint32_t)((raw + 15) / 16 * 16);
+  std::vector<unsigned char> blob(sc->blob_bytes, 0);
+  memcpy(blob.data(), pairs.data(), pairs.size() * 16);
+  memcpy(blob.data() + (size_t)sc->n_pairs * 16, sels.data(), sels.size() * 2);
+
+  auto cleanup = [&](esg_status st) {
+    esg_scorer_free(sc);
+    return st;
+  };
+  cudaError_t e = cudaMalloc(&sc->d_blob, sc->blob_bytes);
+  if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(panel)"));
+  e = cudaMemcpy(sc->d_blob, blob.data(), sc->blob_bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMemcpy(panel)"));
+
+  // --- k3 panel (longest first)
+  {
+    std::vector<uint8_t> rc;
+    std::vector<uint32_t> roff(n_refs), rlen(n_refs);
+    rc.reserve(bases);
+    for (uint32_t k = 0; k < n_refs; ++k) {
+      const uint32_t r = order[k];
+      roff[k] = (uint32_t)rc.size();
+      rlen[k] = ref_len[r];
+      for (uint32_t j = 0; j < ref_len[r]; ++j) rc.push_back((uint8_t)code_of(ref_codes[ref_off[r] + j]));
+    }
+    if ((e = cudaMalloc(&sc->d_rcodes, rc.size())) != cudaSuccess ||
+        (e = cudaMalloc(&sc->d_roff, n_refs * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&sc->d_rlen, n_refs * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&sc->d_ridx, n_refs * 4)) != cudaSuccess)
+      return cleanup(cuda_fail(e, "cudaMalloc(k3 panel)"));
+    if ((e = cudaMemcpy(sc->d_rcodes, rc.data(), rc.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(sc->d_roff, roff.data(), n_refs * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(sc->d_rlen, rlen.data(), n_refs * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(sc->d_ridx, order.data(), n_refs * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cleanup(cuda_fail(e, "cudaMemcpy(k3 panel)"));
+  }
+
+  // --- launch geometry
+  const size_t slots = (size_t)kK2Threads * (4 + cap) * 4;
+  sc->smem_panel = (size_t)sc->blob_bytes + slots <= 100 * 1024;
+  set_k2_fn(sc);
+  sc->k2_smem = (sc->smem_panel ? sc->blob_bytes : 0) + slots;
+  if ((e = cudaFuncSetAttribute(sc->k2_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sc->k2_smem)) != cudaSuccess)
+    return cleanup(cuda_fail(e, "cudaFuncSetAttribute(k2)"));
+  int occ2 = 0, occ3 = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, sc->k2_fn, kK2Threads,
+                                                         sc->k2_smem)) != cudaSuccess ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, sc->k3_fn, kK3Threads, 0)) !=
+          cudaSuccess)
+    return cleanup(cuda_fail(e, "cudaOccupancy"));
+  sc->k2_blocks = std::max(1, occ2) * sc->sm_count;
+  sc->k3_blocks = std::max(1, occ3) * sc->sm_count;
+  // k3's stripe boundary: one int2 per reference column per thread, at most 2 GiB
+  const size_t per_thread = (size_t)max_len * sizeof(int2);
+  const size_t budget = (size_t)2 << 30;
+  while ((size_t)sc->k3_blocks * kK3Threads * per_thread > budget && sc->k3_blocks > 1)
+    sc->k3_blocks /= 2;
+  if ((e = cudaMalloc(&sc->d_scratch, (size_t)sc->k3_blocks * kK3Threads * per_thread)) !=
+      cudaSuccess)
+    return cleanup(cuda_fail(e, "cudaMalloc(k3 scratch)"));
+
+  // --- info
+  esg_info& inf = sc->info;
+  snprintf(inf.device_name, sizeof inf.device_name, "%s", prop.name);
+  inf.device = device;
+  inf.sm_count = sc->sm_count;
+  inf.n_refs = n_refs;
+  inf.max_ref_len = max_len;
+  inf.n_ref_pairs = sc->n_pairs;
+  inf.panel_bytes = sc->smem_panel ? sc->blob_bytes : 0;
+  inf.batched_ok = sc->batched_ok;
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, sc->k2_fn) == cudaSuccess) {
+    inf.regs_batched = fa.numRegs;
+    inf.local_bytes_batched = (int)fa.localSizeBytes;
+  }
+  if (cudaFuncGetAttributes(&fa, sc->k3_fn) == cudaSuccess) {
+    inf.regs_plain = fa.numRegs;
+    inf.local_bytes_plain = (int)fa.localSizeBytes;
+  }
+  inf.batched_blocks = sc->k2_blocks;
+  inf.batched_threads = kK2Threads;
+  inf.plain_blocks = sc->k3_blocks;
+  inf.plain_threads = kK3Threads;
+  *out = sc;
+  return ESG_OK;
+}
+
+void esg_scorer_free(esg_scorer* sc) {
+  if (!sc) return;
+  cudaSetDevice(sc->device);
+  if (sc->stream) cudaStreamSynchronize(sc->stream);
+  cudaFree(sc->d_blob);
+  cudaFree(sc->d_rcodes);
+  cudaFree(sc->d_roff);
+  cudaFree(sc->d_rlen);
+  cudaFree(sc->d_ridx);
+  cudaFree(sc->d_scratch);
+  if (sc->own_stream && sc->stream) cudaStreamDestroy(sc->stream);
+  delete sc;
+}
+
+esg_status esg_scorer_info(const esg_scorer* sc, esg_info* out) {
+  if (!sc || !out) return fail(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  *out = sc->info;
+  return ESG_OK;
+}
+
+esg_status esg_scorer_set_kernel(esg_scorer* sc, int32_t kernel) {
+  if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");
+  if (kernel != ESG_KERNEL_AUTO && kernel != ESG_KERNEL_PLAIN32)
+    return fail(ESG_ERR_BAD_ARGUMENT, "unknown kernel %d", kernel);
+  sc->kernel = kernel;
+  return ESG_OK;
+}
+
+int32_t esg_scores_len(const esg_scorer* sc, uint64_t len) { return sc && len > 0; }
+
+// ---------------------------------------------------------------- prepare
+esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                       const uint32_t* len, uint32_t n_reads, uint32_t flags, esg_batch** out) {
+  g_err.clear();
+  if (!sc || !out) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer or out");
+  *out = nullptr;
+  if (flags & ~(ESG_BOTH_STRANDS | ESG_FULL_ROWS))
+    return fail(ESG_ERR_BAD_ARGUMENT, "unknown flags 0x%x", flags);
+  if (n_reads && (!off || !len)) return fail(ESG_ERR_BAD_ARGUMENT, "off/len must not be NULL");
+  if (n_reads >= (1u << 30)) return fail(ESG_ERR_BAD_ARGUMENT, "too many reads (%u)", n_reads);
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < n_reads; ++k) total += len[k];
+  if (total && !codes) return fail(ESG_ERR_BAD_ARGUMENT, "codes must not be NULL");
+
+  auto* b = new esg_batch();
+  b->owner = sc;
+  b->n_reads = n_reads;
+  b->flags = flags;
+  b->kernel = sc->kernel;
+  const bool both = flags & ESG_BOTH_STRANDS;
+  b->n_q = n_reads * (both ? 2u : 1u);
+  b->total_bases = total;
+
+  // --- plan: which queries go where
+  std::vector<uint32_t> by_s_count(kMaxStripes + 1, 0);
+  std::vector<uint8_t> route(b->n_q, 0);  // 0 empty, 1 k2, 2 k3
+  uint32_t n_k2 = 0, n_k3 = 0, n_empty = 0, redo_cap = 0;
+  uint64_t cells = 0;
+  for (uint32_t q = 0; q < b->n_q; ++q) {
+    const uint32_t n = len[q < n_reads ? q : q - n_reads];
+    if (n == 0) {
+      ++n_empty;
+      continue;
+    }
+    cells += (uint64_t)n * sc->panel_bases;
+    if (b->kernel == ESG_KERNEL_AUTO && k2_takes(sc, n)) {
+      route[q] = 1;
+      ++n_k2;
+      ++by_s_count[(n + kRows - 1) / kRows];
+      if (k2_may_flag(sc, n)) ++redo_cap;
+    } else {
+      route[q] = 2;
+      ++n_k3;
+    }
+  }
+  b->host_list = n_k3;
+  b->redo_cap = redo_cap;
+
+  // best-fit decreasing of query stripes into 32-lane tiles
+  std::vector<uint32_t> start_of(kMaxStripes + 2, 0);
+  for (int S = kMaxStripes; S >= 1; --S) start_of[S - 1] = start_of[S] + by_s_count[S];
+  // queries sorted by stripe count, descending (stable within a count)
+  std::vector<uint32_t> sorted(n_k2);
+  {
+    std::vector<uint32_t> fill(start_of);
+    for (uint32_t q = 0; q < b->n_q; ++q)
+      if (route[q] == 1) {
+        const uint32_t n = len[q < n_reads ? q : q - n_reads];
+        const uint32_t S = (n + kRows - 1) / kRows;
+        sorted[fill[S]++] = q;
+      }
+  }
+  std::vector<uint32_t> bin_of(n_k2);
+  std::vector<uint8_t> bin_free, bin_smax;
+  std::vector<uint16_t> bin_count;
+  std::vector<std::vector<uint32_t>> open(kMaxStripes);  // by free capacity 1..31
+  uint32_t open_mask = 0;
+  for (uint32_t i = 0; i < n_k2; ++i) {
+    const uint32_t q = sorted[i];
+    const uint32_t n = len[q < n_reads ? q : q - n_reads];
+    const uint32_t S = (n + kRows - 1) / kRows;
+    const uint32_t cand = open_mask & ~((1u << S) - 1u);
+    uint32_t bin;
+    if (cand) {
+      const uint32_t f = __builtin_ctz(cand);
+      bin = open[f].back();
+      open[f].pop_back();
+      if (open[f].empty()) open_mask &= ~(1u << f);
+    } else {
+      bin = (uint32_t)bin_free.size();
+      bin_free.push_back(kMaxStripes);
+      bin_smax.push_back((uint8_t)S);
+      bin_count.push_back(0);
+    }
+    bin_of[i] = bin;
+    bin_free[bin] = (uint8_t)(bin_free[bin] - S);
+    bin_count[bin]++;
+    const uint32_t f = bin_free[bin];
+    if (f > 0) {
+      open[f].push_back(bin);
+      open_mask |= 1u << f;
+    }
+  }
+  b->n_tasks = (uint32_t)bin_free.size();
+  b->n_order = n_k2;
+
+  // --- pinned staging for the inputs
+  const size_t sz_codes = carve_size(total ? total : 1, 1);
+  const size_t sz_off = carve_size(n_reads ? n_reads : 1, 8);
+  const size_t sz_len = carve_size(n_reads ? n_reads : 1, 4);
+  const size_t sz_order = carve_size(n_k2 ? n_k2 : 1, 4);
+  const size_t sz_tasks = carve_size(b->n_tasks ? b->n_tasks : 1, 8);
+  const size_t sz_list = carve_size(n_k3 + redo_cap ? n_k3 + redo_cap : 1, 4);
+  b->in_bytes = sz_codes + sz_off + sz_len + sz_order + sz_tasks + sz_list;
+  b->in_buf.p = sc->pinned.get(b->in_bytes, &b->in_buf.cap);
+  if (!b->in_buf.p) {
+    delete b;
+    return fail(ESG_ERR_OUT_OF_MEMORY, "pinned host memory (%zu bytes)", (size_t)b->in_bytes);
+  }
+  char* at = (char*)b->in_buf.p;
+  b->h_codes = carve<uint8_t>(at, total ? total : 1);
+  b->h_off = carve<uint64_t>(at, n_reads ? n_reads : 1);
+  b->h_len = carve<uint32_t>(at, n_reads ? n_reads : 1);
+  b->h_order = carve<uint32_t>(at, n_k2 ? n_k2 : 1);
+  b->h_tasks = carve<uint2>(at, b->n_tasks ? b->n_tasks : 1);
+  b->h_list = carve<uint32_t>(at, n_k3 + redo_cap ? n_k3 + redo_cap : 1);
+  uint64_t pos = 0;
+  for (uint32_t k = 0; k < n_reads; ++k) {
+    b->h_off[k] = pos;
+    b->h_len[k] = len[k];
+    if (len[k]) memcpy(b->h_codes + pos, codes + off[k], len[k]);
+    pos += len[k];
+  }
+  // order[] grouped by task, tasks[] = {start, count | smax << 16}
+  {
+    std::vector<uint32_t> tstart(b->n_tasks + 1, 0);
+    for (uint32_t t = 0; t < b->n_tasks; ++t) tstart[t + 1] = tstart[t] + bin_count[t];
+    std::vector<uint32_t> fill(tstart.begin(), tstart.end() - 1);
+    for (uint32_t i = 0; i < n_k2; ++i) b->h_order[fill[bin_of[i]]++] = sorted[i];
+    uint32_t lanes = 0;
+    for (uint32_t t = 0; t < b->n_tasks; ++t) {
+      b->h_tasks[t] = make_uint2(tstart[t], (uint32_t)bin_count[t] | ((uint32_t)bin_smax[t] << 16));
+      lanes += kMaxStripes - bin_free[t];
+    }
+    b->stats.lanes_used = lanes;
+  }
+  {
+    uint32_t w = 0;
+    for (uint32_t q = 0; q < b->n_q; ++q)
+      if (route[q] == 2) b->h_list[w++] = q;
+  }
+  b->stats.n_reads = n_reads;
+  b->stats.n_queries = b->n_q;
+  b->stats.n_empty = n_empty;
+  b->stats.queries_batched = n_k2;
+  b->stats.queries_plain = n_k3;
+  b->stats.tasks = b->n_tasks;
+  b->stats.cells = cells;
+  *out = b;
+  return ESG_OK;
+}
+
+// ---------------------------------------------------------------- device work
+static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t st) {
+  const bool both = b->flags & ESG_BOTH_STRANDS;
+  uint32_t kernels = 0;
+  const bool rows = b->flags & ESG_FULL_ROWS;
+  ESG_CUDA(cudaMemsetAsync(b->d_counters, 0, 16, st));
+  if (b->n_tasks) {
+    K2Params P{};
+    P.blob = (const uint4*)sc->d_blob;
+    P.blob_bytes = sc->blob_bytes;
+    P.n_pairs = sc->n_pairs;
+    P.sel_base = sc->sel_base;
+    P.codes = b->d_codes;
+    P.off = b->d_off;
+    P.len = b->d_len;
+    P.n_reads = b->n_reads;
+    P.order = b->d_order;
+    P.tasks = b->d_tasks;
+    P.n_tasks = b->n_tasks;
+    P.counters = b->d_counters;
+    P.qhead = b->d_qhead;
+    P.qties = b->d_qties;
+    P.rows = rows ? b->d_rows : nullptr;
+    P.n_refs = sc->n_refs;
+    P.redo_list = b->d_list;
+    P.redo_base = b->host_list;
+    P.redo_cap = b->redo_cap;
+    memcpy(P.tab_a, sc->tab_a, sizeof P.tab_a);
+    memcpy(P.tab_b, sc->tab_b, sizeof P.tab_b);
+    P.o2 = pack16x2(sc->scoring.gap_open, sc->scoring.gap_open);
+    P.e2 = pack16x2(sc->scoring.gap_extend, sc->scoring.gap_extend);
+    P.o = sc->scoring.gap_open;
+    P.sat = sc->sat;
+    P.cap = sc->cap;
+    const int blocks =
+        (int)std::min<uint64_t>((uint64_t)sc->k2_blocks, (b->n_tasks + kK2Warps - 1) / kK2Warps);
+    void* args[] = {&P};
+    ESG_CUDA(cudaLaunchKernel(sc->k2_fn, dim3(blocks), dim3(kK2Threads), args, sc->k2_smem, st));
+    ++kernels;
+  }
+  const bool k3 = b->host_list + b->redo_cap > 0;
+  if (k3) {
+    K3Params P{};
+    P.codes = b->d_codes;
+    P.off = b->d_off;
+    P.len = b->d_len;
+    P.n_reads = b->n_reads;
+    P.rcodes = sc->d_rcodes;
+    P.roff = sc->d_roff;
+    P.rlen = sc->d_rlen;
+    P.ridx = sc->d_ridx;
+    P.n_refs = sc->n_refs;
+    P.list = b->d_list;
+    P.host_count = b->host_list;
+    P.redo_count = b->redo_cap ? b->d_counters + 1 : nullptr;
+    P.redo_cap = b->redo_cap;
+    P.out = b->d_k3out;
+    P.rows = rows ? b->d_rows : nullptr;
+    P.scratch = sc->d_scratch;
+    P.ma = sc->scoring.match_score;
+    P.mi = sc->scoring.mismatch;
+    P.o = sc->scoring.gap_open;
+    P.e = sc->scoring.gap_extend;
+    P.local = sc->mode == ESG_MODE_LOCAL;
+    void* args[] = {&P};
+    ESG_CUDA(cudaLaunchKernel(sc->k3_fn, dim3(sc->k3_blocks), dim3(kK3Threads), args, 0, st));
+    ++kernels;
+    K4Params Q{};
+    Q.list = b->d_list;
+    Q.host_count = b->host_list;
+    Q.redo_count = P.redo_count;
+    Q.redo_cap = b->redo_cap;
+    Q.rows = b->d_k3out;
+    Q.n_refs = sc->n_refs;
+    Q.n_reads = b->n_reads;
+    Q.qhead = b->d_qhead;
+    Q.qties = b->d_qties;
+    Q.cap = sc->cap;
+    const uint32_t need = b->host_list + b->redo_cap;
+    const int blocks = (int)std::max<uint64_t>(
+        1, std::min<uint64_t>((uint64_t)sc->sm_count * 8, (need + 7) / 8));
+    void* qargs[] = {&Q};
+    ESG_CUDA(cudaLaunchKernel((const void*)k4_rows, dim3(blocks), dim3(256), qargs, 0, st));
+    ++kernels;
+  }
+  if (b->n_reads) {
+    K5Params M{};
+    M.len = b->d_len;
+    M.n_reads = b->n_reads;
+    M.both = both;
+    M.qhead = b->d_qhead;
+    M.qties = b->d_qties;
+    M.cap = sc->cap;
+    M.results = b->d_results;
+    M.ties = b->d_ties;
+    const int blocks = (int)std::min<uint64_t>(4096, (b->n_reads + 255) / 256);
+    void* margs[] = {&M};
+    ESG_CUDA(cudaLaunchKernel((const void*)k5_merge, dim3(blocks), dim3(256), margs, 0, st));
+    ++kernels;
+  }
+  b->stats.kernels = kernels;
+  return ESG_OK;
+}
+
+esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
+  g_err.clear();
+  if (!sc || !b || b->owner != sc) return fail(ESG_ERR_BAD_ARGUMENT, "batch/scorer mismatch");
+  if (b->submitted) return fail(ESG_ERR_BAD_ARGUMENT, "batch already submitted");
+  ESG_CUDA(cudaSetDevice(sc->device));
+  cudaStream_t st = sc->stream;
+  const bool rows = b->flags & ESG_FULL_ROWS;
+  const uint32_t nlist = b->host_list + b->redo_cap;
+  const size_t nr = b->n_reads ? b->n_reads : 1, nq = b->n_q ? b->n_q : 1;
+  // device buffers, one stream-ordered allocation
+  size_t sizes[] = {
+      carve_size(b->total_bases ? b->total_bases : 1, 1),
+      carve_size(nr, 8),
+      carve_size(nr, 4),
+      carve_size(b->n_order ? b->n_order : 1, 4),
+      carve_size(b->n_tasks ? b->n_tasks : 1, 8),
+      carve_size(nlist ? nlist : 1, 4),
+      carve_size(4, 4),
+      carve_size(nq, 16),
+      carve_size(nq * sc->cap, 4),
+      carve_size(nlist ? (size_t)nlist * sc->n_refs : 1, 4),
+      carve_size(nr, 16),
+      carve_size(nr * sc->cap, 4),
+      rows ? carve_size(nq * sc->n_refs, 4) : 0,
+  };
+  size_t total = 0;
+  for (size_t v : sizes) total += v;
+  ESG_CUDA(cudaMallocAsync(&b->d_mem, total, st));
+  b->d_bytes = total;
+  char* at = (char*)b->d_mem;
+  b->d_codes = carve<uint8_t>(at, b->total_bases ? b->total_bases : 1);
+  b->d_off = carve<uint64_t>(at, nr);
+  b->d_len = carve<uint32_t>(at, nr);
+  b->d_order = carve<uint32_t>(at, b->n_order ? b->n_order : 1);
+  b->d_tasks = carve<uint2>(at, b->n_tasks ? b->n_tasks : 1);
+  b->d_list = carve<uint32_t>(at, nlist ? nlist : 1);
+  b->d_counters = carve<uint32_t>(at, 4);
+  b->d_qhead = carve<int4>(at, nq);
+  b->d_qties = carve<uint32_t>(at, nq * sc->cap);
+  b->d_k3out = carve<int32_t>(at, nlist ? (size_t)nlist * sc->n_refs : 1);
+  b->d_results = carve<int4>(at, nr);
+  b->d_ties = carve<uint32_t>(at, nr * sc->cap);
+  b->d_rows = rows ? carve<int32_t>(at, nq * sc->n_refs) : nullptr;
+  // uploads: the pinned staging is one contiguous block laid out the same way
+  // for the first six buffers
+  ESG_CUDA(cudaMemcpyAsync(b->d_codes, b->in_buf.p, b->in_bytes, cudaMemcpyHostToDevice, st));
+  b->stats.h2d_bytes = b->in_bytes;
+  esg_status s = launch_device_work(sc, b, st);
+  if (s != ESG_OK) return s;
+  // downloads into pinned staging
+  const size_t out_bytes = carve_size(nr, 16) + carve_size(nr * sc->cap, 4) +
+                           (rows ? carve_size(nq * sc->n_refs, 4) : 0) + carve_size(4, 4);
+  b->out_buf.p = sc->pinned.get(out_bytes, &b->out_buf.cap);
+  if (!b->out_buf.p) return fail(ESG_ERR_OUT_OF_MEMORY, "pinned host memory (%zu bytes)", out_bytes);
+  char* o = (char*)b->out_buf.p;
+  b->h_results = carve<int4>(o, nr);
+  b->h_ties = carve<uint32_t>(o, nr * sc->cap);
+  b->h_counters = carve<uint32_t>(o, 4);
+  b->h_rows = rows ? carve<int32_t>(o, nq * sc->n_refs) : nullptr;
+  // d_results and d_ties are adjacent in device memory, as in the staging
+  ESG_CUDA(cudaMemcpyAsync(b->h_results, b->d_results,
+                           carve_size(nr, 16) + carve_size(nr * sc->cap, 4),
+                           cudaMemcpyDeviceToHost, st));
+  ESG_CUDA(cudaMemcpyAsync(b->h_counters, b->d_counters, 16, cudaMemcpyDeviceToHost, st));
+  if (rows)
+    ESG_CUDA(cudaMemcpyAsync(b->h_rows, b->d_rows, (size_t)b->n_q * sc->n_refs * 4,
+                             cudaMemcpyDeviceToHost, st));
+  b->stats.d2h_bytes = carve_size(nr, 16) + carve_size(nr * sc->cap, 4) + 16 +
+                       (rows ? (size_t)b->n_q * sc->n_refs * 4 : 0);
+  ESG_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+  ESG_CUDA(cudaEventRecord(b->done, st));
+  b->submitted = true;
+  return ESG_OK;
+}
+
+esg_status esg_relaunch(esg_scorer* sc, esg_batch* b, void* stream) {
+  g_err.clear();
+  if (!sc || !b || b->owner != sc || !b->submitted)
+    return fail(ESG_ERR_BAD_ARGUMENT, "relaunch needs a submitted batch of this scorer");
+  ESG_CUDA(cudaSetDevice(sc->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : sc->stream;
+  return launch_device_work(sc, b, st);
+}
+
+esg_status esg_finish(esg_scorer* sc, esg_batch* b, esg_read_result* results, uint32_t* ties,
+                      int32_t* rows) {
+  g_err.clear();
+  if (!sc || !b || b->owner != sc || !b->submitted)
+    return fail(ESG_ERR_BAD_ARGUMENT, "finish needs a submitted batch of this scorer");
+  ESG_CUDA(cudaSetDevice(sc->device));
+  ESG_CUDA(cudaEventSynchronize(b->done));
+  ESG_CUDA(cudaGetLastError());
+  const uint32_t errbits = b->h_counters[2];
+  b->stats.queries_rescored = std::min(b->h_counters[1], b->redo_cap);
+  if (errbits & kErrPanelWait)
+    return fail(ESG_ERR_TIMEOUT, "the panel's shared-memory staging did not complete");
+  if (errbits & kErrRedoOverflow)
+    return fail(ESG_ERR_DRIVER, "re-score list overflow (internal error)");
+  if (results && b->n_reads) memcpy(results, b->h_results, (size_t)b->n_reads * 16);
+  if (ties && b->n_reads) memcpy(ties, b->h_ties, (size_t)b->n_reads * sc->cap * 4);
+  if (rows) {
+    if (!(b->flags & ESG_FULL_ROWS)) return fail(ESG_ERR_BAD_ARGUMENT, "batch has no rows");
+    memcpy(rows, b->h_rows, (size_t)b->n_q * sc->n_refs * 4);
+  }
+  return ESG_OK;
+}
+
+void esg_batch_free(esg_batch* b) {
+  if (!b) return;
+  esg_scorer* sc = b->owner;
+  if (sc) {
+    cudaSetDevice(sc->device);
+    if (b->done) {
+      cudaEventSynchronize(b->done);
+      cudaEventDestroy(b->done);
+    }
+    if (b->d_mem) cudaFreeAsync(b->d_mem, sc->stream);
+    sc->pinned.put(b->in_buf.p, b->in_buf.cap);
+    sc->pinned.put(b->out_buf.p, b->out_buf.cap);
+  }
+  delete b;
+}
+
+esg_status esg_batch_stats_get(const esg_batch* b, esg_batch_stats* out) {
+  if (!b || !out) return fail(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  *out = b->stats;
+  return ESG_OK;
+}
+
+esg_status esg_score_batch(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                           const uint32_t* len, uint32_t n_reads, uint32_t flags,
+                           esg_read_result* results, uint32_t* ties, int32_t* rows) {
+  esg_batch* b = nullptr;
+  esg_status s = esg_prepare(sc, codes, off, len, n_reads, flags, &b);
+  if (s != ESG_OK) return s;
+  s = esg_submit(sc, b);
+  if (s == ESG_OK) s = esg_finish(sc, b, results, ties, rows);
+  const std::string keep = g_err;
+  esg_batch_free(b);
+  g_err = keep;
+  return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,681 @@
+// esg_kernels.cuh -- device code of the B200 panel scorer (sm_100a).
+//
+// Four kernels, launched in this order on one stream per batch:
+//
+//   k2_batched   the product: every (query, reference pair) of the panel in
+//                int16x2 lanes.  One warp is a 32-lane systolic array: each
+//                lane holds a 16-row stripe of one query (H, E and the
+//                row's substitution table in registers) and walks the
+//                columns of a reference pair; the stripe's bottom row goes
+//                to the next lane by shuffle, so no DP state ever leaves the
+//                register file.  The two 16-bit halves of every register are
+//                two references (a length-sorted pair).  Substitution is one
+//                PRMT per cell pair, the recurrence three VIADDMNMX and one
+//                VIMNMX (DPX) plus one packed add.  The argmax / tie / XS
+//                reduction is folded in per query, online, in shared memory.
+//                Pairs that may have left int16 are flagged and their query
+//                is re-scored by the int32 kernel.
+//   k3_plain     one thread per (query, reference), int32, the recurrence of
+//                crates/eschalign/src/scalar.rs:120-163 over 16-row register
+//                stripes with the stripe boundary in global scratch.  The
+//                comparison arm, and the exact path for what k2 cannot take.
+//   k4_rows      per-query reduction of k3's rows (mapper.rs:444-472).
+//   k5_merge     per read: forward and reverse-complement query states
+//                merged into the read's result.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace esg {
+
+constexpr int kRows = 16;             // rows per lane stripe (k2)
+constexpr int kMaxStripes = 32;       // a query spans at most one warp (k2)
+constexpr int kNeg16 = -30000;        // int16 stand-in for -infinity
+constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
+constexpr int kK2Warps = 8;           // warps per k2 CTA
+constexpr int kK2Threads = kK2Warps * 32;
+constexpr int kK3Threads = 256;
+constexpr uint32_t kFull = 0xffffffffu;
+constexpr uint32_t kNoRef = 0xffffffffu;
+
+// error bits in counters[2]
+constexpr uint32_t kErrPanelWait = 1u;
+constexpr uint32_t kErrRedoOverflow = 2u;
+
+// query-state flags (device side, mirrored into esg_read_result.flags)
+constexpr int kQRedo = 8;       // k2 flagged a pair; the query is re-scored by k3
+constexpr int kQRescored = 4;   // == ESG_RESULT_RESCORED32
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+  return d;
+}
+__device__ __forceinline__ uint32_t add16x2(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("add.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+__device__ __forceinline__ uint32_t max16x2(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("max.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+__device__ __forceinline__ int lo16(uint32_t v) { return (int)(int16_t)(v & 0xffffu); }
+__device__ __forceinline__ int hi16(uint32_t v) { return ((int)v) >> 16; }
+__host__ __device__ __forceinline__ uint32_t pack16x2(int lo, int hi) {
+  return (uint32_t)(uint16_t)(int16_t)lo | ((uint32_t)(uint16_t)(int16_t)hi << 16);
+}
+
+// Online reduction of one query's candidates (mapper.rs:444-472): best, XS,
+// n_tied counted in full, and the `cap` smallest tie candidates in order.
+// Candidates may arrive in any order; the result does not depend on it.
+// slot = {best, suboptimal, n_tied, flags}; ties = cap entries.
+__device__ __forceinline__ void slot_add(int* slot, uint32_t* ties, uint32_t cap, uint32_t idx,
+                                         int score) {
+  const int best = slot[0];
+  if (score > best) {
+    if (slot[2] > 0) slot[1] = max(slot[1], best);
+    slot[0] = score;
+    slot[2] = 1;
+    ties[0] = idx;
+  } else if (score == best) {
+    const uint32_t n = (uint32_t)slot[2];
+    slot[2] = (int)(n + 1);
+    const uint32_t listed = n < cap ? n : cap;
+    if (listed < cap || idx < ties[cap - 1]) {
+      uint32_t pos = listed < cap ? listed : cap - 1;
+      while (pos > 0 && ties[pos - 1] > idx) {
+        ties[pos] = ties[pos - 1];
+        --pos;
+      }
+      ties[pos] = idx;
+    }
+  } else {
+    slot[1] = max(slot[1], score);
+  }
+}
+
+// ---------------------------------------------------------------- k2
+struct K2Params {
+  // panel blob: n_pairs uint4 {sel offset, mA | mB << 16, refA, refB} then the
+  // 16-bit PRMT selectors of every pair's columns
+  const uint4* blob;
+  uint32_t blob_bytes;   // multiple of 16
+  uint32_t n_pairs;
+  uint32_t sel_base;     // uint16 index of the first selector in the blob
+  // reads (codes 0..4); query q < n_reads is read q forward, else the
+  // reverse complement of read q - n_reads
+  const uint8_t* codes;
+  const uint64_t* off;
+  const uint32_t* len;
+  uint32_t n_reads;
+  // work tiles: tasks[t] = {start in order[], count | smax << 16}
+  const uint32_t* order;
+  const uint2* tasks;
+  uint32_t n_tasks;
+  uint32_t* counters;    // [0] task counter, [1] redo count, [2] error bits
+  // outputs
+  int4* qhead;           // per query {best, suboptimal, n_tied, flags}
+  uint32_t* qties;       // per query cap candidates
+  int32_t* rows;         // optional [q * n_refs + r]
+  uint32_t n_refs;
+  uint32_t* redo_list;   // k3 list; redo entries go after redo_base
+  uint32_t redo_base;
+  uint32_t redo_cap;
+  // scoring, pre-shifted by the gap open (see k2_batched)
+  uint32_t tab_a[6];
+  uint32_t tab_b[6];
+  uint32_t o2, e2;
+  int32_t o;
+  int32_t sat;           // local: a best at or above this may have wrapped
+  uint32_t cap;
+};
+
+// Bounded wait on an mbarrier phase (a TMA bulk copy's completion).  Gives
+// up after ~2^26 polls, setting an error bit the host reads.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_t* err) {
+  const uint32_t addr = (uint32_t)__cvta_generic_to_shared(bar);
+  for (uint32_t it = 0; it < (1u << 26); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  atomicOr(err, kErrPanelWait);
+  return false;
+}
+
+// Stage the panel blob into shared memory with TMA bulk copies (no
+// multicast): one thread arms an mbarrier with the byte count and issues
+// cp.async.bulk in chunks; every thread waits on the phase.
+__device__ __forceinline__ bool stage_panel(void* smem, const void* gsrc, uint32_t bytes,
+                                            uint64_t* bar, uint32_t* err) {
+  const uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes)
+                 : "memory");
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem);
+    const char* src = (const char*)gsrc;
+    constexpr uint32_t kChunk = 32768;
+    for (uint32_t at = 0; at < bytes; at += kChunk) {
+      const uint32_t n = (bytes - at) < kChunk ? (bytes - at) : kChunk;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              dst + at),
+          "l"(src + at), "r"(n), "r"(bar_a)
+          : "memory");
+    }
+  }
+  const bool ok = mbar_wait(bar, 0, err);
+  __syncthreads();
+  return ok;
+}
+
+// One warp, one task: up to 32 queries whose stripes fill the warp's lanes,
+// scored against every reference pair of the panel.
+//
+// Lane state (rows r = 0..15 of the lane's stripe):
+//   ta[r], tb[r]  PRMT tables of the row's read code c: byte x of {tb, ta} is
+//                 s(c, x) - o for reference code x = 0..3, 4 (wildcard), and
+//                 a padding column's score at x = 5.  Both halves of a
+//                 register use the same table; the column's selector picks a
+//                 byte per half and sign-extends it to 16 bits.
+//   ho[r]         H + o of the row at the previous column (both halves)
+//   e[r]          E of the row at the previous column
+// Keeping H + o instead of H lets one packed add per cell feed both the E
+// of the next column and the F of the next row: the diagonal term is then
+// (H_diag + o) + (s - o), which is why the tables hold s - o.
+//
+// A query of n rows takes S = ceil(n / 16) lanes; its stripes are aligned so
+// the read's last row is row 15 of its last lane, and the P = 16 S - n rows
+// before the read's first row score 0 against every real column: they hold
+// H = 0 exactly, the top border the first real row needs, in both modes.
+// Lane l with stripe index s works on column j = t - s at step t; its top
+// input (H + o and F of the row above) is lane l-1's bottom output of step
+// t-1, fetched by shuffle; a query's first lane takes the border instead.
+template <bool kLocal, bool kPanelW, bool kSmemPanel>
+__global__ void __launch_bounds__(kK2Threads, 2) k2_batched(const K2Params P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint64_t panel_bar;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const uint32_t cap = P.cap;
+
+  const uint4* pairs;
+  const uint16_t* sels;
+  int* slots;
+  if constexpr (kSmemPanel) {
+    if (!stage_panel(smem_raw, P.blob, P.blob_bytes, &panel_bar, &P.counters[2])) return;
+    pairs = reinterpret_cast<const uint4*>(smem_raw);
+    sels = reinterpret_cast<const uint16_t*>(smem_raw) + P.sel_base;
+    slots = reinterpret_cast<int*>(smem_raw + P.blob_bytes);
+  } else {
+    pairs = P.blob;
+    sels = reinterpret_cast<const uint16_t*>(P.blob) + P.sel_base;
+    slots = reinterpret_cast<int*>(smem_raw);
+  }
+  // this lane's query slot: {best, suboptimal, n_tied, flags, ties[cap]}
+  int* slot = slots + (size_t)(wib * 32 + lane) * (4 + cap);
+  uint32_t* sties = reinterpret_cast<uint32_t*>(slot + 4);
+
+  const uint32_t o2 = P.o2, e2 = P.e2;
+  const uint32_t neg2 = pack16x2(kNeg16, kNeg16);
+
+  for (;;) {
+    uint32_t task = 0;
+    if (lane == 0) task = atomicAdd(&P.counters[0], 1u);
+    task = __shfl_sync(kFull, task, 0);
+    if (task >= P.n_tasks) break;
+    const uint2 tk = P.tasks[task];
+    const uint32_t count = tk.y & 0xffffu;
+    const int smax = (int)(tk.y >> 16);
+
+    // --- which query and stripe this lane holds
+    uint32_t kq = 0, kn = 0, kS = 0;
+    if ((uint32_t)lane < count) {
+      kq = P.order[tk.x + lane];
+      const uint32_t rd = kq < P.n_reads ? kq : kq - P.n_reads;
+      kn = P.len[rd];
+      kS = (kn + kRows - 1) / kRows;
+    }
+    uint32_t incl = kS;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(kFull, incl, d);
+      if (lane >= d) incl += v;
+    }
+    uint32_t qid = 0, n = 0;
+    int s = 1 << 20, S = 0;  // lanes past the task's queries never become active
+    bool valid = false;
+    for (uint32_t k = 0; k < count; ++k) {
+      const uint32_t ek = __shfl_sync(kFull, incl, k);
+      const uint32_t sk = __shfl_sync(kFull, kS, k);
+      const uint32_t qk = __shfl_sync(kFull, kq, k);
+      const uint32_t nk = __shfl_sync(kFull, kn, k);
+      if ((uint32_t)lane >= ek - sk && (uint32_t)lane < ek) {
+        qid = qk;
+        n = nk;
+        s = lane - (int)(ek - sk);
+        S = (int)sk;
+        valid = true;
+      }
+    }
+    const bool first = valid ? (s == 0) : true;
+    const bool last = valid && (s == S - 1);
+    const int pad = valid ? S * kRows - (int)n : 0;
+    const bool rc = qid >= P.n_reads;
+    const uint32_t rd = rc ? qid - P.n_reads : qid;
+
+    // --- the stripe's row tables
+    uint32_t ta[kRows];
+    uint32_t tb[kPanelW ? kRows : 1];
+    {
+      const uint8_t* q = valid ? P.codes + P.off[rd] : P.codes;
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int i = s * kRows + r - pad;
+        uint32_t c = 5;  // padding row
+        if (valid && i >= 0) {
+          uint32_t x = rc ? q[n - 1 - i] : q[i];
+          x = x > 4 ? 4 : x;
+          c = (rc && x < 4) ? 3 - x : x;
+        }
+        ta[r] = P.tab_a[c];
+        if constexpr (kPanelW) tb[r] = P.tab_b[c];
+      }
+      if constexpr (!kPanelW) tb[0] = P.tab_b[0];
+    }
+    // rows of the read's top padding (first lane only): excluded from the
+    // semi-global last-column maximum
+    const uint32_t padmask = (valid && first) ? ((1u << pad) - 1u) : 0u;
+
+    if (last) {
+      slot[0] = INT32_MIN;
+      slot[1] = INT32_MIN;
+      slot[2] = 0;
+      slot[3] = 0;
+    }
+
+    for (uint32_t p = 0; p < P.n_pairs; ++p) {
+      const uint4 pm = pairs[p];
+      const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);
+      const int m = max(mA, mB);
+      const int mshort = min(mA, mB);
+      const int jshort = (mB > 0 && mshort < m) ? mshort - 1 : -1;
+      const uint16_t* sp = sels + pm.x;
+      const int steps = m + smax - 1;
+
+      uint32_t ho[kRows], ev[kRows];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        ho[r] = o2;
+        ev[r] = neg2;
+      }
+      uint32_t hdc = o2;              // H + o of the row above, previous column
+      uint32_t hobot = o2, fbot = neg2;
+      uint32_t best = 0;              // local: max H over this lane's cells
+      uint32_t lastrow = neg2;        // semi-global: max H of row 15 over columns
+      uint32_t s_col = neg2, s_last = neg2;  // semi-global short-half snapshot
+
+#pragma unroll 1
+      for (int t = 0; t < steps; ++t) {
+        const int j = t - s;
+        uint32_t hot = __shfl_up_sync(kFull, hobot, 1);
+        uint32_t ft = __shfl_up_sync(kFull, fbot, 1);
+        if (first) {
+          hot = o2;
+          ft = neg2;
+        }
+        if ((unsigned)j < (unsigned)m) {
+          const uint32_t sel = sp[j];
+          uint32_t hd = hdc;
+          hdc = hot;
+          uint32_t hup = hot, f = ft, hprev = 0, h15 = 0;
+#pragma unroll
+          for (int r = 0; r < kRows; ++r) {
+            const uint32_t sc = prmt(ta[r], tb[kPanelW ? r : 0], sel);
+            ev[r] = __viaddmax_s16x2(ev[r], e2, ho[r]);
+            f = __viaddmax_s16x2(f, e2, hup);
+            const uint32_t h1 = __viaddmax_s16x2(hd, sc, ev[r]);
+            uint32_t h;
+            if constexpr (kLocal) {
+              h = __vimax_s16x2_relu(h1, f);
+            } else {
+              h = max16x2(h1, f);
+            }
+            hd = ho[r];
+            ho[r] = add16x2(h, o2);
+            hup = ho[r];
+            if constexpr (kLocal) {
+              if (r & 1)
+                best = __vimax3_s16x2(best, hprev, h);
+              else
+                hprev = h;
+            }
+            if (r == kRows - 1) h15 = h;
+          }
+          hobot = ho[kRows - 1];
+          fbot = f;
+          if constexpr (!kLocal) {
+            lastrow = max16x2(lastrow, h15);
+            if (j == jshort) {
+              uint32_t cm = neg2;
+#pragma unroll
+              for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? neg2 : ho[r]);
+              s_col = cm;
+              s_last = lastrow;
+            }
+          }
+        }
+      }
+
+      // --- per-query scores of this pair, to the query's last lane
+      uint32_t v, lr = 0;
+      if constexpr (kLocal) {
+        v = best;
+      } else {
+        uint32_t cm = neg2;
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? neg2 : ho[r]);
+        lr = lastrow;
+        if (jshort >= 0) {
+          // the short half's last column and last row were taken at its end
+          if (mA < mB) {
+            cm = (cm & 0xffff0000u) | (s_col & 0xffffu);
+            lr = (lr & 0xffff0000u) | (s_last & 0xffffu);
+          } else {
+            cm = (cm & 0xffffu) | (s_col & 0xffff0000u);
+            lr = (lr & 0xffffu) | (s_last & 0xffff0000u);
+          }
+        }
+        v = cm;
+      }
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t w = __shfl_up_sync(kFull, v, d);
+        if (s >= d) v = max16x2(v, w);
+      }
+      if (last) {
+        int scA, scB;
+        if constexpr (kLocal) {
+          scA = lo16(v);
+          scB = hi16(v);
+          if (scA >= P.sat || (mB > 0 && scB >= P.sat)) slot[3] |= kQRedo;
+        } else {
+          scA = max(lo16(v) - P.o, lo16(lr));
+          scB = max(hi16(v) - P.o, hi16(lr));
+        }
+        const uint32_t rbit = rc ? 1u : 0u;
+        slot_add(slot, sties, cap, (pm.z << 1) | rbit, scA);
+        if (P.rows) P.rows[(size_t)qid * P.n_refs + pm.z] = scA;
+        if (pm.w != kNoRef) {
+          slot_add(slot, sties, cap, (pm.w << 1) | rbit, scB);
+          if (P.rows) P.rows[(size_t)qid * P.n_refs + pm.w] = scB;
+        }
+      }
+    }
+
+    // --- flush the query states of this task
+    if (last) {
+      const int fl = slot[3];
+      P.qhead[qid] = make_int4(slot[0], slot[1], slot[2], fl);
+      const uint32_t nl = min((uint32_t)slot[2], cap);
+      for (uint32_t k = 0; k < nl; ++k) P.qties[(size_t)qid * cap + k] = sties[k];
+      if (fl & kQRedo) {
+        const uint32_t at = atomicAdd(&P.counters[1], 1u);
+        if (at < P.redo_cap)
+          P.redo_list[P.redo_base + at] = qid;
+        else
+          atomicOr(&P.counters[2], kErrRedoOverflow);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- k3
+struct K3Params {
+  const uint8_t* codes;
+  const uint64_t* off;
+  const uint32_t* len;
+  uint32_t n_reads;
+  // references in longest-first order: slot k is panel reference ridx[k]
+  const uint8_t* rcodes;
+  const uint32_t* roff;
+  const uint32_t* rlen;
+  const uint32_t* ridx;
+  uint32_t n_refs;
+  const uint32_t* list;        // queries to score
+  uint32_t host_count;
+  const uint32_t* redo_count;  // device count of entries after host_count (may be null)
+  uint32_t redo_cap;           // list capacity after host_count
+  int32_t* out;                // [pos * n_refs + r], panel order
+  int32_t* rows;               // optional [q * n_refs + r]
+  int2* scratch;               // stripe boundary, [col * threads + tid]
+  int32_t ma, mi, o, e;
+  int local;
+};
+
+__device__ __forceinline__ uint32_t code_mask(uint32_t c) { return c < 4 ? 1u << c : 0xfu; }
+
+template <bool kLocal, bool kTail>
+__device__ __forceinline__ void k3_stripe(const uint8_t* __restrict__ rc_codes, int m,
+                                          const uint32_t (&qm)[kRows], int rows, bool first,
+                                          int2* __restrict__ bnd, size_t bstride, int ma, int mi,
+                                          int o, int e, int& best) {
+  int H[kRows], E[kRows];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    H[r] = 0;
+    E[r] = kNeg32;
+  }
+  int diag_top = 0;
+  for (int j = 0; j < m; ++j) {
+    const uint32_t rm = code_mask(__ldg(rc_codes + j));
+    int hup, f;
+    if (first) {
+      hup = 0;
+      f = kNeg32;
+    } else {
+      const int2 b = bnd[(size_t)j * bstride];
+      hup = b.x;
+      f = b.y;
+    }
+    int hdiag = diag_top;
+    diag_top = hup;
+    int last = kNeg32;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const int hleft = H[r];
+      const int ev = max(hleft + o, E[r] + e);
+      E[r] = ev;
+      f = max(hup + o, f + e);
+      const int sc = (qm[r] & rm) ? ma : mi;
+      int h = max(max(hdiag + sc, ev), f);
+      if (kLocal) h = max(h, 0);
+      hdiag = hleft;
+      H[r] = h;
+      hup = h;
+      if (kLocal) {
+        if (!kTail || r < rows) best = max(best, h);
+      } else if (kTail) {
+        if (r == rows - 1) last = h;
+      }
+    }
+    if (!kTail) bnd[(size_t)j * bstride] = make_int2(hup, f);
+    if (!kLocal && kTail) best = max(best, last);
+  }
+  if (!kLocal) {
+#pragma unroll
+    for (int r = 0; r < kRows; ++r)
+      if (!kTail || r < rows) best = max(best, H[r]);
+  }
+}
+
+template <bool kLocal>
+__global__ void __launch_bounds__(kK3Threads) k3_plain(const K3Params P) {
+  const uint32_t n_list = P.host_count + (P.redo_count ? min(*P.redo_count, P.redo_cap) : 0u);
+  const uint64_t total = (uint64_t)n_list * P.n_refs;
+  const size_t nthreads = (size_t)gridDim.x * blockDim.x;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int2* bnd = P.scratch + tid;
+  for (uint64_t idx = tid; idx < total; idx += nthreads) {
+    const uint32_t pos = (uint32_t)(idx / P.n_refs);
+    const uint32_t k = (uint32_t)(idx % P.n_refs);
+    const uint32_t q = P.list[pos];
+    const bool rc = q >= P.n_reads;
+    const uint32_t rd = rc ? q - P.n_reads : q;
+    const int n = (int)P.len[rd];
+    const uint8_t* qc = P.codes + P.off[rd];
+    const int m = (int)P.rlen[k];
+    const uint8_t* rcodes = P.rcodes + P.roff[k];
+    int best = kLocal ? 0 : kNeg32;
+    for (int i0 = 0; i0 < n; i0 += kRows) {
+      uint32_t qm[kRows];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int i = i0 + r;
+        uint32_t c = 0xffu;
+        if (i < n) {
+          uint32_t x = rc ? qc[n - 1 - i] : qc[i];
+          x = x > 4 ? 4 : x;
+          c = (rc && x < 4) ? 3 - x : x;
+        }
+        qm[r] = c == 0xffu ? 0u : code_mask(c);
+      }
+      const int rows = min(kRows, n - i0);
+      const bool first = i0 == 0;
+      if (i0 + kRows >= n)
+        k3_stripe<kLocal, true>(rcodes, m, qm, rows, first, bnd, nthreads, P.ma, P.mi, P.o, P.e,
+                                best);
+      else
+        k3_stripe<kLocal, false>(rcodes, m, qm, rows, first, bnd, nthreads, P.ma, P.mi, P.o,
+                                 P.e, best);
+    }
+    if (n == 0) best = 0;
+    const uint32_t ref = P.ridx[k];
+    P.out[(size_t)pos * P.n_refs + ref] = best;
+    if (P.rows) P.rows[(size_t)q * P.n_refs + ref] = best;
+  }
+}
+
+// ---------------------------------------------------------------- k4
+struct K4Params {
+  const uint32_t* list;
+  uint32_t host_count;
+  const uint32_t* redo_count;
+  uint32_t redo_cap;
+  const int32_t* rows;  // k3 output, [pos * n_refs + r]
+  uint32_t n_refs;
+  uint32_t n_reads;
+  int4* qhead;
+  uint32_t* qties;
+  uint32_t cap;
+};
+
+// One warp per listed query: mapper.rs:444-472 over its row.
+__global__ void __launch_bounds__(256) k4_rows(const K4Params P) {
+  const uint32_t n_list = P.host_count + (P.redo_count ? min(*P.redo_count, P.redo_cap) : 0u);
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t pos = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; pos < n_list; pos += warps) {
+    const uint32_t q = P.list[pos];
+    const uint32_t rbit = q >= P.n_reads ? 1u : 0u;
+    const int32_t* row = P.rows + (size_t)pos * P.n_refs;
+    int best = INT32_MIN;
+    for (uint32_t r = lane; r < P.n_refs; r += 32) best = max(best, row[r]);
+#pragma unroll
+    for (int d = 16; d; d >>= 1) best = max(best, __shfl_xor_sync(kFull, best, d));
+    int sub = INT32_MIN;
+    uint32_t n_tied = 0, listed = 0;
+    for (uint32_t base = 0; base < P.n_refs; base += 32) {
+      const uint32_t r = base + lane;
+      const int v = r < P.n_refs ? row[r] : INT32_MIN;
+      const bool tie = r < P.n_refs && v == best;
+      if (r < P.n_refs && !tie) sub = max(sub, v);
+      const uint32_t bal = __ballot_sync(kFull, tie);
+      if (tie) {
+        const uint32_t rank = listed + __popc(bal & ((1u << lane) - 1u));
+        if (rank < P.cap) P.qties[(size_t)q * P.cap + rank] = (r << 1) | rbit;
+      }
+      listed += __popc(bal);
+      n_tied += __popc(bal);
+    }
+#pragma unroll
+    for (int d = 16; d; d >>= 1) sub = max(sub, __shfl_xor_sync(kFull, sub, d));
+    if (lane == 0) P.qhead[q] = make_int4(best, sub, (int)n_tied, kQRescored);
+  }
+}
+
+// ---------------------------------------------------------------- k5
+struct K5Params {
+  const uint32_t* len;
+  uint32_t n_reads;
+  int both;
+  const int4* qhead;
+  const uint32_t* qties;
+  uint32_t cap;
+  int4* results;       // esg_read_result layout
+  uint32_t* ties;      // [read * cap + k]
+};
+
+__global__ void __launch_bounds__(256) k5_merge(const K5Params P) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < P.n_reads;
+       r += gridDim.x * blockDim.x) {
+    const uint32_t cap = P.cap;
+    uint32_t* out_t = P.ties + (size_t)r * cap;
+    if (P.len[r] == 0) {
+      P.results[r] = make_int4(INT32_MIN, INT32_MIN, 0, 1 /* ESG_RESULT_EMPTY */);
+      continue;
+    }
+    const int4 a = P.qhead[r];
+    const uint32_t* ta = P.qties + (size_t)r * cap;
+    int best = a.x, sub = a.y, flags = a.w & kQRescored;
+    uint32_t n_tied = (uint32_t)a.z;
+    if (!P.both) {
+      const uint32_t nl = min(n_tied, cap);
+      for (uint32_t k = 0; k < nl; ++k) out_t[k] = ta[k];
+    } else {
+      const uint32_t qb = P.n_reads + r;
+      const int4 b = P.qhead[qb];
+      const uint32_t* tb = P.qties + (size_t)qb * cap;
+      flags |= b.w & kQRescored;
+      const uint32_t na = min((uint32_t)a.z, cap), nb = min((uint32_t)b.z, cap);
+      if (a.x > b.x) {
+        sub = max(max(a.y, b.y), b.x);
+        for (uint32_t k = 0; k < na; ++k) out_t[k] = ta[k];
+      } else if (b.x > a.x) {
+        best = b.x;
+        n_tied = (uint32_t)b.z;
+        sub = max(max(a.y, b.y), a.x);
+        for (uint32_t k = 0; k < nb; ++k) out_t[k] = tb[k];
+      } else {
+        n_tied = (uint32_t)a.z + (uint32_t)b.z;
+        sub = max(a.y, b.y);
+        uint32_t i = 0, k2 = 0, w = 0;
+        while (w < cap && (i < na || k2 < nb)) {
+          if (k2 >= nb || (i < na && ta[i] < tb[k2]))
+            out_t[w++] = ta[i++];
+          else
+            out_t[w++] = tb[k2++];
+        }
+      }
+    }
+    if (n_tied > cap) flags |= 2;  // ESG_RESULT_TIES_TRUNCATED
+    P.results[r] = make_int4(best, sub, (int)n_tied, flags);
+  }
+}
+
+}  // namespace esg

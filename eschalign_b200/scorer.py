@@ -1,0 +1,350 @@
+"""Host mirror of eschalign's GPU scorer (crates/eschalign/src/cuda/mod.rs:328-709).
+
+Same names, argument meaning and error behaviour as the Rust ``GpuScorer``:
+
+* :meth:`GpuScorer.new` / :meth:`GpuScorer.new_on_device` lay a panel out on
+  a device under one scoring and one mode (cuda/mod.rs:345-443) and raise
+  :class:`GpuError` where the reference returns ``Err(GpuError)``;
+* :meth:`GpuScorer.score_batch` = :meth:`prepare` + :meth:`submit` +
+  :meth:`finish` (cuda/mod.rs:524-708), ``prepare`` touching no device
+  state so it can overlap a running batch.
+
+What a batch returns differs by design: the reference hands back a full
+``ScoreMatrix`` (mapper.rs:95-139) for the CPU to reduce; here each read's
+best score, suboptimal score (XS), tie count and first tie candidates come
+back reduced on the device (mapper.rs:444-472), and the full rows only when
+asked for.  Every read is scored on the GPU -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from .panel import Panel
+from .scoring import Mode, Scoring
+
+NO_SCORE = -(2**31)
+RESULT_EMPTY = 1
+RESULT_TIES_TRUNCATED = 2
+RESULT_RESCORED32 = 4
+
+KERNEL_AUTO = 0
+KERNEL_PLAIN32 = 1
+BOTH_STRANDS = 1
+FULL_ROWS = 2
+
+RESULT_DTYPE = np.dtype([("best", "<i4"), ("suboptimal", "<i4"),
+                         ("n_tied", "<u4"), ("flags", "<u4")])
+
+_STATUS = {
+    1: "Unavailable", 2: "Driver", 3: "ReferenceTooLong", 4: "ScoringInvalid",
+    5: "EmptyPanel", 6: "EmptyReference", 7: "BadArgument", 8: "OutOfMemory", 9: "Timeout",
+}
+
+
+class GpuError(RuntimeError):
+    """GpuError (cuda/mod.rs:144-153) and the panel/scoring refusals of
+    AlignError (error.rs:7-28), with the C status code."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.kind = _STATUS.get(status, "Unknown")
+        super().__init__(f"{self.kind}: {message}")
+
+
+def _check(lib, st: int):
+    if st != 0:
+        raise GpuError(st, lib.esg_last_error().decode(errors="replace"))
+
+
+def _ptr(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def pack_reads(reads):
+    """A list of code arrays -> contiguous (codes u8, off u64, len u32)."""
+    lens = np.fromiter((len(r) for r in reads), dtype=np.uint32, count=len(reads))
+    off = np.zeros(len(reads), dtype=np.uint64)
+    if len(reads) > 1:
+        off[1:] = np.cumsum(lens[:-1], dtype=np.uint64)
+    if lens.sum():
+        codes = np.concatenate([np.asarray(r, dtype=np.uint8) for r in reads])
+    else:
+        codes = np.zeros(1, dtype=np.uint8)
+    return np.ascontiguousarray(codes), off, lens
+
+
+def device_visible() -> bool:
+    """cuda/mod.rs:130-140."""
+    lib = _native.load()
+    n = C.c_int32(0)
+    lib.esg_device_count(C.byref(n))
+    return n.value > 0
+
+
+def fits_i16(n: int, max_ref_len: int, scoring: Scoring) -> bool:
+    """simd/mod.rs:222-227 (the reference's SIMD/GPU admission bound)."""
+    lib = _native.load()
+    s = _native.EsgScoring(*scoring.astuple())
+    return bool(lib.esg_fits_i16(n, max_ref_len, C.byref(s)))
+
+
+class ScoreMatrix:
+    """mapper.rs:95-139: row-major scores, row k = query k in panel order.
+    Every row is scored here (int32, so scores past int16 are kept)."""
+
+    def __init__(self, n_refs: int, scores: np.ndarray, scored: np.ndarray):
+        assert scores.shape == (scored.size, n_refs)
+        self._n_refs = n_refs
+        self.scores = scores
+        self.scored = scored
+
+    def __len__(self):
+        return self.scored.size
+
+    def n_refs(self) -> int:
+        return self._n_refs
+
+    def n_scored(self) -> int:
+        return int(self.scored.sum())
+
+    def row(self, k: int):
+        return self.scores[k] if self.scored[k] else None
+
+
+@dataclass
+class ReadScores:
+    best: int | None
+    suboptimal: int | None
+    n_tied: int
+    ties: list          # (reference, reverse) in tie order, at most tie_capacity
+    truncated: bool
+    rescored32: bool
+
+
+class BatchResult:
+    """Per-read reduction of one batch (+ optional rows)."""
+
+    def __init__(self, results, ties, rows, n_refs, stats, cap):
+        self.results = results
+        self.ties = ties
+        self.rows = rows
+        self.n_refs = n_refs
+        self.stats = stats
+        self.cap = cap
+
+    def __len__(self):
+        return self.results.size
+
+    @property
+    def best(self):
+        return self.results["best"]
+
+    @property
+    def suboptimal(self):
+        return self.results["suboptimal"]
+
+    @property
+    def n_tied(self):
+        return self.results["n_tied"]
+
+    @property
+    def flags(self):
+        return self.results["flags"]
+
+    def read(self, k: int) -> ReadScores:
+        r = self.results[k]
+        if r["flags"] & RESULT_EMPTY:
+            return ReadScores(None, None, 0, [], False, False)
+        n = min(int(r["n_tied"]), self.cap)
+        ties = [(int(c) >> 1, bool(int(c) & 1)) for c in self.ties[k, :n]]
+        sub = None if r["suboptimal"] == NO_SCORE else int(r["suboptimal"])
+        return ReadScores(int(r["best"]), sub, int(r["n_tied"]), ties,
+                          bool(r["flags"] & RESULT_TIES_TRUNCATED),
+                          bool(r["flags"] & RESULT_RESCORED32))
+
+    def matrix(self) -> ScoreMatrix | None:
+        if self.rows is None:
+            return None
+        return ScoreMatrix(self.n_refs, self.rows, np.ones(self.rows.shape[0], dtype=bool))
+
+
+class PreparedBatch:
+    """cuda/mod.rs:711-728: a batch planned on the host."""
+
+    def __init__(self, scorer, handle, n_reads, flags, keep):
+        self._scorer = scorer
+        self._h = handle
+        self.n_reads = n_reads
+        self.flags = flags
+        self._keep = keep
+
+    def stats(self) -> dict:
+        st = _native.EsgBatchStats()
+        _check(self._scorer._lib, self._scorer._lib.esg_batch_stats_get(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def work_split(self):
+        """cuda/mod.rs:723-727: (queries on the int16x2 kernel, on int32)."""
+        s = self.stats()
+        return s["queries_batched"], s["queries_plain"]
+
+    def free(self):
+        if self._h:
+            self._scorer._lib.esg_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+PendingBatch = PreparedBatch
+
+
+class GpuScorer:
+    """A panel resident on a device under one scoring and one mode."""
+
+    def __init__(self, panel: Panel, scoring: Scoring, mode: Mode, device: int = 0,
+                 tie_capacity: int = 8, kernel: int = KERNEL_AUTO, stream: int | None = None):
+        self._lib = _native.load()
+        self._h = None
+        if not isinstance(panel, Panel):
+            panel = Panel.from_codes(panel)
+        self.panel = panel
+        self.scoring = scoring
+        self.mode = Mode(mode)
+        self.cap = int(tie_capacity)
+        codes, off, lens = panel.packed()
+        self._panel_arrays = (codes, off, lens)
+        sc = _native.EsgScoring(*scoring.astuple())
+        opts = _native.EsgOptions(self.cap, int(kernel), stream)
+        h = C.c_void_p()
+        st = self._lib.esg_scorer_new(int(device), _ptr(codes, C.c_uint8), _ptr(off, C.c_uint64),
+                                      _ptr(lens, C.c_uint32), len(panel), C.byref(sc),
+                                      int(self.mode), C.byref(opts), C.byref(h))
+        _check(self._lib, st)
+        self._h = h
+
+    # -- cuda/mod.rs:345-350
+    @classmethod
+    def new(cls, panel, scoring, mode, **kw):
+        return cls(panel, scoring, mode, device=0, **kw)
+
+    @classmethod
+    def new_on_device(cls, ordinal, panel, scoring, mode, **kw):
+        return cls(panel, scoring, mode, device=ordinal, **kw)
+
+    def close(self):
+        if self._h:
+            self._lib.esg_scorer_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- introspection (cuda/mod.rs:446-514)
+    def info(self) -> dict:
+        inf = _native.EsgInfo()
+        _check(self._lib, self._lib.esg_scorer_info(self._h, C.byref(inf)))
+        d = {k: getattr(inf, k) for k, _ in inf._fields_}
+        d["device_name"] = inf.device_name.decode()
+        return d
+
+    def device_name(self) -> str:
+        return self.info()["device_name"]
+
+    def geometry(self):
+        i = self.info()
+        return (i["batched_threads"], i["n_ref_pairs"], i["batched_blocks"])
+
+    def registers(self):
+        return self.info()["regs_batched"]
+
+    def local_bytes(self):
+        return self.info()["local_bytes_batched"]
+
+    def set_kernel(self, kernel: int):
+        _check(self._lib, self._lib.esg_scorer_set_kernel(self._h, int(kernel)))
+
+    def set_plain(self, plain: bool):
+        """The A/B lever (GpuScorer::set_half2, cuda/mod.rs:500): every
+        query on the plain int32 kernel, or the batched kernel where it can."""
+        self.set_kernel(KERNEL_PLAIN32 if plain else KERNEL_AUTO)
+
+    def scores_len(self, n: int) -> bool:
+        return bool(self._lib.esg_scores_len(self._h, n))
+
+    # -- batches
+    def _inputs(self, reads):
+        if isinstance(reads, tuple) and len(reads) == 3:
+            codes, off, lens = reads
+            codes = np.ascontiguousarray(codes, dtype=np.uint8)
+            off = np.ascontiguousarray(off, dtype=np.uint64)
+            lens = np.ascontiguousarray(lens, dtype=np.uint32)
+            if codes.size == 0:
+                codes = np.zeros(1, dtype=np.uint8)
+            return codes, off, lens
+        return pack_reads(reads)
+
+    def prepare(self, reads, both_strands: bool = False, full_rows: bool = False) -> PreparedBatch:
+        codes, off, lens = self._inputs(reads)
+        flags = (BOTH_STRANDS if both_strands else 0) | (FULL_ROWS if full_rows else 0)
+        h = C.c_void_p()
+        _check(self._lib, self._lib.esg_prepare(self._h, _ptr(codes, C.c_uint8),
+                                                _ptr(off, C.c_uint64), _ptr(lens, C.c_uint32),
+                                                lens.size, flags, C.byref(h)))
+        return PreparedBatch(self, h, int(lens.size), flags, None)
+
+    def submit(self, batch: PreparedBatch) -> PendingBatch:
+        _check(self._lib, self._lib.esg_submit(self._h, batch._h))
+        return batch
+
+    def relaunch(self, batch: PendingBatch, stream: int | None = None):
+        _check(self._lib, self._lib.esg_relaunch(self._h, batch._h, stream))
+
+    def finish(self, batch: PendingBatch, keep: bool = False) -> BatchResult:
+        n = batch.n_reads
+        res = np.zeros(n, dtype=RESULT_DTYPE)
+        ties = np.zeros((n, self.cap), dtype=np.uint32)
+        rows = None
+        nq = n * (2 if batch.flags & BOTH_STRANDS else 1)
+        if batch.flags & FULL_ROWS:
+            rows = np.zeros((nq, len(self.panel)), dtype=np.int32)
+        _check(self._lib, self._lib.esg_finish(self._h, batch._h, res.ctypes.data,
+                                               _ptr(ties, C.c_uint32),
+                                               _ptr(rows, C.c_int32) if rows is not None else None))
+        stats = batch.stats()
+        if not keep:
+            batch.free()
+        return BatchResult(res, ties, rows, len(self.panel), stats, self.cap)
+
+    def score_batch(self, reads, both_strands: bool = False, full_rows: bool = False) -> BatchResult:
+        """cuda/mod.rs:524-528."""
+        return self.finish(self.submit(self.prepare(reads, both_strands, full_rows)))
+
+
+def select_hits(scores: ReadScores, min_score: int = 0, max_ties: int | None = None):
+    """The tie-set members a caller traces (mapper.rs:466-472): the first
+    min(n_tied, max_ties + 1) ties when best >= min_score, else none."""
+    if scores.best is None or scores.best < min_score:
+        return []
+    k = scores.n_tied if max_ties is None else min(scores.n_tied, max_ties + 1)
+    if k > len(scores.ties):
+        raise ValueError(f"{k} ties requested but only {len(scores.ties)} listed; "
+                         "raise tie_capacity or ask for full rows")
+    return scores.ties[:k]

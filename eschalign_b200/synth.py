@@ -1,0 +1,219 @@
+"""Seeded synthetic panels and reads with the shapes of the benchmark configs.
+
+They stand in for the reference's real samples (tRNA reads M1/M4 and the
+sacCer3 panel of benchmarks/README.md), which are not shipped: uniform ACGT
+references, reads cut from a random reference and mutated with the stated
+substitution / insertion / deletion rates (indel lengths geometric), plus a
+share of unrelated random reads.  Everything is vectorised numpy (PCG64 from
+a named seed), so a million reads take about a second and every machine
+builds the same bytes.
+
+Sizes:
+* ``panel_tiles``   164 references, lengths uniform 70-180 (C1, C2, C4)
+* ``reads_c1``      10 000 reads, 90 % cut from a reference (start 0-20,
+                    length 60-200 with a random 0-30 nt 3' tail), 8 % subs,
+                    2 % insertions, 1 % deletions; 10 % random of 60-200 nt
+* ``reads_c2``      1 000 000 reads, lengths lognormal (median 110, sigma
+                    0.4) clipped to 20-1000, same mutation model
+* ``panel_c3``      10 000 references of 300-1000 nt (GC 0.5)
+* ``reads_c3``      200 000 reads of 50-1000 nt, 70 % derived (10 % subs,
+                    3 % indels), 30 % random
+* ``pairs_c4``      2 x 150 nt mates, inserts lognormal (median 90) clipped
+                    to 40-600, adapter read-through past short inserts
+"""
+from __future__ import annotations
+
+import numpy as np
+
+TRUSEQ_R1 = b"AGATCGGAAGAGCACACGTCTGAACTCCAGTCA"  # crates/eschalign/src/adapter.rs:40
+TRUSEQ_R2 = b"AGATCGGAAGAGCGTCGTGTAGGGAAAGAGTGT"  # adapter.rs:42
+
+SEED_PANEL = 0x5EED_C1C2
+SEED_C1 = 0x5EED_0C01
+SEED_C2 = 0x5EED_0C02
+SEED_C3_PANEL = 0x5EED_C3A0
+SEED_C3 = 0x5EED_0C03
+SEED_C4 = 0x5EED_0C04
+
+
+class Packed:
+    """Reads as the C ABI takes them: contiguous codes, u64 offsets, u32 lengths."""
+
+    def __init__(self, codes, off, lens):
+        self.codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        self.off = np.ascontiguousarray(off, dtype=np.uint64)
+        self.lens = np.ascontiguousarray(lens, dtype=np.uint32)
+
+    def __len__(self):
+        return int(self.lens.size)
+
+    def tuple(self):
+        return self.codes, self.off, self.lens
+
+    def read(self, k):
+        o = int(self.off[k])
+        return self.codes[o:o + int(self.lens[k])]
+
+    def list(self):
+        return [self.read(k) for k in range(len(self))]
+
+    def subset(self, idx):
+        idx = np.asarray(idx)
+        parts = [self.read(int(k)) for k in idx]
+        lens = self.lens[idx].astype(np.uint32)
+        off = np.zeros(idx.size, dtype=np.uint64)
+        if idx.size > 1:
+            off[1:] = np.cumsum(lens[:-1], dtype=np.uint64)
+        codes = np.concatenate(parts) if lens.sum() else np.zeros(1, np.uint8)
+        return Packed(codes, off, lens)
+
+    def bases(self) -> int:
+        return int(self.lens.sum(dtype=np.uint64))
+
+
+def _offsets(lens):
+    off = np.zeros(lens.size, dtype=np.uint64)
+    if lens.size > 1:
+        off[1:] = np.cumsum(lens[:-1].astype(np.uint64))
+    return off
+
+
+def random_bases(rng, n, gc=0.5):
+    if gc == 0.5:
+        return rng.integers(0, 4, n, dtype=np.uint8)
+    u = rng.random(n)
+    at = (1 - gc) / 2
+    return np.searchsorted(np.cumsum([at, gc / 2, gc / 2]), u).astype(np.uint8)
+
+
+def panel(n_refs, lo, hi, seed, gc=0.5):
+    """n_refs uniform references with lengths uniform in [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(lo, hi + 1, n_refs)
+    return [random_bases(rng, int(m), gc) for m in lens]
+
+
+def panel_tiles(seed=SEED_PANEL):
+    return panel(164, 70, 180, seed)
+
+
+def panel_c3(seed=SEED_C3_PANEL, n_refs=10_000):
+    return panel(n_refs, 300, 1000, seed)
+
+
+def mutate(rng, codes, lens, p_sub, p_ins, p_del, p_geom=0.6):
+    """Mutate concatenated sequences (segment lengths `lens`): per base a
+    deletion starts with p_del (geometric length), the base is substituted
+    with p_sub (by a different base), and an insertion (geometric length of
+    random bases) follows it with p_ins.  Returns (codes, lens)."""
+    n = codes.size
+    if n == 0:
+        return codes, lens
+    seg = np.repeat(np.arange(lens.size), lens)
+    seg_end = np.repeat(np.cumsum(lens), lens)
+    pos = np.arange(n)
+    keep = np.ones(n, dtype=np.int64)
+    starts = np.nonzero(rng.random(n) < p_del)[0]
+    if starts.size:
+        dl = rng.geometric(p_geom, starts.size)
+        ends = np.minimum(starts + dl, seg_end[starts])
+        diff = np.zeros(n + 1, dtype=np.int64)
+        np.add.at(diff, starts, 1)
+        np.add.at(diff, ends, -1)
+        keep[np.cumsum(diff[:-1]) > 0] = 0
+    out = codes.copy()
+    sub = np.nonzero(rng.random(n) < p_sub)[0]
+    if sub.size:
+        out[sub] = (out[sub] + rng.integers(1, 4, sub.size)) % 4
+    ins = np.zeros(n, dtype=np.int64)
+    ii = np.nonzero(rng.random(n) < p_ins)[0]
+    if ii.size:
+        ins[ii] = rng.geometric(p_geom, ii.size)
+    reps = keep + ins
+    src = np.repeat(pos, reps)
+    new = out[src]
+    # inserted copies (all but the first of a kept base, all of a deleted one)
+    first = np.zeros(src.size, dtype=bool)
+    starts_out = np.cumsum(reps) - reps
+    has = reps > 0
+    first[starts_out[has]] = True
+    is_ins = ~first | (keep[src] == 0)
+    new[is_ins] = rng.integers(0, 4, int(is_ins.sum()), dtype=np.uint8)
+    new_lens = np.bincount(seg[src], minlength=lens.size).astype(np.int64)
+    return new, new_lens
+
+
+def _ranges(starts, lens):
+    """Concatenated index ranges [starts[i], starts[i] + lens[i])."""
+    lens = np.asarray(lens, dtype=np.int64)
+    total = int(lens.sum())
+    base = np.repeat(np.asarray(starts, dtype=np.int64) - (np.cumsum(lens) - lens), lens)
+    return base + np.arange(total, dtype=np.int64)
+
+
+def derived_reads(rng, refs, target, p_sub, p_ins, p_del, start_max=20, tail_max=30):
+    """Reads of exactly `target` bases cut from random references: a body
+    starting 0..start_max into the reference, mutated, then a random 3'
+    tail of 0..tail_max bases (more when the reference runs out)."""
+    target = np.asarray(target, dtype=np.int64)
+    ref_lens = np.array([r.size for r in refs], dtype=np.int64)
+    ref_off = _offsets(ref_lens).astype(np.int64)
+    cat = np.concatenate(refs)
+    n = target.size
+    which = rng.integers(0, len(refs), n)
+    start = np.minimum(rng.integers(0, start_max + 1, n), ref_lens[which] - 1)
+    tail = rng.integers(0, tail_max + 1, n)
+    body = np.minimum(np.clip(target - tail, 1, None), ref_lens[which] - start)
+    codes = cat[_ranges(ref_off[which] + start, body)]
+    codes, lens = mutate(rng, codes, body, p_sub, p_ins, p_del)
+    take = np.minimum(lens, target)
+    pad = target - take
+    out = np.empty(int(target.sum()), dtype=np.uint8)
+    o_off = np.cumsum(target) - target
+    src_off = np.cumsum(lens) - lens
+    out[_ranges(o_off, take)] = codes[_ranges(src_off, take)]
+    out[_ranges(o_off + take, pad)] = random_bases(rng, int(pad.sum()))
+    return out, target
+
+
+def mixed_reads(rng, refs, lens, frac_derived, p_sub, p_ins, p_del):
+    n = lens.size
+    derived = rng.random(n) < frac_derived
+    d_codes, d_lens = derived_reads(rng, refs, lens[derived], p_sub, p_ins, p_del)
+    r_lens = lens[~derived]
+    r_codes = random_bases(rng, int(r_lens.sum()))
+    # stitch back in read order
+    all_lens = np.zeros(n, dtype=np.int64)
+    all_lens[derived] = d_lens
+    all_lens[~derived] = r_lens
+    off = _offsets(all_lens)
+    codes = np.empty(int(all_lens.sum()), dtype=np.uint8)
+    di = np.nonzero(derived)[0]
+    ri = np.nonzero(~derived)[0]
+    for idx_set, src, src_lens in ((di, d_codes, d_lens), (ri, r_codes, r_lens)):
+        if idx_set.size == 0:
+            continue
+        codes[_ranges(off[idx_set], src_lens)] = src
+    return Packed(codes, off, all_lens.astype(np.uint32))
+
+
+def reads_c1(refs, n=10_000, seed=SEED_C1):
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(60, 201, n)
+    return mixed_reads(rng, refs, lens, 0.9, 0.08, 0.02, 0.01)
+
+
+def lognormal_lengths(rng, n, median, sigma, lo, hi):
+    return np.clip(np.round(median * np.exp(sigma * rng.standard_normal(n))), lo, hi).astype(np.int64)
+
+
+def reads_c2(refs, n=1_000_000, seed=SEED_C2):
+    rng = np.random.default_rng(seed)
+    lens = lognormal_lengths(rng, n, 110, 0.4, 20, 1000)
+    return mixed_reads(rng, refs, lens, 0.9, 0.08, 0.02, 0.01)
+
+
+def reads_c3(refs, n=200_000, seed=SEED_C3):
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(50, 1001, n)
+    return mixed_reads(rng, refs, lens, 0.7, 0.10, 0.015, 0.015)

@@ -1,0 +1,188 @@
+/*
+ * eschalign_b200.h -- C ABI of the B200 panel scorer.
+ *
+ * Scores every read of a batch against every reference of a panel with the
+ * Gotoh affine-gap recurrence (local or semi-global), on the forward strand
+ * and optionally the reverse complement, and reduces each read on the device
+ * to its best score, suboptimal score (SAM XS) and tie set.
+ *
+ * This is the boundary eschalign's `--device gpu` path calls in place of the
+ * Rust `eschalign::cuda::GpuScorer` (crates/eschalign/src/cuda/mod.rs:328-709).
+ * Every entry point cites the reference interface it replaces.  Inputs are
+ * alphabet codes (0..3 = A,C,G,T; 4 = any other letter, a wildcard that
+ * matches everything), exactly what GpuScorer::score_batch takes
+ * (cuda/mod.rs:524).  Plain pointers and sizes only; the library owns all
+ * device memory; a scorer is used by one thread at a time, like GpuScorer
+ * (`&mut self`, cuda/mod.rs:326-327).
+ */
+#ifndef ESCHALIGN_B200_H
+#define ESCHALIGN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ESG_ABI_VERSION 1
+
+/* ---- status codes: GpuError (cuda/mod.rs:144-153) + AlignError (error.rs:7-28) */
+typedef int32_t esg_status;
+#define ESG_OK 0
+#define ESG_ERR_UNAVAILABLE 1        /* GpuError::Unavailable: no driver or no device   */
+#define ESG_ERR_DRIVER 2             /* GpuError::Driver: a CUDA call failed             */
+#define ESG_ERR_REFERENCE_TOO_LONG 3 /* GpuError::ReferenceTooLong                       */
+#define ESG_ERR_SCORING_INVALID 4    /* AlignError::ScoringInvalid (scoring.rs:70-100)   */
+#define ESG_ERR_EMPTY_PANEL 5        /* AlignError::EmptyPanel (panel.rs:264-266)        */
+#define ESG_ERR_EMPTY_REFERENCE 6    /* AlignError::EmptyReference (panel.rs:257-259)    */
+#define ESG_ERR_BAD_ARGUMENT 7       /* a NULL pointer, a bad flag, a mode out of range  */
+#define ESG_ERR_OUT_OF_MEMORY 8      /* device or pinned memory exhausted                */
+#define ESG_ERR_TIMEOUT 9            /* a bounded device wait gave up                    */
+
+/* ---- scoring: Scoring (scoring.rs:27-36) and Mode (scoring.rs:151-165) */
+typedef struct esg_scoring {
+    int32_t match_score; /* > 0                                   */
+    int32_t mismatch;    /* < match_score                         */
+    int32_t gap_open;    /* whole cost of a one-base gap, <= 0    */
+    int32_t gap_extend;  /* each further base of the same gap, <= 0 */
+} esg_scoring;
+
+#define ESG_MODE_LOCAL 0
+#define ESG_MODE_SEMIGLOBAL 1
+
+/* ---- kernel choice: the A/B lever of GpuScorer::set_half2 (cuda/mod.rs:500) */
+#define ESG_KERNEL_AUTO 0    /* batched int16x2 kernel, int32 for what it cannot take */
+#define ESG_KERNEL_PLAIN32 1 /* every query on the plain one-thread-per-pair kernel  */
+
+/* ---- batch flags */
+#define ESG_BOTH_STRANDS 1u /* also score each read's reverse complement (align.rs:2865-2872) */
+#define ESG_FULL_ROWS 2u    /* also return every query's scores (ScoreMatrix, mapper.rs:95-139) */
+
+/* ---- per-read result: the scored half of Aligner::map_reads_scored
+ * (mapper.rs:444-472).  Candidates are (reference r, strand) in the order
+ * r = 0.. in panel order, forward before reverse; a candidate is written as
+ * (r << 1) | reverse. */
+typedef struct esg_read_result {
+    int32_t best;       /* max over the read's candidates                        */
+    int32_t suboptimal; /* max over candidates != best (XS); ESG_NO_SCORE if none */
+    uint32_t n_tied;    /* how many candidates score `best`, counted in full     */
+    uint32_t flags;     /* ESG_RESULT_* */
+} esg_read_result;
+
+#define ESG_NO_SCORE INT32_MIN
+#define ESG_RESULT_EMPTY 1u          /* empty read: no candidates (best = ESG_NO_SCORE) */
+#define ESG_RESULT_TIES_TRUNCATED 2u /* n_tied > tie_capacity: only the first listed    */
+#define ESG_RESULT_RESCORED32 4u     /* some pair was (re)scored by the int32 kernel    */
+
+#define ESG_MAX_TIE_CAPACITY 32
+
+typedef struct esg_options {
+    uint32_t tie_capacity; /* ties listed per read, 1..ESG_MAX_TIE_CAPACITY (default 8)  */
+    int32_t kernel;        /* ESG_KERNEL_*                                                */
+    void* stream;          /* cudaStream_t to run on; NULL: the scorer makes its own      */
+} esg_options;
+
+typedef struct esg_info {
+    char device_name[256]; /* GpuScorer::device_name (cuda/mod.rs:446)                */
+    int32_t device;
+    int32_t sm_count;
+    uint32_t n_refs;
+    uint32_t max_ref_len;
+    uint32_t n_ref_pairs;     /* references paired into int16x2 lanes               */
+    uint32_t panel_bytes;     /* shared-memory panel staged per CTA (0: read from L2) */
+    int32_t batched_ok;       /* the scoring scheme fits the batched kernel's tables  */
+    int32_t regs_batched;     /* GpuScorer::registers analogue (cuda/mod.rs:466)      */
+    int32_t regs_plain;
+    int32_t local_bytes_batched; /* GpuScorer::local_bytes analogue (cuda/mod.rs:479) */
+    int32_t local_bytes_plain;
+    int32_t batched_blocks;   /* persistent CTAs of the batched kernel                 */
+    int32_t batched_threads;  /* threads per CTA                                       */
+    int32_t plain_blocks;
+    int32_t plain_threads;
+} esg_info;
+
+typedef struct esg_batch_stats {
+    uint32_t n_reads;
+    uint32_t n_queries;         /* reads x strands                                     */
+    uint32_t n_empty;
+    uint32_t queries_batched;   /* on the int16x2 kernel                               */
+    uint32_t queries_plain;     /* put on the int32 kernel by the host                 */
+    uint32_t queries_rescored;  /* flagged by the int16x2 kernel, re-scored in int32   */
+    uint32_t tasks;             /* 32-lane work tiles of the batched kernel            */
+    uint32_t lanes_used;        /* of tasks * 32                                       */
+    uint32_t kernels;           /* kernels one launch of the batch runs                */
+    uint64_t cells;             /* sum over scored queries of len * panel bases        */
+    uint64_t h2d_bytes;
+    uint64_t d2h_bytes;
+} esg_batch_stats;
+
+typedef struct esg_scorer esg_scorer;
+typedef struct esg_batch esg_batch;
+
+int esg_abi_version(void);
+const char* esg_status_string(esg_status status);
+/* Message of the last failure on this thread ("" if none). */
+const char* esg_last_error(void);
+
+/* device_visible (cuda/mod.rs:130-140): number of CUDA devices, 0 if none. */
+esg_status esg_device_count(int32_t* out);
+
+/* fits_i16 (crates/eschalign/src/simd/mod.rs:222-227): whether the reference's
+ * SIMD kernels score a read of `len` bases; the reference GPU scorer's
+ * scores_len (cuda/mod.rs:506-508) also requires 0 < len <= 4096.  This
+ * scorer scores every non-empty read whatever this says. */
+int32_t esg_fits_i16(uint64_t len, uint64_t max_ref_len, const esg_scoring* scoring);
+
+/* GpuScorer::new_on_device (cuda/mod.rs:350-443): lay `n_refs` references
+ * (codes, concatenated; reference r is ref_codes[ref_off[r] .. +ref_len[r]])
+ * out on device `device` under one scoring and mode.  Refuses an invalid
+ * scheme, an empty panel or reference, or a reference longer than 32768. */
+esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64_t* ref_off,
+                          const uint32_t* ref_len, uint32_t n_refs, const esg_scoring* scoring,
+                          int32_t mode, const esg_options* options, esg_scorer** out);
+void esg_scorer_free(esg_scorer* scorer);
+
+esg_status esg_scorer_info(const esg_scorer* scorer, esg_info* out);
+/* GpuScorer::set_half2 (cuda/mod.rs:500-502): ESG_KERNEL_AUTO or _PLAIN32. */
+esg_status esg_scorer_set_kernel(esg_scorer* scorer, int32_t kernel);
+/* GpuScorer::scores_len (cuda/mod.rs:506-508): 1 for every len > 0 -- nothing
+ * is left to a CPU path. */
+int32_t esg_scores_len(const esg_scorer* scorer, uint64_t len);
+
+/* GpuScorer::score_batch (cuda/mod.rs:524-528): prepare + submit + finish.
+ * Read k is codes[off[k] .. off[k] + len[k]].  `results` gets n_reads
+ * entries, `ties` n_reads * tie_capacity candidates (first n_listed of each
+ * read are valid, n_listed = min(n_tied, tie_capacity)).  With
+ * ESG_FULL_ROWS, `rows` gets every query's scores in panel order, forward
+ * rows 0..n_reads-1 then (ESG_BOTH_STRANDS) reverse rows n_reads..2n-1 --
+ * the reference's batch layout (align.rs:1484-1494). */
+esg_status esg_score_batch(esg_scorer* scorer, const uint8_t* codes, const uint64_t* off,
+                           const uint32_t* len, uint32_t n_reads, uint32_t flags,
+                           esg_read_result* results, uint32_t* ties, int32_t* rows);
+
+/* GpuScorer::prepare (cuda/mod.rs:533-576): host only, touches no device
+ * state, so it may run while an earlier batch's kernels do.  Copies the
+ * reads into pinned staging and plans the work (length buckets, 32-lane
+ * tiles, int32 list). */
+esg_status esg_prepare(esg_scorer* scorer, const uint8_t* codes, const uint64_t* off,
+                       const uint32_t* len, uint32_t n_reads, uint32_t flags, esg_batch** out);
+/* GpuScorer::submit (cuda/mod.rs:581-699): upload and queue the kernels on
+ * the scorer's stream; returns without waiting. */
+esg_status esg_submit(esg_scorer* scorer, esg_batch* batch);
+/* GpuScorer::finish (cuda/mod.rs:702-708): wait for the batch and copy its
+ * results to the caller's buffers (any of ties/rows may be NULL). */
+esg_status esg_finish(esg_scorer* scorer, esg_batch* batch, esg_read_result* results,
+                      uint32_t* ties, int32_t* rows);
+void esg_batch_free(esg_batch* batch);
+esg_status esg_batch_stats_get(const esg_batch* batch, esg_batch_stats* out);
+
+/* Re-run the device work of a submitted batch on `stream` (NULL: the
+ * scorer's) with its inputs already resident, no copies.  For measuring the
+ * kernels alone; the batch's results are overwritten with identical ones. */
+esg_status esg_relaunch(esg_scorer* scorer, esg_batch* batch, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

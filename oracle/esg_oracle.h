@@ -1,0 +1,117 @@
+/*
+ * esg_oracle.h -- CPU restatement of eschalign's panel-scoring path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker the CUDA path is
+ * compared against (tests/, __graft_entry__.smoke(), and bench.py's
+ * cpu_baseline leg and `--impl reference` arm).  Nothing in the product
+ * (eschalign_b200/) links, loads or calls it.
+ *
+ * Parity is pinned: the scalar score is checked against the reference's 192
+ * parasail golden scores (tests/golden/align_golden_scores.json, extracted
+ * from crates/eschalign/tests/fixtures/align_golden.json by
+ * tests/golden/make_golden.py) and the unit known-answers of
+ * crates/eschalign/src/scalar.rs:378-430 and mapper.rs:570-589.
+ *
+ * Two scorers live here:
+ *   - eo_score: the scalar Gotoh (crates/eschalign/src/scalar.rs:120-163),
+ *     the oracle every other path must equal;
+ *   - eo_profile_*: the AVX-512BW inter-sequence kernels of
+ *     crates/eschalign/src/simd/avx512.rs (row-major :43-107, transposed
+ *     :278-354) with the reference's dispatch (mapper.rs:216-222,
+ *     simd/mod.rs:222-227), the timed CPU baseline.
+ */
+#ifndef ESG_ORACLE_H
+#define ESG_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Codes of crates/eschalign/src/alphabet.rs:7-16. */
+enum { EO_A = 0, EO_C = 1, EO_G = 2, EO_T = 3, EO_WILDCARD = 4, EO_N_CODES = 5 };
+
+/* Same layout as the product's esg_read_result (include/eschalign_b200.h). */
+typedef struct eo_result {
+    int32_t best;       /* max over the read's candidates                     */
+    int32_t suboptimal; /* best score not equal to `best`; INT32_MIN if none  */
+    uint32_t n_tied;    /* candidates scoring `best`                           */
+    uint32_t flags;     /* EO_RESULT_* */
+} eo_result;
+
+#define EO_NO_SCORE INT32_MIN
+#define EO_RESULT_EMPTY 1u          /* empty read: no candidates at all         */
+#define EO_RESULT_TIES_TRUNCATED 2u /* n_tied exceeds the tie list's capacity  */
+
+/* alphabet.rs:29-50: A/C/G/T(U) either case -> 0..3, every other byte -> 4. */
+uint8_t eo_encode_base(uint8_t letter);
+void eo_encode(const uint8_t* letters, size_t n, uint8_t* codes);
+/* alphabet.rs:58-64: reverse, complement c -> 3-c, the wildcard stays. */
+void eo_revcomp_codes(const uint8_t* codes, size_t n, uint8_t* out);
+
+/* scoring.rs:70-100.  0 = valid; 1 match <= 0; 2 mismatch >= match;
+ * 3 a gap score > 0; 4 a magnitude above 1000. */
+int eo_scoring_validate(int32_t ma, int32_t mi, int32_t o, int32_t e);
+
+/* scalar.rs:120-163: best Gotoh score of query (n codes) vs reference (m). */
+int32_t eo_score(const uint8_t* q, size_t n, const uint8_t* r, size_t m,
+                 int32_t ma, int32_t mi, int32_t o, int32_t e, int local);
+
+/* simd/mod.rs:222-227 */
+int eo_fits_i16(size_t n, size_t max_ref_len, int32_t ma, int32_t mi, int32_t o, int32_t e);
+
+/* mapper.rs:444-472: candidates in order (ref 0 fwd, ref 0 rev, ref 1 fwd, ...);
+ * `rev` may be NULL (forward strand only).  Writes the first min(n_tied, cap)
+ * tie candidates as (ref << 1) | reverse into `ties`. */
+void eo_select(const int32_t* fwd, const int32_t* rev, uint32_t n_refs, uint32_t cap,
+               eo_result* out, uint32_t* ties);
+
+/* Every query against every reference with eo_score, out[q * n_refs + r];
+ * `threads` <= 0 uses all cores. */
+void eo_score_matrix(const uint8_t* codes, const uint64_t* off, const uint32_t* len, uint32_t n_q,
+                     const uint8_t* ref_codes, const uint64_t* ref_off, const uint32_t* ref_len,
+                     uint32_t n_refs, int32_t ma, int32_t mi, int32_t o, int32_t e, int local,
+                     int threads, int32_t* out);
+
+/* ---- AVX-512BW baseline (simd/mod.rs + simd/avx512.rs) ---------------- */
+typedef struct eo_profile eo_profile;
+
+/* Profile::from_codes (simd/mod.rs:292-331) at 32 lanes, plus the transposed
+ * profile (simd/mod.rs:255-269).  NULL if the CPU lacks AVX-512BW. */
+eo_profile* eo_profile_build(const uint8_t* ref_codes, const uint64_t* ref_off,
+                             const uint32_t* ref_len, uint32_t n_refs,
+                             int32_t ma, int32_t mi, int32_t o, int32_t e);
+void eo_profile_free(eo_profile* p);
+int eo_cpu_has_avx512bw(void);
+
+/* Aligner::score_all (mapper.rs:242-252): SIMD when fits_i16, row-major
+ * below 256 nt and transposed from 256 nt (kernel = 0), or forced
+ * (1 row-major, 2 transposed); scalar outside fits_i16. out[n_refs]. */
+void eo_profile_score_all(const eo_profile* p, const uint8_t* q, size_t n, int local,
+                          int kernel, int32_t* out);
+
+/* The CPU baseline end to end: per read, score the forward strand (and the
+ * reverse complement when both_strands), then eo_select.  Reads are handed
+ * out to `threads` workers (<= 0: all cores) in chunks of 64 reads
+ * (crates/eschalign-cli/src/align.rs:1470-1473).  Returns the thread count
+ * used.  `rows`, when not NULL, receives every query's scores: forward rows
+ * 0..n-1 then reverse rows n..2n-1. */
+int eo_cpu_map_batch(const eo_profile* p, const uint8_t* codes, const uint64_t* off,
+                     const uint32_t* len, uint32_t n_reads, int both_strands, int local,
+                     int threads, uint32_t cap, eo_result* results, uint32_t* ties,
+                     int32_t* rows);
+
+/* Same, with the scalar oracle instead of the SIMD kernels (used at test
+ * sizes; identical results by construction of the reference). */
+int eo_scalar_map_batch(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
+                        uint32_t n_reads, const uint8_t* ref_codes, const uint64_t* ref_off,
+                        const uint32_t* ref_len, uint32_t n_refs, int32_t ma, int32_t mi,
+                        int32_t o, int32_t e, int both_strands, int local, int threads,
+                        uint32_t cap, eo_result* results, uint32_t* ties, int32_t* rows);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,84 @@
+"""Extract golden vectors for the panel-scoring path from the reference's own fixtures.
+
+Run once, in a container where the reference tree is mounted:
+
+    python tests/golden/make_golden.py /root/reference
+
+It reads, as data:
+
+* ``crates/eschalign/tests/fixtures/align_golden.json`` -- parasail 1.3.4
+  (``sw_trace`` / ``sg_trace``) scores for 48 pairs x {local, semiglobal} x
+  {``2,-1,-10,-1``, ``1,-1,-2,-1``}, generated by the reference's
+  ``gen_align_golden.py`` (seed 395) and checked by its
+  ``tests/parasail_golden.rs:48-77``;
+* ``crates/eschalign-cli/tests/fixtures/trna_reference.fa`` and
+  ``trna_reference_ambiguous.fa`` -- the 47-reference tRNA panels the
+  reference's ``tests/gpu_parity.rs:249-260`` scores the fixture reads against.
+
+and writes the subset this project tests against into ``tests/golden/``:
+``align_golden_scores.json`` (query, reference, mode, scheme, score and the
+parasail end coordinates) and the two panels as ``panel_trna*.json``
+(name + letters, file order).  Nothing else from the reference is copied.
+"""
+import json
+import os
+import sys
+
+
+def read_fasta(path):
+    """Minimal FASTA reader: first word of the header, sequence lines joined."""
+    recs, name, seq = [], None, []
+    with open(path, "rb") as fh:
+        for raw in fh:
+            line = raw.rstrip(b"\r\n")
+            if line.startswith(b">"):
+                if name is not None:
+                    recs.append((name, b"".join(seq).decode()))
+                words = line[1:].split()
+                name, seq = words[0].decode(), []
+            elif name is not None:
+                seq.append(b"".join(line.split()))
+    if name is not None:
+        recs.append((name, b"".join(seq).decode()))
+    return recs
+
+
+def main(ref_root):
+    here = os.path.dirname(os.path.abspath(__file__))
+    src = os.path.join(ref_root, "crates/eschalign/tests/fixtures/align_golden.json")
+    with open(src) as fh:
+        g = json.load(fh)
+    cases = []
+    for p in g["pairs"]:
+        for r in p["results"]:
+            cases.append({
+                "name": p["name"],
+                "source": p["source"],
+                "query": p["query"],
+                "reference": p["reference"],
+                "mode": r["mode"],
+                "scheme": g["schemes"][r["scheme"]],
+                "score": r["score"],
+                "query_start": r["query_start"],
+                "query_end": r["query_end"],
+                "ref_start": r["ref_start"],
+                "ref_end": r["ref_end"],
+            })
+    out = {
+        "about": "parasail 1.3.4 golden scores (reference fixture align_golden.json, seed 395)",
+        "cases": cases,
+        "fixture_reads": [p["query"] for p in g["pairs"] if p["source"] != "random"],
+    }
+    with open(os.path.join(here, "align_golden_scores.json"), "w") as fh:
+        json.dump(out, fh, indent=0)
+    for fa, tag in (("trna_reference.fa", "panel_trna.json"),
+                    ("trna_reference_ambiguous.fa", "panel_trna_ambiguous.json")):
+        recs = read_fasta(os.path.join(ref_root, "crates/eschalign-cli/tests/fixtures", fa))
+        with open(os.path.join(here, tag), "w") as fh:
+            json.dump({"source": fa, "references": [{"name": n, "seq": s} for n, s in recs]},
+                      fh, indent=0)
+    print(f"{len(cases)} golden scores, {len(out['fixture_reads'])} fixture reads")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

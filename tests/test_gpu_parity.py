@@ -1,0 +1,262 @@
+"""The CUDA path against the CPU oracle, by equality (no tolerance: integer
+scores).  Mirrors crates/eschalign/tests/gpu_parity.rs: every check runs on
+both kernels (the batched int16x2 kernel with int32 for what it cannot take,
+and the plain int32 kernel), reverse complements included, and compares
+every query's full row with the scalar oracle and every read's reduced
+result (best, XS, tie count, tie list) with the oracle's selection
+(mapper.rs:444-472)."""
+import numpy as np
+import pytest
+
+from eschalign_b200 import (KERNEL_AUTO, KERNEL_PLAIN32, GpuError, GpuScorer, Mode, Scoring,
+                            encode, pack_reads, synth)
+from tests.helpers import (SCHEMES, Rng, fixture_panel, fixture_reads, golden, random_panel,
+                           random_seq, reads_for)
+
+pytestmark = pytest.mark.gpu
+
+CAP = 8
+
+
+def cpu_results(O, refs, packed, scoring, local, both):
+    """Per-read results of the reference's CPU path: the AVX-512 restatement
+    where the host has AVX-512BW, else the scalar oracle (equal by test)."""
+    if O.lib().eo_cpu_has_avx512bw():
+        r, t, _, _ = O.Profile(refs, scoring).map_batch(*packed.tuple(), local=local,
+                                                       both_strands=both, cap=CAP)
+        return r, t
+    r, t, _ = O.scalar_map_batch(packed.list(), refs, scoring, local, both, cap=CAP)
+    return r, t
+
+
+def oracle_rows(O, reads, panel, scoring, local):
+    """Forward rows then reverse-complement rows, scalar oracle."""
+    rc = [O.revcomp(r) for r in reads]
+    return O.score_matrix(list(reads) + rc, panel, scoring, local)
+
+
+def check(O, panel, reads, scoring, mode, what, kernels=(KERNEL_AUTO, KERNEL_PLAIN32),
+          tie_capacity=CAP):
+    """gpu_parity.rs:132-192."""
+    local = mode == Mode.LOCAL
+    want_rows = oracle_rows(O, reads, panel, scoring, local)
+    want_res, want_ties, _ = O.scalar_map_batch(reads, panel, scoring, local, True,
+                                               cap=tie_capacity)
+    n = len(reads)
+    stats = {}
+    with GpuScorer(panel, Scoring(*scoring), mode, tie_capacity=tie_capacity) as g:
+        for kernel in kernels:
+            g.set_kernel(kernel)
+            res = g.score_batch(reads, both_strands=True, full_rows=True)
+            got = res.rows
+            assert got.shape == want_rows.shape
+            bad = np.argwhere(got != want_rows)
+            assert bad.size == 0, (f"{what} {mode.label} {scoring} kernel {kernel}: query "
+                                   f"{bad[0][0]} ref {bad[0][1]} got {got[tuple(bad[0])]} "
+                                   f"want {want_rows[tuple(bad[0])]}")
+            for field in ("best", "suboptimal", "n_tied"):
+                assert (res.results[field] == want_res[field]).all(), (what, field, kernel)
+            assert ((res.results["flags"] & 3) == (want_res["flags"] & 3)).all(), (what, kernel)
+            for k in range(n):
+                nl = min(int(want_res["n_tied"][k]), tie_capacity)
+                assert (res.ties[k, :nl] == want_ties[k, :nl]).all(), (what, k, kernel)
+            stats[kernel] = res.stats
+    return stats
+
+
+def test_gpu_scores_equal_scalar_random_panel(oracle):
+    """gpu_parity.rs:217-232: 37 references, ragged, five schemes."""
+    rng = Rng(0x5EED_0101)
+    letters = random_panel(rng, 37, 20, 280)
+    panel = [encode(s) for s in letters]
+    reads = reads_for(rng, letters, 60)
+    for scoring in SCHEMES:
+        for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+            st = check(oracle, panel, reads, scoring, mode, "random 37-ref panel")
+            assert st[KERNEL_AUTO]["queries_batched"] == 2 * len(reads)
+
+
+def test_gpu_scores_equal_scalar_wide_panel(oracle):
+    """gpu_parity.rs:234-247: 300 references up to 620 nt -- too big for the
+    shared-memory panel, so the batched kernel reads it through L2."""
+    rng = Rng(0x5EED_0101 + 7)
+    letters = random_panel(rng, 300, 20, 600)
+    panel = [encode(s) for s in letters]
+    reads = reads_for(rng, letters, 6)
+    for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+        check(oracle, panel, reads, (2, -1, -10, -1), mode, "random 300-ref panel")
+
+
+@pytest.mark.parametrize("tag", ["trna", "trna_ambiguous"])
+def test_gpu_fixture_reads_on_trna_panels(oracle, tag):
+    """gpu_parity.rs:249-260: the real tRNA reads against both 47-reference
+    fixture panels (the ambiguous one carries wildcards)."""
+    panel = fixture_panel(tag)
+    reads = fixture_reads()
+    assert len(panel) == 47 and len(reads) >= 5
+    for scoring in SCHEMES:
+        for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+            check(oracle, panel, reads, scoring, mode, tag)
+
+
+def test_gpu_golden_pairs(oracle):
+    """The 192 parasail golden pairs, each read against its own reference."""
+    g = golden()
+    for c in g["cases"]:
+        q, r = encode(c["query"]), encode(c["reference"])
+        mode = Mode.LOCAL if c["mode"] == "local" else Mode.SEMIGLOBAL
+        with GpuScorer([r], Scoring(*c["scheme"]), mode) as s:
+            for kernel in (KERNEL_AUTO, KERNEL_PLAIN32):
+                s.set_kernel(kernel)
+                res = s.score_batch([q], full_rows=True)
+                assert res.rows[0, 0] == c["score"], (c["name"], c["mode"], kernel)
+
+
+def test_gpu_long_and_straddling_reads(oracle):
+    """gpu_parity.rs:269-321 in spirit: reads either side of the batched
+    kernel's 512-row limit, against references of 900-1000 nt."""
+    rng = Rng(0x5EED_0103)
+    letters = random_panel(rng, 21, 900, 100)
+    panel = [encode(s) for s in letters]
+    reads = []
+    for t in range(24):
+        ln = 440 + 12 * t
+        r = letters[rng.below(len(letters))]
+        read = random_seq(rng, ln, 0.01) if t % 3 == 2 else mutate_trunc(rng, r, ln)
+        reads.append(encode(read))
+    for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+        st = check(oracle, panel, reads, (3, -2, -5, -2), mode, "straddling batch")
+        a = st[KERNEL_AUTO]
+        assert a["queries_batched"] > 0 and a["queries_plain"] > 0
+
+
+def mutate_trunc(rng, r, ln):
+    from tests.helpers import mutate
+    return mutate(rng, r[:ln])[:ln]
+
+
+def test_gpu_scores_everything_it_is_given(oracle):
+    """gpu_parity.rs:355-378, inverted: empty reads come back empty, and a
+    read over the reference GPU's 4096 nt limit is scored here too."""
+    rng = Rng(0x5EED_0102)
+    letters = random_panel(rng, 20, 50, 100)
+    panel = [encode(s) for s in letters]
+    long = encode(random_seq(rng, 4097, 0.0))
+    ok = encode(random_seq(rng, 120, 0.0))
+    edge = encode(random_seq(rng, 4096, 0.0))
+    reads = [ok, np.zeros(0, np.uint8), long, edge, ok]
+    with GpuScorer(panel, Scoring(), Mode.LOCAL) as g:
+        res = g.score_batch(reads, full_rows=True)
+        assert res.read(1).best is None and res.results["flags"][1] & 1
+        for k in (0, 2, 3, 4):
+            for r, ref in enumerate(panel):
+                assert res.rows[k, r] == oracle.score(reads[k], ref, (2, -1, -10, -1), True)
+        assert len(g.score_batch([])) == 0
+
+
+def test_gpu_refuses_a_reference_it_cannot_hold():
+    """gpu_parity.rs:380-389."""
+    with pytest.raises(GpuError) as ei:
+        GpuScorer([np.zeros(32769, np.uint8)], Scoring(), Mode.LOCAL)
+    assert ei.value.kind == "ReferenceTooLong"
+
+
+def test_gpu_int16_saturation_is_rescored_in_int32(oracle):
+    """Scores past int16: 100,-100,-27,-27 on 400-500 nt exact matches reach
+    40 000-50 000.  The batched kernel flags them and the int32 kernel
+    re-scores them; results equal the oracle's int32 scores."""
+    rng = Rng(0x5EED_0105)
+    letters = random_panel(rng, 9, 480, 40)
+    panel = [encode(s) for s in letters]
+    reads = [encode(letters[k][:400 + 10 * k]) for k in range(9)]
+    reads += [encode(random_seq(rng, 300, 0.0)) for _ in range(5)]
+    scoring = (100, -100, -27, -27)
+    st = check(oracle, panel, reads, scoring, Mode.LOCAL, "saturating")
+    assert st[KERNEL_AUTO]["queries_rescored"] >= 9
+    assert st[KERNEL_AUTO]["queries_batched"] == 2 * len(reads)
+    st = check(oracle, panel, reads, scoring, Mode.SEMIGLOBAL, "saturating semi-global")
+    assert st[KERNEL_AUTO]["queries_plain"] == 2 * len(reads)
+
+
+def test_gpu_ties_truncated_and_counted_in_full(oracle):
+    """A panel of identical references: every candidate ties; the count is
+    complete and the list holds the first tie_capacity in candidate order."""
+    ref = encode(b"ACGTTGCAACGTAGCTAGCTAGGATCCA")
+    panel = [ref] * 12 + [encode(b"TTTTTTTTTTTT")]
+    reads = [ref, encode(b"ACGTTGCAACG"), encode(b"GGGG")]
+    for cap in (1, 3, 8, 32):
+        check(oracle, panel, reads, (2, -1, -10, -1), Mode.LOCAL, f"ties cap {cap}",
+              tie_capacity=cap)
+
+
+def test_gpu_config1_reads_equal_avx512(oracle):
+    """Config C1 at full size: 10 000 reads vs the 164-reference panel,
+    local 2,-1,-10,-1, forward strand -- every read's result equal to the
+    AVX-512 baseline's (itself equal to the scalar oracle by test)."""
+    refs = synth.panel_tiles()
+    reads = synth.reads_c1(refs)
+    want, want_t = cpu_results(oracle, refs, reads, (2, -1, -10, -1), True, False)
+    with GpuScorer(refs, Scoring(), Mode.LOCAL) as g:
+        for kernel in (KERNEL_AUTO, KERNEL_PLAIN32):
+            g.set_kernel(kernel)
+            res = g.score_batch(reads.tuple())
+            assert (res.results["best"] == want["best"]).all()
+            assert (res.results["suboptimal"] == want["suboptimal"]).all()
+            assert (res.results["n_tied"] == want["n_tied"]).all()
+            n_l = np.minimum(want["n_tied"], CAP)
+            mask = np.arange(CAP)[None, :] < n_l[:, None]
+            assert (res.ties[mask] == want_t[mask]).all()
+
+
+@pytest.mark.parametrize("mode", [Mode.LOCAL, Mode.SEMIGLOBAL])
+@pytest.mark.parametrize("scoring", [(2, -1, -10, -1), (1, -1, -2, -1)])
+def test_gpu_config2_sample_both_strands(oracle, mode, scoring):
+    """Config C2 shape (lognormal lengths, both strands, both modes, both
+    schemes) on a 20 000-read sample, against the AVX-512 baseline."""
+    refs = synth.panel_tiles()
+    reads = synth.reads_c2(refs, n=20_000)
+    local = mode == Mode.LOCAL
+    want, want_t = cpu_results(oracle, refs, reads, scoring, local, True)
+    with GpuScorer(refs, Scoring(*scoring), mode) as g:
+        res = g.score_batch(reads.tuple(), both_strands=True)
+        for f in ("best", "suboptimal", "n_tied"):
+            assert (res.results[f] == want[f]).all(), f
+        n_l = np.minimum(want["n_tied"], CAP)
+        mask = np.arange(CAP)[None, :] < n_l[:, None]
+        assert (res.ties[mask] == want_t[mask]).all()
+
+
+def test_gpu_prepare_submit_finish_overlap(oracle):
+    """cuda/mod.rs:520-528 / align.rs:2817-2887: batch k+1 prepared while k
+    runs, results identical to score_batch one at a time."""
+    refs = synth.panel_tiles()
+    reads = synth.reads_c2(refs, n=6000)
+    chunks = [reads.subset(np.arange(k, min(k + 1500, len(reads)))) for k in range(0, 6000, 1500)]
+    with GpuScorer(refs, Scoring(), Mode.LOCAL) as g:
+        one = [g.score_batch(c.tuple(), both_strands=True) for c in chunks]
+        pending = None
+        got = []
+        for c in chunks + [None]:
+            prepared = g.prepare(c.tuple(), both_strands=True) if c is not None else None
+            if pending is not None:
+                got.append(g.finish(pending))
+            pending = g.submit(prepared) if prepared is not None else None
+        for a, b in zip(one, got):
+            assert (a.results == b.results).all() and (a.ties == b.ties).all()
+
+
+def test_gpu_strand_swap_property():
+    """Scoring the reverse complements with both strands swaps every
+    candidate's strand: best, XS and tie counts are unchanged, tie
+    candidates flip their strand bit."""
+    refs = synth.panel_tiles()
+    reads = synth.reads_c2(refs, n=4000)
+    rc = [np.where(r[::-1] >= 4, 4, 3 - r[::-1]).astype(np.uint8) for r in reads.list()]
+    with GpuScorer(refs, Scoring(), Mode.SEMIGLOBAL) as g:
+        a = g.score_batch(reads.tuple(), both_strands=True)
+        b = g.score_batch(pack_reads(rc), both_strands=True)
+    for f in ("best", "suboptimal", "n_tied"):
+        assert (a.results[f] == b.results[f]).all()
+    for k in range(len(reads)):
+        n = min(int(a.results["n_tied"][k]), CAP)
+        assert sorted(a.ties[k, :n] ^ 1) == sorted(b.ties[k, :n]) or a.results["n_tied"][k] > CAP

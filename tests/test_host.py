@@ -1,0 +1,58 @@
+"""Host-side logic: scoring, alphabet, panel, synthetic workloads, tie
+selection helper."""
+import numpy as np
+import pytest
+
+from eschalign_b200 import (Mode, Panel, PanelError, Scoring, ScoringError, encode,
+                            reverse_complement_codes, select_hits, synth)
+from eschalign_b200.scorer import ReadScores
+
+
+def test_scoring_parse_and_validate():
+    """scoring.rs:192-213."""
+    s = Scoring.parse("2,-1,-10,-1")
+    assert s == Scoring() and str(s) == "2,-1,-10,-1"
+    assert s.gap(1) == -10 and s.gap(3) == -12
+    for bad in ("2,-1,-10", "2,-1,10,-1", "0,-1,-10,-1", "2,3,-10,-1", "2,-1,-10,-x"):
+        with pytest.raises(ScoringError):
+            Scoring.parse(bad)
+    assert Mode.parse("overlap") is Mode.SEMIGLOBAL and Mode.parse("local") is Mode.LOCAL
+
+
+def test_alphabet():
+    assert list(encode("ACGTUacgtu")) == [0, 1, 2, 3, 3, 0, 1, 2, 3, 3]
+    assert all(v == 4 for v in encode("NnRYKMSWBDHV-*.X"))
+    assert list(reverse_complement_codes(encode("ACGTN"))) == list(encode("NACGT"))
+
+
+def test_panel_refusals():
+    with pytest.raises(PanelError):
+        Panel([])
+    with pytest.raises(PanelError):
+        Panel([("a", b"")])
+    p = Panel([("a", b"ACGT"), ("b", b"AC")])
+    assert len(p) == 2 and p.max_len() == 4 and p.total_len() == 6
+
+
+def test_synthetic_workloads_are_deterministic():
+    a = synth.panel_tiles()
+    b = synth.panel_tiles()
+    assert len(a) == 164 and all((x == y).all() for x, y in zip(a, b))
+    lens = np.array([r.size for r in a])
+    assert lens.min() >= 70 and lens.max() <= 180
+    r1 = synth.reads_c1(a, n=2000)
+    r2 = synth.reads_c1(a, n=2000)
+    assert (r1.codes == r2.codes).all() and (r1.lens == r2.lens).all()
+    assert r1.lens.min() >= 60 and r1.lens.max() <= 200 and r1.codes.max() <= 3
+    c2 = synth.reads_c2(a, n=20000)
+    assert c2.lens.min() >= 20 and c2.lens.max() <= 1000
+    assert 100 <= np.median(c2.lens) <= 120
+
+
+def test_select_hits():
+    """mapper.rs:466-472."""
+    s = ReadScores(24, 20, 3, [(0, False), (0, True), (5, False)], False, False)
+    assert select_hits(s) == s.ties
+    assert select_hits(s, max_ties=0) == [(0, False)]
+    assert select_hits(s, min_score=25) == []
+    assert select_hits(ReadScores(None, None, 0, [], False, False)) == []

@@ -1,0 +1,110 @@
+"""The CPU oracle pinned against the reference's golden vectors and known
+answers, and the AVX-512 baseline against the scalar oracle."""
+import numpy as np
+import pytest
+
+from tests.helpers import SCHEMES, Rng, fixture_panel, fixture_reads, golden, random_panel, reads_for
+
+D = (2, -1, -10, -1)
+
+
+def test_scalar_matches_parasail_golden(oracle):
+    """parasail_golden.rs:48-77: the 192 parasail 1.3.4 scores."""
+    g = golden()
+    assert len(g["cases"]) == 192
+    for c in g["cases"]:
+        q, r = oracle.encode(c["query"]), oracle.encode(c["reference"])
+        got = oracle.score(q, r, c["scheme"], c["mode"] == "local")
+        assert got == c["score"], (c["name"], c["mode"], c["scheme"])
+
+
+def test_scalar_known_answers(oracle):
+    """scalar.rs:378-430."""
+    E = oracle.encode
+    assert oracle.score(E("ACGTACGT"), E("TTACGTACGTTT"), D, True) == 16
+    assert oracle.score(E("ACGTA"), E("ACNTA"), D, True) == 10
+    assert oracle.score(E("AAAACCCGGGGTTTT"), E("AAAACCCCGGGGTTTT"), (2, -4, -3, -1), True) == 27
+    assert oracle.score(E("ACGTACGTCCCCC"), E("GGGGGACGTACGT"), D, False) == 16
+    assert oracle.score(E("AAAA"), E("CCCC"), D, True) == 0
+    assert oracle.score(E(""), E("ACGT"), D, True) == 0
+
+
+def test_alphabet_and_scoring(oracle):
+    """alphabet.rs:513-537, scoring.rs:192-213."""
+    assert list(oracle.encode("ACGTUacgtu")) == [0, 1, 2, 3, 3, 0, 1, 2, 3, 3]
+    assert all(v == 4 for v in oracle.encode("NnRYKMSWBDHV-*.X"))
+    assert list(oracle.revcomp(oracle.encode("ACGTN"))) == list(oracle.encode("NACGT"))
+    assert oracle.validate(D) == 0
+    assert oracle.validate((0, -1, -10, -1)) != 0
+    assert oracle.validate((2, 3, -10, -1)) != 0
+    assert oracle.validate((2, -1, 10, -1)) != 0
+    assert oracle.validate((2, -1, -1001, -1)) != 0
+    assert oracle.fits_i16(5000, 200, D)
+    assert not oracle.fits_i16(20000, 20000, D)
+
+
+def test_tie_selection_known_answers(oracle):
+    """mapper.rs:570-589: two ties in reference order, XS below the best."""
+    E = oracle.encode
+    panel = [E("GGGGACGTACGTACGTTTTT"), E("CCCCACGTACGTACGTAAAA"), E("TTTTTTTTTTTTTTTTTTTT")]
+    q = E("ACGTACGTACGT")
+    fwd = [oracle.score(q, r, D, True) for r in panel]
+    best, sub, n_tied, flags, ties = oracle.select(fwd, None, cap=8)
+    assert best == 24 and n_tied == 2 and ties == [0 << 1, 1 << 1] and sub < 24
+    # mapper.rs:722-739: the reverse strand wins when it scores higher
+    read = oracle.revcomp(E("CGTACGTAAAA"))
+    f = [oracle.score(read, r, D, True) for r in panel]
+    rv = [oracle.score(oracle.revcomp(read), r, D, True) for r in panel]
+    b2, _, n2, _, t2 = oracle.select(f, rv)
+    assert b2 > max(f) and t2[0] == (1 << 1) | 1
+    # every candidate tied: no suboptimal
+    b3, s3, n3, fl3, t3 = oracle.select([5, 5, 5], [5, 5, 5], cap=2)
+    assert (b3, s3, n3) == (5, oracle.NO_SCORE, 6) and fl3 & oracle.RESULT_TIES_TRUNCATED
+    assert t3 == [0, 1]
+
+
+@pytest.mark.parametrize("scoring", SCHEMES)
+def test_avx512_equals_scalar(oracle, scoring):
+    """simd/mod.rs:752-810 / 917-1002: both loop orders and the dispatch,
+    by equality, on a ragged 37-reference panel."""
+    rng = Rng(0x5EED_0002)
+    letters = random_panel(rng, 37, 20, 280)
+    panel = [oracle.encode(s) for s in letters]
+    reads = reads_for(rng, letters, 16)
+    reads.append(oracle.encode(b"ACGT" * 80))  # >= 256 nt: the transposed kernel
+    prof = oracle.Profile(panel, scoring)
+    for local in (True, False):
+        want = oracle.score_matrix(reads, panel, scoring, local)
+        for k, q in enumerate(reads):
+            for kernel in (0, 1, 2):
+                got = prof.score_all(q, local, kernel)
+                assert (got == want[k]).all(), (scoring, local, kernel, len(q))
+
+
+def test_avx512_on_fixture_panels(oracle):
+    """simd/mod.rs:817-863: the tRNA fixture reads against both panels."""
+    reads = fixture_reads()
+    assert len(reads) >= 5
+    for tag in ("trna", "trna_ambiguous"):
+        panel = fixture_panel(tag)
+        assert len(panel) == 47
+        for scoring in SCHEMES:
+            prof = oracle.Profile(panel, scoring)
+            for local in (True, False):
+                want = oracle.score_matrix(reads, panel, scoring, local)
+                for k, q in enumerate(reads):
+                    assert (prof.score_all(q, local) == want[k]).all()
+
+
+def test_cpu_batch_equals_scalar_batch(oracle):
+    rng = Rng(0x5EED_0101)
+    letters = random_panel(rng, 37, 20, 280)
+    panel = [oracle.encode(s) for s in letters]
+    reads = reads_for(rng, letters, 30) + [np.zeros(0, np.uint8)]
+    prof = oracle.Profile(panel, D)
+    codes, off, lens = oracle.pack(reads)
+    for local in (True, False):
+        for both in (False, True):
+            a, ta, ra, _ = prof.map_batch(codes, off, lens, local, both, cap=4, rows=True)
+            b, tb, rb = oracle.scalar_map_batch(reads, panel, D, local, both, cap=4, rows=True)
+            assert (a == b).all() and (ta == tb).all() and (ra == rb).all()
