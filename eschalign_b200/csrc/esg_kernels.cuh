@@ -638,6 +638,7 @@ __global__ void __launch_bounds__(256) k5_merge(const K5Params P) {
     uint32_t* out_t = P.ties + (size_t)r * cap;
     if (P.len[r] == 0) {
       P.results[r] = make_int4(INT32_MIN, INT32_MIN, 0, 1 /* ESG_RESULT_EMPTY */);
+      for (uint32_t k = 0; k < cap; ++k) out_t[k] = kNoRef;
       continue;
     }
     const int4 a = P.qhead[r];
@@ -673,6 +674,7 @@ __global__ void __launch_bounds__(256) k5_merge(const K5Params P) {
         }
       }
     }
+    for (uint32_t k = min(n_tied, cap); k < cap; ++k) out_t[k] = kNoRef;  // ESG_NO_TIE
     if (n_tied > cap) flags |= 2;  // ESG_RESULT_TIES_TRUNCATED
     P.results[r] = make_int4(best, sub, (int)n_tied, flags);
   }

@@ -71,6 +71,7 @@ typedef struct esg_read_result {
 } esg_read_result;
 
 #define ESG_NO_SCORE INT32_MIN
+#define ESG_NO_TIE 0xffffffffu       /* tie-list slots past min(n_tied, tie_capacity)  */
 #define ESG_RESULT_EMPTY 1u          /* empty read: no candidates (best = ESG_NO_SCORE) */
 #define ESG_RESULT_TIES_TRUNCATED 2u /* n_tied > tie_capacity: only the first listed    */
 #define ESG_RESULT_RESCORED32 4u     /* some pair was (re)scored by the int32 kernel    */

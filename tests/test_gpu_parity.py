@@ -243,6 +243,10 @@ def test_gpu_prepare_submit_finish_overlap(oracle):
             pending = g.submit(prepared) if prepared is not None else None
         for a, b in zip(one, got):
             assert (a.results == b.results).all() and (a.ties == b.ties).all()
+            # slots past the listed ties hold ESG_NO_TIE
+            n_l = np.minimum(a.results["n_tied"], CAP)
+            unused = np.arange(CAP)[None, :] >= n_l[:, None]
+            assert (a.ties[unused] == 0xFFFFFFFF).all()
 
 
 def test_gpu_strand_swap_property():
