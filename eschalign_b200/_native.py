@@ -34,8 +34,10 @@ def sources():
             if f.endswith((".cu", ".cuh", ".h"))] + [os.path.join(INCLUDE, "eschalign_b200.h")]
 
 
-def _compile(src: str, out: str, verbose: bool) -> None:
-    cmd = [nvcc(), *ARCH_FLAGS, *NVCC_FLAGS, os.path.join(CSRC, src), "-o", out + ".tmp"]
+def _compile(src, out: str, verbose: bool) -> None:
+    srcs = [src] if isinstance(src, str) else list(src)
+    cmd = [nvcc(), *ARCH_FLAGS, *NVCC_FLAGS, *(os.path.join(CSRC, f) for f in srcs), "-o",
+           out + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)
@@ -46,7 +48,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     """Compile csrc/esg_api.cu into libeschalign_b200.so and the integer-pipe
     probe csrc/esg_probe.cu into libesg_probe.so (sm_100a, ahead of time)."""
     newest = max(os.path.getmtime(s) for s in sources())
-    for src, out in (("esg_api.cu", LIB_PATH), ("esg_probe.cu", PROBE_PATH)):
+    for src, out in ((("esg_api.cu", "esg_noalloc.cu"), LIB_PATH), ("esg_probe.cu", PROBE_PATH)):
         if force or not os.path.exists(out) or os.path.getmtime(out) < newest:
             _compile(src, out, verbose)
     return LIB_PATH
@@ -122,6 +124,10 @@ SIGNATURES = {
     "esg_batch_free": (None, [C.c_void_p]),
     "esg_batch_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(EsgBatchStats)]),
     "esg_relaunch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "esg_score_rows_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                           C.c_uint32, C.POINTER(EsgScoring), C.c_int32,
+                                           C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

@@ -260,6 +260,13 @@ const char* esg_status_string(esg_status st) {
 
 const char* esg_last_error(void) { return g_err.c_str(); }
 
+// Lets the other translation unit of the library (esg_noalloc.cu) report
+// through esg_last_error.
+void esg_internal_set_error(esg_status st, const char* msg) {
+  (void)st;
+  g_err = msg ? msg : "";
+}
+
 esg_status esg_device_count(int32_t* out) {
   if (!out) return fail(ESG_ERR_BAD_ARGUMENT, "out is NULL");
   int n = 0;

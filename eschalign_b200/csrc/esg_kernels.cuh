@@ -586,7 +586,7 @@ struct K4Params {
 };
 
 // One warp per listed query: mapper.rs:444-472 over its row.
-__global__ void __launch_bounds__(256) k4_rows(const K4Params P) {
+static __global__ void __launch_bounds__(256) k4_rows(const K4Params P) {
   const uint32_t n_list = P.host_count + (P.redo_count ? min(*P.redo_count, P.redo_cap) : 0u);
   const int lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -631,7 +631,7 @@ struct K5Params {
   uint32_t* ties;      // [read * cap + k]
 };
 
-__global__ void __launch_bounds__(256) k5_merge(const K5Params P) {
+static __global__ void __launch_bounds__(256) k5_merge(const K5Params P) {
   for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < P.n_reads;
        r += gridDim.x * blockDim.x) {
     const uint32_t cap = P.cap;

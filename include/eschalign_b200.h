@@ -183,6 +183,37 @@ esg_status esg_batch_stats_get(const esg_batch* batch, esg_batch_stats* out);
  * kernels alone; the batch's results are overwritten with identical ones. */
 esg_status esg_relaunch(esg_scorer* scorer, esg_batch* batch, void* stream);
 
+/* Scoring for callers that cannot allocate.  No counterpart in the reference.
+ *
+ * Code that runs where cudaMalloc is off limits -- inside someone else's
+ * stream capture, under a framework that owns the device allocator, in a
+ * real-time loop that must not touch the allocator after start-up -- calls
+ * this instead of a scorer: it allocates nothing, host or device.  The
+ * caller passes device buffers: queries (codes 0..4, query q is
+ * d_codes[d_off[q] .. +d_len[q]], scored as given, forward only),
+ * references (d_ref_codes[d_ref_off[r] .. +d_ref_len[r]]) and the output
+ * d_rows[q * n_refs + r] (int32, the scalar oracle's score of every pair,
+ * scalar.rs:120-163).  It runs the plain int32 kernel on `stream` (NULL:
+ * the legacy default stream) and returns without waiting.
+ *
+ * The kernel's scratch is a 16 MiB array reserved on every GPU that loads
+ * the library, held until exit; it limits references to
+ * ESG_NOALLOC_MAX_REF_LEN bases (`max_ref_len`, which must be at least
+ * every d_ref_len; larger values are refused with
+ * ESG_ERR_REFERENCE_TOO_LONG, and a reference longer than the stated
+ * max_ref_len scores ESG_NO_SCORE).  The first call on a device looks up
+ * the array's device address on that device, so make that first call
+ * before any stream capture.  Every call shares the one array: calls whose
+ * kernels overlap on the GPU (other streams, other threads) race and must
+ * be serialized by the caller.  Nothing in the array needs to start at zero. */
+#define ESG_NOALLOC_MAX_REF_LEN 8192
+esg_status esg_score_rows_noalloc(const uint8_t* d_codes, const uint64_t* d_off,
+                                  const uint32_t* d_len, uint32_t n_queries,
+                                  const uint8_t* d_ref_codes, const uint32_t* d_ref_off,
+                                  const uint32_t* d_ref_len, uint32_t n_refs,
+                                  uint32_t max_ref_len, const esg_scoring* scoring, int32_t mode,
+                                  int32_t* d_rows, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
