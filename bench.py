@@ -70,6 +70,10 @@ def args_parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--profile-case", type=int, default=0, metavar="READS",
+                    help="score READS reads of the workload once per kernel and exit "
+                         "(a small target for ncu)")
+    ap.add_argument("--mode", default="local", choices=["local", "semiglobal"])
     return ap.parse_args()
 
 
@@ -246,6 +250,16 @@ def main():
 
     refs = synth.panel_tiles()
     panel_bases = sum(len(r) for r in refs)
+    if a.profile_case:
+        reads = synth.reads_c2(refs, n=a.profile_case)
+        for kernel in (KERNEL_AUTO, KERNEL_PLAIN32):
+            g = GpuScorer(refs, Scoring(*HEADLINE[0]), Mode.parse(a.mode), device=local_rank,
+                          kernel=kernel)
+            r = g.score_batch(reads.tuple(), both_strands=True)
+            print(json.dumps({"profile_case": a.profile_case, "kernel": kernel,
+                              "stats": r.stats}), flush=True)
+            g.close()
+        return
     reads = synth.reads_c2(refs, n=a.reads)  # weak scaling: every rank scores the full batch
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > L2 (126 MB)

@@ -192,9 +192,10 @@ bool k2_takes(const esg_scorer* sc, uint64_t n) {
   if (!sc->batched_ok || n == 0) return false;
   if ((n + kRows - 1) / kRows > (uint64_t)kMaxStripes) return false;
   if (sc->mode == ESG_MODE_SEMIGLOBAL) {
-    // semi-global cells go negative: both sides must stay inside int16
+    // semi-global cells go negative: the biased lanes (H - 16384) must stay
+    // negative and above the -infinity stand-in
     const int64_t mm = std::max(std::abs(sc->scoring.match_score), std::abs(sc->scoring.mismatch));
-    return value_bound(n, sc->max_ref_len, sc->scoring) + mm < 28000;
+    return value_bound(n, sc->max_ref_len, sc->scoring) + mm < 12000;
   }
   return true;  // local: a wrap is detected by the kernel (K2Params::sat)
 }
@@ -406,7 +407,9 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
       sc->tab_a[c] = a;
       sc->tab_b[c] = b;
     }
-    sc->sat = 32767 - ma;
+    // local: a best H at or above this may have left the int16 lanes (the
+    // diagonal term reaches H + ma + bias); such queries are re-scored in int32
+    sc->sat = 32767 - ma - kBiasLocal;
   }
 
   // --- reference pairs and their selectors
@@ -729,9 +732,11 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
     P.redo_cap = b->redo_cap;
     memcpy(P.tab_a, sc->tab_a, sizeof P.tab_a);
     memcpy(P.tab_b, sc->tab_b, sizeof P.tab_b);
-    P.o2 = pack16x2(sc->scoring.gap_open, sc->scoring.gap_open);
     P.e2 = pack16x2(sc->scoring.gap_extend, sc->scoring.gap_extend);
     P.o = sc->scoring.gap_open;
+    P.e = sc->scoring.gap_extend;
+    P.bias = sc->mode == ESG_MODE_LOCAL ? kBiasLocal : kBiasSemiGlobal;
+    P.one = 1;
     P.sat = sc->sat;
     P.cap = sc->cap;
     const int blocks =

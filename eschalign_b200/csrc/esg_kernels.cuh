@@ -30,9 +30,20 @@ namespace esg {
 
 constexpr int kRows = 16;             // rows per lane stripe (k2)
 constexpr int kMaxStripes = 32;       // a query spans at most one warp (k2)
-constexpr int kNeg16 = -30000;        // int16 stand-in for -infinity
+constexpr int kNeg16 = -31500;        // int16 stand-in for -infinity (biased domain)
+constexpr int kBiasLocal = 2048;      // local: H + B >= B >= |o|, |e|
+constexpr int kBiasSemiGlobal = -16384;  // semi-global: H + B < 0 while |H| < 12000
 constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
-constexpr int kK2Warps = 8;           // warps per k2 CTA
+// k2 CTA shape: 4 warps, 5 resident CTAs per SM (20 warps, <= 102 registers;
+// 4 CTAs for panels with wildcards, whose per-row tables need more) measured
+// fastest on B200 for the C2 workload (vs 8 warps x 2 CTAs).
+#ifndef ESG_K2_WARPS
+#define ESG_K2_WARPS 4
+#endif
+#ifndef ESG_K2_MIN_BLOCKS
+#define ESG_K2_MIN_BLOCKS 5
+#endif
+constexpr int kK2Warps = ESG_K2_WARPS;  // warps per k2 CTA
 constexpr int kK2Threads = kK2Warps * 32;
 constexpr int kK3Threads = 256;
 constexpr uint32_t kFull = 0xffffffffu;
@@ -55,6 +66,13 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
 __device__ __forceinline__ uint32_t add16x2(uint32_t a, uint32_t b) {
   uint32_t d;
   asm("add.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+// a * b + c as a 32-bit IMAD, which issues to the FMA pipe and so keeps the
+// integer ALU free for the DPX ops
+__device__ __forceinline__ uint32_t mad_lo(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
   return d;
 }
 __device__ __forceinline__ uint32_t max16x2(uint32_t a, uint32_t b) {
@@ -127,9 +145,11 @@ struct K2Params {
   // scoring, pre-shifted by the gap open (see k2_batched)
   uint32_t tab_a[6];
   uint32_t tab_b[6];
-  uint32_t o2, e2;
-  int32_t o;
-  int32_t sat;           // local: a best at or above this may have wrapped
+  uint32_t e2;           // e in both halves
+  int32_t o, e;
+  int32_t bias;          // value bias of the int16 lanes
+  uint32_t one;          // the constant 1 (a multiplier the compiler cannot fold)
+  int32_t sat;           // local: a best (unbiased) at or above this may have wrapped
   uint32_t cap;
 };
 
@@ -186,27 +206,42 @@ __device__ __forceinline__ bool stage_panel(void* smem, const void* gsrc, uint32
 // One warp, one task: up to 32 queries whose stripes fill the warp's lanes,
 // scored against every reference pair of the panel.
 //
+// Values are held biased: every H, E, F of the recurrence is stored as
+// value + B (B = P.bias: +2048 in local mode, -16384 in semi-global), in
+// signed 16-bit halves, two references per register (low half: the longer
+// reference of the pair, high half: the shorter one).
+//
 // Lane state (rows r = 0..15 of the lane's stripe):
 //   ta[r], tb[r]  PRMT tables of the row's read code c: byte x of {tb, ta} is
 //                 s(c, x) - o for reference code x = 0..3, 4 (wildcard), and
-//                 a padding column's score at x = 5.  Both halves of a
-//                 register use the same table; the column's selector picks a
-//                 byte per half and sign-extends it to 16 bits.
-//   ho[r]         H + o of the row at the previous column (both halves)
-//   e[r]          E of the row at the previous column
-// Keeping H + o instead of H lets one packed add per cell feed both the E
-// of the next column and the F of the next row: the diagonal term is then
-// (H_diag + o) + (s - o), which is why the tables hold s - o.
+//                 a padding column's score at x = 5.  Both halves use the
+//                 same table; the column's selector picks a byte per half
+//                 and sign-extends it to 16 bits.
+//   g[r]          G = H + o + B of the row at the previous column
+//   ev[r]         E + B of the row at the previous column
+// Every integer ALU instruction (PRMT, the DPX VIADDMNMX / VIMNMX3, plain
+// MAX) takes the same ALU issue slot, so the loop is written for the fewest
+// of them: G feeds E of the next column and F of the next row (one
+// VIADDMNMX each: max(X + e, G)); the diagonal term is G_diag + (s - o), which
+// is why the tables hold s - o (one VIADDMNMX); H + B = max(h1, F, B) is one
+// VIMNMX3 in local mode (B, the zero floor), one MAX in semi-global; the
+// running best takes one VIMNMX3 per two rows.  G = H + B + o is a 32-bit
+// IMAD (H * 1 + o * 65537, on the FMA pipe): exact in both halves because
+// the low half's value is never in [0, |o|) -- local H + B >= B >= |o|,
+// semi-global H + B < 0 -- so its borrow cancels the constant's, and the
+// high half's carry-out is discarded.  Padding columns (garbage that may
+// wrap) are only ever in the high half.  5.5 ALU instructions per cell pair
+// in local mode, 5 in semi-global, plus one IMAD.
 //
 // A query of n rows takes S = ceil(n / 16) lanes; its stripes are aligned so
 // the read's last row is row 15 of its last lane, and the P = 16 S - n rows
 // before the read's first row score 0 against every real column: they hold
 // H = 0 exactly, the top border the first real row needs, in both modes.
 // Lane l with stripe index s works on column j = t - s at step t; its top
-// input (H + o and F of the row above) is lane l-1's bottom output of step
-// t-1, fetched by shuffle; a query's first lane takes the border instead.
+// input (G and F of the row above) is lane l-1's bottom output of step t-1,
+// fetched by shuffle; a query's first lane takes the border instead.
 template <bool kLocal, bool kPanelW, bool kSmemPanel>
-__global__ void __launch_bounds__(kK2Threads, 2) k2_batched(const K2Params P) {
+__global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k2_batched(const K2Params P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint64_t panel_bar;
   const int lane = threadIdx.x & 31;
@@ -230,7 +265,12 @@ __global__ void __launch_bounds__(kK2Threads, 2) k2_batched(const K2Params P) {
   int* slot = slots + (size_t)(wib * 32 + lane) * (4 + cap);
   uint32_t* sties = reinterpret_cast<uint32_t*>(slot + 4);
 
-  const uint32_t o2 = P.o2, e2 = P.e2;
+  const int bias = P.bias;
+  const uint32_t g0 = pack16x2(bias + P.o, bias + P.o);  // G of a zero border cell
+  const uint32_t bias2 = pack16x2(bias, bias);           // H = 0 (the local floor)
+  const uint32_t o32 = (uint32_t)(P.o * 65537);           // + o in both halves, 32-bit add
+  const uint32_t e2 = P.e2;
+  const uint32_t one = P.one;  // 1, opaque to the compiler: keeps G's add an IMAD
   const uint32_t neg2 = pack16x2(kNeg16, kNeg16);
 
   for (;;) {
@@ -310,70 +350,67 @@ __global__ void __launch_bounds__(kK2Threads, 2) k2_batched(const K2Params P) {
 
     for (uint32_t p = 0; p < P.n_pairs; ++p) {
       const uint4 pm = pairs[p];
-      const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);
-      const int m = max(mA, mB);
-      const int mshort = min(mA, mB);
-      const int jshort = (mB > 0 && mshort < m) ? mshort - 1 : -1;
+      const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);  // mA >= mB
+      const int m = mA;
+      const int jshort = (mB > 0 && mB < mA) ? mB - 1 : -1;
       const uint16_t* sp = sels + pm.x;
       const int steps = m + smax - 1;
 
-      uint32_t ho[kRows], ev[kRows];
+      uint32_t g[kRows], ev[kRows];
 #pragma unroll
       for (int r = 0; r < kRows; ++r) {
-        ho[r] = o2;
+        g[r] = g0;
         ev[r] = neg2;
       }
-      uint32_t hdc = o2;              // H + o of the row above, previous column
-      uint32_t hobot = o2, fbot = neg2;
-      uint32_t best = 0;              // local: max H over this lane's cells
-      uint32_t lastrow = neg2;        // semi-global: max H of row 15 over columns
+      uint32_t gdc = g0;              // G of the row above, previous column
+      uint32_t gbot = g0, fbot = neg2;
+      uint32_t best = bias2;          // local: max H + B over this lane's cells
+      uint32_t lastrow = neg2;        // semi-global: max H + B of row 15 over columns
       uint32_t s_col = neg2, s_last = neg2;  // semi-global short-half snapshot
 
 #pragma unroll 1
       for (int t = 0; t < steps; ++t) {
         const int j = t - s;
-        uint32_t hot = __shfl_up_sync(kFull, hobot, 1);
+        uint32_t gt = __shfl_up_sync(kFull, gbot, 1);
         uint32_t ft = __shfl_up_sync(kFull, fbot, 1);
         if (first) {
-          hot = o2;
+          gt = g0;
           ft = neg2;
         }
         if ((unsigned)j < (unsigned)m) {
           const uint32_t sel = sp[j];
-          uint32_t hd = hdc;
-          hdc = hot;
-          uint32_t hup = hot, f = ft, hprev = 0, h15 = 0;
+          uint32_t gd = gdc;
+          gdc = gt;
+          uint32_t gup = gt, f = ft, h15 = 0, hprev = 0;
 #pragma unroll
           for (int r = 0; r < kRows; ++r) {
             const uint32_t sc = prmt(ta[r], tb[kPanelW ? r : 0], sel);
-            ev[r] = __viaddmax_s16x2(ev[r], e2, ho[r]);
-            f = __viaddmax_s16x2(f, e2, hup);
-            const uint32_t h1 = __viaddmax_s16x2(hd, sc, ev[r]);
+            ev[r] = __viaddmax_s16x2(ev[r], e2, g[r]);
+            f = __viaddmax_s16x2(f, e2, gup);
+            const uint32_t h1 = __viaddmax_s16x2(gd, sc, ev[r]);
             uint32_t h;
             if constexpr (kLocal) {
-              h = __vimax_s16x2_relu(h1, f);
-            } else {
-              h = max16x2(h1, f);
-            }
-            hd = ho[r];
-            ho[r] = add16x2(h, o2);
-            hup = ho[r];
-            if constexpr (kLocal) {
+              h = __vimax3_s16x2(h1, f, bias2);
               if (r & 1)
                 best = __vimax3_s16x2(best, hprev, h);
               else
                 hprev = h;
+            } else {
+              h = max16x2(h1, f);
             }
+            gd = g[r];
+            g[r] = mad_lo(h, one, o32);
+            gup = g[r];
             if (r == kRows - 1) h15 = h;
           }
-          hobot = ho[kRows - 1];
+          gbot = g[kRows - 1];
           fbot = f;
           if constexpr (!kLocal) {
             lastrow = max16x2(lastrow, h15);
             if (j == jshort) {
               uint32_t cm = neg2;
 #pragma unroll
-              for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? neg2 : ho[r]);
+              for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? neg2 : g[r]);
               s_col = cm;
               s_last = lastrow;
             }
@@ -388,17 +425,12 @@ __global__ void __launch_bounds__(kK2Threads, 2) k2_batched(const K2Params P) {
       } else {
         uint32_t cm = neg2;
 #pragma unroll
-        for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? neg2 : ho[r]);
+        for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? neg2 : g[r]);
         lr = lastrow;
         if (jshort >= 0) {
-          // the short half's last column and last row were taken at its end
-          if (mA < mB) {
-            cm = (cm & 0xffff0000u) | (s_col & 0xffffu);
-            lr = (lr & 0xffff0000u) | (s_last & 0xffffu);
-          } else {
-            cm = (cm & 0xffffu) | (s_col & 0xffff0000u);
-            lr = (lr & 0xffffu) | (s_last & 0xffff0000u);
-          }
+          // the short (high) half's last column and last row, taken at its end
+          cm = (cm & 0xffffu) | (s_col & 0xffff0000u);
+          lr = (lr & 0xffffu) | (s_last & 0xffff0000u);
         }
         v = cm;
       }
@@ -410,12 +442,12 @@ __global__ void __launch_bounds__(kK2Threads, 2) k2_batched(const K2Params P) {
       if (last) {
         int scA, scB;
         if constexpr (kLocal) {
-          scA = lo16(v);
-          scB = hi16(v);
+          scA = lo16(v) - bias;
+          scB = hi16(v) - bias;
           if (scA >= P.sat || (mB > 0 && scB >= P.sat)) slot[3] |= kQRedo;
         } else {
-          scA = max(lo16(v) - P.o, lo16(lr));
-          scB = max(hi16(v) - P.o, hi16(lr));
+          scA = max(lo16(v) - P.o, lo16(lr)) - bias;
+          scB = max(hi16(v) - P.o, hi16(lr)) - bias;
         }
         const uint32_t rbit = rc ? 1u : 0u;
         slot_add(slot, sties, cap, (pm.z << 1) | rbit, scA);
