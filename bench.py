@@ -46,9 +46,10 @@ HEADLINE = ((2, -1, -10, -1), "local")
 COMBOS = [((2, -1, -10, -1), "local"), ((2, -1, -10, -1), "semiglobal"),
           ((1, -1, -2, -1), "local"), ((1, -1, -2, -1), "semiglobal")]
 OPS_PER_CELL = {"local": 12, "semiglobal": 11}
-# DRAM bytes per DP cell of the batched kernel, from the ncu capture summarised
-# in profiles/k2_batched_c2.md (None until measured).
-K2_DRAM_BYTES_PER_CELL = None
+# DRAM bytes per DP cell of the batched kernel: 3.22 MB over 9.71e10 cells in
+# the ncu capture of a 20 000-read C2 launch (profiles/k2_batched_c2.md);
+# traffic grows with the reads, so it scales by cells to the full launch.
+K2_DRAM_BYTES_PER_CELL = 3.22e6 / 9.7056e10
 
 
 def env_int(name, default):
