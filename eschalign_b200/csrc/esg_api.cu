@@ -119,7 +119,12 @@ struct esg_scorer {
   int sat = 0;
   int k2_blocks = 0;
   size_t k2_smem = 0;
+  uint2* d_lbuf = nullptr;   // long queries: one column buffer per k2 warp
+  uint32_t lbuf_cols = 0;
   const void* k2_fn = nullptr;
+  const void* k2_long_fn = nullptr;
+  cudaStream_t aux = nullptr;          // second stream: the long-query kernel
+  cudaEvent_t fork = nullptr, join = nullptr;
   // k3 panel (longest first)
   uint8_t* d_rcodes = nullptr;
   uint32_t* d_roff = nullptr;
@@ -140,6 +145,7 @@ struct esg_batch {
   uint64_t total_bases = 0;
   // host plan
   uint32_t n_tasks = 0;
+  uint32_t n_long = 0;   // the first n_long tasks are single long queries
   uint32_t n_order = 0;
   uint32_t host_list = 0;
   uint32_t redo_cap = 0;
@@ -190,7 +196,9 @@ int64_t value_bound(uint64_t n, uint32_t max_ref_len, const esg_scoring& s) {
 
 bool k2_takes(const esg_scorer* sc, uint64_t n) {
   if (!sc->batched_ok || n == 0) return false;
-  if ((n + kRows - 1) / kRows > (uint64_t)kMaxStripes) return false;
+  // queries over 32 stripes run in passes chained through the column buffer
+  if ((n + kRows - 1) / kRows > (uint64_t)kMaxStripes && !sc->d_lbuf) return false;
+  if ((n + kRows - 1) / kRows > 0xffffu) return false;
   if (sc->mode == ESG_MODE_SEMIGLOBAL) {
     // semi-global cells go negative: the biased lanes (H - 16384) must stay
     // negative and above the -infinity stand-in
@@ -215,23 +223,26 @@ T* carve(char*& at, size_t count) {
 
 size_t carve_size(size_t count, size_t elem) { return (count * elem + 255) / 256 * 256; }
 
+template <bool kLong>
+const void* pick_k2(bool local, bool w, bool smem) {
+  if (local) {
+    if (w)
+      return smem ? (const void*)k2_batched<true, true, true, kLong>
+                  : (const void*)k2_batched<true, true, false, kLong>;
+    return smem ? (const void*)k2_batched<true, false, true, kLong>
+                : (const void*)k2_batched<true, false, false, kLong>;
+  }
+  if (w)
+    return smem ? (const void*)k2_batched<false, true, true, kLong>
+                : (const void*)k2_batched<false, true, false, kLong>;
+  return smem ? (const void*)k2_batched<false, false, true, kLong>
+              : (const void*)k2_batched<false, false, false, kLong>;
+}
+
 void set_k2_fn(esg_scorer* sc) {
   const bool local = sc->mode == ESG_MODE_LOCAL;
-  if (local) {
-    if (sc->panel_w)
-      sc->k2_fn = sc->smem_panel ? (const void*)k2_batched<true, true, true>
-                                 : (const void*)k2_batched<true, true, false>;
-    else
-      sc->k2_fn = sc->smem_panel ? (const void*)k2_batched<true, false, true>
-                                 : (const void*)k2_batched<true, false, false>;
-  } else {
-    if (sc->panel_w)
-      sc->k2_fn = sc->smem_panel ? (const void*)k2_batched<false, true, true>
-                                 : (const void*)k2_batched<false, true, false>;
-    else
-      sc->k2_fn = sc->smem_panel ? (const void*)k2_batched<false, false, true>
-                                 : (const void*)k2_batched<false, false, false>;
-  }
+  sc->k2_fn = pick_k2<false>(local, sc->panel_w, sc->smem_panel);
+  sc->k2_long_fn = pick_k2<true>(local, sc->panel_w, sc->smem_panel);
   sc->k3_fn = local ? (const void*)k3_plain<true> : (const void*)k3_plain<false>;
 }
 
@@ -475,8 +486,14 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
   set_k2_fn(sc);
   sc->k2_smem = (sc->smem_panel ? sc->blob_bytes : 0) + slots;
   if ((e = cudaFuncSetAttribute(sc->k2_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sc->k2_smem)) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(sc->k2_long_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sc->k2_smem)) != cudaSuccess)
     return cleanup(cuda_fail(e, "cudaFuncSetAttribute(k2)"));
+  if ((e = cudaStreamCreateWithFlags(&sc->aux, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&sc->fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&sc->join, cudaEventDisableTiming)) != cudaSuccess)
+    return cleanup(cuda_fail(e, "cudaStreamCreate(aux)"));
   int occ2 = 0, occ3 = 0;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, sc->k2_fn, kK2Threads,
                                                          sc->k2_smem)) != cudaSuccess ||
@@ -484,6 +501,12 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
           cudaSuccess)
     return cleanup(cuda_fail(e, "cudaOccupancy"));
   sc->k2_blocks = std::max(1, occ2) * sc->sm_count;
+  if (sc->batched_ok && max_len <= 8192) {
+    sc->lbuf_cols = max_len;
+    const size_t lb = (size_t)sc->k2_blocks * kK2Warps * max_len * sizeof(uint2);
+    if ((e = cudaMalloc(&sc->d_lbuf, lb)) != cudaSuccess)
+      return cleanup(cuda_fail(e, "cudaMalloc(long-query buffer)"));
+  }
   sc->k3_blocks = std::max(1, occ3) * sc->sm_count;
   // k3's stripe boundary: one int2 per reference column per thread, at most 2 GiB
   const size_t per_thread = (size_t)max_len * sizeof(int2);
@@ -531,6 +554,13 @@ void esg_scorer_free(esg_scorer* sc) {
   cudaFree(sc->d_rlen);
   cudaFree(sc->d_ridx);
   cudaFree(sc->d_scratch);
+  cudaFree(sc->d_lbuf);
+  if (sc->aux) {
+    cudaStreamSynchronize(sc->aux);
+    cudaStreamDestroy(sc->aux);
+  }
+  if (sc->fork) cudaEventDestroy(sc->fork);
+  if (sc->join) cudaEventDestroy(sc->join);
   if (sc->own_stream && sc->stream) cudaStreamDestroy(sc->stream);
   delete sc;
 }
@@ -576,6 +606,7 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
 
   // --- plan: which queries go where
   std::vector<uint32_t> by_s_count(kMaxStripes + 1, 0);
+  std::vector<std::pair<uint32_t, uint32_t>> long_q;  // (stripes, query), one task each
   std::vector<uint8_t> route(b->n_q, 0);  // 0 empty, 1 k2, 2 k3
   uint32_t n_k2 = 0, n_k3 = 0, n_empty = 0, redo_cap = 0;
   uint64_t cells = 0;
@@ -587,9 +618,14 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
     }
     cells += (uint64_t)n * sc->panel_bases;
     if (b->kernel == ESG_KERNEL_AUTO && k2_takes(sc, n)) {
-      route[q] = 1;
-      ++n_k2;
-      ++by_s_count[(n + kRows - 1) / kRows];
+      const uint32_t S = (n + kRows - 1) / kRows;
+      if (S > (uint32_t)kMaxStripes) {
+        long_q.push_back({S, q});
+      } else {
+        route[q] = 1;
+        ++n_k2;
+        ++by_s_count[S];
+      }
       if (k2_may_flag(sc, n)) ++redo_cap;
     } else {
       route[q] = 2;
@@ -644,14 +680,21 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
       open_mask |= 1u << f;
     }
   }
-  b->n_tasks = (uint32_t)bin_free.size();
-  b->n_order = n_k2;
+  // long queries first (longest first), then the packed tiles
+  std::sort(long_q.begin(), long_q.end(),
+            [](const std::pair<uint32_t, uint32_t>& a, const std::pair<uint32_t, uint32_t>& c) {
+              return a.first > c.first;
+            });
+  const uint32_t n_long = (uint32_t)long_q.size();
+  b->n_long = n_long;
+  b->n_tasks = n_long + (uint32_t)bin_free.size();
+  b->n_order = n_k2 + n_long;
 
   // --- pinned staging for the inputs
   const size_t sz_codes = carve_size(total ? total : 1, 1);
   const size_t sz_off = carve_size(n_reads ? n_reads : 1, 8);
   const size_t sz_len = carve_size(n_reads ? n_reads : 1, 4);
-  const size_t sz_order = carve_size(n_k2 ? n_k2 : 1, 4);
+  const size_t sz_order = carve_size(b->n_order ? b->n_order : 1, 4);
   const size_t sz_tasks = carve_size(b->n_tasks ? b->n_tasks : 1, 8);
   const size_t sz_list = carve_size(n_k3 + redo_cap ? n_k3 + redo_cap : 1, 4);
   b->in_bytes = sz_codes + sz_off + sz_len + sz_order + sz_tasks + sz_list;
@@ -664,7 +707,7 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   b->h_codes = carve<uint8_t>(at, total ? total : 1);
   b->h_off = carve<uint64_t>(at, n_reads ? n_reads : 1);
   b->h_len = carve<uint32_t>(at, n_reads ? n_reads : 1);
-  b->h_order = carve<uint32_t>(at, n_k2 ? n_k2 : 1);
+  b->h_order = carve<uint32_t>(at, b->n_order ? b->n_order : 1);
   b->h_tasks = carve<uint2>(at, b->n_tasks ? b->n_tasks : 1);
   b->h_list = carve<uint32_t>(at, n_k3 + redo_cap ? n_k3 + redo_cap : 1);
   uint64_t pos = 0;
@@ -674,15 +717,23 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
     if (len[k]) memcpy(b->h_codes + pos, codes + off[k], len[k]);
     pos += len[k];
   }
-  // order[] grouped by task, tasks[] = {start, count | smax << 16}
+  // order[] grouped by task, tasks[] = {start, count | smax << 16}; long
+  // queries are single-query tasks whose smax is their stripe count (> 32)
   {
-    std::vector<uint32_t> tstart(b->n_tasks + 1, 0);
-    for (uint32_t t = 0; t < b->n_tasks; ++t) tstart[t + 1] = tstart[t] + bin_count[t];
+    uint32_t lanes = 0;
+    for (uint32_t t = 0; t < n_long; ++t) {
+      b->h_order[t] = long_q[t].second;
+      b->h_tasks[t] = make_uint2(t, 1u | (long_q[t].first << 16));
+      lanes += long_q[t].first;
+    }
+    const uint32_t n_bins = (uint32_t)bin_free.size();
+    std::vector<uint32_t> tstart(n_bins + 1, n_long);
+    for (uint32_t t = 0; t < n_bins; ++t) tstart[t + 1] = tstart[t] + bin_count[t];
     std::vector<uint32_t> fill(tstart.begin(), tstart.end() - 1);
     for (uint32_t i = 0; i < n_k2; ++i) b->h_order[fill[bin_of[i]]++] = sorted[i];
-    uint32_t lanes = 0;
-    for (uint32_t t = 0; t < b->n_tasks; ++t) {
-      b->h_tasks[t] = make_uint2(tstart[t], (uint32_t)bin_count[t] | ((uint32_t)bin_smax[t] << 16));
+    for (uint32_t t = 0; t < n_bins; ++t) {
+      b->h_tasks[n_long + t] =
+          make_uint2(tstart[t], (uint32_t)bin_count[t] | ((uint32_t)bin_smax[t] << 16));
       lanes += kMaxStripes - bin_free[t];
     }
     b->stats.lanes_used = lanes;
@@ -695,7 +746,7 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   b->stats.n_reads = n_reads;
   b->stats.n_queries = b->n_q;
   b->stats.n_empty = n_empty;
-  b->stats.queries_batched = n_k2;
+  b->stats.queries_batched = n_k2 + n_long;
   b->stats.queries_plain = n_k3;
   b->stats.tasks = b->n_tasks;
   b->stats.cells = cells;
@@ -737,13 +788,39 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
     P.e = sc->scoring.gap_extend;
     P.bias = sc->mode == ESG_MODE_LOCAL ? kBiasLocal : kBiasSemiGlobal;
     P.one = 1;
+    P.lbuf = sc->d_lbuf;
+    P.lbuf_cols = sc->lbuf_cols;
     P.sat = sc->sat;
     P.cap = sc->cap;
-    const int blocks =
-        (int)std::min<uint64_t>((uint64_t)sc->k2_blocks, (b->n_tasks + kK2Warps - 1) / kK2Warps);
-    void* args[] = {&P};
-    ESG_CUDA(cudaLaunchKernel(sc->k2_fn, dim3(blocks), dim3(kK2Threads), args, sc->k2_smem, st));
-    ++kernels;
+    // long queries on the aux stream, launched first so their CTAs are
+    // resident beside the persistent tile kernel rather than after it
+    const uint32_t n_long = b->n_long, n_tiles = b->n_tasks - b->n_long;
+    if (n_long) {
+      K2Params L = P;
+      L.n_tasks = n_long;
+      const int lblocks =
+          (int)std::min<uint64_t>((uint64_t)sc->k2_blocks, (n_long + kK2Warps - 1) / kK2Warps);
+      ESG_CUDA(cudaEventRecord(sc->fork, st));
+      ESG_CUDA(cudaStreamWaitEvent(sc->aux, sc->fork, 0));
+      void* largs[] = {&L};
+      ESG_CUDA(cudaLaunchKernel(sc->k2_long_fn, dim3(lblocks), dim3(kK2Threads), largs,
+                                sc->k2_smem, sc->aux));
+      ++kernels;
+    }
+    if (n_tiles) {
+      K2Params T = P;
+      T.tasks = P.tasks + n_long;
+      T.n_tasks = n_tiles;
+      const int blocks =
+          (int)std::min<uint64_t>((uint64_t)sc->k2_blocks, (n_tiles + kK2Warps - 1) / kK2Warps);
+      void* args[] = {&T};
+      ESG_CUDA(cudaLaunchKernel(sc->k2_fn, dim3(blocks), dim3(kK2Threads), args, sc->k2_smem, st));
+      ++kernels;
+    }
+    if (n_long) {
+      ESG_CUDA(cudaEventRecord(sc->join, sc->aux));
+      ESG_CUDA(cudaStreamWaitEvent(st, sc->join, 0));
+    }
   }
   const bool k3 = b->host_list + b->redo_cap > 0;
   if (k3) {

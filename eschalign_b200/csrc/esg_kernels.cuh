@@ -133,7 +133,7 @@ struct K2Params {
   const uint32_t* order;
   const uint2* tasks;
   uint32_t n_tasks;
-  uint32_t* counters;    // [0] task counter, [1] redo count, [2] error bits
+  uint32_t* counters;    // [0] tile counter, [1] redo count, [2] error bits, [3] long counter
   // outputs
   int4* qhead;           // per query {best, suboptimal, n_tied, flags}
   uint32_t* qties;       // per query cap candidates
@@ -149,6 +149,8 @@ struct K2Params {
   int32_t o, e;
   int32_t bias;          // value bias of the int16 lanes
   uint32_t one;          // the constant 1 (a multiplier the compiler cannot fold)
+  uint2* lbuf;           // long queries: per-warp column buffer (G, F), lbuf_cols each
+  uint32_t lbuf_cols;
   int32_t sat;           // local: a best (unbiased) at or above this may have wrapped
   uint32_t cap;
 };
@@ -203,12 +205,11 @@ __device__ __forceinline__ bool stage_panel(void* smem, const void* gsrc, uint32
   return ok;
 }
 
-// One warp, one task: up to 32 queries whose stripes fill the warp's lanes,
-// scored against every reference pair of the panel.
+// One systolic pass of a warp over the columns of one reference pair.
 //
 // Values are held biased: every H, E, F of the recurrence is stored as
-// value + B (B = P.bias: +2048 in local mode, -16384 in semi-global), in
-// signed 16-bit halves, two references per register (low half: the longer
+// value + B (B = bias: +2048 in local mode, -16384 in semi-global), in signed
+// 16-bit halves, two references per register (low half: the longer
 // reference of the pair, high half: the shorter one).
 //
 // Lane state (rows r = 0..15 of the lane's stripe):
@@ -233,14 +234,192 @@ __device__ __forceinline__ bool stage_panel(void* smem, const void* gsrc, uint32
 // wrap) are only ever in the high half.  5.5 ALU instructions per cell pair
 // in local mode, 5 in semi-global, plus one IMAD.
 //
-// A query of n rows takes S = ceil(n / 16) lanes; its stripes are aligned so
-// the read's last row is row 15 of its last lane, and the P = 16 S - n rows
-// before the read's first row score 0 against every real column: they hold
-// H = 0 exactly, the top border the first real row needs, in both modes.
-// Lane l with stripe index s works on column j = t - s at step t; its top
-// input (G and F of the row above) is lane l-1's bottom output of step t-1,
-// fetched by shuffle; a query's first lane takes the border instead.
-template <bool kLocal, bool kPanelW, bool kSmemPanel>
+// The lane with skew k works on column j = t - k at step t; its top input
+// (G and F of the row above) is the previous lane's bottom output of step
+// t-1, fetched by shuffle.  A query's first lane takes the border instead.
+// In a long pass (kLong), lane 0 takes its top input from `buf` (the bottom
+// row of the previous pass) when `from_buf`, and lane 31 writes its bottom
+// row to `buf` when `to_buf`: lane 0 reads column j at step j, lane 31
+// overwrites it at step j + 31, so one buffer serves every pass.
+//
+// Returns, per lane, the pass's local best (H + B) or semi-global last-column
+// maximum (G, the short half's taken at its own end) in `v`, and the
+// semi-global maximum of row 15 over the lane's columns (H + B) in `lr`.
+struct PassConst {
+  uint32_t g0, neg2, e2, o32, one, bias2;
+};
+
+// A column's 16-bit PRMT selector: an explicit shared-memory load when the
+// panel is staged in shared memory, a read-only global load otherwise.
+template <bool kSmem>
+__device__ __forceinline__ uint32_t load_sel(const uint16_t* sp, int j) {
+  if constexpr (kSmem) {
+    uint16_t v;
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(sp + j);
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
+    return v;
+  } else {
+    return __ldg(sp + j);
+  }
+}
+
+template <bool kLocal, bool kPanelW, bool kLong, bool kSmem>
+__device__ __forceinline__ void pair_pass(const uint32_t (&ta)[kRows],
+                                          const uint32_t (&tb)[kPanelW ? kRows : 1], int skew,
+                                          bool active_lane, bool first, uint32_t padmask, int m,
+                                          int jshort, const uint16_t* __restrict__ sp, int steps,
+                                          const PassConst& K, uint2* buf, bool from_buf,
+                                          bool to_buf, uint32_t& v, uint32_t& lr) {
+  const int lane = threadIdx.x & 31;
+  uint32_t g[kRows], ev[kRows];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    g[r] = K.g0;
+    ev[r] = K.neg2;
+  }
+  uint32_t gdc = K.g0;  // G of the row above, previous column
+  uint32_t gbot = K.g0, fbot = K.neg2;
+  uint32_t best = K.bias2;                 // local: max H + B over this lane's cells
+  uint32_t lastrow = K.neg2;               // semi-global: max H + B of row 15
+  uint32_t s_col = K.neg2, s_last = K.neg2;  // semi-global short-half snapshot
+  // inactive lanes of a tile sit at a skew no step reaches; only the long
+  // path needs the per-lane bound (its lanes past the query's last stripe)
+  const int mlim = (kLong && !active_lane) ? 0 : m;
+
+#pragma unroll 1
+  for (int t = 0; t < steps; ++t) {
+    const int j = t - skew;
+    uint32_t gt = __shfl_up_sync(kFull, gbot, 1);
+    uint32_t ft = __shfl_up_sync(kFull, fbot, 1);
+    if (first) {
+      gt = K.g0;
+      ft = K.neg2;
+    }
+    if ((unsigned)j < (unsigned)mlim) {
+      if constexpr (kLong) {
+        if (from_buf && lane == 0) {
+          const uint2 b = buf[j];
+          gt = b.x;
+          ft = b.y;
+        }
+      }
+      const uint32_t sel = load_sel<kSmem>(sp, j);
+      uint32_t gd = gdc;
+      gdc = gt;
+      uint32_t gup = gt, f = ft, h15 = 0, hprev = 0;
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const uint32_t sc = prmt(ta[r], tb[kPanelW ? r : 0], sel);
+        ev[r] = __viaddmax_s16x2(ev[r], K.e2, g[r]);
+        f = __viaddmax_s16x2(f, K.e2, gup);
+        const uint32_t h1 = __viaddmax_s16x2(gd, sc, ev[r]);
+        uint32_t h;
+        if constexpr (kLocal) {
+          h = __vimax3_s16x2(h1, f, K.bias2);
+          if (r & 1)
+            best = __vimax3_s16x2(best, hprev, h);
+          else
+            hprev = h;
+        } else {
+          h = max16x2(h1, f);
+        }
+        gd = g[r];
+        g[r] = mad_lo(h, K.one, K.o32);
+        gup = g[r];
+        if (r == kRows - 1) h15 = h;
+      }
+      gbot = g[kRows - 1];
+      fbot = f;
+      if constexpr (kLong) {
+        if (to_buf && lane == 31) buf[j] = make_uint2(gbot, fbot);
+      }
+      if constexpr (!kLocal) {
+        lastrow = max16x2(lastrow, h15);
+        if (j == jshort) {
+          uint32_t cm = K.neg2;
+#pragma unroll
+          for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
+          s_col = cm;
+          s_last = lastrow;
+        }
+      }
+    }
+  }
+  if constexpr (kLocal) {
+    v = best;
+    lr = 0;
+  } else {
+    uint32_t cm = K.neg2;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
+    if (jshort >= 0) {
+      // the short (high) half's last column and last row, taken at its end
+      cm = (cm & 0xffffu) | (s_col & 0xffff0000u);
+      lastrow = (lastrow & 0xffffu) | (s_last & 0xffff0000u);
+    }
+    v = active_lane ? cm : K.neg2;
+    lr = lastrow;
+  }
+}
+
+// Row tables of stripe `s` of a query (n codes at q, reverse complement if
+// rc): row r is read row i = 16 s + r - pad; rows before the read are padding.
+template <bool kPanelW>
+__device__ __forceinline__ void row_tables(const K2Params& P, const uint8_t* q, uint32_t n,
+                                           bool rc, bool valid, int s, int pad,
+                                           uint32_t (&ta)[kRows],
+                                           uint32_t (&tb)[kPanelW ? kRows : 1]) {
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    const int i = s * kRows + r - pad;
+    uint32_t c = 5;  // padding row
+    if (valid && i >= 0) {
+      uint32_t x = rc ? q[n - 1 - i] : q[i];
+      x = x > 4 ? 4 : x;
+      c = (rc && x < 4) ? 3 - x : x;
+    }
+    ta[r] = P.tab_a[c];
+    if constexpr (kPanelW) tb[r] = P.tab_b[c];
+  }
+  if constexpr (!kPanelW) tb[0] = P.tab_b[0];
+}
+
+// The last lane of a query folds one reference pair's two scores into the
+// query's slot (and its rows, when asked for).
+template <bool kLocal>
+__device__ __forceinline__ void fold_pair(const K2Params& P, int* slot, uint32_t* sties,
+                                          uint32_t cap, uint4 pm, int mB, bool rc, uint32_t qid,
+                                          uint32_t v, uint32_t lr, int bias) {
+  int scA, scB;
+  if constexpr (kLocal) {
+    scA = lo16(v) - bias;
+    scB = hi16(v) - bias;
+    if (scA >= P.sat || (mB > 0 && scB >= P.sat)) slot[3] |= kQRedo;
+  } else {
+    scA = max(lo16(v) - P.o, lo16(lr)) - bias;
+    scB = max(hi16(v) - P.o, hi16(lr)) - bias;
+  }
+  const uint32_t rbit = rc ? 1u : 0u;
+  slot_add(slot, sties, cap, (pm.z << 1) | rbit, scA);
+  if (P.rows) P.rows[(size_t)qid * P.n_refs + pm.z] = scA;
+  if (pm.w != kNoRef) {
+    slot_add(slot, sties, cap, (pm.w << 1) | rbit, scB);
+    if (P.rows) P.rows[(size_t)qid * P.n_refs + pm.w] = scB;
+  }
+}
+
+// One warp, one task at a time, tasks pulled from an atomic counter.  The
+// kernel is instantiated twice: kLong = false takes tiles of up to 32
+// queries whose stripes fill the warp's lanes (a query of n rows takes
+// S = ceil(n / 16) lanes), scored in one pass per reference pair; kLong =
+// true takes one long query (S > 32) per task, scored in ceil(S / 32) passes
+// per pair chained through a per-warp column buffer in global memory.  Two
+// instantiations keep the register allocation of the short-read path free of
+// the long path's state; the host runs them concurrently.
+// Stripes are aligned so the read's last row is row 15 of its last stripe;
+// the 16 S - n rows before the read's first row score 0 against every real
+// column and hold H = 0 exactly, the top border the first real row needs.
+template <bool kLocal, bool kPanelW, bool kSmemPanel, bool kLong>
 __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k2_batched(const K2Params P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint64_t panel_bar;
@@ -264,25 +443,85 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
   // this lane's query slot: {best, suboptimal, n_tied, flags, ties[cap]}
   int* slot = slots + (size_t)(wib * 32 + lane) * (4 + cap);
   uint32_t* sties = reinterpret_cast<uint32_t*>(slot + 4);
+  uint2* lbuf = P.lbuf ? P.lbuf + ((size_t)blockIdx.x * kK2Warps + wib) * P.lbuf_cols : nullptr;
 
   const int bias = P.bias;
-  const uint32_t g0 = pack16x2(bias + P.o, bias + P.o);  // G of a zero border cell
-  const uint32_t bias2 = pack16x2(bias, bias);           // H = 0 (the local floor)
-  const uint32_t o32 = (uint32_t)(P.o * 65537);           // + o in both halves, 32-bit add
-  const uint32_t e2 = P.e2;
-  const uint32_t one = P.one;  // 1, opaque to the compiler: keeps G's add an IMAD
-  const uint32_t neg2 = pack16x2(kNeg16, kNeg16);
+  PassConst K;
+  K.g0 = pack16x2(bias + P.o, bias + P.o);  // G of a zero border cell
+  K.bias2 = pack16x2(bias, bias);           // H = 0 (the local floor)
+  K.o32 = (uint32_t)(P.o * 65537);           // + o in both halves, one 32-bit add
+  K.e2 = P.e2;
+  K.one = P.one;  // 1, opaque to the compiler: keeps G's add an IMAD
+  K.neg2 = pack16x2(kNeg16, kNeg16);
 
   for (;;) {
     uint32_t task = 0;
-    if (lane == 0) task = atomicAdd(&P.counters[0], 1u);
+    if (lane == 0) task = atomicAdd(&P.counters[kLong ? 3 : 0], 1u);
     task = __shfl_sync(kFull, task, 0);
     if (task >= P.n_tasks) break;
     const uint2 tk = P.tasks[task];
     const uint32_t count = tk.y & 0xffffu;
     const int smax = (int)(tk.y >> 16);
 
-    // --- which query and stripe this lane holds
+    if constexpr (kLong) {
+      // ---------------- one long query, ceil(S / 32) passes per pair
+      const uint32_t qid = P.order[tk.x];
+      const bool rc = qid >= P.n_reads;
+      const uint32_t rd = rc ? qid - P.n_reads : qid;
+      const uint32_t n = P.len[rd];
+      const int S = smax;
+      const int pad = S * kRows - (int)n;
+      const int passes = (S + 31) / 32;
+      const int owner = (S - 1) & 31;  // lane holding the last stripe
+      const uint8_t* q = P.codes + P.off[rd];
+      if (lane == owner) {
+        slot[0] = INT32_MIN;
+        slot[1] = INT32_MIN;
+        slot[2] = 0;
+        slot[3] = 0;
+      }
+      for (uint32_t p = 0; p < P.n_pairs; ++p) {
+        const uint4 pm = pairs[p];
+        const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);  // mA >= mB
+        const int jshort = (mB > 0 && mB < mA) ? mB - 1 : -1;
+        const uint16_t* sp = sels + pm.x;
+        uint32_t acc = kLocal ? K.bias2 : K.neg2, lr_last = K.neg2;
+        for (int pass = 0; pass < passes; ++pass) {
+          const int s = pass * 32 + lane;
+          const bool valid = s < S;
+          uint32_t ta[kRows];
+          uint32_t tb[kPanelW ? kRows : 1];
+          row_tables<kPanelW>(P, q, n, rc, valid, s, pad, ta, tb);
+          const uint32_t padmask = (s == 0) ? ((1u << pad) - 1u) : 0u;
+          uint32_t v, lr;
+          pair_pass<kLocal, kPanelW, true, kSmemPanel>(ta, tb, lane, valid, s == 0, padmask, mA,
+                                                       jshort, sp,
+                                           mA + 31, K, lbuf, pass > 0, pass + 1 < passes, v, lr);
+          acc = max16x2(acc, v);
+          if (pass + 1 == passes) lr_last = lr;
+          __syncwarp();  // the buffer's writes are visible to the next pass
+        }
+#pragma unroll
+        for (int d = 16; d; d >>= 1) acc = max16x2(acc, __shfl_xor_sync(kFull, acc, d));
+        if (lane == owner) fold_pair<kLocal>(P, slot, sties, cap, pm, mB, rc, qid, acc, lr_last, bias);
+      }
+      if (lane == owner) {
+        const int fl = slot[3];
+        P.qhead[qid] = make_int4(slot[0], slot[1], slot[2], fl);
+        const uint32_t nl = min((uint32_t)slot[2], cap);
+        for (uint32_t k = 0; k < nl; ++k) P.qties[(size_t)qid * cap + k] = sties[k];
+        if (fl & kQRedo) {
+          const uint32_t at = atomicAdd(&P.counters[1], 1u);
+          if (at < P.redo_cap)
+            P.redo_list[P.redo_base + at] = qid;
+          else
+            atomicOr(&P.counters[2], kErrRedoOverflow);
+        }
+      }
+      __syncwarp();
+      continue;
+    } else {
+    // ---------------- up to 32 queries, one pass per pair
     uint32_t kq = 0, kn = 0, kS = 0;
     if ((uint32_t)lane < count) {
       kq = P.order[tk.x + lane];
@@ -318,25 +557,9 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
     const bool rc = qid >= P.n_reads;
     const uint32_t rd = rc ? qid - P.n_reads : qid;
 
-    // --- the stripe's row tables
     uint32_t ta[kRows];
     uint32_t tb[kPanelW ? kRows : 1];
-    {
-      const uint8_t* q = valid ? P.codes + P.off[rd] : P.codes;
-#pragma unroll
-      for (int r = 0; r < kRows; ++r) {
-        const int i = s * kRows + r - pad;
-        uint32_t c = 5;  // padding row
-        if (valid && i >= 0) {
-          uint32_t x = rc ? q[n - 1 - i] : q[i];
-          x = x > 4 ? 4 : x;
-          c = (rc && x < 4) ? 3 - x : x;
-        }
-        ta[r] = P.tab_a[c];
-        if constexpr (kPanelW) tb[r] = P.tab_b[c];
-      }
-      if constexpr (!kPanelW) tb[0] = P.tab_b[0];
-    }
+    row_tables<kPanelW>(P, valid ? P.codes + P.off[rd] : P.codes, n, rc, valid, s, pad, ta, tb);
     // rows of the read's top padding (first lane only): excluded from the
     // semi-global last-column maximum
     const uint32_t padmask = (valid && first) ? ((1u << pad) - 1u) : 0u;
@@ -351,112 +574,18 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
     for (uint32_t p = 0; p < P.n_pairs; ++p) {
       const uint4 pm = pairs[p];
       const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);  // mA >= mB
-      const int m = mA;
       const int jshort = (mB > 0 && mB < mA) ? mB - 1 : -1;
-      const uint16_t* sp = sels + pm.x;
-      const int steps = m + smax - 1;
-
-      uint32_t g[kRows], ev[kRows];
-#pragma unroll
-      for (int r = 0; r < kRows; ++r) {
-        g[r] = g0;
-        ev[r] = neg2;
-      }
-      uint32_t gdc = g0;              // G of the row above, previous column
-      uint32_t gbot = g0, fbot = neg2;
-      uint32_t best = bias2;          // local: max H + B over this lane's cells
-      uint32_t lastrow = neg2;        // semi-global: max H + B of row 15 over columns
-      uint32_t s_col = neg2, s_last = neg2;  // semi-global short-half snapshot
-
-#pragma unroll 1
-      for (int t = 0; t < steps; ++t) {
-        const int j = t - s;
-        uint32_t gt = __shfl_up_sync(kFull, gbot, 1);
-        uint32_t ft = __shfl_up_sync(kFull, fbot, 1);
-        if (first) {
-          gt = g0;
-          ft = neg2;
-        }
-        if ((unsigned)j < (unsigned)m) {
-          const uint32_t sel = sp[j];
-          uint32_t gd = gdc;
-          gdc = gt;
-          uint32_t gup = gt, f = ft, h15 = 0, hprev = 0;
-#pragma unroll
-          for (int r = 0; r < kRows; ++r) {
-            const uint32_t sc = prmt(ta[r], tb[kPanelW ? r : 0], sel);
-            ev[r] = __viaddmax_s16x2(ev[r], e2, g[r]);
-            f = __viaddmax_s16x2(f, e2, gup);
-            const uint32_t h1 = __viaddmax_s16x2(gd, sc, ev[r]);
-            uint32_t h;
-            if constexpr (kLocal) {
-              h = __vimax3_s16x2(h1, f, bias2);
-              if (r & 1)
-                best = __vimax3_s16x2(best, hprev, h);
-              else
-                hprev = h;
-            } else {
-              h = max16x2(h1, f);
-            }
-            gd = g[r];
-            g[r] = mad_lo(h, one, o32);
-            gup = g[r];
-            if (r == kRows - 1) h15 = h;
-          }
-          gbot = g[kRows - 1];
-          fbot = f;
-          if constexpr (!kLocal) {
-            lastrow = max16x2(lastrow, h15);
-            if (j == jshort) {
-              uint32_t cm = neg2;
-#pragma unroll
-              for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? neg2 : g[r]);
-              s_col = cm;
-              s_last = lastrow;
-            }
-          }
-        }
-      }
-
-      // --- per-query scores of this pair, to the query's last lane
-      uint32_t v, lr = 0;
-      if constexpr (kLocal) {
-        v = best;
-      } else {
-        uint32_t cm = neg2;
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? neg2 : g[r]);
-        lr = lastrow;
-        if (jshort >= 0) {
-          // the short (high) half's last column and last row, taken at its end
-          cm = (cm & 0xffffu) | (s_col & 0xffff0000u);
-          lr = (lr & 0xffffu) | (s_last & 0xffff0000u);
-        }
-        v = cm;
-      }
+      uint32_t v, lr;
+      pair_pass<kLocal, kPanelW, false, kSmemPanel>(ta, tb, s, valid, first, padmask, mA, jshort,
+                                        sels + pm.x, mA + smax - 1, K, nullptr, false, false, v,
+                                        lr);
+      // per-query maximum, to the query's last lane
 #pragma unroll
       for (int d = 1; d < 32; d <<= 1) {
         const uint32_t w = __shfl_up_sync(kFull, v, d);
         if (s >= d) v = max16x2(v, w);
       }
-      if (last) {
-        int scA, scB;
-        if constexpr (kLocal) {
-          scA = lo16(v) - bias;
-          scB = hi16(v) - bias;
-          if (scA >= P.sat || (mB > 0 && scB >= P.sat)) slot[3] |= kQRedo;
-        } else {
-          scA = max(lo16(v) - P.o, lo16(lr)) - bias;
-          scB = max(hi16(v) - P.o, hi16(lr)) - bias;
-        }
-        const uint32_t rbit = rc ? 1u : 0u;
-        slot_add(slot, sties, cap, (pm.z << 1) | rbit, scA);
-        if (P.rows) P.rows[(size_t)qid * P.n_refs + pm.z] = scA;
-        if (pm.w != kNoRef) {
-          slot_add(slot, sties, cap, (pm.w << 1) | rbit, scB);
-          if (P.rows) P.rows[(size_t)qid * P.n_refs + pm.w] = scB;
-        }
-      }
+      if (last) fold_pair<kLocal>(P, slot, sties, cap, pm, mB, rc, qid, v, lr, bias);
     }
 
     // --- flush the query states of this task
@@ -474,6 +603,7 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
       }
     }
     __syncwarp();
+    }
   }
 }
 

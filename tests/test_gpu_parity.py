@@ -127,7 +127,33 @@ def test_gpu_long_and_straddling_reads(oracle):
     for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
         st = check(oracle, panel, reads, (3, -2, -5, -2), mode, "straddling batch")
         a = st[KERNEL_AUTO]
-        assert a["queries_batched"] > 0 and a["queries_plain"] > 0
+        # reads over 512 nt run on the batched kernel in several passes
+        assert a["queries_batched"] == 2 * len(reads) and a["queries_plain"] == 0
+
+
+@pytest.mark.parametrize("tag", ["trna_ambiguous", "random"])
+def test_gpu_multipass_reads(oracle, tag):
+    """Reads either side of every pass boundary of the batched kernel's long
+    path (32 stripes of 16 rows per pass): 511-513, 527-529, 1023-1025 nt,
+    and 2000 / 5000 nt (4 and 10 passes), on a tRNA panel with wildcards
+    and on a random panel, both modes, two schemes."""
+    rng = Rng(0x5EED_0106)
+    if tag == "random":
+        letters = random_panel(rng, 11, 60, 200)
+        panel = [encode(s) for s in letters]
+    else:
+        panel = fixture_panel(tag)[:13]
+        letters = [bytes(np.frombuffer(b"ACGTN", np.uint8)[p]) for p in panel]
+    reads = []
+    for ln in (511, 512, 513, 527, 528, 529, 1023, 1024, 1025, 2000, 5000):
+        r = letters[rng.below(len(letters))]
+        body = b"".join(mutate_trunc(rng, r, len(r)) for _ in range(ln // 60 + 2))
+        reads.append(encode((random_seq(rng, 7, 0.01) + body)[:ln]))
+    reads.append(encode(random_seq(rng, 700, 0.02)))
+    for scoring in ((2, -1, -10, -1), (3, 1, -5, -2)):
+        for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+            st = check(oracle, panel, reads, scoring, mode, f"multipass {tag}")
+            assert st[KERNEL_AUTO]["queries_plain"] == 0
 
 
 def mutate_trunc(rng, r, ln):
