@@ -293,6 +293,7 @@ def main():
     scoring, mode = HEADLINE
     g = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank,
                   stream=stream.cuda_stream)
+    tune = g.autotune()  # tile shape for this panel, before any timing
     info = g.info()
     batch = g.submit(g.prepare(reads.tuple(), both_strands=True))
     first = g.finish(batch, keep=True)
@@ -334,6 +335,7 @@ def main():
         for sc_, md in COMBOS[1:]:
             g2 = GpuScorer(refs, Scoring(*sc_), Mode.parse(md), device=local_rank,
                            stream=stream.cuda_stream)
+            g2.autotune()
             b2 = g2.submit(g2.prepare(reads.tuple(), both_strands=True))
             r2 = g2.finish(b2, keep=True)
             t2 = max_over_ranks(device_time(g2, b2, 1, 1))
@@ -410,7 +412,8 @@ def main():
             "gpu_launches": launches_per_step * a.steps,
             "kernel_info": {k: info[k] for k in ("regs_batched", "regs_plain",
                                                  "local_bytes_batched", "batched_blocks",
-                                                 "panel_bytes", "sm_count")},
+                                                 "panel_bytes", "sm_count", "split_len")},
+            "autotune": tune,
             "batch_stats": {k: st[k] for k in ("queries_batched", "queries_plain",
                                                "queries_rescored", "tasks", "lanes_used")},
         }

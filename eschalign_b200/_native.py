@@ -86,7 +86,13 @@ class EsgInfo(C.Structure):
                 ("regs_plain", C.c_int32), ("local_bytes_batched", C.c_int32),
                 ("local_bytes_plain", C.c_int32), ("batched_blocks", C.c_int32),
                 ("batched_threads", C.c_int32), ("plain_blocks", C.c_int32),
-                ("plain_threads", C.c_int32)]
+                ("plain_threads", C.c_int32), ("split_len", C.c_uint32), ("tuned", C.c_int32)]
+
+
+class EsgTuneReport(C.Structure):
+    _fields_ = [("n_lengths", C.c_uint32), ("lengths", C.c_uint32 * 8),
+                ("ms_rows16", C.c_float * 8), ("ms_rows32", C.c_float * 8),
+                ("split_len", C.c_uint32)]
 
 
 class EsgBatchStats(C.Structure):
@@ -115,6 +121,8 @@ SIGNATURES = {
     "esg_scorer_info": (C.c_int32, [C.c_void_p, C.POINTER(EsgInfo)]),
     "esg_scorer_set_kernel": (C.c_int32, [C.c_void_p, C.c_int32]),
     "esg_scores_len": (C.c_int32, [C.c_void_p, C.c_uint64]),
+    "esg_scorer_autotune": (C.c_int32, [C.c_void_p, C.POINTER(EsgTuneReport)]),
+    "esg_scorer_set_split": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "esg_score_batch": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32, C.c_uint32,
                                     C.c_void_p, _u32p, _i32p]),
     "esg_prepare": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32, C.c_uint32,

@@ -117,12 +117,17 @@ struct esg_scorer {
   void* d_blob = nullptr;
   uint32_t tab_a[6]{}, tab_b[6]{};
   int sat = 0;
-  int k2_blocks = 0;
   size_t k2_smem = 0;
   uint2* d_lbuf = nullptr;   // long queries: one column buffer per k2 warp
   uint32_t lbuf_cols = 0;
-  const void* k2_fn = nullptr;
-  const void* k2_long_fn = nullptr;
+  const void* k2_t16 = nullptr;   // tiles of 16-row stripes
+  const void* k2_t32 = nullptr;   // tiles of 32-row stripes
+  const void* k2_long = nullptr;  // one long query, 32-row stripes, in passes
+  int blocks_t16 = 0, blocks_t32 = 0, blocks_long = 0;
+  // queries up to split_len bases take 16-row stripes, longer ones 32-row
+  // stripes (esg_scorer_autotune measures where 32 rows start to win)
+  uint32_t split_len = 256;
+  bool tuned = false;
   cudaStream_t aux = nullptr;          // second stream: the long-query kernel
   cudaEvent_t fork = nullptr, join = nullptr;
   // k3 panel (longest first)
@@ -145,7 +150,9 @@ struct esg_batch {
   uint64_t total_bases = 0;
   // host plan
   uint32_t n_tasks = 0;
-  uint32_t n_long = 0;   // the first n_long tasks are single long queries
+  uint32_t n_long = 0;   // tasks are [n_long long | n_t32 tiles | n_t16 tiles]
+  uint32_t n_t32 = 0;
+  uint32_t n_t16 = 0;
   uint32_t n_order = 0;
   uint32_t host_list = 0;
   uint32_t redo_cap = 0;
@@ -184,6 +191,10 @@ struct esg_batch {
   esg_batch_stats stats{};
 };
 
+extern "C" {
+static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t st);
+}
+
 namespace {
 
 // Static bound on every cell of a query of n rows (simd/mod.rs:59-69 argues
@@ -196,9 +207,10 @@ int64_t value_bound(uint64_t n, uint32_t max_ref_len, const esg_scoring& s) {
 
 bool k2_takes(const esg_scorer* sc, uint64_t n) {
   if (!sc->batched_ok || n == 0) return false;
-  // queries over 32 stripes run in passes chained through the column buffer
-  if ((n + kRows - 1) / kRows > (uint64_t)kMaxStripes && !sc->d_lbuf) return false;
-  if ((n + kRows - 1) / kRows > 0xffffu) return false;
+  // queries over 32 stripes of 32 rows run in passes chained through the
+  // column buffer
+  if ((n + 31) / 32 > (uint64_t)kMaxStripes && !sc->d_lbuf) return false;
+  if ((n + 31) / 32 > 0xffffu) return false;
   if (sc->mode == ESG_MODE_SEMIGLOBAL) {
     // semi-global cells go negative: the biased lanes (H - 16384) must stay
     // negative and above the -infinity stand-in
@@ -223,27 +235,92 @@ T* carve(char*& at, size_t count) {
 
 size_t carve_size(size_t count, size_t elem) { return (count * elem + 255) / 256 * 256; }
 
-template <bool kLong>
+template <int R, bool kLong>
 const void* pick_k2(bool local, bool w, bool smem) {
   if (local) {
     if (w)
-      return smem ? (const void*)k2_batched<true, true, true, kLong>
-                  : (const void*)k2_batched<true, true, false, kLong>;
-    return smem ? (const void*)k2_batched<true, false, true, kLong>
-                : (const void*)k2_batched<true, false, false, kLong>;
+      return smem ? (const void*)k2_batched<R, true, true, true, kLong>
+                  : (const void*)k2_batched<R, true, true, false, kLong>;
+    return smem ? (const void*)k2_batched<R, true, false, true, kLong>
+                : (const void*)k2_batched<R, true, false, false, kLong>;
   }
   if (w)
-    return smem ? (const void*)k2_batched<false, true, true, kLong>
-                : (const void*)k2_batched<false, true, false, kLong>;
-  return smem ? (const void*)k2_batched<false, false, true, kLong>
-              : (const void*)k2_batched<false, false, false, kLong>;
+    return smem ? (const void*)k2_batched<R, false, true, true, kLong>
+                : (const void*)k2_batched<R, false, true, false, kLong>;
+  return smem ? (const void*)k2_batched<R, false, false, true, kLong>
+              : (const void*)k2_batched<R, false, false, false, kLong>;
 }
 
 void set_k2_fn(esg_scorer* sc) {
   const bool local = sc->mode == ESG_MODE_LOCAL;
-  sc->k2_fn = pick_k2<false>(local, sc->panel_w, sc->smem_panel);
-  sc->k2_long_fn = pick_k2<true>(local, sc->panel_w, sc->smem_panel);
+  sc->k2_t16 = pick_k2<16, false>(local, sc->panel_w, sc->smem_panel);
+  sc->k2_t32 = pick_k2<32, false>(local, sc->panel_w, sc->smem_panel);
+  sc->k2_long = pick_k2<32, true>(local, sc->panel_w, sc->smem_panel);
   sc->k3_fn = local ? (const void*)k3_plain<true> : (const void*)k3_plain<false>;
+}
+
+// 32-lane tiles of query stripes: best-fit decreasing.  `qs` holds
+// (stripes, query) with stripes <= 32; the plan lists queries tile by tile
+// and one task per tile {start, count | stripes of its largest query << 16}.
+struct TilePlan {
+  std::vector<uint32_t> order;
+  std::vector<uint2> tasks;
+  uint32_t lanes = 0;
+};
+
+void pack_tiles(std::vector<std::pair<uint32_t, uint32_t>>& qs, TilePlan& out) {
+  const size_t nq = qs.size();
+  if (!nq) return;
+  std::vector<uint32_t> count(kMaxStripes + 2, 0);
+  for (const auto& x : qs) ++count[x.first];
+  std::vector<uint32_t> start(kMaxStripes + 2, 0);  // descending stripes
+  for (int S = kMaxStripes; S >= 1; --S) start[S - 1] = start[S] + count[S];
+  std::vector<uint32_t> sorted(nq), sorted_s(nq);
+  for (const auto& x : qs) {
+    const uint32_t at = start[x.first]++;
+    sorted[at] = x.second;
+    sorted_s[at] = x.first;
+  }
+  std::vector<uint32_t> bin_of(nq);
+  std::vector<uint8_t> bin_free, bin_smax;
+  std::vector<uint16_t> bin_count;
+  std::vector<std::vector<uint32_t>> open(kMaxStripes);  // by free capacity 1..31
+  uint32_t open_mask = 0;
+  for (size_t i = 0; i < nq; ++i) {
+    const uint32_t S = sorted_s[i];
+    const uint32_t cand = open_mask & ~((1u << S) - 1u);
+    uint32_t bin;
+    if (cand) {
+      const uint32_t f = __builtin_ctz(cand);
+      bin = open[f].back();
+      open[f].pop_back();
+      if (open[f].empty()) open_mask &= ~(1u << f);
+    } else {
+      bin = (uint32_t)bin_free.size();
+      bin_free.push_back(kMaxStripes);
+      bin_smax.push_back((uint8_t)S);
+      bin_count.push_back(0);
+    }
+    bin_of[i] = bin;
+    bin_free[bin] = (uint8_t)(bin_free[bin] - S);
+    bin_count[bin]++;
+    const uint32_t f = bin_free[bin];
+    if (f > 0) {
+      open[f].push_back(bin);
+      open_mask |= 1u << f;
+    }
+  }
+  const uint32_t n_bins = (uint32_t)bin_free.size();
+  std::vector<uint32_t> tstart(n_bins + 1, 0);
+  for (uint32_t t = 0; t < n_bins; ++t) tstart[t + 1] = tstart[t] + bin_count[t];
+  std::vector<uint32_t> fill(tstart.begin(), tstart.end() - 1);
+  out.order.assign(nq, 0);
+  for (size_t i = 0; i < nq; ++i) out.order[fill[bin_of[i]]++] = sorted[i];
+  out.tasks.resize(n_bins);
+  for (uint32_t t = 0; t < n_bins; ++t) {
+    out.tasks[t] = make_uint2(tstart[t], (uint32_t)bin_count[t] | ((uint32_t)bin_smax[t] << 16));
+    out.lanes += kMaxStripes - bin_free[t];
+  }
 }
 
 }  // namespace
@@ -485,25 +562,30 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
   sc->smem_panel = (size_t)sc->blob_bytes + slots <= 100 * 1024;
   set_k2_fn(sc);
   sc->k2_smem = (sc->smem_panel ? sc->blob_bytes : 0) + slots;
-  if ((e = cudaFuncSetAttribute(sc->k2_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sc->k2_smem)) != cudaSuccess ||
-      (e = cudaFuncSetAttribute(sc->k2_long_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sc->k2_smem)) != cudaSuccess)
-    return cleanup(cuda_fail(e, "cudaFuncSetAttribute(k2)"));
+  for (const void* fn : {sc->k2_t16, sc->k2_t32, sc->k2_long})
+    if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sc->k2_smem)) != cudaSuccess)
+      return cleanup(cuda_fail(e, "cudaFuncSetAttribute(k2)"));
   if ((e = cudaStreamCreateWithFlags(&sc->aux, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&sc->fork, cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&sc->join, cudaEventDisableTiming)) != cudaSuccess)
     return cleanup(cuda_fail(e, "cudaStreamCreate(aux)"));
-  int occ2 = 0, occ3 = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, sc->k2_fn, kK2Threads,
+  int occ16 = 0, occ32 = 0, occl = 0, occ3 = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ16, sc->k2_t16, kK2Threads,
+                                                         sc->k2_smem)) != cudaSuccess ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, sc->k2_t32, kK2Threads,
+                                                         sc->k2_smem)) != cudaSuccess ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occl, sc->k2_long, kK2Threads,
                                                          sc->k2_smem)) != cudaSuccess ||
       (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, sc->k3_fn, kK3Threads, 0)) !=
           cudaSuccess)
     return cleanup(cuda_fail(e, "cudaOccupancy"));
-  sc->k2_blocks = std::max(1, occ2) * sc->sm_count;
+  sc->blocks_t16 = std::max(1, occ16) * sc->sm_count;
+  sc->blocks_t32 = std::max(1, occ32) * sc->sm_count;
+  sc->blocks_long = std::max(1, occl) * sc->sm_count;
   if (sc->batched_ok && max_len <= 8192) {
     sc->lbuf_cols = max_len;
-    const size_t lb = (size_t)sc->k2_blocks * kK2Warps * max_len * sizeof(uint2);
+    const size_t lb = (size_t)sc->blocks_long * kK2Warps * max_len * sizeof(uint2);
     if ((e = cudaMalloc(&sc->d_lbuf, lb)) != cudaSuccess)
       return cleanup(cuda_fail(e, "cudaMalloc(long-query buffer)"));
   }
@@ -528,7 +610,7 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
   inf.panel_bytes = sc->smem_panel ? sc->blob_bytes : 0;
   inf.batched_ok = sc->batched_ok;
   cudaFuncAttributes fa{};
-  if (cudaFuncGetAttributes(&fa, sc->k2_fn) == cudaSuccess) {
+  if (cudaFuncGetAttributes(&fa, sc->k2_t16) == cudaSuccess) {
     inf.regs_batched = fa.numRegs;
     inf.local_bytes_batched = (int)fa.localSizeBytes;
   }
@@ -536,10 +618,12 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
     inf.regs_plain = fa.numRegs;
     inf.local_bytes_plain = (int)fa.localSizeBytes;
   }
-  inf.batched_blocks = sc->k2_blocks;
+  inf.batched_blocks = sc->blocks_t16;
   inf.batched_threads = kK2Threads;
   inf.plain_blocks = sc->k3_blocks;
   inf.plain_threads = kK3Threads;
+  inf.split_len = sc->split_len;
+  inf.tuned = 0;
   *out = sc;
   return ESG_OK;
 }
@@ -581,6 +665,101 @@ esg_status esg_scorer_set_kernel(esg_scorer* sc, int32_t kernel) {
 
 int32_t esg_scores_len(const esg_scorer* sc, uint64_t len) { return sc && len > 0; }
 
+esg_status esg_scorer_set_split(esg_scorer* sc, uint32_t split_len) {
+  if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");
+  sc->split_len = split_len;
+  sc->info.split_len = split_len;
+  return ESG_OK;
+}
+
+esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
+  g_err.clear();
+  if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");
+  esg_tune_report rep{};
+  if (!sc->batched_ok || sc->kernel != ESG_KERNEL_AUTO) {
+    rep.split_len = sc->split_len;
+    if (out) *out = rep;
+    return ESG_OK;
+  }
+  ESG_CUDA(cudaSetDevice(sc->device));
+  static const uint32_t kLens[] = {48, 80, 112, 160, 224, 320, 448};
+  const uint32_t n_lens = sizeof(kLens) / sizeof(kLens[0]);
+  const uint32_t keep = sc->split_len;
+  uint64_t x = 0x9e3779b97f4a7c15ull;  // xorshift64* calibration reads
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ESG_CUDA(cudaEventCreate(&e0));
+  ESG_CUDA(cudaEventCreate(&e1));
+  esg_status st = ESG_OK;
+  for (uint32_t li = 0; li < n_lens && st == ESG_OK; ++li) {
+    const uint32_t L = kLens[li];
+    // about 2e10 cells per batch (a few ms of device time), both strands
+    const uint64_t want = (uint64_t)(2.0e10 / (2.0 * L * (double)sc->panel_bases));
+    const uint32_t n = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 512), 200000);
+    // lengths spread over L +- 25 %, as a real batch has, so the tiles pack
+    // as they would in use
+    auto next = [&x]() {
+      x ^= x >> 12;
+      x ^= x << 25;
+      x ^= x >> 27;
+      return x * 0x2545F4914F6CDD1Dull;
+    };
+    std::vector<uint64_t> off(n);
+    std::vector<uint32_t> len(n);
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+      len[k] = L - L / 4 + (uint32_t)(next() % (L / 2 + 1));
+      off[k] = total;
+      total += len[k];
+    }
+    std::vector<uint8_t> codes(total);
+    for (auto& c : codes) c = (uint8_t)(next() >> 62);
+    float ms[2] = {0, 0};
+    for (int cfg = 0; cfg < 2 && st == ESG_OK; ++cfg) {
+      sc->split_len = cfg == 0 ? 512u : 0u;
+      esg_batch* b = nullptr;
+      st = esg_prepare(sc, codes.data(), off.data(), len.data(), n, ESG_BOTH_STRANDS, &b);
+      if (st == ESG_OK) st = esg_submit(sc, b);
+      if (st == ESG_OK) st = esg_finish(sc, b, nullptr, nullptr, nullptr);
+      if (st == ESG_OK) {
+        cudaEventRecord(e0, sc->stream);
+        for (int rep_i = 0; rep_i < 2 && st == ESG_OK; ++rep_i) st = launch_device_work(sc, b, sc->stream);
+        cudaEventRecord(e1, sc->stream);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms[cfg], e0, e1);
+        ms[cfg] /= 2;
+      }
+      esg_batch_free(b);
+    }
+    rep.lengths[li] = L;
+    rep.ms_rows16[li] = ms[0];
+    rep.ms_rows32[li] = ms[1];
+    rep.n_lengths = li + 1;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != ESG_OK) {
+    sc->split_len = keep;
+    return st;
+  }
+  // 16-row stripes up to the last length where they are at least as fast,
+  // counting from the shortest; 32-row stripes from the first length they win
+  uint32_t split = 0;
+  for (uint32_t li = 0; li < rep.n_lengths; ++li) {
+    if (rep.ms_rows16[li] <= rep.ms_rows32[li])
+      split = rep.lengths[li];
+    else
+      break;
+  }
+  if (split == kLens[n_lens - 1]) split = 512;
+  sc->split_len = split;
+  sc->tuned = true;
+  sc->info.split_len = split;
+  sc->info.tuned = 1;
+  rep.split_len = split;
+  if (out) *out = rep;
+  return ESG_OK;
+}
+
 // ---------------------------------------------------------------- prepare
 esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
                        const uint32_t* len, uint32_t n_reads, uint32_t flags, esg_batch** out) {
@@ -604,12 +783,15 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   b->n_q = n_reads * (both ? 2u : 1u);
   b->total_bases = total;
 
-  // --- plan: which queries go where
-  std::vector<uint32_t> by_s_count(kMaxStripes + 1, 0);
-  std::vector<std::pair<uint32_t, uint32_t>> long_q;  // (stripes, query), one task each
-  std::vector<uint8_t> route(b->n_q, 0);  // 0 empty, 1 k2, 2 k3
-  uint32_t n_k2 = 0, n_k3 = 0, n_empty = 0, redo_cap = 0;
+  // --- plan: which queries go where.  Short queries take 16-row stripes,
+  // longer ones 32-row stripes (from sc->split_len, set by the autotuner),
+  // queries over 32 stripes of 32 rows run alone in passes; what the
+  // batched kernel cannot take goes to the int32 kernel.
+  std::vector<std::pair<uint32_t, uint32_t>> q16, q32, qlong;  // (stripes, query)
+  std::vector<uint8_t> route(b->n_q, 0);  // 0 empty or k2, 2 k3
+  uint32_t n_k3 = 0, n_empty = 0, redo_cap = 0;
   uint64_t cells = 0;
+  const uint32_t split = std::min<uint32_t>(sc->split_len, 16 * kMaxStripes);
   for (uint32_t q = 0; q < b->n_q; ++q) {
     const uint32_t n = len[q < n_reads ? q : q - n_reads];
     if (n == 0) {
@@ -618,14 +800,12 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
     }
     cells += (uint64_t)n * sc->panel_bases;
     if (b->kernel == ESG_KERNEL_AUTO && k2_takes(sc, n)) {
-      const uint32_t S = (n + kRows - 1) / kRows;
-      if (S > (uint32_t)kMaxStripes) {
-        long_q.push_back({S, q});
-      } else {
-        route[q] = 1;
-        ++n_k2;
-        ++by_s_count[S];
-      }
+      if (n <= split)
+        q16.push_back({(n + 15) / 16, q});
+      else if (n <= 32 * kMaxStripes)
+        q32.push_back({(n + 31) / 32, q});
+      else
+        qlong.push_back({(n + 31) / 32, q});
       if (k2_may_flag(sc, n)) ++redo_cap;
     } else {
       route[q] = 2;
@@ -634,61 +814,18 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   }
   b->host_list = n_k3;
   b->redo_cap = redo_cap;
-
-  // best-fit decreasing of query stripes into 32-lane tiles
-  std::vector<uint32_t> start_of(kMaxStripes + 2, 0);
-  for (int S = kMaxStripes; S >= 1; --S) start_of[S - 1] = start_of[S] + by_s_count[S];
-  // queries sorted by stripe count, descending (stable within a count)
-  std::vector<uint32_t> sorted(n_k2);
-  {
-    std::vector<uint32_t> fill(start_of);
-    for (uint32_t q = 0; q < b->n_q; ++q)
-      if (route[q] == 1) {
-        const uint32_t n = len[q < n_reads ? q : q - n_reads];
-        const uint32_t S = (n + kRows - 1) / kRows;
-        sorted[fill[S]++] = q;
-      }
-  }
-  std::vector<uint32_t> bin_of(n_k2);
-  std::vector<uint8_t> bin_free, bin_smax;
-  std::vector<uint16_t> bin_count;
-  std::vector<std::vector<uint32_t>> open(kMaxStripes);  // by free capacity 1..31
-  uint32_t open_mask = 0;
-  for (uint32_t i = 0; i < n_k2; ++i) {
-    const uint32_t q = sorted[i];
-    const uint32_t n = len[q < n_reads ? q : q - n_reads];
-    const uint32_t S = (n + kRows - 1) / kRows;
-    const uint32_t cand = open_mask & ~((1u << S) - 1u);
-    uint32_t bin;
-    if (cand) {
-      const uint32_t f = __builtin_ctz(cand);
-      bin = open[f].back();
-      open[f].pop_back();
-      if (open[f].empty()) open_mask &= ~(1u << f);
-    } else {
-      bin = (uint32_t)bin_free.size();
-      bin_free.push_back(kMaxStripes);
-      bin_smax.push_back((uint8_t)S);
-      bin_count.push_back(0);
-    }
-    bin_of[i] = bin;
-    bin_free[bin] = (uint8_t)(bin_free[bin] - S);
-    bin_count[bin]++;
-    const uint32_t f = bin_free[bin];
-    if (f > 0) {
-      open[f].push_back(bin);
-      open_mask |= 1u << f;
-    }
-  }
-  // long queries first (longest first), then the packed tiles
-  std::sort(long_q.begin(), long_q.end(),
-            [](const std::pair<uint32_t, uint32_t>& a, const std::pair<uint32_t, uint32_t>& c) {
-              return a.first > c.first;
-            });
-  const uint32_t n_long = (uint32_t)long_q.size();
+  std::stable_sort(qlong.begin(), qlong.end(),
+                   [](const std::pair<uint32_t, uint32_t>& a,
+                      const std::pair<uint32_t, uint32_t>& c) { return a.first > c.first; });
+  TilePlan p32, p16;
+  pack_tiles(q32, p32);
+  pack_tiles(q16, p16);
+  const uint32_t n_long = (uint32_t)qlong.size();
   b->n_long = n_long;
-  b->n_tasks = n_long + (uint32_t)bin_free.size();
-  b->n_order = n_k2 + n_long;
+  b->n_t32 = (uint32_t)p32.tasks.size();
+  b->n_t16 = (uint32_t)p16.tasks.size();
+  b->n_tasks = b->n_long + b->n_t32 + b->n_t16;
+  b->n_order = n_long + (uint32_t)(q32.size() + q16.size());
 
   // --- pinned staging for the inputs
   const size_t sz_codes = carve_size(total ? total : 1, 1);
@@ -717,24 +854,20 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
     if (len[k]) memcpy(b->h_codes + pos, codes + off[k], len[k]);
     pos += len[k];
   }
-  // order[] grouped by task, tasks[] = {start, count | smax << 16}; long
-  // queries are single-query tasks whose smax is their stripe count (> 32)
+  // order[] and tasks[] laid out [long | 32-row tiles | 16-row tiles];
+  // tasks[t] = {start in order[], count | stripes << 16}
   {
-    uint32_t lanes = 0;
-    for (uint32_t t = 0; t < n_long; ++t) {
-      b->h_order[t] = long_q[t].second;
-      b->h_tasks[t] = make_uint2(t, 1u | (long_q[t].first << 16));
-      lanes += long_q[t].first;
+    uint32_t lanes = 0, o = 0, t = 0;
+    for (const auto& lq : qlong) {
+      b->h_order[o] = lq.second;
+      b->h_tasks[t++] = make_uint2(o++, 1u | (lq.first << 16));
+      lanes += lq.first;
     }
-    const uint32_t n_bins = (uint32_t)bin_free.size();
-    std::vector<uint32_t> tstart(n_bins + 1, n_long);
-    for (uint32_t t = 0; t < n_bins; ++t) tstart[t + 1] = tstart[t] + bin_count[t];
-    std::vector<uint32_t> fill(tstart.begin(), tstart.end() - 1);
-    for (uint32_t i = 0; i < n_k2; ++i) b->h_order[fill[bin_of[i]]++] = sorted[i];
-    for (uint32_t t = 0; t < n_bins; ++t) {
-      b->h_tasks[n_long + t] =
-          make_uint2(tstart[t], (uint32_t)bin_count[t] | ((uint32_t)bin_smax[t] << 16));
-      lanes += kMaxStripes - bin_free[t];
+    for (const TilePlan* tp : {&p32, &p16}) {
+      const uint32_t base = o;
+      for (uint32_t q : tp->order) b->h_order[o++] = q;
+      for (const uint2& tk : tp->tasks) b->h_tasks[t++] = make_uint2(base + tk.x, tk.y);
+      lanes += tp->lanes;
     }
     b->stats.lanes_used = lanes;
   }
@@ -746,7 +879,7 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   b->stats.n_reads = n_reads;
   b->stats.n_queries = b->n_q;
   b->stats.n_empty = n_empty;
-  b->stats.queries_batched = n_k2 + n_long;
+  b->stats.queries_batched = n_long + (uint32_t)(q32.size() + q16.size());
   b->stats.queries_plain = n_k3;
   b->stats.tasks = b->n_tasks;
   b->stats.cells = cells;
@@ -759,7 +892,7 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
   const bool both = b->flags & ESG_BOTH_STRANDS;
   uint32_t kernels = 0;
   const bool rows = b->flags & ESG_FULL_ROWS;
-  ESG_CUDA(cudaMemsetAsync(b->d_counters, 0, 16, st));
+  ESG_CUDA(cudaMemsetAsync(b->d_counters, 0, 8 * sizeof(uint32_t), st));
   if (b->n_tasks) {
     K2Params P{};
     P.blob = (const uint4*)sc->d_blob;
@@ -792,32 +925,50 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
     P.lbuf_cols = sc->lbuf_cols;
     P.sat = sc->sat;
     P.cap = sc->cap;
-    // long queries on the aux stream, launched first so their CTAs are
-    // resident beside the persistent tile kernel rather than after it
-    const uint32_t n_long = b->n_long, n_tiles = b->n_tasks - b->n_long;
+    // The three task groups: long queries, then 32-row tiles, on the aux
+    // stream; 16-row tiles on the batch's stream.  Launched first, the aux
+    // kernels' CTAs share the SMs with the persistent 16-row kernel and
+    // fill its tail, instead of queueing behind it.
+    const uint32_t n_long = b->n_long, n_t32 = b->n_t32, n_t16 = b->n_t16;
+    auto grid = [](int cap, uint32_t tasks) {
+      return (int)std::max<uint64_t>(
+          1, std::min<uint64_t>((uint64_t)cap, (tasks + kK2Warps - 1) / kK2Warps));
+    };
+    const bool aux = n_long || n_t32;
+    if (aux) {
+      ESG_CUDA(cudaEventRecord(sc->fork, st));
+      ESG_CUDA(cudaStreamWaitEvent(sc->aux, sc->fork, 0));
+    }
     if (n_long) {
       K2Params L = P;
       L.n_tasks = n_long;
-      const int lblocks =
-          (int)std::min<uint64_t>((uint64_t)sc->k2_blocks, (n_long + kK2Warps - 1) / kK2Warps);
-      ESG_CUDA(cudaEventRecord(sc->fork, st));
-      ESG_CUDA(cudaStreamWaitEvent(sc->aux, sc->fork, 0));
+      L.task_counter = b->d_counters + 3;
       void* largs[] = {&L};
-      ESG_CUDA(cudaLaunchKernel(sc->k2_long_fn, dim3(lblocks), dim3(kK2Threads), largs,
-                                sc->k2_smem, sc->aux));
+      ESG_CUDA(cudaLaunchKernel(sc->k2_long, dim3(grid(sc->blocks_long, n_long)),
+                                dim3(kK2Threads), largs, sc->k2_smem, sc->aux));
       ++kernels;
     }
-    if (n_tiles) {
+    if (n_t32) {
       K2Params T = P;
       T.tasks = P.tasks + n_long;
-      T.n_tasks = n_tiles;
-      const int blocks =
-          (int)std::min<uint64_t>((uint64_t)sc->k2_blocks, (n_tiles + kK2Warps - 1) / kK2Warps);
-      void* args[] = {&T};
-      ESG_CUDA(cudaLaunchKernel(sc->k2_fn, dim3(blocks), dim3(kK2Threads), args, sc->k2_smem, st));
+      T.n_tasks = n_t32;
+      T.task_counter = b->d_counters + 4;
+      void* targs[] = {&T};
+      ESG_CUDA(cudaLaunchKernel(sc->k2_t32, dim3(grid(sc->blocks_t32, n_t32)), dim3(kK2Threads),
+                                targs, sc->k2_smem, sc->aux));
       ++kernels;
     }
-    if (n_long) {
+    if (n_t16) {
+      K2Params T = P;
+      T.tasks = P.tasks + n_long + n_t32;
+      T.n_tasks = n_t16;
+      T.task_counter = b->d_counters + 0;
+      void* targs[] = {&T};
+      ESG_CUDA(cudaLaunchKernel(sc->k2_t16, dim3(grid(sc->blocks_t16, n_t16)), dim3(kK2Threads),
+                                targs, sc->k2_smem, st));
+      ++kernels;
+    }
+    if (aux) {
       ESG_CUDA(cudaEventRecord(sc->join, sc->aux));
       ESG_CUDA(cudaStreamWaitEvent(st, sc->join, 0));
     }
@@ -903,7 +1054,7 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
       carve_size(b->n_order ? b->n_order : 1, 4),
       carve_size(b->n_tasks ? b->n_tasks : 1, 8),
       carve_size(nlist ? nlist : 1, 4),
-      carve_size(4, 4),
+      carve_size(8, 4),
       carve_size(nq, 16),
       carve_size(nq * sc->cap, 4),
       carve_size(nlist ? (size_t)nlist * sc->n_refs : 1, 4),
@@ -922,7 +1073,7 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   b->d_order = carve<uint32_t>(at, b->n_order ? b->n_order : 1);
   b->d_tasks = carve<uint2>(at, b->n_tasks ? b->n_tasks : 1);
   b->d_list = carve<uint32_t>(at, nlist ? nlist : 1);
-  b->d_counters = carve<uint32_t>(at, 4);
+  b->d_counters = carve<uint32_t>(at, 8);
   b->d_qhead = carve<int4>(at, nq);
   b->d_qties = carve<uint32_t>(at, nq * sc->cap);
   b->d_k3out = carve<int32_t>(at, nlist ? (size_t)nlist * sc->n_refs : 1);

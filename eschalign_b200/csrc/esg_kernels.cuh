@@ -35,8 +35,9 @@ constexpr int kBiasLocal = 2048;      // local: H + B >= B >= |o|, |e|
 constexpr int kBiasSemiGlobal = -16384;  // semi-global: H + B < 0 while |H| < 12000
 constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
 // k2 CTA shape: 4 warps, 5 resident CTAs per SM (20 warps, <= 102 registers;
-// 4 CTAs for panels with wildcards, whose per-row tables need more) measured
-// fastest on B200 for the C2 workload (vs 8 warps x 2 CTAs).
+// 4 CTAs for panels with wildcards, whose per-row tables need more; 3 for
+// 32-row stripes) measured fastest on B200 for the C2 workload (vs 8 warps x
+// 2 CTAs).
 #ifndef ESG_K2_WARPS
 #define ESG_K2_WARPS 4
 #endif
@@ -133,7 +134,8 @@ struct K2Params {
   const uint32_t* order;
   const uint2* tasks;
   uint32_t n_tasks;
-  uint32_t* counters;    // [0] tile counter, [1] redo count, [2] error bits, [3] long counter
+  uint32_t* counters;    // [1] redo count, [2] error bits (and the task counters)
+  uint32_t* task_counter;  // this launch's task counter
   // outputs
   int4* qhead;           // per query {best, suboptimal, n_tied, flags}
   uint32_t* qties;       // per query cap candidates
@@ -263,17 +265,17 @@ __device__ __forceinline__ uint32_t load_sel(const uint16_t* sp, int j) {
   }
 }
 
-template <bool kLocal, bool kPanelW, bool kLong, bool kSmem>
-__device__ __forceinline__ void pair_pass(const uint32_t (&ta)[kRows],
-                                          const uint32_t (&tb)[kPanelW ? kRows : 1], int skew,
+template <int R, bool kLocal, bool kPanelW, bool kLong, bool kSmem>
+__device__ __forceinline__ void pair_pass(const uint32_t (&ta)[R],
+                                          const uint32_t (&tb)[kPanelW ? R : 1], int skew,
                                           bool active_lane, bool first, uint32_t padmask, int m,
                                           int jshort, const uint16_t* __restrict__ sp, int steps,
                                           const PassConst& K, uint2* buf, bool from_buf,
                                           bool to_buf, uint32_t& v, uint32_t& lr) {
   const int lane = threadIdx.x & 31;
-  uint32_t g[kRows], ev[kRows];
+  uint32_t g[R], ev[R];
 #pragma unroll
-  for (int r = 0; r < kRows; ++r) {
+  for (int r = 0; r < R; ++r) {
     g[r] = K.g0;
     ev[r] = K.neg2;
   }
@@ -308,7 +310,7 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[kRows],
       gdc = gt;
       uint32_t gup = gt, f = ft, h15 = 0, hprev = 0;
 #pragma unroll
-      for (int r = 0; r < kRows; ++r) {
+      for (int r = 0; r < R; ++r) {
         const uint32_t sc = prmt(ta[r], tb[kPanelW ? r : 0], sel);
         ev[r] = __viaddmax_s16x2(ev[r], K.e2, g[r]);
         f = __viaddmax_s16x2(f, K.e2, gup);
@@ -326,9 +328,9 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[kRows],
         gd = g[r];
         g[r] = mad_lo(h, K.one, K.o32);
         gup = g[r];
-        if (r == kRows - 1) h15 = h;
+        if (r == R - 1) h15 = h;
       }
-      gbot = g[kRows - 1];
+      gbot = g[R - 1];
       fbot = f;
       if constexpr (kLong) {
         if (to_buf && lane == 31) buf[j] = make_uint2(gbot, fbot);
@@ -338,7 +340,7 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[kRows],
         if (j == jshort) {
           uint32_t cm = K.neg2;
 #pragma unroll
-          for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
+          for (int r = 0; r < R; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
           s_col = cm;
           s_last = lastrow;
         }
@@ -351,7 +353,7 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[kRows],
   } else {
     uint32_t cm = K.neg2;
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
+    for (int r = 0; r < R; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
     if (jshort >= 0) {
       // the short (high) half's last column and last row, taken at its end
       cm = (cm & 0xffffu) | (s_col & 0xffff0000u);
@@ -364,14 +366,14 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[kRows],
 
 // Row tables of stripe `s` of a query (n codes at q, reverse complement if
 // rc): row r is read row i = 16 s + r - pad; rows before the read are padding.
-template <bool kPanelW>
+template <int R, bool kPanelW>
 __device__ __forceinline__ void row_tables(const K2Params& P, const uint8_t* q, uint32_t n,
                                            bool rc, bool valid, int s, int pad,
-                                           uint32_t (&ta)[kRows],
-                                           uint32_t (&tb)[kPanelW ? kRows : 1]) {
+                                           uint32_t (&ta)[R],
+                                           uint32_t (&tb)[kPanelW ? R : 1]) {
 #pragma unroll
-  for (int r = 0; r < kRows; ++r) {
-    const int i = s * kRows + r - pad;
+  for (int r = 0; r < R; ++r) {
+    const int i = s * R + r - pad;
     uint32_t c = 5;  // padding row
     if (valid && i >= 0) {
       uint32_t x = rc ? q[n - 1 - i] : q[i];
@@ -419,8 +421,9 @@ __device__ __forceinline__ void fold_pair(const K2Params& P, int* slot, uint32_t
 // Stripes are aligned so the read's last row is row 15 of its last stripe;
 // the 16 S - n rows before the read's first row score 0 against every real
 // column and hold H = 0 exactly, the top border the first real row needs.
-template <bool kLocal, bool kPanelW, bool kSmemPanel, bool kLong>
-__global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k2_batched(const K2Params P) {
+template <int R, bool kLocal, bool kPanelW, bool kSmemPanel, bool kLong>
+__global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2_MIN_BLOCKS))
+    k2_batched(const K2Params P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint64_t panel_bar;
   const int lane = threadIdx.x & 31;
@@ -456,7 +459,7 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
 
   for (;;) {
     uint32_t task = 0;
-    if (lane == 0) task = atomicAdd(&P.counters[kLong ? 3 : 0], 1u);
+    if (lane == 0) task = atomicAdd(P.task_counter, 1u);
     task = __shfl_sync(kFull, task, 0);
     if (task >= P.n_tasks) break;
     const uint2 tk = P.tasks[task];
@@ -470,7 +473,7 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
       const uint32_t rd = rc ? qid - P.n_reads : qid;
       const uint32_t n = P.len[rd];
       const int S = smax;
-      const int pad = S * kRows - (int)n;
+      const int pad = S * R - (int)n;
       const int passes = (S + 31) / 32;
       const int owner = (S - 1) & 31;  // lane holding the last stripe
       const uint8_t* q = P.codes + P.off[rd];
@@ -489,12 +492,12 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
         for (int pass = 0; pass < passes; ++pass) {
           const int s = pass * 32 + lane;
           const bool valid = s < S;
-          uint32_t ta[kRows];
-          uint32_t tb[kPanelW ? kRows : 1];
-          row_tables<kPanelW>(P, q, n, rc, valid, s, pad, ta, tb);
+          uint32_t ta[R];
+          uint32_t tb[kPanelW ? R : 1];
+          row_tables<R, kPanelW>(P, q, n, rc, valid, s, pad, ta, tb);
           const uint32_t padmask = (s == 0) ? ((1u << pad) - 1u) : 0u;
           uint32_t v, lr;
-          pair_pass<kLocal, kPanelW, true, kSmemPanel>(ta, tb, lane, valid, s == 0, padmask, mA,
+          pair_pass<R, kLocal, kPanelW, true, kSmemPanel>(ta, tb, lane, valid, s == 0, padmask, mA,
                                                        jshort, sp,
                                            mA + 31, K, lbuf, pass > 0, pass + 1 < passes, v, lr);
           acc = max16x2(acc, v);
@@ -527,7 +530,7 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
       kq = P.order[tk.x + lane];
       const uint32_t rd = kq < P.n_reads ? kq : kq - P.n_reads;
       kn = P.len[rd];
-      kS = (kn + kRows - 1) / kRows;
+      kS = (kn + R - 1) / R;
     }
     uint32_t incl = kS;
 #pragma unroll
@@ -553,13 +556,13 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
     }
     const bool first = valid ? (s == 0) : true;
     const bool last = valid && (s == S - 1);
-    const int pad = valid ? S * kRows - (int)n : 0;
+    const int pad = valid ? S * R - (int)n : 0;
     const bool rc = qid >= P.n_reads;
     const uint32_t rd = rc ? qid - P.n_reads : qid;
 
-    uint32_t ta[kRows];
-    uint32_t tb[kPanelW ? kRows : 1];
-    row_tables<kPanelW>(P, valid ? P.codes + P.off[rd] : P.codes, n, rc, valid, s, pad, ta, tb);
+    uint32_t ta[R];
+    uint32_t tb[kPanelW ? R : 1];
+    row_tables<R, kPanelW>(P, valid ? P.codes + P.off[rd] : P.codes, n, rc, valid, s, pad, ta, tb);
     // rows of the read's top padding (first lane only): excluded from the
     // semi-global last-column maximum
     const uint32_t padmask = (valid && first) ? ((1u << pad) - 1u) : 0u;
@@ -576,7 +579,7 @@ __global__ void __launch_bounds__(kK2Threads, kPanelW ? 4 : ESG_K2_MIN_BLOCKS) k
       const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);  // mA >= mB
       const int jshort = (mB > 0 && mB < mA) ? mB - 1 : -1;
       uint32_t v, lr;
-      pair_pass<kLocal, kPanelW, false, kSmemPanel>(ta, tb, s, valid, first, padmask, mA, jshort,
+      pair_pass<R, kLocal, kPanelW, false, kSmemPanel>(ta, tb, s, valid, first, padmask, mA, jshort,
                                         sels + pm.x, mA + smax - 1, K, nullptr, false, false, v,
                                         lr);
       // per-query maximum, to the query's last lane

@@ -286,6 +286,18 @@ class GpuScorer:
         query on the plain int32 kernel, or the batched kernel where it can."""
         self.set_kernel(KERNEL_PLAIN32 if plain else KERNEL_AUTO)
 
+    def autotune(self) -> dict:
+        """Measure the 16/32-row stripe split on this panel (esg_scorer_autotune)."""
+        rep = _native.EsgTuneReport()
+        _check(self._lib, self._lib.esg_scorer_autotune(self._h, C.byref(rep)))
+        n = rep.n_lengths
+        return {"split_len": rep.split_len, "lengths": list(rep.lengths[:n]),
+                "ms_rows16": [round(v, 3) for v in rep.ms_rows16[:n]],
+                "ms_rows32": [round(v, 3) for v in rep.ms_rows32[:n]]}
+
+    def set_split(self, split_len: int):
+        _check(self._lib, self._lib.esg_scorer_set_split(self._h, int(split_len)))
+
     def scores_len(self, n: int) -> bool:
         return bool(self._lib.esg_scores_len(self._h, n))
 

@@ -101,7 +101,20 @@ typedef struct esg_info {
     int32_t batched_threads;  /* threads per CTA                                       */
     int32_t plain_blocks;
     int32_t plain_threads;
+    uint32_t split_len;       /* queries up to this length take 16-row stripes  */
+    int32_t tuned;            /* split_len was measured by esg_scorer_autotune   */
 } esg_info;
+
+/* What esg_scorer_autotune measured: device time of the batched kernels on
+ * calibration batches of each read length, with 16-row and 32-row stripes. */
+#define ESG_TUNE_MAX_LENGTHS 8
+typedef struct esg_tune_report {
+    uint32_t n_lengths;
+    uint32_t lengths[ESG_TUNE_MAX_LENGTHS];
+    float ms_rows16[ESG_TUNE_MAX_LENGTHS];
+    float ms_rows32[ESG_TUNE_MAX_LENGTHS];
+    uint32_t split_len;
+} esg_tune_report;
 
 typedef struct esg_batch_stats {
     uint32_t n_reads;
@@ -147,6 +160,15 @@ void esg_scorer_free(esg_scorer* scorer);
 esg_status esg_scorer_info(const esg_scorer* scorer, esg_info* out);
 /* GpuScorer::set_half2 (cuda/mod.rs:500-502): ESG_KERNEL_AUTO or _PLAIN32. */
 esg_status esg_scorer_set_kernel(esg_scorer* scorer, int32_t kernel);
+/* Tile-shape autotuner (no counterpart in the reference, whose one kernel
+ * shape is fixed): times the batched kernels on synthetic calibration
+ * batches of read lengths 48..448 (each +-25 %) against this panel, with 16-row and
+ * 32-row stripes per lane, and sets the length up to which 16-row stripes
+ * are used.  Scores do not depend on the choice.  `out` may be NULL. */
+esg_status esg_scorer_autotune(esg_scorer* scorer, esg_tune_report* out);
+/* Set the 16/32-row split by hand (0: every query on 32-row stripes). */
+esg_status esg_scorer_set_split(esg_scorer* scorer, uint32_t split_len);
+
 /* GpuScorer::scores_len (cuda/mod.rs:506-508): 1 for every len > 0 -- nothing
  * is left to a CPU path. */
 int32_t esg_scores_len(const esg_scorer* scorer, uint64_t len);

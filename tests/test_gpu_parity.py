@@ -35,8 +35,12 @@ def oracle_rows(O, reads, panel, scoring, local):
     return O.score_matrix(list(reads) + rc, panel, scoring, local)
 
 
-def check(O, panel, reads, scoring, mode, what, kernels=(KERNEL_AUTO, KERNEL_PLAIN32),
-          tie_capacity=CAP):
+# (kernel, 16/32-row split): 16-row stripes up to 512 nt, every query on
+# 32-row stripes, the plain int32 kernel
+CONFIGS = ((KERNEL_AUTO, 512), (KERNEL_AUTO, 0), (KERNEL_PLAIN32, 256))
+
+
+def check(O, panel, reads, scoring, mode, what, kernels=CONFIGS, tie_capacity=CAP):
     """gpu_parity.rs:132-192."""
     local = mode == Mode.LOCAL
     want_rows = oracle_rows(O, reads, panel, scoring, local)
@@ -45,8 +49,9 @@ def check(O, panel, reads, scoring, mode, what, kernels=(KERNEL_AUTO, KERNEL_PLA
     n = len(reads)
     stats = {}
     with GpuScorer(panel, Scoring(*scoring), mode, tie_capacity=tie_capacity) as g:
-        for kernel in kernels:
+        for kernel, split in kernels:
             g.set_kernel(kernel)
+            g.set_split(split)
             res = g.score_batch(reads, both_strands=True, full_rows=True)
             got = res.rows
             assert got.shape == want_rows.shape
@@ -60,7 +65,8 @@ def check(O, panel, reads, scoring, mode, what, kernels=(KERNEL_AUTO, KERNEL_PLA
             for k in range(n):
                 nl = min(int(want_res["n_tied"][k]), tie_capacity)
                 assert (res.ties[k, :nl] == want_ties[k, :nl]).all(), (what, k, kernel)
-            stats[kernel] = res.stats
+            stats[(kernel, split)] = res.stats
+            stats.setdefault(kernel, res.stats)
     return stats
 
 
@@ -106,10 +112,11 @@ def test_gpu_golden_pairs(oracle):
         q, r = encode(c["query"]), encode(c["reference"])
         mode = Mode.LOCAL if c["mode"] == "local" else Mode.SEMIGLOBAL
         with GpuScorer([r], Scoring(*c["scheme"]), mode) as s:
-            for kernel in (KERNEL_AUTO, KERNEL_PLAIN32):
+            for kernel, split in CONFIGS:
                 s.set_kernel(kernel)
+                s.set_split(split)
                 res = s.score_batch([q], full_rows=True)
-                assert res.rows[0, 0] == c["score"], (c["name"], c["mode"], kernel)
+                assert res.rows[0, 0] == c["score"], (c["name"], c["mode"], kernel, split)
 
 
 def test_gpu_long_and_straddling_reads(oracle):
@@ -290,3 +297,19 @@ def test_gpu_strand_swap_property():
     for k in range(len(reads)):
         n = min(int(a.results["n_tied"][k]), CAP)
         assert sorted(a.ties[k, :n] ^ 1) == sorted(b.ties[k, :n]) or a.results["n_tied"][k] > CAP
+
+
+def test_gpu_autotune_measures_and_keeps_results(oracle):
+    """The tile-shape autotuner times 16- and 32-row stripes on this panel,
+    picks a split, and the scores do not change with it."""
+    refs = synth.panel_tiles()
+    reads = synth.reads_c2(refs, n=3000)
+    with GpuScorer(refs, Scoring(), Mode.LOCAL) as g:
+        before = g.score_batch(reads.tuple(), both_strands=True)
+        rep = g.autotune()
+        assert len(rep["lengths"]) == 7 and all(t > 0 for t in rep["ms_rows16"] + rep["ms_rows32"])
+        assert rep["split_len"] in (0, 48, 80, 112, 160, 224, 320, 512)
+        info = g.info()
+        assert info["tuned"] == 1 and info["split_len"] == rep["split_len"]
+        after = g.score_batch(reads.tuple(), both_strands=True)
+        assert (before.results == after.results).all() and (before.ties == after.ties).all()
