@@ -99,8 +99,15 @@ class EsgBatchStats(C.Structure):
     _fields_ = [("n_reads", C.c_uint32), ("n_queries", C.c_uint32), ("n_empty", C.c_uint32),
                 ("queries_batched", C.c_uint32), ("queries_plain", C.c_uint32),
                 ("queries_rescored", C.c_uint32), ("tasks", C.c_uint32),
-                ("lanes_used", C.c_uint32), ("kernels", C.c_uint32), ("cells", C.c_uint64), ("h2d_bytes", C.c_uint64),
-                ("d2h_bytes", C.c_uint64)]
+                ("lanes_used", C.c_uint32), ("kernels", C.c_uint32), ("cells", C.c_uint64),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("n_pairs", C.c_uint32),
+                ("mates_trimmed", C.c_uint32), ("bases_trimmed", C.c_uint64)]
+
+
+class EsgAdapterConfig(C.Structure):
+    _fields_ = [("r1", C.c_void_p), ("r1_len", C.c_uint32), ("r2", C.c_void_p),
+                ("r2_len", C.c_uint32), ("min_overlap", C.c_uint32),
+                ("max_read_len", C.c_uint32)]
 
 
 # every entry point include/eschalign_b200.h declares: name -> (restype, argtypes)
@@ -132,6 +139,16 @@ SIGNATURES = {
     "esg_batch_free": (None, [C.c_void_p]),
     "esg_batch_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(EsgBatchStats)]),
     "esg_relaunch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "esg_pair_adapters": (C.c_int32, [_u8p, _u64p, _u32p, C.c_uint32,
+                                      C.POINTER(EsgAdapterConfig), _u32p, _u32p]),
+    "esg_prepare_pairs": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32,
+                                      C.POINTER(EsgAdapterConfig), C.c_int32, C.c_uint32,
+                                      C.POINTER(C.c_void_p)]),
+    "esg_finish_pairs": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, _u32p, C.c_void_p,
+                                     _u32p, _u32p, _i32p]),
+    "esg_score_pairs": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32,
+                                    C.POINTER(EsgAdapterConfig), C.c_int32, C.c_uint32,
+                                    C.c_void_p, _u32p, C.c_void_p, _u32p, _u32p, _i32p]),
     "esg_score_rows_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_uint32, C.POINTER(EsgScoring), C.c_int32,

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace esg;
@@ -156,6 +157,12 @@ struct esg_batch {
   uint32_t n_order = 0;
   uint32_t host_list = 0;
   uint32_t redo_cap = 0;
+  // paired batches (esg_prepare_pairs): reads 2p, 2p + 1 are pair p's mates
+  bool paired = false;
+  bool pair_both = false;   // rank both template strands
+  int32_t min_score = 0;
+  uint32_t n_pairs = 0;
+  std::vector<uint32_t> adapters;  // adapter bases removed, per mate
   // pinned staging (inputs, then outputs)
   Pinned in_buf, out_buf;
   uint8_t* h_codes = nullptr;
@@ -169,6 +176,8 @@ struct esg_batch {
   uint32_t* h_ties = nullptr;
   int32_t* h_rows = nullptr;
   uint32_t* h_counters = nullptr;
+  int4* h_pairs = nullptr;
+  uint32_t* h_pties = nullptr;
   // device
   void* d_mem = nullptr;
   size_t d_bytes = 0;
@@ -185,6 +194,8 @@ struct esg_batch {
   int4* d_results = nullptr;
   uint32_t* d_ties = nullptr;
   int32_t* d_rows = nullptr;
+  int4* d_pairs = nullptr;
+  uint32_t* d_pties = nullptr;
   cudaEvent_t done = nullptr;
   bool submitted = false;
   esg_scorer* owner = nullptr;
@@ -891,7 +902,7 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
 static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t st) {
   const bool both = b->flags & ESG_BOTH_STRANDS;
   uint32_t kernels = 0;
-  const bool rows = b->flags & ESG_FULL_ROWS;
+  const bool rows = b->d_rows != nullptr;
   ESG_CUDA(cudaMemsetAsync(b->d_counters, 0, 8 * sizeof(uint32_t), st));
   if (b->n_tasks) {
     K2Params P{};
@@ -1028,9 +1039,29 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
     M.cap = sc->cap;
     M.results = b->d_results;
     M.ties = b->d_ties;
+    M.rows = b->d_rows;
+    M.n_refs = sc->n_refs;
     const int blocks = (int)std::min<uint64_t>(4096, (b->n_reads + 255) / 256);
     void* margs[] = {&M};
     ESG_CUDA(cudaLaunchKernel((const void*)k5_merge, dim3(blocks), dim3(256), margs, 0, st));
+    ++kernels;
+  }
+  if (b->paired && b->n_pairs) {
+    K6Params X{};
+    X.rows = b->d_rows;
+    X.len = b->d_len;
+    X.mates = b->d_results;
+    X.n_pairs = b->n_pairs;
+    X.n_reads = b->n_reads;
+    X.n_refs = sc->n_refs;
+    X.cap = sc->cap;
+    X.min_score = b->min_score;
+    X.both = b->pair_both;
+    X.out = b->d_pairs;
+    X.ties = b->d_pties;
+    const int blocks = (int)std::min<uint64_t>((uint64_t)sc->sm_count * 16, (b->n_pairs + 7) / 8);
+    void* xargs[] = {&X};
+    ESG_CUDA(cudaLaunchKernel((const void*)k6_pairs, dim3(blocks), dim3(256), xargs, 0, st));
     ++kernels;
   }
   b->stats.kernels = kernels;
@@ -1044,6 +1075,8 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   ESG_CUDA(cudaSetDevice(sc->device));
   cudaStream_t st = sc->stream;
   const bool rows = b->flags & ESG_FULL_ROWS;
+  const bool dev_rows = rows || b->paired;  // the pair ranking reads the rows
+  const size_t np = b->paired ? std::max<uint32_t>(b->n_pairs, 1) : 0;
   const uint32_t nlist = b->host_list + b->redo_cap;
   const size_t nr = b->n_reads ? b->n_reads : 1, nq = b->n_q ? b->n_q : 1;
   // device buffers, one stream-ordered allocation
@@ -1060,7 +1093,9 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
       carve_size(nlist ? (size_t)nlist * sc->n_refs : 1, 4),
       carve_size(nr, 16),
       carve_size(nr * sc->cap, 4),
-      rows ? carve_size(nq * sc->n_refs, 4) : 0,
+      dev_rows ? carve_size(nq * sc->n_refs, 4) : 0,
+      carve_size(2 * np, 16),
+      carve_size(np * sc->cap, 4),
   };
   size_t total = 0;
   for (size_t v : sizes) total += v;
@@ -1079,7 +1114,9 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   b->d_k3out = carve<int32_t>(at, nlist ? (size_t)nlist * sc->n_refs : 1);
   b->d_results = carve<int4>(at, nr);
   b->d_ties = carve<uint32_t>(at, nr * sc->cap);
-  b->d_rows = rows ? carve<int32_t>(at, nq * sc->n_refs) : nullptr;
+  b->d_rows = dev_rows ? carve<int32_t>(at, nq * sc->n_refs) : nullptr;
+  b->d_pairs = np ? carve<int4>(at, 2 * np) : nullptr;
+  b->d_pties = np ? carve<uint32_t>(at, np * sc->cap) : nullptr;
   // uploads: the pinned staging is one contiguous block laid out the same way
   // for the first six buffers
   ESG_CUDA(cudaMemcpyAsync(b->d_codes, b->in_buf.p, b->in_bytes, cudaMemcpyHostToDevice, st));
@@ -1088,7 +1125,8 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   if (s != ESG_OK) return s;
   // downloads into pinned staging
   const size_t out_bytes = carve_size(nr, 16) + carve_size(nr * sc->cap, 4) +
-                           (rows ? carve_size(nq * sc->n_refs, 4) : 0) + carve_size(4, 4);
+                           (rows ? carve_size(nq * sc->n_refs, 4) : 0) + carve_size(4, 4) +
+                           carve_size(2 * np, 16) + carve_size(np * sc->cap, 4);
   b->out_buf.p = sc->pinned.get(out_bytes, &b->out_buf.cap);
   if (!b->out_buf.p) return fail(ESG_ERR_OUT_OF_MEMORY, "pinned host memory (%zu bytes)", out_bytes);
   char* o = (char*)b->out_buf.p;
@@ -1096,6 +1134,8 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   b->h_ties = carve<uint32_t>(o, nr * sc->cap);
   b->h_counters = carve<uint32_t>(o, 4);
   b->h_rows = rows ? carve<int32_t>(o, nq * sc->n_refs) : nullptr;
+  b->h_pairs = np ? carve<int4>(o, 2 * np) : nullptr;
+  b->h_pties = np ? carve<uint32_t>(o, np * sc->cap) : nullptr;
   // d_results and d_ties are adjacent in device memory, as in the staging
   ESG_CUDA(cudaMemcpyAsync(b->h_results, b->d_results,
                            carve_size(nr, 16) + carve_size(nr * sc->cap, 4),
@@ -1104,8 +1144,12 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   if (rows)
     ESG_CUDA(cudaMemcpyAsync(b->h_rows, b->d_rows, (size_t)b->n_q * sc->n_refs * 4,
                              cudaMemcpyDeviceToHost, st));
+  if (np)  // d_pairs and d_pties are adjacent too
+    ESG_CUDA(cudaMemcpyAsync(b->h_pairs, b->d_pairs, carve_size(2 * np, 16) + np * sc->cap * 4,
+                             cudaMemcpyDeviceToHost, st));
   b->stats.d2h_bytes = carve_size(nr, 16) + carve_size(nr * sc->cap, 4) + 16 +
-                       (rows ? (size_t)b->n_q * sc->n_refs * 4 : 0);
+                       (rows ? (size_t)b->n_q * sc->n_refs * 4 : 0) +
+                       (np ? carve_size(2 * np, 16) + np * sc->cap * 4 : 0);
   ESG_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
   ESG_CUDA(cudaEventRecord(b->done, st));
   b->submitted = true;
@@ -1174,6 +1218,198 @@ esg_status esg_score_batch(esg_scorer* sc, const uint8_t* codes, const uint64_t*
   if (s != ESG_OK) return s;
   s = esg_submit(sc, b);
   if (s == ESG_OK) s = esg_finish(sc, b, results, ties, rows);
+  const std::string keep = g_err;
+  esg_batch_free(b);
+  g_err = keep;
+  return s;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- pairs
+namespace {
+
+// Adapter bases at the 3' end of `read` (crates/eschalign/src/adapter.rs:68-91):
+// the leftmost start whose overlap with the adapter's prefix has at most one
+// mismatch per ten bases (the wildcard matching anything) marks everything
+// from there as adapter.  A start is given up at its first mismatch past
+// the allowance, which gives the same answer as counting them all.
+uint32_t adapter_at(const uint8_t* read, uint32_t n, const uint8_t* ad, uint32_t a,
+                    uint32_t min_overlap) {
+  if (n < min_overlap || a == 0) return 0;
+  for (uint32_t p = 0; p + min_overlap <= n; ++p) {
+    const uint32_t overlap = std::min(a, n - p);
+    if (overlap < min_overlap) break;
+    const uint32_t allow = overlap / 10;
+    uint32_t mism = 0, k = 0;
+    for (; k < overlap; ++k) {
+      const uint8_t x = read[p + k], y = ad[k];
+      if (x != y && x != 4 && y != 4 && ++mism > allow) break;
+    }
+    if (k == overlap) return n - p;
+  }
+  return 0;
+}
+
+// pair_adapters (crates/eschalign-cli/src/align.rs:934-949) and detect_pair
+// (adapter.rs:95-110): a mate over max_read_len is neither aligned nor
+// searched; otherwise both are searched and, where their insert ends
+// disagree, the weaker detection (shorter overlap) is dropped, both on a tie.
+void pair_adapters(const uint8_t* m1, uint32_t l1, const uint8_t* m2, uint32_t l2,
+                   const esg_adapter_config& c, uint32_t out[2]) {
+  const uint32_t mo = std::max<uint32_t>(c.min_overlap, 1);
+  const bool o1 = c.max_read_len && l1 > c.max_read_len;
+  const bool o2 = c.max_read_len && l2 > c.max_read_len;
+  out[0] = o1 ? 0 : adapter_at(m1, l1, c.r1, c.r1_len, mo);
+  out[1] = o2 ? 0 : adapter_at(m2, l2, c.r2, c.r2_len, mo);
+  if (!o1 && !o2 && out[0] && out[1] && l1 - out[0] != l2 - out[1]) {
+    const uint32_t e1 = std::min(out[0], c.r1_len), e2 = std::min(out[1], c.r2_len);
+    if (e1 > e2)
+      out[1] = 0;
+    else if (e1 < e2)
+      out[0] = 0;
+    else
+      out[0] = out[1] = 0;
+  }
+}
+
+// Adapters and aligned lengths of every mate of a batch (align.rs:2844-2863:
+// the mate less its 3' adapter; nothing for a mate over max_read_len), on up
+// to 32 host threads.
+void trim_batch(const uint8_t* codes, const uint64_t* off, const uint32_t* len, uint32_t n_pairs,
+                const esg_adapter_config& cfg, uint32_t* ads, uint32_t* tl) {
+  const bool trim = cfg.r1_len || cfg.r2_len;
+  auto work = [&](uint32_t p0, uint32_t p1) {
+    for (uint32_t p = p0; p < p1; ++p) {
+      const uint32_t a = 2 * p, b = a + 1;
+      uint32_t ad[2] = {0, 0};
+      if (trim) pair_adapters(codes + off[a], len[a], codes + off[b], len[b], cfg, ad);
+      for (uint32_t m = 0; m < 2; ++m) {
+        const uint32_t k = a + m;
+        ads[k] = ad[m];
+        tl[k] = (cfg.max_read_len && len[k] > cfg.max_read_len) ? 0 : len[k] - ad[m];
+      }
+    }
+  };
+  const uint32_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const uint32_t nt = std::max(1u, std::min(hw, n_pairs / 8192));
+  if (nt == 1) {
+    work(0, n_pairs);
+    return;
+  }
+  std::vector<std::thread> th;
+  const uint32_t per = (n_pairs + nt - 1) / nt;
+  for (uint32_t t = 0; t < nt; ++t)
+    th.emplace_back(work, std::min(n_pairs, t * per), std::min(n_pairs, (t + 1) * per));
+  for (auto& x : th) x.join();
+}
+
+esg_status check_adapters(const esg_adapter_config* adapters, esg_adapter_config* cfg) {
+  *cfg = esg_adapter_config{};
+  if (!adapters) return ESG_OK;
+  *cfg = *adapters;
+  if ((cfg->r1_len && !cfg->r1) || (cfg->r2_len && !cfg->r2))
+    return fail(ESG_ERR_BAD_ARGUMENT, "adapter codes must not be NULL");
+  return ESG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+esg_status esg_pair_adapters(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
+                             uint32_t n_pairs, const esg_adapter_config* adapters,
+                             uint32_t* adapter_bases, uint32_t* aligned_len) {
+  g_err.clear();
+  if (n_pairs && (!off || !len || !adapter_bases || !aligned_len))
+    return fail(ESG_ERR_BAD_ARGUMENT, "off/len/outputs must not be NULL");
+  esg_adapter_config cfg{};
+  if (esg_status s = check_adapters(adapters, &cfg); s != ESG_OK) return s;
+  if (n_pairs && !codes && (cfg.r1_len || cfg.r2_len)) {
+    uint64_t total = 0;
+    for (uint64_t k = 0; k < 2ull * n_pairs; ++k) total += len[k];
+    if (total) return fail(ESG_ERR_BAD_ARGUMENT, "codes must not be NULL");
+  }
+  trim_batch(codes, off, len, n_pairs, cfg, adapter_bases, aligned_len);
+  return ESG_OK;
+}
+
+esg_status esg_prepare_pairs(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                             const uint32_t* len, uint32_t n_pairs,
+                             const esg_adapter_config* adapters, int32_t min_score,
+                             uint32_t flags, esg_batch** out) {
+  g_err.clear();
+  if (!sc || !out) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer or out");
+  *out = nullptr;
+  if (flags & ~(ESG_BOTH_STRANDS | ESG_FULL_ROWS))
+    return fail(ESG_ERR_BAD_ARGUMENT, "unknown flags 0x%x", flags);
+  if (n_pairs >= (1u << 29)) return fail(ESG_ERR_BAD_ARGUMENT, "too many pairs (%u)", n_pairs);
+  if (n_pairs && (!off || !len)) return fail(ESG_ERR_BAD_ARGUMENT, "off/len must not be NULL");
+  const uint32_t n_reads = 2 * n_pairs;
+  std::vector<uint32_t> tl(n_reads), ads(n_reads, 0);
+  esg_adapter_config cfg{};
+  if (esg_status s = check_adapters(adapters, &cfg); s != ESG_OK) return s;
+  if (n_reads && !codes) {
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < n_reads; ++k) total += len[k];
+    if (total) return fail(ESG_ERR_BAD_ARGUMENT, "codes must not be NULL");
+  }
+  trim_batch(codes, off, len, n_pairs, cfg, ads.data(), tl.data());
+  esg_batch* b = nullptr;
+  // every mate on both strands: the template strands need mate 1 forward and
+  // mate 2 reverse-complemented (and the opposite), the Separate fallback
+  // ranks each mate on both strands (pair.rs:366-387)
+  esg_status s = esg_prepare(sc, codes, off, tl.data(), n_reads,
+                             ESG_BOTH_STRANDS | (flags & ESG_FULL_ROWS), &b);
+  if (s != ESG_OK) return s;
+  b->paired = true;
+  b->pair_both = flags & ESG_BOTH_STRANDS;
+  b->min_score = min_score;
+  b->n_pairs = n_pairs;
+  uint32_t mt = 0;
+  uint64_t bt = 0;
+  for (uint32_t v : ads) {
+    mt += v != 0;
+    bt += v;
+  }
+  b->adapters = std::move(ads);
+  b->stats.n_pairs = n_pairs;
+  b->stats.mates_trimmed = mt;
+  b->stats.bases_trimmed = bt;
+  *out = b;
+  return ESG_OK;
+}
+
+esg_status esg_finish_pairs(esg_scorer* sc, esg_batch* b, esg_pair_result* pairs,
+                            uint32_t* pair_ties, esg_read_result* mates, uint32_t* mate_ties,
+                            uint32_t* adapter_bases, int32_t* rows) {
+  if (b && !b->paired) {
+    g_err.clear();
+    return fail(ESG_ERR_BAD_ARGUMENT, "not a paired batch");
+  }
+  esg_status s = esg_finish(sc, b, mates, mate_ties, rows);
+  if (s != ESG_OK) return s;
+  if (pairs && b->n_pairs) {
+    static_assert(sizeof(esg_pair_result) == 32, "esg_pair_result is two int4");
+    memcpy(pairs, b->h_pairs, (size_t)b->n_pairs * 32);
+  }
+  if (pair_ties && b->n_pairs) memcpy(pair_ties, b->h_pties, (size_t)b->n_pairs * sc->cap * 4);
+  if (adapter_bases && b->n_pairs)
+    memcpy(adapter_bases, b->adapters.data(), (size_t)b->n_pairs * 2 * 4);
+  return ESG_OK;
+}
+
+esg_status esg_score_pairs(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                           const uint32_t* len, uint32_t n_pairs,
+                           const esg_adapter_config* adapters, int32_t min_score, uint32_t flags,
+                           esg_pair_result* pairs, uint32_t* pair_ties, esg_read_result* mates,
+                           uint32_t* mate_ties, uint32_t* adapter_bases, int32_t* rows) {
+  esg_batch* b = nullptr;
+  esg_status s = esg_prepare_pairs(sc, codes, off, len, n_pairs, adapters, min_score, flags, &b);
+  if (s != ESG_OK) return s;
+  s = esg_submit(sc, b);
+  if (s == ESG_OK)
+    s = esg_finish_pairs(sc, b, pairs, pair_ties, mates, mate_ties, adapter_bases, rows);
   const std::string keep = g_err;
   esg_batch_free(b);
   g_err = keep;

@@ -22,6 +22,9 @@
 //   k4_rows      per-query reduction of k3's rows (mapper.rs:444-472).
 //   k5_merge     per read: forward and reverse-complement query states
 //                merged into the read's result.
+//   k6_pairs     paired batches: per pair, the (reference, template strand)
+//                candidates of crates/eschalign/src/mapper/pair.rs:195-234
+//                ranked from the four mate rows (one warp per pair).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -794,6 +797,8 @@ struct K5Params {
   uint32_t cap;
   int4* results;       // esg_read_result layout
   uint32_t* ties;      // [read * cap + k]
+  int32_t* rows;       // optional rows: an empty read's rows score 0 (no cell)
+  uint32_t n_refs;
 };
 
 static __global__ void __launch_bounds__(256) k5_merge(const K5Params P) {
@@ -804,6 +809,12 @@ static __global__ void __launch_bounds__(256) k5_merge(const K5Params P) {
     if (P.len[r] == 0) {
       P.results[r] = make_int4(INT32_MIN, INT32_MIN, 0, 1 /* ESG_RESULT_EMPTY */);
       for (uint32_t k = 0; k < cap; ++k) out_t[k] = kNoRef;
+      if (P.rows) {
+        for (uint32_t j = 0; j < P.n_refs; ++j) P.rows[(size_t)r * P.n_refs + j] = 0;
+        if (P.both)
+          for (uint32_t j = 0; j < P.n_refs; ++j)
+            P.rows[((size_t)P.n_reads + r) * P.n_refs + j] = 0;
+      }
       continue;
     }
     const int4 a = P.qhead[r];
@@ -842,6 +853,113 @@ static __global__ void __launch_bounds__(256) k5_merge(const K5Params P) {
     for (uint32_t k = min(n_tied, cap); k < cap; ++k) out_t[k] = kNoRef;  // ESG_NO_TIE
     if (n_tied > cap) flags |= 2;  // ESG_RESULT_TIES_TRUNCATED
     P.results[r] = make_int4(best, sub, (int)n_tied, flags);
+  }
+}
+
+// ---------------------------------------------------------------- k6_pairs
+// One warp per read pair.  Rows: mate m of pair p is read 2p + m; its
+// forward row is query 2p + m, its reverse-complement row n_reads + 2p + m.
+// Candidate (r, t): t = 0 pairs mate 1 forward with mate 2 reverse-
+// complemented, t = 1 mate 1 reverse-complemented with mate 2 forward
+// (pair.rs:135-137); eligible when both mate scores are >= min_score.
+// Pass 1 takes the best eligible sum; pass 2 walks the references in
+// 32-wide chunks and, in (r, t) order, lists the first tier (ballots give
+// each tie its rank), and takes the next tier's sum and the per-mate best
+// over candidates outside the tier (pair.rs:297-314).
+struct K6Params {
+  const int32_t* rows;   // [q * n_refs + r], q < 2 n_reads
+  const uint32_t* len;   // trimmed mate lengths [n_reads]
+  const int4* mates;     // k5's per-mate results (for RESCORED32)
+  uint32_t n_pairs;
+  uint32_t n_reads;
+  uint32_t n_refs;
+  uint32_t cap;
+  int32_t min_score;
+  int both;              // both template strands
+  int4* out;             // [2 p]: best, next, n_tied, flags; [2 p + 1]: xs[2], primary[2]
+  uint32_t* ties;        // [p * cap + k]
+};
+
+static __global__ void __launch_bounds__(256) k6_pairs(const K6Params P) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t wpb = blockDim.x >> 5;
+  const int32_t ms = P.min_score;
+  for (uint32_t p = blockIdx.x * wpb + (threadIdx.x >> 5); p < P.n_pairs; p += gridDim.x * wpb) {
+    uint32_t* out_t = P.ties + (size_t)p * P.cap;
+    const size_t nr = P.n_refs;
+    const int32_t* f0 = P.rows + (size_t)(2 * p) * nr;
+    const int32_t* f1 = f0 + nr;
+    const int32_t* r0 = P.rows + (size_t)(P.n_reads + 2 * p) * nr;
+    const int32_t* r1 = r0 + nr;
+    const bool empty = P.len[2 * p] == 0 || P.len[2 * p + 1] == 0;
+    int32_t best = INT32_MIN;
+    if (!empty) {
+      for (uint32_t r = lane; r < P.n_refs; r += 32) {
+        const int32_t a = f0[r], b = r1[r];
+        if (a >= ms && b >= ms) best = max(best, a + b);
+        if (P.both) {
+          const int32_t c = r0[r], d = f1[r];
+          if (c >= ms && d >= ms) best = max(best, c + d);
+        }
+      }
+    }
+    best = __reduce_max_sync(kFull, best);
+    const bool any = best != INT32_MIN;
+    int32_t next = INT32_MIN, xs0 = INT32_MIN, xs1 = INT32_MIN, pa = INT32_MIN, pb = INT32_MIN;
+    uint32_t n = 0;
+    if (!empty) {
+      for (uint32_t c0 = 0; c0 < P.n_refs; c0 += 32) {
+        const uint32_t r = c0 + lane;
+        const bool valid = r < P.n_refs;
+        int32_t a = 0, b = 0, c = 0, d = 0;
+        bool tie0 = false, tie1 = false;
+        if (valid) {
+          a = f0[r];
+          b = r1[r];
+          const bool e0 = a >= ms && b >= ms;
+          tie0 = e0 && a + b == best;
+          if (!tie0) {
+            if (e0) next = max(next, a + b);
+            xs0 = max(xs0, a);
+            xs1 = max(xs1, b);
+          }
+          if (P.both) {
+            c = r0[r];
+            d = f1[r];
+            const bool e1 = c >= ms && d >= ms;
+            tie1 = e1 && c + d == best;
+            if (!tie1) {
+              if (e1) next = max(next, c + d);
+              xs0 = max(xs0, c);
+              xs1 = max(xs1, d);
+            }
+          }
+        }
+        const uint32_t b0 = __ballot_sync(kFull, tie0), b1 = __ballot_sync(kFull, tie1);
+        if ((b0 | b1) == 0) continue;
+        if (n == 0) {  // the primary: the first tie in (r, t) order
+          const int src = __ffs(b0 | b1) - 1;
+          const bool t0 = (b0 >> src) & 1u;
+          pa = __shfl_sync(kFull, t0 ? a : c, src);
+          pb = __shfl_sync(kFull, t0 ? b : d, src);
+        }
+        const uint32_t pre = n + __popc(b0 & lt) + __popc(b1 & lt);
+        if (tie0 && pre < P.cap) out_t[pre] = r << 1;
+        if (tie1 && pre + tie0 < P.cap) out_t[pre + tie0] = (r << 1) | 1u;
+        n += __popc(b0) + __popc(b1);
+      }
+    }
+    next = __reduce_max_sync(kFull, next);
+    xs0 = __reduce_max_sync(kFull, xs0);
+    xs1 = __reduce_max_sync(kFull, xs1);
+    for (uint32_t k = min(n, P.cap) + lane; k < P.cap; k += 32) out_t[k] = kNoRef;  // ESG_NO_TIE
+    if (lane == 0) {
+      int flags = (any ? 0 : 1) | (n > P.cap ? 2 : 0);  // ESG_RESULT_EMPTY / _TIES_TRUNCATED
+      if (!empty) flags |= (P.mates[2 * p].w | P.mates[2 * p + 1].w) & kQRescored;
+      P.out[2 * p] = make_int4(best, next, (int)n, flags);
+      P.out[2 * p + 1] = make_int4(xs0, xs1, pa, pb);
+    }
   }
 }
 

@@ -77,6 +77,22 @@ def pack_reads(reads):
     return np.ascontiguousarray(codes), off, lens
 
 
+def _inputs_of(reads):
+    """(codes, off, lens) arrays as the C ABI takes them, from a list of code
+    arrays, a Packed-like object or a (codes, off, lens) tuple."""
+    if hasattr(reads, "tuple") and callable(reads.tuple):
+        reads = reads.tuple()
+    if isinstance(reads, tuple) and len(reads) == 3:
+        codes, off, lens = reads
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        lens = np.ascontiguousarray(lens, dtype=np.uint32)
+        if codes.size == 0:
+            codes = np.zeros(1, dtype=np.uint8)
+        return codes, off, lens
+    return pack_reads(reads)
+
+
 def device_visible() -> bool:
     """cuda/mod.rs:130-140."""
     lib = _native.load()
@@ -207,6 +223,57 @@ class PreparedBatch:
 PendingBatch = PreparedBatch
 
 
+PAIR_DTYPE = np.dtype([("best", "<i4"), ("next", "<i4"), ("n_tied", "<u4"), ("flags", "<u4"),
+                       ("xs", "<i4", (2,)), ("primary", "<i4", (2,))])
+
+
+@dataclass
+class PairScores:
+    """One pair's ranked candidates (pair.rs:195-234): the first tier's
+    summed score, its members as (reference, template_reverse), the next
+    tier's sum, per-mate XS outside the tier (pair.rs:297-314) and the
+    primary's mate scores.  ``best is None``: no eligible candidate, the
+    pair falls back to each mate on its own (pair.rs:366-387)."""
+    best: int | None
+    next: int | None
+    n_tied: int
+    ties: list
+    xs: tuple
+    primary: tuple
+    truncated: bool
+    rescored32: bool
+
+
+class PairBatchResult:
+    """What esg_finish_pairs returns for one paired batch."""
+
+    def __init__(self, pairs, pair_ties, mates: BatchResult, adapters, stats, cap):
+        self.pairs = pairs
+        self.pair_ties = pair_ties
+        self.mates = mates
+        self.adapters = adapters
+        self.stats = stats
+        self.cap = cap
+
+    def __len__(self):
+        return self.pairs.size
+
+    def pair(self, p: int) -> PairScores:
+        r = self.pairs[p]
+        opt = lambda v: None if v == NO_SCORE else int(v)  # noqa: E731
+        n = min(int(r["n_tied"]), self.cap)
+        ties = [(int(c) >> 1, bool(int(c) & 1)) for c in self.pair_ties[p, :n]]
+        return PairScores(opt(r["best"]), opt(r["next"]), int(r["n_tied"]), ties,
+                          (opt(r["xs"][0]), opt(r["xs"][1])),
+                          (opt(r["primary"][0]), opt(r["primary"][1])),
+                          bool(r["flags"] & RESULT_TIES_TRUNCATED),
+                          bool(r["flags"] & RESULT_RESCORED32))
+
+    def mate(self, p: int, m: int) -> ReadScores:
+        """Mate m (0 or 1) of pair p alone, both strands (the Separate fallback)."""
+        return self.mates.read(2 * p + m)
+
+
 class GpuScorer:
     """A panel resident on a device under one scoring and one mode."""
 
@@ -302,16 +369,9 @@ class GpuScorer:
         return bool(self._lib.esg_scores_len(self._h, n))
 
     # -- batches
-    def _inputs(self, reads):
-        if isinstance(reads, tuple) and len(reads) == 3:
-            codes, off, lens = reads
-            codes = np.ascontiguousarray(codes, dtype=np.uint8)
-            off = np.ascontiguousarray(off, dtype=np.uint64)
-            lens = np.ascontiguousarray(lens, dtype=np.uint32)
-            if codes.size == 0:
-                codes = np.zeros(1, dtype=np.uint8)
-            return codes, off, lens
-        return pack_reads(reads)
+    @staticmethod
+    def _inputs(reads):
+        return _inputs_of(reads)
 
     def prepare(self, reads, both_strands: bool = False, full_rows: bool = False) -> PreparedBatch:
         codes, off, lens = self._inputs(reads)
@@ -348,6 +408,60 @@ class GpuScorer:
     def score_batch(self, reads, both_strands: bool = False, full_rows: bool = False) -> BatchResult:
         """cuda/mod.rs:524-528."""
         return self.finish(self.submit(self.prepare(reads, both_strands, full_rows)))
+
+    # -- paired-end (pair.rs:157-234, fed as align.rs:2844-2872 feeds it)
+    def prepare_pairs(self, mates, adapters=None, min_score: int = 0, both_strands: bool = True,
+                      full_rows: bool = False) -> PreparedBatch:
+        """Mates 2p (mate 1) and 2p + 1 (mate 2), as sequenced.  ``adapters``:
+        None, or dict(r1=codes, r2=codes, min_overlap=5, max_read_len=0)
+        (adapter.rs:46-54; align.rs:934-949)."""
+        codes, off, lens = self._inputs(mates)
+        if lens.size % 2:
+            raise ValueError("mates come in pairs: an even number of reads is needed")
+        flags = (BOTH_STRANDS if both_strands else 0) | (FULL_ROWS if full_rows else 0)
+        cfg_p, keep = None, None
+        if adapters is not None:
+            r1 = np.ascontiguousarray(adapters.get("r1", np.zeros(0)), dtype=np.uint8)
+            r2 = np.ascontiguousarray(adapters.get("r2", np.zeros(0)), dtype=np.uint8)
+            cfg = _native.EsgAdapterConfig(r1.ctypes.data if r1.size else None, r1.size,
+                                           r2.ctypes.data if r2.size else None, r2.size,
+                                           int(adapters.get("min_overlap", 5)),
+                                           int(adapters.get("max_read_len", 0)))
+            cfg_p, keep = C.byref(cfg), (r1, r2, cfg)
+        h = C.c_void_p()
+        _check(self._lib, self._lib.esg_prepare_pairs(
+            self._h, _ptr(codes, C.c_uint8), _ptr(off, C.c_uint64), _ptr(lens, C.c_uint32),
+            lens.size // 2, cfg_p, int(min_score), flags, C.byref(h)))
+        del keep
+        b = PreparedBatch(self, h, int(lens.size), flags | BOTH_STRANDS, None)
+        b.paired = True
+        return b
+
+    def finish_pairs(self, batch: PendingBatch, keep: bool = False) -> PairBatchResult:
+        n = batch.n_reads
+        npairs = n // 2
+        pairs = np.zeros(npairs, dtype=PAIR_DTYPE)
+        pties = np.zeros((npairs, self.cap), dtype=np.uint32)
+        res = np.zeros(n, dtype=RESULT_DTYPE)
+        ties = np.zeros((n, self.cap), dtype=np.uint32)
+        ads = np.zeros(n, dtype=np.uint32)
+        rows = (np.zeros((2 * n, len(self.panel)), dtype=np.int32)
+                if batch.flags & FULL_ROWS else None)
+        _check(self._lib, self._lib.esg_finish_pairs(
+            self._h, batch._h, pairs.ctypes.data, _ptr(pties, C.c_uint32), res.ctypes.data,
+            _ptr(ties, C.c_uint32), _ptr(ads, C.c_uint32),
+            _ptr(rows, C.c_int32) if rows is not None else None))
+        stats = batch.stats()
+        if not keep:
+            batch.free()
+        mates = BatchResult(res, ties, rows, len(self.panel), stats, self.cap)
+        return PairBatchResult(pairs, pties, mates, ads, stats, self.cap)
+
+    def score_pairs(self, mates, adapters=None, min_score: int = 0, both_strands: bool = True,
+                    full_rows: bool = False) -> PairBatchResult:
+        """prepare_pairs + submit + finish_pairs."""
+        return self.finish_pairs(self.submit(self.prepare_pairs(
+            mates, adapters, min_score, both_strands, full_rows)))
 
 
 def select_hits(scores: ReadScores, min_score: int = 0, max_ties: int | None = None):

@@ -25,8 +25,7 @@ from __future__ import annotations
 
 import numpy as np
 
-TRUSEQ_R1 = b"AGATCGGAAGAGCACACGTCTGAACTCCAGTCA"  # crates/eschalign/src/adapter.rs:40
-TRUSEQ_R2 = b"AGATCGGAAGAGCGTCGTGTAGGGAAAGAGTGT"  # adapter.rs:42
+from .adapter import TRUSEQ_R1, TRUSEQ_R2
 
 SEED_PANEL = 0x5EED_C1C2
 SEED_C1 = 0x5EED_0C01
@@ -217,3 +216,82 @@ def reads_c3(refs, n=200_000, seed=SEED_C3):
     rng = np.random.default_rng(seed)
     lens = rng.integers(50, 1001, n)
     return mixed_reads(rng, refs, lens, 0.7, 0.10, 0.015, 0.015)
+
+
+def _seg_revcomp(codes, off, lens):
+    """Reverse-complement every segment of a concatenation (wildcard stays)."""
+    lens = np.asarray(lens, dtype=np.int64)
+    off = np.asarray(off, dtype=np.int64)
+    k = np.arange(int(lens.sum()), dtype=np.int64) - np.repeat(np.cumsum(lens) - lens, lens)
+    src = np.repeat(off + lens - 1, lens) - k
+    c = codes[src]
+    return np.where(c == 4, 4, 3 - c).astype(np.uint8)
+
+
+def _fix_length(rng, codes, lens, target):
+    """Cut or pad (random bases) each segment to `target` bases."""
+    lens = np.asarray(lens, dtype=np.int64)
+    n = lens.size
+    take = np.minimum(lens, target)
+    out = random_bases(rng, n * target)
+    o_off = np.arange(n, dtype=np.int64) * target
+    out[_ranges(o_off, take)] = codes[_ranges(np.cumsum(lens) - lens, take)]
+    return out
+
+
+def pairs_c4(refs, n=2_000_000, seed=SEED_C4, read_len=150, median=90, sigma=0.5,
+             insert_lo=40, insert_hi=600, p_adapter=0.01, p_sub=0.01, p_ins=0.001,
+             p_del=0.001):
+    """Read pairs of 2 x read_len: a fragment (the insert, lognormal around
+    `median`, clipped to [insert_lo, insert_hi]) from a random reference on
+    a random template strand; mate 1 reads the fragment from its 5' end,
+    mate 2 its reverse complement.  A mate longer than the insert reads on
+    into its adapter (TRUSEQ_R1 / _R2 with p_adapter substitutions, random
+    bases past the adapter's end).  A fragment longer than its reference
+    gets random flanks.  Each mate then takes p_sub substitutions and
+    p_ins + p_del indels and is cut or padded back to read_len.  Returns a
+    Packed of 2n reads, mate 1 of pair p at 2p, mate 2 at 2p + 1, and the
+    inserts."""
+    from .alphabet import encode
+
+    rng = np.random.default_rng(seed)
+    ref_lens = np.array([r.size for r in refs], dtype=np.int64)
+    ref_off = _offsets(ref_lens).astype(np.int64)
+    cat = np.concatenate(refs)
+    which = rng.integers(0, len(refs), n)
+    rev = rng.random(n) < 0.5
+    ins = lognormal_lengths(rng, n, median, sigma, insert_lo, insert_hi)
+    rl = ref_lens[which]
+    # fragment: a window of the reference, or the reference inside random flanks
+    span = np.minimum(ins, rl)
+    s_ref = rng.integers(0, np.maximum(rl - ins, 0) + 1)
+    s_dst = rng.integers(0, np.maximum(ins - rl, 0) + 1)
+    frag_off = _offsets(ins).astype(np.int64)
+    frag = random_bases(rng, int(ins.sum()))
+    frag[_ranges(frag_off + s_dst, span)] = cat[_ranges(ref_off[which] + s_ref, span)]
+    # template strand
+    if rev.any():
+        idx = np.nonzero(rev)[0]
+        sel = _ranges(frag_off[idx], ins[idx])
+        frag[sel] = _seg_revcomp(frag, frag_off[idx], ins[idx])
+    frag_rc = _seg_revcomp(frag, frag_off, ins)
+    mates = []
+    for src, adapter in ((frag, TRUSEQ_R1), (frag_rc, TRUSEQ_R2)):
+        m = random_bases(rng, n * read_len)
+        m_off = np.arange(n, dtype=np.int64) * read_len
+        body = np.minimum(ins, read_len)
+        m[_ranges(m_off, body)] = src[_ranges(frag_off, body)]
+        ad = encode(adapter)
+        short = np.nonzero(ins < read_len)[0]
+        if short.size:
+            k = np.minimum(read_len - ins[short], ad.size)
+            pos = _ranges(m_off[short] + ins[short], k)
+            a = ad[_ranges(np.zeros(short.size, dtype=np.int64), k)].copy()
+            err = rng.random(a.size) < p_adapter
+            a[err] = (a[err] + rng.integers(1, 4, int(err.sum()))) % 4
+            m[pos] = a
+        mc, ml = mutate(rng, m, np.full(n, read_len, dtype=np.int64), p_sub, p_ins, p_del)
+        mates.append(_fix_length(rng, mc, ml, read_len).reshape(n, read_len))
+    codes = np.stack(mates, axis=1).reshape(-1)
+    lens = np.full(2 * n, read_len, dtype=np.uint32)
+    return Packed(codes, _offsets(lens), lens), ins

@@ -129,6 +129,9 @@ typedef struct esg_batch_stats {
     uint64_t cells;             /* sum over scored queries of len * panel bases        */
     uint64_t h2d_bytes;
     uint64_t d2h_bytes;
+    uint32_t n_pairs;           /* paired batches: read pairs (n_reads / 2)           */
+    uint32_t mates_trimmed;     /* mates with an adapter found                         */
+    uint64_t bases_trimmed;     /* adapter bases removed                               */
 } esg_batch_stats;
 
 typedef struct esg_scorer esg_scorer;
@@ -179,7 +182,8 @@ int32_t esg_scores_len(const esg_scorer* scorer, uint64_t len);
  * read are valid, n_listed = min(n_tied, tie_capacity)).  With
  * ESG_FULL_ROWS, `rows` gets every query's scores in panel order, forward
  * rows 0..n_reads-1 then (ESG_BOTH_STRANDS) reverse rows n_reads..2n-1 --
- * the reference's batch layout (align.rs:1484-1494). */
+ * the reference's batch layout (align.rs:1484-1494); an empty read's rows
+ * are 0, the score of an empty query (scalar.rs:120-163). */
 esg_status esg_score_batch(esg_scorer* scorer, const uint8_t* codes, const uint64_t* off,
                            const uint32_t* len, uint32_t n_reads, uint32_t flags,
                            esg_read_result* results, uint32_t* ties, int32_t* rows);
@@ -204,6 +208,79 @@ esg_status esg_batch_stats_get(const esg_batch* batch, esg_batch_stats* out);
  * scorer's) with its inputs already resident, no copies.  For measuring the
  * kernels alone; the batch's results are overwritten with identical ones. */
 esg_status esg_relaunch(esg_scorer* scorer, esg_batch* batch, void* stream);
+
+/* ---- paired-end: the scored half of Aligner::map_pairs_scored
+ * (crates/eschalign/src/mapper/pair.rs:157-234) fed the way the CLI's GPU
+ * thread feeds it (crates/eschalign-cli/src/align.rs:2844-2872): mates
+ * trimmed of their 3' adapter (adapter.rs:68-110, align.rs:934-949), each
+ * mate scored as sequenced and reverse-complemented, and the candidates
+ * (reference, template strand) ranked on the device. */
+
+/* AdapterConfig (adapter.rs:46-54) plus the CLI's --max-read-len.  Adapters
+ * are codes (alphabet.rs); r1_len = r2_len = 0 trims nothing. */
+typedef struct esg_adapter_config {
+    const uint8_t* r1;     /* adapter prefix on mate 1's 3' end (TRUSEQ_R1, adapter.rs:40) */
+    uint32_t r1_len;
+    const uint8_t* r2;     /* on mate 2's (TRUSEQ_R2, adapter.rs:42)                        */
+    uint32_t r2_len;
+    uint32_t min_overlap;  /* DEFAULT_MIN_OVERLAP = 5 (adapter.rs:44); 0 counts as 1       */
+    uint32_t max_read_len; /* a longer mate is not aligned nor searched; 0 = no limit      */
+} esg_adapter_config;
+
+/* pair_adapters (crates/eschalign-cli/src/align.rs:934-949) over a batch,
+ * host only (no device needed): mates 2p and 2p + 1; adapter_bases[2n] gets
+ * each mate's adapter bases, aligned_len[2n] the bases left to align (0 for
+ * a mate over max_read_len, align.rs:2851-2853).  esg_prepare_pairs trims
+ * with this same code. */
+esg_status esg_pair_adapters(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
+                             uint32_t n_pairs, const esg_adapter_config* adapters,
+                             uint32_t* adapter_bases, uint32_t* aligned_len);
+
+/* One pair's ranked candidates (pair.rs:195-234).  Candidate (r, t): t = 0
+ * mate 1 as sequenced + mate 2 reverse-complemented, t = 1 the opposite;
+ * eligible when both mate scores are >= min_score; ranked by (-sum, r, t).
+ * The first tier is the tie set the reference traces first; `next` lets it
+ * fall through without rescoring.  `xs` is PairMapping::Proper's per-mate
+ * suboptimal (pair.rs:297-314) for a pair whose whole first tier passes the
+ * pair constraints.  No eligible candidate (or an empty mate):
+ * ESG_RESULT_EMPTY, and the per-mate read results are the Separate fallback
+ * (pair.rs:366-387). */
+typedef struct esg_pair_result {
+    int32_t best;       /* first tier's summed score; ESG_NO_SCORE if no candidate */
+    int32_t next;       /* the next tier's sum; ESG_NO_SCORE if none                */
+    uint32_t n_tied;    /* candidates in the first tier, counted in full            */
+    uint32_t flags;     /* ESG_RESULT_EMPTY / _TIES_TRUNCATED / _RESCORED32         */
+    int32_t xs[2];      /* per mate: best score over candidates outside the tier   */
+    int32_t primary[2]; /* the first tie's two mate scores                          */
+} esg_pair_result;
+
+/* Pair flag for esg_prepare_pairs: ESG_BOTH_STRANDS ranks both template
+ * strands (PairOptions::both_strands, pair.rs:52); ESG_FULL_ROWS returns the
+ * four rows per pair. */
+/* Plan a paired batch: mates are reads 2p (mate 1) and 2p + 1 (mate 2) of
+ * codes/off/len (as sequenced).  Trims them (host threads) per `adapters`
+ * (NULL: no trimming), then plans every mate on both strands.  Submit and
+ * relaunch as any batch. */
+esg_status esg_prepare_pairs(esg_scorer* scorer, const uint8_t* codes, const uint64_t* off,
+                             const uint32_t* len, uint32_t n_pairs,
+                             const esg_adapter_config* adapters, int32_t min_score,
+                             uint32_t flags, esg_batch** out);
+/* Wait for a paired batch and copy out (any pointer may be NULL):
+ *   pairs[n_pairs], pair_ties[n_pairs * tie_capacity] as (ref << 1) | t;
+ *   mates[2 n_pairs], mate_ties[2 n_pairs * tie_capacity]: each mate alone on
+ *     both strands, as map_reads_scored ranks it (mapper.rs:444-472);
+ *   adapters[2 n_pairs]: adapter bases removed from each mate;
+ *   rows[4 n_pairs * n_refs] (ESG_FULL_ROWS): forward rows of the 2 n_pairs
+ *     mates, then their reverse-complement rows. */
+esg_status esg_finish_pairs(esg_scorer* scorer, esg_batch* batch, esg_pair_result* pairs,
+                            uint32_t* pair_ties, esg_read_result* mates, uint32_t* mate_ties,
+                            uint32_t* adapters, int32_t* rows);
+/* prepare_pairs + submit + finish_pairs. */
+esg_status esg_score_pairs(esg_scorer* scorer, const uint8_t* codes, const uint64_t* off,
+                           const uint32_t* len, uint32_t n_pairs,
+                           const esg_adapter_config* adapters, int32_t min_score, uint32_t flags,
+                           esg_pair_result* pairs, uint32_t* pair_ties, esg_read_result* mates,
+                           uint32_t* mate_ties, uint32_t* adapter_bases, int32_t* rows);
 
 /* Scoring for callers that cannot allocate.  No counterpart in the reference.
  *

@@ -111,6 +111,46 @@ int eo_scalar_map_batch(const uint8_t* codes, const uint64_t* off, const uint32_
                         int32_t o, int32_t e, int both_strands, int local, int threads,
                         uint32_t cap, eo_result* results, uint32_t* ties, int32_t* rows);
 
+/* ---- paired-end (adapter.rs, mapper/pair.rs) --------------------------- */
+/* adapter.rs:68-91 on codes: adapter bases at the 3' end of `read` (0 = none). */
+size_t eo_adapter_find(const uint8_t* read, size_t n, const uint8_t* adapter, size_t a,
+                       size_t min_overlap);
+/* adapter.rs:95-110: out = {ad1, ad2}, the two mates' insert ends reconciled. */
+void eo_adapter_detect_pair(const uint8_t* r1, size_t l1, const uint8_t* r2, size_t l2,
+                            const uint8_t* a1, size_t al1, const uint8_t* a2, size_t al2,
+                            size_t min_overlap, size_t out[2]);
+/* align.rs:934-949 (pair_adapters), with the over-length rule. */
+void eo_pair_adapters(const uint8_t* r1, size_t l1, const uint8_t* r2, size_t l2,
+                      const uint8_t* a1, size_t al1, const uint8_t* a2, size_t al2,
+                      size_t min_overlap, size_t max_read_len, size_t out[2]);
+
+/* Same layout as the product's esg_pair_result. */
+typedef struct eo_pair_result {
+    int32_t best;       /* best summed mate score; INT32_MIN if no candidate   */
+    int32_t next;       /* the next tier's sum; INT32_MIN if none               */
+    uint32_t n_tied;    /* candidates in the first tier                         */
+    uint32_t flags;     /* EO_RESULT_EMPTY: no eligible candidate; TRUNCATED    */
+    int32_t xs[2];      /* per mate: best over candidates outside the tier     */
+    int32_t primary[2]; /* the first tie's mate scores                          */
+} eo_pair_result;
+
+/* pair.rs:195-234 and :297-314.  f0/r0: mate 1 forward / reverse-complement
+ * row, f1/r1 mate 2's.  Ties as (ref << 1) | template_reverse. */
+void eo_pair_select(const int32_t* f0, const int32_t* r0, const int32_t* f1, const int32_t* r1,
+                    uint32_t n_refs, int both_strands, int32_t min_score, uint32_t cap,
+                    eo_pair_result* out, uint32_t* ties);
+/* The ranking over rows in the CUDA path's layout (forward rows of the
+ * 2 n_pairs mates, then their reverse-complement rows); len = mate lengths. */
+void eo_pairs_from_rows(const int32_t* rows, const uint32_t* len, uint32_t n_pairs,
+                        uint32_t n_refs, int both_strands, int32_t min_score, uint32_t cap,
+                        eo_pair_result* results, uint32_t* ties);
+/* Pairs end to end with the scalar oracle; mates 2 per pair, already trimmed. */
+int eo_scalar_map_pairs(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
+                        uint32_t n_pairs, const uint8_t* ref_codes, const uint64_t* ref_off,
+                        const uint32_t* ref_len, uint32_t n_refs, int32_t ma, int32_t mi,
+                        int32_t o, int32_t e, int both_strands, int local, int32_t min_score,
+                        int threads, uint32_t cap, eo_pair_result* results, uint32_t* ties);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,6 +32,8 @@ class EoResult(C.Structure):
 
 RESULT_DTYPE = np.dtype([("best", "<i4"), ("suboptimal", "<i4"),
                          ("n_tied", "<u4"), ("flags", "<u4")])
+PAIR_DTYPE = np.dtype([("best", "<i4"), ("next", "<i4"), ("n_tied", "<u4"), ("flags", "<u4"),
+                       ("xs", "<i4", (2,)), ("primary", "<i4", (2,))])
 
 
 def build() -> str:
@@ -79,6 +81,27 @@ def lib():
         L.eo_cpu_has_avx512bw.restype = C.c_int
         L.eo_profile_score_all.restype = None
         L.eo_profile_score_all.argtypes = [C.c_void_p, u8p, C.c_size_t, C.c_int, C.c_int, i32p]
+        L.eo_adapter_find.restype = C.c_size_t
+        L.eo_adapter_find.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, C.c_size_t]
+        L.eo_adapter_detect_pair.restype = None
+        L.eo_adapter_detect_pair.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, u8p, C.c_size_t,
+                                             u8p, C.c_size_t, C.c_size_t,
+                                             C.POINTER(C.c_size_t)]
+        L.eo_pair_adapters.restype = None
+        L.eo_pair_adapters.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, u8p, C.c_size_t,
+                                       u8p, C.c_size_t, C.c_size_t, C.c_size_t,
+                                       C.POINTER(C.c_size_t)]
+        L.eo_pair_select.restype = None
+        L.eo_pair_select.argtypes = [i32p, i32p, i32p, i32p, C.c_uint32, C.c_int, C.c_int32,
+                                     C.c_uint32, C.c_void_p, u32p]
+        L.eo_pairs_from_rows.restype = None
+        L.eo_pairs_from_rows.argtypes = [i32p, u32p, C.c_uint32, C.c_uint32, C.c_int, C.c_int32,
+                                         C.c_uint32, C.c_void_p, u32p]
+        L.eo_scalar_map_pairs.restype = C.c_int
+        L.eo_scalar_map_pairs.argtypes = [u8p, u64p, u32p, C.c_uint32, u8p, u64p, u32p,
+                                          C.c_uint32, C.c_int32, C.c_int32, C.c_int32,
+                                          C.c_int32, C.c_int, C.c_int, C.c_int32, C.c_int,
+                                          C.c_uint32, C.c_void_p, u32p]
         L.eo_cpu_map_batch.restype = C.c_int
         L.eo_cpu_map_batch.argtypes = [C.c_void_p, u8p, u64p, u32p, C.c_uint32, C.c_int, C.c_int,
                                        C.c_int, C.c_uint32, C.c_void_p, u32p, i32p]
@@ -217,3 +240,95 @@ class Profile:
                                       _p(ties, C.c_uint32),
                                       _p(out_rows, C.c_int32) if rows else None)
         return res, ties, out_rows, used
+
+
+TRUSEQ_R1 = b"AGATCGGAAGAGCACACGTCTGAACTCCAGTCA"  # adapter.rs:40
+TRUSEQ_R2 = b"AGATCGGAAGAGCGTCGTGTAGGGAAAGAGTGT"  # adapter.rs:42
+
+
+def _codes(x) -> np.ndarray:
+    """Letters (bytes/str) or codes (uint8 array) -> contiguous codes."""
+    if isinstance(x, np.ndarray):
+        return np.ascontiguousarray(x, dtype=np.uint8)
+    return np.ascontiguousarray(encode(x) if len(x) else np.zeros(0, np.uint8))
+
+
+def adapter_find(read, adapter=TRUSEQ_R1, min_overlap=5) -> int:
+    """adapter.rs:68-91 (letters or codes)."""
+    q, a = _codes(read), _codes(adapter)
+    return int(lib().eo_adapter_find(_p(q, C.c_uint8), q.size, _p(a, C.c_uint8), a.size,
+                                     min_overlap))
+
+
+def adapter_detect_pair(r1, r2, a1=TRUSEQ_R1, a2=TRUSEQ_R2, min_overlap=5):
+    """adapter.rs:95-110 (letters or codes)."""
+    q1, q2, x1, x2 = _codes(r1), _codes(r2), _codes(a1), _codes(a2)
+    out = (C.c_size_t * 2)()
+    lib().eo_adapter_detect_pair(_p(q1, C.c_uint8), q1.size, _p(q2, C.c_uint8), q2.size,
+                                 _p(x1, C.c_uint8), x1.size, _p(x2, C.c_uint8), x2.size,
+                                 min_overlap, out)
+    return [int(out[0]), int(out[1])]
+
+
+def pair_adapters(r1, r2, a1=TRUSEQ_R1, a2=TRUSEQ_R2, min_overlap=5, max_read_len=0):
+    """crates/eschalign-cli/src/align.rs:934-949 (letters or codes)."""
+    q1, q2, x1, x2 = _codes(r1), _codes(r2), _codes(a1), _codes(a2)
+    out = (C.c_size_t * 2)()
+    lib().eo_pair_adapters(_p(q1, C.c_uint8), q1.size, _p(q2, C.c_uint8), q2.size,
+                           _p(x1, C.c_uint8), x1.size, _p(x2, C.c_uint8), x2.size,
+                           min_overlap, max_read_len, out)
+    return [int(out[0]), int(out[1])]
+
+
+def trim_pairs(mates, a1=TRUSEQ_R1, a2=TRUSEQ_R2, min_overlap=5, max_read_len=0):
+    """The aligned bases of each mate (align.rs:2844-2863): mate less its 3'
+    adapter, empty when over max_read_len.  Returns (trimmed mates, adapters)."""
+    out, ads = [], []
+    for p in range(len(mates) // 2):
+        m1, m2 = _codes(mates[2 * p]), _codes(mates[2 * p + 1])
+        ad = pair_adapters(m1, m2, a1, a2, min_overlap, max_read_len)
+        for m, a in ((m1, ad[0]), (m2, ad[1])):
+            if max_read_len and m.size > max_read_len:
+                out.append(np.zeros(0, np.uint8))
+            else:
+                out.append(m[:m.size - a])
+        ads.extend(ad)
+    return out, np.array(ads, dtype=np.uint32)
+
+
+def pair_select(f0, r0, f1, r1, both_strands=True, min_score=0, cap=8):
+    """pair.rs:195-234, :297-314 on one pair's four rows."""
+    rows = [np.ascontiguousarray(x, dtype=np.int32) for x in (f0, r0, f1, r1)]
+    res = np.zeros(1, dtype=PAIR_DTYPE)
+    ties = np.zeros(max(cap, 1), dtype=np.uint32)
+    lib().eo_pair_select(*[_p(x, C.c_int32) for x in rows], rows[0].size, int(bool(both_strands)),
+                         min_score, cap, res.ctypes.data, _p(ties, C.c_uint32))
+    return res[0], ties[:min(int(res[0]["n_tied"]), cap)].tolist()
+
+
+def pairs_from_rows(rows, lens, n_refs, both_strands=True, min_score=0, cap=8):
+    """The ranking over rows laid out as the CUDA path returns them
+    (forward rows of the 2n mates, then reverse-complement rows)."""
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    lens = np.ascontiguousarray(lens, dtype=np.uint32)
+    n = lens.size // 2
+    res = np.zeros(n, dtype=PAIR_DTYPE)
+    ties = np.zeros((n, max(cap, 1)), dtype=np.uint32)
+    lib().eo_pairs_from_rows(_p(rows, C.c_int32), _p(lens, C.c_uint32), n, n_refs,
+                             int(bool(both_strands)), min_score, cap, res.ctypes.data,
+                             _p(ties, C.c_uint32))
+    return res, ties
+
+
+def scalar_map_pairs(mates, refs, scoring, local, both_strands, min_score=0, cap=8, threads=0):
+    """Pairs (mate codes, 2 per pair, trimmed) end to end with the scalar oracle."""
+    qc, qo, ql = pack(mates)
+    rc, ro, rl = pack(refs)
+    n = len(mates) // 2
+    res = np.zeros(n, dtype=PAIR_DTYPE)
+    ties = np.zeros((n, max(cap, 1)), dtype=np.uint32)
+    lib().eo_scalar_map_pairs(_p(qc, C.c_uint8), _p(qo, C.c_uint64), _p(ql, C.c_uint32), n,
+                              _p(rc, C.c_uint8), _p(ro, C.c_uint64), _p(rl, C.c_uint32), len(refs),
+                              *scoring, int(bool(both_strands)), int(bool(local)), min_score,
+                              threads, cap, res.ctypes.data, _p(ties, C.c_uint32))
+    return res, ties

@@ -13,12 +13,18 @@ It reads, as data:
   ``tests/parasail_golden.rs:48-77``;
 * ``crates/eschalign-cli/tests/fixtures/trna_reference.fa`` and
   ``trna_reference_ambiguous.fa`` -- the 47-reference tRNA panels the
-  reference's ``tests/gpu_parity.rs:249-260`` scores the fixture reads against.
+  reference's ``tests/gpu_parity.rs:249-260`` scores the fixture reads against;
+* ``crates/eschalign-cli/tests/fixtures/pairs/pairs_panel.fa``,
+  ``pairs_R1.fq`` and ``pairs_R2.fq`` -- the 4-reference paired-end fixture
+  (``gen_pair_fixture.py``, seed 20261004) the reference's
+  ``tests/align_paired.rs`` aligns.
 
 and writes the subset this project tests against into ``tests/golden/``:
 ``align_golden_scores.json`` (query, reference, mode, scheme, score and the
-parasail end coordinates) and the two panels as ``panel_trna*.json``
-(name + letters, file order).  Nothing else from the reference is copied.
+parasail end coordinates), the two panels as ``panel_trna*.json`` (name +
+letters, file order) and the paired fixture as ``pairs_fixture.json`` (panel
+and each pair's name and mate letters).  Nothing else from the reference is
+copied.
 """
 import json
 import os
@@ -77,7 +83,20 @@ def main(ref_root):
         with open(os.path.join(here, tag), "w") as fh:
             json.dump({"source": fa, "references": [{"name": n, "seq": s} for n, s in recs]},
                       fh, indent=0)
-    print(f"{len(cases)} golden scores, {len(out['fixture_reads'])} fixture reads")
+    pdir = os.path.join(ref_root, "crates/eschalign-cli/tests/fixtures/pairs")
+    mates = []
+    for fq in ("pairs_R1.fq", "pairs_R2.fq"):
+        with open(os.path.join(pdir, fq)) as fh:
+            lines = fh.read().splitlines()
+        mates.append([(lines[i][1:], lines[i + 1]) for i in range(0, len(lines), 4)])
+    pairs = [{"name": a[0], "r1": a[1], "r2": b[1]} for a, b in zip(*mates)]
+    panel = read_fasta(os.path.join(pdir, "pairs_panel.fa"))
+    with open(os.path.join(here, "pairs_fixture.json"), "w") as fh:
+        json.dump({"source": "pairs/pairs_panel.fa, pairs_R1.fq, pairs_R2.fq",
+                   "references": [{"name": n, "seq": s} for n, s in panel],
+                   "pairs": pairs}, fh, indent=0)
+    print(f"{len(cases)} golden scores, {len(out['fixture_reads'])} fixture reads, "
+          f"{len(pairs)} fixture pairs")
 
 
 if __name__ == "__main__":

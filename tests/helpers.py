@@ -95,3 +95,39 @@ def fixture_reads():
 def revcomp(c):
     c = np.asarray(c, dtype=np.uint8)[::-1]
     return np.where(c >= 4, 4, 3 - c).astype(np.uint8)
+
+
+def pairs_fixture():
+    """The reference's paired fixture (crates/eschalign-cli/tests/fixtures/pairs,
+    via tests/golden/make_golden.py): reference names, reference codes, and
+    {pair name: (mate 1 codes, mate 2 codes)} in file order."""
+    with open(os.path.join(GOLDEN, "pairs_fixture.json")) as fh:
+        d = json.load(fh)
+    names = [r["name"] for r in d["references"]]
+    refs = [encode(r["seq"]) for r in d["references"]]
+    pairs = {p["name"]: (encode(p["r1"]), encode(p["r2"])) for p in d["pairs"]}
+    return names, refs, pairs
+
+
+def brute_pair_select(f0, r0, f1, r1, both, min_score, cap):
+    """pair.rs:195-234 spelled out: every candidate, sorted by (-sum, r, t)."""
+    cands = []
+    for r in range(len(f0)):
+        for t in ((0, 1) if both else (0,)):
+            a, b = (int(r0[r]), int(f1[r])) if t else (int(f0[r]), int(r1[r]))
+            cands.append((a, b, r, t))
+    elig = sorted([c for c in cands if c[0] >= min_score and c[1] >= min_score],
+                  key=lambda c: (-(c[0] + c[1]), c[2], c[3]))
+    if not elig:
+        best = None
+        tier = []
+    else:
+        best = elig[0][0] + elig[0][1]
+        tier = [c for c in elig if c[0] + c[1] == best]
+    rest = [c for c in elig if c[0] + c[1] != best]
+    nxt = rest[0][0] + rest[0][1] if rest else None
+    in_tier = {(c[2], c[3]) for c in tier}
+    outside = [c for c in cands if (c[2], c[3]) not in in_tier]
+    xs = (max((c[0] for c in outside), default=None), max((c[1] for c in outside), default=None))
+    prim = (tier[0][0], tier[0][1]) if tier else (None, None)
+    return best, nxt, len(tier), [(c[2] << 1) | c[3] for c in tier[:cap]], xs, prim

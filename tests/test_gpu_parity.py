@@ -181,6 +181,7 @@ def test_gpu_scores_everything_it_is_given(oracle):
     with GpuScorer(panel, Scoring(), Mode.LOCAL) as g:
         res = g.score_batch(reads, full_rows=True)
         assert res.read(1).best is None and res.results["flags"][1] & 1
+        assert not res.rows[1].any()  # an empty query scores 0 against everything
         for k in (0, 2, 3, 4):
             for r, ref in enumerate(panel):
                 assert res.rows[k, r] == oracle.score(reads[k], ref, (2, -1, -10, -1), True)
