@@ -25,6 +25,20 @@ other three (mode, scheme) combinations are measured once each.
             run.
 * --impl reference  the reference's CPU path (AVX-512BW score kernels +
             selection, restated in oracle/) on all host cores.
+
+Other workloads (``--workload``), one JSON line each, same keys:
+
+* c4  2 000 000 read pairs of 2 x 150 nt (inserts lognormal, median 90 nt,
+      40-600; adapter read-through past short inserts, 1 % errors; 1 % subs,
+      0.2 % indels) on the 164-reference panel, semi-global 2,-1,-10,-1:
+      each mate trimmed of its adapter on the host (the reference's rule),
+      all four mate queries scored, the (reference, template strand)
+      candidates of both template strands ranked on the device; GCUPS and
+      pairs/s.  CPU arm: trimming + AVX-512BW rows + the same ranking.
+* c3  the uneven panel: 10 000 references of 300-1000 nt, reads of
+      50-1000 nt (70 % derived, 10 % subs, 3 % indels), local, both
+      strands, autotuned tile shape; a bounded read sample per step (the
+      full 200 000 reads are about 1.4e15 cells).
 """
 from __future__ import annotations
 
@@ -46,6 +60,8 @@ HEADLINE = ((2, -1, -10, -1), "local")
 COMBOS = [((2, -1, -10, -1), "local"), ((2, -1, -10, -1), "semiglobal"),
           ((1, -1, -2, -1), "local"), ((1, -1, -2, -1), "semiglobal")]
 OPS_PER_CELL = {"local": 12, "semiglobal": 11}
+C4_SCORING = (2, -1, -10, -1)
+C3_SCORING = (2, -1, -10, -1)
 # DRAM bytes per DP cell of the batched kernel: 3.22 MB over 9.71e10 cells in
 # the ncu capture of a 20 000-read C2 launch (profiles/k2_batched_c2.md);
 # traffic grows with the reads, so it scales by cells to the full launch.
@@ -75,6 +91,11 @@ def args_parse():
                     help="score READS reads of the workload once per kernel and exit "
                          "(a small target for ncu)")
     ap.add_argument("--mode", default="local", choices=["local", "semiglobal"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"])
+    ap.add_argument("--pairs", type=int, default=2_000_000, help="c4: read pairs")
+    ap.add_argument("--pair-chunk", type=int, default=125_000,
+                    help="c4: pairs per prepare/submit/finish batch in the e2e feeder")
+    ap.add_argument("--c3-reads", type=int, default=4000, help="c3: reads per step")
     return ap.parse_args()
 
 
@@ -160,30 +181,73 @@ def int_peak(device):
     return {"peak_lane_ops_per_s": peak, "ops": ops, "sms": sms.value}
 
 
-def cpu_baseline(refs, reads, scoring, mode, seconds, threads=0):
+def roofline_of(peak, per_gpu_cells_s, mode, traffic):
+    achieved = per_gpu_cells_s * OPS_PER_CELL[mode] / 2.0
+    return {"bound": "int_alu", "achieved": achieved / 1e12,
+            "peak": (peak["peak_lane_ops_per_s"] / 1e12) if peak else None,
+            "unit": "T lane-ops/s",
+            "frac": (achieved / peak["peak_lane_ops_per_s"]) if peak else None,
+            "traffic": traffic, "kernel": "k2_batched",
+            "note": f"achieved = cells/s x {OPS_PER_CELL[mode]} int ops / 2 cells per "
+                    "int16x2 lane-op; peak = measured iadd32/imax32 lane-op rate "
+                    "(csrc/esg_probe.cu), measured in this run"}
+
+
+def cpu_baseline(refs, reads, scoring, mode, seconds, threads=0, chunk=64):
     """The reference's CPU path (AVX-512BW kernels + selection, restated in
-    oracle/) on a bounded sample of the workload, all host threads."""
+    oracle/) on a bounded sample of the workload, all host threads; `chunk`
+    reads per work unit (the reference's 64; fewer for a small sample of
+    long reads, so every core has work)."""
     from oracle import oracle as O
     O.build()
+    O.lib().eo_cpu_set_chunk(chunk)
     prof = O.Profile(refs, scoring)
     panel_bases = sum(len(r) for r in refs)
     local = mode == "local"
-    n_cal = min(len(reads), 2000)
-    cal = reads.subset(np.arange(n_cal))
+    # calibrate on about 1e11 cells (a second or so), at least 16 reads
+    cells_per_read = 2 * panel_bases * reads.bases() / max(1, len(reads))
+    n_cal = int(min(len(reads), 2000, max(16, 1e11 / max(cells_per_read, 1.0))))
+    cal = reads.slice(0, n_cal)
     t = time.perf_counter()
     _, _, _, used = prof.map_batch(*cal.tuple(), local=local, both_strands=True, threads=threads)
     dt = time.perf_counter() - t
     n = int(min(len(reads), max(n_cal, n_cal * seconds / max(dt, 1e-3))))
-    sample = reads.subset(np.arange(n))
+    sample = reads.slice(0, n)
     t = time.perf_counter()
     _, _, _, used = prof.map_batch(*sample.tuple(), local=local, both_strands=True,
                                    threads=threads)
     dt = time.perf_counter() - t
     cells = 2 * sample.bases() * panel_bases
+    O.lib().eo_cpu_set_chunk(64)
     return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": int(used), "kind": "port",
             "sample": f"first {n} of {len(reads)} reads, both strands, {mode} "
-                      f"{','.join(map(str, scoring))}; {dt:.1f} s; reads/s {n / dt:.0f}",
+                      f"{','.join(map(str, scoring))}; {dt:.1f} s; reads/s {n / dt:.0f}; "
+                      f"{chunk} reads per work unit",
             "reads_per_s": n / dt, "seconds": dt}
+
+
+def cpu_pairs_baseline(refs, pairs, scoring, seconds, threads=0):
+    """The reference's CPU path for pairs (trimming, AVX-512BW rows, ranking;
+    oracle/esg_cpu_avx512.c eo_cpu_map_pairs) on a bounded sample."""
+    from oracle import oracle as O
+    O.build()
+    prof = O.Profile(refs, scoring)
+    panel_bases = sum(len(r) for r in refs)
+    n_all = len(pairs) // 2
+    n_cal = min(n_all, 1000)
+    t = time.perf_counter()
+    prof.map_pairs(*pairs.slice(0, 2 * n_cal).tuple(), local=False, threads=threads)
+    dt = time.perf_counter() - t
+    n = int(min(n_all, max(n_cal, n_cal * seconds / max(dt, 1e-3))))
+    sample = pairs.slice(0, 2 * n)
+    t = time.perf_counter()
+    _, _, _, _, ads, used = prof.map_pairs(*sample.tuple(), local=False, threads=threads)
+    dt = time.perf_counter() - t
+    cells = 2 * (sample.bases() - int(ads.sum(dtype=np.uint64))) * panel_bases
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": int(used), "kind": "port",
+            "sample": f"first {n} of {n_all} pairs: trim, 4 mate rows, both template strands "
+                      f"ranked, semiglobal {','.join(map(str, scoring))}; {dt:.1f} s",
+            "pairs_per_s": n / dt, "seconds": dt}
 
 
 def run_reference(a, rank, world):
@@ -191,29 +255,352 @@ def run_reference(a, rank, world):
     if rank != 0:
         return
     from eschalign_b200 import synth
-    refs = synth.panel_tiles()
-    reads = synth.reads_c2(refs, n=a.reads)
-    scoring, mode = HEADLINE
     per_step = max(2.0, min(a.cpu_seconds, 120.0 / max(1, a.steps + a.warmup)))
+    extra = {}
+    if a.workload == "c4":
+        refs = synth.panel_tiles()
+        data = synth.pairs_c4(refs, n=a.pairs)[0]
+        fn = lambda s: cpu_pairs_baseline(refs, data, C4_SCORING, s)  # noqa: E731
+        warm = lambda: cpu_pairs_baseline(refs, data.slice(0, 2000), C4_SCORING, 0.5)  # noqa: E731
+        workload = (f"C4 {a.pairs} pairs 2x150 x 164-ref panel, semiglobal 2,-1,-10,-1, "
+                    "adapter trimming, both template strands ranked")
+        dtype = "int16"
+    elif a.workload == "c3":
+        refs = synth.panel_c3()
+        data = synth.reads_c3(refs, n=a.c3_reads)
+        fn = lambda s: cpu_baseline(refs, data, C3_SCORING, "local", s, chunk=1)  # noqa: E731
+        warm = lambda: cpu_baseline(refs, data.slice(0, 64), C3_SCORING, "local", 0.5,  # noqa: E731
+                                    chunk=1)
+        workload = "C3 10000 refs (300-1000 nt) x reads 50-1000 nt, both strands, local"
+        dtype = "int16"
+    else:
+        refs = synth.panel_tiles()
+        data = synth.reads_c2(refs, n=a.reads)
+        scoring, mode = HEADLINE
+        fn = lambda s: cpu_baseline(refs, data, scoring, mode, s)  # noqa: E731
+        warm = lambda: cpu_baseline(refs, data.slice(0, 2000), scoring, mode, 0.5)  # noqa: E731
+        workload = "C2 1M reads x 164-ref panel, both strands, local 2,-1,-10,-1"
+        dtype = "int16"
     for _ in range(a.warmup):
-        cpu_baseline(refs, reads.subset(np.arange(2000)), scoring, mode, 0.5)
+        warm()
     vals, last = [], None
     for _ in range(a.steps):
-        last = cpu_baseline(refs, reads, scoring, mode, per_step)
+        last = fn(per_step)
         vals.append(last["value"])
     v = statistics.median(vals)
-    cells_per_read = 2 * (reads.bases() / len(reads)) * sum(len(r) for r in refs)
+    if a.workload == "c4":
+        extra["pairs_per_s"] = last["pairs_per_s"] * v / last["value"]
+    elif a.workload == "c2":
+        cells_per_read = 2 * (data.bases() / len(data)) * sum(len(r) for r in refs)
+        extra["reads_per_s"] = v * 1e9 / cells_per_read
     line = {
         "impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * last["seconds"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16",
-        "data": "synthetic", "reads_per_s": v * 1e9 / cells_per_read,
-        "config": {"workload": "C2 1M reads x 164-ref panel, both strands, local 2,-1,-10,-1",
-                   "reads": a.reads, "refs": len(refs)},
-        "cpu_baseline": {**last, "value": v},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+        "data": "synthetic", **extra,
+        "config": {"workload": workload, "refs": len(refs)},
+        "cpu_baseline": {k: v2 for k, v2 in {**last, "value": v}.items()
+                         if k not in ("seconds", "reads_per_s", "pairs_per_s")},
         "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+class Ctx:
+    """Per-rank device plumbing: stream, L2 flush buffer, barrier, max over
+    ranks, and the device timer of a batch's launch sequence."""
+
+    def __init__(self, torch, dist, dev, local_rank, world):
+        self.torch, self.dist, self.dev = torch, dist, dev
+        self.local_rank, self.world = local_rank, world
+        self.stream = torch.cuda.Stream(device=dev)
+        self.flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max_over_ranks(self, x):
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def device_time(self, scorer, batch, steps, warmup, sampler=None):
+        torch, stream = self.torch, self.stream
+        for _ in range(warmup):
+            scorer.relaunch(batch, stream.cuda_stream)
+        torch.cuda.synchronize()
+        self.barrier()
+        total = 0.0
+        with (sampler if sampler is not None else _Null()):
+            for k in range(steps):
+                with torch.cuda.stream(stream):
+                    self.flush.fill_(k & 0xFF)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                scorer.relaunch(batch, stream.cuda_stream)
+                e1.record(stream)
+                e1.synchronize()
+                total += e0.elapsed_time(e1) / 1e3
+        torch.cuda.synchronize()
+        self.barrier()
+        return total
+
+
+def feeder(ctx, chunks, prepare, submit, finish, steps):
+    """Double-buffered prepare / submit / finish over host chunks (the GPU
+    feeder thread of crates/eschalign-cli/src/align.rs:2801-2917); returns
+    (seconds of the timed passes, h2d bytes, d2h bytes per pass).  The first
+    pass warms the pinned pool and the allocator and is not timed."""
+    times, h2d, d2h = [], 0, 0
+    for it in range(steps + 1):
+        ctx.barrier()
+        t0 = time.perf_counter()
+        pending = None
+        h2d = d2h = 0
+        for c in chunks + [None]:
+            prepared = prepare(c) if c is not None else None
+            if pending is not None:
+                st = finish(pending)
+                h2d += st["h2d_bytes"]
+                d2h += st["d2h_bytes"]
+            pending = submit(prepared) if prepared is not None else None
+        ctx.torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if it > 0:
+            times.append(dt)
+    return ctx.max_over_ranks(sum(times)), len(times), h2d, d2h
+
+
+def common_line(a, ctx, value, ms_per_step, workload, extra_config, e2e, roofline, clocks,
+                launches, dtype="int16x2"):
+    return {
+        "metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": ctx.world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+        "data": "synthetic",
+        "config": {"workload": workload, **extra_config, "parallelism": f"replicas x{ctx.world}",
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches,
+    }
+
+
+# ---------------------------------------------------------------- C2
+def run_c2(a, ctx, rank):
+    from eschalign_b200 import KERNEL_AUTO, KERNEL_PLAIN32, GpuScorer, Mode, Scoring, synth
+    world, local_rank = ctx.world, ctx.local_rank
+    refs = synth.panel_tiles()
+    panel_bases = sum(len(r) for r in refs)
+    if a.profile_case:
+        reads = synth.reads_c2(refs, n=a.profile_case)
+        for kernel in (KERNEL_AUTO, KERNEL_PLAIN32):
+            g = GpuScorer(refs, Scoring(*HEADLINE[0]), Mode.parse(a.mode), device=local_rank,
+                          kernel=kernel)
+            r = g.score_batch(reads.tuple(), both_strands=True)
+            print(json.dumps({"profile_case": a.profile_case, "kernel": kernel,
+                              "stats": r.stats}), flush=True)
+            g.close()
+        return
+    reads = synth.reads_c2(refs, n=a.reads)  # weak scaling: every rank scores the full batch
+    extras = {}
+    scoring, mode = HEADLINE
+    g = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank,
+                  stream=ctx.stream.cuda_stream)
+    tune = g.autotune()  # tile shape for this panel, before any timing
+    info = g.info()
+    batch = g.submit(g.prepare(reads.tuple(), both_strands=True))
+    st = g.finish(batch, keep=True).stats
+    cells = st["cells"]
+    sampler = ClockSampler(local_rank)
+    t = ctx.device_time(g, batch, a.steps, a.warmup, sampler)
+    clocks = sampler.summary()
+    t_max = ctx.max_over_ranks(t)
+    value = world * cells * a.steps / t_max / 1e9
+    peak = int_peak(local_rank)
+    roofline = roofline_of(peak, cells * a.steps / t, mode,
+                           K2_DRAM_BYTES_PER_CELL * cells if K2_DRAM_BYTES_PER_CELL else None)
+    if peak:
+        extras["int_probe"] = {k: round(v["lane_ops_per_s"] / 1e12, 3)
+                               for k, v in peak["ops"].items()}
+        extras["int_probe_per_sm_clk"] = {k: round(v["per_sm_per_clk"], 2)
+                                          for k, v in peak["ops"].items()}
+    batch.free()
+
+    if not a.no_extras:
+        combos = {}
+        for sc_, md in COMBOS[1:]:
+            g2 = GpuScorer(refs, Scoring(*sc_), Mode.parse(md), device=local_rank,
+                           stream=ctx.stream.cuda_stream)
+            g2.autotune()
+            b2 = g2.submit(g2.prepare(reads.tuple(), both_strands=True))
+            r2 = g2.finish(b2, keep=True)
+            t2 = ctx.max_over_ranks(ctx.device_time(g2, b2, 1, 1))
+            combos[f"{md} {','.join(map(str, sc_))}"] = round(world * r2.stats["cells"] / t2 / 1e9, 1)
+            b2.free()
+            g2.close()
+        combos[f"{mode} {','.join(map(str, scoring))}"] = round(value, 1)
+        extras["gcups_by_combo"] = combos
+        # the plain one-thread-per-pair kernel on a sample of the same batch
+        sub = reads.slice(0, min(a.plain_reads, len(reads)))
+        g.set_kernel(KERNEL_PLAIN32)
+        bp = g.submit(g.prepare(sub.tuple(), both_strands=True))
+        rp = g.finish(bp, keep=True)
+        tp = ctx.max_over_ranks(ctx.device_time(g, bp, 1, 1))
+        plain = world * rp.stats["cells"] / tp / 1e9
+        bp.free()
+        g.set_kernel(KERNEL_AUTO)
+        extras["plain_gcups"] = plain
+        extras["batched_over_plain"] = value / plain
+        extras["plain_sample"] = f"first {len(sub)} reads, both strands"
+
+    chunks = [reads.slice(k, k + a.chunk) for k in range(0, len(reads), a.chunk)]
+    te, n_pass, h2d, d2h = feeder(
+        ctx, chunks, lambda c: g.prepare(c.tuple(), both_strands=True), g.submit,
+        lambda b: g.finish(b).stats, max(1, min(2, a.steps)))
+    e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "reads_per_s": world * len(reads) * n_pass / te, "chunk_reads": a.chunk}
+    g.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(refs, reads, scoring, mode, a.cpu_seconds)
+        extras["cpu_reads_per_s"] = cpu.pop("reads_per_s")
+        cpu.pop("seconds", None)
+    if rank == 0:
+        line = common_line(
+            a, ctx, value, 1e3 * t_max / a.steps,
+            "C2: 1M reads (lognormal median 110 nt) x 164-ref panel (70-180 nt), both "
+            "strands, local 2,-1,-10,-1, best + XS + 8 ties per read",
+            {"reads": a.reads, "refs": len(refs), "panel_bases": panel_bases,
+             "cells_per_step": cells},
+            e2e, roofline, clocks, st["kernels"] * a.steps)
+        line["reads_per_s"] = world * len(reads) * a.steps / t_max
+        line["kernel_info"] = {k: info[k] for k in (
+            "regs_batched", "regs_plain", "local_bytes_batched", "batched_blocks",
+            "panel_bytes", "sm_count", "split_len")}
+        line["autotune"] = tune
+        line["batch_stats"] = {k: st[k] for k in ("queries_batched", "queries_plain",
+                                                  "queries_rescored", "tasks", "lanes_used")}
+        if cpu:
+            line["cpu_baseline"] = cpu
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- C4
+def run_c4(a, ctx, rank):
+    from eschalign_b200 import GpuScorer, Mode, Scoring, adapter, synth
+    world, local_rank = ctx.world, ctx.local_rank
+    refs = synth.panel_tiles()
+    panel_bases = sum(len(r) for r in refs)
+    t0 = time.perf_counter()
+    pairs, _ = synth.pairs_c4(refs, n=a.pairs)
+    gen_s = time.perf_counter() - t0
+    n_pairs = len(pairs) // 2
+    cfg = adapter.config()
+    g = GpuScorer(refs, Scoring(*C4_SCORING), Mode.SEMIGLOBAL, device=local_rank,
+                  stream=ctx.stream.cuda_stream)
+    tune = g.autotune()
+    batch = g.submit(g.prepare_pairs(pairs.tuple(), adapters=cfg, both_strands=True))
+    st = g.finish_pairs(batch, keep=True).stats
+    cells = st["cells"]
+    sampler = ClockSampler(local_rank)
+    t = ctx.device_time(g, batch, a.steps, a.warmup, sampler)
+    clocks = sampler.summary()
+    t_max = ctx.max_over_ranks(t)
+    value = world * cells * a.steps / t_max / 1e9
+    peak = int_peak(local_rank)
+    roofline = roofline_of(peak, cells * a.steps / t, "semiglobal", None)
+    batch.free()
+    step_pairs = a.pair_chunk
+    chunks = [pairs.slice(2 * k, 2 * (k + step_pairs)) for k in range(0, n_pairs, step_pairs)]
+    te, n_pass, h2d, d2h = feeder(
+        ctx, chunks, lambda c: g.prepare_pairs(c.tuple(), adapters=cfg, both_strands=True),
+        g.submit, lambda b: g.finish_pairs(b).stats, max(1, min(2, a.steps)))
+    e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "pairs_per_s": world * n_pairs * n_pass / te, "chunk_pairs": step_pairs}
+    g.close()
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_pairs_baseline(refs, pairs, C4_SCORING, a.cpu_seconds)
+        cpu.pop("seconds", None)
+    if rank == 0:
+        line = common_line(
+            a, ctx, value, 1e3 * t_max / a.steps,
+            f"C4: {n_pairs} pairs 2x150 (insert lognormal median 90, adapter read-through) x "
+            "164-ref panel, semiglobal 2,-1,-10,-1; mates trimmed on the host, 4 mate queries "
+            "per pair, both template strands ranked on the device (best sum, tie set, next "
+            "tier, per-mate XS) + each mate's own both-strand result",
+            {"pairs": n_pairs, "refs": len(refs), "panel_bases": panel_bases,
+             "cells_per_step": cells, "mates_trimmed": st["mates_trimmed"],
+             "bases_trimmed": st["bases_trimmed"], "generate_s": round(gen_s, 1)},
+            e2e, roofline, clocks, st["kernels"] * a.steps)
+        line["pairs_per_s"] = world * n_pairs * a.steps / t_max
+        line["reads_per_s"] = 2 * line["pairs_per_s"]
+        line["autotune"] = tune
+        line["batch_stats"] = {k: st[k] for k in ("queries_batched", "queries_plain",
+                                                  "queries_rescored", "tasks", "lanes_used",
+                                                  "kernels")}
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- C3
+def run_c3(a, ctx, rank):
+    from eschalign_b200 import GpuScorer, Mode, Scoring, synth
+    world, local_rank = ctx.world, ctx.local_rank
+    refs = synth.panel_c3()
+    panel_bases = sum(len(r) for r in refs)
+    reads = synth.reads_c3(refs, n=a.c3_reads)
+    g = GpuScorer(refs, Scoring(*C3_SCORING), Mode.LOCAL, device=local_rank,
+                  stream=ctx.stream.cuda_stream)
+    tune = g.autotune()
+    info = g.info()
+    batch = g.submit(g.prepare(reads.tuple(), both_strands=True))
+    st = g.finish(batch, keep=True).stats
+    cells = st["cells"]
+    sampler = ClockSampler(local_rank)
+    t = ctx.device_time(g, batch, a.steps, a.warmup, sampler)
+    clocks = sampler.summary()
+    t_max = ctx.max_over_ranks(t)
+    value = world * cells * a.steps / t_max / 1e9
+    peak = int_peak(local_rank)
+    roofline = roofline_of(peak, cells * a.steps / t, "local", None)
+    batch.free()
+    te, n_pass, h2d, d2h = feeder(
+        ctx, [reads], lambda c: g.prepare(c.tuple(), both_strands=True), g.submit,
+        lambda b: g.finish(b).stats, 1)
+    e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+    g.close()
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(refs, reads, C3_SCORING, "local", a.cpu_seconds, chunk=1)
+        cpu.pop("seconds", None)
+        cpu.pop("reads_per_s", None)
+    if rank == 0:
+        line = common_line(
+            a, ctx, value, 1e3 * t_max / a.steps,
+            f"C3: {len(reads)} reads (50-1000 nt, 70 % derived) x 10 000-ref panel "
+            "(300-1000 nt), both strands, local 2,-1,-10,-1, autotuned tile shape",
+            {"reads": len(reads), "refs": len(refs), "panel_bases": panel_bases,
+             "cells_per_step": cells},
+            e2e, roofline, clocks, st["kernels"] * a.steps)
+        line["autotune"] = tune
+        line["kernel_info"] = {k: info[k] for k in ("panel_bytes", "split_len",
+                                                    "batched_blocks")}
+        line["batch_stats"] = {k: st[k] for k in ("queries_batched", "queries_plain",
+                                                  "queries_rescored", "tasks", "lanes_used",
+                                                  "kernels")}
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
 
 
 def main():
@@ -228,199 +615,14 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from eschalign_b200 import GpuScorer, Mode, Scoring, synth
-    from eschalign_b200 import KERNEL_PLAIN32, KERNEL_AUTO
-
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    refs = synth.panel_tiles()
-    panel_bases = sum(len(r) for r in refs)
-    if a.profile_case:
-        reads = synth.reads_c2(refs, n=a.profile_case)
-        for kernel in (KERNEL_AUTO, KERNEL_PLAIN32):
-            g = GpuScorer(refs, Scoring(*HEADLINE[0]), Mode.parse(a.mode), device=local_rank,
-                          kernel=kernel)
-            r = g.score_batch(reads.tuple(), both_strands=True)
-            print(json.dumps({"profile_case": a.profile_case, "kernel": kernel,
-                              "stats": r.stats}), flush=True)
-            g.close()
-        return
-    reads = synth.reads_c2(refs, n=a.reads)  # weak scaling: every rank scores the full batch
-    stream = torch.cuda.Stream(device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
-
-    def device_time(scorer, batch, steps, warmup, sampler=None):
-        for _ in range(warmup):
-            scorer.relaunch(batch, stream.cuda_stream)
-        torch.cuda.synchronize()
-        barrier()
-        total = 0.0
-        ctx = sampler if sampler is not None else _Null()
-        with ctx:
-            for k in range(steps):
-                with torch.cuda.stream(stream):
-                    flush.fill_(k & 0xFF)
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                scorer.relaunch(batch, stream.cuda_stream)
-                e1.record(stream)
-                e1.synchronize()
-                total += e0.elapsed_time(e1) / 1e3
-        torch.cuda.synchronize()
-        barrier()
-        return total
-
-    results = {}
-    extras = {}
-    # ---- headline: batched kernel, local 2,-1,-10,-1, inputs resident
-    scoring, mode = HEADLINE
-    g = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank,
-                  stream=stream.cuda_stream)
-    tune = g.autotune()  # tile shape for this panel, before any timing
-    info = g.info()
-    batch = g.submit(g.prepare(reads.tuple(), both_strands=True))
-    first = g.finish(batch, keep=True)
-    st = first.stats
-    cells = st["cells"]
-    launches_per_step = st["kernels"]
-    sampler = ClockSampler(local_rank)
-    t = device_time(g, batch, a.steps, a.warmup, sampler)
-    clocks = sampler.summary()
-    t_max = max_over_ranks(t)
-    value = world * cells * a.steps / t_max / 1e9
-    ms_per_step = 1e3 * t_max / a.steps
-    reads_per_s = world * len(reads) * a.steps / t_max
-    results["headline"] = value
-
-    # ---- roofline of the batched kernel (integer ALU)
-    peak = int_peak(local_rank)
-    per_gpu_cells_s = cells * a.steps / t
-    achieved = per_gpu_cells_s * OPS_PER_CELL[mode] / 2.0
-    roofline = {"bound": "int_alu", "achieved": achieved / 1e12,
-                "peak": (peak["peak_lane_ops_per_s"] / 1e12) if peak else None,
-                "unit": "T lane-ops/s",
-                "frac": (achieved / peak["peak_lane_ops_per_s"]) if peak else None,
-                "traffic": (K2_DRAM_BYTES_PER_CELL * cells if K2_DRAM_BYTES_PER_CELL else None),
-                "kernel": "k2_batched",
-                "note": "achieved = cells/s x 12 int ops (11 semi-global) / 2 cells per "
-                        "int16x2 lane-op; peak = measured iadd32/imax32 lane-op rate "
-                        "(csrc/esg_probe.cu), measured in this run"}
-    if peak:
-        extras["int_probe"] = {k: round(v["lane_ops_per_s"] / 1e12, 3)
-                               for k, v in peak["ops"].items()}
-        extras["int_probe_per_sm_clk"] = {k: round(v["per_sm_per_clk"], 2)
-                                          for k, v in peak["ops"].items()}
-    batch.free()
-
-    # ---- the other (mode, scheme) combinations, one timed step each
-    if not a.no_extras:
-        combos = {}
-        for sc_, md in COMBOS[1:]:
-            g2 = GpuScorer(refs, Scoring(*sc_), Mode.parse(md), device=local_rank,
-                           stream=stream.cuda_stream)
-            g2.autotune()
-            b2 = g2.submit(g2.prepare(reads.tuple(), both_strands=True))
-            r2 = g2.finish(b2, keep=True)
-            t2 = max_over_ranks(device_time(g2, b2, 1, 1))
-            combos[f"{md} {','.join(map(str, sc_))}"] = round(world * r2.stats["cells"] / t2 / 1e9, 1)
-            b2.free()
-            g2.close()
-        combos[f"{mode} {','.join(map(str, scoring))}"] = round(value, 1)
-        extras["gcups_by_combo"] = combos
-
-        # ---- plain one-thread-per-pair kernel on a sample of the same batch
-        sub = reads.subset(np.arange(min(a.plain_reads, len(reads))))
-        g.set_kernel(KERNEL_PLAIN32)
-        bp = g.submit(g.prepare(sub.tuple(), both_strands=True))
-        rp = g.finish(bp, keep=True)
-        tp = max_over_ranks(device_time(g, bp, 1, 1))
-        plain = world * rp.stats["cells"] / tp / 1e9
-        bp.free()
-        g.set_kernel(KERNEL_AUTO)
-        extras["plain_gcups"] = plain
-        extras["batched_over_plain"] = value / plain
-        extras["plain_sample"] = f"first {len(sub)} reads, both strands"
-
-    # ---- e2e through the public API with host buffers (double-buffered feeder)
-    chunks = [reads.subset(np.arange(k, min(k + a.chunk, len(reads))))
-              for k in range(0, len(reads), a.chunk)]
-    e2e_steps = max(1, min(2, a.steps))
-    h2d = d2h = 0
-    e2e_times = []
-    for it in range(e2e_steps + 1):
-        barrier()
-        t0 = time.perf_counter()
-        pending = None
-        h2d = d2h = 0
-        for c in chunks + [None]:
-            prepared = g.prepare(c.tuple(), both_strands=True) if c is not None else None
-            if pending is not None:
-                out = g.finish(pending)
-                h2d += out.stats["h2d_bytes"]
-                d2h += out.stats["d2h_bytes"]
-            pending = g.submit(prepared) if prepared is not None else None
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        if it > 0:  # the first pass is a warm-up (pinned pool, allocator)
-            e2e_times.append(dt)
-    te = max_over_ranks(sum(e2e_times))
-    e2e = {"value": world * cells * len(e2e_times) / te / 1e9, "unit": "GCUPS",
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "reads_per_s": world * len(reads) * len(e2e_times) / te,
-           "chunk_reads": a.chunk}
-    g.close()
-
-    cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(refs, reads, scoring, mode, a.cpu_seconds)
-        extras["cpu_reads_per_s"] = cpu.pop("reads_per_s")
-        cpu.pop("seconds", None)
-
-    if rank == 0:
-        line = {
-            "metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16x2",
-            "data": "synthetic",
-            "config": {"workload": "C2: 1M reads (lognormal median 110 nt) x 164-ref panel "
-                                   "(70-180 nt), both strands, local 2,-1,-10,-1, best + XS + "
-                                   "8 ties per read",
-                       "reads": a.reads, "refs": len(refs), "panel_bases": panel_bases,
-                       "cells_per_step": cells, "parallelism": f"replicas x{world}",
-                       "l2": "flushed (256 MB write) between timed steps"},
-            "reads_per_s": reads_per_s,
-            "e2e": e2e,
-            "roofline": roofline,
-            "clocks": clocks,
-            "gpu_launches": launches_per_step * a.steps,
-            "kernel_info": {k: info[k] for k in ("regs_batched", "regs_plain",
-                                                 "local_bytes_batched", "batched_blocks",
-                                                 "panel_bytes", "sm_count", "split_len")},
-            "autotune": tune,
-            "batch_stats": {k: st[k] for k in ("queries_batched", "queries_plain",
-                                               "queries_rescored", "tasks", "lanes_used")},
-        }
-        if cpu:
-            line["cpu_baseline"] = cpu
-        line.update(extras)
-        print(json.dumps(line), flush=True)
+    ctx = Ctx(torch, dist, dev, local_rank, world)
+    {"c2": run_c2, "c3": run_c3, "c4": run_c4}[a.workload](a, ctx, rank)
     if world > 1:
         dist.destroy_process_group()
 

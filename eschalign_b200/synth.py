@@ -56,6 +56,16 @@ class Packed:
     def list(self):
         return [self.read(k) for k in range(len(self))]
 
+    def slice(self, k0, k1):
+        """Reads k0..k1-1 as a view (reads are stored in order)."""
+        k1 = min(k1, len(self))
+        if k1 <= k0:
+            return Packed(np.zeros(1, np.uint8), np.zeros(0, np.uint64), np.zeros(0, np.uint32))
+        o0 = int(self.off[k0])
+        o1 = int(self.off[k1 - 1]) + int(self.lens[k1 - 1])
+        return Packed(self.codes[o0:max(o1, o0 + 1)], self.off[k0:k1] - np.uint64(o0),
+                      self.lens[k0:k1])
+
     def subset(self, idx):
         idx = np.asarray(idx)
         parts = [self.read(int(k)) for k in idx]
@@ -108,15 +118,15 @@ def mutate(rng, codes, lens, p_sub, p_ins, p_del, p_geom=0.6):
     n = codes.size
     if n == 0:
         return codes, lens
-    seg = np.repeat(np.arange(lens.size), lens)
-    seg_end = np.repeat(np.cumsum(lens), lens)
-    pos = np.arange(n)
-    keep = np.ones(n, dtype=np.int64)
+    lens = np.asarray(lens, dtype=np.int64)
+    bounds = np.cumsum(lens)
+    keep = np.ones(n, dtype=np.int8)
     starts = np.nonzero(rng.random(n) < p_del)[0]
     if starts.size:
         dl = rng.geometric(p_geom, starts.size)
-        ends = np.minimum(starts + dl, seg_end[starts])
-        diff = np.zeros(n + 1, dtype=np.int64)
+        seg_end = bounds[np.searchsorted(bounds, starts, side="right")]
+        ends = np.minimum(starts + dl, seg_end)
+        diff = np.zeros(n + 1, dtype=np.int32)
         np.add.at(diff, starts, 1)
         np.add.at(diff, ends, -1)
         keep[np.cumsum(diff[:-1]) > 0] = 0
@@ -124,21 +134,22 @@ def mutate(rng, codes, lens, p_sub, p_ins, p_del, p_geom=0.6):
     sub = np.nonzero(rng.random(n) < p_sub)[0]
     if sub.size:
         out[sub] = (out[sub] + rng.integers(1, 4, sub.size)) % 4
-    ins = np.zeros(n, dtype=np.int64)
+    reps = keep.astype(np.int32)
     ii = np.nonzero(rng.random(n) < p_ins)[0]
     if ii.size:
-        ins[ii] = rng.geometric(p_geom, ii.size)
-    reps = keep + ins
-    src = np.repeat(pos, reps)
+        reps[ii] += rng.geometric(p_geom, ii.size).astype(np.int32)
+    idx_t = np.int32 if n < (1 << 31) else np.int64
+    src = np.repeat(np.arange(n, dtype=idx_t), reps)
     new = out[src]
     # inserted copies (all but the first of a kept base, all of a deleted one)
+    cs = np.cumsum(reps, dtype=np.int64)
     first = np.zeros(src.size, dtype=bool)
-    starts_out = np.cumsum(reps) - reps
-    has = reps > 0
-    first[starts_out[has]] = True
+    starts_out = cs - reps
+    first[starts_out[reps > 0]] = True
     is_ins = ~first | (keep[src] == 0)
     new[is_ins] = rng.integers(0, 4, int(is_ins.sum()), dtype=np.uint8)
-    new_lens = np.bincount(seg[src], minlength=lens.size).astype(np.int64)
+    cs0 = np.concatenate(([0], cs))
+    new_lens = cs0[bounds] - cs0[bounds - lens]
     return new, new_lens
 
 
@@ -241,7 +252,7 @@ def _fix_length(rng, codes, lens, target):
 
 def pairs_c4(refs, n=2_000_000, seed=SEED_C4, read_len=150, median=90, sigma=0.5,
              insert_lo=40, insert_hi=600, p_adapter=0.01, p_sub=0.01, p_ins=0.001,
-             p_del=0.001):
+             p_del=0.001, chunk=8192):
     """Read pairs of 2 x read_len: a fragment (the insert, lognormal around
     `median`, clipped to [insert_lo, insert_hi]) from a random reference on
     a random template strand; mate 1 reads the fragment from its 5' end,
@@ -249,12 +260,27 @@ def pairs_c4(refs, n=2_000_000, seed=SEED_C4, read_len=150, median=90, sigma=0.5
     into its adapter (TRUSEQ_R1 / _R2 with p_adapter substitutions, random
     bases past the adapter's end).  A fragment longer than its reference
     gets random flanks.  Each mate then takes p_sub substitutions and
-    p_ins + p_del indels and is cut or padded back to read_len.  Returns a
-    Packed of 2n reads, mate 1 of pair p at 2p, mate 2 at 2p + 1, and the
-    inserts."""
+    p_ins + p_del indels and is cut or padded back to read_len.  Built in
+    chunks of `chunk` pairs (generator seeded by (seed, chunk index)).
+    Returns a Packed of 2n reads, mate 1 of pair p at 2p, mate 2 at 2p + 1,
+    and the inserts."""
+    codes, inserts = [], []
+    for c0 in range(0, n, chunk):
+        rng = np.random.default_rng([seed, c0 // chunk])
+        cc, ins = _pairs_chunk(rng, refs, min(chunk, n - c0), read_len, median, sigma,
+                               insert_lo, insert_hi, p_adapter, p_sub, p_ins, p_del)
+        codes.append(cc)
+        inserts.append(ins)
+    codes = np.concatenate(codes) if codes else np.zeros(0, np.uint8)
+    ins = np.concatenate(inserts) if inserts else np.zeros(0, np.int64)
+    lens = np.full(2 * n, read_len, dtype=np.uint32)
+    return Packed(codes, _offsets(lens), lens), ins
+
+
+def _pairs_chunk(rng, refs, n, read_len, median, sigma, insert_lo, insert_hi, p_adapter, p_sub,
+                 p_ins, p_del):
     from .alphabet import encode
 
-    rng = np.random.default_rng(seed)
     ref_lens = np.array([r.size for r in refs], dtype=np.int64)
     ref_off = _offsets(ref_lens).astype(np.int64)
     cat = np.concatenate(refs)
@@ -292,6 +318,4 @@ def pairs_c4(refs, n=2_000_000, seed=SEED_C4, read_len=150, median=90, sigma=0.5
             m[pos] = a
         mc, ml = mutate(rng, m, np.full(n, read_len, dtype=np.int64), p_sub, p_ins, p_del)
         mates.append(_fix_length(rng, mc, ml, read_len).reshape(n, read_len))
-    codes = np.stack(mates, axis=1).reshape(-1)
-    lens = np.full(2 * n, read_len, dtype=np.uint32)
-    return Packed(codes, _offsets(lens), lens), ins
+    return np.stack(mates, axis=1).reshape(-1), ins

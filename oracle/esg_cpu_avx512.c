@@ -297,6 +297,13 @@ void eo_profile_score_all(const eo_profile* p, const uint8_t* q, size_t n, int l
     free(sc.e);
 }
 
+/* Reads per work unit handed to a worker: 64 as the reference's CLI
+ * (align.rs:1470-1473); a bounded sample of very long reads needs smaller
+ * units to keep every core busy. */
+static int g_chunk = 64;
+
+void eo_cpu_set_chunk(int reads) { g_chunk = reads > 0 ? reads : 64; }
+
 int eo_cpu_map_batch(const eo_profile* p, const uint8_t* codes, const uint64_t* off,
                      const uint32_t* len, uint32_t n_reads, int both_strands, int local,
                      int threads, uint32_t cap, eo_result* results, uint32_t* ties,
@@ -317,7 +324,7 @@ int eo_cpu_map_batch(const eo_profile* p, const uint8_t* codes, const uint64_t* 
         int32_t* rev = (int32_t*)malloc((size_t)n_refs * sizeof(int32_t));
         uint8_t* rc = NULL;
         size_t rc_cap = 0;
-#pragma omp for schedule(dynamic, 64)
+#pragma omp for schedule(dynamic, g_chunk)
         for (long k = 0; k < (long)n_reads; k++) {
             const uint8_t* q = codes + off[k];
             const size_t n = len[k];
@@ -355,6 +362,94 @@ int eo_cpu_map_batch(const eo_profile* p, const uint8_t* codes, const uint64_t* 
         }
         free(fwd);
         free(rev);
+        free(rc);
+        free(sc.h);
+        free(sc.e);
+    }
+    return nt;
+}
+
+/* The reference's CPU path for pairs, the timed baseline of the paired
+ * workload: per pair (OpenMP, chunks of 32 pairs) pair_adapters
+ * (align.rs:934-949), then the four mate rows with the SIMD kernels
+ * (score_all, mapper.rs:242-252), the pair ranking (pair.rs:195-234) and
+ * each mate's own both-strand selection (mapper.rs:444-472, the Separate
+ * fallback).  mate_results / mate_ties may be NULL. */
+int eo_cpu_map_pairs(const eo_profile* p, const uint8_t* codes, const uint64_t* off,
+                     const uint32_t* len, uint32_t n_pairs, const uint8_t* a1, size_t al1,
+                     const uint8_t* a2, size_t al2, size_t min_overlap, size_t max_read_len,
+                     int both_strands, int local, int32_t min_score, int threads, uint32_t cap,
+                     eo_pair_result* results, uint32_t* ties, eo_result* mate_results,
+                     uint32_t* mate_ties, uint32_t* adapters)
+{
+    int nt = threads;
+#ifdef _OPENMP
+    extern int omp_get_max_threads(void);
+    if (nt <= 0) nt = omp_get_max_threads();
+#else
+    if (nt <= 0) nt = 1;
+#endif
+    const uint32_t n_refs = p->n_refs;
+#pragma omp parallel num_threads(nt)
+    {
+        scratch sc = {0};
+        int32_t* rows = (int32_t*)malloc((size_t)4 * n_refs * sizeof(int32_t));
+        uint8_t* rc = NULL;
+        size_t rc_cap = 0;
+#pragma omp for schedule(dynamic, 32)
+        for (long pp = 0; pp < (long)n_pairs; pp++) {
+            const size_t a = 2 * (size_t)pp, b = a + 1;
+            size_t ad[2] = {0, 0}, n[2];
+            eo_pair_adapters(codes + off[a], len[a], codes + off[b], len[b], a1, al1, a2, al2,
+                             min_overlap, max_read_len, ad);
+            for (int m = 0; m < 2; m++) {
+                const size_t l = len[a + m];
+                n[m] = (max_read_len && l > max_read_len) ? 0 : l - ad[m];
+                if (adapters) adapters[a + m] = (uint32_t)ad[m];
+            }
+            /* rows: mate m forward at 2m, reverse complement at 2m + 1 */
+            for (int m = 0; m < 2; m++) {
+                int32_t* f = rows + (size_t)(2 * m) * n_refs;
+                int32_t* r = f + n_refs;
+                if (n[m] == 0) {
+                    memset(f, 0, (size_t)2 * n_refs * sizeof(int32_t));
+                    continue;
+                }
+                const uint8_t* q = codes + off[a + m];
+                if (rc_cap < n[m]) {
+                    free(rc);
+                    rc = (uint8_t*)malloc(n[m]);
+                    rc_cap = n[m];
+                }
+                eo_revcomp_codes(q, n[m], rc);
+                score_all_scratch(p, q, n[m], local, 0, f, &sc);
+                score_all_scratch(p, rc, n[m], local, 0, r, &sc);
+            }
+            eo_pair_result* res = &results[pp];
+            if (n[0] == 0 || n[1] == 0) {
+                res->best = res->next = EO_NO_SCORE;
+                res->n_tied = 0;
+                res->flags = EO_RESULT_EMPTY;
+                res->xs[0] = res->xs[1] = res->primary[0] = res->primary[1] = EO_NO_SCORE;
+            } else {
+                eo_pair_select(rows, rows + n_refs, rows + 2 * (size_t)n_refs,
+                               rows + 3 * (size_t)n_refs, n_refs, both_strands, min_score, cap,
+                               res, ties + (size_t)pp * cap);
+            }
+            if (mate_results)
+                for (int m = 0; m < 2; m++) {
+                    eo_result* mr = &mate_results[a + m];
+                    if (n[m] == 0) {
+                        mr->best = mr->suboptimal = EO_NO_SCORE;
+                        mr->n_tied = 0;
+                        mr->flags = EO_RESULT_EMPTY;
+                        continue;
+                    }
+                    eo_select(rows + (size_t)(2 * m) * n_refs, rows + (size_t)(2 * m + 1) * n_refs,
+                              n_refs, cap, mr, mate_ties + (a + m) * cap);
+                }
+        }
+        free(rows);
         free(rc);
         free(sc.h);
         free(sc.e);

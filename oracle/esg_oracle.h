@@ -103,6 +103,9 @@ int eo_cpu_map_batch(const eo_profile* p, const uint8_t* codes, const uint64_t* 
                      int threads, uint32_t cap, eo_result* results, uint32_t* ties,
                      int32_t* rows);
 
+/* Reads per work unit of eo_cpu_map_batch's workers (default 64). */
+void eo_cpu_set_chunk(int reads);
+
 /* Same, with the scalar oracle instead of the SIMD kernels (used at test
  * sizes; identical results by construction of the reference). */
 int eo_scalar_map_batch(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
@@ -144,6 +147,15 @@ void eo_pair_select(const int32_t* f0, const int32_t* r0, const int32_t* f1, con
 void eo_pairs_from_rows(const int32_t* rows, const uint32_t* len, uint32_t n_pairs,
                         uint32_t n_refs, int both_strands, int32_t min_score, uint32_t cap,
                         eo_pair_result* results, uint32_t* ties);
+/* The reference's CPU path for pairs (the timed baseline): trimming, the
+ * four mate rows with the SIMD kernels, the pair ranking and each mate's
+ * both-strand selection, OpenMP over pairs.  Returns the thread count. */
+int eo_cpu_map_pairs(const eo_profile* p, const uint8_t* codes, const uint64_t* off,
+                     const uint32_t* len, uint32_t n_pairs, const uint8_t* a1, size_t al1,
+                     const uint8_t* a2, size_t al2, size_t min_overlap, size_t max_read_len,
+                     int both_strands, int local, int32_t min_score, int threads, uint32_t cap,
+                     eo_pair_result* results, uint32_t* ties, eo_result* mate_results,
+                     uint32_t* mate_ties, uint32_t* adapters);
 /* Pairs end to end with the scalar oracle; mates 2 per pair, already trimmed. */
 int eo_scalar_map_pairs(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
                         uint32_t n_pairs, const uint8_t* ref_codes, const uint64_t* ref_off,

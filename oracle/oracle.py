@@ -102,6 +102,13 @@ def lib():
                                           C.c_uint32, C.c_int32, C.c_int32, C.c_int32,
                                           C.c_int32, C.c_int, C.c_int, C.c_int32, C.c_int,
                                           C.c_uint32, C.c_void_p, u32p]
+        L.eo_cpu_map_pairs.restype = C.c_int
+        L.eo_cpu_map_pairs.argtypes = [C.c_void_p, u8p, u64p, u32p, C.c_uint32, u8p, C.c_size_t,
+                                       u8p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_int, C.c_int,
+                                       C.c_int32, C.c_int, C.c_uint32, C.c_void_p, u32p,
+                                       C.c_void_p, u32p, u32p]
+        L.eo_cpu_set_chunk.restype = None
+        L.eo_cpu_set_chunk.argtypes = [C.c_int]
         L.eo_cpu_map_batch.restype = C.c_int
         L.eo_cpu_map_batch.argtypes = [C.c_void_p, u8p, u64p, u32p, C.c_uint32, C.c_int, C.c_int,
                                        C.c_int, C.c_uint32, C.c_void_p, u32p, i32p]
@@ -240,6 +247,30 @@ class Profile:
                                       _p(ties, C.c_uint32),
                                       _p(out_rows, C.c_int32) if rows else None)
         return res, ties, out_rows, used
+
+    def map_pairs(self, codes, off, lens, local, both_strands=True, min_score=0, cap=8,
+                  threads=0, a1=None, a2=None, min_overlap=5, max_read_len=0):
+        """The reference's CPU path for pairs (eo_cpu_map_pairs): returns
+        (pair results, pair ties, mate results, mate ties, adapters, threads)."""
+        n = int(lens.size) // 2
+        x1 = _codes(TRUSEQ_R1 if a1 is None else a1)
+        x2 = _codes(TRUSEQ_R2 if a2 is None else a2)
+        res = np.zeros(n, dtype=PAIR_DTYPE)
+        ties = np.zeros((n, max(cap, 1)), dtype=np.uint32)
+        mres = np.zeros(2 * n, dtype=RESULT_DTYPE)
+        mties = np.zeros((2 * n, max(cap, 1)), dtype=np.uint32)
+        ads = np.zeros(2 * n, dtype=np.uint32)
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        lens = np.ascontiguousarray(lens, dtype=np.uint32)
+        used = lib().eo_cpu_map_pairs(self._h, _p(codes, C.c_uint8), _p(off, C.c_uint64),
+                                      _p(lens, C.c_uint32), n, _p(x1, C.c_uint8), x1.size,
+                                      _p(x2, C.c_uint8), x2.size, min_overlap, max_read_len,
+                                      int(bool(both_strands)), int(bool(local)), min_score,
+                                      threads, cap, res.ctypes.data, _p(ties, C.c_uint32),
+                                      mres.ctypes.data, _p(mties, C.c_uint32),
+                                      _p(ads, C.c_uint32))
+        return res, ties, mres, mties, ads, used
 
 
 TRUSEQ_R1 = b"AGATCGGAAGAGCACACGTCTGAACTCCAGTCA"  # adapter.rs:40
