@@ -101,7 +101,8 @@ class EsgBatchStats(C.Structure):
                 ("queries_rescored", C.c_uint32), ("tasks", C.c_uint32),
                 ("lanes_used", C.c_uint32), ("kernels", C.c_uint32), ("cells", C.c_uint64),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("n_pairs", C.c_uint32),
-                ("mates_trimmed", C.c_uint32), ("bases_trimmed", C.c_uint64)]
+                ("mates_trimmed", C.c_uint32), ("bases_trimmed", C.c_uint64),
+                ("panel_chunks", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class EsgAdapterConfig(C.Structure):
@@ -130,6 +131,7 @@ SIGNATURES = {
     "esg_scores_len": (C.c_int32, [C.c_void_p, C.c_uint64]),
     "esg_scorer_autotune": (C.c_int32, [C.c_void_p, C.POINTER(EsgTuneReport)]),
     "esg_scorer_set_split": (C.c_int32, [C.c_void_p, C.c_uint32]),
+    "esg_scorer_set_chunking": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "esg_score_batch": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32, C.c_uint32,
                                     C.c_void_p, _u32p, _i32p]),
     "esg_prepare": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32, C.c_uint32,

@@ -116,6 +116,7 @@ struct esg_scorer {
   uint32_t sel_base = 0;
   bool smem_panel = false;
   void* d_blob = nullptr;
+  std::vector<uint64_t> pair_cols;  // prefix sums of the pairs' column counts
   uint32_t tab_a[6]{}, tab_b[6]{};
   int sat = 0;
   size_t k2_smem = 0;
@@ -129,6 +130,7 @@ struct esg_scorer {
   // stripes (esg_scorer_autotune measures where 32 rows start to win)
   uint32_t split_len = 256;
   bool tuned = false;
+  uint32_t max_chunks = 64;  // panel chunks per tile at most (1: never chunk)
   cudaStream_t aux = nullptr;          // second stream: the long-query kernel
   cudaEvent_t fork = nullptr, join = nullptr;
   // k3 panel (longest first)
@@ -157,6 +159,7 @@ struct esg_batch {
   uint32_t n_order = 0;
   uint32_t host_list = 0;
   uint32_t redo_cap = 0;
+  uint32_t n_chunks = 1;  // panel chunks per tile (k2 tasks = tiles x chunks)
   // paired batches (esg_prepare_pairs): reads 2p, 2p + 1 are pair p's mates
   bool paired = false;
   bool pair_both = false;   // rank both template strands
@@ -171,6 +174,7 @@ struct esg_batch {
   uint32_t* h_order = nullptr;
   uint2* h_tasks = nullptr;
   uint32_t* h_list = nullptr;
+  uint32_t* h_chunks = nullptr;
   size_t in_bytes = 0;
   int4* h_results = nullptr;
   uint32_t* h_ties = nullptr;
@@ -187,6 +191,9 @@ struct esg_batch {
   uint32_t* d_order = nullptr;
   uint2* d_tasks = nullptr;
   uint32_t* d_list = nullptr;
+  uint32_t* d_chunks = nullptr;
+  int4* d_part_head = nullptr;
+  uint32_t* d_part_ties = nullptr;
   uint32_t* d_counters = nullptr;
   int4* d_qhead = nullptr;
   uint32_t* d_qties = nullptr;
@@ -529,6 +536,9 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
     }
   }
   // m is stored in 16 bits: lengths up to kMaxRefLen (32768) fit.
+  sc->pair_cols.assign(sc->n_pairs + 1, 0);
+  for (uint32_t p = 0; p < sc->n_pairs; ++p)
+    sc->pair_cols[p + 1] = sc->pair_cols[p] + (pairs[p].y & 0xffffu);
   sc->sel_base = sc->n_pairs * 8;  // uint16 units after the pair table
   const size_t raw = (size_t)sc->n_pairs * 16 + sels.size() * 2;
   sc->blob_bytes = (uint32_t)((raw + 15) / 16 * 16);
@@ -675,6 +685,15 @@ esg_status esg_scorer_set_kernel(esg_scorer* sc, int32_t kernel) {
 }
 
 int32_t esg_scores_len(const esg_scorer* sc, uint64_t len) { return sc && len > 0; }
+
+esg_status esg_scorer_set_chunking(esg_scorer* sc, uint32_t max_chunks) {
+  g_err.clear();
+  if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");
+  if (max_chunks < 1 || max_chunks > 64)
+    return fail(ESG_ERR_BAD_ARGUMENT, "max_chunks %u outside 1..64", max_chunks);
+  sc->max_chunks = max_chunks;
+  return ESG_OK;
+}
 
 esg_status esg_scorer_set_split(esg_scorer* sc, uint32_t split_len) {
   if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");
@@ -837,6 +856,19 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   b->n_t16 = (uint32_t)p16.tasks.size();
   b->n_tasks = b->n_long + b->n_t32 + b->n_t16;
   b->n_order = n_long + (uint32_t)(q32.size() + q16.size());
+  // --- panel chunks: when the tiles are too few to keep every resident warp
+  // busy to the end (few reads, or a large panel), each tile's reference
+  // pairs are cut into chunks of about equal columns, one task each, and
+  // the per-chunk query states are merged afterwards
+  {
+    const uint64_t tiles = b->n_tasks;
+    const uint64_t target = 8ull * (uint64_t)std::max(sc->blocks_t16, 1) * kK2Warps;
+    uint32_t nc = 1;
+    if (tiles && tiles < target) nc = (uint32_t)((target + tiles - 1) / tiles);
+    nc = std::min<uint32_t>(nc, std::max<uint32_t>(1, sc->n_pairs / 4));
+    nc = std::min<uint32_t>(nc, sc->max_chunks);
+    b->n_chunks = std::max<uint32_t>(nc, 1);
+  }
 
   // --- pinned staging for the inputs
   const size_t sz_codes = carve_size(total ? total : 1, 1);
@@ -845,7 +877,8 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   const size_t sz_order = carve_size(b->n_order ? b->n_order : 1, 4);
   const size_t sz_tasks = carve_size(b->n_tasks ? b->n_tasks : 1, 8);
   const size_t sz_list = carve_size(n_k3 + redo_cap ? n_k3 + redo_cap : 1, 4);
-  b->in_bytes = sz_codes + sz_off + sz_len + sz_order + sz_tasks + sz_list;
+  const size_t sz_chunks = carve_size(b->n_chunks + 1, 4);
+  b->in_bytes = sz_codes + sz_off + sz_len + sz_order + sz_tasks + sz_list + sz_chunks;
   b->in_buf.p = sc->pinned.get(b->in_bytes, &b->in_buf.cap);
   if (!b->in_buf.p) {
     delete b;
@@ -858,6 +891,23 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   b->h_order = carve<uint32_t>(at, b->n_order ? b->n_order : 1);
   b->h_tasks = carve<uint2>(at, b->n_tasks ? b->n_tasks : 1);
   b->h_list = carve<uint32_t>(at, n_k3 + redo_cap ? n_k3 + redo_cap : 1);
+  b->h_chunks = carve<uint32_t>(at, b->n_chunks + 1);
+  {
+    // chunk c covers pairs [h_chunks[c], h_chunks[c + 1]) of about equal columns
+    const uint32_t nc = b->n_chunks, np = sc->n_pairs;
+    const uint64_t total_cols = sc->pair_cols.empty() ? 0 : sc->pair_cols[np];
+    b->h_chunks[0] = 0;
+    uint32_t p = 0;
+    for (uint32_t c = 1; c < nc; ++c) {
+      const uint64_t want = total_cols * c / nc;
+      while (p < np && sc->pair_cols[p] < want) ++p;
+      // every chunk keeps at least one pair
+      p = std::max(p, b->h_chunks[c - 1] + 1);
+      p = std::min(p, np - (nc - c));
+      b->h_chunks[c] = p;
+    }
+    b->h_chunks[nc] = np;
+  }
   uint64_t pos = 0;
   for (uint32_t k = 0; k < n_reads; ++k) {
     b->h_off[k] = pos;
@@ -893,6 +943,7 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   b->stats.queries_batched = n_long + (uint32_t)(q32.size() + q16.size());
   b->stats.queries_plain = n_k3;
   b->stats.tasks = b->n_tasks;
+  b->stats.panel_chunks = b->n_chunks;
   b->stats.cells = cells;
   *out = b;
   return ESG_OK;
@@ -925,6 +976,10 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
     P.redo_list = b->d_list;
     P.redo_base = b->host_list;
     P.redo_cap = b->redo_cap;
+    P.n_chunks = b->n_chunks;
+    P.chunk_lo = b->d_chunks;
+    P.part_head = b->d_part_head;
+    P.part_ties = b->d_part_ties;
     memcpy(P.tab_a, sc->tab_a, sizeof P.tab_a);
     memcpy(P.tab_b, sc->tab_b, sizeof P.tab_b);
     P.e2 = pack16x2(sc->scoring.gap_extend, sc->scoring.gap_extend);
@@ -940,7 +995,9 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
     // stream; 16-row tiles on the batch's stream.  Launched first, the aux
     // kernels' CTAs share the SMs with the persistent 16-row kernel and
     // fill its tail, instead of queueing behind it.
-    const uint32_t n_long = b->n_long, n_t32 = b->n_t32, n_t16 = b->n_t16;
+    // tasks of a group: its tiles x the panel chunks
+    const uint32_t nc = b->n_chunks;
+    const uint32_t n_long = b->n_long * nc, n_t32 = b->n_t32 * nc, n_t16 = b->n_t16 * nc;
     auto grid = [](int cap, uint32_t tasks) {
       return (int)std::max<uint64_t>(
           1, std::min<uint64_t>((uint64_t)cap, (tasks + kK2Warps - 1) / kK2Warps));
@@ -961,7 +1018,7 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
     }
     if (n_t32) {
       K2Params T = P;
-      T.tasks = P.tasks + n_long;
+      T.tasks = P.tasks + b->n_long;
       T.n_tasks = n_t32;
       T.task_counter = b->d_counters + 4;
       void* targs[] = {&T};
@@ -971,7 +1028,7 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
     }
     if (n_t16) {
       K2Params T = P;
-      T.tasks = P.tasks + n_long + n_t32;
+      T.tasks = P.tasks + b->n_long + b->n_t32;
       T.n_tasks = n_t16;
       T.task_counter = b->d_counters + 0;
       void* targs[] = {&T};
@@ -982,6 +1039,27 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
     if (aux) {
       ESG_CUDA(cudaEventRecord(sc->join, sc->aux));
       ESG_CUDA(cudaStreamWaitEvent(st, sc->join, 0));
+    }
+    if (nc > 1) {
+      KMParams M{};
+      M.order = b->d_order;
+      M.n_order = b->n_order;
+      M.n_chunks = nc;
+      M.part_head = b->d_part_head;
+      M.part_ties = b->d_part_ties;
+      M.qhead = b->d_qhead;
+      M.qties = b->d_qties;
+      M.cap = sc->cap;
+      M.counters = b->d_counters;
+      M.redo_list = b->d_list;
+      M.redo_base = b->host_list;
+      M.redo_cap = b->redo_cap;
+      const int blocks =
+          (int)std::max<uint64_t>(1, std::min<uint64_t>(4096, (b->n_order + 127) / 128));
+      void* margs[] = {&M};
+      ESG_CUDA(cudaLaunchKernel((const void*)k2_merge_chunks, dim3(blocks), dim3(128), margs, 0,
+                                st));
+      ++kernels;
     }
   }
   const bool k3 = b->host_list + b->redo_cap > 0;
@@ -1087,6 +1165,7 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
       carve_size(b->n_order ? b->n_order : 1, 4),
       carve_size(b->n_tasks ? b->n_tasks : 1, 8),
       carve_size(nlist ? nlist : 1, 4),
+      carve_size(b->n_chunks + 1, 4),
       carve_size(8, 4),
       carve_size(nq, 16),
       carve_size(nq * sc->cap, 4),
@@ -1096,6 +1175,8 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
       dev_rows ? carve_size(nq * sc->n_refs, 4) : 0,
       carve_size(2 * np, 16),
       carve_size(np * sc->cap, 4),
+      b->n_chunks > 1 ? carve_size(nq * b->n_chunks, 16) : 0,
+      b->n_chunks > 1 ? carve_size(nq * b->n_chunks * sc->cap, 4) : 0,
   };
   size_t total = 0;
   for (size_t v : sizes) total += v;
@@ -1108,6 +1189,7 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   b->d_order = carve<uint32_t>(at, b->n_order ? b->n_order : 1);
   b->d_tasks = carve<uint2>(at, b->n_tasks ? b->n_tasks : 1);
   b->d_list = carve<uint32_t>(at, nlist ? nlist : 1);
+  b->d_chunks = carve<uint32_t>(at, b->n_chunks + 1);
   b->d_counters = carve<uint32_t>(at, 8);
   b->d_qhead = carve<int4>(at, nq);
   b->d_qties = carve<uint32_t>(at, nq * sc->cap);
@@ -1117,8 +1199,12 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   b->d_rows = dev_rows ? carve<int32_t>(at, nq * sc->n_refs) : nullptr;
   b->d_pairs = np ? carve<int4>(at, 2 * np) : nullptr;
   b->d_pties = np ? carve<uint32_t>(at, np * sc->cap) : nullptr;
+  if (b->n_chunks > 1) {
+    b->d_part_head = carve<int4>(at, nq * b->n_chunks);
+    b->d_part_ties = carve<uint32_t>(at, nq * b->n_chunks * sc->cap);
+  }
   // uploads: the pinned staging is one contiguous block laid out the same way
-  // for the first six buffers
+  // for the first seven buffers
   ESG_CUDA(cudaMemcpyAsync(b->d_codes, b->in_buf.p, b->in_bytes, cudaMemcpyHostToDevice, st));
   b->stats.h2d_bytes = b->in_bytes;
   esg_status s = launch_device_work(sc, b, st);

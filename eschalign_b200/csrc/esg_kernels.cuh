@@ -52,6 +52,7 @@ constexpr int kK2Threads = kK2Warps * 32;
 constexpr int kK3Threads = 256;
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kNoRef = 0xffffffffu;
+constexpr uint32_t kMaxCap = 32;       // largest tie capacity (ESG_MAX_TIE_CAPACITY)
 
 // error bits in counters[2]
 constexpr uint32_t kErrPanelWait = 1u;
@@ -147,6 +148,14 @@ struct K2Params {
   uint32_t* redo_list;   // k3 list; redo entries go after redo_base
   uint32_t redo_base;
   uint32_t redo_cap;
+  // panel chunks: with n_chunks > 1 a task is (tile, chunk), the chunk's
+  // reference pairs are chunk_lo[c] .. chunk_lo[c + 1], and each query's
+  // partial state goes to part_head / part_ties [q * n_chunks + c] for
+  // k2_merge_chunks; with n_chunks == 1 a task is a tile over every pair
+  uint32_t n_chunks;
+  const uint32_t* chunk_lo;
+  int4* part_head;
+  uint32_t* part_ties;
   // scoring, pre-shifted by the gap open (see k2_batched)
   uint32_t tab_a[6];
   uint32_t tab_b[6];
@@ -413,6 +422,31 @@ __device__ __forceinline__ void fold_pair(const K2Params& P, int* slot, uint32_t
   }
 }
 
+// A query's state at the end of a task: its final state (and a re-score
+// request if it may have wrapped), or with panel chunks its partial state
+// for k2_merge_chunks.
+__device__ __forceinline__ void flush_query(const K2Params& P, uint32_t qid, uint32_t chunk,
+                                            const int* slot, const uint32_t* sties,
+                                            uint32_t cap) {
+  const int fl = slot[3];
+  const uint32_t nl = min((uint32_t)slot[2], cap);
+  if (P.n_chunks > 1) {
+    const size_t at = (size_t)qid * P.n_chunks + chunk;
+    P.part_head[at] = make_int4(slot[0], slot[1], slot[2], fl);
+    for (uint32_t k = 0; k < nl; ++k) P.part_ties[at * cap + k] = sties[k];
+    return;
+  }
+  P.qhead[qid] = make_int4(slot[0], slot[1], slot[2], fl);
+  for (uint32_t k = 0; k < nl; ++k) P.qties[(size_t)qid * cap + k] = sties[k];
+  if (fl & kQRedo) {
+    const uint32_t at = atomicAdd(&P.counters[1], 1u);
+    if (at < P.redo_cap)
+      P.redo_list[P.redo_base + at] = qid;
+    else
+      atomicOr(&P.counters[2], kErrRedoOverflow);
+  }
+}
+
 // One warp, one task at a time, tasks pulled from an atomic counter.  The
 // kernel is instantiated twice: kLong = false takes tiles of up to 32
 // queries whose stripes fill the warp's lanes (a query of n rows takes
@@ -465,7 +499,11 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2
     if (lane == 0) task = atomicAdd(P.task_counter, 1u);
     task = __shfl_sync(kFull, task, 0);
     if (task >= P.n_tasks) break;
-    const uint2 tk = P.tasks[task];
+    const uint32_t tile = P.n_chunks > 1 ? task / P.n_chunks : task;
+    const uint32_t chunk = task - tile * P.n_chunks;
+    const uint32_t p_lo = P.n_chunks > 1 ? P.chunk_lo[chunk] : 0u;
+    const uint32_t p_hi = P.n_chunks > 1 ? P.chunk_lo[chunk + 1] : P.n_pairs;
+    const uint2 tk = P.tasks[tile];
     const uint32_t count = tk.y & 0xffffu;
     const int smax = (int)(tk.y >> 16);
 
@@ -486,7 +524,7 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2
         slot[2] = 0;
         slot[3] = 0;
       }
-      for (uint32_t p = 0; p < P.n_pairs; ++p) {
+      for (uint32_t p = p_lo; p < p_hi; ++p) {
         const uint4 pm = pairs[p];
         const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);  // mA >= mB
         const int jshort = (mB > 0 && mB < mA) ? mB - 1 : -1;
@@ -511,19 +549,7 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2
         for (int d = 16; d; d >>= 1) acc = max16x2(acc, __shfl_xor_sync(kFull, acc, d));
         if (lane == owner) fold_pair<kLocal>(P, slot, sties, cap, pm, mB, rc, qid, acc, lr_last, bias);
       }
-      if (lane == owner) {
-        const int fl = slot[3];
-        P.qhead[qid] = make_int4(slot[0], slot[1], slot[2], fl);
-        const uint32_t nl = min((uint32_t)slot[2], cap);
-        for (uint32_t k = 0; k < nl; ++k) P.qties[(size_t)qid * cap + k] = sties[k];
-        if (fl & kQRedo) {
-          const uint32_t at = atomicAdd(&P.counters[1], 1u);
-          if (at < P.redo_cap)
-            P.redo_list[P.redo_base + at] = qid;
-          else
-            atomicOr(&P.counters[2], kErrRedoOverflow);
-        }
-      }
+      if (lane == owner) flush_query(P, qid, chunk, slot, sties, cap);
       __syncwarp();
       continue;
     } else {
@@ -577,7 +603,7 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2
       slot[3] = 0;
     }
 
-    for (uint32_t p = 0; p < P.n_pairs; ++p) {
+    for (uint32_t p = p_lo; p < p_hi; ++p) {
       const uint4 pm = pairs[p];
       const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);  // mA >= mB
       const int jshort = (mB > 0 && mB < mA) ? mB - 1 : -1;
@@ -595,20 +621,80 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2
     }
 
     // --- flush the query states of this task
-    if (last) {
-      const int fl = slot[3];
-      P.qhead[qid] = make_int4(slot[0], slot[1], slot[2], fl);
-      const uint32_t nl = min((uint32_t)slot[2], cap);
-      for (uint32_t k = 0; k < nl; ++k) P.qties[(size_t)qid * cap + k] = sties[k];
-      if (fl & kQRedo) {
-        const uint32_t at = atomicAdd(&P.counters[1], 1u);
-        if (at < P.redo_cap)
-          P.redo_list[P.redo_base + at] = qid;
-        else
-          atomicOr(&P.counters[2], kErrRedoOverflow);
-      }
-    }
+    if (last) flush_query(P, qid, chunk, slot, sties, cap);
     __syncwarp();
+    }
+  }
+}
+
+// ---------------------------------------------------------------- chunk merge
+// Two query states over disjoint candidate sets, each with its first
+// min(n_tied, cap) ties in candidate order, into one (mapper.rs:444-472
+// over the union): the higher best wins, equal bests add their tie counts
+// and merge their lists in candidate order.  `out` must not alias ta / tb.
+__device__ __forceinline__ int4 merge_state(int4 a, const uint32_t* ta, int4 b,
+                                            const uint32_t* tb, uint32_t cap, uint32_t* out) {
+  const uint32_t na = min((uint32_t)a.z, cap), nb = min((uint32_t)b.z, cap);
+  if (a.x > b.x) {
+    for (uint32_t k = 0; k < na; ++k) out[k] = ta[k];
+    return make_int4(a.x, max(max(a.y, b.y), b.x), a.z, a.w | b.w);
+  }
+  if (b.x > a.x) {
+    for (uint32_t k = 0; k < nb; ++k) out[k] = tb[k];
+    return make_int4(b.x, max(max(a.y, b.y), a.x), b.z, a.w | b.w);
+  }
+  uint32_t i = 0, j = 0, w = 0;
+  while (w < cap && (i < na || j < nb)) {
+    if (j >= nb || (i < na && ta[i] < tb[j]))
+      out[w++] = ta[i++];
+    else
+      out[w++] = tb[j++];
+  }
+  return make_int4(a.x, max(a.y, b.y), a.z + b.z, a.w | b.w);
+}
+
+struct KMParams {
+  const uint32_t* order;   // the queries k2 scored
+  uint32_t n_order;
+  uint32_t n_chunks;
+  const int4* part_head;   // [q * n_chunks + c]
+  const uint32_t* part_ties;
+  int4* qhead;
+  uint32_t* qties;
+  uint32_t cap;
+  uint32_t* counters;      // [1] redo count, [2] error bits
+  uint32_t* redo_list;
+  uint32_t redo_base;
+  uint32_t redo_cap;
+};
+
+// One thread per query: its panel chunks' partial states merged in chunk
+// order, and a re-score request where any chunk may have wrapped.
+static __global__ void __launch_bounds__(128) k2_merge_chunks(const KMParams P) {
+  uint32_t buf[2][kMaxCap];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n_order;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t q = P.order[i];
+    const size_t base = (size_t)q * P.n_chunks;
+    const uint32_t cap = P.cap;
+    int4 acc = P.part_head[base];
+    const uint32_t n0 = min((uint32_t)acc.z, cap);
+    for (uint32_t k = 0; k < n0; ++k) buf[0][k] = P.part_ties[base * cap + k];
+    int cur = 0;
+    for (uint32_t c = 1; c < P.n_chunks; ++c) {
+      const int4 b = P.part_head[base + c];
+      acc = merge_state(acc, buf[cur], b, P.part_ties + (base + c) * cap, cap, buf[cur ^ 1]);
+      cur ^= 1;
+    }
+    P.qhead[q] = acc;
+    const uint32_t nl = min((uint32_t)acc.z, cap);
+    for (uint32_t k = 0; k < nl; ++k) P.qties[(size_t)q * cap + k] = buf[cur][k];
+    if (acc.w & kQRedo) {
+      const uint32_t at = atomicAdd(&P.counters[1], 1u);
+      if (at < P.redo_cap)
+        P.redo_list[P.redo_base + at] = q;
+      else
+        atomicOr(&P.counters[2], kErrRedoOverflow);
     }
   }
 }

@@ -365,6 +365,10 @@ class GpuScorer:
     def set_split(self, split_len: int):
         _check(self._lib, self._lib.esg_scorer_set_split(self._h, int(split_len)))
 
+    def set_chunking(self, max_chunks: int):
+        """Cap the panel chunks per tile (1: every task walks the whole panel)."""
+        _check(self._lib, self._lib.esg_scorer_set_chunking(self._h, int(max_chunks)))
+
     def scores_len(self, n: int) -> bool:
         return bool(self._lib.esg_scores_len(self._h, n))
 

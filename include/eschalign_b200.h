@@ -132,6 +132,8 @@ typedef struct esg_batch_stats {
     uint32_t n_pairs;           /* paired batches: read pairs (n_reads / 2)           */
     uint32_t mates_trimmed;     /* mates with an adapter found                         */
     uint64_t bases_trimmed;     /* adapter bases removed                               */
+    uint32_t panel_chunks;      /* reference-pair chunks per tile (1: whole panel)     */
+    uint32_t reserved;
 } esg_batch_stats;
 
 typedef struct esg_scorer esg_scorer;
@@ -171,6 +173,14 @@ esg_status esg_scorer_set_kernel(esg_scorer* scorer, int32_t kernel);
 esg_status esg_scorer_autotune(esg_scorer* scorer, esg_tune_report* out);
 /* Set the 16/32-row split by hand (0: every query on 32-row stripes). */
 esg_status esg_scorer_set_split(esg_scorer* scorer, uint32_t split_len);
+
+/* Panel chunking (no counterpart in the reference): when a batch has too
+ * few 32-lane tiles to keep every resident warp busy to the end (few reads,
+ * or a large panel), each tile's reference pairs are cut into up to
+ * `max_chunks` chunks of about equal columns, one task each, and the
+ * per-chunk states are merged on the device.  1 turns it off; default 64.
+ * Scores do not depend on it. */
+esg_status esg_scorer_set_chunking(esg_scorer* scorer, uint32_t max_chunks);
 
 /* GpuScorer::scores_len (cuda/mod.rs:506-508): 1 for every len > 0 -- nothing
  * is left to a CPU path. */

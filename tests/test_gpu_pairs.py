@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 SG = (2, -1, -10, -1)
 NO_TIE = 0xFFFFFFFF
-CONFIGS = ((KERNEL_AUTO, 512), (KERNEL_AUTO, 0), (KERNEL_PLAIN32, 256))
+CONFIGS = ((KERNEL_AUTO, 512, 64), (KERNEL_AUTO, 0, 1), (KERNEL_PLAIN32, 256, 64))
 
 
 def expected(O, mates, refs, scoring, local, both, min_score, cap, max_read_len=0,
@@ -64,9 +64,10 @@ def test_fixture_pairs(oracle):
     mates = [m for n in order for m in pairs[n]]
     want = expected(oracle, mates, refs, SG, False, False, 40, 8)
     with GpuScorer(refs, Scoring(*SG), Mode.SEMIGLOBAL, tie_capacity=8) as g:
-        for kernel, split in CONFIGS:
+        for kernel, split, chunks in CONFIGS:
             g.set_kernel(kernel)
             g.set_split(split)
+            g.set_chunking(chunks)
             got = g.score_pairs(mates, adapters=adapter.config(), min_score=40,
                                 both_strands=False, full_rows=True)
             compare(got, want, 8, f"fixture kernel {kernel}/{split}")
@@ -108,9 +109,10 @@ def test_synthetic_pairs(oracle, mode, both, min_score, cap):
     local = mode == Mode.LOCAL
     want = expected(oracle, mates, refs, SG, local, both, min_score, cap)
     with GpuScorer(refs, Scoring(*SG), mode, tie_capacity=cap) as g:
-        for kernel, split in CONFIGS:
+        for kernel, split, chunks in CONFIGS:
             g.set_kernel(kernel)
             g.set_split(split)
+            g.set_chunking(chunks)
             got = g.score_pairs(mates, adapters=adapter.config(), min_score=min_score,
                                 both_strands=both, full_rows=True)
             compare(got, want, cap, f"{mode.label} both={both} min={min_score} kernel {kernel}")

@@ -35,9 +35,11 @@ def oracle_rows(O, reads, panel, scoring, local):
     return O.score_matrix(list(reads) + rc, panel, scoring, local)
 
 
-# (kernel, 16/32-row split): 16-row stripes up to 512 nt, every query on
-# 32-row stripes, the plain int32 kernel
-CONFIGS = ((KERNEL_AUTO, 512), (KERNEL_AUTO, 0), (KERNEL_PLAIN32, 256))
+# (kernel, 16/32-row split, panel chunks at most): 16-row stripes up to
+# 512 nt with the panel chunked or whole, every query on 32-row stripes
+# chunked or whole, the plain int32 kernel
+CONFIGS = ((KERNEL_AUTO, 512, 64), (KERNEL_AUTO, 512, 1), (KERNEL_AUTO, 0, 64),
+           (KERNEL_AUTO, 0, 1), (KERNEL_PLAIN32, 256, 64))
 
 
 def check(O, panel, reads, scoring, mode, what, kernels=CONFIGS, tie_capacity=CAP):
@@ -49,9 +51,10 @@ def check(O, panel, reads, scoring, mode, what, kernels=CONFIGS, tie_capacity=CA
     n = len(reads)
     stats = {}
     with GpuScorer(panel, Scoring(*scoring), mode, tie_capacity=tie_capacity) as g:
-        for kernel, split in kernels:
+        for kernel, split, chunks in kernels:
             g.set_kernel(kernel)
             g.set_split(split)
+            g.set_chunking(chunks)
             res = g.score_batch(reads, both_strands=True, full_rows=True)
             got = res.rows
             assert got.shape == want_rows.shape
@@ -65,7 +68,7 @@ def check(O, panel, reads, scoring, mode, what, kernels=CONFIGS, tie_capacity=CA
             for k in range(n):
                 nl = min(int(want_res["n_tied"][k]), tie_capacity)
                 assert (res.ties[k, :nl] == want_ties[k, :nl]).all(), (what, k, kernel)
-            stats[(kernel, split)] = res.stats
+            stats[(kernel, split, chunks)] = res.stats
             stats.setdefault(kernel, res.stats)
     return stats
 
@@ -80,6 +83,9 @@ def test_gpu_scores_equal_scalar_random_panel(oracle):
         for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
             st = check(oracle, panel, reads, scoring, mode, "random 37-ref panel")
             assert st[KERNEL_AUTO]["queries_batched"] == 2 * len(reads)
+            # a small batch cuts the panel into chunks, unless told not to
+            assert st[(KERNEL_AUTO, 512, 64)]["panel_chunks"] > 1
+            assert st[(KERNEL_AUTO, 512, 1)]["panel_chunks"] == 1
 
 
 def test_gpu_scores_equal_scalar_wide_panel(oracle):
@@ -112,9 +118,10 @@ def test_gpu_golden_pairs(oracle):
         q, r = encode(c["query"]), encode(c["reference"])
         mode = Mode.LOCAL if c["mode"] == "local" else Mode.SEMIGLOBAL
         with GpuScorer([r], Scoring(*c["scheme"]), mode) as s:
-            for kernel, split in CONFIGS:
+            for kernel, split, chunks in CONFIGS:
                 s.set_kernel(kernel)
                 s.set_split(split)
+                s.set_chunking(chunks)
                 res = s.score_batch([q], full_rows=True)
                 assert res.rows[0, 0] == c["score"], (c["name"], c["mode"], kernel, split)
 
@@ -200,13 +207,16 @@ def test_gpu_int16_saturation_is_rescored_in_int32(oracle):
     40 000-50 000.  The batched kernel flags them and the int32 kernel
     re-scores them; results equal the oracle's int32 scores."""
     rng = Rng(0x5EED_0105)
-    letters = random_panel(rng, 9, 480, 40)
+    letters = random_panel(rng, 40, 480, 40)
     panel = [encode(s) for s in letters]
     reads = [encode(letters[k][:400 + 10 * k]) for k in range(9)]
     reads += [encode(random_seq(rng, 300, 0.0)) for _ in range(5)]
     scoring = (100, -100, -27, -27)
     st = check(oracle, panel, reads, scoring, Mode.LOCAL, "saturating")
-    assert st[KERNEL_AUTO]["queries_rescored"] >= 9
+    for key in ((KERNEL_AUTO, 512, 64), (KERNEL_AUTO, 512, 1), (KERNEL_AUTO, 0, 64)):
+        assert st[key]["queries_rescored"] >= 9, key
+    # the re-score requests also come through the panel-chunk merge
+    assert st[(KERNEL_AUTO, 512, 64)]["panel_chunks"] > 1
     assert st[KERNEL_AUTO]["queries_batched"] == 2 * len(reads)
     st = check(oracle, panel, reads, scoring, Mode.SEMIGLOBAL, "saturating semi-global")
     assert st[KERNEL_AUTO]["queries_plain"] == 2 * len(reads)
