@@ -15,8 +15,8 @@ other three (mode, scheme) combinations are measured once each.
             kernel with the batch resident on the device, CUDA events on the
             launching stream, L2 flushed between steps, max over ranks.
 * e2e       the same metric through the public API with host buffers: the
-            batch fed in chunks through prepare / submit / finish,
-            double-buffered like eschalign's GPU feeder thread
+            batch fed in chunks through prepare / submit / finish, two
+            batches in flight, like eschalign's GPU feeder thread
             (crates/eschalign-cli/src/align.rs:2801-2917), host<->device
             copies inside the timed region.
 * roofline  integer ALU: the batched kernel's algorithmic work (12 int ops a
@@ -351,27 +351,49 @@ class Ctx:
 
 
 def feeder(ctx, chunks, prepare, submit, finish, steps):
-    """Double-buffered prepare / submit / finish over host chunks (the GPU
-    feeder thread of crates/eschalign-cli/src/align.rs:2801-2917); returns
-    (seconds of the timed passes, h2d bytes, d2h bytes per pass).  The first
-    pass warms the pinned pool and the allocator and is not timed."""
+    """prepare / submit / finish over host chunks, like the GPU feeder thread
+    of crates/eschalign-cli/src/align.rs:2801-2917, with two batches in
+    flight: chunk k + 1 is prepared and queued before chunk k is waited for,
+    so the device never drains between chunks.  Returns (seconds of the
+    timed passes, passes, h2d bytes, d2h bytes per pass); the host time split
+    is left in feeder.last_split.  The first pass warms the pinned pool and
+    the allocator and is not timed."""
     times, h2d, d2h = [], 0, 0
+    host = {"prepare_s": 0.0, "submit_s": 0.0, "finish_s": 0.0}
+    pc = time.perf_counter
     for it in range(steps + 1):
         ctx.barrier()
-        t0 = time.perf_counter()
-        pending = None
+        t0 = pc()
+        inflight = []
         h2d = d2h = 0
-        for c in chunks + [None]:
-            prepared = prepare(c) if c is not None else None
-            if pending is not None:
-                st = finish(pending)
-                h2d += st["h2d_bytes"]
-                d2h += st["d2h_bytes"]
-            pending = submit(prepared) if prepared is not None else None
+        split = {"prepare_s": 0.0, "submit_s": 0.0, "finish_s": 0.0}
+
+        def done(b):
+            nonlocal h2d, d2h
+            a = pc()
+            st = finish(b)
+            split["finish_s"] += pc() - a
+            h2d += st["h2d_bytes"]
+            d2h += st["d2h_bytes"]
+
+        for c in chunks:
+            a = pc()
+            prepared = prepare(c)
+            b = pc()
+            inflight.append(submit(prepared))
+            split["prepare_s"] += b - a
+            split["submit_s"] += pc() - b
+            if len(inflight) > 1:
+                done(inflight.pop(0))
+        while inflight:
+            done(inflight.pop(0))
         ctx.torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
+        dt = pc() - t0
         if it > 0:
             times.append(dt)
+            for k in host:
+                host[k] += split[k] / steps
+    feeder.last_split = {k: round(v, 4) for k, v in host.items()}
     return ctx.max_over_ranks(sum(times)), len(times), h2d, d2h
 
 
@@ -462,7 +484,8 @@ def run_c2(a, ctx, rank):
         lambda b: g.finish(b).stats, max(1, min(2, a.steps)))
     e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "reads_per_s": world * len(reads) * n_pass / te, "chunk_reads": a.chunk}
+           "reads_per_s": world * len(reads) * n_pass / te, "chunk_reads": a.chunk,
+           "host_seconds_per_pass": feeder.last_split}
     g.close()
 
     cpu = None
@@ -523,7 +546,8 @@ def run_c4(a, ctx, rank):
         g.submit, lambda b: g.finish_pairs(b).stats, max(1, min(2, a.steps)))
     e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "pairs_per_s": world * n_pairs * n_pass / te, "chunk_pairs": step_pairs}
+           "pairs_per_s": world * n_pairs * n_pass / te, "chunk_pairs": step_pairs,
+           "host_seconds_per_pass": feeder.last_split}
     g.close()
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

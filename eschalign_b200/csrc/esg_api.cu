@@ -132,6 +132,9 @@ struct esg_scorer {
   bool tuned = false;
   uint32_t max_chunks = 64;  // panel chunks per tile at most (1: never chunk)
   cudaStream_t aux = nullptr;          // second stream: the long-query kernel
+  // batches' device memory: a pool of this scorer's own that keeps what
+  // finished batches return, so the next batch maps no new memory
+  cudaMemPool_t pool = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   // k3 panel (longest first)
   uint8_t* d_rcodes = nullptr;
@@ -591,6 +594,18 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
       (e = cudaEventCreateWithFlags(&sc->fork, cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&sc->join, cudaEventDisableTiming)) != cudaSuccess)
     return cleanup(cuda_fail(e, "cudaStreamCreate(aux)"));
+  {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if ((e = cudaMemPoolCreate(&sc->pool, &props)) != cudaSuccess)
+      return cleanup(cuda_fail(e, "cudaMemPoolCreate"));
+    uint64_t keep = UINT64_MAX;
+    if ((e = cudaMemPoolSetAttribute(sc->pool, cudaMemPoolAttrReleaseThreshold, &keep)) !=
+        cudaSuccess)
+      return cleanup(cuda_fail(e, "cudaMemPoolSetAttribute"));
+  }
   int occ16 = 0, occ32 = 0, occl = 0, occ3 = 0;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ16, sc->k2_t16, kK2Threads,
                                                          sc->k2_smem)) != cudaSuccess ||
@@ -666,6 +681,7 @@ void esg_scorer_free(esg_scorer* sc) {
   }
   if (sc->fork) cudaEventDestroy(sc->fork);
   if (sc->join) cudaEventDestroy(sc->join);
+  if (sc->pool) cudaMemPoolDestroy(sc->pool);
   if (sc->own_stream && sc->stream) cudaStreamDestroy(sc->stream);
   delete sc;
 }
@@ -1180,7 +1196,7 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   };
   size_t total = 0;
   for (size_t v : sizes) total += v;
-  ESG_CUDA(cudaMallocAsync(&b->d_mem, total, st));
+  ESG_CUDA(cudaMallocFromPoolAsync(&b->d_mem, total, sc->pool, st));
   b->d_bytes = total;
   char* at = (char*)b->d_mem;
   b->d_codes = carve<uint8_t>(at, b->total_bases ? b->total_bases : 1);

@@ -300,64 +300,100 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[R],
   // path needs the per-lane bound (its lanes past the query's last stripe)
   const int mlim = (kLong && !active_lane) ? 0 : m;
 
-#pragma unroll 1
-  for (int t = 0; t < steps; ++t) {
-    const int j = t - skew;
-    uint32_t gt = __shfl_up_sync(kFull, gbot, 1);
-    uint32_t ft = __shfl_up_sync(kFull, fbot, 1);
+  // One column of the lane's stripe, given the top input (G, F of the row
+  // above at this column).
+  auto column = [&](int j, uint32_t gt, uint32_t ft) {
+    if constexpr (kLong) {
+      if (from_buf && lane == 0) {
+        const uint2 b = buf[j];
+        gt = b.x;
+        ft = b.y;
+      }
+    }
+    const uint32_t sel = load_sel<kSmem>(sp, j);
+    uint32_t gd = gdc;
+    gdc = gt;
+    uint32_t gup = gt, f = ft, h15 = 0, hprev = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const uint32_t sc = prmt(ta[r], tb[kPanelW ? r : 0], sel);
+      ev[r] = __viaddmax_s16x2(ev[r], K.e2, g[r]);
+      f = __viaddmax_s16x2(f, K.e2, gup);
+      const uint32_t h1 = __viaddmax_s16x2(gd, sc, ev[r]);
+      uint32_t h;
+      if constexpr (kLocal) {
+        h = __vimax3_s16x2(h1, f, K.bias2);
+        if (r & 1)
+          best = __vimax3_s16x2(best, hprev, h);
+        else
+          hprev = h;
+      } else {
+        h = max16x2(h1, f);
+      }
+      gd = g[r];
+      g[r] = mad_lo(h, K.one, K.o32);
+      gup = g[r];
+      if (r == R - 1) h15 = h;
+    }
+    gbot = g[R - 1];
+    fbot = f;
+    if constexpr (kLong) {
+      if (to_buf && lane == 31) buf[j] = make_uint2(gbot, fbot);
+    }
+    if constexpr (!kLocal) {
+      lastrow = max16x2(lastrow, h15);
+      if (j == jshort) {
+        uint32_t cm = K.neg2;
+#pragma unroll
+        for (int r = 0; r < R; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
+        s_col = cm;
+        s_last = lastrow;
+      }
+    }
+  };
+  // The top input: the previous lane's bottom row of the previous step, or
+  // the border for a query's first lane.
+  auto top = [&](uint32_t& gt, uint32_t& ft) {
+    gt = __shfl_up_sync(kFull, gbot, 1);
+    ft = __shfl_up_sync(kFull, fbot, 1);
     if (first) {
       gt = K.g0;
       ft = K.neg2;
     }
-    if ((unsigned)j < (unsigned)mlim) {
-      if constexpr (kLong) {
-        if (from_buf && lane == 0) {
-          const uint2 b = buf[j];
-          gt = b.x;
-          ft = b.y;
-        }
+  };
+
+  int t = 0;
+  if constexpr (kLocal && !kLong) {
+    // Steps fill .. m - 1, where fill = steps - m is the tile's largest skew,
+    // have every lane of the tile's queries inside the pair's columns: they
+    // run without the column check.  Lanes past the tile's queries take
+    // skew 0 there (columns in range, values nobody reads: only later lanes,
+    // also past the queries, see them).
+    const int fill = steps - m;
+    if (fill < m) {
+#pragma unroll 1
+      for (; t < fill; ++t) {
+        uint32_t gt, ft;
+        top(gt, ft);
+        const int j = t - skew;
+        if ((unsigned)j < (unsigned)mlim) column(j, gt, ft);
       }
-      const uint32_t sel = load_sel<kSmem>(sp, j);
-      uint32_t gd = gdc;
-      gdc = gt;
-      uint32_t gup = gt, f = ft, h15 = 0, hprev = 0;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const uint32_t sc = prmt(ta[r], tb[kPanelW ? r : 0], sel);
-        ev[r] = __viaddmax_s16x2(ev[r], K.e2, g[r]);
-        f = __viaddmax_s16x2(f, K.e2, gup);
-        const uint32_t h1 = __viaddmax_s16x2(gd, sc, ev[r]);
-        uint32_t h;
-        if constexpr (kLocal) {
-          h = __vimax3_s16x2(h1, f, K.bias2);
-          if (r & 1)
-            best = __vimax3_s16x2(best, hprev, h);
-          else
-            hprev = h;
-        } else {
-          h = max16x2(h1, f);
-        }
-        gd = g[r];
-        g[r] = mad_lo(h, K.one, K.o32);
-        gup = g[r];
-        if (r == R - 1) h15 = h;
-      }
-      gbot = g[R - 1];
-      fbot = f;
-      if constexpr (kLong) {
-        if (to_buf && lane == 31) buf[j] = make_uint2(gbot, fbot);
-      }
-      if constexpr (!kLocal) {
-        lastrow = max16x2(lastrow, h15);
-        if (j == jshort) {
-          uint32_t cm = K.neg2;
-#pragma unroll
-          for (int r = 0; r < R; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
-          s_col = cm;
-          s_last = lastrow;
-        }
+      const int sk = active_lane ? skew : 0;
+      constexpr int kUnroll = R <= 16 ? 2 : 1;  // 32-row stripes: no registers to spare
+#pragma unroll kUnroll
+      for (; t < m; ++t) {
+        uint32_t gt, ft;
+        top(gt, ft);
+        column(t - sk, gt, ft);
       }
     }
+  }
+#pragma unroll 1
+  for (; t < steps; ++t) {
+    uint32_t gt, ft;
+    top(gt, ft);
+    const int j = t - skew;
+    if ((unsigned)j < (unsigned)mlim) column(j, gt, ft);
   }
   if constexpr (kLocal) {
     v = best;

@@ -160,6 +160,11 @@ int32_t esg_fits_i16(uint64_t len, uint64_t max_ref_len, const esg_scoring* scor
 esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64_t* ref_off,
                           const uint32_t* ref_len, uint32_t n_refs, const esg_scoring* scoring,
                           int32_t mode, const esg_options* options, esg_scorer** out);
+/* Frees the scorer and the device memory its batches used: batches take
+ * their device memory from a pool the scorer owns, which keeps what a freed
+ * batch returns for the next one (device memory in use grows to the largest
+ * set of batches alive at once and is returned here).  Free every batch
+ * first. */
 void esg_scorer_free(esg_scorer* scorer);
 
 esg_status esg_scorer_info(const esg_scorer* scorer, esg_info* out);
