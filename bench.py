@@ -62,10 +62,11 @@ COMBOS = [((2, -1, -10, -1), "local"), ((2, -1, -10, -1), "semiglobal"),
 OPS_PER_CELL = {"local": 12, "semiglobal": 11}
 C4_SCORING = (2, -1, -10, -1)
 C3_SCORING = (2, -1, -10, -1)
-# DRAM bytes per DP cell of the batched kernel: 3.22 MB over 9.71e10 cells in
-# the ncu capture of a 20 000-read C2 launch (profiles/k2_batched_c2.md);
-# traffic grows with the reads, so it scales by cells to the full launch.
-K2_DRAM_BYTES_PER_CELL = 3.22e6 / 9.7056e10
+# DRAM bytes per DP cell of the batched kernel: 8.29 MB read, 0 written, over
+# the 2.678e11 cells of the 16-row launch in the ncu capture of a 60 000-read
+# C2 case (profiles/k2_batched_c2.md); the traffic is the reads' codes and
+# the plan, which grow with the reads, so it scales by cells to a full launch.
+K2_DRAM_BYTES_PER_CELL = 8.288256e6 / 2.67805237160e11
 
 
 def env_int(name, default):
@@ -96,6 +97,9 @@ def args_parse():
     ap.add_argument("--pair-chunk", type=int, default=125_000,
                     help="c4: pairs per prepare/submit/finish batch in the e2e feeder")
     ap.add_argument("--c3-reads", type=int, default=4000, help="c3: reads per step")
+    ap.add_argument("--split", type=int, default=-1,
+                    help="16/32-row split in nt, set instead of autotuning (for runs under a "
+                         "profiler, whose serialised launches would skew the autotuner)")
     return ap.parse_args()
 
 
@@ -397,6 +401,14 @@ def feeder(ctx, chunks, prepare, submit, finish, steps):
     return ctx.max_over_ranks(sum(times)), len(times), h2d, d2h
 
 
+def tune(g, a):
+    """The autotuner's report, or the pinned split (--split)."""
+    if a.split >= 0:
+        g.set_split(a.split)
+        return {"split_len": a.split, "pinned": True}
+    return g.autotune()
+
+
 def common_line(a, ctx, value, ms_per_step, workload, extra_config, e2e, roofline, clocks,
                 launches, dtype="int16x2"):
     return {
@@ -421,6 +433,8 @@ def run_c2(a, ctx, rank):
         for kernel in (KERNEL_AUTO, KERNEL_PLAIN32):
             g = GpuScorer(refs, Scoring(*HEADLINE[0]), Mode.parse(a.mode), device=local_rank,
                           kernel=kernel)
+            if a.split >= 0:
+                g.set_split(a.split)
             r = g.score_batch(reads.tuple(), both_strands=True)
             print(json.dumps({"profile_case": a.profile_case, "kernel": kernel,
                               "stats": r.stats}), flush=True)
@@ -431,7 +445,7 @@ def run_c2(a, ctx, rank):
     scoring, mode = HEADLINE
     g = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank,
                   stream=ctx.stream.cuda_stream)
-    tune = g.autotune()  # tile shape for this panel, before any timing
+    tune_rep = tune(g, a)  # tile shape for this panel, before any timing
     info = g.info()
     batch = g.submit(g.prepare(reads.tuple(), both_strands=True))
     st = g.finish(batch, keep=True).stats
@@ -456,7 +470,7 @@ def run_c2(a, ctx, rank):
         for sc_, md in COMBOS[1:]:
             g2 = GpuScorer(refs, Scoring(*sc_), Mode.parse(md), device=local_rank,
                            stream=ctx.stream.cuda_stream)
-            g2.autotune()
+            tune(g2, a)
             b2 = g2.submit(g2.prepare(reads.tuple(), both_strands=True))
             r2 = g2.finish(b2, keep=True)
             t2 = ctx.max_over_ranks(ctx.device_time(g2, b2, 1, 1))
@@ -505,7 +519,7 @@ def run_c2(a, ctx, rank):
         line["kernel_info"] = {k: info[k] for k in (
             "regs_batched", "regs_plain", "local_bytes_batched", "batched_blocks",
             "panel_bytes", "sm_count", "split_len")}
-        line["autotune"] = tune
+        line["autotune"] = tune_rep
         line["batch_stats"] = {k: st[k] for k in ("queries_batched", "queries_plain",
                                                   "queries_rescored", "tasks", "lanes_used")}
         if cpu:
@@ -527,7 +541,7 @@ def run_c4(a, ctx, rank):
     cfg = adapter.config()
     g = GpuScorer(refs, Scoring(*C4_SCORING), Mode.SEMIGLOBAL, device=local_rank,
                   stream=ctx.stream.cuda_stream)
-    tune = g.autotune()
+    tune_rep = tune(g, a)
     batch = g.submit(g.prepare_pairs(pairs.tuple(), adapters=cfg, both_strands=True))
     st = g.finish_pairs(batch, keep=True).stats
     cells = st["cells"]
@@ -566,7 +580,7 @@ def run_c4(a, ctx, rank):
             e2e, roofline, clocks, st["kernels"] * a.steps)
         line["pairs_per_s"] = world * n_pairs * a.steps / t_max
         line["reads_per_s"] = 2 * line["pairs_per_s"]
-        line["autotune"] = tune
+        line["autotune"] = tune_rep
         line["batch_stats"] = {k: st[k] for k in ("queries_batched", "queries_plain",
                                                   "queries_rescored", "tasks", "lanes_used",
                                                   "kernels")}
@@ -584,7 +598,7 @@ def run_c3(a, ctx, rank):
     reads = synth.reads_c3(refs, n=a.c3_reads)
     g = GpuScorer(refs, Scoring(*C3_SCORING), Mode.LOCAL, device=local_rank,
                   stream=ctx.stream.cuda_stream)
-    tune = g.autotune()
+    tune_rep = tune(g, a)
     info = g.info()
     batch = g.submit(g.prepare(reads.tuple(), both_strands=True))
     st = g.finish(batch, keep=True).stats
@@ -616,7 +630,7 @@ def run_c3(a, ctx, rank):
             {"reads": len(reads), "refs": len(refs), "panel_bases": panel_bases,
              "cells_per_step": cells},
             e2e, roofline, clocks, st["kernels"] * a.steps)
-        line["autotune"] = tune
+        line["autotune"] = tune_rep
         line["kernel_info"] = {k: info[k] for k in ("panel_bytes", "split_len",
                                                     "batched_blocks")}
         line["batch_stats"] = {k: st[k] for k in ("queries_batched", "queries_plain",
