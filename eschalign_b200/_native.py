@@ -48,7 +48,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     """Compile csrc/esg_api.cu into libeschalign_b200.so and the integer-pipe
     probe csrc/esg_probe.cu into libesg_probe.so (sm_100a, ahead of time)."""
     newest = max(os.path.getmtime(s) for s in sources())
-    for src, out in ((("esg_api.cu", "esg_noalloc.cu"), LIB_PATH), ("esg_probe.cu", PROBE_PATH)):
+    for src, out in ((("esg_api.cu", "esg_server.cu", "esg_noalloc.cu"), LIB_PATH),
+                     ("esg_probe.cu", PROBE_PATH)):
         if force or not os.path.exists(out) or os.path.getmtime(out) < newest:
             _compile(src, out, verbose)
     return LIB_PATH
@@ -102,13 +103,31 @@ class EsgBatchStats(C.Structure):
                 ("lanes_used", C.c_uint32), ("kernels", C.c_uint32), ("cells", C.c_uint64),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("n_pairs", C.c_uint32),
                 ("mates_trimmed", C.c_uint32), ("bases_trimmed", C.c_uint64),
-                ("panel_chunks", C.c_uint32), ("reserved", C.c_uint32)]
+                ("panel_chunks", C.c_uint32), ("reserved", C.c_uint32),
+                ("device_bytes", C.c_uint64)]
 
 
 class EsgAdapterConfig(C.Structure):
     _fields_ = [("r1", C.c_void_p), ("r1_len", C.c_uint32), ("r2", C.c_void_p),
                 ("r2_len", C.c_uint32), ("min_overlap", C.c_uint32),
                 ("max_read_len", C.c_uint32)]
+
+
+class EsgServerOptions(C.Structure):
+    _fields_ = [("max_batch_reads", C.c_uint32), ("max_inflight", C.c_uint32),
+                ("memory_budget", C.c_uint64), ("memory_headroom", C.c_uint64)]
+
+
+class EsgRequestTiming(C.Structure):
+    _fields_ = [("queued_ms", C.c_double), ("total_ms", C.c_double),
+                ("batch_reads", C.c_uint32), ("batch_requests", C.c_uint32)]
+
+
+class EsgServerStats(C.Structure):
+    _fields_ = [("requests", C.c_uint64), ("completed", C.c_uint64), ("refused", C.c_uint64),
+                ("batches", C.c_uint64), ("cells", C.c_uint64), ("bytes_in_flight", C.c_uint64),
+                ("peak_bytes_in_flight", C.c_uint64), ("admission_waits", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 # every entry point include/eschalign_b200.h declares: name -> (restype, argtypes)
@@ -151,6 +170,14 @@ SIGNATURES = {
     "esg_score_pairs": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32,
                                     C.POINTER(EsgAdapterConfig), C.c_int32, C.c_uint32,
                                     C.c_void_p, _u32p, C.c_void_p, _u32p, _u32p, _i32p]),
+    "esg_server_new": (C.c_int32, [C.POINTER(EsgServerOptions), C.POINTER(C.c_void_p)]),
+    "esg_server_add_scorer": (C.c_int32, [C.c_void_p, C.c_void_p, _u32p]),
+    "esg_server_submit": (C.c_int32, [C.c_void_p, C.c_uint32, _u8p, _u64p, _u32p, C.c_uint32,
+                                      C.c_uint32, _u64p]),
+    "esg_server_wait": (C.c_int32, [C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p, _u32p,
+                                    C.POINTER(EsgRequestTiming)]),
+    "esg_server_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(EsgServerStats)]),
+    "esg_server_free": (None, [C.c_void_p]),
     "esg_score_rows_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_uint32, C.POINTER(EsgScoring), C.c_int32,

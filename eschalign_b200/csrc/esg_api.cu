@@ -8,6 +8,7 @@
 // query is scored on the GPU -- nothing is left unscored for a CPU path --
 // and the per-read best / XS / tie reduction runs there too.
 #include "../../include/eschalign_b200.h"
+#include "esg_internal.h"
 #include "esg_kernels.cuh"
 
 #include <algorithm>
@@ -807,18 +808,24 @@ esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
 }
 
 // ---------------------------------------------------------------- prepare
-esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
-                       const uint32_t* len, uint32_t n_reads, uint32_t flags, esg_batch** out) {
+}  // extern "C"
+
+// The planning half of esg_prepare.  Read k is `ptrs[k]` when `ptrs` is
+// given (reads gathered from several requests), else codes + off[k].
+static esg_status prepare_impl(esg_scorer* sc, const uint8_t* const* ptrs, const uint8_t* codes,
+                               const uint64_t* off, const uint32_t* len, uint32_t n_reads,
+                               uint32_t flags, esg_batch** out) {
   g_err.clear();
   if (!sc || !out) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer or out");
   *out = nullptr;
   if (flags & ~(ESG_BOTH_STRANDS | ESG_FULL_ROWS))
     return fail(ESG_ERR_BAD_ARGUMENT, "unknown flags 0x%x", flags);
-  if (n_reads && (!off || !len)) return fail(ESG_ERR_BAD_ARGUMENT, "off/len must not be NULL");
+  if (n_reads && (!(off || ptrs) || !len))
+    return fail(ESG_ERR_BAD_ARGUMENT, "off/len must not be NULL");
   if (n_reads >= (1u << 30)) return fail(ESG_ERR_BAD_ARGUMENT, "too many reads (%u)", n_reads);
   uint64_t total = 0;
   for (uint32_t k = 0; k < n_reads; ++k) total += len[k];
-  if (total && !codes) return fail(ESG_ERR_BAD_ARGUMENT, "codes must not be NULL");
+  if (total && !codes && !ptrs) return fail(ESG_ERR_BAD_ARGUMENT, "codes must not be NULL");
 
   auto* b = new esg_batch();
   b->owner = sc;
@@ -928,7 +935,7 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   for (uint32_t k = 0; k < n_reads; ++k) {
     b->h_off[k] = pos;
     b->h_len[k] = len[k];
-    if (len[k]) memcpy(b->h_codes + pos, codes + off[k], len[k]);
+    if (len[k]) memcpy(b->h_codes + pos, ptrs ? ptrs[k] : codes + off[k], len[k]);
     pos += len[k];
   }
   // order[] and tasks[] laid out [long | 32-row tiles | 16-row tiles];
@@ -963,6 +970,66 @@ esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off
   b->stats.cells = cells;
   *out = b;
   return ESG_OK;
+}
+
+esg_status esg_internal_prepare_ptrs(esg_scorer* sc, const uint8_t* const* reads,
+                                     const uint32_t* len, uint32_t n_reads, uint32_t flags,
+                                     esg_batch** out) {
+  return prepare_impl(sc, reads, nullptr, nullptr, len, n_reads, flags, out);
+}
+
+size_t esg_internal_pool_spare(esg_scorer* sc) {
+  if (!sc || !sc->pool) return 0;
+  cudaSetDevice(sc->device);
+  uint64_t reserved = 0, used = 0;
+  if (cudaMemPoolGetAttribute(sc->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) !=
+          cudaSuccess ||
+      cudaMemPoolGetAttribute(sc->pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+    return 0;
+  return reserved > used ? (size_t)(reserved - used) : 0;
+}
+
+int esg_internal_device(const esg_scorer* sc) { return sc ? sc->device : 0; }
+
+uint32_t esg_internal_tie_capacity(const esg_scorer* sc) { return sc ? sc->cap : 0; }
+
+extern "C" {
+
+esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                       const uint32_t* len, uint32_t n_reads, uint32_t flags, esg_batch** out) {
+  return prepare_impl(sc, nullptr, codes, off, len, n_reads, flags, out);
+}
+
+// Device bytes of a batch: the one allocation esg_submit carves (and the
+// figure admission control weighs).
+static size_t batch_device_bytes(const esg_scorer* sc, const esg_batch* b) {
+  const bool dev_rows = (b->flags & ESG_FULL_ROWS) || b->paired;
+  const size_t np = b->paired ? std::max<uint32_t>(b->n_pairs, 1) : 0;
+  const uint32_t nlist = b->host_list + b->redo_cap;
+  const size_t nr = b->n_reads ? b->n_reads : 1, nq = b->n_q ? b->n_q : 1;
+  const size_t sizes[] = {
+      carve_size(b->total_bases ? b->total_bases : 1, 1),
+      carve_size(nr, 8),
+      carve_size(nr, 4),
+      carve_size(b->n_order ? b->n_order : 1, 4),
+      carve_size(b->n_tasks ? b->n_tasks : 1, 8),
+      carve_size(nlist ? nlist : 1, 4),
+      carve_size(b->n_chunks + 1, 4),
+      carve_size(8, 4),
+      carve_size(nq, 16),
+      carve_size(nq * sc->cap, 4),
+      carve_size(nlist ? (size_t)nlist * sc->n_refs : 1, 4),
+      carve_size(nr, 16),
+      carve_size(nr * sc->cap, 4),
+      dev_rows ? carve_size(nq * sc->n_refs, 4) : 0,
+      carve_size(2 * np, 16),
+      carve_size(np * sc->cap, 4),
+      b->n_chunks > 1 ? carve_size(nq * b->n_chunks, 16) : 0,
+      b->n_chunks > 1 ? carve_size(nq * b->n_chunks * sc->cap, 4) : 0,
+  };
+  size_t total = 0;
+  for (size_t v : sizes) total += v;
+  return total;
 }
 
 // ---------------------------------------------------------------- device work
@@ -1174,28 +1241,7 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   const uint32_t nlist = b->host_list + b->redo_cap;
   const size_t nr = b->n_reads ? b->n_reads : 1, nq = b->n_q ? b->n_q : 1;
   // device buffers, one stream-ordered allocation
-  size_t sizes[] = {
-      carve_size(b->total_bases ? b->total_bases : 1, 1),
-      carve_size(nr, 8),
-      carve_size(nr, 4),
-      carve_size(b->n_order ? b->n_order : 1, 4),
-      carve_size(b->n_tasks ? b->n_tasks : 1, 8),
-      carve_size(nlist ? nlist : 1, 4),
-      carve_size(b->n_chunks + 1, 4),
-      carve_size(8, 4),
-      carve_size(nq, 16),
-      carve_size(nq * sc->cap, 4),
-      carve_size(nlist ? (size_t)nlist * sc->n_refs : 1, 4),
-      carve_size(nr, 16),
-      carve_size(nr * sc->cap, 4),
-      dev_rows ? carve_size(nq * sc->n_refs, 4) : 0,
-      carve_size(2 * np, 16),
-      carve_size(np * sc->cap, 4),
-      b->n_chunks > 1 ? carve_size(nq * b->n_chunks, 16) : 0,
-      b->n_chunks > 1 ? carve_size(nq * b->n_chunks * sc->cap, 4) : 0,
-  };
-  size_t total = 0;
-  for (size_t v : sizes) total += v;
+  const size_t total = batch_device_bytes(sc, b);
   ESG_CUDA(cudaMallocFromPoolAsync(&b->d_mem, total, sc->pool, st));
   b->d_bytes = total;
   char* at = (char*)b->d_mem;
@@ -1309,6 +1355,7 @@ void esg_batch_free(esg_batch* b) {
 esg_status esg_batch_stats_get(const esg_batch* b, esg_batch_stats* out) {
   if (!b || !out) return fail(ESG_ERR_BAD_ARGUMENT, "NULL argument");
   *out = b->stats;
+  if (b->owner) out->device_bytes = batch_device_bytes(b->owner, b);
   return ESG_OK;
 }
 

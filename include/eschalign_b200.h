@@ -134,6 +134,7 @@ typedef struct esg_batch_stats {
     uint64_t bases_trimmed;     /* adapter bases removed                               */
     uint32_t panel_chunks;      /* reference-pair chunks per tile (1: whole panel)     */
     uint32_t reserved;
+    uint64_t device_bytes;      /* device memory the batch takes while submitted       */
 } esg_batch_stats;
 
 typedef struct esg_scorer esg_scorer;
@@ -296,6 +297,69 @@ esg_status esg_score_pairs(esg_scorer* scorer, const uint8_t* codes, const uint6
                            const esg_adapter_config* adapters, int32_t min_score, uint32_t flags,
                            esg_pair_result* pairs, uint32_t* pair_ties, esg_read_result* mates,
                            uint32_t* mate_ties, uint32_t* adapter_bases, int32_t* rows);
+
+/* ---- serving: a request queue over resident scorers.  No counterpart in
+ * the reference, which scores batches of one stream of reads and has no
+ * serving mode.  Requests name a scorer slot (a resident panel under one
+ * scoring and mode) and a strand flag; each slot's worker thread batches
+ * whatever requests of that slot are waiting (continuous batching: up to
+ * max_batch_reads reads per batch, max_inflight batches queued on the
+ * scorer's stream) and admits a batch only when its device memory fits the
+ * free device memory (cudaMemGetInfo, plus what the scorer's pool holds
+ * spare) less a headroom, and the budget if one is set.  A request that can
+ * never fit is refused with ESG_ERR_OUT_OF_MEMORY.  Results are the ones
+ * esg_score_batch gives for the same reads alone. */
+typedef struct esg_server esg_server;
+
+typedef struct esg_server_options {
+    uint32_t max_batch_reads;  /* reads per batch at most (0: 262144); a larger request runs alone */
+    uint32_t max_inflight;     /* batches queued per scorer (0: 2)                               */
+    uint64_t memory_budget;    /* device bytes of admitted batches at most (0: free memory only) */
+    uint64_t memory_headroom;  /* device bytes admission leaves free (0: 256 MiB)                */
+} esg_server_options;
+
+typedef struct esg_request_timing {
+    double queued_ms;          /* submit -> its batch went to the device                         */
+    double total_ms;           /* submit -> its results were ready                               */
+    uint32_t batch_reads;      /* reads of the batch it rode in                                  */
+    uint32_t batch_requests;   /* requests of that batch                                         */
+} esg_request_timing;
+
+typedef struct esg_server_stats {
+    uint64_t requests;         /* submitted                                                      */
+    uint64_t completed;        /* results ready (scored or failed)                               */
+    uint64_t refused;          /* refused by admission (could never fit)                         */
+    uint64_t batches;          /* batches run                                                    */
+    uint64_t cells;            /* DP cells of the batches run                                    */
+    uint64_t bytes_in_flight;  /* device bytes of admitted batches now                           */
+    uint64_t peak_bytes_in_flight;
+    uint32_t admission_waits;  /* times a batch waited for device memory                         */
+    uint32_t reserved;
+} esg_server_stats;
+
+esg_status esg_server_new(const esg_server_options* options, esg_server** out);
+/* Add a resident scorer as slot *slot (its worker starts).  The server does
+ * not own the scorer: free the server first.  Use the scorer only through
+ * the server afterwards. */
+esg_status esg_server_add_scorer(esg_server* server, esg_scorer* scorer, uint32_t* slot);
+/* Queue a request (thread-safe): the reads are copied, the caller's buffers
+ * may be reused on return.  flags: 0 or ESG_BOTH_STRANDS. */
+esg_status esg_server_submit(esg_server* server, uint32_t slot, const uint8_t* codes,
+                             const uint64_t* off, const uint32_t* len, uint32_t n_reads,
+                             uint32_t flags, uint64_t* ticket);
+/* Wait up to timeout_ms (< 0: no limit; a host-side wait) for a request; on success copy its
+ * results (n_reads entries) and ties (n_reads * tie_capacity; any pointer
+ * may be NULL) and release the ticket.  ESG_ERR_TIMEOUT leaves the request
+ * queued (wait again); any other error is the request's own status (its
+ * ticket released). */
+esg_status esg_server_wait(esg_server* server, uint64_t ticket, int32_t timeout_ms,
+                           esg_read_result* results, uint32_t* ties, esg_request_timing* timing);
+esg_status esg_server_stats_get(esg_server* server, esg_server_stats* out);
+/* Stop: each worker finishes its batches on the device and fails the
+ * requests still queued; then the workers are joined and the server freed.
+ * Call it once no other thread is inside esg_server_submit / _wait;
+ * requests nobody waited for are dropped. */
+void esg_server_free(esg_server* server);
 
 /* Scoring for callers that cannot allocate.  No counterpart in the reference.
  *

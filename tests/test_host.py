@@ -56,3 +56,35 @@ def test_select_hits():
     assert select_hits(s, max_ties=0) == [(0, False)]
     assert select_hits(s, min_score=25) == []
     assert select_hits(ReadScores(None, None, 0, [], False, False)) == []
+
+
+def test_server_refuses_bad_requests_on_the_host():
+    """esg_server_*: a request for a slot that does not exist, an unknown
+    flag, a wait on an unknown ticket -- refused before anything reaches a
+    device (no scorer needed)."""
+    import ctypes as C
+
+    from eschalign_b200 import _native
+    from eschalign_b200.scorer import GpuError, _check
+
+    lib = _native.load()
+    h = C.c_void_p()
+    _check(lib, lib.esg_server_new(None, C.byref(h)))
+    try:
+        codes = np.array([0, 1, 2, 3], np.uint8)
+        off = np.array([0], np.uint64)
+        lens = np.array([4], np.uint32)
+        t = C.c_uint64()
+        args = (codes.ctypes.data_as(C.POINTER(C.c_uint8)), off.ctypes.data_as(C.POINTER(C.c_uint64)),
+                lens.ctypes.data_as(C.POINTER(C.c_uint32)), 1)
+        assert lib.esg_server_submit(h, 0, *args, 0, C.byref(t)) == 7  # no slot 0
+        assert b"slot" in lib.esg_last_error()
+        assert lib.esg_server_submit(h, 0, *args, 2, C.byref(t)) == 7  # FULL_ROWS not served
+        assert lib.esg_server_wait(h, 12345, 0, None, None, None) == 7
+        st = _native.EsgServerStats()
+        _check(lib, lib.esg_server_stats_get(h, C.byref(st)))
+        assert st.requests == 0
+        with pytest.raises(GpuError):
+            _check(lib, lib.esg_server_add_scorer(h, None, None))
+    finally:
+        lib.esg_server_free(h)
