@@ -35,6 +35,14 @@ Other workloads (``--workload``), one JSON line each, same keys:
       all four mate queries scored, the (reference, template strand)
       candidates of both template strands ranked on the device; GCUPS and
       pairs/s.  CPU arm: trimming + AVX-512BW rows + the same ranking.
+* c5  serving: Poisson arrivals at each rate of --rates; a request is
+      log-uniform 1-50 000 reads (C2 lengths) for panel A (C2's 164 refs)
+      or B (2000 x 300 nt), local or semi-global, forward or both strands,
+      through the library's request queue (esg_server: continuous batching
+      over four resident scorers, admission by free device memory); per
+      rate p50/p99/p99.9 latency (submit to results, the server's own
+      clock) and aggregate GCUPS; a sample of requests re-scored alone must
+      be equal.
 * c3  the uneven panel: 10 000 references of 300-1000 nt, reads of
       50-1000 nt (70 % derived, 10 % subs, 3 % indels), local, both
       strands, autotuned tile shape; a bounded read sample per step (the
@@ -92,11 +100,14 @@ def args_parse():
                     help="score READS reads of the workload once per kernel and exit "
                          "(a small target for ncu)")
     ap.add_argument("--mode", default="local", choices=["local", "semiglobal"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"])
     ap.add_argument("--pairs", type=int, default=2_000_000, help="c4: read pairs")
     ap.add_argument("--pair-chunk", type=int, default=125_000,
                     help="c4: pairs per prepare/submit/finish batch in the e2e feeder")
     ap.add_argument("--c3-reads", type=int, default=4000, help="c3: reads per step")
+    ap.add_argument("--rates", default="10,30,100,300,1000,2000",
+                    help="c5: Poisson arrival rates swept (requests/s)")
+    ap.add_argument("--requests", type=int, default=200, help="c5: requests per rate")
     ap.add_argument("--split", type=int, default=-1,
                     help="16/32-row split in nt, set instead of autotuning (for runs under a "
                          "profiler, whose serialised launches would skew the autotuner)")
@@ -641,6 +652,146 @@ def run_c3(a, ctx, rank):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- C5
+def run_c5(a, ctx, rank):
+    import threading
+
+    from eschalign_b200 import GpuScorer, Mode, Scoring, synth
+    from eschalign_b200.server import Server
+    world, local_rank = ctx.world, ctx.local_rank
+    scoring = (2, -1, -10, -1)
+    panels = {"A": synth.panel_tiles(), "B": synth.panel(2000, 300, 300, 0x5EED_0C5B)}
+    pbases = {k: sum(len(r) for r in v) for k, v in panels.items()}
+    rng = np.random.default_rng(0x5EED_0C05)
+    pool_n = 400_000
+    pools = {"A": synth.reads_c2(panels["A"], n=pool_n, seed=0x5EED_0C5A),
+             "B": synth.mixed_reads(rng, panels["B"],
+                                    synth.lognormal_lengths(rng, pool_n, 110, 0.4, 20, 1000),
+                                    0.9, 0.08, 0.02, 0.01)}
+    specs = [("A", Mode.LOCAL), ("A", Mode.SEMIGLOBAL), ("B", Mode.LOCAL), ("B", Mode.SEMIGLOBAL)]
+    scorers = []
+    tunes = {}
+    for pk, md in specs:
+        g = GpuScorer(panels[pk], Scoring(*scoring), md, device=local_rank)
+        tunes[f"{pk} {md.label}"] = tune(g, a)["split_len"]
+        scorers.append(g)
+    rates = [float(x) for x in a.rates.split(",") if x]
+    per_rate = []
+    verify = []
+    clocks = None
+    with Server(scorers) as sv:
+        for ri, rate in enumerate(rates):
+            rr = np.random.default_rng([0x5EED_0C05, ri])
+            n_req = a.requests
+            sizes = np.floor(np.exp(rr.uniform(0, np.log(50_000), n_req))).astype(np.int64)
+            slots = rr.integers(0, 4, n_req)
+            both = rr.random(n_req) < 0.5
+            gaps = rr.exponential(1.0 / rate, n_req)
+            reqs = []
+            for k in range(n_req):
+                pk = specs[slots[k]][0]
+                start = int(rr.integers(0, pool_n - sizes[k] + 1))
+                reqs.append((int(slots[k]), pools[pk].slice(start, start + int(sizes[k])),
+                             bool(both[k])))
+            cells = sum(int(r[1].bases()) * (2 if r[2] else 1) * pbases[specs[r[0]][0]]
+                        for r in reqs)
+            tickets = [None] * n_req
+            results = [None] * n_req
+            ready = threading.Semaphore(0)
+
+            def waiter():
+                for k in range(n_req):
+                    ready.acquire()
+                    results[k] = sv.wait(tickets[k])
+
+            th = threading.Thread(target=waiter)
+            th.start()
+            sampler = ClockSampler(local_rank)
+            with sampler:
+                t0 = time.perf_counter()
+                due = t0
+                for k in range(n_req):
+                    due += gaps[k]
+                    dt = due - time.perf_counter()
+                    if dt > 0:
+                        time.sleep(dt)
+                    slot, rd, bs = reqs[k]
+                    tickets[k] = sv.submit(slot, rd.tuple(), bs)
+                    ready.release()
+                th.join()
+                t_end = time.perf_counter()
+            if ri == len(rates) - 1:
+                clocks = sampler.summary()
+            else:
+                sampler.summary()
+            lat = np.array([results[k][1].total_ms for k in range(n_req)])
+            queued = np.array([results[k][1].queued_ms for k in range(n_req)])
+            bsz = np.array([results[k][1].batch_requests for k in range(n_req)])
+            span = t_end - t0
+            per_rate.append({
+                "rate_req_s": rate, "requests": n_req, "reads": int(sizes.sum()),
+                "achieved_req_s": round(n_req / span, 1),
+                "gcups": round(cells / span / 1e9, 1),
+                "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                "p99_ms": round(float(np.percentile(lat, 99)), 2),
+                "p999_ms": round(float(np.percentile(lat, 99.9)), 2),
+                "mean_queued_ms": round(float(queued.mean()), 2),
+                "mean_requests_per_batch": round(float(bsz.mean()), 2),
+                "seconds": round(span, 2),
+                "h2d_bytes": int(sum(r[1].bases() for r in reqs)),
+                "d2h_bytes": int(sizes.sum()) * (16 + 4 * scorers[0].cap)})
+            # bit-exact in the mix: a sample re-scored alone after the run
+            for k in list(np.argsort(sizes)[:3]) + [int(np.argmax(sizes))]:
+                verify.append((reqs[k], results[k][0]))
+        st = sv.stats()
+    ok = 0
+    alone = {}
+    for (slot, rd, bs), got in verify:
+        pk, md = specs[slot]
+        key = (pk, md)
+        if key not in alone:
+            alone[key] = GpuScorer(panels[pk], Scoring(*scoring), md, device=local_rank)
+        want = alone[key].score_batch(rd.tuple(), both_strands=bs)
+        same = all(np.array_equal(got.results[f], want.results[f])
+                   for f in ("best", "suboptimal", "n_tied", "flags"))
+        n = rd.lens.size
+        for i in range(n):
+            m = min(int(want.results["n_tied"][i]), got.cap)
+            same = same and np.array_equal(got.ties[i, :m], want.ties[i, :m])
+        ok += int(same)
+    for g in list(alone.values()) + scorers:
+        g.close()
+    best = max(per_rate, key=lambda x: x["gcups"])
+    peak = int_peak(local_rank)
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(panels["B"], pools["B"], scoring, "local", a.cpu_seconds)
+        cpu.pop("seconds", None)
+        cpu.pop("reads_per_s", None)
+        cpu["sample"] = "panel B (2000 x 300 nt) reads: " + cpu["sample"]
+    if rank == 0:
+        line = common_line(
+            a, ctx, best["gcups"], 1e3 * best["seconds"],
+            "C5: serving, Poisson arrivals at " + a.rates + " req/s, requests of log-uniform "
+            "1-50 000 C2-length reads for panel A (164 x 70-180 nt) or B (2000 x 300 nt), "
+            "local or semi-global 2,-1,-10,-1, forward or both strands, through esg_server",
+            {"requests_per_rate": a.requests, "panels": {k: len(v) for k, v in panels.items()}},
+            {"value": best["gcups"], "unit": "GCUPS", "h2d_bytes_per_step": best["h2d_bytes"],
+             "d2h_bytes_per_step": best["d2h_bytes"],
+             "note": "serving is end to end: host requests in, results out"},
+            roofline_of(peak, best["gcups"] * 1e9, "local", None), clocks,
+            int(st["kernels"]))
+        line["value_note"] = ("aggregate GCUPS at the busiest rate (all requests, wall clock); "
+                              "gpu_launches = kernels of every batch of the sweep")
+        line["latency_by_rate"] = per_rate
+        line["server_stats"] = st
+        line["bit_exact_alone_vs_mix"] = f"{ok} of {len(verify)} sampled requests equal"
+        line["autotune_split"] = tunes
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+
+
 def main():
     a = args_parse()
     rank = env_int("RANK", 0)
@@ -660,7 +811,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
     ctx = Ctx(torch, dist, dev, local_rank, world)
-    {"c2": run_c2, "c3": run_c3, "c4": run_c4}[a.workload](a, ctx, rank)
+    {"c2": run_c2, "c3": run_c3, "c4": run_c4, "c5": run_c5}[a.workload](a, ctx, rank)
     if world > 1:
         dist.destroy_process_group()
 

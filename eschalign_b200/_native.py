@@ -115,7 +115,8 @@ class EsgAdapterConfig(C.Structure):
 
 class EsgServerOptions(C.Structure):
     _fields_ = [("max_batch_reads", C.c_uint32), ("max_inflight", C.c_uint32),
-                ("memory_budget", C.c_uint64), ("memory_headroom", C.c_uint64)]
+                ("memory_budget", C.c_uint64), ("memory_headroom", C.c_uint64),
+                ("max_batch_cells", C.c_uint64)]
 
 
 class EsgRequestTiming(C.Structure):
@@ -127,7 +128,7 @@ class EsgServerStats(C.Structure):
     _fields_ = [("requests", C.c_uint64), ("completed", C.c_uint64), ("refused", C.c_uint64),
                 ("batches", C.c_uint64), ("cells", C.c_uint64), ("bytes_in_flight", C.c_uint64),
                 ("peak_bytes_in_flight", C.c_uint64), ("admission_waits", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("kernels", C.c_uint32)]
 
 
 # every entry point include/eschalign_b200.h declares: name -> (restype, argtypes)

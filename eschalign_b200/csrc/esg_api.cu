@@ -993,6 +993,8 @@ int esg_internal_device(const esg_scorer* sc) { return sc ? sc->device : 0; }
 
 uint32_t esg_internal_tie_capacity(const esg_scorer* sc) { return sc ? sc->cap : 0; }
 
+uint64_t esg_internal_panel_bases(const esg_scorer* sc) { return sc ? sc->panel_bases : 0; }
+
 extern "C" {
 
 esg_status esg_prepare(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,

@@ -21,3 +21,5 @@ ESG_HIDDEN size_t esg_internal_pool_spare(esg_scorer* sc);
 // The scorer's device ordinal and tie capacity.
 ESG_HIDDEN int esg_internal_device(const esg_scorer* sc);
 ESG_HIDDEN uint32_t esg_internal_tie_capacity(const esg_scorer* sc);
+// Bases of the scorer's panel (DP cells per read base and strand).
+ESG_HIDDEN uint64_t esg_internal_panel_bases(const esg_scorer* sc);

@@ -54,21 +54,37 @@ struct Request {
   std::vector<uint8_t> codes;
   std::vector<uint64_t> off;
   std::vector<uint32_t> len;
-  // results
+  // results, filled piece by piece
   std::vector<esg_read_result> results;
   std::vector<uint32_t> ties;
+  uint32_t pieces_left = 0;
+  std::vector<std::pair<uint32_t, uint64_t>> cuts;  // piece ends (k1) and cells
+  uint32_t next_piece = 0;                          // the next piece to queue
   esg_status status = ESG_OK;
   std::string error;
   bool done = false;
+  bool started = false;
   Clock::time_point t_submit, t_device, t_done;
   uint32_t batch_reads = 0, batch_requests = 0;
 };
 
 using RequestP = std::shared_ptr<Request>;
 
+// A request's reads k0 .. k1 - 1: the unit of batching.  A request whose
+// cells exceed max_batch_cells is cut into several pieces, so no batch runs
+// much longer than that.  Only a request's next piece waits in the queue,
+// and the one after it joins the back when it is taken: requests share the
+// scorer round-robin, and a small one is not stuck behind a giant.
+struct Piece {
+  RequestP r;
+  uint32_t k0 = 0, k1 = 0;
+  uint64_t cells = 0;
+  uint32_t reads() const { return k1 - k0; }
+};
+
 struct InFlight {
   esg_batch* batch = nullptr;
-  std::vector<RequestP> reqs;
+  std::vector<Piece> pieces;
   uint64_t bytes = 0;
   uint32_t n_reads = 0;
 };
@@ -77,8 +93,9 @@ struct Slot {
   esg_scorer* scorer = nullptr;
   uint32_t cap = 8;
   int device = 0;
-  std::deque<RequestP> pending;
-  RequestP solo;  // goes next, alone (its batch with others did not fit)
+  uint64_t panel_bases = 0;
+  std::deque<Piece> pending;
+  std::deque<Piece> solo;  // go next, one at a time (their batch with others did not fit)
   std::deque<InFlight> inflight;
   std::condition_variable cv;
   std::thread worker;
@@ -110,16 +127,32 @@ esg_status set_err(esg_status st, const char* fmt, ...) {
   return st;
 }
 
-// Fail a set of requests (lock held by the caller).
-void fail_requests(esg_server* sv, std::vector<RequestP>& reqs, esg_status st, const std::string& msg) {
+// The request's next piece, if any, to the back of the slot's queue (lock
+// held by the caller).
+void queue_next(Slot& s, const RequestP& r) {
+  if (r->next_piece >= r->cuts.size()) return;
+  Piece p;
+  p.r = r;
+  p.k0 = r->next_piece ? r->cuts[r->next_piece - 1].first : 0;
+  p.k1 = r->cuts[r->next_piece].first;
+  p.cells = r->cuts[r->next_piece].second;
+  r->next_piece++;
+  s.pending.push_back(p);
+}
+
+// A piece failed: its request fails (once).  Lock held by the caller.
+void fail_pieces(esg_server* sv, std::vector<Piece>& ps, esg_status st, const std::string& msg) {
   const auto now = Clock::now();
-  for (auto& r : reqs) {
-    r->status = st;
-    r->error = msg;
-    r->done = true;
-    r->t_done = now;
-    if (r->t_device == Clock::time_point{}) r->t_device = now;
+  for (auto& p : ps) {
+    Request& r = *p.r;
+    if (r.done) continue;
+    r.status = st;
+    r.error = msg;
+    r.done = true;
+    r.t_done = now;
+    if (!r.started) r.t_device = now;
     sv->stats.completed++;
+    if (st == ESG_ERR_OUT_OF_MEMORY) sv->stats.refused++;
   }
 }
 
@@ -128,6 +161,7 @@ void finish_oldest(esg_server* sv, Slot& s) {
   InFlight f;
   {
     std::lock_guard<std::mutex> lk(sv->mu);
+    if (s.inflight.empty()) return;  // (woken for pieces that turned out dead)
     f = std::move(s.inflight.front());
     s.inflight.pop_front();
   }
@@ -138,20 +172,27 @@ void finish_oldest(esg_server* sv, Slot& s) {
   esg_batch_free(f.batch);
   std::lock_guard<std::mutex> lk(sv->mu);
   if (st != ESG_OK) {
-    fail_requests(sv, f.reqs, st, msg);
+    fail_pieces(sv, f.pieces, st, msg);
   } else {
     const auto now = Clock::now();
     size_t at = 0;
-    for (auto& r : f.reqs) {
-      r->results.assign(res.begin() + at, res.begin() + at + r->n_reads);
-      r->ties.assign(ties.begin() + at * s.cap, ties.begin() + (at + r->n_reads) * s.cap);
-      at += r->n_reads;
-      r->status = ESG_OK;
-      r->done = true;
-      r->t_done = now;
-      r->codes.clear();
-      r->codes.shrink_to_fit();
-      sv->stats.completed++;
+    for (auto& p : f.pieces) {
+      Request& r = *p.r;
+      const uint32_t n = p.reads();
+      if (!r.done) {
+        std::copy(res.begin() + at, res.begin() + at + n, r.results.begin() + p.k0);
+        std::copy(ties.begin() + at * s.cap, ties.begin() + (at + n) * s.cap,
+                  r.ties.begin() + (size_t)p.k0 * s.cap);
+        if (--r.pieces_left == 0) {
+          r.status = ESG_OK;
+          r.done = true;
+          r.t_done = now;
+          r.codes.clear();
+          r.codes.shrink_to_fit();
+          sv->stats.completed++;
+        }
+      }
+      at += n;
     }
   }
   sv->stats.bytes_in_flight -= f.bytes;
@@ -163,44 +204,58 @@ void worker(esg_server* sv, Slot* sp) {
   Slot& s = *sp;
   cudaSetDevice(s.device);
   const uint32_t max_reads = sv->opt.max_batch_reads;
+  const uint64_t max_cells = sv->opt.max_batch_cells;
   const uint32_t max_inflight = sv->opt.max_inflight;
   for (;;) {
-    std::vector<RequestP> group;
+    std::vector<Piece> group;
     uint32_t flags = 0, n_reads = 0;
     {
       std::unique_lock<std::mutex> lk(sv->mu);
       s.cv.wait(lk, [&] {
         return sv->stop ||
-               ((!s.pending.empty() || s.solo) && s.inflight.size() < max_inflight) ||
+               ((!s.pending.empty() || !s.solo.empty()) && s.inflight.size() < max_inflight) ||
                !s.inflight.empty();
       });
       if (sv->stop && s.inflight.empty()) {
-        std::vector<RequestP> left(s.pending.begin(), s.pending.end());
-        if (s.solo) left.push_back(s.solo);
-        s.solo.reset();
+        std::vector<Piece> left(s.pending.begin(), s.pending.end());
+        left.insert(left.end(), s.solo.begin(), s.solo.end());
         s.pending.clear();
-        fail_requests(sv, left, ESG_ERR_BAD_ARGUMENT, "server stopped");
+        s.solo.clear();
+        fail_pieces(sv, left, ESG_ERR_BAD_ARGUMENT, "server stopped");
         sv->done_cv.notify_all();
         return;
       }
-      if (s.solo && !sv->stop && s.inflight.size() < max_inflight) {
-        // a request whose batch with others did not fit: alone this time
-        group.push_back(s.solo);
-        flags = s.solo->flags;
-        n_reads = s.solo->n_reads;
-        s.solo.reset();
+      // pieces of a request that already failed do not run
+      auto dead = [](const Piece& p) { return p.r->done; };
+      s.pending.erase(std::remove_if(s.pending.begin(), s.pending.end(), dead), s.pending.end());
+      s.solo.erase(std::remove_if(s.solo.begin(), s.solo.end(), dead), s.solo.end());
+      if (!sv->stop && !s.solo.empty() && s.inflight.size() < max_inflight) {
+        // a piece whose batch with others did not fit: alone this time
+        group.push_back(s.solo.front());
+        s.solo.pop_front();
+        flags = group[0].r->flags;
+        n_reads = group[0].reads();
       } else if (!sv->stop && !s.pending.empty() && s.inflight.size() < max_inflight) {
-        // the waiting requests with the first one's strand flag, in order
-        flags = s.pending.front()->flags;
+        // the waiting pieces with the first one's strand flag, in order, up
+        // to the batch's read and cell caps
+        flags = s.pending.front().r->flags;
+        uint64_t cells = 0;
         for (auto it = s.pending.begin(); it != s.pending.end();) {
-          if ((*it)->flags != flags) {
+          if (it->r->flags != flags) {
             ++it;
             continue;
           }
-          if (!group.empty() && n_reads + (*it)->n_reads > max_reads) break;
-          n_reads += (*it)->n_reads;
+          if (!group.empty() &&
+              (n_reads + it->reads() > max_reads || cells + it->cells > max_cells))
+            break;
+          n_reads += it->reads();
+          cells += it->cells;
           group.push_back(*it);
+          const RequestP r = it->r;
           it = s.pending.erase(it);
+          const size_t at = it - s.pending.begin();
+          queue_next(s, r);  // at the back: behind what already waits
+          it = s.pending.begin() + at;
         }
       }
     }
@@ -213,17 +268,17 @@ void worker(esg_server* sv, Slot* sp) {
     std::vector<uint32_t> lens;
     ptrs.reserve(n_reads);
     lens.reserve(n_reads);
-    for (auto& r : group)
-      for (uint32_t k = 0; k < r->n_reads; ++k) {
-        ptrs.push_back(r->codes.data() + r->off[k]);
-        lens.push_back(r->len[k]);
+    for (auto& p : group)
+      for (uint32_t k = p.k0; k < p.k1; ++k) {
+        ptrs.push_back(p.r->codes.data() + p.r->off[k]);
+        lens.push_back(p.r->len[k]);
       }
     esg_batch* b = nullptr;
     esg_status st = esg_internal_prepare_ptrs(s.scorer, ptrs.data(), lens.data(), n_reads, flags, &b);
     if (st != ESG_OK) {
       const std::string msg = esg_last_error();
       std::lock_guard<std::mutex> lk(sv->mu);
-      fail_requests(sv, group, st, msg);
+      fail_pieces(sv, group, st, msg);
       sv->done_cv.notify_all();
       continue;
     }
@@ -270,13 +325,11 @@ void worker(esg_server* sv, Slot* sp) {
       sv->done_cv.wait_for(lk, std::chrono::milliseconds(2));
     }
     if (refused && group.size() > 1) {
-      // too big together: back to the queue's front, in order, and the
-      // first request goes alone (only a request that cannot fit by itself
-      // is refused)
+      // too big together: one at a time, in order (only a piece that cannot
+      // fit by itself is refused)
       esg_batch_free(b);
       std::lock_guard<std::mutex> lk(sv->mu);
-      for (size_t k = group.size(); k-- > 1;) s.pending.push_front(group[k]);
-      s.solo = group[0];
+      for (size_t k = group.size(); k-- > 0;) s.solo.push_front(group[k]);
       continue;
     }
     if (refused) {
@@ -286,8 +339,7 @@ void worker(esg_server* sv, Slot* sp) {
       snprintf(msg, sizeof msg,
                "batch of %u reads needs %llu device bytes, above what admission allows",
                n_reads, (unsigned long long)need);
-      sv->stats.refused += group.size();
-      fail_requests(sv, group, ESG_ERR_OUT_OF_MEMORY, msg);
+      fail_pieces(sv, group, ESG_ERR_OUT_OF_MEMORY, msg);
       sv->done_cv.notify_all();
       continue;
     }
@@ -297,21 +349,27 @@ void worker(esg_server* sv, Slot* sp) {
       const std::string msg = esg_last_error();
       esg_batch_free(b);
       sv->stats.bytes_in_flight -= need;
-      fail_requests(sv, group, st, msg);
+      fail_pieces(sv, group, st, msg);
       sv->done_cv.notify_all();
       continue;
     }
     const auto now = Clock::now();
-    for (auto& r : group) {
-      r->t_device = now;
-      r->batch_reads = n_reads;
-      r->batch_requests = (uint32_t)group.size();
+    for (auto& p : group) {
+      Request& r = *p.r;
+      if (!r.started) {
+        r.started = true;
+        r.t_device = now;
+        r.batch_reads = n_reads;
+        r.batch_requests = (uint32_t)group.size();
+      }
     }
+    esg_batch_stats_get(b, &bst);  // the kernel count is known once submitted
     sv->stats.batches++;
     sv->stats.cells += bst.cells;
+    sv->stats.kernels += bst.kernels;
     InFlight f;
     f.batch = b;
-    f.reqs = std::move(group);
+    f.pieces = std::move(group);
     f.bytes = need;
     f.n_reads = n_reads;
     s.inflight.push_back(std::move(f));
@@ -328,6 +386,7 @@ esg_status esg_server_new(const esg_server_options* options, esg_server** out) {
   auto* sv = new esg_server();
   if (options) sv->opt = *options;
   if (!sv->opt.max_batch_reads) sv->opt.max_batch_reads = 262144;
+  if (!sv->opt.max_batch_cells) sv->opt.max_batch_cells = 150000000000ull;
   if (!sv->opt.max_inflight) sv->opt.max_inflight = 2;
   if (!sv->opt.memory_headroom) sv->opt.memory_headroom = 256ull << 20;
   *out = sv;
@@ -345,6 +404,7 @@ esg_status esg_server_add_scorer(esg_server* sv, esg_scorer* sc, uint32_t* slot)
   auto s = std::make_unique<Slot>();
   s->scorer = sc;
   s->cap = esg_internal_tie_capacity(sc);
+  s->panel_bases = esg_internal_panel_bases(sc);
   s->device = esg_internal_device(sc);
   *slot = (uint32_t)sv->slots.size();
   Slot* raw = s.get();
@@ -380,11 +440,29 @@ esg_status esg_server_submit(esg_server* sv, uint32_t slot, const uint8_t* codes
   std::lock_guard<std::mutex> lk(sv->mu);
   if (slot >= sv->slots.size()) return set_err(ESG_ERR_BAD_ARGUMENT, "no scorer slot %u", slot);
   if (sv->stop) return set_err(ESG_ERR_BAD_ARGUMENT, "server stopped");
+  Slot& sl = *sv->slots[slot];
   r->id = sv->next_id++;
   r->slot = slot;
+  r->results.resize(n_reads);
+  r->ties.resize((size_t)n_reads * sl.cap);
+  // pieces of at most max_batch_cells cells (at least one read each)
+  const uint64_t per_base = sl.panel_bases * ((flags & ESG_BOTH_STRANDS) ? 2 : 1);
+  uint32_t k0 = 0;
+  uint64_t cells = 0;
+  for (uint32_t k = 0; k < n_reads; ++k) {
+    const uint64_t c = (uint64_t)len[k] * per_base;
+    if (k > k0 && cells + c > sv->opt.max_batch_cells) {
+      r->cuts.push_back({k, cells});
+      k0 = k;
+      cells = 0;
+    }
+    cells += c;
+  }
+  r->cuts.push_back({n_reads, cells});  // the last (for an empty request, the only) piece
+  r->pieces_left = (uint32_t)r->cuts.size();
   r->t_submit = Clock::now();
   sv->requests[r->id] = r;
-  sv->slots[slot]->pending.push_back(r);
+  queue_next(sl, r);
   sv->stats.requests++;
   sv->slots[slot]->cv.notify_all();
   *ticket = r->id;

@@ -33,11 +33,11 @@ class Server:
     """esg_server: resident scorers behind one request queue."""
 
     def __init__(self, scorers, max_batch_reads: int = 0, max_inflight: int = 0,
-                 memory_budget: int = 0, memory_headroom: int = 0):
+                 memory_budget: int = 0, memory_headroom: int = 0, max_batch_cells: int = 0):
         self._lib = _native.load()
         self._h = None
         opts = _native.EsgServerOptions(max_batch_reads, max_inflight, memory_budget,
-                                        memory_headroom)
+                                        memory_headroom, max_batch_cells)
         h = C.c_void_p()
         _check(self._lib, self._lib.esg_server_new(C.byref(opts), C.byref(h)))
         self._h = h
@@ -78,7 +78,7 @@ class Server:
     def stats(self) -> dict:
         st = _native.EsgServerStats()
         _check(self._lib, self._lib.esg_server_stats_get(self._h, C.byref(st)))
-        return {k: getattr(st, k) for k, _ in st._fields_ if k != "reserved"}
+        return {k: getattr(st, k) for k, _ in st._fields_}
 
     def close(self):
         if self._h:

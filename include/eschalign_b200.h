@@ -303,7 +303,8 @@ esg_status esg_score_pairs(esg_scorer* scorer, const uint8_t* codes, const uint6
  * serving mode.  Requests name a scorer slot (a resident panel under one
  * scoring and mode) and a strand flag; each slot's worker thread batches
  * whatever requests of that slot are waiting (continuous batching: up to
- * max_batch_reads reads per batch, max_inflight batches queued on the
+ * max_batch_reads reads and max_batch_cells DP cells per batch -- a larger
+ * request runs as several batches -- and max_inflight batches queued on the
  * scorer's stream) and admits a batch only when its device memory fits the
  * free device memory (cudaMemGetInfo, plus what the scorer's pool holds
  * spare) less a headroom, and the budget if one is set.  A request that can
@@ -312,10 +313,12 @@ esg_status esg_score_pairs(esg_scorer* scorer, const uint8_t* codes, const uint6
 typedef struct esg_server esg_server;
 
 typedef struct esg_server_options {
-    uint32_t max_batch_reads;  /* reads per batch at most (0: 262144); a larger request runs alone */
+    uint32_t max_batch_reads;  /* reads per batch at most (0: 262144)                            */
     uint32_t max_inflight;     /* batches queued per scorer (0: 2)                               */
     uint64_t memory_budget;    /* device bytes of admitted batches at most (0: free memory only) */
     uint64_t memory_headroom;  /* device bytes admission leaves free (0: 256 MiB)                */
+    uint64_t max_batch_cells;  /* DP cells per batch at most (0: 1.5e11, ~30 ms); a larger
+                                  request is cut into pieces of whole reads                      */
 } esg_server_options;
 
 typedef struct esg_request_timing {
@@ -334,7 +337,7 @@ typedef struct esg_server_stats {
     uint64_t bytes_in_flight;  /* device bytes of admitted batches now                           */
     uint64_t peak_bytes_in_flight;
     uint32_t admission_waits;  /* times a batch waited for device memory                         */
-    uint32_t reserved;
+    uint32_t kernels;          /* kernel launches of the batches run                             */
 } esg_server_stats;
 
 esg_status esg_server_new(const esg_server_options* options, esg_server** out);

@@ -125,3 +125,32 @@ def test_server_wait_timeout_is_host_side():
         assert res.results["best"][0] == 2 * pb[0].size
         assert tm.batch_reads == 3000
     g.close()
+
+
+def test_server_splits_large_requests_into_pieces():
+    """A request above max_batch_cells runs as several batches of whole
+    reads; its results are reassembled in order, equal to scoring it alone,
+    and small requests queued behind it ride in between."""
+    rng, pa, pb = _panels()
+    g = GpuScorer(pb, Scoring(*SCORING), Mode.SEMIGLOBAL, tie_capacity=CAP)
+    solo = GpuScorer(pb, Scoring(*SCORING), Mode.SEMIGLOBAL, tie_capacity=CAP)
+    letters = None
+    big = [pb[(7 * k) % len(pb)][k % 50:k % 50 + 60 + k % 90] for k in range(300)]
+    small = [pb[3][10:70]]
+    with Server([g], max_batch_cells=50_000_000) as sv:
+        tb = sv.submit(0, big, True)
+        ts = sv.submit(0, small, False)
+        rb, tmb = sv.wait(tb, 120_000)
+        rs, tms = sv.wait(ts, 120_000)
+        st = sv.stats()
+    assert st["batches"] >= 10  # 300 reads x ~1.1e7 cells each, 5e7 cells per batch
+    want = solo.score_batch(big, both_strands=True)
+    for f in ("best", "suboptimal", "n_tied", "flags"):
+        assert np.array_equal(rb.results[f], want.results[f]), f
+    for k in range(len(big)):
+        n = min(int(want.results["n_tied"][k]), CAP)
+        assert np.array_equal(rb.ties[k, :n], want.ties[k, :n]), k
+    assert rs.results["best"][0] == 120
+    assert tms.total_ms <= tmb.total_ms  # the small one did not wait for all of the big one
+    g.close()
+    solo.close()
