@@ -265,6 +265,29 @@ def cpu_pairs_baseline(refs, pairs, scoring, seconds, threads=0):
             "pairs_per_s": n / dt, "seconds": dt}
 
 
+def reference_gpu_arms(refs, reads, scoring, local, device):
+    """Comparison arms: the reference's own align_score_kernel (int) and
+    align_score_kernel_h2 (half2), compiled ahead of time for sm_100a from its
+    source and launched as its GpuScorer does (oracle/ref_gpu, built where
+    the reference tree is present), on `reads` and their reverse complements
+    -- the queries its CLI feeder submits for both strands.  A reported
+    baseline, like cpu_baseline; None where the arms were not built."""
+    from oracle import oracle as O
+    if not (os.path.exists(O.REF_GPU_LIB) and os.path.exists(O.REF_GPU_CUBIN)):
+        return None
+    rg = O.RefGpu(refs, device=device)
+    fwd = reads.list()
+    qc, qo, ql = O.pack(fwd + [O.revcomp(r) for r in fwd])
+    cells = int(ql.sum(dtype=np.uint64)) * sum(len(r) for r in refs)
+    out = {"kind": "reference", "sample": f"{len(fwd)} reads + reverse complements"}
+    for kernel, name in ((0, "int"), (1, "half2")):
+        _, ms = rg.score(qc, qo, ql, scoring, local, kernel=kernel, reps=2, rows=False)
+        out[f"{name}_gcups"] = cells / (ms / 1e3) / 1e9
+        out[f"{name}_geometry"] = rg.geometry(kernel)
+    rg.close()
+    return out
+
+
 def run_reference(a, rank, world):
     """--impl reference: rank 0 times the CPU path; other ranks exit."""
     if rank != 0:
@@ -502,6 +525,10 @@ def run_c2(a, ctx, rank):
         extras["plain_gcups"] = plain
         extras["batched_over_plain"] = value / plain
         extras["plain_sample"] = f"first {len(sub)} reads, both strands"
+        arms = reference_gpu_arms(refs, sub, scoring, mode == "local", local_rank)
+        if arms:
+            arms["batched_over_ref_half2"] = value / arms["half2_gcups"]
+            extras["reference_gpu_kernels"] = arms
 
     chunks = [reads.slice(k, k + a.chunk) for k in range(0, len(reads), a.chunk)]
     te, n_pass, h2d, d2h = feeder(

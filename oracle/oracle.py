@@ -42,6 +42,82 @@ def build() -> str:
     return LIB_PATH
 
 
+REF_ROOT = "/root/reference"
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libref_gpu.so")
+REF_GPU_CUBIN = os.path.join(HERE, "_ref", "ref_kernels.cubin")
+
+
+def build_ref_gpu() -> bool:
+    """Compile the reference's own GPU kernels (comparison arms) when its
+    tree is present here; elsewhere whatever was built travels as files."""
+    if not os.path.isdir(REF_ROOT):
+        return os.path.exists(REF_GPU_LIB) and os.path.exists(REF_GPU_CUBIN)
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_ROOT}"], check=True)
+    return True
+
+
+class RefGpu:
+    """The reference's align_score_kernel (kernel 0, int) and
+    align_score_kernel_h2 (kernel 1, half2), laid out and launched as
+    crates/eschalign/src/cuda/mod.rs does (oracle/ref_gpu/ref_gpu.cu).
+    Comparison arms only."""
+
+    def __init__(self, refs, device=0):
+        self._L = C.CDLL(REF_GPU_LIB)
+        L = self._L
+        L.rg_new.restype = C.c_int
+        L.rg_new.argtypes = [C.c_int, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_uint32, C.POINTER(C.c_void_p)]
+        L.rg_score.restype = C.c_int
+        L.rg_score.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_uint32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int,
+                               C.c_int, C.c_void_p, C.POINTER(C.c_float)]
+        L.rg_error.restype = C.c_char_p
+        L.rg_error.argtypes = [C.c_void_p]
+        L.rg_free.argtypes = [C.c_void_p]
+        L.rg_geometry.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+        self.n_refs = len(refs)
+        c, o, l = pack(refs)
+        self._h = C.c_void_p()
+        rc = L.rg_new(device, REF_GPU_CUBIN.encode(), c.ctypes.data, o.ctypes.data, l.ctypes.data,
+                      len(refs), C.byref(self._h))
+        if rc:
+            msg = L.rg_error(self._h).decode()
+            L.rg_free(self._h)
+            self._h = None
+            raise RuntimeError(msg)
+
+    def geometry(self, kernel):
+        g = (C.c_int * 4)()
+        self._L.rg_geometry(self._h, kernel, g)
+        return tuple(g)
+
+    def score(self, codes, off, lens, scoring, local, kernel=0, reps=1, rows=True):
+        """(int16 rows [q, n_refs] or None, mean ms per launch)."""
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        lens = np.ascontiguousarray(lens, dtype=np.uint32)
+        out = np.zeros((lens.size, self.n_refs), dtype=np.int16) if rows else None
+        ms = C.c_float()
+        rc = self._L.rg_score(self._h, kernel, codes.ctypes.data, off.ctypes.data,
+                              lens.ctypes.data, lens.size, *scoring, int(bool(local)), reps,
+                              out.ctypes.data if rows else None, C.byref(ms))
+        if rc:
+            raise RuntimeError(self._L.rg_error(self._h).decode())
+        return out, ms.value
+
+    def close(self):
+        if self._h:
+            self._L.rg_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 _lib = None
 
 
