@@ -35,6 +35,10 @@ Other workloads (``--workload``), one JSON line each, same keys:
       all four mate queries scored, the (reference, template strand)
       candidates of both template strands ranked on the device; GCUPS and
       pairs/s.  CPU arm: trimming + AVX-512BW rows + the same ranking.
+* c1  the reference's CPU-sized case: 10 000 reads (90 % cut from a
+      reference, 8 % subs, 2 % ins, 1 % del; 10 % random) of 60-200 nt
+      against the 164-reference panel, local 2,-1,-10,-1, forward strand;
+      GPU device time and e2e beside the CPU path on the whole set.
 * c5  serving: Poisson arrivals at each rate of --rates; a request is
       log-uniform 1-50 000 reads (C2 lengths) for panel A (C2's 164 refs)
       or B (2000 x 300 nt), local or semi-global, forward or both strands,
@@ -100,7 +104,7 @@ def args_parse():
                     help="score READS reads of the workload once per kernel and exit "
                          "(a small target for ncu)")
     ap.add_argument("--mode", default="local", choices=["local", "semiglobal"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--pairs", type=int, default=2_000_000, help="c4: read pairs")
     ap.add_argument("--pair-chunk", type=int, default=125_000,
                     help="c4: pairs per prepare/submit/finish batch in the e2e feeder")
@@ -566,6 +570,63 @@ def run_c2(a, ctx, rank):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- C1
+def run_c1(a, ctx, rank):
+    from eschalign_b200 import GpuScorer, Mode, Scoring, synth
+    world, local_rank = ctx.world, ctx.local_rank
+    scoring = (2, -1, -10, -1)
+    refs = synth.panel_tiles()
+    panel_bases = sum(len(r) for r in refs)
+    reads = synth.reads_c1(refs)
+    g = GpuScorer(refs, Scoring(*scoring), Mode.LOCAL, device=local_rank,
+                  stream=ctx.stream.cuda_stream)
+    tune_rep = tune(g, a)
+    batch = g.submit(g.prepare(reads.tuple()))
+    st = g.finish(batch, keep=True).stats
+    cells = st["cells"]
+    sampler = ClockSampler(local_rank)
+    t = ctx.device_time(g, batch, a.steps, a.warmup, sampler)
+    clocks = sampler.summary()
+    t_max = ctx.max_over_ranks(t)
+    value = world * cells * a.steps / t_max / 1e9
+    peak = int_peak(local_rank)
+    roofline = roofline_of(peak, cells * a.steps / t, "local", None)
+    batch.free()
+    te, n_pass, h2d, d2h = feeder(ctx, [reads], lambda c: g.prepare(c.tuple()), g.submit,
+                                  lambda b: g.finish(b).stats, max(3, a.steps))
+    e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "reads_per_s": world * len(reads) * n_pass / te}
+    g.close()
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        prof = O.Profile(refs, scoring)
+        prof.map_batch(*reads.tuple(), local=True, both_strands=False)  # warm-up
+        t0 = time.perf_counter()
+        _, _, _, used = prof.map_batch(*reads.tuple(), local=True, both_strands=False)
+        dt = time.perf_counter() - t0
+        cpu = {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": int(used), "kind": "port",
+               "sample": f"all {len(reads)} reads, forward strand; {dt:.3f} s; "
+                         f"reads/s {len(reads) / dt:.0f}"}
+    if rank == 0:
+        line = common_line(
+            a, ctx, value, 1e3 * t_max / a.steps,
+            "C1: 10 000 reads (60-200 nt, 90 % derived) x 164-ref panel (70-180 nt), local "
+            "2,-1,-10,-1, forward strand, int32 scores",
+            {"reads": len(reads), "refs": len(refs), "panel_bases": panel_bases,
+             "cells_per_step": cells},
+            e2e, roofline, clocks, st["kernels"] * a.steps)
+        line["reads_per_s"] = world * len(reads) * a.steps / t_max
+        line["autotune"] = tune_rep
+        line["batch_stats"] = {k: st[k] for k in ("queries_batched", "tasks", "panel_chunks",
+                                                  "kernels")}
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- C4
 def run_c4(a, ctx, rank):
     from eschalign_b200 import GpuScorer, Mode, Scoring, adapter, synth
@@ -838,7 +899,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
     ctx = Ctx(torch, dist, dev, local_rank, world)
-    {"c2": run_c2, "c3": run_c3, "c4": run_c4, "c5": run_c5}[a.workload](a, ctx, rank)
+    {"c1": run_c1, "c2": run_c2, "c3": run_c3, "c4": run_c4,
+     "c5": run_c5}[a.workload](a, ctx, rank)
     if world > 1:
         dist.destroy_process_group()
 

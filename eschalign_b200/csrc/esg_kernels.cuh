@@ -363,12 +363,15 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[R],
   };
 
   int t = 0;
+  // (local mode only: semi-global measured slower with a second copy of the
+  // column body, whose last-row and short-reference state cost it registers)
   if constexpr (kLocal && !kLong) {
     // Steps fill .. m - 1, where fill = steps - m is the tile's largest skew,
     // have every lane of the tile's queries inside the pair's columns: they
     // run without the column check.  Lanes past the tile's queries take
     // skew 0 there (columns in range, values nobody reads: only later lanes,
-    // also past the queries, see them).
+    // also past the queries, see them, and a pass's results are taken from
+    // the queries' own lanes).
     const int fill = steps - m;
     if (fill < m) {
 #pragma unroll 1
