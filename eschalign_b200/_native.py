@@ -149,6 +149,7 @@ SIGNATURES = {
     "esg_scorer_info": (C.c_int32, [C.c_void_p, C.POINTER(EsgInfo)]),
     "esg_scorer_set_kernel": (C.c_int32, [C.c_void_p, C.c_int32]),
     "esg_scores_len": (C.c_int32, [C.c_void_p, C.c_uint64]),
+    "esg_batched_takes": (C.c_int32, [C.c_void_p, C.c_uint64]),
     "esg_scorer_autotune": (C.c_int32, [C.c_void_p, C.POINTER(EsgTuneReport)]),
     "esg_scorer_set_split": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "esg_scorer_set_chunking": (C.c_int32, [C.c_void_p, C.c_uint32]),

@@ -703,6 +703,10 @@ esg_status esg_scorer_set_kernel(esg_scorer* sc, int32_t kernel) {
 
 int32_t esg_scores_len(const esg_scorer* sc, uint64_t len) { return sc && len > 0; }
 
+int32_t esg_batched_takes(const esg_scorer* sc, uint64_t len) {
+  return sc && sc->kernel == ESG_KERNEL_AUTO && k2_takes(sc, len);
+}
+
 esg_status esg_scorer_set_chunking(esg_scorer* sc, uint32_t max_chunks) {
   g_err.clear();
   if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");

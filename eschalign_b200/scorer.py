@@ -101,6 +101,23 @@ def device_visible() -> bool:
     return n.value > 0
 
 
+# Limits beside the reference's (cuda/mod.rs:90-99: MAX_READ_LEN 4096,
+# MAX_REF_LEN 3072, MAX_REF_LEN_H2 1536): every non-empty read is scored
+# here, and references up to 32 768 bases are taken by both kernels.
+MAX_READ_LEN = None
+MAX_REF_LEN = 32768
+MAX_REF_LEN_H2 = MAX_REF_LEN
+
+
+def fits_f16(n: int, max_ref_len: int, scoring: Scoring) -> bool:
+    """cuda/mod.rs:116-122, for callers that route like the reference: a
+    read whose whole DP stays within fp16's exact integers (2048)."""
+    k = min(n, max_ref_len)
+    m = max(abs(scoring.match_score), abs(scoring.mismatch))
+    o, e = abs(scoring.gap_open), abs(scoring.gap_extend)
+    return k * m + o + e + o <= 2048
+
+
 def fits_i16(n: int, max_ref_len: int, scoring: Scoring) -> bool:
     """simd/mod.rs:222-227 (the reference's SIMD/GPU admission bound)."""
     lib = _native.load()
@@ -289,6 +306,7 @@ class GpuScorer:
         self.cap = int(tie_capacity)
         codes, off, lens = panel.packed()
         self._panel_arrays = (codes, off, lens)
+        self._kernel = int(kernel)
         sc = _native.EsgScoring(*scoring.astuple())
         opts = _native.EsgOptions(self.cap, int(kernel), stream)
         h = C.c_void_p()
@@ -335,23 +353,58 @@ class GpuScorer:
     def device_name(self) -> str:
         return self.info()["device_name"]
 
+    # The reference has an int kernel and a half2 "fast" kernel
+    # (cuda/mod.rs:452-514); here the plain int32 kernel stands for the
+    # first and the batched int16x2 kernel for the second.
     def geometry(self):
+        """The int32 kernel's (threads per block, groups, blocks)."""
         i = self.info()
+        return (i["plain_threads"], 1, i["plain_blocks"])
+
+    def geometry_h2(self):
+        """The batched kernel's (threads per block, reference pairs, persistent
+        blocks), or None where the scoring scheme rules it out."""
+        i = self.info()
+        if not i["batched_ok"]:
+            return None
         return (i["batched_threads"], i["n_ref_pairs"], i["batched_blocks"])
 
     def registers(self):
-        return self.info()["regs_batched"]
+        return self.info()["regs_plain"]
+
+    def registers_h2(self):
+        i = self.info()
+        return i["regs_batched"] if i["batched_ok"] else None
 
     def local_bytes(self):
-        return self.info()["local_bytes_batched"]
+        return self.info()["local_bytes_plain"]
+
+    def local_bytes_h2(self):
+        i = self.info()
+        return i["local_bytes_batched"] if i["batched_ok"] else None
 
     def set_kernel(self, kernel: int):
         _check(self._lib, self._lib.esg_scorer_set_kernel(self._h, int(kernel)))
+        self._kernel = int(kernel)
 
     def set_plain(self, plain: bool):
-        """The A/B lever (GpuScorer::set_half2, cuda/mod.rs:500): every
-        query on the plain int32 kernel, or the batched kernel where it can."""
+        """Every query on the plain int32 kernel, or the batched kernel where
+        it can take it."""
         self.set_kernel(KERNEL_PLAIN32 if plain else KERNEL_AUTO)
+
+    def half2(self) -> bool:
+        """GpuScorer::half2: the fast (batched) kernel is in use."""
+        return bool(self.info()["batched_ok"]) and getattr(self, "_kernel", KERNEL_AUTO) == KERNEL_AUTO
+
+    def set_half2(self, enabled: bool):
+        """GpuScorer::set_half2 (cuda/mod.rs:500-502): the A/B lever; results
+        are the same either way."""
+        self.set_plain(not enabled)
+
+    def half2_scores_len(self, n: int) -> bool:
+        """GpuScorer::half2_scores_len: a query of n bases goes to the batched
+        kernel (else the int32 kernel)."""
+        return bool(self._lib.esg_batched_takes(self._h, int(n)))
 
     def autotune(self) -> dict:
         """Measure the 16/32-row stripe split on this panel (esg_scorer_autotune)."""

@@ -191,6 +191,11 @@ esg_status esg_scorer_set_chunking(esg_scorer* scorer, uint32_t max_chunks);
 /* GpuScorer::scores_len (cuda/mod.rs:506-508): 1 for every len > 0 -- nothing
  * is left to a CPU path. */
 int32_t esg_scores_len(const esg_scorer* scorer, uint64_t len);
+/* GpuScorer::half2_scores_len (cuda/mod.rs:509-514), the fast kernel's
+ * share: 1 when a query of `len` bases goes to the batched int16x2 kernel
+ * (ESG_KERNEL_AUTO, inside its value bound), 0 when it goes to the int32
+ * kernel. */
+int32_t esg_batched_takes(const esg_scorer* scorer, uint64_t len);
 
 /* GpuScorer::score_batch (cuda/mod.rs:524-528): prepare + submit + finish.
  * Read k is codes[off[k] .. off[k] + len[k]].  `results` gets n_reads

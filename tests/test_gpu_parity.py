@@ -324,3 +324,28 @@ def test_gpu_autotune_measures_and_keeps_results(oracle):
         assert info["tuned"] == 1 and info["split_len"] == rep["split_len"]
         after = g.score_batch(reads.tuple(), both_strands=True)
         assert (before.results == after.results).all() and (before.ties == after.ties).all()
+
+
+def test_gpu_half2_lever_and_introspection(oracle):
+    """cuda/mod.rs:446-514 mirrored: set_half2 moves every query between the
+    fast (batched) kernel and the int32 kernel, half2_scores_len says where a
+    length goes, the two geometries / register counts are reported, and the
+    scores do not change."""
+    rng = Rng(0x5EED_0107)
+    letters = random_panel(rng, 20, 60, 100)
+    panel = [encode(s) for s in letters]
+    reads = reads_for(rng, letters, 30)
+    with GpuScorer(panel, Scoring(), Mode.SEMIGLOBAL) as g:
+        assert g.half2() and g.half2_scores_len(120) and not g.half2_scores_len(0)
+        assert g.geometry()[0] > 0 and g.geometry_h2()[0] > 0
+        assert g.registers() > 0 and g.registers_h2() > 0
+        fast = g.score_batch(reads, both_strands=True, full_rows=True)
+        assert fast.stats["queries_batched"] == 2 * len(reads)
+        g.set_half2(False)
+        assert not g.half2() and not g.half2_scores_len(120)
+        slow = g.score_batch(reads, both_strands=True, full_rows=True)
+        assert slow.stats["queries_plain"] == 2 * len(reads)
+        assert np.array_equal(fast.rows, slow.rows)
+        # semi-global past the batched kernel's value bound goes to int32
+        g.set_half2(True)
+        assert not g.half2_scores_len(20000)

@@ -88,3 +88,15 @@ def test_server_refuses_bad_requests_on_the_host():
             _check(lib, lib.esg_server_add_scorer(h, None, None))
     finally:
         lib.esg_server_free(h)
+
+
+def test_fits_f16_matches_the_reference_bound():
+    """cuda/mod.rs:116-122 with the module's own example: the tRNA panel at
+    the default scoring is ~420, far inside 2048."""
+    from eschalign_b200.scorer import fits_f16
+    s = Scoring(2, -1, -10, -1)
+    assert fits_f16(150, 150, s)            # 150 * 2 + 21 = 321
+    assert fits_f16(5000, 1000, s)          # min(n, L) = 1000: 2021
+    assert not fits_f16(5000, 1100, s)      # 2221
+    assert not fits_f16(1014, 1014, s)      # 2049
+    assert fits_f16(1013, 1013, s)          # 2047
