@@ -346,6 +346,8 @@ def test_gpu_half2_lever_and_introspection(oracle):
         slow = g.score_batch(reads, both_strands=True, full_rows=True)
         assert slow.stats["queries_plain"] == 2 * len(reads)
         assert np.array_equal(fast.rows, slow.rows)
-        # semi-global past the batched kernel's value bound goes to int32
-        g.set_half2(True)
-        assert not g.half2_scores_len(20000)
+    # semi-global past the batched kernel's value bound goes to int32: the
+    # bound is min(read, reference) x max |match|, |mismatch| plus the gaps
+    assert max(len(p) for p in panel) >= 125
+    with GpuScorer(panel, Scoring(100, -100, -27, -27), Mode.SEMIGLOBAL) as g:
+        assert g.half2_scores_len(10) and not g.half2_scores_len(400)
