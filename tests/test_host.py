@@ -91,12 +91,14 @@ def test_server_refuses_bad_requests_on_the_host():
 
 
 def test_fits_f16_matches_the_reference_bound():
-    """cuda/mod.rs:116-122 with the module's own example: the tRNA panel at
-    the default scoring is ~420, far inside 2048."""
+    """The known answers of crates/eschalign/src/cuda/mod.rs:783-792."""
     from eschalign_b200.scorer import fits_f16
     s = Scoring(2, -1, -10, -1)
-    assert fits_f16(150, 150, s)            # 150 * 2 + 21 = 321
-    assert fits_f16(5000, 1000, s)          # min(n, L) = 1000: 2021
-    assert not fits_f16(5000, 1100, s)      # 2221
-    assert not fits_f16(1014, 1014, s)      # 2049
-    assert fits_f16(1013, 1013, s)          # 2047
+    assert fits_f16(130, 200, s)
+    assert fits_f16(4096, 200, s)           # min(n, L) = 200: 421
+    assert fits_f16(1013, 4096, s)          # 2047
+    assert not fits_f16(1014, 4096, s)      # 2049
+    assert not fits_f16(1, 10, Scoring(1000, -1000, -1000, -1000))  # gaps alone 3000
+    s = Scoring(3, -2, -5, -2)
+    assert fits_f16(678, 1000, s)
+    assert not fits_f16(679, 1000, s)

@@ -43,6 +43,17 @@ def test_alphabet_and_scoring(oracle):
     assert not oracle.fits_i16(20000, 20000, D)
 
 
+def test_gap_convention(oracle):
+    """scoring.rs:199-204: gap(1) = -10, gap(3) = -12 at 2,-1,-10,-1 -- seen
+    through the score of a read that is its reference less 1 or 3 bases:
+    matches * 2 + open + (k - 1) * extend, end to end."""
+    from tests.helpers import Rng, random_seq
+    ref = oracle.encode(random_seq(Rng(0x5EED_6A9), 60, 0.0))
+    for k, gap in ((1, -10), (3, -12)):
+        q = np.concatenate([ref[:30], ref[30 + k:]])
+        assert oracle.score(q, ref, D, local=False) == 2 * (60 - k) + gap
+
+
 def test_tie_selection_known_answers(oracle):
     """mapper.rs:570-589: two ties in reference order, XS below the best."""
     E = oracle.encode
