@@ -1,0 +1,141 @@
+/*
+ * esg_align.c -- restatement of eschalign's traceback alignment.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker; see esg_oracle.h).
+ *   - eo_align: crates/eschalign/src/scalar.rs:182-206 (align), :213-289
+ *     (fill: the traceback DP, one trace code per cell, the end cell as the
+ *     first maximum of a column-major scan) and :292-364 (walk: diagonal,
+ *     then insertion, then deletion; extending inside a gap; local mode
+ *     stops at the first zero cell).
+ * Ops are written run-length encoded as BAM CIGAR words (len << 4 | op with
+ * M = 0, I = 1, D = 2), first to last.
+ */
+#include "esg_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+#define NEG (INT32_MIN / 4)
+/* trace codes (scalar.rs:167-175) */
+#define T_STOP 0
+#define T_DIAG 1
+#define T_INS 2
+#define T_DEL 3
+#define T_E_EXT 4
+#define T_F_EXT 8
+
+static int32_t sub_of(uint8_t a, uint8_t b, int32_t ma, int32_t mi)
+{
+    return (a == b || a == EO_WILDCARD || b == EO_WILDCARD) ? ma : mi;
+}
+
+int eo_align(const uint8_t* q, size_t n, const uint8_t* r, size_t m, int32_t ma, int32_t mi,
+             int32_t o, int32_t e, int local, eo_alignment* out, uint32_t* ops, size_t ops_cap)
+{
+    memset(out, 0, sizeof *out);
+    if (n == 0 || m == 0) return 0;
+    const size_t rows = n + 1;
+    uint8_t* trace = (uint8_t*)calloc(rows * (m + 1), 1);
+    int32_t* hcol = (int32_t*)calloc(rows, sizeof(int32_t));
+    int32_t* ecol = (int32_t*)malloc(rows * sizeof(int32_t));
+    if (!trace || !hcol || !ecol) {
+        free(trace);
+        free(hcol);
+        free(ecol);
+        return -1;
+    }
+    for (size_t i = 0; i < rows; i++) ecol[i] = NEG;
+    int32_t best = local ? 0 : NEG;
+    size_t bi = 0, bj = 0;
+    for (size_t j = 1; j <= m; j++) {
+        const uint8_t rj = r[j - 1];
+        uint8_t* col = trace + j * rows;
+        int32_t hdiag = 0, hup = 0, f = NEG;
+        const int last_col = j == m;
+        for (size_t k = 0; k < n; k++) {
+            const int32_t hleft = hcol[k + 1];
+            const int32_t e_open = hleft + o, e_ext = ecol[k + 1] + e;
+            const int32_t ev = e_open > e_ext ? e_open : e_ext;
+            const int32_t f_open = hup + o, f_ext = f + e;
+            f = f_open > f_ext ? f_open : f_ext;
+            const int32_t hd = hdiag + sub_of(q[k], rj, ma, mi);
+            int32_t h = hd > ev ? hd : ev;
+            if (f > h) h = f;
+            if (local && h < 0) h = 0;
+            uint8_t t = h == f ? T_INS : T_DEL;
+            if (h == hd) t = T_DIAG;
+            if (local && h == 0) t = T_STOP;
+            if (ev == e_ext) t |= T_E_EXT;
+            if (f == f_ext) t |= T_F_EXT;
+            col[k + 1] = t;
+            ecol[k + 1] = ev;
+            hdiag = hleft;
+            hcol[k + 1] = h;
+            hup = h;
+            if ((local || last_col) && h > best) {
+                best = h;
+                bi = k + 1;
+                bj = j;
+            }
+        }
+        if (!local && !last_col && hup > best) {
+            best = hup;
+            bi = n;
+            bj = j;
+        }
+    }
+    /* walk */
+    int rc = 0;
+    if (bi && bj) {
+        size_t i = bi, j = bj, n_rev = 0;
+        uint8_t* rev = (uint8_t*)malloc(n + m + 1);
+        int state = 0; /* 0 H, 1 E, 2 F */
+        while (i > 0 && j > 0) {
+            const uint8_t t = trace[j * rows + i];
+            if (state == 0) {
+                const uint8_t src = t & 3;
+                if (src == T_STOP) break;
+                if (src == T_DIAG) {
+                    rev[n_rev++] = 0;
+                    i--;
+                    j--;
+                } else if (src == T_INS) {
+                    state = 2;
+                } else {
+                    state = 1;
+                }
+            } else if (state == 2) {
+                rev[n_rev++] = 1;
+                if (!(t & T_F_EXT)) state = 0;
+                i--;
+            } else {
+                rev[n_rev++] = 2;
+                if (!(t & T_E_EXT)) state = 0;
+                j--;
+            }
+        }
+        size_t w = 0;
+        for (size_t k = n_rev; k-- > 0;) {
+            const uint32_t op = rev[k];
+            if (w && (ops[w - 1] & 0xf) == op) {
+                ops[w - 1] += 16;
+            } else if (w < ops_cap) {
+                ops[w++] = 16 | op;
+            } else {
+                rc = -2;
+                break;
+            }
+        }
+        free(rev);
+        out->score = best;
+        out->query_start = (uint32_t)i;
+        out->query_end = (uint32_t)bi;
+        out->ref_start = (uint32_t)j;
+        out->ref_end = (uint32_t)bj;
+        out->n_ops = (uint32_t)w;
+    }
+    free(trace);
+    free(hcol);
+    free(ecol);
+    return rc;
+}

@@ -163,6 +163,20 @@ int eo_scalar_map_pairs(const uint8_t* codes, const uint64_t* off, const uint32_
                         int32_t o, int32_t e, int both_strands, int local, int32_t min_score,
                         int threads, uint32_t cap, eo_pair_result* results, uint32_t* ties);
 
+/* ---- traceback (scalar.rs:182-364) ---------------------------------- */
+typedef struct eo_alignment {
+    int32_t score;
+    uint32_t query_start, query_end; /* 0-based, half-open */
+    uint32_t ref_start, ref_end;
+    uint32_t n_ops;                  /* BAM CIGAR words written */
+} eo_alignment;
+
+/* The best alignment's score, coordinates and ops (len << 4 | M=0 I=1 D=2).
+ * Returns 0, -1 out of memory, -2 ops_cap too small.  n or m empty, or a
+ * local alignment with no positive cell: all zero. */
+int eo_align(const uint8_t* q, size_t n, const uint8_t* r, size_t m, int32_t ma, int32_t mi,
+             int32_t o, int32_t e, int local, eo_alignment* out, uint32_t* ops, size_t ops_cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -185,6 +185,9 @@ def lib():
                                        C.c_void_p, u32p, u32p]
         L.eo_cpu_set_chunk.restype = None
         L.eo_cpu_set_chunk.argtypes = [C.c_int]
+        L.eo_align.restype = C.c_int
+        L.eo_align.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, C.c_int32, C.c_int32, C.c_int32,
+                               C.c_int32, C.c_int, C.c_void_p, u32p, C.c_size_t]
         L.eo_cpu_map_batch.restype = C.c_int
         L.eo_cpu_map_batch.argtypes = [C.c_void_p, u8p, u64p, u32p, C.c_uint32, C.c_int, C.c_int,
                                        C.c_int, C.c_uint32, C.c_void_p, u32p, i32p]
@@ -208,6 +211,49 @@ def revcomp(codes: np.ndarray) -> np.ndarray:
     """alphabet.rs:58-64."""
     c = np.asarray(codes, dtype=np.uint8)[::-1]
     return np.where(c == 4, 4, 3 - c).astype(np.uint8)
+
+
+ALIGN_DTYPE = np.dtype([("score", "<i4"), ("query_start", "<u4"), ("query_end", "<u4"),
+                        ("ref_start", "<u4"), ("ref_end", "<u4"), ("n_ops", "<u4")])
+CIGAR_OPS = "MID"
+
+
+def align(q, r, scoring, local: bool):
+    """scalar.rs:182-364: (record of ALIGN_DTYPE, ops as BAM CIGAR words)."""
+    q = np.ascontiguousarray(q, dtype=np.uint8)
+    r = np.ascontiguousarray(r, dtype=np.uint8)
+    out = np.zeros(1, dtype=ALIGN_DTYPE)
+    ops = np.zeros(q.size + r.size + 1, dtype=np.uint32)
+    rc = lib().eo_align(_p(q, C.c_uint8), q.size, _p(r, C.c_uint8), r.size, *scoring,
+                        int(bool(local)), out.ctypes.data, _p(ops, C.c_uint32), ops.size)
+    if rc:
+        raise RuntimeError(f"eo_align failed ({rc})")
+    return out[0], ops[:int(out[0]["n_ops"])]
+
+
+def cigar_string(ops) -> str:
+    return "".join(f"{int(w) >> 4}{CIGAR_OPS[int(w) & 0xf]}" for w in ops)
+
+
+def rescore(q, r, a, ops, scoring) -> int:
+    """Alignment::rescore (scalar.rs:90-117): the ops scored on their own."""
+    ma, mi, o, e = scoring
+    i, j, total = int(a["query_start"]), int(a["ref_start"]), 0
+    for w in ops:
+        op, n = int(w) & 0xf, int(w) >> 4
+        if op == 0:
+            for _ in range(n):
+                x, y = int(q[i]), int(r[j])
+                total += ma if (x == y or x == 4 or y == 4) else mi
+                i += 1
+                j += 1
+        else:
+            total += o + (n - 1) * e
+            if op == 1:
+                i += n
+            else:
+                j += n
+    return total
 
 
 def score(q, r, scoring, local: bool) -> int:

@@ -119,3 +119,42 @@ def test_cpu_batch_equals_scalar_batch(oracle):
             a, ta, ra, _ = prof.map_batch(codes, off, lens, local, both, cap=4, rows=True)
             b, tb, rb = oracle.scalar_map_batch(reads, panel, D, local, both, cap=4, rows=True)
             assert (a == b).all() and (ta == tb).all() and (ra == rb).all()
+
+
+def test_align_matches_parasail_golden(oracle):
+    """parasail_golden.rs:48-110 on the oracle's traceback: the 192 golden
+    cases' scores and coordinates (query_start, query_end, ref_start,
+    ref_end), and ops that re-score to the score, span the coordinates and
+    start and end with M."""
+    for c in golden()["cases"]:
+        q, r = oracle.encode(c["query"]), oracle.encode(c["reference"])
+        local = c["mode"] == "local"
+        a, ops = oracle.align(q, r, tuple(c["scheme"]), local)
+        label = (c["name"], c["mode"], c["scheme"])
+        assert int(a["score"]) == c["score"], label
+        assert oracle.score(q, r, tuple(c["scheme"]), local) == c["score"], label
+        assert (int(a["query_start"]), int(a["query_end"]), int(a["ref_start"]),
+                int(a["ref_end"])) == (c["query_start"], c["query_end"], c["ref_start"],
+                                       c["ref_end"]), label
+        assert oracle.rescore(q, r, a, ops, tuple(c["scheme"])) == c["score"], label
+        qs = sum(int(w) >> 4 for w in ops if int(w) & 0xf in (0, 1))
+        rs = sum(int(w) >> 4 for w in ops if int(w) & 0xf in (0, 2))
+        assert qs == a["query_end"] - a["query_start"] and rs == a["ref_end"] - a["ref_start"]
+        if len(ops):
+            assert int(ops[0]) & 0xf == 0 and int(ops[-1]) & 0xf == 0, label
+
+
+def test_align_known_answers(oracle):
+    """scalar.rs:378-430."""
+    E = oracle.encode
+    a, ops = oracle.align(E("ACGTACGT"), E("TTACGTACGTTT"), D, True)
+    assert (a["score"], a["query_start"], a["query_end"], a["ref_start"], a["ref_end"]) == \
+        (16, 0, 8, 2, 10) and oracle.cigar_string(ops) == "8M"
+    s = (2, -4, -3, -1)
+    a, ops = oracle.align(E("AAAACCCGGGGTTTT"), E("AAAACCCCGGGGTTTT"), s, True)
+    assert a["score"] == 15 * 2 - 3 and "1D" in oracle.cigar_string(ops)
+    a, ops = oracle.align(E("ACGTACGTCCCCC"), E("GGGGGACGTACGT"), D, False)
+    assert (a["score"], a["ref_start"], a["ref_end"], a["query_start"], a["query_end"]) == \
+        (16, 5, 13, 0, 8)
+    a, ops = oracle.align(E("AAAA"), E("CCCC"), D, True)
+    assert a["score"] == 0 and len(ops) == 0
