@@ -48,7 +48,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     """Compile csrc/esg_api.cu into libeschalign_b200.so and the integer-pipe
     probe csrc/esg_probe.cu into libesg_probe.so (sm_100a, ahead of time)."""
     newest = max(os.path.getmtime(s) for s in sources())
-    for src, out in ((("esg_api.cu", "esg_server.cu", "esg_noalloc.cu"), LIB_PATH),
+    for src, out in ((("esg_api.cu", "esg_server.cu", "esg_trace.cu", "esg_noalloc.cu"), LIB_PATH),
                      ("esg_probe.cu", PROBE_PATH)):
         if force or not os.path.exists(out) or os.path.getmtime(out) < newest:
             _compile(src, out, verbose)
@@ -113,6 +113,16 @@ class EsgAdapterConfig(C.Structure):
                 ("max_read_len", C.c_uint32)]
 
 
+class EsgAlignJob(C.Structure):
+    _fields_ = [("read", C.c_uint32), ("ref", C.c_uint32), ("reverse", C.c_uint32)]
+
+
+class EsgAlignment(C.Structure):
+    _fields_ = [("score", C.c_int32), ("query_start", C.c_uint32), ("query_end", C.c_uint32),
+                ("ref_start", C.c_uint32), ("ref_end", C.c_uint32), ("n_ops", C.c_uint32),
+                ("ops_offset", C.c_uint64)]
+
+
 class EsgServerOptions(C.Structure):
     _fields_ = [("max_batch_reads", C.c_uint32), ("max_inflight", C.c_uint32),
                 ("memory_budget", C.c_uint64), ("memory_headroom", C.c_uint64),
@@ -172,6 +182,10 @@ SIGNATURES = {
     "esg_score_pairs": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32,
                                     C.POINTER(EsgAdapterConfig), C.c_int32, C.c_uint32,
                                     C.c_void_p, _u32p, C.c_void_p, _u32p, _u32p, _i32p]),
+    "esg_align_batch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                    _u32p, C.c_uint64, _u64p]),
+    "esg_align_reads": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32, C.c_void_p,
+                                    C.c_uint32, C.c_void_p, _u32p, C.c_uint64, _u64p]),
     "esg_server_new": (C.c_int32, [C.POINTER(EsgServerOptions), C.POINTER(C.c_void_p)]),
     "esg_server_add_scorer": (C.c_int32, [C.c_void_p, C.c_void_p, _u32p]),
     "esg_server_submit": (C.c_int32, [C.c_void_p, C.c_uint32, _u8p, _u64p, _u32p, C.c_uint32,

@@ -142,6 +142,8 @@ struct esg_scorer {
   uint32_t* d_roff = nullptr;
   uint32_t* d_rlen = nullptr;
   uint32_t* d_ridx = nullptr;
+  std::vector<uint32_t> slot_of;   // reference -> slot of the k3 panel
+  std::vector<uint32_t> len_of;    // reference lengths, panel order
   int2* d_scratch = nullptr;
   int k3_blocks = 0;
   const void* k3_fn = nullptr;
@@ -580,6 +582,9 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
         (e = cudaMemcpy(sc->d_rlen, rlen.data(), n_refs * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(sc->d_ridx, order.data(), n_refs * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
       return cleanup(cuda_fail(e, "cudaMemcpy(k3 panel)"));
+    sc->slot_of.assign(n_refs, 0);
+    sc->len_of.assign(ref_len, ref_len + n_refs);
+    for (uint32_t k = 0; k < n_refs; ++k) sc->slot_of[order[k]] = k;
   }
 
   // --- launch geometry
@@ -998,6 +1003,31 @@ int esg_internal_device(const esg_scorer* sc) { return sc ? sc->device : 0; }
 uint32_t esg_internal_tie_capacity(const esg_scorer* sc) { return sc ? sc->cap : 0; }
 
 uint64_t esg_internal_panel_bases(const esg_scorer* sc) { return sc ? sc->panel_bases : 0; }
+
+void esg_internal_panel_of(esg_scorer* sc, esg_internal_panel* p) {
+  p->rcodes = sc->d_rcodes;
+  p->roff = sc->d_roff;
+  p->rlen = sc->d_rlen;
+  p->slot_of = sc->slot_of.data();
+  p->len_of = sc->len_of.data();
+  p->n_refs = sc->n_refs;
+  p->max_ref_len = sc->max_ref_len;
+  p->device = sc->device;
+  p->sm_count = sc->sm_count;
+  p->mode = sc->mode;
+  p->scoring = sc->scoring;
+  p->stream = sc->stream;
+  p->pool = sc->pool;
+}
+
+void esg_internal_batch_reads(const esg_batch* b, const uint8_t** codes, const uint64_t** off,
+                              const uint32_t** len, uint32_t* n_reads, const uint32_t** host_len) {
+  *codes = b->submitted ? b->d_codes : nullptr;
+  *off = b->d_off;
+  *len = b->d_len;
+  *n_reads = b->n_reads;
+  *host_len = b->h_len;
+}
 
 extern "C" {
 

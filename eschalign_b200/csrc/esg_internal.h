@@ -4,9 +4,36 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 #include "../../include/eschalign_b200.h"
 
 #define ESG_HIDDEN __attribute__((visibility("hidden")))
+
+// What the traceback needs of a scorer: the int32 kernel's panel copy
+// (1 B codes, references longest first: slot k is reference ridx[k]), the
+// host map reference -> slot, the scheme, and where to run.
+struct esg_internal_panel {
+  const uint8_t* rcodes;
+  const uint32_t* roff;
+  const uint32_t* rlen;
+  const uint32_t* slot_of;  // host array, n_refs entries
+  const uint32_t* len_of;   // host array: reference lengths, panel order
+  uint32_t n_refs;
+  uint32_t max_ref_len;
+  int device;
+  int sm_count;
+  int mode;
+  esg_scoring scoring;
+  cudaStream_t stream;
+  cudaMemPool_t pool;
+};
+ESG_HIDDEN void esg_internal_panel_of(esg_scorer* sc, esg_internal_panel* out);
+
+// A submitted batch's reads on the device (NULL codes if not submitted).
+ESG_HIDDEN void esg_internal_batch_reads(const esg_batch* b, const uint8_t** codes,
+                                         const uint64_t** off, const uint32_t** len,
+                                         uint32_t* n_reads, const uint32_t** host_len);
 
 // esg_prepare with read k at reads[k] (reads gathered from several requests,
 // no staging copy of their own).

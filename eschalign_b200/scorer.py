@@ -466,6 +466,25 @@ class GpuScorer:
         """cuda/mod.rs:524-528."""
         return self.finish(self.submit(self.prepare(reads, both_strands, full_rows)))
 
+    # -- traceback of winners (scalar.rs:182-364)
+    def align(self, reads, jobs) -> "Alignments":
+        """Trace (read, reference, reverse) jobs against `reads` (uploaded
+        here): coordinates and CIGAR of each, as scalar::align gives them."""
+        codes, off, lens = self._inputs(reads)
+        jobs = _jobs_array(jobs)
+        ref_len = self._panel_arrays[2]
+        bound = int(lens[jobs[:, 0]].sum(dtype=np.uint64) + ref_len[jobs[:, 1]].sum(dtype=np.uint64)) \
+            if jobs.shape[0] and (jobs[:, 0] < lens.size).all() and (jobs[:, 1] < ref_len.size).all() \
+            else 0
+        return _align_call(self._lib, self._lib.esg_align_reads,
+                           (self._h, _ptr(codes, C.c_uint8), _ptr(off, C.c_uint64),
+                            _ptr(lens, C.c_uint32), lens.size), jobs, bound)
+
+    def align_batch(self, batch: PendingBatch, jobs) -> "Alignments":
+        """The same against a finished batch's reads, still on the device
+        (finish it with keep=True)."""
+        return _align_call(self._lib, self._lib.esg_align_batch, (self._h, batch._h), jobs)
+
     # -- paired-end (pair.rs:157-234, fed as align.rs:2844-2872 feeds it)
     def prepare_pairs(self, mates, adapters=None, min_score: int = 0, both_strands: bool = True,
                       full_rows: bool = False) -> PreparedBatch:
@@ -519,6 +538,61 @@ class GpuScorer:
         """prepare_pairs + submit + finish_pairs."""
         return self.finish_pairs(self.submit(self.prepare_pairs(
             mates, adapters, min_score, both_strands, full_rows)))
+
+
+ALIGN_DTYPE = np.dtype([("score", "<i4"), ("query_start", "<u4"), ("query_end", "<u4"),
+                        ("ref_start", "<u4"), ("ref_end", "<u4"), ("n_ops", "<u4"),
+                        ("ops_offset", "<u8")])
+CIGAR_OPS = "MID"
+
+
+def cigar_string(ops) -> str:
+    """BAM CIGAR words (len << 4 | op) as text."""
+    return "".join(f"{int(w) >> 4}{CIGAR_OPS[int(w) & 0xf]}" for w in ops)
+
+
+def _jobs_array(jobs):
+    jobs = np.ascontiguousarray(np.asarray(jobs, dtype=np.uint32).reshape(-1, 3))
+    return jobs
+
+
+class Alignments:
+    """Traced alignments of a list of jobs: records (ALIGN_DTYPE) and the
+    CIGAR words they point into."""
+
+    def __init__(self, records, ops):
+        self.records = records
+        self.ops = ops
+
+    def __len__(self):
+        return self.records.size
+
+    def ops_of(self, k: int):
+        r = self.records[k]
+        o = int(r["ops_offset"])
+        return self.ops[o:o + int(r["n_ops"])]
+
+    def cigar(self, k: int) -> str:
+        return cigar_string(self.ops_of(k))
+
+
+def _align_call(lib, fn, args_head, jobs, bound=0):
+    """One call with room for `bound` words (an upper bound when known:
+    runs <= read + reference length per job), a second if it was short."""
+    jobs = _jobs_array(jobs)
+    n = jobs.shape[0]
+    rec = np.zeros(max(n, 1), dtype=ALIGN_DTYPE)
+    need = C.c_uint64()
+    cap = int(bound)
+    ops = np.zeros(max(cap, 1), dtype=np.uint32)
+    st = fn(*args_head, jobs.ctypes.data, n, rec.ctypes.data, _ptr(ops, C.c_uint32), cap,
+            C.byref(need))
+    if st == 7 and need.value > cap:  # room for the words, then again
+        ops = np.zeros(max(need.value, 1), dtype=np.uint32)
+        st = fn(*args_head, jobs.ctypes.data, n, rec.ctypes.data, _ptr(ops, C.c_uint32),
+                ops.size, C.byref(need))
+    _check(lib, st)
+    return Alignments(rec[:n], ops[:need.value])
 
 
 def select_hits(scores: ReadScores, min_score: int = 0, max_ties: int | None = None):

@@ -303,6 +303,43 @@ esg_status esg_score_pairs(esg_scorer* scorer, const uint8_t* codes, const uint6
                            esg_pair_result* pairs, uint32_t* pair_ties, esg_read_result* mates,
                            uint32_t* mate_ties, uint32_t* adapter_bases, int32_t* rows);
 
+/* ---- traceback of winners: scalar::align (crates/eschalign/src/scalar.rs:
+ * 182-364), the alignment eschalign traces for each read's tie set after
+ * scoring (mapper.rs:494-495 -> simd::align_pairs, simd/mod.rs:405-499).
+ * Same end cell (the first maximum of a column-major scan), same path
+ * (diagonal, then insertion, then deletion; extending inside a gap; local
+ * mode stops at the first zero cell). */
+typedef struct esg_align_job {
+    uint32_t read;     /* read index in the batch                         */
+    uint32_t ref;      /* reference, panel order                          */
+    uint32_t reverse;  /* 1: align the read's reverse complement          */
+} esg_align_job;
+
+/* One traced alignment.  Coordinates 0-based, half-open; ops are BAM CIGAR
+ * words (len << 4 | op; M = 0, I = 1, D = 2), ops[ops_offset ..
+ * ops_offset + n_ops), first to last.  A local alignment with no positive
+ * cell is all zero (scalar.rs:81-85). */
+typedef struct esg_alignment {
+    int32_t score;
+    uint32_t query_start, query_end;
+    uint32_t ref_start, ref_end;
+    uint32_t n_ops;
+    uint64_t ops_offset;
+} esg_alignment;
+
+/* Trace `jobs` against the reads of a submitted batch (its reads are still
+ * on the device: call after esg_finish, before esg_batch_free).  `ops`
+ * holds ops_capacity words; ESG_ERR_BAD_ARGUMENT if the alignments need
+ * more (the needed count is then in *ops_needed, which may be NULL). */
+esg_status esg_align_batch(esg_scorer* scorer, esg_batch* batch, const esg_align_job* jobs,
+                           uint32_t n_jobs, esg_alignment* out, uint32_t* ops,
+                           uint64_t ops_capacity, uint64_t* ops_needed);
+/* The same for reads given here (uploaded, then traced). */
+esg_status esg_align_reads(esg_scorer* scorer, const uint8_t* codes, const uint64_t* off,
+                           const uint32_t* len, uint32_t n_reads, const esg_align_job* jobs,
+                           uint32_t n_jobs, esg_alignment* out, uint32_t* ops,
+                           uint64_t ops_capacity, uint64_t* ops_needed);
+
 /* ---- serving: a request queue over resident scorers.  No counterpart in
  * the reference, which scores batches of one stream of reads and has no
  * serving mode.  Requests name a scorer slot (a resident panel under one
