@@ -269,6 +269,36 @@ def cpu_pairs_baseline(refs, pairs, scoring, seconds, threads=0):
             "pairs_per_s": n / dt, "seconds": dt}
 
 
+def traceback_stage(g, refs, reads, scoring, local, skip_cpu):
+    """The stage after scoring: trace each read's first tie (the primary,
+    mapper.rs:494-495) through esg_align_batch from a scored batch's reads on
+    the device; wall time incl. the host plan and copies.  Beside it the
+    CPU restatement (scalar align per job on all host threads) on a sample."""
+    b = g.submit(g.prepare(reads.tuple(), both_strands=True))
+    res = g.finish(b, keep=True)
+    has = np.nonzero(res.results["n_tied"] > 0)[0]
+    jobs = np.stack([has, res.ties[has, 0] >> 1, res.ties[has, 0] & 1], 1).astype(np.uint32)
+    g.align_batch(b, jobs[:1000])  # warm-up
+    t0 = time.perf_counter()
+    al = g.align_batch(b, jobs)
+    dt = time.perf_counter() - t0
+    b.free()
+    ref_len = np.array([len(r) for r in refs], dtype=np.int64)
+    cells = int((reads.lens[jobs[:, 0]].astype(np.int64) * ref_len[jobs[:, 1]]).sum())
+    out = {"jobs": int(jobs.shape[0]), "seconds": round(dt, 4),
+           "alignments_per_s": jobs.shape[0] / dt, "gcups": cells / dt / 1e9,
+           "cigar_words": int(al.ops.size)}
+    if not skip_cpu:
+        from oracle import oracle as O
+        n = min(jobs.shape[0], 40_000)
+        t0 = time.perf_counter()
+        _, _, used = O.align_batch(*reads.tuple(), refs, jobs[:n], scoring, local)
+        dt_c = time.perf_counter() - t0
+        out["cpu"] = {"alignments_per_s": n / dt_c, "cores": used, "kind": "port",
+                      "sample": f"first {n} jobs, scalar traceback per job"}
+    return out
+
+
 def reference_gpu_arms(refs, reads, scoring, local, device):
     """Comparison arms: the reference's own align_score_kernel (int) and
     align_score_kernel_h2 (half2), compiled ahead of time for sm_100a from its
@@ -529,6 +559,8 @@ def run_c2(a, ctx, rank):
         extras["plain_gcups"] = plain
         extras["batched_over_plain"] = value / plain
         extras["plain_sample"] = f"first {len(sub)} reads, both strands"
+        extras["traceback"] = traceback_stage(g, refs, sub, scoring, mode == "local",
+                                              a.no_cpu_baseline or rank != 0 or world != 1)
         arms = reference_gpu_arms(refs, sub, scoring, mode == "local", local_rank)
         if arms:
             arms["batched_over_ref_half2"] = value / arms["half2_gcups"]

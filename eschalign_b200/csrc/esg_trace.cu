@@ -388,7 +388,23 @@ esg_status align_impl(esg_scorer* sc, const uint8_t* d_codes, const uint64_t* d_
     if (S[k] > 0xffffu) return terr(ESG_ERR_BAD_ARGUMENT, "job %u: read too long", k);
   }
   // tiles of jobs up to 32 stripes (next fit, longest first); longer jobs alone
-  std::stable_sort(live.begin(), live.end(), [&](uint32_t a, uint32_t b) { return S[a] > S[b]; });
+  {
+    // longest first, stable: a counting sort on the stripes (long jobs, over
+    // 32 stripes, are few and sorted apart)
+    std::vector<uint32_t> longs, cnt(34, 0), sorted(live.size());
+    for (uint32_t k : live) ++cnt[std::min<uint32_t>(S[k], 33)];
+    uint32_t at = 0;
+    std::vector<uint32_t> start(34, 0);
+    for (int v = 33; v >= 1; --v) {
+      start[v] = at;
+      at += cnt[v];
+    }
+    for (uint32_t k : live) sorted[start[std::min<uint32_t>(S[k], 33)]++] = k;
+    const uint32_t n_long = cnt[33];
+    std::stable_sort(sorted.begin(), sorted.begin() + n_long,
+                     [&](uint32_t a, uint32_t b) { return S[a] > S[b]; });
+    live.swap(sorted);
+  }
   std::vector<uint32_t> order;
   std::vector<uint2> tasks;
   order.reserve(live.size());

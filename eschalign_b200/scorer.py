@@ -437,7 +437,9 @@ class GpuScorer:
         _check(self._lib, self._lib.esg_prepare(self._h, _ptr(codes, C.c_uint8),
                                                 _ptr(off, C.c_uint64), _ptr(lens, C.c_uint32),
                                                 lens.size, flags, C.byref(h)))
-        return PreparedBatch(self, h, int(lens.size), flags, None)
+        pb = PreparedBatch(self, h, int(lens.size), flags, None)
+        pb.lens = lens
+        return pb
 
     def submit(self, batch: PreparedBatch) -> PendingBatch:
         _check(self._lib, self._lib.esg_submit(self._h, batch._h))
@@ -483,7 +485,15 @@ class GpuScorer:
     def align_batch(self, batch: PendingBatch, jobs) -> "Alignments":
         """The same against a finished batch's reads, still on the device
         (finish it with keep=True)."""
-        return _align_call(self._lib, self._lib.esg_align_batch, (self._h, batch._h), jobs)
+        jobs = _jobs_array(jobs)
+        lens = getattr(batch, "lens", None)
+        ref_len = self._panel_arrays[2]
+        bound = 0
+        if lens is not None and jobs.shape[0] and (jobs[:, 0] < lens.size).all() and \
+                (jobs[:, 1] < ref_len.size).all():
+            bound = int(lens[jobs[:, 0]].sum(dtype=np.uint64) +
+                        ref_len[jobs[:, 1]].sum(dtype=np.uint64))
+        return _align_call(self._lib, self._lib.esg_align_batch, (self._h, batch._h), jobs, bound)
 
     # -- paired-end (pair.rs:157-234, fed as align.rs:2844-2872 feeds it)
     def prepare_pairs(self, mates, adapters=None, min_score: int = 0, both_strands: bool = True,
@@ -584,11 +594,11 @@ def _align_call(lib, fn, args_head, jobs, bound=0):
     rec = np.zeros(max(n, 1), dtype=ALIGN_DTYPE)
     need = C.c_uint64()
     cap = int(bound)
-    ops = np.zeros(max(cap, 1), dtype=np.uint32)
+    ops = np.empty(max(cap, 1), dtype=np.uint32)  # only the words written are touched
     st = fn(*args_head, jobs.ctypes.data, n, rec.ctypes.data, _ptr(ops, C.c_uint32), cap,
             C.byref(need))
     if st == 7 and need.value > cap:  # room for the words, then again
-        ops = np.zeros(max(need.value, 1), dtype=np.uint32)
+        ops = np.empty(max(need.value, 1), dtype=np.uint32)
         st = fn(*args_head, jobs.ctypes.data, n, rec.ctypes.data, _ptr(ops, C.c_uint32),
                 ops.size, C.byref(need))
     _check(lib, st)

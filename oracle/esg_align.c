@@ -139,3 +139,48 @@ int eo_align(const uint8_t* q, size_t n, const uint8_t* r, size_t m, int32_t ma,
     free(ecol);
     return rc;
 }
+
+/* The reference's CPU traceback of a batch of winners, the timed baseline:
+ * eo_align per job over OpenMP threads (the scalar path; the reference runs
+ * the same walk over its SIMD trace_pairs for up to 32 jobs at a time).
+ * Job k aligns read job_read[k] (reverse-complemented when job_rev[k])
+ * against reference job_ref[k]; ops go to ops + k * ops_stride. */
+int eo_align_batch(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
+                   const uint8_t* ref_codes, const uint64_t* ref_off, const uint32_t* ref_len,
+                   const uint32_t* job_read, const uint32_t* job_ref, const uint8_t* job_rev,
+                   uint32_t n_jobs, int32_t ma, int32_t mi, int32_t o, int32_t e, int local,
+                   int threads, eo_alignment* out, uint32_t* ops, size_t ops_stride)
+{
+    int nt = threads;
+#ifdef _OPENMP
+    extern int omp_get_max_threads(void);
+    if (nt <= 0) nt = omp_get_max_threads();
+#else
+    if (nt <= 0) nt = 1;
+#endif
+    int bad = 0;
+#pragma omp parallel num_threads(nt)
+    {
+        uint8_t* rc = NULL;
+        size_t rc_cap = 0;
+#pragma omp for schedule(dynamic, 64)
+        for (long k = 0; k < (long)n_jobs; k++) {
+            const uint8_t* q = codes + off[job_read[k]];
+            const size_t n = len[job_read[k]];
+            if (job_rev[k]) {
+                if (rc_cap < n) {
+                    free(rc);
+                    rc = (uint8_t*)malloc(n ? n : 1);
+                    rc_cap = n;
+                }
+                eo_revcomp_codes(q, n, rc);
+                q = rc;
+            }
+            if (eo_align(q, n, ref_codes + ref_off[job_ref[k]], ref_len[job_ref[k]], ma, mi, o,
+                         e, local, &out[k], ops + (size_t)k * ops_stride, ops_stride))
+                bad = 1;
+        }
+        free(rc);
+    }
+    return bad ? -1 : nt;
+}

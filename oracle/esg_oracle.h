@@ -176,6 +176,13 @@ typedef struct eo_alignment {
  * local alignment with no positive cell: all zero. */
 int eo_align(const uint8_t* q, size_t n, const uint8_t* r, size_t m, int32_t ma, int32_t mi,
              int32_t o, int32_t e, int local, eo_alignment* out, uint32_t* ops, size_t ops_cap);
+/* eo_align over a batch of jobs on OpenMP threads (the timed CPU baseline);
+ * returns the thread count, -1 if an ops stride was too small. */
+int eo_align_batch(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
+                   const uint8_t* ref_codes, const uint64_t* ref_off, const uint32_t* ref_len,
+                   const uint32_t* job_read, const uint32_t* job_ref, const uint8_t* job_rev,
+                   uint32_t n_jobs, int32_t ma, int32_t mi, int32_t o, int32_t e, int local,
+                   int threads, eo_alignment* out, uint32_t* ops, size_t ops_stride);
 
 #ifdef __cplusplus
 }

@@ -188,6 +188,10 @@ def lib():
         L.eo_align.restype = C.c_int
         L.eo_align.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, C.c_int32, C.c_int32, C.c_int32,
                                C.c_int32, C.c_int, C.c_void_p, u32p, C.c_size_t]
+        L.eo_align_batch.restype = C.c_int
+        L.eo_align_batch.argtypes = [u8p, u64p, u32p, u8p, u64p, u32p, u32p, u32p, u8p, C.c_uint32,
+                                     C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int, C.c_int,
+                                     C.c_void_p, u32p, C.c_size_t]
         L.eo_cpu_map_batch.restype = C.c_int
         L.eo_cpu_map_batch.argtypes = [C.c_void_p, u8p, u64p, u32p, C.c_uint32, C.c_int, C.c_int,
                                        C.c_int, C.c_uint32, C.c_void_p, u32p, i32p]
@@ -229,6 +233,29 @@ def align(q, r, scoring, local: bool):
     if rc:
         raise RuntimeError(f"eo_align failed ({rc})")
     return out[0], ops[:int(out[0]["n_ops"])]
+
+
+def align_batch(codes, off, lens, refs, jobs, scoring, local, threads=0):
+    """eo_align_batch: (records, ops [n_jobs, stride], threads used)."""
+    rc_, ro, rl = pack(refs)
+    jobs = np.asarray(jobs, dtype=np.uint32).reshape(-1, 3)
+    jr = np.ascontiguousarray(jobs[:, 0])
+    jf = np.ascontiguousarray(jobs[:, 1])
+    jv = np.ascontiguousarray(jobs[:, 2].astype(np.uint8))
+    codes = np.ascontiguousarray(codes, dtype=np.uint8)
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    lens = np.ascontiguousarray(lens, dtype=np.uint32)
+    stride = int(lens.max(initial=0)) + int(rl.max(initial=0)) + 1
+    out = np.zeros(jobs.shape[0], dtype=ALIGN_DTYPE)
+    ops = np.zeros((max(jobs.shape[0], 1), stride), dtype=np.uint32)
+    used = lib().eo_align_batch(_p(codes, C.c_uint8), _p(off, C.c_uint64), _p(lens, C.c_uint32),
+                                _p(rc_, C.c_uint8), _p(ro, C.c_uint64), _p(rl, C.c_uint32),
+                                _p(jr, C.c_uint32), _p(jf, C.c_uint32), _p(jv, C.c_uint8),
+                                jobs.shape[0], *scoring, int(bool(local)), threads,
+                                out.ctypes.data, _p(ops, C.c_uint32), stride)
+    if used < 0:
+        raise RuntimeError("eo_align_batch: ops stride too small")
+    return out, ops, used
 
 
 def cigar_string(ops) -> str:
