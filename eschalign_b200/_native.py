@@ -182,6 +182,8 @@ SIGNATURES = {
     "esg_score_pairs": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32,
                                     C.POINTER(EsgAdapterConfig), C.c_int32, C.c_uint32,
                                     C.c_void_p, _u32p, C.c_void_p, _u32p, _u32p, _i32p]),
+    "esg_merge_read_results": (C.c_int32, [C.c_void_p, _u32p, C.c_void_p, _u32p, C.c_uint32,
+                                           C.c_uint32, C.c_void_p, _u32p]),
     "esg_align_batch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                     _u32p, C.c_uint64, _u64p]),
     "esg_align_reads": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32, C.c_void_p,

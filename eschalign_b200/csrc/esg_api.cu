@@ -1388,6 +1388,64 @@ void esg_batch_free(esg_batch* b) {
   delete b;
 }
 
+esg_status esg_merge_read_results(const esg_read_result* a, const uint32_t* ta,
+                                  const esg_read_result* b, const uint32_t* tb, uint32_t n,
+                                  uint32_t cap, esg_read_result* out, uint32_t* tout) {
+  g_err.clear();
+  if (n && (!a || !b || !out || !ta || !tb || !tout))
+    return fail(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  if (cap < 1 || cap > ESG_MAX_TIE_CAPACITY)
+    return fail(ESG_ERR_BAD_ARGUMENT, "tie_capacity %u outside 1..%d", cap, ESG_MAX_TIE_CAPACITY);
+  std::vector<uint32_t> buf(cap);
+  for (uint32_t k = 0; k < n; ++k) {
+    const esg_read_result x = a[k], y = b[k];
+    const uint32_t* tx = ta + (size_t)k * cap;
+    const uint32_t* ty = tb + (size_t)k * cap;
+    esg_read_result r{};
+    const uint32_t keep = (x.flags | y.flags) & ESG_RESULT_RESCORED32;
+    if ((x.flags & ESG_RESULT_EMPTY) && (y.flags & ESG_RESULT_EMPTY)) {
+      r = x;
+      r.flags = ESG_RESULT_EMPTY;
+      for (uint32_t w = 0; w < cap; ++w) buf[w] = ESG_NO_TIE;
+    } else if (x.flags & ESG_RESULT_EMPTY || y.flags & ESG_RESULT_EMPTY) {
+      const bool use_x = !(x.flags & ESG_RESULT_EMPTY);
+      r = use_x ? x : y;
+      const uint32_t* t = use_x ? tx : ty;
+      for (uint32_t w = 0; w < cap; ++w) buf[w] = t[w];
+    } else {
+      const uint32_t nx = std::min(x.n_tied, cap), ny = std::min(y.n_tied, cap);
+      uint32_t w = 0;
+      if (x.best > y.best) {
+        r.best = x.best;
+        r.n_tied = x.n_tied;
+        r.suboptimal = std::max(std::max(x.suboptimal, y.suboptimal), y.best);
+        for (; w < nx; ++w) buf[w] = tx[w];
+      } else if (y.best > x.best) {
+        r.best = y.best;
+        r.n_tied = y.n_tied;
+        r.suboptimal = std::max(std::max(x.suboptimal, y.suboptimal), x.best);
+        for (; w < ny; ++w) buf[w] = ty[w];
+      } else {
+        r.best = x.best;
+        r.n_tied = x.n_tied + y.n_tied;
+        r.suboptimal = std::max(x.suboptimal, y.suboptimal);
+        uint32_t i = 0, j = 0;
+        while (w < cap && (i < nx || j < ny)) {
+          if (j >= ny || (i < nx && tx[i] < ty[j]))
+            buf[w++] = tx[i++];
+          else
+            buf[w++] = ty[j++];
+        }
+      }
+      for (; w < cap; ++w) buf[w] = ESG_NO_TIE;
+      r.flags = keep | (r.n_tied > cap ? ESG_RESULT_TIES_TRUNCATED : 0u);
+    }
+    out[k] = r;
+    memcpy(tout + (size_t)k * cap, buf.data(), (size_t)cap * 4);
+  }
+  return ESG_OK;
+}
+
 esg_status esg_batch_stats_get(const esg_batch* b, esg_batch_stats* out) {
   if (!b || !out) return fail(ESG_ERR_BAD_ARGUMENT, "NULL argument");
   *out = b->stats;

@@ -303,6 +303,17 @@ esg_status esg_score_pairs(esg_scorer* scorer, const uint8_t* codes, const uint6
                            esg_pair_result* pairs, uint32_t* pair_ties, esg_read_result* mates,
                            uint32_t* mate_ties, uint32_t* adapter_bases, int32_t* rows);
 
+/* Merge two sets of per-read results over disjoint candidate sets (e.g. two
+ * panel shards; candidate numbers global, (ref << 1) | reverse) into the
+ * result over their union, as mapper.rs:444-472 would give it: the higher
+ * best wins, equal bests add their tie counts and merge their lists in
+ * candidate order, XS is the best score outside the union's tie set.  Host
+ * only.  `out`/`out_ties` may alias `a`/`a_ties`. */
+esg_status esg_merge_read_results(const esg_read_result* a, const uint32_t* a_ties,
+                                  const esg_read_result* b, const uint32_t* b_ties,
+                                  uint32_t n_reads, uint32_t tie_capacity, esg_read_result* out,
+                                  uint32_t* out_ties);
+
 /* ---- traceback of winners: scalar::align (crates/eschalign/src/scalar.rs:
  * 182-364), the alignment eschalign traces for each read's tie set after
  * scoring (mapper.rs:494-495 -> simd::align_pairs, simd/mod.rs:405-499).

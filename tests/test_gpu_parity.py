@@ -351,3 +351,28 @@ def test_gpu_half2_lever_and_introspection(oracle):
     assert max(len(p) for p in panel) >= 125
     with GpuScorer(panel, Scoring(100, -100, -27, -27), Mode.SEMIGLOBAL) as g:
         assert g.half2_scores_len(10) and not g.half2_scores_len(400)
+
+
+def test_gpu_panel_shards_merge_to_the_whole_panel(oracle):
+    """Panel shards on one GPU (the multi-GPU path's scoring and merge, no
+    exchange): three shard scorers over a 300-ref panel with copies across
+    the cuts, merged, equal the whole-panel scorer."""
+    from eschalign_b200 import shards
+    rng = Rng(0x5EED_0109)
+    letters = random_panel(rng, 300, 200, 300)
+    panel = [encode(s) for s in letters]
+    panel += [panel[3].copy(), panel[150].copy(), panel[3].copy()]
+    reads = reads_for(rng, letters, 40)
+    cap = 4
+    ranges = shards.shard_ranges([len(p) for p in panel], 3)
+    parts = []
+    for lo, hi in ranges:
+        with GpuScorer(panel[lo:hi], Scoring(), Mode.LOCAL, tie_capacity=cap) as g:
+            r = g.score_batch(reads, both_strands=True)
+            parts.append((r.results, shards.globalize_ties(r.ties, lo)))
+    got_r, got_t = shards.merge(parts, cap)
+    with GpuScorer(panel, Scoring(), Mode.LOCAL, tie_capacity=cap) as g:
+        want = g.score_batch(reads, both_strands=True)
+    for f in ("best", "suboptimal", "n_tied", "flags"):
+        assert np.array_equal(got_r[f], want.results[f]), f
+    assert np.array_equal(got_t, want.ties)
