@@ -521,6 +521,7 @@ class GpuScorer:
         del keep
         b = PreparedBatch(self, h, int(lens.size), flags | BOTH_STRANDS, None)
         b.paired = True
+        b.lens = lens  # untrimmed: an upper bound for the traceback's CIGAR room
         return b
 
     def finish_pairs(self, batch: PendingBatch, keep: bool = False) -> PairBatchResult:

@@ -116,3 +116,40 @@ def test_trace_winners_of_a_scored_batch(oracle):
         assert (int(rec["query_start"]), int(rec["ref_start"]), int(rec["ref_end"])) == \
             (int(want["query_start"]), int(want["ref_start"]), int(want["ref_end"]))
         assert list(got.ops_of(k)) == list(wops)
+
+
+def test_trace_pair_winners_on_trimmed_mates(oracle):
+    """A paired batch's reads on the device are the trimmed mates: trace the
+    first tie of each pair (mate 1 on the template strand, mate 2 on the
+    other, pair.rs:135-137) against the oracle on the trimmed codes."""
+    from eschalign_b200 import adapter
+    refs = synth.panel_tiles()[:40]
+    P, _ = synth.pairs_c4(refs, n=200, seed=21)
+    mates = P.list()
+    trimmed, _ = oracle.trim_pairs(mates)
+    with GpuScorer(refs, Scoring(), Mode.SEMIGLOBAL) as g:
+        b = g.submit(g.prepare_pairs(mates, adapters=adapter.config()))
+        got = g.finish_pairs(b, keep=True)
+        jobs = []
+        for p in range(len(mates) // 2):
+            if got.pairs["n_tied"][p] == 0:
+                continue
+            c = int(got.pair_ties[p, 0])
+            ref, t = c >> 1, c & 1
+            jobs += [(2 * p, ref, t), (2 * p + 1, ref, 1 - t)]
+        al = g.align_batch(b, jobs)
+        b.free()
+    for k, (rd, ref, rev) in enumerate(jobs):
+        q = revcomp(trimmed[rd]) if rev else trimmed[rd]
+        want, wops = oracle.align(q, refs[ref], (2, -1, -10, -1), False)
+        rec = al.records[k]
+        assert int(rec["score"]) == int(want["score"]), k
+        assert (int(rec["query_start"]), int(rec["query_end"]), int(rec["ref_start"]),
+                int(rec["ref_end"])) == (int(want["query_start"]), int(want["query_end"]),
+                                         int(want["ref_start"]), int(want["ref_end"])), k
+        assert list(al.ops_of(k)) == list(wops), k
+    # each pair's two traced mates add up to the ranked sum
+    for p in range(0, len(jobs), 2):
+        pi = jobs[p][0] // 2
+        assert int(al.records[p]["score"]) + int(al.records[p + 1]["score"]) == \
+            int(got.pairs["best"][pi])
