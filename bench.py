@@ -345,6 +345,36 @@ def run_reference(a, rank, world):
                                     chunk=1)
         workload = "C3 10000 refs (300-1000 nt) x reads 50-1000 nt, both strands, local"
         dtype = "int16"
+    elif a.workload == "c1":
+        refs = synth.panel_tiles()
+        data = synth.reads_c1(refs)
+        panel_bases = sum(len(r) for r in refs)
+
+        def fn(_s):
+            from oracle import oracle as O
+            O.build()
+            prof = O.Profile(refs, C3_SCORING)
+            t0 = time.perf_counter()
+            _, _, _, used = prof.map_batch(*data.tuple(), local=True, both_strands=False)
+            dt = time.perf_counter() - t0
+            return {"value": data.bases() * panel_bases / dt / 1e9, "unit": "GCUPS",
+                    "cores": int(used), "kind": "port", "seconds": dt,
+                    "sample": f"all {len(data)} reads, forward strand, local 2,-1,-10,-1"}
+        warm = lambda: fn(0)  # noqa: E731
+        workload = "C1 10 000 reads x 164-ref panel, forward strand, local 2,-1,-10,-1"
+        dtype = "int16"
+    elif a.workload == "c5":
+        # the reference has no serving mode: its CPU path's throughput on the
+        # request mix's large panel (2000 x 300 nt), both strands
+        refs = synth.panel(2000, 300, 300, 0x5EED_0C5B)
+        rng = np.random.default_rng(0x5EED_0C05)
+        data = synth.mixed_reads(rng, refs, synth.lognormal_lengths(rng, 50_000, 110, 0.4, 20,
+                                                                    1000), 0.9, 0.08, 0.02, 0.01)
+        fn = lambda s: cpu_baseline(refs, data, C3_SCORING, "local", s)  # noqa: E731
+        warm = lambda: cpu_baseline(refs, data.slice(0, 500), C3_SCORING, "local", 0.5)  # noqa: E731
+        workload = ("C5 request mix: the reference has no serving mode; its CPU path on "
+                    "panel B (2000 x 300 nt) reads, both strands, local 2,-1,-10,-1")
+        dtype = "int16"
     else:
         refs = synth.panel_tiles()
         data = synth.reads_c2(refs, n=a.reads)
