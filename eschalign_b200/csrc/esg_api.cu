@@ -547,7 +547,8 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
     sc->pair_cols[p + 1] = sc->pair_cols[p] + (pairs[p].y & 0xffffu);
   sc->sel_base = sc->n_pairs * 8;  // uint16 units after the pair table
   const size_t raw = (size_t)sc->n_pairs * 16 + sels.size() * 2;
-  sc->blob_bytes = (uint32_t)((raw + 15) / 16 * 16);
+  // one spare selector past the last pair: a lane may load column m
+  sc->blob_bytes = (uint32_t)((raw + 2 + 15) / 16 * 16);
   std::vector<unsigned char> blob(sc->blob_bytes, 0);
   memcpy(blob.data(), pairs.data(), pairs.size() * 16);
   memcpy(blob.data() + (size_t)sc->n_pairs * 16, sels.data(), sels.size() * 2);
@@ -588,7 +589,7 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
   }
 
   // --- launch geometry
-  const size_t slots = (size_t)kK2Threads * (4 + cap) * 4;
+  const size_t slots = (size_t)kK2Threads * (4 + cap + kScrWords) * 4;
   sc->smem_panel = (size_t)sc->blob_bytes + slots <= 100 * 1024;
   set_k2_fn(sc);
   sc->k2_smem = (sc->smem_panel ? sc->blob_bytes : 0) + slots;

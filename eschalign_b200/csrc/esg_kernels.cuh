@@ -37,15 +37,33 @@ constexpr int kNeg16 = -31500;        // int16 stand-in for -infinity (biased do
 constexpr int kBiasLocal = 2048;      // local: H + B >= B >= |o|, |e|
 constexpr int kBiasSemiGlobal = -16384;  // semi-global: H + B < 0 while |H| < 12000
 constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
-// k2 CTA shape: 4 warps, 5 resident CTAs per SM (20 warps, <= 102 registers;
-// 4 CTAs for panels with wildcards, whose per-row tables need more; 3 for
-// 32-row stripes) measured fastest on B200 for the C2 workload (vs 8 warps x
-// 2 CTAs).
+// k2 CTA shape: 4 warps, 4 resident CTAs per SM (16 warps, <= 128
+// registers; 3 for 32-row stripes).  Tuning knobs, each measured on B200 on
+// the C2 workload (1 M reads of ~110 nt x 164 references, both strands):
+//   ESG_K2_WARPS / ESG_K2_MIN_BLOCKS  CTA shape (4 x 4 beat 4 x 5 at 96
+//       registers once local mode reads its scores from shared memory, and
+//       8 warps x 2 CTAs)
+//   ESG_SC_LDS  modes whose per-cell scores come from a per-thread record in
+//       shared memory (bit 0 local, bit 1 semi-global) instead of one PRMT
+//       per cell: local +5.0 %, semi-global -1.5 % (spills)
+//   ESG_SEL_PREFETCH  modes that load a lane's next column selector a column
+//       ahead (bit 0 local, bit 1 semi-global): +2 % in both with the above
+//   ESG_STEADY_UNROLL  unroll of local mode's unchecked column loop, 16-row
+//       stripes (8: +0.9 % over 4; 32-row stripes have no registers for it)
 #ifndef ESG_K2_WARPS
 #define ESG_K2_WARPS 4
 #endif
 #ifndef ESG_K2_MIN_BLOCKS
-#define ESG_K2_MIN_BLOCKS 5
+#define ESG_K2_MIN_BLOCKS 4
+#endif
+#ifndef ESG_SC_LDS
+#define ESG_SC_LDS 1
+#endif
+#ifndef ESG_SEL_PREFETCH
+#define ESG_SEL_PREFETCH 3
+#endif
+#ifndef ESG_STEADY_UNROLL
+#define ESG_STEADY_UNROLL 8
 #endif
 constexpr int kK2Warps = ESG_K2_WARPS;  // warps per k2 CTA
 constexpr int kK2Threads = kK2Warps * 32;
@@ -53,6 +71,16 @@ constexpr int kK3Threads = 256;
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kNoRef = 0xffffffffu;
 constexpr uint32_t kMaxCap = 32;       // largest tie capacity (ESG_MAX_TIE_CAPACITY)
+// per-thread shared words of the column score record (one per row code
+// 0-5), word c of thread t at c * kK2Threads + t: every thread in its own bank
+constexpr int kScrWords = ESG_SC_LDS ? 6 : 0;
+constexpr uint32_t kScrStride = (uint32_t)kK2Threads * 4;  // bytes between code words
+template <bool kLocal>
+__host__ __device__ constexpr bool sc_lds() { return (ESG_SC_LDS & (kLocal ? 1 : 2)) != 0; }
+template <bool kLocal>
+__host__ __device__ constexpr bool sel_prefetch() {
+  return (ESG_SEL_PREFETCH & (kLocal ? 1 : 2)) != 0;
+}
 
 // error bits in counters[2]
 constexpr uint32_t kErrPanelWait = 1u;
@@ -67,6 +95,14 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   uint32_t d;
   asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
   return d;
+}
+__device__ __forceinline__ void st_shared_u32(uint32_t addr, uint32_t v) {
+  asm volatile("st.shared.u32 [%0], %1;" ::"r"(addr), "r"(v));
+}
+__device__ __forceinline__ uint32_t ld_shared_u32(uint32_t addr) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr));
+  return v;
 }
 __device__ __forceinline__ uint32_t add16x2(uint32_t a, uint32_t b) {
   uint32_t d;
@@ -227,7 +263,8 @@ __device__ __forceinline__ bool stage_panel(void* smem, const void* gsrc, uint32
 // reference of the pair, high half: the shorter one).
 //
 // Lane state (rows r = 0..15 of the lane's stripe):
-//   ta[r], tb[r]  PRMT tables of the row's read code c: byte x of {tb, ta} is
+//   ta[r], tb[r]  PRMT tables of the row's read code c (or, with score
+//                 records, the shared address of code c's word): byte x of {tb, ta} is
 //                 s(c, x) - o for reference code x = 0..3, 4 (wildcard), and
 //                 a padding column's score at x = 5.  Both halves use the
 //                 same table; the column's selector picks a byte per half
@@ -247,6 +284,18 @@ __device__ __forceinline__ bool stage_panel(void* smem, const void* gsrc, uint32
 // high half's carry-out is discarded.  Padding columns (garbage that may
 // wrap) are only ever in the high half.  5.5 ALU instructions per cell pair
 // in local mode, 5 in semi-global, plus one IMAD.
+//
+// Score records (kLds, local mode): the PRMT moves from every cell to every
+// column.  At each column the lane writes the column's score word for each
+// read code (PRMT of that code's tables, codes 0-3, and the wildcard code 4
+// when the warp holds a wildcard row) to its own record in shared memory,
+// then each row loads its code's word: ta[r] holds that word's shared
+// address instead of a table.  The padding code's word is a constant written
+// once per pass (local: -128 in both halves, H stays 0 under the floor).
+// The record's words of one code are kK2Threads words apart, so every lane
+// reads and writes its own bank.  4.5 ALU instructions per cell pair plus
+// four PRMTs per column, one shared load per cell pair, one IMAD; the
+// loads go to the otherwise idle load/store pipe (C2 local: +5 %).
 //
 // The lane with skew k works on column j = t - k at step t; its top input
 // (G and F of the row above) is the previous lane's bottom output of step
@@ -278,13 +327,22 @@ __device__ __forceinline__ uint32_t load_sel(const uint16_t* sp, int j) {
 }
 
 template <int R, bool kLocal, bool kPanelW, bool kLong, bool kSmem>
-__device__ __forceinline__ void pair_pass(const uint32_t (&ta)[R],
+__device__ __forceinline__ void pair_pass(const K2Params& P, uint32_t scr, bool wild,
+                                          const uint32_t (&ta)[R],
                                           const uint32_t (&tb)[kPanelW ? R : 1], int skew,
                                           bool active_lane, bool first, uint32_t padmask, int m,
                                           int jshort, const uint16_t* __restrict__ sp, int steps,
                                           const PassConst& K, uint2* buf, bool from_buf,
                                           bool to_buf, uint32_t& v, uint32_t& lr) {
   const int lane = threadIdx.x & 31;
+  constexpr bool kLds = sc_lds<kLocal>() && !kLong;
+  constexpr bool kPre = sel_prefetch<kLocal>();
+  if constexpr (kLds) {
+    // padding rows: local, -128 against every column (H stays 0 under the
+    // floor); semi-global, s = 0 (H = 0 exactly against real columns; the
+    // short half's columns past its end are never read)
+    st_shared_u32(scr + 5 * kScrStride, kLocal ? 0xff80ff80u : pack16x2(-P.o, -P.o));
+  }
   uint32_t g[R], ev[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
@@ -299,6 +357,7 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[R],
   // inactive lanes of a tile sit at a skew no step reaches; only the long
   // path needs the per-lane bound (its lanes past the query's last stripe)
   const int mlim = (kLong && !active_lane) ? 0 : m;
+  uint32_t seln = kPre ? load_sel<kSmem>(sp, 0) : 0u;
 
   // One column of the lane's stripe, given the top input (G, F of the row
   // above at this column).
@@ -310,13 +369,33 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[R],
         ft = b.y;
       }
     }
-    const uint32_t sel = load_sel<kSmem>(sp, j);
+    uint32_t sel;
+    if constexpr (kPre) {
+      // columns of a lane come in order: the next one's selector is loaded
+      // a column ahead (the blob holds one spare selector past the last pair)
+      sel = seln;
+      seln = load_sel<kSmem>(sp, j + 1);
+    } else {
+      sel = load_sel<kSmem>(sp, j);
+    }
+    if constexpr (kLds) {
+      // the column's score record: one word per read code, in this thread's
+      // own bank, read back per row below (wildcard rows only when the warp
+      // has some)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) st_shared_u32(scr + c * kScrStride, prmt(P.tab_a[c], P.tab_b[c], sel));
+      if (wild) st_shared_u32(scr + 4 * kScrStride, prmt(P.tab_a[4], P.tab_b[4], sel));
+    }
     uint32_t gd = gdc;
     gdc = gt;
     uint32_t gup = gt, f = ft, h15 = 0, hprev = 0;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const uint32_t sc = prmt(ta[r], tb[kPanelW ? r : 0], sel);
+      uint32_t sc;
+      if constexpr (kLds)
+        sc = ld_shared_u32(ta[r]);
+      else
+        sc = prmt(ta[r], tb[kPanelW ? r : 0], sel);
       ev[r] = __viaddmax_s16x2(ev[r], K.e2, g[r]);
       f = __viaddmax_s16x2(f, K.e2, gup);
       const uint32_t h1 = __viaddmax_s16x2(gd, sc, ev[r]);
@@ -382,9 +461,9 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[R],
         if ((unsigned)j < (unsigned)mlim) column(j, gt, ft);
       }
       const int sk = active_lane ? skew : 0;
-      // unrolled by 4 (C2: +1.2 % over 2; 8 measured slower); 32-row stripes
+      // unrolled (ESG_STEADY_UNROLL) for 16-row stripes; 32-row stripes
       // have no registers to spare
-      constexpr int kUnroll = R <= 16 ? 4 : 1;
+      constexpr int kUnroll = R <= 16 ? ESG_STEADY_UNROLL : 1;
 #pragma unroll kUnroll
       for (; t < m; ++t) {
         uint32_t gt, ft;
@@ -419,11 +498,12 @@ __device__ __forceinline__ void pair_pass(const uint32_t (&ta)[R],
 
 // Row tables of stripe `s` of a query (n codes at q, reverse complement if
 // rc): row r is read row i = 16 s + r - pad; rows before the read are padding.
-template <int R, bool kPanelW>
-__device__ __forceinline__ void row_tables(const K2Params& P, const uint8_t* q, uint32_t n,
+template <int R, bool kPanelW, bool kLds>
+__device__ __forceinline__ bool row_tables(const K2Params& P, const uint8_t* q, uint32_t n,
                                            bool rc, bool valid, int s, int pad,
                                            uint32_t (&ta)[R],
-                                           uint32_t (&tb)[kPanelW ? R : 1]) {
+                                           uint32_t (&tb)[kPanelW ? R : 1], uint32_t scr = 0) {
+  bool wild = false;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int i = s * R + r - pad;
@@ -433,10 +513,16 @@ __device__ __forceinline__ void row_tables(const K2Params& P, const uint8_t* q, 
       x = x > 4 ? 4 : x;
       c = (rc && x < 4) ? 3 - x : x;
     }
-    ta[r] = P.tab_a[c];
-    if constexpr (kPanelW) tb[r] = P.tab_b[c];
+    wild |= c == 4;
+    if constexpr (kLds) {
+      ta[r] = scr + c * kScrStride;  // the row code's word in the column record
+    } else {
+      ta[r] = P.tab_a[c];
+      if constexpr (kPanelW) tb[r] = P.tab_b[c];
+    }
   }
   if constexpr (!kPanelW) tb[0] = P.tab_b[0];
+  return __any_sync(kFull, wild);
 }
 
 // The last lane of a query folds one reference pair's two scores into the
@@ -524,6 +610,9 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2
   // this lane's query slot: {best, suboptimal, n_tied, flags, ties[cap]}
   int* slot = slots + (size_t)(wib * 32 + lane) * (4 + cap);
   uint32_t* sties = reinterpret_cast<uint32_t*>(slot + 4);
+  // column score records: word c * kK2Threads + thread (bank = lane)
+  const uint32_t scr = (uint32_t)__cvta_generic_to_shared(slots + (size_t)kK2Threads * (4 + cap)) +
+                       threadIdx.x * 4u;
   uint2* lbuf = P.lbuf ? P.lbuf + ((size_t)blockIdx.x * kK2Warps + wib) * P.lbuf_cols : nullptr;
 
   const int bias = P.bias;
@@ -576,10 +665,10 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2
           const bool valid = s < S;
           uint32_t ta[R];
           uint32_t tb[kPanelW ? R : 1];
-          row_tables<R, kPanelW>(P, q, n, rc, valid, s, pad, ta, tb);
+          row_tables<R, kPanelW, false>(P, q, n, rc, valid, s, pad, ta, tb);
           const uint32_t padmask = (s == 0) ? ((1u << pad) - 1u) : 0u;
           uint32_t v, lr;
-          pair_pass<R, kLocal, kPanelW, true, kSmemPanel>(ta, tb, lane, valid, s == 0, padmask, mA,
+          pair_pass<R, kLocal, kPanelW, true, kSmemPanel>(P, 0u, false, ta, tb, lane, valid, s == 0, padmask, mA,
                                                        jshort, sp,
                                            mA + 31, K, lbuf, pass > 0, pass + 1 < passes, v, lr);
           acc = max16x2(acc, v);
@@ -632,7 +721,8 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2
 
     uint32_t ta[R];
     uint32_t tb[kPanelW ? R : 1];
-    row_tables<R, kPanelW>(P, valid ? P.codes + P.off[rd] : P.codes, n, rc, valid, s, pad, ta, tb);
+    const bool wild = row_tables<R, kPanelW, sc_lds<kLocal>()>(
+        P, valid ? P.codes + P.off[rd] : P.codes, n, rc, valid, s, pad, ta, tb, scr);
     // rows of the read's top padding (first lane only): excluded from the
     // semi-global last-column maximum
     const uint32_t padmask = (valid && first) ? ((1u << pad) - 1u) : 0u;
@@ -649,7 +739,7 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2
       const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);  // mA >= mB
       const int jshort = (mB > 0 && mB < mA) ? mB - 1 : -1;
       uint32_t v, lr;
-      pair_pass<R, kLocal, kPanelW, false, kSmemPanel>(ta, tb, s, valid, first, padmask, mA, jshort,
+      pair_pass<R, kLocal, kPanelW, false, kSmemPanel>(P, scr, wild, ta, tb, s, valid, first, padmask, mA, jshort,
                                         sels + pm.x, mA + smax - 1, K, nullptr, false, false, v,
                                         lr);
       // per-query maximum, to the query's last lane
