@@ -48,7 +48,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     """Compile csrc/esg_api.cu into libeschalign_b200.so and the integer-pipe
     probe csrc/esg_probe.cu into libesg_probe.so (sm_100a, ahead of time)."""
     newest = max(os.path.getmtime(s) for s in sources())
-    for src, out in ((("esg_api.cu", "esg_server.cu", "esg_trace.cu", "esg_noalloc.cu"), LIB_PATH),
+    for src, out in ((("esg_api.cu", "esg_server.cu", "esg_trace.cu", "esg_map.cu",
+                        "esg_noalloc.cu"), LIB_PATH),
                      ("esg_probe.cu", PROBE_PATH)):
         if force or not os.path.exists(out) or os.path.getmtime(out) < newest:
             _compile(src, out, verbose)
@@ -123,6 +124,11 @@ class EsgAlignment(C.Structure):
                 ("ops_offset", C.c_uint64)]
 
 
+class EsgMapOptions(C.Structure):
+    _fields_ = [("min_score", C.c_int32), ("max_ties", C.c_uint32),
+                ("both_strands", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class EsgServerOptions(C.Structure):
     _fields_ = [("max_batch_reads", C.c_uint32), ("max_inflight", C.c_uint32),
                 ("memory_budget", C.c_uint64), ("memory_headroom", C.c_uint64),
@@ -188,6 +194,13 @@ SIGNATURES = {
                                     _u32p, C.c_uint64, _u64p]),
     "esg_align_reads": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32, C.c_void_p,
                                     C.c_uint32, C.c_void_p, _u32p, C.c_uint64, _u64p]),
+    "esg_map_reads": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32,
+                                  C.POINTER(EsgMapOptions), _u8p, _u64p, C.POINTER(C.c_void_p)]),
+    "esg_mapping_reads": (C.c_void_p, [C.c_void_p, _u32p]),
+    "esg_mapping_hits": (C.c_void_p, [C.c_void_p, _u64p]),
+    "esg_mapping_ops": (C.c_void_p, [C.c_void_p, _u64p]),
+    "esg_mapping_md": (C.c_void_p, [C.c_void_p, _u64p]),
+    "esg_mapping_free": (None, [C.c_void_p]),
     "esg_server_new": (C.c_int32, [C.POINTER(EsgServerOptions), C.POINTER(C.c_void_p)]),
     "esg_server_add_scorer": (C.c_int32, [C.c_void_p, C.c_void_p, _u32p]),
     "esg_server_submit": (C.c_int32, [C.c_void_p, C.c_uint32, _u8p, _u64p, _u32p, C.c_uint32,

@@ -144,6 +144,8 @@ struct esg_scorer {
   uint32_t* d_ridx = nullptr;
   std::vector<uint32_t> slot_of;   // reference -> slot of the k3 panel
   std::vector<uint32_t> len_of;    // reference lengths, panel order
+  std::vector<uint8_t> h_codes;    // the panel's codes (0-4), panel order (host)
+  std::vector<uint64_t> h_off;     // reference r at h_codes[h_off[r]]
   int2* d_scratch = nullptr;
   int k3_blocks = 0;
   const void* k3_fn = nullptr;
@@ -585,6 +587,13 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
       return cleanup(cuda_fail(e, "cudaMemcpy(k3 panel)"));
     sc->slot_of.assign(n_refs, 0);
     sc->len_of.assign(ref_len, ref_len + n_refs);
+    sc->h_off.resize(n_refs);
+    sc->h_codes.reserve(bases);
+    for (uint32_t r = 0; r < n_refs; ++r) {
+      sc->h_off[r] = sc->h_codes.size();
+      for (uint32_t j = 0; j < ref_len[r]; ++j)
+        sc->h_codes.push_back((uint8_t)code_of(ref_codes[ref_off[r] + j]));
+    }
     for (uint32_t k = 0; k < n_refs; ++k) sc->slot_of[order[k]] = k;
   }
 
@@ -1011,6 +1020,8 @@ void esg_internal_panel_of(esg_scorer* sc, esg_internal_panel* p) {
   p->rlen = sc->d_rlen;
   p->slot_of = sc->slot_of.data();
   p->len_of = sc->len_of.data();
+  p->h_codes = sc->h_codes.data();
+  p->h_off = sc->h_off.data();
   p->n_refs = sc->n_refs;
   p->max_ref_len = sc->max_ref_len;
   p->device = sc->device;

@@ -3,6 +3,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -19,6 +20,8 @@ struct esg_internal_panel {
   const uint32_t* rlen;
   const uint32_t* slot_of;  // host array, n_refs entries
   const uint32_t* len_of;   // host array: reference lengths, panel order
+  const uint8_t* h_codes;   // host array: the panel's codes (0-4), panel order
+  const uint64_t* h_off;    // host array: reference r at h_codes[h_off[r]]
   uint32_t n_refs;
   uint32_t max_ref_len;
   int device;
@@ -50,3 +53,8 @@ ESG_HIDDEN int esg_internal_device(const esg_scorer* sc);
 ESG_HIDDEN uint32_t esg_internal_tie_capacity(const esg_scorer* sc);
 // Bases of the scorer's panel (DP cells per read base and strand).
 ESG_HIDDEN uint64_t esg_internal_panel_bases(const esg_scorer* sc);
+
+// esg_align_batch with the CIGAR words into a vector sized to fit.
+ESG_HIDDEN esg_status esg_internal_align_batch(esg_scorer* sc, esg_batch* b,
+                                               const esg_align_job* jobs, uint32_t n_jobs,
+                                               esg_alignment* out, std::vector<uint32_t>* ops);

@@ -358,7 +358,8 @@ size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 esg_status align_impl(esg_scorer* sc, const uint8_t* d_codes, const uint64_t* d_off,
                       const uint32_t* d_len, uint32_t n_reads, const uint32_t* h_len,
                       const esg_align_job* jobs, uint32_t n_jobs, esg_alignment* out,
-                      uint32_t* ops, uint64_t ops_capacity, uint64_t* ops_needed) {
+                      uint32_t* ops, uint64_t ops_capacity, uint64_t* ops_needed,
+                      std::vector<uint32_t>* grow = nullptr) {
   esg_internal_panel P{};
   esg_internal_panel_of(sc, &P);
   if (n_jobs && (!jobs || !out)) return terr(ESG_ERR_BAD_ARGUMENT, "jobs/out must not be NULL");
@@ -542,6 +543,11 @@ esg_status align_impl(esg_scorer* sc, const uint8_t* d_codes, const uint64_t* d_
     need += (uint32_t)res2[k].y;
   }
   if (ops_needed) *ops_needed = need;
+  if (grow) {
+    grow->resize(need);
+    ops = grow->data();
+    ops_capacity = need;
+  }
   if (need > ops_capacity || (need && !ops)) {
     cudaFreeAsync(mem, st);
     return terr(ESG_ERR_BAD_ARGUMENT, "the alignments need %llu CIGAR words, room for %llu",
@@ -578,6 +584,20 @@ esg_status align_impl(esg_scorer* sc, const uint8_t* d_codes, const uint64_t* d_
 }
 
 }  // namespace
+
+esg_status esg_internal_align_batch(esg_scorer* sc, esg_batch* b, const esg_align_job* jobs,
+                                    uint32_t n_jobs, esg_alignment* out,
+                                    std::vector<uint32_t>* ops) {
+  const uint8_t* codes = nullptr;
+  const uint64_t* off = nullptr;
+  const uint32_t* len = nullptr;
+  const uint32_t* h_len = nullptr;
+  uint32_t n_reads = 0;
+  esg_internal_batch_reads(b, &codes, &off, &len, &n_reads, &h_len);
+  if (!codes) return terr(ESG_ERR_BAD_ARGUMENT, "the batch is not submitted");
+  return align_impl(sc, codes, off, len, n_reads, h_len, jobs, n_jobs, out, nullptr, 0, nullptr,
+                    ops);
+}
 
 extern "C" {
 

@@ -495,6 +495,41 @@ class GpuScorer:
                         ref_len[jobs[:, 1]].sum(dtype=np.uint64))
         return _align_call(self._lib, self._lib.esg_align_batch, (self._h, batch._h), jobs, bound)
 
+    # -- mapping (mapper.rs:400-552)
+    def map_reads(self, reads, min_score: int = 0, max_ties: int | None = None,
+                  both_strands: bool = False, ref_letters=None) -> "Mappings":
+        """Aligner::map_reads_scored over this scorer: per read the best, XS,
+        tie count and the traced hits (primary first) with MD and NM.
+        `ref_letters`: the panel's letters (a list of str/bytes, panel order)
+        for MD; without them MD spells the panel's codes as A/C/G/T/N."""
+        codes, off, lens = self._inputs(reads)
+        opts = _native.EsgMapOptions(int(min_score),
+                                     0xFFFFFFFF if max_ties is None else int(max_ties),
+                                     int(bool(both_strands)), 0)
+        if max_ties is not None and not 0 <= int(max_ties) < 0xFFFFFFFF:
+            raise ValueError("max_ties must be in [0, 2^32 - 1)")
+        lp = lo = None
+        if ref_letters is not None:
+            if len(ref_letters) != len(self.panel):
+                raise ValueError("ref_letters: one entry per reference")
+            bl = [r.encode() if isinstance(r, str) else bytes(r) for r in ref_letters]
+            for k, b in enumerate(bl):
+                if len(b) != int(self._panel_arrays[2][k]):
+                    raise ValueError(f"ref_letters[{k}]: length differs from the reference")
+            letters = np.frombuffer(b"".join(bl) or b"\0", dtype=np.uint8)
+            loff = np.zeros(len(bl), dtype=np.uint64)
+            if len(bl) > 1:
+                loff[1:] = np.cumsum([len(b) for b in bl[:-1]], dtype=np.uint64)
+            lp, lo = _ptr(letters, C.c_uint8), _ptr(loff, C.c_uint64)
+        h = C.c_void_p()
+        _check(self._lib, self._lib.esg_map_reads(self._h, _ptr(codes, C.c_uint8),
+                                                  _ptr(off, C.c_uint64), _ptr(lens, C.c_uint32),
+                                                  lens.size, C.byref(opts), lp, lo, C.byref(h)))
+        try:
+            return Mappings._copy(self._lib, h)
+        finally:
+            self._lib.esg_mapping_free(h)
+
     # -- paired-end (pair.rs:157-234, fed as align.rs:2844-2872 feeds it)
     def prepare_pairs(self, mates, adapters=None, min_score: int = 0, both_strands: bool = True,
                       full_rows: bool = False) -> PreparedBatch:
@@ -585,6 +620,73 @@ class Alignments:
 
     def cigar(self, k: int) -> str:
         return cigar_string(self.ops_of(k))
+
+
+MAPPING_DTYPE = np.dtype([("best_score", "<i4"), ("suboptimal", "<i4"), ("n_tied", "<u4"),
+                          ("flags", "<u4"), ("n_hits", "<u4"), ("reserved", "<u4"),
+                          ("first_hit", "<u8")])
+HIT_DTYPE = np.dtype([("reference", "<u4"), ("reverse", "<u4"), ("score", "<i4"),
+                      ("query_start", "<u4"), ("query_end", "<u4"), ("ref_start", "<u4"),
+                      ("ref_end", "<u4"), ("n_ops", "<u4"), ("ops_offset", "<u8"),
+                      ("nm", "<u4"), ("md_len", "<u4"), ("md_offset", "<u8")])
+MAPPING_HAS_BEST = 1
+MAPPING_HAS_SUBOPTIMAL = 2
+
+
+class Mappings:
+    """esg_map_reads' output: per read a MAPPING_DTYPE record, its hits
+    (HIT_DTYPE) and their CIGAR words and MD strings."""
+
+    def __init__(self, reads, hits, ops, md: bytes):
+        self.reads = reads
+        self.hits = hits
+        self.ops = ops
+        self.md_bytes = md
+
+    @classmethod
+    def _copy(cls, lib, h):
+        def arr(fn, ct, dtype, count_t):
+            n = count_t()
+            p = fn(h, C.byref(n))
+            if not n.value:
+                return np.zeros(0, dtype=dtype)
+            buf = (ct * (n.value * dtype.itemsize // C.sizeof(ct))).from_address(p)
+            return np.frombuffer(bytes(buf), dtype=dtype).copy()
+        reads = arr(lib.esg_mapping_reads, C.c_uint8, MAPPING_DTYPE, C.c_uint32)
+        hits = arr(lib.esg_mapping_hits, C.c_uint8, HIT_DTYPE, C.c_uint64)
+        ops = arr(lib.esg_mapping_ops, C.c_uint8, np.dtype("<u4"), C.c_uint64)
+        md = arr(lib.esg_mapping_md, C.c_uint8, np.dtype("u1"), C.c_uint64).tobytes()
+        return cls(reads, hits, ops, md)
+
+    def __len__(self):
+        return self.reads.size
+
+    def md(self, i: int) -> str:
+        h = self.hits[i]
+        o = int(h["md_offset"])
+        return self.md_bytes[o:o + int(h["md_len"])].decode()
+
+    def ops_of(self, i: int):
+        h = self.hits[i]
+        o = int(h["ops_offset"])
+        return self.ops[o:o + int(h["n_ops"])]
+
+    def mapping(self, k: int) -> dict:
+        """Read k as a plain dict (ReadMapping's fields, mapper.rs:60-70)."""
+        r = self.reads[k]
+        f = int(r["flags"])
+        hits = []
+        for i in range(int(r["first_hit"]), int(r["first_hit"]) + int(r["n_hits"])):
+            h = self.hits[i]
+            hits.append({"reference": int(h["reference"]), "reverse": bool(h["reverse"]),
+                         "score": int(h["score"]), "query_start": int(h["query_start"]),
+                         "query_end": int(h["query_end"]), "ref_start": int(h["ref_start"]),
+                         "ref_end": int(h["ref_end"]), "cigar": cigar_string(self.ops_of(i)),
+                         "md": self.md(i), "nm": int(h["nm"])})
+        return {"best_score": int(r["best_score"]) if f & MAPPING_HAS_BEST else None,
+                "n_tied": int(r["n_tied"]),
+                "suboptimal": int(r["suboptimal"]) if f & MAPPING_HAS_SUBOPTIMAL else None,
+                "hits": hits}
 
 
 def _align_call(lib, fn, args_head, jobs, bound=0):

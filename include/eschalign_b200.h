@@ -351,6 +351,64 @@ esg_status esg_align_reads(esg_scorer* scorer, const uint8_t* codes, const uint6
                            uint32_t n_jobs, esg_alignment* out, uint32_t* ops,
                            uint64_t ops_capacity, uint64_t* ops_needed);
 
+/* ---- mapping: Aligner::map_reads_scored (crates/eschalign/src/mapper.rs:
+ * 400-552) fed by this scorer's fused reduction instead of a ScoreMatrix.
+ * Every read is scored against the panel (its reverse complement too with
+ * both_strands), its tie set taken in candidate order -- the first
+ * min(n_tied, max_ties + 1) members, none below min_score -- and each taken
+ * member traced on the device (esg_align_batch); the read is unmapped when
+ * it takes none or its primary traces to no aligned base (a local score of
+ * zero).  Reads whose taken ties outrun the scorer's tie capacity are scored
+ * again with full rows for the rest of their list.  Each hit carries MD and
+ * NM as samtools calmd writes them (sam.rs:71-121): a base matches only when
+ * both are A/C/G/T (U as T) and equal; mismatched and deleted reference
+ * letters are written upper-cased from `ref_letters` (panel letters, reference
+ * r at ref_letters[ref_letter_off[r] .. + its length]), or, when that is
+ * NULL, as A/C/G/T/N from the panel's codes. */
+#define ESG_ALL_TIES 0xffffffffu /* MapOptions::max_ties = None: trace every tie */
+
+typedef struct esg_map_options {   /* MapOptions (mapper.rs:32-40)                   */
+    int32_t min_score;             /* a read whose best is below this is unmapped    */
+    uint32_t max_ties;             /* ties traced besides the primary; ESG_ALL_TIES  */
+    uint32_t both_strands;         /* also score and trace the reverse complement    */
+    uint32_t reserved;             /* 0                                              */
+} esg_map_options;
+
+#define ESG_MAPPING_HAS_BEST 1u       /* best_score is set (the read is not empty) */
+#define ESG_MAPPING_HAS_SUBOPTIMAL 2u /* suboptimal is set (not every candidate ties) */
+
+typedef struct esg_read_mapping {  /* ReadMapping (mapper.rs:60-70)                    */
+    int32_t best_score;
+    int32_t suboptimal;            /* SAM XS                                          */
+    uint32_t n_tied;
+    uint32_t flags;                /* ESG_MAPPING_*                                   */
+    uint32_t n_hits;               /* primary first, then the other taken ties; 0 = unmapped */
+    uint32_t reserved;
+    uint64_t first_hit;            /* this read's hits: hits[first_hit .. + n_hits)    */
+} esg_read_mapping;
+
+typedef struct esg_hit {           /* Hit (mapper.rs:43-56)                            */
+    uint32_t reference;            /* panel order                                     */
+    uint32_t reverse;              /* the read's reverse complement aligned           */
+    esg_alignment alignment;       /* coordinates on the read as aligned; ops in esg_mapping_ops */
+    uint32_t nm;
+    uint32_t md_len;
+    uint64_t md_offset;            /* MD at md[md_offset .. + md_len), not NUL-terminated */
+} esg_hit;
+
+typedef struct esg_mapping esg_mapping;
+
+esg_status esg_map_reads(esg_scorer* scorer, const uint8_t* codes, const uint64_t* off,
+                         const uint32_t* len, uint32_t n_reads, const esg_map_options* options,
+                         const uint8_t* ref_letters, const uint64_t* ref_letter_off,
+                         esg_mapping** out);
+/* The arrays of a mapping (owned by it; valid until esg_mapping_free). */
+const esg_read_mapping* esg_mapping_reads(const esg_mapping* mapping, uint32_t* n);
+const esg_hit* esg_mapping_hits(const esg_mapping* mapping, uint64_t* n);
+const uint32_t* esg_mapping_ops(const esg_mapping* mapping, uint64_t* n);
+const char* esg_mapping_md(const esg_mapping* mapping, uint64_t* n);
+void esg_mapping_free(esg_mapping* mapping);
+
 /* ---- serving: a request queue over resident scorers.  No counterpart in
  * the reference, which scores batches of one stream of reads and has no
  * serving mode.  Requests name a scorer slot (a resident panel under one

@@ -7,7 +7,10 @@ bench.py's CPU-baseline / reference legs, never by the product package.
 * :func:`select` -- tie set / XS, crates/eschalign/src/mapper.rs:444-472;
 * :class:`Profile` -- the AVX-512BW inter-sequence kernels,
   crates/eschalign/src/simd/avx512.rs:43-107 and :278-354, with the
-  reference's dispatch (mapper.rs:216-222).
+  reference's dispatch (mapper.rs:216-222);
+* :func:`md_nm` -- MD / NM as samtools calmd writes them,
+  crates/eschalign/src/sam.rs:55-121;
+* :func:`map_reads` -- Aligner::map_reads_scored, mapper.rs:400-552.
 """
 from __future__ import annotations
 
@@ -512,3 +515,112 @@ def scalar_map_pairs(mates, refs, scoring, local, both_strands, min_score=0, cap
                               *scoring, int(bool(both_strands)), int(bool(local)), min_score,
                               threads, cap, res.ctypes.data, _p(ties, C.c_uint32))
     return res, ties
+
+
+# ------------------------------------------------------------------ mapping
+def _norm(b: int) -> int:
+    """sam.rs:55-61: upper case, U as T."""
+    u = b - 32 if 97 <= b <= 122 else b
+    return 84 if u == 85 else u
+
+
+def calmd_match(read_base: int, ref_base: int) -> bool:
+    """sam.rs:63-69."""
+    q, r = _norm(read_base), _norm(ref_base)
+    return q == r and r in (65, 67, 71, 84)
+
+
+def md_nm(read: bytes, reference: bytes, query_start: int, ref_start: int, ops):
+    """sam.rs:76-121 on letters; ops are BAM CIGAR words (len << 4 | op)."""
+    md, nm, run = [], 0, 0
+    i, j = query_start, ref_start
+    for w in ops:
+        op, n = int(w) & 0xf, int(w) >> 4
+        if op == 0:
+            for _ in range(n):
+                if calmd_match(read[i], reference[j]):
+                    run += 1
+                else:
+                    md.append(str(run))
+                    md.append(chr(reference[j]).upper())
+                    run = 0
+                    nm += 1
+                i += 1
+                j += 1
+        elif op == 1:
+            i += n
+            nm += n
+        else:
+            md.append(str(run))
+            md.append("^")
+            md.extend(chr(reference[j + k]).upper() for k in range(n))
+            run = 0
+            j += n
+            nm += n
+    md.append(str(run))
+    return "".join(md), nm
+
+
+def revcomp_letters(seq: bytes) -> bytes:
+    """alphabet.rs:66-80: upper case, U to A, other letters N."""
+    comp = {65: 84, 67: 71, 71: 67, 84: 65}
+    return bytes(comp.get(_norm(b), 78) for b in reversed(seq))
+
+
+def map_reads(reads, refs, scoring, local, min_score=0, max_ties=None, both_strands=False,
+              threads=0):
+    """Aligner::map_reads_scored (mapper.rs:400-552) with the scalar scores:
+    `reads` and `refs` are letters (bytes/str).  Returns one dict per read:
+    best_score, n_tied, suboptimal, hits [reference, reverse, score,
+    coordinates, cigar, md, nm]."""
+    reads = [r.encode() if isinstance(r, str) else bytes(r) for r in reads]
+    refs = [r.encode() if isinstance(r, str) else bytes(r) for r in refs]
+    rcodes = [encode(r) for r in refs]
+    fwd = [encode(r) if len(r) else np.zeros(0, np.uint8) for r in reads]
+    nonempty = [k for k in range(len(reads)) if len(reads[k])]
+    qs = [fwd[k] for k in nonempty]
+    if both_strands:
+        qs += [revcomp(fwd[k]) for k in nonempty]
+    m = score_matrix(qs, rcodes, scoring, local, threads) if qs else np.zeros((0, len(refs)))
+    row_of = {k: i for i, k in enumerate(nonempty)}
+    out = []
+    for k, read in enumerate(reads):
+        if not len(read):
+            out.append({"best_score": None, "n_tied": 0, "suboptimal": None, "hits": []})
+            continue
+        i = row_of[k]
+        cands = []
+        for r in range(len(refs)):
+            cands.append((r, False, int(m[i, r])))
+            if both_strands:
+                cands.append((r, True, int(m[len(nonempty) + i, r])))
+        best = max(s for _, _, s in cands)
+        ties = [(r, rv) for r, rv, s in cands if s == best]
+        others = [s for _, _, s in cands if s != best]
+        sub = max(others) if others else None
+        n_tied = len(ties)
+        if best < min_score:
+            take = []
+        else:
+            kk = n_tied if max_ties is None else min(n_tied, max_ties + 1)
+            take = ties[:kk]
+        rec = {"best_score": best, "n_tied": n_tied, "suboptimal": sub, "hits": []}
+        traced = []
+        for r, rv in take:
+            q = revcomp(fwd[k]) if rv else fwd[k]
+            a, ops = align(q, rcodes[r], scoring, local)
+            traced.append((r, rv, a, ops))
+        if not take or not any((int(w) & 0xf) == 0 for w in traced[0][3]):
+            out.append(rec)
+            continue
+        letters_rev = revcomp_letters(read) if any(rv for _, rv in take) else b""
+        for r, rv, a, ops in traced:
+            md, nm = md_nm(letters_rev if rv else read, refs[r], int(a["query_start"]),
+                           int(a["ref_start"]), ops)
+            rec["hits"].append({"reference": r, "reverse": rv, "score": int(a["score"]),
+                                "query_start": int(a["query_start"]),
+                                "query_end": int(a["query_end"]),
+                                "ref_start": int(a["ref_start"]), "ref_end": int(a["ref_end"]),
+                                "cigar": cigar_string(ops), "md": md, "nm": nm})
+        out.append(rec)
+    return out

@@ -19,12 +19,17 @@ It reads, as data:
   (``gen_pair_fixture.py``, seed 20261004) the reference's
   ``tests/align_paired.rs`` aligns.
 
+* ``crates/eschalign/tests/fixtures/calmd_golden.json`` -- MD / NM that
+  samtools calmd wrote for 21 CIGARs over reference ``N``, IUPAC, lower case
+  and ``U`` (the reference's ``gen_calmd_golden.py``, checked by its
+  ``tests/sam_fields.rs``);
+
 and writes the subset this project tests against into ``tests/golden/``:
 ``align_golden_scores.json`` (query, reference, mode, scheme, score and the
 parasail end coordinates), the two panels as ``panel_trna*.json`` (name +
 letters, file order) and the paired fixture as ``pairs_fixture.json`` (panel
-and each pair's name and mate letters).  Nothing else from the reference is
-copied.
+and each pair's name and mate letters), and the calmd records as
+``calmd_golden.json``.  Nothing else from the reference is copied.
 """
 import json
 import os
@@ -95,8 +100,16 @@ def main(ref_root):
         json.dump({"source": "pairs/pairs_panel.fa, pairs_R1.fq, pairs_R2.fq",
                    "references": [{"name": n, "seq": s} for n, s in panel],
                    "pairs": pairs}, fh, indent=0)
+    with open(os.path.join(ref_root, "crates/eschalign/tests/fixtures/calmd_golden.json")) as fh:
+        cm = json.load(fh)
+    with open(os.path.join(here, "calmd_golden.json"), "w") as fh:
+        json.dump({"about": "MD/NM as samtools calmd wrote them (reference fixture "
+                            "calmd_golden.json, " + str(cm.get("samtools", "")) + ")",
+                   "reference": cm["reference"]["seq"],
+                   "records": [{k: r[k] for k in ("name", "pos", "cigar", "seq", "md", "nm")}
+                               for r in cm["records"]]}, fh, indent=0)
     print(f"{len(cases)} golden scores, {len(out['fixture_reads'])} fixture reads, "
-          f"{len(pairs)} fixture pairs")
+          f"{len(pairs)} fixture pairs, {len(cm['records'])} calmd records")
 
 
 if __name__ == "__main__":

@@ -1,0 +1,121 @@
+"""Mapping on the CUDA path (esg_map_reads) against the oracle's
+map_reads_scored restatement (crates/eschalign/src/mapper.rs:400-552 with
+sam.rs:55-121's MD / NM): per read the best score, tie count, XS and every
+traced hit -- reference, strand, score, coordinates, CIGAR, MD, NM -- equal
+field for field."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from eschalign_b200 import GpuScorer, Mode, Scoring, encode, synth
+from tests.helpers import GOLDEN, Rng, golden, mutate, random_seq
+
+pytestmark = pytest.mark.gpu
+
+SCHEME = (2, -1, -10, -1)
+# the panel and reads of mapper.rs's unit tests (556-620)
+UNIT_PANEL = [b"GGGGACGTACGTACGTTTTT", b"CCCCACGTACGTACGTAAAA", b"TTTTTTTTTTTTTTTTTTTT"]
+UNIT_READS = [b"ACGTACGTACGT", b"CCCCACGTACGTACGTAAAA", b"TTTTTTTTTTTT", b"",
+              b"GGGGACGTACGTACGTTTTT", b"NNNN"]
+
+
+def code_letters(codes):
+    return bytes(b"ACGTN"[min(int(c), 4)] for c in codes)
+
+
+def panel_letters(tag):
+    with open(os.path.join(GOLDEN, f"panel_{tag}.json")) as fh:
+        return [r["seq"].encode() for r in json.load(fh)["references"]]
+
+
+def run(oracle, panel, reads, scoring, mode, cap=8, give_letters=True, **opts):
+    codes = [encode(p) for p in panel]
+    with GpuScorer(codes, Scoring(*scoring), mode, tie_capacity=cap) as g:
+        got = g.map_reads([encode(r) if len(r) else np.zeros(0, np.uint8) for r in reads],
+                          ref_letters=panel if give_letters else None, **opts)
+    want = oracle.map_reads(reads, panel if give_letters else [code_letters(c) for c in codes],
+                            scoring, mode == Mode.LOCAL, **opts)
+    assert len(got) == len(want)
+    for k, w in enumerate(want):
+        assert got.mapping(k) == w, (k, reads[k], opts, cap)
+    return got, want
+
+
+@pytest.mark.parametrize("mode", [Mode.LOCAL, Mode.SEMIGLOBAL])
+def test_map_unit_panel(oracle, mode):
+    for both in (False, True):
+        for max_ties in (None, 0, 1):
+            for min_score in (0, 20, 1000):
+                run(oracle, UNIT_PANEL, UNIT_READS, SCHEME, mode, both_strands=both,
+                    max_ties=max_ties, min_score=min_score)
+
+
+def test_map_unit_answers(oracle):
+    """mapper.rs:569-590, 739-758 through the CUDA path."""
+    got, _ = run(oracle, UNIT_PANEL, [b"ACGTACGTACGT"], SCHEME, Mode.LOCAL)
+    m = got.mapping(0)
+    assert m["best_score"] == 24 and m["n_tied"] == 2
+    assert [h["reference"] for h in m["hits"]] == [0, 1]
+    read = oracle.revcomp_letters(b"CGTACGTAAAA")
+    got, _ = run(oracle, UNIT_PANEL, [read], SCHEME, Mode.LOCAL, both_strands=True)
+    h = got.mapping(0)["hits"][0]
+    assert h["reference"] == 1 and h["reverse"] and h["md"] == "11"
+
+
+@pytest.mark.parametrize("tag", ["trna", "trna_ambiguous"])
+@pytest.mark.parametrize("mode", [Mode.LOCAL, Mode.SEMIGLOBAL])
+def test_map_trna_panels(oracle, tag, mode):
+    """The 47-reference tRNA panels (near-identical isodecoders: large tie
+    sets; the ambiguous one carries N, an MD mismatch the scorer calls a
+    match), the golden fixture reads and reads cut from the panel."""
+    panel = panel_letters(tag)
+    rng = Rng(0x5EED_0901)
+    reads = [s.encode() for s in golden()["fixture_reads"]]
+    for _ in range(120):
+        r = panel[rng.below(len(panel))]
+        a = rng.below(len(r) // 4 + 1)
+        b = len(r) - rng.below(len(r) // 4 + 1)
+        reads.append(random_seq(rng, rng.below(8), 0.0) + mutate(rng, r[a:max(b, a)]))
+    reads.append(b"")
+    for cap, max_ties, min_score, both in ((8, None, 0, True), (1, None, 0, True),
+                                           (2, 3, 40, False), (32, 0, 0, True)):
+        for give in (True, False):
+            run(oracle, panel, reads, SCHEME, mode, cap=cap, give_letters=give,
+                max_ties=max_ties, min_score=min_score, both_strands=both)
+
+
+def test_map_letters_verbatim(oracle):
+    """Reference letters in lower case, U and IUPAC codes: MD writes them
+    upper-cased but otherwise verbatim, and counts each non-ACGT as a
+    mismatch (sam.rs:17-27)."""
+    panel = [b"ggggACGUACGTACGTRTTT", b"CCCCacgtacgtNCGTAAAA", b"TTTTTTTTYTTTTTTTTTTT"]
+    reads = [b"ACGTACGTACGT", b"GGGGACGTACGTACGTATTT", b"CCCCACGTACGTACGTAAAA", b"TTTTTTTTTT",
+             b"acgtNcgt"]
+    for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+        got, want = run(oracle, panel, reads, SCHEME, mode, both_strands=True)
+        assert any("R" in h["md"] or "N" in h["md"] or "U" in h["md"]
+                   for w in want for h in w["hits"])
+
+
+def test_map_c1_sample(oracle):
+    """2000 reads of the C1 workload on the 164-reference panel, local,
+    forward strand: a batch of the size the reference's feeder sends."""
+    refs = synth.panel_tiles()
+    data = synth.reads_c1(refs)
+    reads = [code_letters(data.read(k)) for k in range(2000)]
+    panel = [code_letters(r) for r in refs]
+    got, want = run(oracle, panel, reads, SCHEME, Mode.LOCAL)
+    assert sum(1 for w in want if w["hits"]) > 1500
+
+
+def test_map_bad_arguments(oracle):
+    codes = [encode(p) for p in UNIT_PANEL]
+    with GpuScorer(codes, Scoring(*SCHEME), Mode.LOCAL) as g:
+        with pytest.raises(ValueError):
+            g.map_reads([encode(b"ACGT")], ref_letters=UNIT_PANEL[:2])
+        with pytest.raises(ValueError):
+            g.map_reads([encode(b"ACGT")], ref_letters=[b"ACGT"] * 3)
+        m = g.map_reads([])
+        assert len(m) == 0

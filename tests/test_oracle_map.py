@@ -1,0 +1,87 @@
+"""The oracle's mapping stage pinned on the reference's own answers:
+MD / NM against the samtools calmd records of calmd_golden.json (checked in
+the reference by tests/sam_fields.rs) and sam.rs's unit case, and
+map_reads against the known answers of mapper.rs's unit tests (556-760)."""
+import json
+import os
+import re
+
+import pytest
+
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "calmd_golden.json")
+SCHEME = (2, -1, -10, -1)  # Scoring::default (scoring.rs:38-49)
+PANEL = [b"GGGGACGTACGTACGTTTTT", b"CCCCACGTACGTACGTAAAA", b"TTTTTTTTTTTTTTTTTTTT"]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    O.build()
+
+
+def parse_cigar(s):
+    """A SAM CIGAR into (leading clip, BAM words, trailing clip)."""
+    lead = tail = 0
+    words = []
+    for n, op in re.findall(r"(\d+)([MIDS])", s):
+        n = int(n)
+        if op == "S":
+            if words:
+                tail = n
+            else:
+                lead = n
+        else:
+            words.append((n << 4) | "MID".index(op))
+    return lead, words, tail
+
+
+def test_md_nm_matches_samtools_calmd():
+    g = json.load(open(GOLDEN))
+    ref = g["reference"].encode()
+    names = {r["name"] for r in g["records"]}
+    assert {"n_under_read_base", "n_under_read_n", "n_inside_deletion"} <= names
+    for r in g["records"]:
+        lead, words, _ = parse_cigar(r["cigar"])
+        md, nm = O.md_nm(r["seq"].encode(), ref, lead, r["pos"] - 1, words)
+        assert (md, nm) == (r["md"], r["nm"]), r["name"]
+
+
+def test_md_nm_reference_n_is_a_mismatch():
+    # sam.rs:134-140
+    assert O.md_nm(b"ACGTAACGTA", b"ACGTANCGTA", 0, 0, [10 << 4]) == ("5N4", 1)
+
+
+def test_ties_in_reference_order():
+    # mapper.rs:569-590
+    m = O.map_reads([b"ACGTACGTACGT"], PANEL, SCHEME, True)[0]
+    assert m["best_score"] == 24 and m["n_tied"] == 2
+    assert [h["reference"] for h in m["hits"]] == [0, 1]
+    assert m["suboptimal"] < 24
+    c = O.map_reads([b"ACGTACGTACGT"], PANEL, SCHEME, True, max_ties=0)[0]
+    assert c["n_tied"] == 2 and len(c["hits"]) == 1
+
+
+def test_min_score_unmaps():
+    # mapper.rs:725-737
+    m = O.map_reads([b"ACGTACGTACGT"], PANEL, SCHEME, True, min_score=1000)[0]
+    assert m["hits"] == [] and m["best_score"] == 24
+
+
+def test_reverse_strand_found_when_asked():
+    # mapper.rs:739-758
+    read = O.revcomp_letters(b"CGTACGTAAAA")
+    fwd = O.map_reads([read], PANEL, SCHEME, True)[0]
+    both = O.map_reads([read], PANEL, SCHEME, True, both_strands=True)[0]
+    assert both["best_score"] > fwd["best_score"]
+    h = both["hits"][0]
+    assert h["reference"] == 1 and h["reverse"] and h["md"] == "11"
+
+
+def test_empty_and_wildcard_reads():
+    # the reads of mapper.rs:593-617: an empty read has no best; NNNN scores
+    # (wildcards match) but its MD counts every base a mismatch
+    ms = O.map_reads([b"", b"NNNN"], PANEL, SCHEME, True, both_strands=True)
+    assert ms[0] == {"best_score": None, "n_tied": 0, "suboptimal": None, "hits": []}
+    assert ms[1]["best_score"] == 8 and ms[1]["hits"]
+    assert ms[1]["hits"][0]["nm"] == 4
