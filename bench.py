@@ -299,6 +299,34 @@ def traceback_stage(g, refs, reads, scoring, local, skip_cpu):
     return out
 
 
+def map_stage(g, refs, reads, scoring, local, skip_cpu):
+    """The whole mapping stage through esg_map_reads (mapper.rs:400-552):
+    scoring with the fused reduction, every tie traced (max_ties unset),
+    MD / NM; wall time of the call with host buffers.  Beside it the
+    oracle's map_reads (scalar scores, scalar traceback, MD / NM in Python)
+    on a small sample."""
+    g.map_reads(reads.slice(0, 1000).tuple(), both_strands=True)  # warm-up
+    t0 = time.perf_counter()
+    m = g.map_reads(reads.tuple(), both_strands=True)
+    dt = time.perf_counter() - t0
+    mapped = int((m.reads["n_hits"] > 0).sum())
+    out = {"reads": len(reads), "seconds": round(dt, 4), "reads_per_s": len(reads) / dt,
+           "mapped": mapped, "hits": int(m.hits.size),
+           "options": "both strands, min_score 0, every tie traced, MD/NM without letters"}
+    if not skip_cpu:
+        from oracle import oracle as O
+        n = min(len(reads), 2000)
+        letters = [bytes(b"ACGTN"[min(int(c), 4)] for c in r) for r in refs]
+        rl = [bytes(b"ACGTN"[min(int(c), 4)] for c in reads.read(k)) for k in range(n)]
+        t0 = time.perf_counter()
+        O.map_reads(rl, letters, scoring, local, both_strands=True)
+        dt_c = time.perf_counter() - t0
+        out["cpu"] = {"reads_per_s": n / dt_c, "kind": "port",
+                      "sample": f"first {n} reads: scalar scores on all cores, scalar "
+                                "traceback and MD / NM per hit on one"}
+    return out
+
+
 def reference_gpu_arms(refs, reads, scoring, local, device):
     """Comparison arms: the reference's own align_score_kernel (int) and
     align_score_kernel_h2 (half2), compiled ahead of time for sm_100a from its
@@ -591,6 +619,8 @@ def run_c2(a, ctx, rank):
         extras["plain_sample"] = f"first {len(sub)} reads, both strands"
         extras["traceback"] = traceback_stage(g, refs, sub, scoring, mode == "local",
                                               a.no_cpu_baseline or rank != 0 or world != 1)
+        extras["map"] = map_stage(g, refs, sub, scoring, mode == "local",
+                                  a.no_cpu_baseline or rank != 0 or world != 1)
         arms = reference_gpu_arms(refs, sub, scoring, mode == "local", local_rank)
         if arms:
             arms["batched_over_ref_half2"] = value / arms["half2_gcups"]
