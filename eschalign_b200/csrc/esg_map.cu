@@ -14,6 +14,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 extern "C" void esg_internal_set_error(esg_status st, const char* msg);
@@ -194,43 +195,84 @@ esg_status esg_map_reads(esg_scorer* sc, const uint8_t* codes, const uint64_t* o
                                      &ops)) != ESG_OK)
     return st;
 
-  // --- the mappings (mapper.rs:497-552)
+  // --- the mappings (mapper.rs:497-552), reads split over host threads,
+  // each part's hits / words / MD concatenated in read order
   std::unique_ptr<esg_mapping> m(new esg_mapping);
   m->reads.resize(n_reads);
-  std::string md;
-  for (uint32_t k = 0; k < n_reads; ++k) {
-    esg_read_mapping& rm = m->reads[k];
-    rm = esg_read_mapping{};
-    rm.first_hit = m->hits.size();
-    if (res[k].flags & ESG_RESULT_EMPTY) continue;
-    rm.best_score = res[k].best;
-    rm.n_tied = res[k].n_tied;
-    rm.flags = ESG_MAPPING_HAS_BEST;
-    if (res[k].suboptimal != ESG_NO_SCORE) {
-      rm.suboptimal = res[k].suboptimal;
-      rm.flags |= ESG_MAPPING_HAS_SUBOPTIMAL;
+  struct Part {
+    std::vector<esg_hit> hits;
+    std::vector<uint32_t> ops;
+    std::vector<char> md;
+  };
+  auto assemble = [&](uint32_t k0, uint32_t k1, Part& p) {
+    std::string md;
+    for (uint32_t k = k0; k < k1; ++k) {
+      esg_read_mapping& rm = m->reads[k];
+      rm = esg_read_mapping{};
+      rm.first_hit = p.hits.size();
+      if (res[k].flags & ESG_RESULT_EMPTY) continue;
+      rm.best_score = res[k].best;
+      rm.n_tied = res[k].n_tied;
+      rm.flags = ESG_MAPPING_HAS_BEST;
+      if (res[k].suboptimal != ESG_NO_SCORE) {
+        rm.suboptimal = res[k].suboptimal;
+        rm.flags |= ESG_MAPPING_HAS_SUBOPTIMAL;
+      }
+      const uint64_t j0 = first_job[k], j1 = first_job[k + 1];
+      if (j0 == j1 || !has_match(al[j0], ops.data() + al[j0].ops_offset)) continue;
+      const uint8_t* q = codes + off[k];
+      for (uint64_t jb = j0; jb < j1; ++jb) {
+        const esg_align_job& J = jobs[jb];
+        esg_alignment a = al[jb];
+        const uint32_t* w = ops.data() + a.ops_offset;
+        esg_hit h{};
+        h.reference = J.ref;
+        h.reverse = J.reverse;
+        md_nm(q, len[k], J.reverse != 0, P.h_codes + P.h_off[J.ref],
+              ref_letters ? ref_letters + ref_letter_off[J.ref] : nullptr, a, w, md, h.nm);
+        h.md_offset = p.md.size();
+        h.md_len = (uint32_t)md.size();
+        p.md.insert(p.md.end(), md.begin(), md.end());
+        a.ops_offset = p.ops.size();
+        p.ops.insert(p.ops.end(), w, w + a.n_ops);
+        h.alignment = a;
+        p.hits.push_back(h);
+      }
+      rm.n_hits = (uint32_t)(j1 - j0);
     }
-    const uint64_t j0 = first_job[k], j1 = first_job[k + 1];
-    if (j0 == j1 || !has_match(al[j0], ops.data() + al[j0].ops_offset)) continue;
-    const uint8_t* q = codes + off[k];
-    for (uint64_t jb = j0; jb < j1; ++jb) {
-      const esg_align_job& J = jobs[jb];
-      esg_alignment a = al[jb];
-      const uint32_t* w = ops.data() + a.ops_offset;
-      esg_hit h{};
-      h.reference = J.ref;
-      h.reverse = J.reverse;
-      md_nm(q, len[k], J.reverse != 0, P.h_codes + P.h_off[J.ref],
-            ref_letters ? ref_letters + ref_letter_off[J.ref] : nullptr, a, w, md, h.nm);
-      h.md_offset = m->md.size();
-      h.md_len = (uint32_t)md.size();
-      m->md.insert(m->md.end(), md.begin(), md.end());
-      a.ops_offset = m->ops.size();
-      m->ops.insert(m->ops.end(), w, w + a.n_ops);
-      h.alignment = a;
+  };
+  const uint32_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const uint32_t n_parts = std::max(1u, std::min(hw, n_reads / 4096));
+  std::vector<Part> parts(n_parts);
+  std::vector<uint32_t> cut(n_parts + 1);
+  for (uint32_t t = 0; t <= n_parts; ++t) cut[t] = (uint32_t)((uint64_t)n_reads * t / n_parts);
+  if (n_parts == 1) {
+    assemble(0, n_reads, parts[0]);
+  } else {
+    std::vector<std::thread> th;
+    for (uint32_t t = 0; t < n_parts; ++t)
+      th.emplace_back(assemble, cut[t], cut[t + 1], std::ref(parts[t]));
+    for (auto& x : th) x.join();
+  }
+  size_t nh = 0, no = 0, nm = 0;
+  for (const Part& p : parts) {
+    nh += p.hits.size();
+    no += p.ops.size();
+    nm += p.md.size();
+  }
+  m->hits.reserve(nh);
+  m->ops.reserve(no);
+  m->md.reserve(nm);
+  for (uint32_t t = 0; t < n_parts; ++t) {
+    const uint64_t hb = m->hits.size(), ob = m->ops.size(), mb = m->md.size();
+    for (uint32_t k = cut[t]; k < cut[t + 1]; ++k) m->reads[k].first_hit += hb;
+    for (esg_hit h : parts[t].hits) {
+      h.alignment.ops_offset += ob;
+      h.md_offset += mb;
       m->hits.push_back(h);
     }
-    rm.n_hits = (uint32_t)(j1 - j0);
+    m->ops.insert(m->ops.end(), parts[t].ops.begin(), parts[t].ops.end());
+    m->md.insert(m->md.end(), parts[t].md.begin(), parts[t].md.end());
   }
   *out = m.release();
   esg_internal_set_error(ESG_OK, "");

@@ -119,3 +119,17 @@ def test_map_bad_arguments(oracle):
             g.map_reads([encode(b"ACGT")], ref_letters=[b"ACGT"] * 3)
         m = g.map_reads([])
         assert len(m) == 0
+
+
+def test_map_large_batch_equals_small_ones(oracle):
+    """All 10 000 C1 reads in one call (the hits assembled on several host
+    threads) equal the same reads mapped 2000 at a time, both strands."""
+    refs = synth.panel_tiles()
+    data = synth.reads_c1(refs)
+    with GpuScorer(refs, Scoring(*SCHEME), Mode.LOCAL) as g:
+        whole = g.map_reads(data.tuple(), both_strands=True)
+        assert len(whole) == len(data)
+        for k0 in range(0, len(data), 2000):
+            part = g.map_reads(data.slice(k0, k0 + 2000).tuple(), both_strands=True)
+            for k in range(len(part)):
+                assert whole.mapping(k0 + k) == part.mapping(k), k0 + k
