@@ -129,6 +129,11 @@ class EsgMapOptions(C.Structure):
                 ("both_strands", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class EsgPairMapOptions(C.Structure):
+    _fields_ = [("min_score", C.c_int32), ("max_ties", C.c_uint32),
+                ("max_insert", C.c_uint32), ("both_strands", C.c_uint32)]
+
+
 class EsgServerOptions(C.Structure):
     _fields_ = [("max_batch_reads", C.c_uint32), ("max_inflight", C.c_uint32),
                 ("memory_budget", C.c_uint64), ("memory_headroom", C.c_uint64),
@@ -196,6 +201,11 @@ SIGNATURES = {
                                     C.c_uint32, C.c_void_p, _u32p, C.c_uint64, _u64p]),
     "esg_map_reads": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32,
                                   C.POINTER(EsgMapOptions), _u8p, _u64p, C.POINTER(C.c_void_p)]),
+    "esg_map_pairs": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32,
+                                  C.POINTER(EsgPairMapOptions), _u8p, _u64p,
+                                  C.POINTER(C.c_void_p)]),
+    "esg_mapping_pairs": (C.c_void_p, [C.c_void_p, _u32p]),
+    "esg_mapping_pair_hits": (C.c_void_p, [C.c_void_p, _u64p]),
     "esg_mapping_reads": (C.c_void_p, [C.c_void_p, _u32p]),
     "esg_mapping_hits": (C.c_void_p, [C.c_void_p, _u64p]),
     "esg_mapping_ops": (C.c_void_p, [C.c_void_p, _u64p]),

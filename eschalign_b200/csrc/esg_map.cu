@@ -15,6 +15,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 extern "C" void esg_internal_set_error(esg_status st, const char* msg);
@@ -24,6 +25,8 @@ struct esg_mapping {
   std::vector<esg_hit> hits;
   std::vector<uint32_t> ops;
   std::vector<char> md;
+  std::vector<esg_pair_mapping> pairs;  // esg_map_pairs only
+  std::vector<esg_pair_hit> pair_hits;
 };
 
 namespace {
@@ -107,14 +110,10 @@ bool has_match(const esg_alignment& a, const uint32_t* ops) {
 
 }  // namespace
 
-extern "C" {
-
-esg_status esg_map_reads(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
-                         const uint32_t* len, uint32_t n_reads, const esg_map_options* o,
-                         const uint8_t* ref_letters, const uint64_t* ref_letter_off,
-                         esg_mapping** out) {
-  if (!sc || !o || !out) return merr(ESG_ERR_BAD_ARGUMENT, "NULL scorer, options or out");
-  *out = nullptr;
+static esg_status map_reads_impl(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                          const uint32_t* len, uint32_t n_reads, const esg_map_options* o,
+                          const uint8_t* ref_letters, const uint64_t* ref_letter_off,
+                          std::unique_ptr<esg_mapping>& result) {
   if (n_reads && (!off || !len)) return merr(ESG_ERR_BAD_ARGUMENT, "off/len must not be NULL");
   if (o->both_strands > 1 || o->reserved)
     return merr(ESG_ERR_BAD_ARGUMENT, "both_strands must be 0 or 1, reserved 0");
@@ -274,9 +273,392 @@ esg_status esg_map_reads(esg_scorer* sc, const uint8_t* codes, const uint64_t* o
     m->ops.insert(m->ops.end(), parts[t].ops.begin(), parts[t].ops.end());
     m->md.insert(m->md.end(), parts[t].md.begin(), parts[t].md.end());
   }
+  result = std::move(m);
+  return ESG_OK;
+}
+
+namespace {
+
+// Aligner::pair_ok (pair.rs:392-410): both mates align a base, the mate
+// read as sequenced on the template strand starts before the other ends,
+// the insert (leftmost to rightmost aligned base) within max_insert.
+bool pair_ok(const esg_alignment& a0, const uint32_t* w0, const esg_alignment& a1,
+             const uint32_t* w1, bool template_reverse, uint32_t max_insert) {
+  if (!has_match(a0, w0) || !has_match(a1, w1)) return false;
+  const esg_alignment& fwd = template_reverse ? a1 : a0;
+  const esg_alignment& rev = template_reverse ? a0 : a1;
+  if (fwd.ref_start >= rev.ref_end) return false;
+  const uint32_t lo = std::min(a0.ref_start, a1.ref_start);
+  const uint32_t hi = std::max(a0.ref_end, a1.ref_end);
+  return hi - lo <= max_insert;
+}
+
+// PairState::mate_reverse (pair.rs:135-137)
+inline uint32_t mate_reverse(uint32_t m, uint32_t t) { return t ^ (m == 1 ? 1u : 0u); }
+
+struct PairCand {
+  int32_t sum;
+  uint32_t ref, t;
+  int32_t a, b;
+};
+
+}  // namespace
+
+// Aligner::map_pairs_scored (pair.rs:157-390) over the device ranking.
+// Phase 1 is the device's (k6_pairs): each pair's first tier -- its sum,
+// size, first members and the per-mate XS outside it.  Phase 2 traces the
+// first tier of every pair at once; a pair whose first tier holds members
+// that fail pair_ok keeps the ones that pass and adds the failed members'
+// mate scores to its XS (the device XS excludes the whole tier).  Pairs
+// whose first tier all fails, or is longer than the tie capacity, are
+// scored again with full rows and walked tier by tier on the host as
+// pair.rs:246-292 does, every open pair's next tier traced together.
+// Phase 3 builds the Proper mappings; the rest map each mate on its own,
+// both strands (pair.rs:362-387).
+static esg_status map_pairs_impl(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                                 const uint32_t* len, uint32_t n_pairs,
+                                 const esg_pair_map_options* o, const uint8_t* ref_letters,
+                                 const uint64_t* ref_letter_off,
+                                 std::unique_ptr<esg_mapping>& result) {
+  esg_internal_panel P{};
+  esg_internal_panel_of(sc, &P);
+  const uint32_t cap = esg_internal_tie_capacity(sc), nr = P.n_refs;
+  const uint32_t pflags = o->both_strands ? ESG_BOTH_STRANDS : 0u;
+  const uint32_t n_mates = 2 * n_pairs;
+
+  BatchGuard g;
+  esg_status st = esg_prepare_pairs(sc, codes, off, len, n_pairs, nullptr, o->min_score, pflags,
+                                    &g.b);
+  if (st != ESG_OK) return st;
+  if ((st = esg_submit(sc, g.b)) != ESG_OK) return st;
+  std::vector<esg_pair_result> pr(std::max<uint32_t>(n_pairs, 1));
+  std::vector<uint32_t> pties(std::max<size_t>((size_t)n_pairs * cap, 1));
+  if ((st = esg_finish_pairs(sc, g.b, pr.data(), pties.data(), nullptr, nullptr, nullptr,
+                             nullptr)) != ESG_OK)
+    return st;
+
+  // per pair: the found set (candidates with their two traced jobs)
+  struct Found {
+    PairCand c;
+    esg_alignment al[2];
+    const uint32_t* w[2];
+  };
+  std::vector<std::vector<Found>> found(n_pairs);
+  std::vector<int32_t> xs(2 * (size_t)n_pairs, ESG_NO_SCORE);
+  std::vector<uint8_t> kind(n_pairs, 0);  // 0 separate, 1 proper
+  std::vector<uint32_t> deep;             // pairs for the rows path
+  std::vector<uint8_t> deep_from0;        // ... starting at the first tier
+  std::vector<uint32_t> ops1, ops2;       // CIGAR words: first-tier round, deep rounds' found
+
+  // --- phase 2a: every pair's first tier from the device ranking
+  {
+    std::vector<esg_align_job> jobs;
+    std::vector<uint32_t> tp;  // pair of each candidate
+    for (uint32_t p = 0; p < n_pairs; ++p) {
+      if (pr[p].flags & ESG_RESULT_EMPTY) continue;
+      if (pr[p].n_tied > cap) {
+        deep.push_back(p);
+        deep_from0.push_back(1);
+        continue;
+      }
+      for (uint32_t i = 0; i < pr[p].n_tied; ++i) {
+        const uint32_t c = pties[(size_t)p * cap + i];
+        for (uint32_t m = 0; m < 2; ++m)
+          jobs.push_back(esg_align_job{2 * p + m, c >> 1, mate_reverse(m, c & 1u)});
+        tp.push_back(p);
+      }
+    }
+    std::vector<esg_alignment> al(jobs.size());
+    if (!jobs.empty() &&
+        (st = esg_internal_align_batch(sc, g.b, jobs.data(), (uint32_t)jobs.size(), al.data(),
+                                       &ops1)) != ESG_OK)
+      return st;
+    size_t k = 0;
+    while (k < tp.size()) {
+      const uint32_t p = tp[k];
+      int32_t x0 = pr[p].xs[0], x1 = pr[p].xs[1];
+      for (; k < tp.size() && tp[k] == p; ++k) {
+        const esg_alignment &a0 = al[2 * k], &a1 = al[2 * k + 1];
+        const uint32_t* w0 = ops1.data() + a0.ops_offset;
+        const uint32_t* w1 = ops1.data() + a1.ops_offset;
+        const uint32_t t = jobs[2 * k].reverse;  // mate 1 follows the template
+        if (pair_ok(a0, w0, a1, w1, t != 0, o->max_insert)) {
+          found[p].push_back(Found{PairCand{a0.score + a1.score, jobs[2 * k].ref, t, a0.score,
+                                            a1.score},
+                                   {a0, a1},
+                                   {w0, w1}});
+        } else {
+          x0 = std::max(x0, a0.score);
+          x1 = std::max(x1, a1.score);
+        }
+      }
+      if (found[p].empty()) {
+        deep.push_back(p);
+        deep_from0.push_back(0);
+      } else {
+        kind[p] = 1;
+        xs[2 * (size_t)p] = x0;
+        xs[2 * (size_t)p + 1] = x1;
+      }
+    }
+  }
+
+  // --- phase 2b: full rows, tier by tier on the host
+  if (!deep.empty()) {
+    std::vector<uint32_t> order(deep.size());
+    for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return deep[a] < deep[b]; });
+    std::vector<uint32_t> dp(deep.size());
+    std::vector<uint8_t> d0(deep.size());
+    for (uint32_t i = 0; i < order.size(); ++i) {
+      dp[i] = deep[order[i]];
+      d0[i] = deep_from0[order[i]];
+    }
+    const uint32_t m = (uint32_t)dp.size();
+    std::vector<uint64_t> soff(2 * (size_t)m);
+    std::vector<uint32_t> slen(2 * (size_t)m);
+    for (uint32_t i = 0; i < m; ++i)
+      for (uint32_t q = 0; q < 2; ++q) {
+        soff[2 * i + q] = off[2 * dp[i] + q];
+        slen[2 * i + q] = len[2 * dp[i] + q];
+      }
+    BatchGuard g2;
+    if ((st = esg_prepare_pairs(sc, codes, soff.data(), slen.data(), m, nullptr, o->min_score,
+                                pflags | ESG_FULL_ROWS, &g2.b)) != ESG_OK ||
+        (st = esg_submit(sc, g2.b)) != ESG_OK)
+      return st;
+    std::vector<int32_t> rows((size_t)4 * m * nr);
+    std::vector<esg_pair_result> pr2(m);
+    if ((st = esg_finish_pairs(sc, g2.b, pr2.data(), nullptr, nullptr, nullptr, nullptr,
+                               rows.data())) != ESG_OK)
+      return st;
+    auto row = [&](uint32_t mate, uint32_t rev) {
+      return rows.data() + ((size_t)(rev ? 2 * m : 0) + mate) * nr;
+    };
+    // phase 1 on the host (pair.rs:175-231)
+    std::vector<std::vector<PairCand>> cands(m);
+    std::vector<std::vector<std::pair<size_t, size_t>>> tiers(m);
+    std::vector<size_t> next(m, 0);
+    const uint32_t n_strands = o->both_strands ? 2 : 1;
+    for (uint32_t i = 0; i < m; ++i) {
+      auto& cs = cands[i];
+      for (uint32_t t = 0; t < n_strands; ++t) {
+        const int32_t* r0 = row(2 * i, mate_reverse(0, t));
+        const int32_t* r1 = row(2 * i + 1, mate_reverse(1, t));
+        for (uint32_t r = 0; r < nr; ++r)
+          if (r0[r] >= o->min_score && r1[r] >= o->min_score)
+            cs.push_back(PairCand{r0[r] + r1[r], r, t, r0[r], r1[r]});
+      }
+      std::stable_sort(cs.begin(), cs.end(), [](const PairCand& a, const PairCand& b) {
+        if (a.sum != b.sum) return a.sum > b.sum;
+        if (a.ref != b.ref) return a.ref < b.ref;
+        return a.t < b.t;
+      });
+      size_t start = 0;
+      for (size_t k = 1; k <= cs.size(); ++k)
+        if (k == cs.size() || cs[k].sum != cs[start].sum) {
+          tiers[i].push_back({start, k});
+          start = k;
+        }
+      next[i] = d0[i] ? 0 : 1;  // the first tier already failed on the device path
+    }
+    // phase 2 (pair.rs:246-292): trace every open pair's next tier together
+    std::vector<std::vector<esg_alignment>> kept_al;
+    std::vector<std::vector<uint32_t>> kept_ops;
+    for (;;) {
+      std::vector<esg_align_job> jobs;
+      std::vector<std::pair<uint32_t, size_t>> who;  // (deep pair, candidate)
+      for (uint32_t i = 0; i < m; ++i) {
+        if (!found[dp[i]].empty() || next[i] >= tiers[i].size()) continue;
+        const auto [a, b] = tiers[i][next[i]];
+        for (size_t k = a; k < b; ++k) {
+          for (uint32_t q = 0; q < 2; ++q)
+            jobs.push_back(esg_align_job{2 * i + q, cands[i][k].ref,
+                                         mate_reverse(q, cands[i][k].t)});
+          who.push_back({i, k});
+        }
+      }
+      if (jobs.empty()) break;
+      kept_al.emplace_back(jobs.size());
+      kept_ops.emplace_back();
+      if ((st = esg_internal_align_batch(sc, g2.b, jobs.data(), (uint32_t)jobs.size(),
+                                         kept_al.back().data(), &kept_ops.back())) != ESG_OK)
+        return st;
+      const auto& al = kept_al.back();
+      const auto& w = kept_ops.back();
+      for (size_t k = 0; k < who.size(); ++k) {
+        const auto [i, ci] = who[k];
+        const PairCand& c = cands[i][ci];
+        const uint32_t* w0 = w.data() + al[2 * k].ops_offset;
+        const uint32_t* w1 = w.data() + al[2 * k + 1].ops_offset;
+        if (pair_ok(al[2 * k], w0, al[2 * k + 1], w1, c.t != 0, o->max_insert))
+          found[dp[i]].push_back(Found{c, {al[2 * k], al[2 * k + 1]}, {w0, w1}});
+      }
+      for (uint32_t i = 0; i < m; ++i)
+        if (found[dp[i]].empty() && next[i] < tiers[i].size()) ++next[i];
+    }
+    // XS outside the found set, from the rows (pair.rs:297-314)
+    std::vector<uint8_t> in_set(2 * (size_t)nr);
+    for (uint32_t i = 0; i < m; ++i) {
+      const uint32_t p = dp[i];
+      if (found[p].empty()) continue;
+      kind[p] = 1;
+      std::fill(in_set.begin(), in_set.end(), 0);
+      for (const Found& f : found[p]) in_set[2 * (size_t)f.c.ref + f.c.t] = 1;
+      for (uint32_t t = 0; t < n_strands; ++t)
+        for (uint32_t r = 0; r < nr; ++r) {
+          if (in_set[2 * (size_t)r + t]) continue;
+          for (uint32_t q = 0; q < 2; ++q)
+            xs[2 * (size_t)p + q] = std::max(xs[2 * (size_t)p + q], row(2 * i + q, mate_reverse(q, t))[r]);
+        }
+    }
+    // the found sets' words live in this block's trace rounds: copy them
+    // out for phase 3
+    for (uint32_t i = 0; i < m; ++i)
+      for (Found& f : found[dp[i]])
+        for (uint32_t q = 0; q < 2; ++q) {
+          const size_t at = ops2.size();
+          ops2.insert(ops2.end(), f.w[q], f.w[q] + f.al[q].n_ops);
+          f.al[q].ops_offset = at;
+          f.w[q] = nullptr;  // resolved against ops2 below
+        }
+  }
+
+  // --- phase 3: Proper mappings (pair.rs:294-360)
+  std::unique_ptr<esg_mapping> out(new esg_mapping);
+  out->pairs.resize(n_pairs);
+  out->reads.resize(n_mates);
+  std::string md;
+  for (uint32_t p = 0; p < n_pairs; ++p) {
+    esg_pair_mapping& pm = out->pairs[p];
+    pm = esg_pair_mapping{};
+    pm.first_hit = out->pair_hits.size();
+    pm.suboptimal[0] = pm.suboptimal[1] = ESG_NO_SCORE;
+    if (!kind[p]) continue;
+    const auto& fs = found[p];
+    pm.flags = ESG_PAIR_PROPER;
+    pm.score = fs[0].c.sum;
+    pm.n_tied = (uint32_t)fs.size();
+    for (uint32_t q = 0; q < 2; ++q)
+      if (xs[2 * (size_t)p + q] != ESG_NO_SCORE) {
+        pm.suboptimal[q] = xs[2 * (size_t)p + q];
+        pm.flags |= q ? ESG_PAIR_HAS_XS2 : ESG_PAIR_HAS_XS1;
+      }
+    const uint32_t keep = (o->max_ties == ESG_ALL_TIES || o->max_ties >= pm.n_tied)
+                              ? pm.n_tied
+                              : o->max_ties + 1;
+    for (uint32_t k = 0; k < keep; ++k) {
+      const Found& f = fs[k];
+      esg_pair_hit ph{};
+      ph.reference = f.c.ref;
+      ph.reverse = f.c.t;
+      for (uint32_t q = 0; q < 2; ++q) {
+        const uint32_t* w = f.w[q] ? f.w[q] : ops2.data() + f.al[q].ops_offset;
+        esg_alignment a = f.al[q];
+        esg_hit& h = ph.mates[q];
+        h.reference = f.c.ref;
+        h.reverse = mate_reverse(q, f.c.t);
+        md_nm(codes + off[2 * p + q], len[2 * p + q], h.reverse != 0, P.h_codes + P.h_off[f.c.ref],
+              ref_letters ? ref_letters + ref_letter_off[f.c.ref] : nullptr, a, w, md, h.nm);
+        h.md_offset = out->md.size();
+        h.md_len = (uint32_t)md.size();
+        out->md.insert(out->md.end(), md.begin(), md.end());
+        a.ops_offset = out->ops.size();
+        out->ops.insert(out->ops.end(), w, w + a.n_ops);
+        h.alignment = a;
+      }
+      ph.insert = std::max(ph.mates[0].alignment.ref_end, ph.mates[1].alignment.ref_end) -
+                  std::min(ph.mates[0].alignment.ref_start, ph.mates[1].alignment.ref_start);
+      out->pair_hits.push_back(ph);
+    }
+    pm.n_hits = keep;
+  }
+
+  // --- the rest: each mate on its own, both strands (pair.rs:362-387)
+  std::vector<uint32_t> sep;
+  for (uint32_t p = 0; p < n_pairs; ++p)
+    if (!kind[p]) sep.push_back(p);
+  if (!sep.empty()) {
+    std::vector<uint64_t> soff(2 * sep.size());
+    std::vector<uint32_t> slen(2 * sep.size());
+    for (size_t i = 0; i < sep.size(); ++i)
+      for (uint32_t q = 0; q < 2; ++q) {
+        soff[2 * i + q] = off[2 * sep[i] + q];
+        slen[2 * i + q] = len[2 * sep[i] + q];
+      }
+    esg_map_options mo{o->min_score, o->max_ties, 1u, 0u};
+    std::unique_ptr<esg_mapping> each;
+    if ((st = map_reads_impl(sc, codes, soff.data(), slen.data(), (uint32_t)(2 * sep.size()), &mo,
+                             ref_letters, ref_letter_off, each)) != ESG_OK)
+      return st;
+    const uint64_t hb = out->hits.size(), ob = out->ops.size(), mb = out->md.size();
+    for (esg_hit h : each->hits) {
+      h.alignment.ops_offset += ob;
+      h.md_offset += mb;
+      out->hits.push_back(h);
+    }
+    out->ops.insert(out->ops.end(), each->ops.begin(), each->ops.end());
+    out->md.insert(out->md.end(), each->md.begin(), each->md.end());
+    for (size_t i = 0; i < sep.size(); ++i)
+      for (uint32_t q = 0; q < 2; ++q) {
+        esg_read_mapping rm = each->reads[2 * i + q];
+        rm.first_hit += hb;
+        out->reads[2 * sep[i] + q] = rm;
+      }
+  }
+  for (uint32_t k = 0; k < n_mates; ++k)
+    if (kind[k / 2]) out->reads[k].first_hit = out->hits.size();
+  result = std::move(out);
+  return ESG_OK;
+}
+
+extern "C" {
+
+esg_status esg_map_reads(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                         const uint32_t* len, uint32_t n_reads, const esg_map_options* o,
+                         const uint8_t* ref_letters, const uint64_t* ref_letter_off,
+                         esg_mapping** out) {
+  if (!sc || !o || !out) return merr(ESG_ERR_BAD_ARGUMENT, "NULL scorer, options or out");
+  *out = nullptr;
+  std::unique_ptr<esg_mapping> m;
+  const esg_status st =
+      map_reads_impl(sc, codes, off, len, n_reads, o, ref_letters, ref_letter_off, m);
+  if (st != ESG_OK) return st;
   *out = m.release();
   esg_internal_set_error(ESG_OK, "");
   return ESG_OK;
+}
+
+esg_status esg_map_pairs(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                         const uint32_t* len, uint32_t n_pairs, const esg_pair_map_options* o,
+                         const uint8_t* ref_letters, const uint64_t* ref_letter_off,
+                         esg_mapping** out) {
+  if (!sc || !o || !out) return merr(ESG_ERR_BAD_ARGUMENT, "NULL scorer, options or out");
+  *out = nullptr;
+  if (n_pairs && (!off || !len)) return merr(ESG_ERR_BAD_ARGUMENT, "off/len must not be NULL");
+  if (o->both_strands > 1) return merr(ESG_ERR_BAD_ARGUMENT, "both_strands must be 0 or 1");
+  if (ref_letters && !ref_letter_off)
+    return merr(ESG_ERR_BAD_ARGUMENT, "ref_letters needs ref_letter_off");
+  uint64_t total = 0;
+  for (uint64_t k = 0; k < 2 * (uint64_t)n_pairs; ++k) total += len[k];
+  if (total && !codes) return merr(ESG_ERR_BAD_ARGUMENT, "codes must not be NULL");
+  std::unique_ptr<esg_mapping> m;
+  const esg_status st =
+      map_pairs_impl(sc, codes, off, len, n_pairs, o, ref_letters, ref_letter_off, m);
+  if (st != ESG_OK) return st;
+  *out = m.release();
+  esg_internal_set_error(ESG_OK, "");
+  return ESG_OK;
+}
+
+const esg_pair_mapping* esg_mapping_pairs(const esg_mapping* m, uint32_t* n) {
+  if (n) *n = m ? (uint32_t)m->pairs.size() : 0u;
+  return m ? m->pairs.data() : nullptr;
+}
+
+const esg_pair_hit* esg_mapping_pair_hits(const esg_mapping* m, uint64_t* n) {
+  if (n) *n = m ? m->pair_hits.size() : 0u;
+  return m ? m->pair_hits.data() : nullptr;
 }
 
 const esg_read_mapping* esg_mapping_reads(const esg_mapping* m, uint32_t* n) {

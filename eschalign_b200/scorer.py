@@ -503,24 +503,12 @@ class GpuScorer:
         `ref_letters`: the panel's letters (a list of str/bytes, panel order)
         for MD; without them MD spells the panel's codes as A/C/G/T/N."""
         codes, off, lens = self._inputs(reads)
+        lp, lo, keep = self._letters(ref_letters)
         opts = _native.EsgMapOptions(int(min_score),
                                      0xFFFFFFFF if max_ties is None else int(max_ties),
                                      int(bool(both_strands)), 0)
         if max_ties is not None and not 0 <= int(max_ties) < 0xFFFFFFFF:
             raise ValueError("max_ties must be in [0, 2^32 - 1)")
-        lp = lo = None
-        if ref_letters is not None:
-            if len(ref_letters) != len(self.panel):
-                raise ValueError("ref_letters: one entry per reference")
-            bl = [r.encode() if isinstance(r, str) else bytes(r) for r in ref_letters]
-            for k, b in enumerate(bl):
-                if len(b) != int(self._panel_arrays[2][k]):
-                    raise ValueError(f"ref_letters[{k}]: length differs from the reference")
-            letters = np.frombuffer(b"".join(bl) or b"\0", dtype=np.uint8)
-            loff = np.zeros(len(bl), dtype=np.uint64)
-            if len(bl) > 1:
-                loff[1:] = np.cumsum([len(b) for b in bl[:-1]], dtype=np.uint64)
-            lp, lo = _ptr(letters, C.c_uint8), _ptr(loff, C.c_uint64)
         h = C.c_void_p()
         _check(self._lib, self._lib.esg_map_reads(self._h, _ptr(codes, C.c_uint8),
                                                   _ptr(off, C.c_uint64), _ptr(lens, C.c_uint32),
@@ -529,6 +517,50 @@ class GpuScorer:
             return Mappings._copy(self._lib, h)
         finally:
             self._lib.esg_mapping_free(h)
+
+    def map_pairs(self, mates, min_score: int = 0, max_ties: int | None = None,
+                  max_insert: int = 500, both_strands: bool = False,
+                  ref_letters=None) -> "Mappings":
+        """Aligner::map_pairs_scored (pair.rs:157-390) over this scorer:
+        mates 2p and 2p + 1 are pair p (adapters already trimmed).  Per pair
+        Proper (score, tie count, per-mate XS, pair hits) or Separate (each
+        mate as map_reads maps it on both strands)."""
+        codes, off, lens = self._inputs(mates)
+        if lens.size % 2:
+            raise ValueError("mates come in pairs")
+        if max_ties is not None and not 0 <= int(max_ties) < 0xFFFFFFFF:
+            raise ValueError("max_ties must be in [0, 2^32 - 1)")
+        if not 0 <= int(max_insert) < 2**32:
+            raise ValueError("max_insert must fit 32 bits")
+        lp, lo, keep = self._letters(ref_letters)
+        opts = _native.EsgPairMapOptions(int(min_score),
+                                         0xFFFFFFFF if max_ties is None else int(max_ties),
+                                         int(max_insert), int(bool(both_strands)))
+        h = C.c_void_p()
+        _check(self._lib, self._lib.esg_map_pairs(self._h, _ptr(codes, C.c_uint8),
+                                                  _ptr(off, C.c_uint64), _ptr(lens, C.c_uint32),
+                                                  lens.size // 2, C.byref(opts), lp, lo,
+                                                  C.byref(h)))
+        try:
+            return Mappings._copy(self._lib, h, paired=True)
+        finally:
+            self._lib.esg_mapping_free(h)
+
+    def _letters(self, ref_letters):
+        """The panel's letters as (pointer, offsets pointer, arrays to keep)."""
+        if ref_letters is None:
+            return None, None, None
+        if len(ref_letters) != len(self.panel):
+            raise ValueError("ref_letters: one entry per reference")
+        bl = [r.encode() if isinstance(r, str) else bytes(r) for r in ref_letters]
+        for k, b in enumerate(bl):
+            if len(b) != int(self._panel_arrays[2][k]):
+                raise ValueError(f"ref_letters[{k}]: length differs from the reference")
+        letters = np.frombuffer(b"".join(bl) or b"\0", dtype=np.uint8)
+        loff = np.zeros(len(bl), dtype=np.uint64)
+        if len(bl) > 1:
+            loff[1:] = np.cumsum([len(b) for b in bl[:-1]], dtype=np.uint64)
+        return _ptr(letters, C.c_uint8), _ptr(loff, C.c_uint64), (letters, loff)
 
     # -- paired-end (pair.rs:157-234, fed as align.rs:2844-2872 feeds it)
     def prepare_pairs(self, mates, adapters=None, min_score: int = 0, both_strands: bool = True,
@@ -631,20 +663,29 @@ HIT_DTYPE = np.dtype([("reference", "<u4"), ("reverse", "<u4"), ("score", "<i4")
                       ("nm", "<u4"), ("md_len", "<u4"), ("md_offset", "<u8")])
 MAPPING_HAS_BEST = 1
 MAPPING_HAS_SUBOPTIMAL = 2
+PAIR_MAPPING_DTYPE = np.dtype([("flags", "<u4"), ("score", "<i4"), ("n_tied", "<u4"),
+                               ("n_hits", "<u4"), ("suboptimal", "<i4", (2,)),
+                               ("first_hit", "<u8")])
+PAIR_HIT_DTYPE = np.dtype([("reference", "<u4"), ("reverse", "<u4"), ("insert", "<u8"),
+                           ("mates", HIT_DTYPE, (2,))])
+PAIR_PROPER = 1
+PAIR_HAS_XS = (2, 4)
 
 
 class Mappings:
     """esg_map_reads' output: per read a MAPPING_DTYPE record, its hits
     (HIT_DTYPE) and their CIGAR words and MD strings."""
 
-    def __init__(self, reads, hits, ops, md: bytes):
+    def __init__(self, reads, hits, ops, md: bytes, pairs=None, pair_hits=None):
         self.reads = reads
         self.hits = hits
         self.ops = ops
         self.md_bytes = md
+        self.pairs = pairs
+        self.pair_hits = pair_hits
 
     @classmethod
-    def _copy(cls, lib, h):
+    def _copy(cls, lib, h, paired=False):
         def arr(fn, ct, dtype, count_t):
             n = count_t()
             p = fn(h, C.byref(n))
@@ -656,33 +697,59 @@ class Mappings:
         hits = arr(lib.esg_mapping_hits, C.c_uint8, HIT_DTYPE, C.c_uint64)
         ops = arr(lib.esg_mapping_ops, C.c_uint8, np.dtype("<u4"), C.c_uint64)
         md = arr(lib.esg_mapping_md, C.c_uint8, np.dtype("u1"), C.c_uint64).tobytes()
-        return cls(reads, hits, ops, md)
+        pairs = pair_hits = None
+        if paired:
+            pairs = arr(lib.esg_mapping_pairs, C.c_uint8, PAIR_MAPPING_DTYPE, C.c_uint32)
+            pair_hits = arr(lib.esg_mapping_pair_hits, C.c_uint8, PAIR_HIT_DTYPE, C.c_uint64)
+        return cls(reads, hits, ops, md, pairs, pair_hits)
 
     def __len__(self):
-        return self.reads.size
+        return (self.pairs if self.pairs is not None else self.reads).size
 
     def md(self, i: int) -> str:
-        h = self.hits[i]
+        return self._md_of(self.hits[i])
+
+    def ops_of(self, i: int):
+        return self._ops_of(self.hits[i])
+
+    def _md_of(self, h) -> str:
         o = int(h["md_offset"])
         return self.md_bytes[o:o + int(h["md_len"])].decode()
 
-    def ops_of(self, i: int):
-        h = self.hits[i]
+    def _ops_of(self, h):
         o = int(h["ops_offset"])
         return self.ops[o:o + int(h["n_ops"])]
+
+    def _hit(self, h) -> dict:
+        return {"reference": int(h["reference"]), "reverse": bool(h["reverse"]),
+                "score": int(h["score"]), "query_start": int(h["query_start"]),
+                "query_end": int(h["query_end"]), "ref_start": int(h["ref_start"]),
+                "ref_end": int(h["ref_end"]), "cigar": cigar_string(self._ops_of(h)),
+                "md": self._md_of(h), "nm": int(h["nm"])}
+
+    def pair_mapping(self, p: int) -> dict:
+        """Pair p as a plain dict (PairMapping, pair.rs:89-105)."""
+        r = self.pairs[p]
+        f = int(r["flags"])
+        if not f & PAIR_PROPER:
+            return {"proper": False, "mates": [self.mapping(2 * p), self.mapping(2 * p + 1)]}
+        hits = []
+        for i in range(int(r["first_hit"]), int(r["first_hit"]) + int(r["n_hits"])):
+            ph = self.pair_hits[i]
+            hits.append({"reference": int(ph["reference"]), "reverse": bool(ph["reverse"]),
+                         "insert": int(ph["insert"]),
+                         "mates": [self._hit(ph["mates"][0]), self._hit(ph["mates"][1])]})
+        return {"proper": True, "score": int(r["score"]), "n_tied": int(r["n_tied"]),
+                "suboptimal": [int(r["suboptimal"][m]) if f & PAIR_HAS_XS[m] else None
+                               for m in range(2)],
+                "hits": hits}
 
     def mapping(self, k: int) -> dict:
         """Read k as a plain dict (ReadMapping's fields, mapper.rs:60-70)."""
         r = self.reads[k]
         f = int(r["flags"])
-        hits = []
-        for i in range(int(r["first_hit"]), int(r["first_hit"]) + int(r["n_hits"])):
-            h = self.hits[i]
-            hits.append({"reference": int(h["reference"]), "reverse": bool(h["reverse"]),
-                         "score": int(h["score"]), "query_start": int(h["query_start"]),
-                         "query_end": int(h["query_end"]), "ref_start": int(h["ref_start"]),
-                         "ref_end": int(h["ref_end"]), "cigar": cigar_string(self.ops_of(i)),
-                         "md": self.md(i), "nm": int(h["nm"])})
+        hits = [self._hit(self.hits[i])
+                for i in range(int(r["first_hit"]), int(r["first_hit"]) + int(r["n_hits"]))]
         return {"best_score": int(r["best_score"]) if f & MAPPING_HAS_BEST else None,
                 "n_tied": int(r["n_tied"]),
                 "suboptimal": int(r["suboptimal"]) if f & MAPPING_HAS_SUBOPTIMAL else None,

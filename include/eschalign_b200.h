@@ -402,6 +402,53 @@ esg_status esg_map_reads(esg_scorer* scorer, const uint8_t* codes, const uint64_
                          const uint32_t* len, uint32_t n_reads, const esg_map_options* options,
                          const uint8_t* ref_letters, const uint64_t* ref_letter_off,
                          esg_mapping** out);
+/* ---- paired mapping: Aligner::map_pairs_scored (crates/eschalign/src/
+ * mapper/pair.rs:157-390) over the device ranking.  Mates 2p and 2p + 1 are
+ * pair p as given (trim adapters first, esg_pair_adapters, as the CLI does
+ * before map_pairs_scored).  Each pair's eligible candidates (reference,
+ * template strand) are taken tier by tier in descending summed score; the
+ * first tier with members whose traced mates satisfy the pair constraints
+ * (both aligned, no outie, insert <= max_insert; pair.rs:392-410) is the tie
+ * set, XS per mate is the best mate score outside it, and a pair with no
+ * such tier maps each mate on its own, both strands, as esg_map_reads
+ * does.  The first tier comes from the device ranking; deeper tiers, and a
+ * first tier longer than the tie capacity, from full rows. */
+typedef struct esg_pair_map_options { /* PairOptions (pair.rs:44-65)                  */
+    int32_t min_score;            /* both mates at least this                        */
+    uint32_t max_ties;            /* pair hits besides the primary; ESG_ALL_TIES     */
+    uint32_t max_insert;          /* longest insert, bases (the reference's default 500) */
+    uint32_t both_strands;        /* also the reverse template strand                */
+} esg_pair_map_options;
+
+#define ESG_PAIR_PROPER 1u  /* PairMapping::Proper; else Separate: the mates in esg_mapping_reads */
+#define ESG_PAIR_HAS_XS1 2u /* suboptimal[0] is set                                            */
+#define ESG_PAIR_HAS_XS2 4u /* suboptimal[1] is set                                            */
+
+typedef struct esg_pair_mapping { /* PairMapping (pair.rs:89-105)                       */
+    uint32_t flags;               /* ESG_PAIR_*                                          */
+    int32_t score;                /* Proper: the pair score (both mates summed)          */
+    uint32_t n_tied;              /* Proper: the tie set's size                          */
+    uint32_t n_hits;              /* Proper: primary first, then up to max_ties more     */
+    int32_t suboptimal[2];        /* Proper: per mate XS                                 */
+    uint64_t first_hit;           /* Proper: pair_hits[first_hit .. + n_hits)            */
+} esg_pair_mapping;
+
+typedef struct esg_pair_hit {     /* PairHit (pair.rs:68-81)                             */
+    uint32_t reference;           /* panel order                                         */
+    uint32_t reverse;             /* template on the reverse strand                      */
+    uint64_t insert;              /* leftmost aligned reference base to rightmost        */
+    esg_hit mates[2];             /* each mate's own strand; coordinates on it as aligned */
+} esg_pair_hit;
+
+esg_status esg_map_pairs(esg_scorer* scorer, const uint8_t* codes, const uint64_t* off,
+                         const uint32_t* len, uint32_t n_pairs,
+                         const esg_pair_map_options* options, const uint8_t* ref_letters,
+                         const uint64_t* ref_letter_off, esg_mapping** out);
+/* A paired mapping's pairs and pair hits; its esg_mapping_reads holds the
+ * two mates of each pair (2p, 2p + 1), filled for Separate pairs. */
+const esg_pair_mapping* esg_mapping_pairs(const esg_mapping* mapping, uint32_t* n);
+const esg_pair_hit* esg_mapping_pair_hits(const esg_mapping* mapping, uint64_t* n);
+
 /* The arrays of a mapping (owned by it; valid until esg_mapping_free). */
 const esg_read_mapping* esg_mapping_reads(const esg_mapping* mapping, uint32_t* n);
 const esg_hit* esg_mapping_hits(const esg_mapping* mapping, uint64_t* n);

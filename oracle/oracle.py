@@ -624,3 +624,111 @@ def map_reads(reads, refs, scoring, local, min_score=0, max_ties=None, both_stra
                                 "cigar": cigar_string(ops), "md": md, "nm": nm})
         out.append(rec)
     return out
+
+
+def _aligned_any(ops) -> bool:
+    """Alignment::is_empty's negation (scalar.rs:80-85)."""
+    return any((int(w) & 0xf) == 0 for w in ops)
+
+
+def pair_ok(al, ops, template_reverse: bool, max_insert: int) -> bool:
+    """Aligner::pair_ok (pair.rs:392-410): both mates aligned, no outie, the
+    insert within max_insert."""
+    if not _aligned_any(ops[0]) or not _aligned_any(ops[1]):
+        return False
+    fwd, rev = (al[1], al[0]) if template_reverse else (al[0], al[1])
+    if int(fwd["ref_start"]) >= int(rev["ref_end"]):
+        return False
+    lo = min(int(al[0]["ref_start"]), int(al[1]["ref_start"]))
+    hi = max(int(al[0]["ref_end"]), int(al[1]["ref_end"]))
+    return hi - lo <= max_insert
+
+
+def map_pairs(pairs, refs, scoring, local, min_score=0, max_ties=None, max_insert=500,
+              both_strands=False, threads=0):
+    """Aligner::map_pairs_scored (pair.rs:157-390) with the scalar scores:
+    `pairs` is a list of (mate 1, mate 2) letters, `refs` letters.  One dict
+    per pair: {"proper": True, score, n_tied, suboptimal [2], hits [{reference,
+    reverse, insert, mates [hit, hit]}]} or {"proper": False, "mates": [two
+    map_reads dicts]}."""
+    refs = [r.encode() if isinstance(r, str) else bytes(r) for r in refs]
+    pairs = [tuple(m.encode() if isinstance(m, str) else bytes(m) for m in p) for p in pairs]
+    rcodes = [encode(r) for r in refs]
+    n_refs = len(refs)
+    strands = (False, True) if both_strands else (False,)
+    mr = lambda m, t: t ^ (m == 1)  # noqa: E731  (PairState::mate_reverse)
+    # all four mate rows of every pair with two non-empty mates
+    live = [p for p, (a, b) in enumerate(pairs) if len(a) and len(b)]
+    qs = []
+    for p in live:
+        for m in range(2):
+            c = encode(pairs[p][m])
+            qs += [c, revcomp(c)]
+    mat = score_matrix(qs, rcodes, scoring, local, threads) if qs else None
+    out = [None] * len(pairs)
+    separate = []
+    for i, p in enumerate(live):
+        rows = [[mat[4 * i + 2 * m + rv] for rv in range(2)] for m in range(2)]
+        codes = [[encode(pairs[p][m]), revcomp(encode(pairs[p][m]))] for m in range(2)]
+        cands = []
+        for t in strands:
+            r0, r1 = rows[0][mr(0, t)], rows[1][mr(1, t)]
+            for r in range(n_refs):
+                a, b = int(r0[r]), int(r1[r])
+                if a >= min_score and b >= min_score:
+                    cands.append((a + b, r, t, a, b))
+        cands.sort(key=lambda c: (-c[0], c[1], c[2]))
+        found = []
+        k = 0
+        while k < len(cands) and not found:
+            e = k
+            while e < len(cands) and cands[e][0] == cands[k][0]:
+                e += 1
+            for c in cands[k:e]:
+                als = [align(codes[m][int(mr(m, c[2]))], rcodes[c[1]], scoring, local)
+                       for m in range(2)]
+                if pair_ok([als[0][0], als[1][0]], [als[0][1], als[1][1]], c[2], max_insert):
+                    found.append((c, als))
+            k = e
+        if not found:
+            separate.append(p)
+            continue
+        in_set = {(c[1], c[2]) for c, _ in found}
+        sub = [None, None]
+        for t in strands:
+            for r in range(n_refs):
+                if (r, t) in in_set:
+                    continue
+                for m in range(2):
+                    s = int(rows[m][mr(m, t)][r])
+                    sub[m] = s if sub[m] is None else max(sub[m], s)
+        keep = len(found) if max_ties is None else min(len(found), max_ties + 1)
+        hits = []
+        for c, als in found[:keep]:
+            mates = []
+            for m in range(2):
+                rv = bool(mr(m, c[2]))
+                a, ops = als[m]
+                letters = revcomp_letters(pairs[p][m]) if rv else pairs[p][m]
+                md, nm = md_nm(letters, refs[c[1]], int(a["query_start"]), int(a["ref_start"]),
+                               ops)
+                mates.append({"reference": c[1], "reverse": rv, "score": int(a["score"]),
+                              "query_start": int(a["query_start"]),
+                              "query_end": int(a["query_end"]),
+                              "ref_start": int(a["ref_start"]), "ref_end": int(a["ref_end"]),
+                              "cigar": cigar_string(ops), "md": md, "nm": nm})
+            lo = min(mates[0]["ref_start"], mates[1]["ref_start"])
+            hi = max(mates[0]["ref_end"], mates[1]["ref_end"])
+            hits.append({"reference": c[1], "reverse": bool(c[2]), "insert": hi - lo,
+                         "mates": mates})
+        out[p] = {"proper": True, "score": found[0][0][0], "n_tied": len(found),
+                  "suboptimal": sub, "hits": hits}
+    separate += [p for p in range(len(pairs)) if p not in set(live)]
+    separate.sort()
+    if separate:
+        flat = [pairs[p][m] for p in separate for m in range(2)]
+        mapped = map_reads(flat, refs, scoring, local, min_score=min_score, max_ties=max_ties,
+                           both_strands=True, threads=threads)
+        for i, p in enumerate(separate):
+            out[p] = {"proper": False, "mates": [mapped[2 * i], mapped[2 * i + 1]]}
+    return out

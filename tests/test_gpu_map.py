@@ -133,3 +133,74 @@ def test_map_large_batch_equals_small_ones(oracle):
             part = g.map_reads(data.slice(k0, k0 + 2000).tuple(), both_strands=True)
             for k in range(len(part)):
                 assert whole.mapping(k0 + k) == part.mapping(k), k0 + k
+
+
+# ---------------------------------------------------------------- pairs
+def fixture_pairs(oracle):
+    """The reference's paired fixture, mates trimmed as the CLI trims them."""
+    from tests.helpers import pairs_fixture
+    names, refs, pairs = pairs_fixture()
+    trimmed, _ = oracle.trim_pairs([m for p in pairs.values() for m in p])
+    return ([code_letters(r) for r in refs],
+            [(code_letters(trimmed[2 * i]), code_letters(trimmed[2 * i + 1]))
+             for i in range(len(pairs))])
+
+
+def run_pairs(oracle, panel, pairs, scoring, mode, cap=8, give_letters=True, **opts):
+    codes = [encode(p) for p in panel]
+    mates = [encode(m) if len(m) else np.zeros(0, np.uint8) for p in pairs for m in p]
+    with GpuScorer(codes, Scoring(*scoring), mode, tie_capacity=cap) as g:
+        got = g.map_pairs(mates, ref_letters=panel if give_letters else None, **opts)
+    want = oracle.map_pairs(pairs, panel if give_letters else [code_letters(c) for c in codes],
+                            scoring, mode == Mode.LOCAL, **opts)
+    assert len(got) == len(want)
+    for p, w in enumerate(want):
+        assert got.pair_mapping(p) == w, (p, opts, cap)
+    return got, want
+
+
+@pytest.mark.parametrize("mode", [Mode.SEMIGLOBAL, Mode.LOCAL])
+def test_map_pairs_fixture(oracle, mode):
+    """The paired fixture under the options tests/align_paired.rs uses
+    (--min-score 40, --max-insert 120 and the default 500) and more."""
+    panel, pairs = fixture_pairs(oracle)
+    for min_score, max_insert, both, cap, max_ties in ((40, 500, False, 8, None),
+                                                       (40, 120, False, 8, None),
+                                                       (0, 500, True, 1, None),
+                                                       (40, 60, True, 2, 0)):
+        run_pairs(oracle, panel, pairs, SCHEME, mode, cap=cap, min_score=min_score,
+                  max_insert=max_insert, both_strands=both, max_ties=max_ties)
+
+
+def test_map_pairs_fixture_answers(oracle):
+    """What align_paired.rs pins, through the CUDA path."""
+    from tests.helpers import pairs_fixture
+    names, _, named = pairs_fixture()
+    panel, pairs = fixture_pairs(oracle)
+    by = dict(zip(named, range(len(pairs))))
+    got, _ = run_pairs(oracle, panel, pairs, SCHEME, Mode.SEMIGLOBAL, min_score=40)
+    p = got.pair_mapping(by["paralog"])
+    assert p["proper"] and names[p["hits"][0]["reference"]] == "P1"
+    assert p["suboptimal"][0] == p["hits"][0]["mates"][0]["score"]
+    assert [names[h["reference"]] for h in got.pair_mapping(by["pair_tie"])["hits"]] == ["P1", "P2"]
+    got, _ = run_pairs(oracle, panel, pairs, SCHEME, Mode.SEMIGLOBAL, min_score=40,
+                       max_insert=120)
+    o = got.pair_mapping(by["over_max_insert"])
+    assert not o["proper"] and [m["hits"][0]["reverse"] for m in o["mates"]] == [False, True]
+
+
+@pytest.mark.parametrize("mode", [Mode.SEMIGLOBAL, Mode.LOCAL])
+def test_map_pairs_synthetic(oracle, mode):
+    """C4-style pairs on the 164-reference panel (adapters trimmed): a tight
+    max_insert makes first tiers fail and the pairs walk deeper tiers from
+    full rows; a tie capacity of 1 sends every tied first tier there too."""
+    refs = synth.panel_tiles()
+    P, _ = synth.pairs_c4(refs, n=250, seed=0x5EED_0A01)
+    trimmed, _ = oracle.trim_pairs([P.read(k) for k in range(len(P))])
+    pairs = [(code_letters(trimmed[2 * i]), code_letters(trimmed[2 * i + 1]))
+             for i in range(len(P) // 2)]
+    pairs += [(b"", b"ACGTACGTAC"), (b"ACGT", b"")]
+    panel = [code_letters(r) for r in refs]
+    for max_insert, cap, both in ((500, 8, True), (70, 8, True), (45, 1, False)):
+        run_pairs(oracle, panel, pairs, SCHEME, mode, cap=cap, min_score=20,
+                  max_insert=max_insert, both_strands=both)

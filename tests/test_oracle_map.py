@@ -85,3 +85,42 @@ def test_empty_and_wildcard_reads():
     assert ms[0] == {"best_score": None, "n_tied": 0, "suboptimal": None, "hits": []}
     assert ms[1]["best_score"] == 8 and ms[1]["hits"]
     assert ms[1]["hits"][0]["nm"] == 4
+
+
+def _fixture_pairs():
+    """The reference's paired fixture, mates trimmed of their adapters as the
+    CLI does before map_pairs_scored (align.rs:2844-2863)."""
+    from tests.helpers import pairs_fixture
+    names, refs, pairs = pairs_fixture()
+    mates = [m for p in pairs.values() for m in p]
+    trimmed, _ = O.trim_pairs(mates)
+    L = lambda c: bytes(b"ACGTN"[min(int(x), 4)] for x in c)  # noqa: E731
+    return (names, [L(r) for r in refs], list(pairs),
+            [(L(trimmed[2 * i]), L(trimmed[2 * i + 1])) for i in range(len(pairs))])
+
+
+def test_map_pairs_fixture_answers():
+    """What the reference's tests/align_paired.rs pins for the fixture with
+    --min-score 40, semi-global (the paired default)."""
+    names, refs, pnames, pairs = _fixture_pairs()
+    by = lambda res: dict(zip(pnames, res))  # noqa: E731
+    roomy = by(O.map_pairs(pairs, refs, SCHEME, False, min_score=40))
+    wide = by(O.map_pairs(pairs, refs, SCHEME, False, min_score=40, max_insert=120))
+    p = roomy["paralog"]  # unique on P1, mate-1 XS equal to its AS
+    assert p["proper"] and p["n_tied"] == 1 and names[p["hits"][0]["reference"]] == "P1"
+    assert p["suboptimal"][0] == p["hits"][0]["mates"][0]["score"]
+    t = roomy["pair_tie"]  # the P1 / P2 tie
+    assert t["proper"] and [names[h["reference"]] for h in t["hits"]] == ["P1", "P2"]
+    tm = roomy["terminal_mismatch"]  # kept end to end, 117 + 117
+    assert [m["score"] for m in tm["hits"][0]["mates"]] == [117, 117]
+    assert roomy["over_max_insert"]["proper"] and roomy["over_max_insert"]["hits"][0]["insert"] == 150
+    o = wide["over_max_insert"]  # each mate at its own best (U1), mate 2 reversed
+    assert not o["proper"]
+    assert [(names[m["hits"][0]["reference"]], m["hits"][0]["reverse"]) for m in o["mates"]] == \
+        [("U1", False), ("U1", True)]
+    w = roomy["wrong_orientation"]  # both forward on U2, not proper
+    assert not w["proper"]
+    assert [(names[m["hits"][0]["reference"]], m["hits"][0]["reverse"]) for m in w["mates"]] == \
+        [("U2", False), ("U2", False)]
+    u = roomy["one_unmapped"]  # the junk mate is unmapped
+    assert not u["proper"] and u["mates"][0]["hits"] and not u["mates"][1]["hits"]
