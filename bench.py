@@ -327,6 +327,49 @@ def map_stage(g, refs, reads, scoring, local, skip_cpu):
     return out
 
 
+def map_pairs_stage(g, refs, pairs, scoring, local, skip_cpu, n=100_000):
+    """The whole paired mapping stage: adapters trimmed by the library
+    (esg_pair_adapters), then esg_map_pairs (pair.rs:157-390: the device
+    ranking, the first tiers traced, deeper tiers from full rows, the
+    Separate fallback, MD / NM); wall time of both calls with host buffers,
+    the CLI's paired options (--min-score 40, max insert 500, both template
+    strands).  Beside it the oracle's map_pairs on a small sample."""
+    from eschalign_b200 import adapter
+    sub = pairs.slice(0, 2 * n)
+    codes, off, _ = sub.tuple()
+
+    def run(k0, k1):
+        part = sub.slice(2 * k0, 2 * k1)
+        _, aligned = adapter.pair_adapters(part.tuple())
+        c, o, _ = part.tuple()
+        return g.map_pairs((c, o, aligned), min_score=40, max_insert=500, both_strands=True)
+
+    run(0, 1000)  # warm-up
+    t0 = time.perf_counter()
+    m = run(0, len(sub) // 2)
+    dt = time.perf_counter() - t0
+    n_pairs = len(sub) // 2
+    proper = int((m.pairs["flags"] & 1).sum())
+    out = {"pairs": n_pairs, "seconds": round(dt, 4), "pairs_per_s": n_pairs / dt,
+           "proper": proper, "pair_hits": int(m.pair_hits.size),
+           "options": "trim + map: min_score 40, max_insert 500, both template strands, "
+                      "every tie traced, MD/NM without letters"}
+    if not skip_cpu:
+        from oracle import oracle as O
+        k = min(n_pairs, 300)
+        L = lambda c: bytes(b"ACGTN"[min(int(x), 4)] for x in c)  # noqa: E731
+        t0 = time.perf_counter()
+        trimmed, _ = O.trim_pairs([sub.read(i) for i in range(2 * k)])
+        O.map_pairs([(L(trimmed[2 * i]), L(trimmed[2 * i + 1])) for i in range(k)],
+                    [L(r) for r in refs], scoring, local, min_score=40, max_insert=500,
+                    both_strands=True)
+        dt_c = time.perf_counter() - t0
+        out["cpu"] = {"pairs_per_s": k / dt_c, "kind": "port",
+                      "sample": f"first {k} pairs: trimming, scalar scores on all cores, "
+                                "scalar traceback and MD / NM per hit on one"}
+    return out
+
+
 def reference_gpu_arms(refs, reads, scoring, local, device):
     """Comparison arms: the reference's own align_score_kernel (int) and
     align_score_kernel_h2 (half2), compiled ahead of time for sm_100a from its
@@ -744,6 +787,10 @@ def run_c4(a, ctx, rank):
     peak = int_peak(local_rank)
     roofline = roofline_of(peak, cells * a.steps / t, "semiglobal", None)
     batch.free()
+    map_pairs = None
+    if not a.no_extras:
+        map_pairs = map_pairs_stage(g, refs, pairs, C4_SCORING, False,
+                                    a.no_cpu_baseline or rank != 0 or world != 1)
     step_pairs = a.pair_chunk
     chunks = [pairs.slice(2 * k, 2 * (k + step_pairs)) for k in range(0, n_pairs, step_pairs)]
     te, n_pass, h2d, d2h = feeder(
@@ -777,6 +824,8 @@ def run_c4(a, ctx, rank):
                                                   "kernels")}
         if cpu:
             line["cpu_baseline"] = cpu
+        if map_pairs:
+            line["map_pairs"] = map_pairs
         print(json.dumps(line), flush=True)
 
 
