@@ -50,11 +50,17 @@ constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
 //       ahead (bit 0 local, bit 1 semi-global): +2 % in both with the above
 //   ESG_STEADY_UNROLL  unroll of local mode's unchecked column loop, 16-row
 //       stripes (8: +0.9 % over 4; 32-row stripes have no registers for it)
+//   ESG_K2_R32_BLOCKS  resident CTAs of 32-row stripes (3; 2 lets
+//       semi-global keep its state without spilling but measured -4.6 % on
+//       C2 semi-global, local and C3 unchanged)
 #ifndef ESG_K2_WARPS
 #define ESG_K2_WARPS 4
 #endif
 #ifndef ESG_K2_MIN_BLOCKS
 #define ESG_K2_MIN_BLOCKS 4
+#endif
+#ifndef ESG_K2_R32_BLOCKS
+#define ESG_K2_R32_BLOCKS 3
 #endif
 #ifndef ESG_SC_LDS
 #define ESG_SC_LDS 1
@@ -588,7 +594,7 @@ __device__ __forceinline__ void flush_query(const K2Params& P, uint32_t qid, uin
 // the 16 S - n rows before the read's first row score 0 against every real
 // column and hold H = 0 exactly, the top border the first real row needs.
 template <int R, bool kLocal, bool kPanelW, bool kSmemPanel, bool kLong>
-__global__ void __launch_bounds__(kK2Threads, R > 16 ? 3 : (kPanelW ? 4 : ESG_K2_MIN_BLOCKS))
+__global__ void __launch_bounds__(kK2Threads, R > 16 ? ESG_K2_R32_BLOCKS : (kPanelW ? 4 : ESG_K2_MIN_BLOCKS))
     k2_batched(const K2Params P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint64_t panel_bar;
