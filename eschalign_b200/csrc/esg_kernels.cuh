@@ -45,7 +45,8 @@ constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
 //       8 warps x 2 CTAs)
 //   ESG_SC_LDS  modes whose per-cell scores come from a per-thread record in
 //       shared memory (bit 0 local, bit 1 semi-global) instead of one PRMT
-//       per cell: local +5.0 %, semi-global -1.5 % (spills)
+//       per cell: local +5.0 %, semi-global -1.5 % (spills); semi-global
+//       on 32-row stripes only (ESG_SC_LDS_SG_MINR 32): -1.0 % on C4 pairs
 //   ESG_SEL_PREFETCH  modes that load a lane's next column selector a column
 //       ahead (bit 0 local, bit 1 semi-global): +2 % in both with the above
 //   ESG_STEADY_UNROLL  unroll of local mode's unchecked column loop, 16-row
@@ -81,8 +82,13 @@ constexpr uint32_t kMaxCap = 32;       // largest tie capacity (ESG_MAX_TIE_CAPA
 // 0-5), word c of thread t at c * kK2Threads + t: every thread in its own bank
 constexpr int kScrWords = ESG_SC_LDS ? 6 : 0;
 constexpr uint32_t kScrStride = (uint32_t)kK2Threads * 4;  // bytes between code words
-template <bool kLocal>
-__host__ __device__ constexpr bool sc_lds() { return (ESG_SC_LDS & (kLocal ? 1 : 2)) != 0; }
+#ifndef ESG_SC_LDS_SG_MINR
+#define ESG_SC_LDS_SG_MINR 16
+#endif
+template <bool kLocal, int R>
+__host__ __device__ constexpr bool sc_lds() {
+  return (ESG_SC_LDS & (kLocal ? 1 : 2)) != 0 && (kLocal || R >= ESG_SC_LDS_SG_MINR);
+}
 template <bool kLocal>
 __host__ __device__ constexpr bool sel_prefetch() {
   return (ESG_SEL_PREFETCH & (kLocal ? 1 : 2)) != 0;
@@ -341,7 +347,7 @@ __device__ __forceinline__ void pair_pass(const K2Params& P, uint32_t scr, bool 
                                           const PassConst& K, uint2* buf, bool from_buf,
                                           bool to_buf, uint32_t& v, uint32_t& lr) {
   const int lane = threadIdx.x & 31;
-  constexpr bool kLds = sc_lds<kLocal>() && !kLong;
+  constexpr bool kLds = sc_lds<kLocal, R>() && !kLong;
   constexpr bool kPre = sel_prefetch<kLocal>();
   if constexpr (kLds) {
     // padding rows: local, -128 against every column (H stays 0 under the
@@ -729,7 +735,7 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? ESG_K2_R32_BLOCKS : (kPan
 
     uint32_t ta[R];
     uint32_t tb[kPanelW ? R : 1];
-    const bool wild = row_tables<R, kPanelW, sc_lds<kLocal>()>(
+    const bool wild = row_tables<R, kPanelW, sc_lds<kLocal, R>()>(
         P, valid ? P.codes + P.off[rd] : P.codes, n, rc, valid, s, pad, ta, tb, scr);
     // rows of the read's top padding (first lane only): excluded from the
     // semi-global last-column maximum
