@@ -204,3 +204,24 @@ def test_map_pairs_synthetic(oracle, mode):
     for max_insert, cap, both in ((500, 8, True), (70, 8, True), (45, 1, False)):
         run_pairs(oracle, panel, pairs, SCHEME, mode, cap=cap, min_score=20,
                   max_insert=max_insert, both_strands=both)
+
+
+def test_map_zero_score_ties_and_saturation(oracle):
+    """A read that matches nothing scores 0 locally against every candidate:
+    all 2 x 20 candidates tie (more than the tie capacity, so the list comes
+    from full rows), every trace is empty, and the read is unmapped with its
+    best and tie count kept (mapper.rs:508-512).  Then scores far past int16
+    (re-scored in int32 before tracing) under a large scheme."""
+    panel = [b"A" * (20 + k) for k in range(20)]
+    reads = [b"CCCCCCCC", b"AAAAAAAAAA", b""]
+    for max_ties in (None, 3):
+        got, want = run(oracle, panel, reads, SCHEME, Mode.LOCAL, both_strands=True,
+                        max_ties=max_ties)
+        m = got.mapping(0)
+        assert m["best_score"] == 0 and m["n_tied"] == 40 and m["hits"] == []
+    rng = Rng(0x5EED_0903)
+    big = [random_seq(rng, 600 + 50 * k, 0.0) for k in range(6)]
+    reads = [mutate(rng, r[50:]) for r in big] + [r[::-1] for r in big[:2]]
+    for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+        got, want = run(oracle, big, reads, (100, -100, -27, -27), mode, both_strands=True)
+        assert max(w["best_score"] for w in want) > 32767
