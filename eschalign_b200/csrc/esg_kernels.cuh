@@ -45,8 +45,10 @@ constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
 //       8 warps x 2 CTAs)
 //   ESG_SC_LDS  modes whose per-cell scores come from a per-thread record in
 //       shared memory (bit 0 local, bit 1 semi-global) instead of one PRMT
-//       per cell: local +5.0 %, semi-global -1.5 % (spills); semi-global
-//       on 32-row stripes only (ESG_SC_LDS_SG_MINR 32): -1.0 % on C4 pairs
+//       per cell: local +5.0 %; semi-global on 32-row stripes
+//       (ESG_SC_LDS_SG_MINR 32) +1.9 % on C4 pairs and C2 semi-global once
+//       its last-column snapshot stopped spilling (-1.0 % before), 16-row
+//       stripes as well -0.4 %
 //   ESG_SEL_PREFETCH  modes that load a lane's next column selector a column
 //       ahead (bit 0 local, bit 1 semi-global): +2 % in both with the above
 //   ESG_STEADY_UNROLL  unroll of local mode's unchecked column loop, 16-row
@@ -64,7 +66,7 @@ constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
 #define ESG_K2_R32_BLOCKS 3
 #endif
 #ifndef ESG_SC_LDS
-#define ESG_SC_LDS 1
+#define ESG_SC_LDS 3
 #endif
 #ifndef ESG_SEL_PREFETCH
 #define ESG_SEL_PREFETCH 3
@@ -83,7 +85,7 @@ constexpr uint32_t kMaxCap = 32;       // largest tie capacity (ESG_MAX_TIE_CAPA
 constexpr int kScrWords = ESG_SC_LDS ? 6 : 0;
 constexpr uint32_t kScrStride = (uint32_t)kK2Threads * 4;  // bytes between code words
 #ifndef ESG_SC_LDS_SG_MINR
-#define ESG_SC_LDS_SG_MINR 16
+#define ESG_SC_LDS_SG_MINR 32
 #endif
 template <bool kLocal, int R>
 __host__ __device__ constexpr bool sc_lds() {
@@ -434,9 +436,20 @@ __device__ __forceinline__ void pair_pass(const K2Params& P, uint32_t scr, bool 
     if constexpr (!kLocal) {
       lastrow = max16x2(lastrow, h15);
       if (j == jshort) {
+        // the short half's last column, padding rows left out.  Padding
+        // rows hold G = o + B exactly (H = 0), so a maximum above that is a
+        // read row's and the unmasked maximum stands; only a maximum equal
+        // to it takes the masked one.  (Masking every time kept the pad
+        // mask's selects live across the column loop: 40-52 bytes of spill
+        // in the 32-row kernel.)
         uint32_t cm = K.neg2;
 #pragma unroll
-        for (int r = 0; r < R; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
+        for (int r = 0; r < R; ++r) cm = max16x2(cm, g[r]);
+        if (padmask && (cm >> 16) == (K.g0 >> 16)) {
+          cm = K.neg2;
+#pragma unroll
+          for (int r = 0; r < R; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
+        }
         s_col = cm;
         s_last = lastrow;
       }
