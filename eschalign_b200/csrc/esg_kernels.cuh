@@ -4,15 +4,18 @@
 //
 //   k2_batched   the product: every (query, reference pair) of the panel in
 //                int16x2 lanes.  One warp is a 32-lane systolic array: each
-//                lane holds a 16-row stripe of one query (H, E and the
-//                row's substitution table in registers) and walks the
-//                columns of a reference pair; the stripe's bottom row goes
-//                to the next lane by shuffle, so no DP state ever leaves the
-//                register file.  The two 16-bit halves of every register are
-//                two references (a length-sorted pair).  Substitution is one
-//                PRMT per cell pair, the recurrence three VIADDMNMX and one
-//                VIMNMX (DPX) plus one packed add.  The argmax / tie / XS
-//                reduction is folded in per query, online, in shared memory.
+//                lane holds a 16- or 32-row stripe of one query (G, E and
+//                the row's substitution table or score-record address in
+//                registers) and walks the columns of a reference pair; the
+//                stripe's bottom row goes to the next lane by shuffle, so no
+//                DP state ever leaves the register file.  The two 16-bit
+//                halves of every register are two references (a
+//                length-sorted pair).  Substitution is one PRMT per cell
+//                pair, or (local mode, and semi-global 32-row stripes) one
+//                shared-memory load from the lane's per-column score record;
+//                the recurrence is three VIADDMNMX and one VIMNMX (DPX) plus
+//                one IMAD.  The argmax / tie / XS reduction is folded in per
+//                query, online, in shared memory.
 //                Pairs that may have left int16 are flagged and their query
 //                is re-scored by the int32 kernel.
 //   k3_plain     one thread per (query, reference), int32, the recurrence of
