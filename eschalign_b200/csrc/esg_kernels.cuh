@@ -55,7 +55,10 @@ constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
 //   ESG_SEL_PREFETCH  modes that load a lane's next column selector a column
 //       ahead (bit 0 local, bit 1 semi-global): +2 % in both with the above
 //   ESG_STEADY_UNROLL  unroll of local mode's unchecked column loop, 16-row
-//       stripes (8: +0.9 % over 4; 32-row stripes have no registers for it)
+//       stripes (8: +0.9 % over 4)
+//   ESG_STEADY_UNROLL32  the same for 32-row stripes reading the panel from
+//       L2 (C3: 4 +3.9 % over 1, 8 -1.1 % against 4); with the panel in
+//       shared memory they stay at 1 (unrolled, they spill)
 //   ESG_K2_R32_BLOCKS  resident CTAs of 32-row stripes (3; 2 lets
 //       semi-global keep its state without spilling but measured -4.6 % on
 //       C2 semi-global, local and C3 unchanged)
@@ -76,6 +79,9 @@ constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
 #endif
 #ifndef ESG_STEADY_UNROLL
 #define ESG_STEADY_UNROLL 8
+#endif
+#ifndef ESG_STEADY_UNROLL32
+#define ESG_STEADY_UNROLL32 4
 #endif
 constexpr int kK2Warps = ESG_K2_WARPS;  // warps per k2 CTA
 constexpr int kK2Threads = kK2Warps * 32;
@@ -491,9 +497,9 @@ __device__ __forceinline__ void pair_pass(const K2Params& P, uint32_t scr, bool 
         if ((unsigned)j < (unsigned)mlim) column(j, gt, ft);
       }
       const int sk = active_lane ? skew : 0;
-      // unrolled (ESG_STEADY_UNROLL) for 16-row stripes; 32-row stripes
-      // have no registers to spare
-      constexpr int kUnroll = R <= 16 ? ESG_STEADY_UNROLL : 1;
+      // unrolled (ESG_STEADY_UNROLL, ESG_STEADY_UNROLL32); 32-row stripes
+      // with the panel in shared memory have no registers to spare
+      constexpr int kUnroll = R <= 16 ? ESG_STEADY_UNROLL : (kSmem ? 1 : ESG_STEADY_UNROLL32);
 #pragma unroll kUnroll
       for (; t < m; ++t) {
         uint32_t gt, ft;
