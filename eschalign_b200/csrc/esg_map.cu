@@ -618,8 +618,8 @@ esg_status esg_map_reads(esg_scorer* sc, const uint8_t* codes, const uint64_t* o
                          const uint32_t* len, uint32_t n_reads, const esg_map_options* o,
                          const uint8_t* ref_letters, const uint64_t* ref_letter_off,
                          esg_mapping** out) {
+  if (out) *out = nullptr;
   if (!sc || !o || !out) return merr(ESG_ERR_BAD_ARGUMENT, "NULL scorer, options or out");
-  *out = nullptr;
   std::unique_ptr<esg_mapping> m;
   const esg_status st =
       map_reads_impl(sc, codes, off, len, n_reads, o, ref_letters, ref_letter_off, m);
@@ -633,8 +633,8 @@ esg_status esg_map_pairs(esg_scorer* sc, const uint8_t* codes, const uint64_t* o
                          const uint32_t* len, uint32_t n_pairs, const esg_pair_map_options* o,
                          const uint8_t* ref_letters, const uint64_t* ref_letter_off,
                          esg_mapping** out) {
+  if (out) *out = nullptr;
   if (!sc || !o || !out) return merr(ESG_ERR_BAD_ARGUMENT, "NULL scorer, options or out");
-  *out = nullptr;
   if (n_pairs && (!off || !len)) return merr(ESG_ERR_BAD_ARGUMENT, "off/len must not be NULL");
   if (o->both_strands > 1) return merr(ESG_ERR_BAD_ARGUMENT, "both_strands must be 0 or 1");
   if (ref_letters && !ref_letter_off)

@@ -76,3 +76,33 @@ def test_argument_refusals_before_any_device_call():
     assert _new(lib, ok, mode=7) == 7                           # BadArgument
     assert _new(lib, ok, cap=33) == 7
     assert b"exceeds" in lib.esg_last_error() or lib.esg_last_error()
+
+
+def test_mapping_entry_points_refuse_bad_arguments_on_any_host():
+    """esg_map_reads / esg_map_pairs check their arguments before touching a
+    scorer or a device; the mapping accessors take NULL."""
+    import ctypes
+    import numpy as np
+    from eschalign_b200 import _native
+    lib = eschalign_b200.load()
+    out = ctypes.c_void_p(123)
+    mo = _native.EsgMapOptions(0, 0xFFFFFFFF, 0, 0)
+    po = _native.EsgPairMapOptions(0, 0xFFFFFFFF, 500, 0)
+    lens = np.array([4], np.uint32)
+    off = np.array([0], np.uint64)
+    u32 = ctypes.POINTER(ctypes.c_uint32)
+    u64 = ctypes.POINTER(ctypes.c_uint64)
+    assert lib.esg_map_reads(None, None, None, None, 0, ctypes.byref(mo), None, None,
+                             ctypes.byref(out)) == 7
+    assert out.value is None                                    # cleared on refusal
+    assert lib.esg_map_pairs(None, None, None, None, 0, ctypes.byref(po), None, None,
+                             ctypes.byref(out)) == 7
+    fake = ctypes.c_void_p(1)  # never dereferenced: the options are refused first
+    assert lib.esg_map_reads(fake, None, off.ctypes.data_as(u64), lens.ctypes.data_as(u32), 1,
+                             None, None, None, ctypes.byref(out)) == 7
+    n32, n64 = ctypes.c_uint32(9), ctypes.c_uint64(9)
+    assert lib.esg_mapping_reads(None, ctypes.byref(n32)) is None and n32.value == 0
+    assert lib.esg_mapping_hits(None, ctypes.byref(n64)) is None and n64.value == 0
+    assert lib.esg_mapping_pairs(None, ctypes.byref(n32)) is None and n32.value == 0
+    assert lib.esg_mapping_pair_hits(None, ctypes.byref(n64)) is None
+    lib.esg_mapping_free(None)
