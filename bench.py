@@ -302,9 +302,10 @@ def traceback_stage(g, refs, reads, scoring, local, skip_cpu):
 def map_stage(g, refs, reads, scoring, local, skip_cpu):
     """The whole mapping stage through esg_map_reads (mapper.rs:400-552):
     scoring with the fused reduction, every tie traced (max_ties unset),
-    MD / NM; wall time of the call with host buffers.  Beside it the
-    oracle's map_reads (scalar scores, scalar traceback, MD / NM in Python)
-    on a small sample."""
+    MD / NM; wall time of the call with host buffers.  Beside it the same
+    stage on the host cores as the reference's CPU path runs it (the
+    oracle's cpu_map_reads: AVX-512 scores and tie sets, scalar traceback,
+    MD / NM, all in C on every thread) on a bounded sample."""
     g.map_reads(reads.slice(0, 1000).tuple(), both_strands=True)  # warm-up
     t0 = time.perf_counter()
     m = g.map_reads(reads.tuple(), both_strands=True)
@@ -315,15 +316,18 @@ def map_stage(g, refs, reads, scoring, local, skip_cpu):
            "options": "both strands, min_score 0, every tie traced, MD/NM without letters"}
     if not skip_cpu:
         from oracle import oracle as O
-        n = min(len(reads), 2000)
-        letters = [bytes(b"ACGTN"[min(int(c), 4)] for c in r) for r in refs]
-        rl = [bytes(b"ACGTN"[min(int(c), 4)] for c in reads.read(k)) for k in range(n)]
+        n = min(len(reads), 40_000)
+        prof = O.Profile(refs, scoring)
+        sub = reads.slice(0, n)
+        O.cpu_map_reads(*sub.slice(0, 500).tuple(), refs, scoring, local, both_strands=True,
+                        profile=prof)  # warm-up
         t0 = time.perf_counter()
-        O.map_reads(rl, letters, scoring, local, both_strands=True)
+        *_, used = O.cpu_map_reads(*sub.tuple(), refs, scoring, local, both_strands=True,
+                                   profile=prof)
         dt_c = time.perf_counter() - t0
-        out["cpu"] = {"reads_per_s": n / dt_c, "kind": "port",
-                      "sample": f"first {n} reads: scalar scores on all cores, scalar "
-                                "traceback and MD / NM per hit on one"}
+        out["cpu"] = {"reads_per_s": n / dt_c, "kind": "port", "cores": int(used),
+                      "sample": f"first {n} reads: AVX-512 scores and tie sets, scalar "
+                                "traceback of every taken tie, MD / NM, in C on all threads"}
     return out
 
 

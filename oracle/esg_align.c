@@ -12,6 +12,7 @@
  */
 #include "esg_oracle.h"
 
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -181,6 +182,95 @@ int eo_align_batch(const uint8_t* codes, const uint64_t* off, const uint32_t* le
                 bad = 1;
         }
         free(rc);
+    }
+    return bad ? -1 : nt;
+}
+
+/* crates/eschalign/src/sam.rs:76-121 (md_nm) with calmd_match (sam.rs:63-69)
+ * on codes. */
+static int put_run(char* md, size_t cap, size_t* at, uint32_t run)
+{
+    char buf[16];
+    const int w = snprintf(buf, sizeof buf, "%u", run);
+    if (*at + (size_t)w > cap) return -1;
+    memcpy(md + *at, buf, (size_t)w);
+    *at += (size_t)w;
+    return 0;
+}
+
+static char md_letter(const uint8_t* rc, const uint8_t* rl, size_t j)
+{
+    if (rl) {
+        const uint8_t c = rl[j];
+        return (char)((c >= 'a' && c <= 'z') ? c - 32 : c);
+    }
+    return "ACGTN"[rc[j] > 4 ? 4 : rc[j]];
+}
+
+long eo_md_nm(const uint8_t* q, size_t n, int reverse, const uint8_t* ref_codes,
+              const uint8_t* ref_letters, const eo_alignment* a, const uint32_t* ops, char* md,
+              size_t md_cap, uint32_t* nm_out)
+{
+    size_t at = 0, i = a->query_start, j = a->ref_start;
+    uint32_t run = 0, nm = 0;
+    for (uint32_t k = 0; k < a->n_ops; k++) {
+        const uint32_t op = ops[k] & 0xfu, l = ops[k] >> 4;
+        if (op == 0) {
+            for (uint32_t t = 0; t < l; t++, i++, j++) {
+                uint32_t x = reverse ? q[n - 1 - i] : q[i];
+                x = x > 4 ? 4 : x;
+                if (reverse && x < 4) x = 3 - x;
+                const uint32_t y = ref_codes[j] > 4 ? 4 : ref_codes[j];
+                if (x == y && y < 4) {
+                    run++;
+                } else {
+                    if (put_run(md, md_cap, &at, run) || at + 1 > md_cap) return -1;
+                    md[at++] = md_letter(ref_codes, ref_letters, j);
+                    run = 0;
+                    nm++;
+                }
+            }
+        } else if (op == 1) {
+            i += l;
+            nm += l;
+        } else {
+            if (put_run(md, md_cap, &at, run) || at + 1 + l > md_cap) return -1;
+            md[at++] = '^';
+            for (uint32_t t = 0; t < l; t++) md[at++] = md_letter(ref_codes, ref_letters, j + t);
+            run = 0;
+            j += l;
+            nm += l;
+        }
+    }
+    if (put_run(md, md_cap, &at, run)) return -1;
+    *nm_out = nm;
+    return (long)at;
+}
+
+int eo_md_nm_batch(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
+                   const uint8_t* ref_codes, const uint64_t* ref_off, const uint8_t* ref_letters,
+                   const uint32_t* job_read, const uint32_t* job_ref, const uint8_t* job_rev,
+                   const eo_alignment* al, const uint32_t* ops, size_t ops_stride,
+                   uint32_t n_jobs, int threads, char* md, size_t md_stride, uint32_t* md_len,
+                   uint32_t* nm)
+{
+    int nt = threads;
+#ifdef _OPENMP
+    extern int omp_get_max_threads(void);
+    if (nt <= 0) nt = omp_get_max_threads();
+#else
+    if (nt <= 0) nt = 1;
+#endif
+    int bad = 0;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 256)
+    for (long k = 0; k < (long)n_jobs; k++) {
+        const uint64_t ro = ref_off[job_ref[k]];
+        const long w = eo_md_nm(codes + off[job_read[k]], len[job_read[k]], job_rev[k],
+                                ref_codes + ro, ref_letters ? ref_letters + ro : NULL, &al[k],
+                                ops + (size_t)k * ops_stride, md + (size_t)k * md_stride,
+                                md_stride, &nm[k]);
+        if (w < 0) bad = 1;
+        else md_len[k] = (uint32_t)w;
     }
     return bad ? -1 : nt;
 }

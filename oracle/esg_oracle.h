@@ -184,6 +184,27 @@ int eo_align_batch(const uint8_t* codes, const uint64_t* off, const uint32_t* le
                    uint32_t n_jobs, int32_t ma, int32_t mi, int32_t o, int32_t e, int local,
                    int threads, eo_alignment* out, uint32_t* ops, size_t ops_stride);
 
+/* ---- MD / NM (sam.rs:55-121) ---------------------------------------- */
+/* md_nm on codes: a base matches when both codes are equal and below 4
+ * (calmd_match, sam.rs:63-69, after alphabet.rs:29-50 folds case and U);
+ * reference letters go into MD upper-cased from `ref_letters` (the reference
+ * as in the FASTA), or as A/C/G/T/N from the codes when it is NULL.  The
+ * read is `q` (n codes) as sequenced, aligned reverse-complemented when
+ * `reverse`.  Writes at most md_cap characters (no terminator); returns the
+ * MD length, or -1 if md_cap was too small. */
+long eo_md_nm(const uint8_t* q, size_t n, int reverse, const uint8_t* ref_codes,
+              const uint8_t* ref_letters, const eo_alignment* a, const uint32_t* ops, char* md,
+              size_t md_cap, uint32_t* nm);
+/* eo_md_nm over a batch of traced jobs on OpenMP threads (job k's ops at
+ * ops + k * ops_stride, its MD at md + k * md_stride); returns the thread
+ * count, -1 if an MD stride was too small. */
+int eo_md_nm_batch(const uint8_t* codes, const uint64_t* off, const uint32_t* len,
+                   const uint8_t* ref_codes, const uint64_t* ref_off, const uint8_t* ref_letters,
+                   const uint32_t* job_read, const uint32_t* job_ref, const uint8_t* job_rev,
+                   const eo_alignment* al, const uint32_t* ops, size_t ops_stride,
+                   uint32_t n_jobs, int threads, char* md, size_t md_stride, uint32_t* md_len,
+                   uint32_t* nm);
+
 #ifdef __cplusplus
 }
 #endif

@@ -195,6 +195,13 @@ def lib():
         L.eo_align_batch.argtypes = [u8p, u64p, u32p, u8p, u64p, u32p, u32p, u32p, u8p, C.c_uint32,
                                      C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int, C.c_int,
                                      C.c_void_p, u32p, C.c_size_t]
+        L.eo_md_nm.restype = C.c_long
+        L.eo_md_nm.argtypes = [u8p, C.c_size_t, C.c_int, u8p, u8p, C.c_void_p, u32p, C.c_char_p,
+                               C.c_size_t, u32p]
+        L.eo_md_nm_batch.restype = C.c_int
+        L.eo_md_nm_batch.argtypes = [u8p, u64p, u32p, u8p, u64p, u8p, u32p, u32p, u8p,
+                                     C.c_void_p, u32p, C.c_size_t, C.c_uint32, C.c_int,
+                                     C.c_void_p, C.c_size_t, u32p, u32p]
         L.eo_cpu_map_batch.restype = C.c_int
         L.eo_cpu_map_batch.argtypes = [C.c_void_p, u8p, u64p, u32p, C.c_uint32, C.c_int, C.c_int,
                                        C.c_int, C.c_uint32, C.c_void_p, u32p, i32p]
@@ -731,4 +738,130 @@ def map_pairs(pairs, refs, scoring, local, min_score=0, max_ties=None, max_inser
                            both_strands=True, threads=threads)
         for i, p in enumerate(separate):
             out[p] = {"proper": False, "mates": [mapped[2 * i], mapped[2 * i + 1]]}
+    return out
+
+
+def md_nm_codes(q, reverse, ref_codes, ref_letters, a, ops):
+    """eo_md_nm: md_nm (sam.rs:76-121) on codes, reference letters optional."""
+    q = np.ascontiguousarray(q, dtype=np.uint8)
+    rc = np.ascontiguousarray(ref_codes, dtype=np.uint8)
+    rl = None if ref_letters is None else np.frombuffer(bytes(ref_letters), dtype=np.uint8)
+    rec = np.zeros(1, dtype=ALIGN_DTYPE)
+    rec[0] = a
+    ops = np.ascontiguousarray(ops, dtype=np.uint32)
+    cap = 4 * (q.size + rc.size) + 16
+    buf = C.create_string_buffer(cap)
+    nm = C.c_uint32()
+    w = lib().eo_md_nm(_p(q, C.c_uint8), q.size, int(bool(reverse)), _p(rc, C.c_uint8),
+                       _p(rl, C.c_uint8) if rl is not None else None, rec.ctypes.data,
+                       _p(ops, C.c_uint32), buf, cap, C.byref(nm))
+    if w < 0:
+        raise RuntimeError("eo_md_nm: MD buffer too small")
+    return buf.raw[:w].decode(), nm.value
+
+
+def cpu_map_reads(codes, off, lens, refs, scoring, local, min_score=0, max_ties=None,
+                  both_strands=False, ref_letters=None, cap=32, threads=0, profile=None):
+    """map_reads_scored on the host the way the reference's CPU path runs
+    it, every stage in C on all threads: AVX-512 scores and the tie set
+    (eo_cpu_map_batch; reads whose ties outrun `cap` take their list from
+    full rows), the scalar traceback of the taken ties (eo_align_batch),
+    MD / NM (eo_md_nm_batch).  Returns (results, jobs [read, ref, reverse],
+    alignments, ops [n_jobs, stride], md strings, nm, threads used); the
+    per-read dicts of map_reads come from cpu_mappings()."""
+    prof = profile or Profile(refs, scoring)
+    codes = np.ascontiguousarray(codes, dtype=np.uint8)
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    lens = np.ascontiguousarray(lens, dtype=np.uint32)
+    n = int(lens.size)
+    res, ties, _, used = prof.map_batch(codes, off, lens, local, both_strands, cap=cap,
+                                        threads=threads)
+    take = np.zeros(n, dtype=np.int64)
+    live = (res["flags"] & RESULT_EMPTY) == 0
+    ok = live & (res["best"] >= min_score)
+    nt = res["n_tied"].astype(np.int64)
+    take[ok] = nt[ok] if max_ties is None else np.minimum(nt[ok], max_ties + 1)
+    lists = {}
+    redo = np.nonzero(take > np.minimum(nt, cap))[0]
+    if redo.size:
+        sub_off = off[redo]
+        sub_len = lens[redo]
+        r2, _, rows, _ = prof.map_batch(codes, sub_off, sub_len, local, both_strands, cap=1,
+                                        threads=threads, rows=True)
+        m = redo.size
+        for i, k in enumerate(redo):
+            best = int(res["best"][k])
+            lst = []
+            for r in range(len(refs)):
+                if rows[i, r] == best:
+                    lst.append(r << 1)
+                if both_strands and rows[m + i, r] == best:
+                    lst.append((r << 1) | 1)
+            lists[int(k)] = lst
+    jr, jf, jv = [], [], []
+    for k in np.nonzero(take)[0]:
+        lst = lists.get(int(k))
+        t = int(take[k])
+        cand = lst[:t] if lst is not None else ties[k, :t].tolist()
+        for c in cand:
+            jr.append(k)
+            jf.append(int(c) >> 1)
+            jv.append(int(c) & 1)
+    jobs = np.stack([np.array(jr, np.uint32), np.array(jf, np.uint32),
+                     np.array(jv, np.uint32)], 1) if jr else np.zeros((0, 3), np.uint32)
+    al, ops, _ = align_batch(codes, off, lens, refs, jobs, scoring, local, threads=threads)
+    rc_, ro, rl_ = pack(refs)
+    letters = None
+    if ref_letters is not None:
+        letters = np.frombuffer(b"".join(bytes(x) for x in ref_letters), dtype=np.uint8)
+    stride = ops.shape[1] if ops.ndim == 2 else 1
+    md_stride = 4 * stride + 16
+    nj = jobs.shape[0]
+    md = np.zeros((max(nj, 1), md_stride), dtype=np.uint8)
+    md_len = np.zeros(max(nj, 1), dtype=np.uint32)
+    nm = np.zeros(max(nj, 1), dtype=np.uint32)
+    jr_ = np.ascontiguousarray(jobs[:, 0])
+    jf_ = np.ascontiguousarray(jobs[:, 1])
+    jv_ = np.ascontiguousarray(jobs[:, 2].astype(np.uint8))
+    if nj:
+        w = lib().eo_md_nm_batch(_p(codes, C.c_uint8), _p(off, C.c_uint64), _p(lens, C.c_uint32),
+                                 _p(rc_, C.c_uint8), _p(ro, C.c_uint64),
+                                 _p(letters, C.c_uint8) if letters is not None else None,
+                                 _p(jr_, C.c_uint32), _p(jf_, C.c_uint32), _p(jv_, C.c_uint8),
+                                 al.ctypes.data, _p(ops, C.c_uint32), stride, nj, threads,
+                                 md.ctypes.data, md_stride, _p(md_len, C.c_uint32),
+                                 _p(nm, C.c_uint32))
+        if w < 0:
+            raise RuntimeError("eo_md_nm_batch: MD stride too small")
+    mds = [md[k, :md_len[k]].tobytes().decode() for k in range(nj)]
+    return res, jobs, al, ops, mds, nm[:nj], used
+
+
+def cpu_mappings(res, jobs, al, ops, mds, nm):
+    """cpu_map_reads' output as map_reads' per-read dicts (mapper.rs:497-552)."""
+    out = []
+    by = {}
+    for i, k in enumerate(jobs[:, 0].tolist()):
+        by.setdefault(k, []).append(i)
+    for k in range(res.size):
+        r = res[k]
+        if r["flags"] & RESULT_EMPTY:
+            out.append({"best_score": None, "n_tied": 0, "suboptimal": None, "hits": []})
+            continue
+        rec = {"best_score": int(r["best"]), "n_tied": int(r["n_tied"]),
+               "suboptimal": None if r["suboptimal"] == NO_SCORE else int(r["suboptimal"]),
+               "hits": []}
+        js = by.get(k, [])
+        if js and _aligned_any(ops[js[0], :int(al[js[0]]["n_ops"])]):
+            for i in js:
+                a = al[i]
+                w = ops[i, :int(a["n_ops"])]
+                rec["hits"].append({"reference": int(jobs[i, 1]), "reverse": bool(jobs[i, 2]),
+                                    "score": int(a["score"]),
+                                    "query_start": int(a["query_start"]),
+                                    "query_end": int(a["query_end"]),
+                                    "ref_start": int(a["ref_start"]),
+                                    "ref_end": int(a["ref_end"]), "cigar": cigar_string(w),
+                                    "md": mds[i], "nm": int(nm[i])})
+        out.append(rec)
     return out

@@ -6,6 +6,7 @@ import json
 import os
 import re
 
+import numpy as np
 import pytest
 
 from oracle import oracle as O
@@ -124,3 +125,43 @@ def test_map_pairs_fixture_answers():
         [("U2", False), ("U2", False)]
     u = roomy["one_unmapped"]  # the junk mate is unmapped
     assert not u["proper"] and u["mates"][0]["hits"] and not u["mates"][1]["hits"]
+
+
+def test_md_nm_in_c_matches_samtools_calmd():
+    """eo_md_nm (the C restatement the CPU mapping baseline runs) on codes,
+    with the reference letters, against the same calmd records."""
+    g = json.load(open(GOLDEN))
+    ref = g["reference"].encode()
+    rc = O.encode(ref)
+    for r in g["records"]:
+        lead, words, _ = parse_cigar(r["cigar"])
+        q = O.encode(r["seq"])
+        n_q = sum(w >> 4 for w in words if w & 0xf in (0, 1))
+        n_r = sum(w >> 4 for w in words if w & 0xf in (0, 2))
+        a = (0, lead, lead + n_q, r["pos"] - 1, r["pos"] - 1 + n_r, len(words))
+        assert O.md_nm_codes(q, False, rc, ref, a, words) == (r["md"], r["nm"]), r["name"]
+
+
+@pytest.mark.parametrize("local", [True, False])
+def test_cpu_mapper_equals_the_restatement(local):
+    """The C-composed CPU mapper (AVX-512 scores, scalar traceback, C MD/NM)
+    gives map_reads' dicts exactly, tie lists from full rows included."""
+    if not O.lib().eo_cpu_has_avx512bw():
+        pytest.skip("no AVX-512BW on this host")
+    from tests.helpers import Rng, mutate, random_seq
+    panel = [b"GGGGACGTACGTACGTTTTT", b"CCCCACGTACGTACGTAAAA", b"TTTTTTTTTTTTTTTTTTTT"]
+    panel += [b"A" * (20 + k) for k in range(12)] + [b"ACGTNACGTRACGU" * 3]
+    rng = Rng(0x5EED_0905)
+    reads = [b"ACGTACGTACGT", b"", b"NNNN", b"CCCCCCCC", b"AAAAAAAAAAAA"]
+    reads += [mutate(rng, p[2:]) for p in panel] + [random_seq(rng, 30, 0.05) for _ in range(10)]
+    codes, off, lens = O.pack([O.encode(r) if len(r) else np.zeros(0, np.uint8) for r in reads])
+    refs = [O.encode(p) for p in panel]
+    for both, max_ties, min_score, cap in ((True, None, 0, 2), (False, 0, 10, 8),
+                                           (True, 3, 0, 32)):
+        got = O.cpu_mappings(*O.cpu_map_reads(codes, off, lens, refs, SCHEME, local,
+                                              min_score=min_score, max_ties=max_ties,
+                                              both_strands=both, ref_letters=panel,
+                                              cap=cap)[:6])
+        want = O.map_reads(reads, panel, SCHEME, local, min_score=min_score,
+                           max_ties=max_ties, both_strands=both)
+        assert got == want
