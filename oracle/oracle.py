@@ -865,3 +865,141 @@ def cpu_mappings(res, jobs, al, ops, mds, nm):
                                     "md": mds[i], "nm": int(nm[i])})
         out.append(rec)
     return out
+
+
+def _code_letters(c) -> bytes:
+    return bytes(b"ACGTN"[min(int(x), 4)] for x in c)
+
+
+def cpu_map_pairs(codes, off, lens, refs, scoring, local, min_score=0, max_ties=None,
+                  max_insert=500, both_strands=False, ref_letters=None, cap=32, threads=0,
+                  profile=None, trim=False):
+    """map_pairs_scored on the host cores, the stages in C on all threads:
+    the candidate ranking from AVX-512 rows (eo_cpu_map_pairs, no trimming:
+    the mates come trimmed), the scalar traceback of every pair's first tier
+    (eo_align_batch), the pair constraints on the traced tier, MD / NM
+    (eo_md_nm_batch), and cpu_map_reads for the Separate mates.  Pairs whose
+    first tier all fails or outruns `cap` take the Python restatement
+    (map_pairs).  With `trim` the mates are untrimmed and the ranking call
+    trims them first (TruSeq adapters, adapter.rs:68-110, as the CLI does).
+    Returns (map_pairs' per-pair dicts, threads used)."""
+    prof = profile or Profile(refs, scoring)
+    codes = np.ascontiguousarray(codes, dtype=np.uint8)
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    lens = np.ascontiguousarray(lens, dtype=np.uint32)
+    n = int(lens.size) // 2
+    letters = ref_letters if ref_letters is not None else [_code_letters(r) for r in refs]
+    if trim:
+        res, ties, _, _, ads, used = prof.map_pairs(codes, off, lens, local, both_strands,
+                                                    min_score, cap, threads)
+        lens = np.ascontiguousarray(lens - ads, dtype=np.uint32)
+    else:
+        res, ties, _, _, _, used = prof.map_pairs(codes, off, lens, local, both_strands,
+                                                  min_score, cap, threads, a1=b"", a2=b"")
+    # --- the first tiers, traced together
+    tier = [p for p in range(n) if not res["flags"][p] & RESULT_EMPTY and res["n_tied"][p] <= cap]
+    jr, jf, jv, owner = [], [], [], []
+    for p in tier:
+        for i in range(int(res["n_tied"][p])):
+            c = int(ties[p, i])
+            for m in range(2):
+                jr.append(2 * p + m)
+                jf.append(c >> 1)
+                jv.append((c & 1) ^ (m == 1))
+            owner.append((p, c))
+    jobs = (np.stack([np.array(jr, np.uint32), np.array(jf, np.uint32),
+                      np.array(jv, np.uint32)], 1) if jr else np.zeros((0, 3), np.uint32))
+    al, ops, _ = align_batch(codes, off, lens, refs, jobs, scoring, local, threads=threads)
+    nc = len(owner)
+    ok = np.zeros(nc, dtype=bool)
+    if nc:
+        a0, a1 = al[0::2], al[1::2]
+        cols = np.arange(ops.shape[1])[None, :]
+        matched = ((ops & 0xf) == 0) & (cols < al["n_ops"][:, None].astype(np.int64))
+        aligned = matched.any(axis=1)
+        t = np.array([c & 1 for _, c in owner], dtype=bool)
+        fs = np.where(t, a1["ref_start"], a0["ref_start"]).astype(np.int64)
+        re_ = np.where(t, a0["ref_end"], a1["ref_end"]).astype(np.int64)
+        lo = np.minimum(a0["ref_start"], a1["ref_start"]).astype(np.int64)
+        hi = np.maximum(a0["ref_end"], a1["ref_end"]).astype(np.int64)
+        ok = aligned[0::2] & aligned[1::2] & (fs < re_) & (hi - lo <= max_insert)
+    # --- MD / NM of every traced mate (only the kept ones are read)
+    md_stride = 4 * ops.shape[1] + 16
+    nj = jobs.shape[0]
+    md = np.zeros((max(nj, 1), md_stride), dtype=np.uint8)
+    md_len = np.zeros(max(nj, 1), dtype=np.uint32)
+    nm = np.zeros(max(nj, 1), dtype=np.uint32)
+    if nj:
+        rc_, ro, _ = pack(refs)
+        lt = np.frombuffer(b"".join(bytes(x) for x in letters), dtype=np.uint8)
+        jr_ = np.ascontiguousarray(jobs[:, 0])
+        jf_ = np.ascontiguousarray(jobs[:, 1])
+        jv_ = np.ascontiguousarray(jobs[:, 2].astype(np.uint8))
+        if lib().eo_md_nm_batch(_p(codes, C.c_uint8), _p(off, C.c_uint64), _p(lens, C.c_uint32),
+                                _p(rc_, C.c_uint8), _p(ro, C.c_uint64), _p(lt, C.c_uint8),
+                                _p(jr_, C.c_uint32), _p(jf_, C.c_uint32), _p(jv_, C.c_uint8),
+                                al.ctypes.data, _p(ops, C.c_uint32), ops.shape[1], nj, threads,
+                                md.ctypes.data, md_stride, _p(md_len, C.c_uint32),
+                                _p(nm, C.c_uint32)) < 0:
+            raise RuntimeError("eo_md_nm_batch: MD stride too small")
+
+    def hit(j):
+        a = al[j]
+        w = ops[j, :int(a["n_ops"])]
+        return {"reference": int(jobs[j, 1]), "reverse": bool(jobs[j, 2]),
+                "score": int(a["score"]), "query_start": int(a["query_start"]),
+                "query_end": int(a["query_end"]), "ref_start": int(a["ref_start"]),
+                "ref_end": int(a["ref_end"]), "cigar": cigar_string(w),
+                "md": md[j, :md_len[j]].tobytes().decode(), "nm": int(nm[j])}
+
+    out = [None] * n
+    slow, separate = [], []
+    k = 0
+    for p in range(n):
+        if res["flags"][p] & RESULT_EMPTY:
+            separate.append(p)
+            continue
+        if res["n_tied"][p] > cap:
+            slow.append(p)
+            continue
+        m = int(res["n_tied"][p])
+        idx = list(range(k, k + m))
+        k += m
+        found = [i for i in idx if ok[i]]
+        if not found:
+            slow.append(p)
+            continue
+        sub = [None if res["xs"][p][q] == NO_SCORE else int(res["xs"][p][q]) for q in range(2)]
+        for i in idx:
+            if not ok[i]:
+                for q in range(2):
+                    s = int(al[2 * i + q]["score"])
+                    sub[q] = s if sub[q] is None else max(sub[q], s)
+        keep = len(found) if max_ties is None else min(len(found), max_ties + 1)
+        hits = []
+        for i in found[:keep]:
+            mates = [hit(2 * i), hit(2 * i + 1)]
+            lo = min(mates[0]["ref_start"], mates[1]["ref_start"])
+            hi = max(mates[0]["ref_end"], mates[1]["ref_end"])
+            hits.append({"reference": int(owner[i][1] >> 1), "reverse": bool(owner[i][1] & 1),
+                         "insert": hi - lo, "mates": mates})
+        out[p] = {"proper": True, "score": int(res["best"][p]), "n_tied": len(found),
+                  "suboptimal": sub, "hits": hits}
+    if slow:
+        pl = [(_code_letters(codes[off[2 * p]:off[2 * p] + lens[2 * p]]),
+               _code_letters(codes[off[2 * p + 1]:off[2 * p + 1] + lens[2 * p + 1]]))
+              for p in slow]
+        for p, r in zip(slow, map_pairs(pl, letters, scoring, local, min_score=min_score,
+                                        max_ties=max_ties, max_insert=max_insert,
+                                        both_strands=both_strands, threads=threads)):
+            out[p] = r
+    if separate:
+        so = np.array([off[2 * p + q] for p in separate for q in range(2)], dtype=np.uint64)
+        sl = np.array([lens[2 * p + q] for p in separate for q in range(2)], dtype=np.uint32)
+        mapped = cpu_mappings(*cpu_map_reads(codes, so, sl, refs, scoring, local,
+                                             min_score=min_score, max_ties=max_ties,
+                                             both_strands=True, ref_letters=letters, cap=cap,
+                                             threads=threads, profile=prof)[:6])
+        for i, p in enumerate(separate):
+            out[p] = {"proper": False, "mates": [mapped[2 * i], mapped[2 * i + 1]]}
+    return out, used

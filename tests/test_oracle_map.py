@@ -165,3 +165,51 @@ def test_cpu_mapper_equals_the_restatement(local):
         want = O.map_reads(reads, panel, SCHEME, local, min_score=min_score,
                            max_ties=max_ties, both_strands=both)
         assert got == want
+
+
+@pytest.mark.parametrize("local", [False, True])
+def test_cpu_pair_mapper_equals_the_restatement(local):
+    """The C-composed CPU paired mapper gives map_pairs' dicts exactly: the
+    paired fixture under align_paired.rs's options and synthetic pairs whose
+    first tiers fail (tight max insert) or outrun a small capacity."""
+    if not O.lib().eo_cpu_has_avx512bw():
+        pytest.skip("no AVX-512BW on this host")
+    from eschalign_b200 import synth
+    names, refs, pnames, pairs = _fixture_pairs()
+    cases = [(refs, pairs)]
+    panel = synth.panel_tiles()
+    P, _ = synth.pairs_c4(panel, n=120, seed=0x5EED_0A02)
+    trimmed, _ = O.trim_pairs([P.read(k) for k in range(len(P))])
+    L = lambda c: bytes(b"ACGTN"[min(int(x), 4)] for x in c)  # noqa: E731
+    cases.append(([L(r) for r in panel],
+                  [(L(trimmed[2 * i]), L(trimmed[2 * i + 1])) for i in range(len(P) // 2)]
+                  + [(b"", b"ACGTACGT")]))
+    for letters, prs in cases:
+        rc = [O.encode(x) for x in letters]
+        codes, off, lens = O.pack([O.encode(m) if len(m) else np.zeros(0, np.uint8)
+                                   for p in prs for m in p])
+        for min_score, max_insert, both, cap in ((40, 500, False, 8), (40, 120, True, 2),
+                                                 (20, 45, True, 1), (0, 500, True, 32)):
+            got, _ = O.cpu_map_pairs(codes, off, lens, rc, SCHEME, local, min_score=min_score,
+                                     max_insert=max_insert, both_strands=both,
+                                     ref_letters=letters, cap=cap)
+            want = O.map_pairs(prs, letters, SCHEME, local, min_score=min_score,
+                               max_insert=max_insert, both_strands=both)
+            assert got == want, (min_score, max_insert, both, cap)
+
+
+def test_cpu_pair_mapper_trims_like_the_cli():
+    """trim=True (adapters found by the C ranking call) maps the same pairs
+    as trimming first with the restated pair_adapters."""
+    if not O.lib().eo_cpu_has_avx512bw():
+        pytest.skip("no AVX-512BW on this host")
+    from eschalign_b200 import synth
+    panel = synth.panel_tiles()
+    P, _ = synth.pairs_c4(panel, n=300, seed=0x5EED_0A03)
+    raw = [P.read(k) for k in range(len(P))]
+    trimmed, _ = O.trim_pairs(raw)
+    a, _ = O.cpu_map_pairs(*O.pack(raw), panel, SCHEME, False, min_score=40, both_strands=True,
+                           trim=True)
+    b, _ = O.cpu_map_pairs(*O.pack(trimmed), panel, SCHEME, False, min_score=40,
+                           both_strands=True)
+    assert a == b
