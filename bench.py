@@ -669,7 +669,7 @@ def run_c2(a, ctx, rank):
         extras["plain_sample"] = f"first {len(sub)} reads, both strands"
         extras["traceback"] = traceback_stage(g, refs, sub, scoring, mode == "local",
                                               a.no_cpu_baseline or rank != 0 or world != 1)
-        extras["map"] = map_stage(g, refs, sub, scoring, mode == "local",
+        extras["map"] = map_stage(g, refs, reads, scoring, mode == "local",
                                   a.no_cpu_baseline or rank != 0 or world != 1)
         arms = reference_gpu_arms(refs, sub, scoring, mode == "local", local_rank)
         if arms:

@@ -54,7 +54,13 @@ ESG_HIDDEN uint32_t esg_internal_tie_capacity(const esg_scorer* sc);
 // Bases of the scorer's panel (DP cells per read base and strand).
 ESG_HIDDEN uint64_t esg_internal_panel_bases(const esg_scorer* sc);
 
-// esg_align_batch with the CIGAR words into a vector sized to fit.
+// esg_align_batch with the CIGAR words into a vector sized to fit, on
+// `stream` (NULL: the scorer's stream; the batch must be finished).
 ESG_HIDDEN esg_status esg_internal_align_batch(esg_scorer* sc, esg_batch* b,
                                                const esg_align_job* jobs, uint32_t n_jobs,
-                                               esg_alignment* out, std::vector<uint32_t>* ops);
+                                               esg_alignment* out, std::vector<uint32_t>* ops,
+                                               cudaStream_t stream = nullptr);
+
+// A stream of the scorer's device for the mapping stage's traceback, so
+// that it runs beside the next batch's scoring (NULL if it cannot be made).
+ESG_HIDDEN cudaStream_t esg_internal_trace_stream(esg_scorer* sc);

@@ -110,29 +110,21 @@ bool has_match(const esg_alignment& a, const uint32_t* ops) {
 
 }  // namespace
 
-static esg_status map_reads_impl(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
-                          const uint32_t* len, uint32_t n_reads, const esg_map_options* o,
-                          const uint8_t* ref_letters, const uint64_t* ref_letter_off,
-                          std::unique_ptr<esg_mapping>& result) {
-  if (n_reads && (!off || !len)) return merr(ESG_ERR_BAD_ARGUMENT, "off/len must not be NULL");
-  if (o->both_strands > 1 || o->reserved)
-    return merr(ESG_ERR_BAD_ARGUMENT, "both_strands must be 0 or 1, reserved 0");
-  if (ref_letters && !ref_letter_off)
-    return merr(ESG_ERR_BAD_ARGUMENT, "ref_letters needs ref_letter_off");
-  uint64_t total = 0;
-  for (uint32_t k = 0; k < n_reads; ++k) total += len[k];
-  if (total && !codes) return merr(ESG_ERR_BAD_ARGUMENT, "codes must not be NULL");
-
+// The mapping of reads whose batch `b` is submitted: wait for it, take the
+// tie sets, trace them on `trace_st` (NULL: the scorer's stream), assemble.
+static esg_status map_scored(esg_scorer* sc, esg_batch* b, const uint8_t* codes,
+                             const uint64_t* off, const uint32_t* len, uint32_t n_reads,
+                             const esg_map_options* o, const uint8_t* ref_letters,
+                             const uint64_t* ref_letter_off, cudaStream_t trace_st,
+                             std::unique_ptr<esg_mapping>& result) {
   esg_internal_panel P{};
   esg_internal_panel_of(sc, &P);
   const uint32_t cap = esg_internal_tie_capacity(sc);
   const uint32_t flags = o->both_strands ? ESG_BOTH_STRANDS : 0u;
-
-  // --- score: the fused reduction
-  BatchGuard g;
-  esg_status st = esg_prepare(sc, codes, off, len, n_reads, flags, &g.b);
-  if (st != ESG_OK) return st;
-  if ((st = esg_submit(sc, g.b)) != ESG_OK) return st;
+  struct {
+    esg_batch* b;
+  } g{b};
+  esg_status st;
   std::vector<esg_read_result> res(std::max<uint32_t>(n_reads, 1));
   std::vector<uint32_t> ties(std::max<size_t>((size_t)n_reads * cap, 1));
   if ((st = esg_finish(sc, g.b, res.data(), ties.data(), nullptr)) != ESG_OK) return st;
@@ -191,7 +183,7 @@ static esg_status map_reads_impl(esg_scorer* sc, const uint8_t* codes, const uin
   std::vector<uint32_t> ops;
   if (!jobs.empty() &&
       (st = esg_internal_align_batch(sc, g.b, jobs.data(), (uint32_t)jobs.size(), al.data(),
-                                     &ops)) != ESG_OK)
+                                     &ops, trace_st)) != ESG_OK)
     return st;
 
   // --- the mappings (mapper.rs:497-552), reads split over host threads,
@@ -274,6 +266,75 @@ static esg_status map_reads_impl(esg_scorer* sc, const uint8_t* codes, const uin
     m->md.insert(m->md.end(), parts[t].md.begin(), parts[t].md.end());
   }
   result = std::move(m);
+  return ESG_OK;
+}
+
+// Reads per batch of a large mapping call: batch k + 1 is scored while
+// batch k is traced (on the trace stream) and assembled on the host.
+constexpr uint32_t kMapChunk = 131072;
+
+static esg_status map_reads_impl(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
+                                 const uint32_t* len, uint32_t n_reads, const esg_map_options* o,
+                                 const uint8_t* ref_letters, const uint64_t* ref_letter_off,
+                                 std::unique_ptr<esg_mapping>& result) {
+  if (n_reads && (!off || !len)) return merr(ESG_ERR_BAD_ARGUMENT, "off/len must not be NULL");
+  if (o->both_strands > 1 || o->reserved)
+    return merr(ESG_ERR_BAD_ARGUMENT, "both_strands must be 0 or 1, reserved 0");
+  if (ref_letters && !ref_letter_off)
+    return merr(ESG_ERR_BAD_ARGUMENT, "ref_letters needs ref_letter_off");
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < n_reads; ++k) total += len[k];
+  if (total && !codes) return merr(ESG_ERR_BAD_ARGUMENT, "codes must not be NULL");
+  const uint32_t flags = o->both_strands ? ESG_BOTH_STRANDS : 0u;
+  esg_status st;
+  if (n_reads <= kMapChunk + kMapChunk / 2) {
+    BatchGuard g;
+    if ((st = esg_prepare(sc, codes, off, len, n_reads, flags, &g.b)) != ESG_OK ||
+        (st = esg_submit(sc, g.b)) != ESG_OK)
+      return st;
+    return map_scored(sc, g.b, codes, off, len, n_reads, o, ref_letters, ref_letter_off, nullptr,
+                      result);
+  }
+  cudaStream_t ts = esg_internal_trace_stream(sc);
+  std::vector<uint32_t> cut;
+  for (uint32_t k = 0; k < n_reads; k += kMapChunk) cut.push_back(k);
+  cut.push_back(n_reads);
+  std::unique_ptr<esg_mapping> all(new esg_mapping);
+  all->reads.reserve(n_reads);
+  BatchGuard cur, nxt;
+  if ((st = esg_prepare(sc, codes, off, len, cut[1], flags, &cur.b)) != ESG_OK ||
+      (st = esg_submit(sc, cur.b)) != ESG_OK)
+    return st;
+  for (size_t c = 0; c + 1 < cut.size(); ++c) {
+    const uint32_t k0 = cut[c], nk = cut[c + 1] - cut[c];
+    if (c + 2 < cut.size()) {
+      const uint32_t k1 = cut[c + 1];
+      if ((st = esg_prepare(sc, codes, off + k1, len + k1, cut[c + 2] - k1, flags, &nxt.b)) !=
+              ESG_OK ||
+          (st = esg_submit(sc, nxt.b)) != ESG_OK)
+        return st;
+    }
+    std::unique_ptr<esg_mapping> part;
+    if ((st = map_scored(sc, cur.b, codes, off + k0, len + k0, nk, o, ref_letters,
+                         ref_letter_off, ts, part)) != ESG_OK)
+      return st;
+    const uint64_t hb = all->hits.size(), ob = all->ops.size(), mb = all->md.size();
+    for (esg_read_mapping rm : part->reads) {
+      rm.first_hit += hb;
+      all->reads.push_back(rm);
+    }
+    for (esg_hit h : part->hits) {
+      h.alignment.ops_offset += ob;
+      h.md_offset += mb;
+      all->hits.push_back(h);
+    }
+    all->ops.insert(all->ops.end(), part->ops.begin(), part->ops.end());
+    all->md.insert(all->md.end(), part->md.begin(), part->md.end());
+    esg_batch_free(cur.b);
+    cur.b = nxt.b;
+    nxt.b = nullptr;
+  }
+  result = std::move(all);
   return ESG_OK;
 }
 

@@ -359,7 +359,7 @@ esg_status align_impl(esg_scorer* sc, const uint8_t* d_codes, const uint64_t* d_
                       const uint32_t* d_len, uint32_t n_reads, const uint32_t* h_len,
                       const esg_align_job* jobs, uint32_t n_jobs, esg_alignment* out,
                       uint32_t* ops, uint64_t ops_capacity, uint64_t* ops_needed,
-                      std::vector<uint32_t>* grow = nullptr) {
+                      std::vector<uint32_t>* grow = nullptr, cudaStream_t stream = nullptr) {
   esg_internal_panel P{};
   esg_internal_panel_of(sc, &P);
   if (n_jobs && (!jobs || !out)) return terr(ESG_ERR_BAD_ARGUMENT, "jobs/out must not be NULL");
@@ -469,7 +469,7 @@ esg_status align_impl(esg_scorer* sc, const uint8_t* d_codes, const uint64_t* d_
   };
   size_t total = 0;
   for (size_t v : sizes) total += v;
-  cudaStream_t st = P.stream;
+  cudaStream_t st = stream ? stream : P.stream;
   void* mem = nullptr;
   TCUDA(cudaMallocFromPoolAsync(&mem, total, P.pool, st));
   char* at = (char*)mem;
@@ -587,7 +587,7 @@ esg_status align_impl(esg_scorer* sc, const uint8_t* d_codes, const uint64_t* d_
 
 esg_status esg_internal_align_batch(esg_scorer* sc, esg_batch* b, const esg_align_job* jobs,
                                     uint32_t n_jobs, esg_alignment* out,
-                                    std::vector<uint32_t>* ops) {
+                                    std::vector<uint32_t>* ops, cudaStream_t stream) {
   const uint8_t* codes = nullptr;
   const uint64_t* off = nullptr;
   const uint32_t* len = nullptr;
@@ -596,7 +596,7 @@ esg_status esg_internal_align_batch(esg_scorer* sc, esg_batch* b, const esg_alig
   esg_internal_batch_reads(b, &codes, &off, &len, &n_reads, &h_len);
   if (!codes) return terr(ESG_ERR_BAD_ARGUMENT, "the batch is not submitted");
   return align_impl(sc, codes, off, len, n_reads, h_len, jobs, n_jobs, out, nullptr, 0, nullptr,
-                    ops);
+                    ops, stream);
 }
 
 extern "C" {

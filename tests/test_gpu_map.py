@@ -225,3 +225,28 @@ def test_map_zero_score_ties_and_saturation(oracle):
     for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
         got, want = run(oracle, big, reads, (100, -100, -27, -27), mode, both_strands=True)
         assert max(w["best_score"] for w in want) > 32767
+
+
+def test_map_pipelined_call_equals_single_batches():
+    """300 000 C2 reads in one call (scored in batches, each batch traced on
+    its own stream while the next is scored) equal three single-batch calls
+    of 100 000, array for array."""
+    refs = synth.panel_tiles()
+    data = synth.reads_c2(refs, n=300_000, seed=0x5EED_0907)
+    with GpuScorer(refs, Scoring(*SCHEME), Mode.LOCAL) as g:
+        whole = g.map_reads(data.tuple(), both_strands=True)
+        parts = [g.map_reads(data.slice(k, k + 100_000).tuple(), both_strands=True)
+                 for k in range(0, 300_000, 100_000)]
+    fields = ("best_score", "suboptimal", "n_tied", "flags", "n_hits")
+    for f in fields:
+        assert (whole.reads[f] == np.concatenate([p.reads[f] for p in parts])).all(), f
+    hf = ("reference", "reverse", "score", "query_start", "query_end", "ref_start", "ref_end",
+          "n_ops", "nm", "md_len")
+    for f in hf:
+        assert (whole.hits[f] == np.concatenate([p.hits[f] for p in parts])).all(), f
+    assert (whole.ops == np.concatenate([p.ops for p in parts])).all()
+    assert whole.md_bytes == b"".join(p.md_bytes for p in parts)
+    # offsets are consistent: each read's hits start where the previous ended
+    fh = whole.reads["first_hit"].astype(np.int64)
+    nh = whole.reads["n_hits"].astype(np.int64)
+    assert (fh[1:] == fh[:-1] + nh[:-1]).all()
