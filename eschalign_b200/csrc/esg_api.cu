@@ -133,7 +133,6 @@ struct esg_scorer {
   bool tuned = false;
   uint32_t max_chunks = 64;  // panel chunks per tile at most (1: never chunk)
   cudaStream_t aux = nullptr;          // second stream: the long-query kernel
-  cudaStream_t trace = nullptr;        // the mapping stage's traceback (made on first use)
   // batches' device memory: a pool of this scorer's own that keeps what
   // finished batches return, so the next batch maps no new memory
   cudaMemPool_t pool = nullptr;
@@ -696,10 +695,6 @@ void esg_scorer_free(esg_scorer* sc) {
     cudaStreamSynchronize(sc->aux);
     cudaStreamDestroy(sc->aux);
   }
-  if (sc->trace) {
-    cudaStreamSynchronize(sc->trace);
-    cudaStreamDestroy(sc->trace);
-  }
   if (sc->fork) cudaEventDestroy(sc->fork);
   if (sc->join) cudaEventDestroy(sc->join);
   if (sc->pool) cudaMemPoolDestroy(sc->pool);
@@ -1016,18 +1011,6 @@ size_t esg_internal_pool_spare(esg_scorer* sc) {
 int esg_internal_device(const esg_scorer* sc) { return sc ? sc->device : 0; }
 
 uint32_t esg_internal_tie_capacity(const esg_scorer* sc) { return sc ? sc->cap : 0; }
-
-cudaStream_t esg_internal_trace_stream(esg_scorer* sc) {
-  if (!sc) return nullptr;
-  if (!sc->trace) {
-    cudaSetDevice(sc->device);
-    if (cudaStreamCreateWithFlags(&sc->trace, cudaStreamNonBlocking) != cudaSuccess) {
-      cudaGetLastError();
-      sc->trace = nullptr;
-    }
-  }
-  return sc->trace;
-}
 
 uint64_t esg_internal_panel_bases(const esg_scorer* sc) { return sc ? sc->panel_bases : 0; }
 

@@ -61,6 +61,3 @@ ESG_HIDDEN esg_status esg_internal_align_batch(esg_scorer* sc, esg_batch* b,
                                                esg_alignment* out, std::vector<uint32_t>* ops,
                                                cudaStream_t stream = nullptr);
 
-// A stream of the scorer's device for the mapping stage's traceback, so
-// that it runs beside the next batch's scoring (NULL if it cannot be made).
-ESG_HIDDEN cudaStream_t esg_internal_trace_stream(esg_scorer* sc);

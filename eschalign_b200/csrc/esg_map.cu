@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <string>
 #include <thread>
@@ -111,11 +112,14 @@ bool has_match(const esg_alignment& a, const uint32_t* ops) {
 }  // namespace
 
 // The mapping of reads whose batch `b` is submitted: wait for it, take the
-// tie sets, trace them on `trace_st` (NULL: the scorer's stream), assemble.
+// tie sets, trace them on the scorer's stream, call `after_trace` (the
+// caller queues its next batch there, so the device scores it while this
+// batch is assembled), assemble.
 static esg_status map_scored(esg_scorer* sc, esg_batch* b, const uint8_t* codes,
                              const uint64_t* off, const uint32_t* len, uint32_t n_reads,
                              const esg_map_options* o, const uint8_t* ref_letters,
-                             const uint64_t* ref_letter_off, cudaStream_t trace_st,
+                             const uint64_t* ref_letter_off,
+                             const std::function<esg_status()>& after_trace,
                              std::unique_ptr<esg_mapping>& result) {
   esg_internal_panel P{};
   esg_internal_panel_of(sc, &P);
@@ -183,8 +187,9 @@ static esg_status map_scored(esg_scorer* sc, esg_batch* b, const uint8_t* codes,
   std::vector<uint32_t> ops;
   if (!jobs.empty() &&
       (st = esg_internal_align_batch(sc, g.b, jobs.data(), (uint32_t)jobs.size(), al.data(),
-                                     &ops, trace_st)) != ESG_OK)
+                                     &ops)) != ESG_OK)
     return st;
+  if (after_trace && (st = after_trace()) != ESG_OK) return st;
 
   // --- the mappings (mapper.rs:497-552), reads split over host threads,
   // each part's hits / words / MD concatenated in read order
@@ -269,8 +274,11 @@ static esg_status map_scored(esg_scorer* sc, esg_batch* b, const uint8_t* codes,
   return ESG_OK;
 }
 
-// Reads per batch of a large mapping call: batch k + 1 is scored while
-// batch k is traced (on the trace stream) and assembled on the host.
+// Reads per batch of a large mapping call.  The scoring kernel holds every
+// SM until it ends, so a batch's traceback cannot run beside the next
+// batch's scoring: each batch is traced as soon as it is scored, the next
+// one (prepared meanwhile) is queued, and the traced batch is assembled on
+// the host while the device scores the next.
 constexpr uint32_t kMapChunk = 131072;
 
 static esg_status map_reads_impl(esg_scorer* sc, const uint8_t* codes, const uint64_t* off,
@@ -292,31 +300,29 @@ static esg_status map_reads_impl(esg_scorer* sc, const uint8_t* codes, const uin
     if ((st = esg_prepare(sc, codes, off, len, n_reads, flags, &g.b)) != ESG_OK ||
         (st = esg_submit(sc, g.b)) != ESG_OK)
       return st;
-    return map_scored(sc, g.b, codes, off, len, n_reads, o, ref_letters, ref_letter_off, nullptr,
+    return map_scored(sc, g.b, codes, off, len, n_reads, o, ref_letters, ref_letter_off, {},
                       result);
   }
-  cudaStream_t ts = esg_internal_trace_stream(sc);
   std::vector<uint32_t> cut;
   for (uint32_t k = 0; k < n_reads; k += kMapChunk) cut.push_back(k);
   cut.push_back(n_reads);
   std::unique_ptr<esg_mapping> all(new esg_mapping);
   all->reads.reserve(n_reads);
   BatchGuard cur, nxt;
-  if ((st = esg_prepare(sc, codes, off, len, cut[1], flags, &cur.b)) != ESG_OK ||
-      (st = esg_submit(sc, cur.b)) != ESG_OK)
+  auto prepare = [&](size_t c, BatchGuard& into) {
+    return esg_prepare(sc, codes, off + cut[c], len + cut[c], cut[c + 1] - cut[c], flags,
+                       &into.b);
+  };
+  if ((st = prepare(0, cur)) != ESG_OK || (st = esg_submit(sc, cur.b)) != ESG_OK ||
+      (st = prepare(1, nxt)) != ESG_OK)
     return st;
   for (size_t c = 0; c + 1 < cut.size(); ++c) {
     const uint32_t k0 = cut[c], nk = cut[c + 1] - cut[c];
-    if (c + 2 < cut.size()) {
-      const uint32_t k1 = cut[c + 1];
-      if ((st = esg_prepare(sc, codes, off + k1, len + k1, cut[c + 2] - k1, flags, &nxt.b)) !=
-              ESG_OK ||
-          (st = esg_submit(sc, nxt.b)) != ESG_OK)
-        return st;
-    }
+    const bool more = c + 2 < cut.size();
     std::unique_ptr<esg_mapping> part;
     if ((st = map_scored(sc, cur.b, codes, off + k0, len + k0, nk, o, ref_letters,
-                         ref_letter_off, ts, part)) != ESG_OK)
+                         ref_letter_off,
+                         [&]() { return more ? esg_submit(sc, nxt.b) : ESG_OK; }, part)) != ESG_OK)
       return st;
     const uint64_t hb = all->hits.size(), ob = all->ops.size(), mb = all->md.size();
     for (esg_read_mapping rm : part->reads) {
@@ -333,6 +339,7 @@ static esg_status map_reads_impl(esg_scorer* sc, const uint8_t* codes, const uin
     esg_batch_free(cur.b);
     cur.b = nxt.b;
     nxt.b = nullptr;
+    if (c + 3 < cut.size() && (st = prepare(c + 2, nxt)) != ESG_OK) return st;
   }
   result = std::move(all);
   return ESG_OK;
