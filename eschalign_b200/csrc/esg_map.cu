@@ -125,13 +125,10 @@ static esg_status map_scored(esg_scorer* sc, esg_batch* b, const uint8_t* codes,
   esg_internal_panel_of(sc, &P);
   const uint32_t cap = esg_internal_tie_capacity(sc);
   const uint32_t flags = o->both_strands ? ESG_BOTH_STRANDS : 0u;
-  struct {
-    esg_batch* b;
-  } g{b};
   esg_status st;
   std::vector<esg_read_result> res(std::max<uint32_t>(n_reads, 1));
   std::vector<uint32_t> ties(std::max<size_t>((size_t)n_reads * cap, 1));
-  if ((st = esg_finish(sc, g.b, res.data(), ties.data(), nullptr)) != ESG_OK) return st;
+  if ((st = esg_finish(sc, b, res.data(), ties.data(), nullptr)) != ESG_OK) return st;
 
   // --- the taken ties (mapper.rs:458-465): reads whose list the tie
   // capacity cut short get it from full rows
@@ -186,7 +183,7 @@ static esg_status map_scored(esg_scorer* sc, esg_batch* b, const uint8_t* codes,
   std::vector<esg_alignment> al(jobs.size());
   std::vector<uint32_t> ops;
   if (!jobs.empty() &&
-      (st = esg_internal_align_batch(sc, g.b, jobs.data(), (uint32_t)jobs.size(), al.data(),
+      (st = esg_internal_align_batch(sc, b, jobs.data(), (uint32_t)jobs.size(), al.data(),
                                      &ops)) != ESG_OK)
     return st;
   if (after_trace && (st = after_trace()) != ESG_OK) return st;
