@@ -589,54 +589,91 @@ static esg_status map_pairs_impl(esg_scorer* sc, const uint8_t* codes, const uin
         }
   }
 
-  // --- phase 3: Proper mappings (pair.rs:294-360)
+  // --- phase 3: Proper mappings (pair.rs:294-360), pairs split over host
+  // threads, each part's pair hits / words / MD concatenated in pair order
   std::unique_ptr<esg_mapping> out(new esg_mapping);
   out->pairs.resize(n_pairs);
   out->reads.resize(n_mates);
-  std::string md;
-  for (uint32_t p = 0; p < n_pairs; ++p) {
-    esg_pair_mapping& pm = out->pairs[p];
-    pm = esg_pair_mapping{};
-    pm.first_hit = out->pair_hits.size();
-    pm.suboptimal[0] = pm.suboptimal[1] = ESG_NO_SCORE;
-    if (!kind[p]) continue;
-    const auto& fs = found[p];
-    pm.flags = ESG_PAIR_PROPER;
-    pm.score = fs[0].c.sum;
-    pm.n_tied = (uint32_t)fs.size();
-    for (uint32_t q = 0; q < 2; ++q)
-      if (xs[2 * (size_t)p + q] != ESG_NO_SCORE) {
-        pm.suboptimal[q] = xs[2 * (size_t)p + q];
-        pm.flags |= q ? ESG_PAIR_HAS_XS2 : ESG_PAIR_HAS_XS1;
+  struct Part {
+    std::vector<esg_pair_hit> hits;
+    std::vector<uint32_t> ops;
+    std::vector<char> md;
+  };
+  auto assemble = [&](uint32_t p0, uint32_t p1, Part& part) {
+    std::string md;
+    for (uint32_t p = p0; p < p1; ++p) {
+      esg_pair_mapping& pm = out->pairs[p];
+      pm = esg_pair_mapping{};
+      pm.first_hit = part.hits.size();
+      pm.suboptimal[0] = pm.suboptimal[1] = ESG_NO_SCORE;
+      if (!kind[p]) continue;
+      const auto& fs = found[p];
+      pm.flags = ESG_PAIR_PROPER;
+      pm.score = fs[0].c.sum;
+      pm.n_tied = (uint32_t)fs.size();
+      for (uint32_t q = 0; q < 2; ++q)
+        if (xs[2 * (size_t)p + q] != ESG_NO_SCORE) {
+          pm.suboptimal[q] = xs[2 * (size_t)p + q];
+          pm.flags |= q ? ESG_PAIR_HAS_XS2 : ESG_PAIR_HAS_XS1;
+        }
+      const uint32_t keep = (o->max_ties == ESG_ALL_TIES || o->max_ties >= pm.n_tied)
+                                ? pm.n_tied
+                                : o->max_ties + 1;
+      for (uint32_t k = 0; k < keep; ++k) {
+        const Found& f = fs[k];
+        esg_pair_hit ph{};
+        ph.reference = f.c.ref;
+        ph.reverse = f.c.t;
+        for (uint32_t q = 0; q < 2; ++q) {
+          const uint32_t* w = f.w[q] ? f.w[q] : ops2.data() + f.al[q].ops_offset;
+          esg_alignment a = f.al[q];
+          esg_hit& h = ph.mates[q];
+          h.reference = f.c.ref;
+          h.reverse = mate_reverse(q, f.c.t);
+          md_nm(codes + off[2 * p + q], len[2 * p + q], h.reverse != 0,
+                P.h_codes + P.h_off[f.c.ref],
+                ref_letters ? ref_letters + ref_letter_off[f.c.ref] : nullptr, a, w, md, h.nm);
+          h.md_offset = part.md.size();
+          h.md_len = (uint32_t)md.size();
+          part.md.insert(part.md.end(), md.begin(), md.end());
+          a.ops_offset = part.ops.size();
+          part.ops.insert(part.ops.end(), w, w + a.n_ops);
+          h.alignment = a;
+        }
+        ph.insert = std::max(ph.mates[0].alignment.ref_end, ph.mates[1].alignment.ref_end) -
+                    std::min(ph.mates[0].alignment.ref_start, ph.mates[1].alignment.ref_start);
+        part.hits.push_back(ph);
       }
-    const uint32_t keep = (o->max_ties == ESG_ALL_TIES || o->max_ties >= pm.n_tied)
-                              ? pm.n_tied
-                              : o->max_ties + 1;
-    for (uint32_t k = 0; k < keep; ++k) {
-      const Found& f = fs[k];
-      esg_pair_hit ph{};
-      ph.reference = f.c.ref;
-      ph.reverse = f.c.t;
-      for (uint32_t q = 0; q < 2; ++q) {
-        const uint32_t* w = f.w[q] ? f.w[q] : ops2.data() + f.al[q].ops_offset;
-        esg_alignment a = f.al[q];
-        esg_hit& h = ph.mates[q];
-        h.reference = f.c.ref;
-        h.reverse = mate_reverse(q, f.c.t);
-        md_nm(codes + off[2 * p + q], len[2 * p + q], h.reverse != 0, P.h_codes + P.h_off[f.c.ref],
-              ref_letters ? ref_letters + ref_letter_off[f.c.ref] : nullptr, a, w, md, h.nm);
-        h.md_offset = out->md.size();
-        h.md_len = (uint32_t)md.size();
-        out->md.insert(out->md.end(), md.begin(), md.end());
-        a.ops_offset = out->ops.size();
-        out->ops.insert(out->ops.end(), w, w + a.n_ops);
-        h.alignment = a;
-      }
-      ph.insert = std::max(ph.mates[0].alignment.ref_end, ph.mates[1].alignment.ref_end) -
-                  std::min(ph.mates[0].alignment.ref_start, ph.mates[1].alignment.ref_start);
-      out->pair_hits.push_back(ph);
+      pm.n_hits = keep;
     }
-    pm.n_hits = keep;
+  };
+  {
+    const uint32_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const uint32_t n_parts = std::max(1u, std::min(hw, n_pairs / 2048));
+    std::vector<Part> parts(n_parts);
+    std::vector<uint32_t> cut(n_parts + 1);
+    for (uint32_t t = 0; t <= n_parts; ++t) cut[t] = (uint32_t)((uint64_t)n_pairs * t / n_parts);
+    if (n_parts == 1) {
+      assemble(0, n_pairs, parts[0]);
+    } else {
+      std::vector<std::thread> th;
+      for (uint32_t t = 0; t < n_parts; ++t)
+        th.emplace_back(assemble, cut[t], cut[t + 1], std::ref(parts[t]));
+      for (auto& x : th) x.join();
+    }
+    for (uint32_t t = 0; t < n_parts; ++t) {
+      const uint64_t hb = out->pair_hits.size(), ob = out->ops.size(), mb = out->md.size();
+      for (uint32_t p = cut[t]; p < cut[t + 1]; ++p) out->pairs[p].first_hit += hb;
+      for (esg_pair_hit ph : parts[t].hits) {
+        for (uint32_t q = 0; q < 2; ++q) {
+          ph.mates[q].alignment.ops_offset += ob;
+          ph.mates[q].md_offset += mb;
+        }
+        out->pair_hits.push_back(ph);
+      }
+      out->ops.insert(out->ops.end(), parts[t].ops.begin(), parts[t].ops.end());
+      out->md.insert(out->md.end(), parts[t].md.begin(), parts[t].md.end());
+    }
   }
 
   // --- the rest: each mate on its own, both strands (pair.rs:362-387)

@@ -250,3 +250,21 @@ def test_map_pipelined_call_equals_single_batches():
     fh = whole.reads["first_hit"].astype(np.int64)
     nh = whole.reads["n_hits"].astype(np.int64)
     assert (fh[1:] == fh[:-1] + nh[:-1]).all()
+
+
+def test_map_pairs_large_batch_equals_small_ones():
+    """20 000 trimmed C4 pairs in one call (the Proper pairs' hits assembled
+    on several host threads) equal the same pairs mapped 2000 at a time."""
+    from eschalign_b200 import adapter
+    refs = synth.panel_tiles()
+    P, _ = synth.pairs_c4(refs, n=20_000, seed=0x5EED_0A04)
+    codes, off, _ = P.tuple()
+    _, aligned = adapter.pair_adapters(P.tuple())
+    with GpuScorer(refs, Scoring(*SCHEME), Mode.SEMIGLOBAL) as g:
+        whole = g.map_pairs((codes, off, aligned), min_score=40, both_strands=True)
+        assert len(whole) == 20_000
+        for p0 in range(0, 20_000, 2000):
+            part = g.map_pairs((codes, off[2 * p0:2 * p0 + 4000], aligned[2 * p0:2 * p0 + 4000]),
+                               min_score=40, both_strands=True)
+            for p in range(len(part)):
+                assert whole.pair_mapping(p0 + p) == part.pair_mapping(p), p0 + p
