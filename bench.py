@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the panel-scoring hot path (one JSON line on rank 0).
 
-Workload (BASELINE config "plain vs batched scale-up"): 1 000 000 synthetic
+Workload (C2, the plain-vs-batched scale-up case): 1 000 000 synthetic
 reads, lengths lognormal (median 110, sigma 0.4) clipped to 20-1000, cut from
 a 164-reference panel of 70-180 nt (8 % subs, 2 % ins, 1 % del) or random,
 both strands, scored against every reference and reduced per read to best
