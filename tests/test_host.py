@@ -102,3 +102,49 @@ def test_fits_f16_matches_the_reference_bound():
     s = Scoring(3, -2, -5, -2)
     assert fits_f16(678, 1000, s)
     assert not fits_f16(679, 1000, s)
+
+
+def test_mapping_results_decode_without_a_device():
+    """Mappings turns the C ABI's arrays (esg_read_mapping, esg_hit,
+    esg_pair_mapping, esg_pair_hit, CIGAR words, MD characters) into the
+    reference's ReadMapping / PairMapping fields."""
+    import numpy as np
+    from eschalign_b200.scorer import (HIT_DTYPE, MAPPING_DTYPE, PAIR_HIT_DTYPE,
+                                       PAIR_MAPPING_DTYPE, Mappings)
+    ops = np.array([(5 << 4) | 0, (1 << 4) | 1, (3 << 4) | 0, (2 << 4) | 2, (4 << 4) | 0],
+                   dtype=np.uint32)
+    md = b"8^AC2G1" + b"12"
+    hits = np.zeros(3, dtype=HIT_DTYPE)
+    hits[0] = (2, 1, 17, 1, 10, 4, 15, 5, 0, 4, 7, 0)     # 5M1I3M2D4M, MD 8^AC2G1
+    hits[1] = (0, 0, 24, 0, 12, 0, 12, 1, 4, 0, 2, 7)     # 4M (words 4..5), MD 12
+    reads = np.zeros(3, dtype=MAPPING_DTYPE)
+    reads[0] = (17, 9, 1, 3, 1, 0, 0)
+    reads[1] = (5, 0, 2, 1, 0, 0, 1)                      # no suboptimal, unmapped
+    reads[2] = (0, 0, 0, 0, 0, 0, 1)                      # empty read
+    m = Mappings(reads, hits[:2], ops, md)
+    assert len(m) == 3
+    a = m.mapping(0)
+    assert a["best_score"] == 17 and a["suboptimal"] == 9 and a["n_tied"] == 1
+    assert a["hits"] == [{"reference": 2, "reverse": True, "score": 17, "query_start": 1,
+                          "query_end": 10, "ref_start": 4, "ref_end": 15,
+                          "cigar": "5M1I3M2D4M", "md": "8^AC2G1", "nm": 4}]
+    assert m.mapping(1) == {"best_score": 5, "n_tied": 2, "suboptimal": None, "hits": []}
+    assert m.mapping(2) == {"best_score": None, "n_tied": 0, "suboptimal": None, "hits": []}
+    # a paired result: pair 0 Proper with one hit, pair 1 Separate (mates 2, 3)
+    pairs = np.zeros(2, dtype=PAIR_MAPPING_DTYPE)
+    pairs[0] = (1 | 2, 41, 1, 1, (17, -5), 0)              # XS of mate 1 only
+    ph = np.zeros(1, dtype=PAIR_HIT_DTYPE)
+    ph[0]["reference"], ph[0]["reverse"], ph[0]["insert"] = 2, 0, 22
+    ph[0]["mates"][0] = hits[0]
+    ph[0]["mates"][1] = hits[1]
+    preads = np.zeros(4, dtype=MAPPING_DTYPE)
+    preads[2] = (24, 0, 1, 1, 1, 0, 0)
+    preads[3] = (0, 0, 0, 0, 0, 0, 1)
+    pm = Mappings(preads, hits[1:2], ops, md, pairs, ph)
+    assert len(pm) == 2
+    p0 = pm.pair_mapping(0)
+    assert p0["proper"] and p0["score"] == 41 and p0["suboptimal"] == [17, None]
+    assert p0["hits"][0]["insert"] == 22 and p0["hits"][0]["mates"][1]["md"] == "12"
+    p1 = pm.pair_mapping(1)
+    assert not p1["proper"] and p1["mates"][0]["hits"][0]["cigar"] == "4M"
+    assert p1["mates"][1]["best_score"] is None
