@@ -233,8 +233,8 @@ def cpu_baseline(refs, reads, scoring, mode, seconds, threads=0, chunk=64):
     n = int(min(len(reads), max(n_cal, n_cal * seconds / max(dt, 1e-3))))
     sample = reads.slice(0, n)
     t = time.perf_counter()
-    _, _, _, used = prof.map_batch(*sample.tuple(), local=local, both_strands=True,
-                                   threads=threads)
+    res, ties, _, used = prof.map_batch(*sample.tuple(), local=local, both_strands=True,
+                                        threads=threads)
     dt = time.perf_counter() - t
     cells = 2 * sample.bases() * panel_bases
     O.lib().eo_cpu_set_chunk(64)
@@ -242,7 +242,20 @@ def cpu_baseline(refs, reads, scoring, mode, seconds, threads=0, chunk=64):
             "sample": f"first {n} of {len(reads)} reads, both strands, {mode} "
                       f"{','.join(map(str, scoring))}; {dt:.1f} s; reads/s {n / dt:.0f}; "
                       f"{chunk} reads per work unit",
-            "reads_per_s": n / dt, "seconds": dt}
+            "reads_per_s": n / dt, "seconds": dt, "_results": (res, ties)}
+
+
+def same_results(a, ta, b, tb):
+    """Per-read results equal field for field, and the listed ties (the
+    first min(n_tied, capacity)) equal in order."""
+    if not all(np.array_equal(a[f], b[f]) for f in ("best", "suboptimal", "n_tied")):
+        return False
+    if not np.array_equal(a["flags"] & 3, b["flags"] & 3):
+        return False
+    cap = min(ta.shape[1], tb.shape[1])
+    n_l = np.minimum(a["n_tied"], cap)
+    mask = np.arange(cap)[None, :] < n_l[:, None]
+    return bool(np.array_equal(ta[:, :cap][mask], tb[:, :cap][mask]))
 
 
 def cpu_pairs_baseline(refs, pairs, scoring, seconds, threads=0):
@@ -480,7 +493,8 @@ def run_reference(a, rank, world):
         "data": "synthetic", **extra,
         "config": {"workload": workload, "refs": len(refs)},
         "cpu_baseline": {k: v2 for k, v2 in {**last, "value": v}.items()
-                         if k not in ("seconds", "reads_per_s", "pairs_per_s")},
+                         if k not in ("seconds", "reads_per_s", "pairs_per_s")
+                         and not k.startswith("_")},
         "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -624,13 +638,20 @@ def run_c2(a, ctx, rank):
     tune_rep = tune(g, a)  # tile shape for this panel, before any timing
     info = g.info()
     batch = g.submit(g.prepare(reads.tuple(), both_strands=True))
-    st = g.finish(batch, keep=True).stats
+    first = g.finish(batch, keep=True)
+    st = first.stats
     cells = st["cells"]
     sampler = ClockSampler(local_rank)
     t = ctx.device_time(g, batch, a.steps, a.warmup, sampler)
     clocks = sampler.summary()
     t_max = ctx.max_over_ranks(t)
     value = world * cells * a.steps / t_max / 1e9
+    # the timed launches' results (the last one's, in device memory) against
+    # the submit's, every read
+    timed_res, timed_ties = g.read_results(batch)
+    parity = {"reads": len(reads),
+              "timed_launch_equals_submit": same_results(timed_res, timed_ties, first.results,
+                                                         first.ties)}
     peak = int_peak(local_rank)
     roofline = roofline_of(peak, cells * a.steps / t, mode,
                            K2_DRAM_BYTES_PER_CELL * cells if K2_DRAM_BYTES_PER_CELL else None)
@@ -691,6 +712,13 @@ def run_c2(a, ctx, rank):
         cpu = cpu_baseline(refs, reads, scoring, mode, a.cpu_seconds)
         extras["cpu_reads_per_s"] = cpu.pop("reads_per_s")
         cpu.pop("seconds", None)
+        # the CPU path's results on its sample (the first reads of the
+        # workload) against the GPU's for the same reads
+        c_res, c_ties = cpu.pop("_results")
+        n = len(c_res)
+        parity["cpu_sample_reads"] = n
+        parity["cpu_sample_equal"] = same_results(first.results[:n], first.ties[:n], c_res,
+                                                  c_ties)
     if rank == 0:
         line = common_line(
             a, ctx, value, 1e3 * t_max / a.steps,
@@ -706,6 +734,7 @@ def run_c2(a, ctx, rank):
         line["autotune"] = tune_rep
         line["batch_stats"] = {k: st[k] for k in ("queries_batched", "queries_plain",
                                                   "queries_rescored", "tasks", "lanes_used")}
+        line["parity"] = parity
         if cpu:
             line["cpu_baseline"] = cpu
         line.update(extras)
@@ -869,6 +898,7 @@ def run_c3(a, ctx, rank):
         cpu = cpu_baseline(refs, reads, C3_SCORING, "local", a.cpu_seconds, chunk=1)
         cpu.pop("seconds", None)
         cpu.pop("reads_per_s", None)
+        cpu.pop("_results", None)
     if rank == 0:
         line = common_line(
             a, ctx, value, 1e3 * t_max / a.steps,
@@ -1004,6 +1034,7 @@ def run_c5(a, ctx, rank):
         cpu = cpu_baseline(panels["B"], pools["B"], scoring, "local", a.cpu_seconds)
         cpu.pop("seconds", None)
         cpu.pop("reads_per_s", None)
+        cpu.pop("_results", None)
         cpu["sample"] = "panel B (2000 x 300 nt) reads: " + cpu["sample"]
     if rank == 0:
         line = common_line(

@@ -1361,6 +1361,22 @@ esg_status esg_relaunch(esg_scorer* sc, esg_batch* b, void* stream) {
   return launch_device_work(sc, b, st);
 }
 
+esg_status esg_batch_read_results(esg_scorer* sc, esg_batch* b, esg_read_result* results,
+                                  uint32_t* ties) {
+  g_err.clear();
+  if (!sc || !b || b->owner != sc || !b->submitted || !results)
+    return fail(ESG_ERR_BAD_ARGUMENT, "read_results needs a submitted batch of this scorer");
+  ESG_CUDA(cudaSetDevice(sc->device));
+  ESG_CUDA(cudaDeviceSynchronize());
+  if (b->n_reads) {
+    ESG_CUDA(cudaMemcpy(results, b->d_results, (size_t)b->n_reads * 16, cudaMemcpyDeviceToHost));
+    if (ties)
+      ESG_CUDA(cudaMemcpy(ties, b->d_ties, (size_t)b->n_reads * sc->cap * 4,
+                          cudaMemcpyDeviceToHost));
+  }
+  return ESG_OK;
+}
+
 esg_status esg_finish(esg_scorer* sc, esg_batch* b, esg_read_result* results, uint32_t* ties,
                       int32_t* rows) {
   g_err.clear();

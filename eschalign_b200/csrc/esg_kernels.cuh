@@ -39,7 +39,7 @@ constexpr int kMaxStripes = 32;       // a query spans at most one warp (k2)
 constexpr int kNeg16 = -31500;        // int16 stand-in for -infinity (biased domain)
 constexpr int kBiasLocal = 2048;      // local: H + B >= B >= |o|, |e|
 constexpr int kBiasSemiGlobal = -16384;  // semi-global: H + B < 0 while |H| < 12000
-constexpr int kNeg32 = -(1 << 29);    // int32 stand-in (cuda/kernel.rs:64)
+constexpr int kNeg32 = -(1 << 29);    // int32 stand-in for -infinity, i32::MIN / 4 (scalar.rs:42)
 // k2 CTA shape: 4 warps, 4 resident CTAs per SM (16 warps, <= 128
 // registers; 3 for 32-row stripes).  Tuning knobs, each measured on B200 on
 // the C2 workload (1 M reads of ~110 nt x 164 references, both strands):
@@ -229,7 +229,8 @@ struct K2Params {
 };
 
 // Bounded wait on an mbarrier phase (a TMA bulk copy's completion).  Gives
-// up after ~2^26 polls, setting an error bit the host reads.
+// up after ~2^26 polls, setting an error bit the host reads (when `err` is
+// given).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_t* err) {
   const uint32_t addr = (uint32_t)__cvta_generic_to_shared(bar);
   for (uint32_t it = 0; it < (1u << 26); ++it) {
@@ -243,7 +244,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_
         : "memory");
     if (done) return true;
   }
-  atomicOr(err, kErrPanelWait);
+  if (err) atomicOr(err, kErrPanelWait);
   return false;
 }
 
@@ -274,8 +275,16 @@ __device__ __forceinline__ bool stage_panel(void* smem, const void* gsrc, uint32
     }
   }
   const bool ok = mbar_wait(bar, 0, err);
-  __syncthreads();
-  return ok;
+  // One decision for the whole CTA: a thread that gave up and one that saw
+  // the phase flip must not part ways (the survivors' warp-wide shuffles
+  // would then run with exited lanes).
+  const bool all_ok = __syncthreads_and(ok) != 0;
+  if (!all_ok && threadIdx.x == 0) {
+    // give the copies in flight one more bounded wait before the CTA's
+    // shared memory is released
+    mbar_wait(bar, 0, nullptr);
+  }
+  return all_ok;
 }
 
 // One systolic pass of a warp over the columns of one reference pair.

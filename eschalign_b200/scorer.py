@@ -448,6 +448,16 @@ class GpuScorer:
     def relaunch(self, batch: PendingBatch, stream: int | None = None):
         _check(self._lib, self._lib.esg_relaunch(self._h, batch._h, stream))
 
+    def read_results(self, batch: PendingBatch):
+        """The batch's per-read results and ties as they stand in device
+        memory now (after :meth:`relaunch`, the last launch's)."""
+        n = batch.n_reads
+        res = np.zeros(n, dtype=RESULT_DTYPE)
+        ties = np.zeros((n, self.cap), dtype=np.uint32)
+        _check(self._lib, self._lib.esg_batch_read_results(self._h, batch._h, res.ctypes.data,
+                                                           _ptr(ties, C.c_uint32)))
+        return res, ties
+
     def finish(self, batch: PendingBatch, keep: bool = False) -> BatchResult:
         n = batch.n_reads
         res = np.zeros(n, dtype=RESULT_DTYPE)

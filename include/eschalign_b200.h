@@ -229,6 +229,13 @@ esg_status esg_batch_stats_get(const esg_batch* batch, esg_batch_stats* out);
  * scorer's) with its inputs already resident, no copies.  For measuring the
  * kernels alone; the batch's results are overwritten with identical ones. */
 esg_status esg_relaunch(esg_scorer* scorer, esg_batch* batch, void* stream);
+/* Copy a submitted batch's per-read results and ties as they stand in device
+ * memory now -- after esg_relaunch, the last launch's -- into the caller's
+ * buffers (ties may be NULL), after the device has finished its work.  No
+ * counterpart in the reference: it checks that relaunched work, the work a
+ * benchmark times, gives the results esg_finish returned. */
+esg_status esg_batch_read_results(esg_scorer* scorer, esg_batch* batch, esg_read_result* results,
+                                  uint32_t* ties);
 
 /* ---- paired-end: the scored half of Aligner::map_pairs_scored
  * (crates/eschalign/src/mapper/pair.rs:157-234) fed the way the CLI's GPU

@@ -1,0 +1,90 @@
+"""Parity at the sizes that are timed.
+
+The reference's own harness compares every pair it scores
+(crates/eschalign/tests/gpu_parity.rs:151-192).  Here the whole C2 workload
+-- all 1 000 000 reads, both strands, against the 164-reference panel -- is
+scored on the GPU and every read's best score, XS, tie count and tie list is
+compared with the reference's CPU path (the AVX-512BW restatement with its
+scalar fallback, itself equal to the scalar oracle by test), for the
+headline local scheme and for semi-global.  The uneven C3 panel (10 000
+references of 300-1000 nt, read through L2 in panel chunks) gets a sample of
+its reads on both strands, and a large-score scheme on a slice of it that
+drives long reads past int16 so the re-score path runs at that shape."""
+import numpy as np
+import pytest
+
+from eschalign_b200 import GpuScorer, Mode, Scoring, synth
+
+pytestmark = pytest.mark.gpu
+
+CAP = 8
+
+
+@pytest.fixture(scope="module")
+def c2():
+    refs = synth.panel_tiles()
+    return refs, synth.reads_c2(refs, n=1_000_000)
+
+
+@pytest.fixture(scope="module")
+def c3_panel():
+    return synth.panel_c3()
+
+
+def assert_same(got, got_ties, want, want_ties, cap, what):
+    for f in ("best", "suboptimal", "n_tied"):
+        bad = np.nonzero(got[f] != want[f])[0]
+        assert bad.size == 0, (f"{what}: {f} differs on {bad.size} reads, first read "
+                               f"{bad[0]}: got {got[f][bad[0]]} want {want[f][bad[0]]}")
+    assert ((got["flags"] & 3) == (want["flags"] & 3)).all(), what
+    n_l = np.minimum(want["n_tied"], cap)
+    mask = np.arange(cap)[None, :] < n_l[:, None]
+    bad = np.nonzero((got_ties != want_ties) & mask)[0]
+    assert bad.size == 0, f"{what}: tie lists differ on {np.unique(bad).size} reads"
+
+
+@pytest.mark.parametrize("mode", [Mode.LOCAL, Mode.SEMIGLOBAL])
+def test_gpu_c2_every_read_equals_cpu_path(oracle, c2, mode):
+    """All 1 000 000 C2 reads, both strands, 2,-1,-10,-1: the GPU's per-read
+    results equal the CPU path's, read for read."""
+    refs, reads = c2
+    local = mode == Mode.LOCAL
+    scoring = (2, -1, -10, -1)
+    with GpuScorer(refs, Scoring(*scoring), mode) as g:
+        g.autotune()
+        res = g.score_batch(reads.tuple(), both_strands=True)
+    assert res.stats["queries_batched"] == 2 * len(reads)
+    want, want_t, _, _ = oracle.Profile(refs, scoring).map_batch(
+        *reads.tuple(), local=local, both_strands=True, cap=CAP)
+    assert_same(res.results, res.ties, want, want_t, CAP, f"C2 1M {mode.label}")
+
+
+def test_gpu_c3_sample_on_the_full_panel(oracle, c3_panel):
+    """200 C3 reads (50-1000 nt) against all 10 000 references, local
+    2,-1,-10,-1, both strands: the panel is read through L2 and a small
+    batch is cut into panel chunks whose states are merged."""
+    refs = c3_panel
+    reads = synth.reads_c3(refs, n=200)
+    scoring = (2, -1, -10, -1)
+    with GpuScorer(refs, Scoring(*scoring), Mode.LOCAL) as g:
+        info = g.info()
+        res = g.score_batch(reads.tuple(), both_strands=True)
+    assert info["panel_bytes"] == 0  # too large for shared memory
+    assert res.stats["panel_chunks"] > 1
+    want, want_t, _, _ = oracle.Profile(refs, scoring).map_batch(
+        *reads.tuple(), local=True, both_strands=True, cap=CAP)
+    assert_same(res.results, res.ties, want, want_t, CAP, "C3 sample")
+
+
+def test_gpu_c3_shape_saturating_scheme(oracle, c3_panel):
+    """The C3 shape with a scheme whose long exact matches leave int16
+    (100,-100,-27,-27: a 500-nt match scores 50 000): flagged queries are
+    re-scored in int32 and every result equals the scalar oracle's."""
+    refs = c3_panel[:400]
+    reads = synth.reads_c3(refs, n=24, seed=0x5EED_0C3F)
+    scoring = (100, -100, -27, -27)
+    with GpuScorer(refs, Scoring(*scoring), Mode.LOCAL) as g:
+        res = g.score_batch(reads.tuple(), both_strands=True)
+    assert res.stats["queries_rescored"] > 0
+    want, want_t, _ = oracle.scalar_map_batch(reads.list(), refs, scoring, True, True, cap=CAP)
+    assert_same(res.results, res.ties, want, want_t, CAP, "C3 saturating")
