@@ -45,7 +45,18 @@ def build() -> str:
     return LIB_PATH
 
 
-REF_ROOT = "/root/reference"
+def reference_root():
+    """The reference checkout, where this machine has one: the directory
+    named by ESCHALIGN_REFERENCE, else a `reference` directory beside this
+    repository; None when neither exists (on a GPU box the built files
+    travel instead)."""
+    for cand in (os.environ.get("ESCHALIGN_REFERENCE"),
+                 os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")):
+        if cand and os.path.isdir(os.path.join(cand, "crates", "eschalign")):
+            return cand
+    return None
+
+
 REF_GPU_LIB = os.path.join(HERE, "_ref", "libref_gpu.so")
 REF_GPU_CUBIN = os.path.join(HERE, "_ref", "ref_kernels.cubin")
 
@@ -53,9 +64,10 @@ REF_GPU_CUBIN = os.path.join(HERE, "_ref", "ref_kernels.cubin")
 def build_ref_gpu() -> bool:
     """Compile the reference's own GPU kernels (comparison arms) when its
     tree is present here; elsewhere whatever was built travels as files."""
-    if not os.path.isdir(REF_ROOT):
+    root = reference_root()
+    if root is None:
         return os.path.exists(REF_GPU_LIB) and os.path.exists(REF_GPU_CUBIN)
-    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_ROOT}"], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={root}"], check=True)
     return True
 
 

@@ -40,4 +40,6 @@ def main(root: str) -> str:
 
 
 if __name__ == "__main__":
-    print(main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract.py <reference checkout>")
+    print(main(sys.argv[1]))
