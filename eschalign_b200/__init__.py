@@ -11,14 +11,14 @@ from . import adapter
 from ._native import build, load
 from .alphabet import WILDCARD, encode, reverse_complement_codes
 from .panel import Panel, PanelError, read_fasta
-from .scorer import (BOTH_STRANDS, FULL_ROWS, KERNEL_AUTO, KERNEL_PLAIN32, NO_SCORE,
+from .scorer import (BOTH_STRANDS, FULL_ROWS, KERNEL_AUTO, KERNEL_INT32, KERNEL_PLAIN32, NO_SCORE,
                      BatchResult, GpuError, GpuScorer, PairBatchResult, PairScores, ReadScores,
                      ScoreMatrix, device_visible, fits_i16, pack_reads, select_hits)
 from .scoring import Mode, Scoring, ScoringError
 
 __all__ = [
     "adapter", "build", "load", "WILDCARD", "encode", "reverse_complement_codes", "Panel", "PanelError",
-    "read_fasta", "BOTH_STRANDS", "FULL_ROWS", "KERNEL_AUTO", "KERNEL_PLAIN32", "NO_SCORE",
+    "read_fasta", "BOTH_STRANDS", "FULL_ROWS", "KERNEL_AUTO", "KERNEL_INT32", "KERNEL_PLAIN32", "NO_SCORE",
     "BatchResult", "GpuError", "GpuScorer", "PairBatchResult", "PairScores", "ReadScores", "ScoreMatrix", "device_visible",
     "fits_i16", "pack_reads", "select_hits", "Mode", "Scoring", "ScoringError",
 ]

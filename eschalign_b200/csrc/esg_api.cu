@@ -52,6 +52,8 @@ esg_status cuda_fail(cudaError_t e, const char* what) {
   } while (0)
 
 constexpr uint32_t kMaxRefLen = 32768;
+// device memory k3's column buffers may take (per scorer and arm)
+constexpr size_t kColbufBudget = (size_t)1 << 30;
 constexpr int kPad = 5;     // selector / table index of a padding column or row
 constexpr int kWild = 4;
 
@@ -146,8 +148,13 @@ struct esg_scorer {
   std::vector<uint32_t> len_of;    // reference lengths, panel order
   std::vector<uint8_t> h_codes;    // the panel's codes (0-4), panel order (host)
   std::vector<uint64_t> h_off;     // reference r at h_codes[h_off[r]]
-  int2* d_scratch = nullptr;
-  int k3_blocks = 0;
+  // k3's column buffers (a chain's bottom row between passes): per warp
+  // max_ref_len int2 for the int32 lanes, 32x that for one thread per pair
+  // (32 chains a warp), made when that arm is first chosen
+  int2* d_colbuf = nullptr;
+  int2* d_colbuf1 = nullptr;
+  int k3_blocks = 0;   // CTAs of k3 (int32 lanes)
+  int k3_blocks1 = 0;  // CTAs of k3 as one thread per pair (bounded by its buffer)
   const void* k3_fn = nullptr;
   PinnedPool pinned;
   esg_info info{};
@@ -282,7 +289,7 @@ void set_k2_fn(esg_scorer* sc) {
   sc->k2_t16 = pick_k2<16, false>(local, sc->panel_w, sc->smem_panel);
   sc->k2_t32 = pick_k2<32, false>(local, sc->panel_w, sc->smem_panel);
   sc->k2_long = pick_k2<32, true>(local, sc->panel_w, sc->smem_panel);
-  sc->k3_fn = local ? (const void*)k3_plain<true> : (const void*)k3_plain<false>;
+  sc->k3_fn = local ? (const void*)k3_lanes<true> : (const void*)k3_lanes<false>;
 }
 
 // 32-lane tiles of query stripes: best-fit decreasing.  `qs` holds
@@ -350,6 +357,20 @@ void pack_tiles(std::vector<std::pair<uint32_t, uint32_t>>& qs, TilePlan& out) {
 }
 
 }  // namespace
+
+// The one-thread-per-pair arm's column buffers: 32 chains a warp, each a
+// reference's bottom row per column; the grid shrinks to what kColbufBudget
+// holds.  Made once, on first use.
+static esg_status make_plain_buffers(esg_scorer* sc) {
+  if (sc->d_colbuf1) return ESG_OK;
+  const size_t per_block = (size_t)kK3Warps * 32 * sc->max_ref_len * sizeof(int2);
+  const int blocks = (int)std::max<size_t>(
+      1, std::min<size_t>((size_t)sc->k3_blocks, kColbufBudget / per_block));
+  const cudaError_t e = cudaMalloc(&sc->d_colbuf1, (size_t)blocks * per_block);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(one-thread-per-pair column buffers)");
+  sc->k3_blocks1 = blocks;
+  return ESG_OK;
+}
 
 // ===================================================================== API
 
@@ -450,7 +471,7 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
   }
   if (cap < 1 || cap > ESG_MAX_TIE_CAPACITY)
     return fail(ESG_ERR_BAD_ARGUMENT, "tie_capacity %u outside 1..%d", cap, ESG_MAX_TIE_CAPACITY);
-  if (kernel != ESG_KERNEL_AUTO && kernel != ESG_KERNEL_PLAIN32)
+  if (kernel != ESG_KERNEL_AUTO && kernel != ESG_KERNEL_PLAIN32 && kernel != ESG_KERNEL_INT32)
     return fail(ESG_ERR_BAD_ARGUMENT, "unknown kernel %d", kernel);
 
   int ndev = 0;
@@ -642,14 +663,22 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
       return cleanup(cuda_fail(e, "cudaMalloc(long-query buffer)"));
   }
   sc->k3_blocks = std::max(1, occ3) * sc->sm_count;
-  // k3's stripe boundary: one int2 per reference column per thread, at most 2 GiB
-  const size_t per_thread = (size_t)max_len * sizeof(int2);
-  const size_t budget = (size_t)2 << 30;
-  while ((size_t)sc->k3_blocks * kK3Threads * per_thread > budget && sc->k3_blocks > 1)
-    sc->k3_blocks /= 2;
-  if ((e = cudaMalloc(&sc->d_scratch, (size_t)sc->k3_blocks * kK3Threads * per_thread)) !=
-      cudaSuccess)
-    return cleanup(cuda_fail(e, "cudaMalloc(k3 scratch)"));
+  // k3's column buffers: one reference's bottom row (G, F per column) per
+  // warp, at most kColbufBudget
+  {
+    const size_t per_block = (size_t)kK3Warps * max_len * sizeof(int2);
+    sc->k3_blocks = (int)std::max<size_t>(
+        1, std::min<size_t>((size_t)sc->k3_blocks, kColbufBudget / per_block));
+    if ((e = cudaMalloc(&sc->d_colbuf, (size_t)sc->k3_blocks * per_block)) != cudaSuccess)
+      return cleanup(cuda_fail(e, "cudaMalloc(k3 column buffers)"));
+  }
+  if (kernel == ESG_KERNEL_PLAIN32) {
+    const esg_status pst = make_plain_buffers(sc);
+    if (pst != ESG_OK) {
+      esg_scorer_free(sc);
+      return pst;
+    }
+  }
 
   // --- info
   esg_info& inf = sc->info;
@@ -689,7 +718,8 @@ void esg_scorer_free(esg_scorer* sc) {
   cudaFree(sc->d_roff);
   cudaFree(sc->d_rlen);
   cudaFree(sc->d_ridx);
-  cudaFree(sc->d_scratch);
+  cudaFree(sc->d_colbuf);
+  cudaFree(sc->d_colbuf1);
   cudaFree(sc->d_lbuf);
   if (sc->aux) {
     cudaStreamSynchronize(sc->aux);
@@ -709,9 +739,15 @@ esg_status esg_scorer_info(const esg_scorer* sc, esg_info* out) {
 }
 
 esg_status esg_scorer_set_kernel(esg_scorer* sc, int32_t kernel) {
+  g_err.clear();
   if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");
-  if (kernel != ESG_KERNEL_AUTO && kernel != ESG_KERNEL_PLAIN32)
+  if (kernel != ESG_KERNEL_AUTO && kernel != ESG_KERNEL_PLAIN32 && kernel != ESG_KERNEL_INT32)
     return fail(ESG_ERR_BAD_ARGUMENT, "unknown kernel %d", kernel);
+  if (kernel == ESG_KERNEL_PLAIN32) {
+    ESG_CUDA(cudaSetDevice(sc->device));
+    const esg_status st = make_plain_buffers(sc);
+    if (st != ESG_OK) return st;
+  }
   sc->kernel = kernel;
   return ESG_OK;
 }
@@ -1195,30 +1231,38 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
   }
   const bool k3 = b->host_list + b->redo_cap > 0;
   if (k3) {
+    const bool plain = b->kernel == ESG_KERNEL_PLAIN32;
     K3Params P{};
     P.codes = b->d_codes;
     P.off = b->d_off;
     P.len = b->d_len;
     P.n_reads = b->n_reads;
+    P.list = b->d_list;
+    P.host_count = b->host_list;
+    P.redo_count = b->redo_cap ? b->d_counters + 1 : nullptr;
+    P.redo_cap = b->redo_cap;
     P.rcodes = sc->d_rcodes;
     P.roff = sc->d_roff;
     P.rlen = sc->d_rlen;
     P.ridx = sc->d_ridx;
     P.n_refs = sc->n_refs;
-    P.list = b->d_list;
-    P.host_count = b->host_list;
-    P.redo_count = b->redo_cap ? b->d_counters + 1 : nullptr;
-    P.redo_cap = b->redo_cap;
+    P.max_cols = sc->max_ref_len;
     P.out = b->d_k3out;
     P.rows = rows ? b->d_rows : nullptr;
-    P.scratch = sc->d_scratch;
+    P.wmax = plain ? 1u : 32u;
+    P.refs_per_task = 32;
+    // counters[6..7]: the units' 64-bit counter (8-byte aligned, reset with
+    // the rest each launch)
+    P.task_counter = reinterpret_cast<unsigned long long*>(b->d_counters + 6);
+    P.colbuf = plain ? sc->d_colbuf1 : sc->d_colbuf;
     P.ma = sc->scoring.match_score;
     P.mi = sc->scoring.mismatch;
     P.o = sc->scoring.gap_open;
     P.e = sc->scoring.gap_extend;
-    P.local = sc->mode == ESG_MODE_LOCAL;
+    P.one = 1;
     void* args[] = {&P};
-    ESG_CUDA(cudaLaunchKernel(sc->k3_fn, dim3(sc->k3_blocks), dim3(kK3Threads), args, 0, st));
+    ESG_CUDA(cudaLaunchKernel(sc->k3_fn, dim3(plain ? sc->k3_blocks1 : sc->k3_blocks),
+                              dim3(kK3Threads), args, 0, st));
     ++kernels;
     K4Params Q{};
     Q.list = b->d_list;

@@ -18,10 +18,12 @@
 //                query, online, in shared memory.
 //                Pairs that may have left int16 are flagged and their query
 //                is re-scored by the int32 kernel.
-//   k3_plain     one thread per (query, reference), int32, the recurrence of
-//                crates/eschalign/src/scalar.rs:120-163 over 16-row register
-//                stripes with the stripe boundary in global scratch.  The
-//                comparison arm, and the exact path for what k2 cannot take.
+//   k3_lanes     the exact int32 path: the recurrence of
+//                crates/eschalign/src/scalar.rs:120-163 on chains of lanes
+//                (16-row stripes, bottom rows passed by shuffle, several
+//                references a warp for short queries); what k2 cannot take
+//                or flags.  With one lane a chain it is the one-thread-per-
+//                pair comparison arm.
 //   k4_rows      per-query reduction of k3's rows (mapper.rs:444-472).
 //   k5_merge     per read: forward and reverse-complement query states
 //                merged into the read's result.
@@ -85,7 +87,6 @@ constexpr int kNeg32 = -(1 << 29);    // int32 stand-in for -infinity, i32::MIN 
 #endif
 constexpr int kK2Warps = ESG_K2_WARPS;  // warps per k2 CTA
 constexpr int kK2Threads = kK2Warps * 32;
-constexpr int kK3Threads = 256;
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kNoRef = 0xffffffffu;
 constexpr uint32_t kMaxCap = 32;       // largest tie capacity (ESG_MAX_TIE_CAPACITY)
@@ -877,128 +878,244 @@ static __global__ void __launch_bounds__(128) k2_merge_chunks(const KMParams P) 
 }
 
 // ---------------------------------------------------------------- k3
+// k3_lanes: the exact int32 path.  It scores a list of queries against every
+// reference of the panel and writes the rows (k4 reduces them).  The work
+// unit is (query, a run of references); one warp takes one unit at a time.
+//
+// Lanes hold 16-row stripes of the query.  A query of S stripes is scored
+// against a reference by a chain of W = min(S, wmax) lanes: the lane at
+// position w of the chain holds stripes w, W + w, 2W + w, ... in successive
+// passes, walks the reference's columns one per step, lagging the lane
+// before it by one step, and takes its top input (G and F of the row above)
+// from that lane by shuffle.  The chain's first lane takes the zero border
+// in the first pass and, in later passes, the bottom row the chain's last
+// lane left in the warp's column buffer (global memory) in the pass before.
+// A warp runs 32 / W chains side by side, one reference each, so short
+// queries fill the warp with references instead of idle lanes.  wmax = 32 is
+// the product setting; wmax = 1 makes every lane a chain of its own -- one
+// thread per (query, reference) pair, the stripes' bottom row through the
+// buffer -- the plain comparison arm.
+//
+// Per cell: G = H + o is kept instead of H, so E, F and the diagonal term
+// are one VIADDMNMX each (max(X + e, G) and max(G_diag + (s - o), E)), H one
+// VIMNMX3 (with the zero floor in local mode), G one IMAD on the FMA pipe;
+// the substitution s - o comes from the lane's per-column record in shared
+// memory (word c = the score of read code c against this column, one
+// 16-byte table load and four stores per column), one load per cell.  The
+// query is padded at the top to whole stripes with rows that score 0, which
+// hold H = 0 exactly -- the top border -- and are left out of the
+// semi-global last-column maximum.
+constexpr int kK3Rows = 16;
+constexpr int kK3Warps = 4;
+constexpr int kK3Threads = kK3Warps * 32;
+constexpr uint32_t kK3Stride = (uint32_t)kK3Threads * 4;  // bytes between record words
+
 struct K3Params {
+  // queries: list entry p is query list[p] (q < n_reads: read q forward,
+  // else the reverse complement of read q - n_reads); without a list, entry
+  // p is read p forward
   const uint8_t* codes;
   const uint64_t* off;
   const uint32_t* len;
   uint32_t n_reads;
-  // references in longest-first order: slot k is panel reference ridx[k]
+  const uint32_t* list;
+  uint32_t host_count;         // entries listed by the host
+  const uint32_t* redo_count;  // device count of entries after them (may be null)
+  uint32_t redo_cap;           // capacity after host_count
+  // references: slot k is panel reference ridx[k] (identity without ridx)
   const uint8_t* rcodes;
   const uint32_t* roff;
   const uint32_t* rlen;
   const uint32_t* ridx;
   uint32_t n_refs;
-  const uint32_t* list;        // queries to score
-  uint32_t host_count;
-  const uint32_t* redo_count;  // device count of entries after host_count (may be null)
-  uint32_t redo_cap;           // list capacity after host_count
-  int32_t* out;                // [pos * n_refs + r], panel order
-  int32_t* rows;               // optional [q * n_refs + r]
-  int2* scratch;               // stripe boundary, [col * threads + tid]
+  uint32_t max_cols;           // longer references score kNoScore (no room in colbuf)
+  int32_t* out;                // [p * n_refs + ref] (may be null)
+  int32_t* rows;               // [q * n_refs + ref] (may be null)
+  uint32_t wmax;               // lanes per chain at most: 32, or 1 (one thread per pair)
+  uint32_t refs_per_task;
+  unsigned long long* task_counter;  // null: units taken warp-strided
+  int2* colbuf;                // per warp (32 / wmax) * max_cols int2
   int32_t ma, mi, o, e;
-  int local;
+  int32_t one;                 // 1, opaque to the compiler (keeps G's add an IMAD)
 };
 
-__device__ __forceinline__ uint32_t code_mask(uint32_t c) { return c < 4 ? 1u << c : 0xfu; }
-
-template <bool kLocal, bool kTail>
-__device__ __forceinline__ void k3_stripe(const uint8_t* __restrict__ rc_codes, int m,
-                                          const uint32_t (&qm)[kRows], int rows, bool first,
-                                          int2* __restrict__ bnd, size_t bstride, int ma, int mi,
-                                          int o, int e, int& best) {
-  int H[kRows], E[kRows];
-#pragma unroll
-  for (int r = 0; r < kRows; ++r) {
-    H[r] = 0;
-    E[r] = kNeg32;
-  }
-  int diag_top = 0;
-  for (int j = 0; j < m; ++j) {
-    const uint32_t rm = code_mask(__ldg(rc_codes + j));
-    int hup, f;
-    if (first) {
-      hup = 0;
-      f = kNeg32;
-    } else {
-      const int2 b = bnd[(size_t)j * bstride];
-      hup = b.x;
-      f = b.y;
-    }
-    int hdiag = diag_top;
-    diag_top = hup;
-    int last = kNeg32;
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-      const int hleft = H[r];
-      const int ev = max(hleft + o, E[r] + e);
-      E[r] = ev;
-      f = max(hup + o, f + e);
-      const int sc = (qm[r] & rm) ? ma : mi;
-      int h = max(max(hdiag + sc, ev), f);
-      if (kLocal) h = max(h, 0);
-      hdiag = hleft;
-      H[r] = h;
-      hup = h;
-      if (kLocal) {
-        if (!kTail || r < rows) best = max(best, h);
-      } else if (kTail) {
-        if (r == rows - 1) last = h;
-      }
-    }
-    if (!kTail) bnd[(size_t)j * bstride] = make_int2(hup, f);
-    if (!kLocal && kTail) best = max(best, last);
-  }
-  if (!kLocal) {
-#pragma unroll
-    for (int r = 0; r < kRows; ++r)
-      if (!kTail || r < rows) best = max(best, H[r]);
-  }
-}
+constexpr int32_t kNoScore = INT32_MIN;
 
 template <bool kLocal>
-__global__ void __launch_bounds__(kK3Threads) k3_plain(const K3Params P) {
-  const uint32_t n_list = P.host_count + (P.redo_count ? min(*P.redo_count, P.redo_cap) : 0u);
-  const uint64_t total = (uint64_t)n_list * P.n_refs;
-  const size_t nthreads = (size_t)gridDim.x * blockDim.x;
-  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int2* bnd = P.scratch + tid;
-  for (uint64_t idx = tid; idx < total; idx += nthreads) {
-    const uint32_t pos = (uint32_t)(idx / P.n_refs);
-    const uint32_t k = (uint32_t)(idx % P.n_refs);
-    const uint32_t q = P.list[pos];
+__global__ void __launch_bounds__(kK3Threads, 4) k3_lanes(const K3Params P) {
+  constexpr int R = kK3Rows;
+  __shared__ int4 tab[5];                      // words of read codes 0-3 against reference code x
+  __shared__ uint32_t rec[6 * kK3Threads];     // word c of thread t at c * kK3Threads + t
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int o = P.o, e = P.e;
+  const int mao = P.ma - o, mio = P.mi - o;
+  if (threadIdx.x < 5) {
+    const int x = threadIdx.x;  // 4: a wildcard reference base matches every read code
+    tab[x] = make_int4((x == 0 || x == 4) ? mao : mio, (x == 1 || x == 4) ? mao : mio,
+                       (x == 2 || x == 4) ? mao : mio, (x == 3 || x == 4) ? mao : mio);
+  }
+  const uint32_t my = (uint32_t)__cvta_generic_to_shared(rec) + threadIdx.x * 4u;
+  st_shared_u32(my + 4 * kK3Stride, (uint32_t)mao);  // read wildcard: a match everywhere
+  st_shared_u32(my + 5 * kK3Stride, (uint32_t)-o);   // padding row: s = 0
+  __syncthreads();
+
+  const uint32_t n_list =
+      P.host_count + (P.redo_count ? min(*P.redo_count, P.redo_cap) : 0u);
+  const uint32_t tpq = (P.n_refs + P.refs_per_task - 1) / P.refs_per_task;
+  const unsigned long long n_units = (unsigned long long)n_list * tpq;
+  const size_t warp_id = (size_t)blockIdx.x * kK3Warps + wib;
+  const size_t n_warps = (size_t)gridDim.x * kK3Warps;
+  const int cmax = 32 / (int)P.wmax;
+  int2* const buf = P.colbuf ? P.colbuf + warp_id * (size_t)cmax * P.max_cols : nullptr;
+
+  unsigned long long unit = warp_id;
+  for (;; unit += P.task_counter ? 0ull : n_warps) {
+    if (P.task_counter) {
+      unsigned long long u = 0;
+      if (lane == 0) u = atomicAdd(P.task_counter, 1ull);
+      unit = __shfl_sync(kFull, u, 0);
+    }
+    if (unit >= n_units) break;
+    const uint32_t pos = (uint32_t)(unit / tpq);
+    const uint32_t k_lo = (uint32_t)(unit - (unsigned long long)pos * tpq) * P.refs_per_task;
+    const uint32_t k_hi = min(k_lo + P.refs_per_task, P.n_refs);
+    const uint32_t q = P.list ? P.list[pos] : pos;
     const bool rc = q >= P.n_reads;
     const uint32_t rd = rc ? q - P.n_reads : q;
     const int n = (int)P.len[rd];
     const uint8_t* qc = P.codes + P.off[rd];
-    const int m = (int)P.rlen[k];
-    const uint8_t* rcodes = P.rcodes + P.roff[k];
-    int best = kLocal ? 0 : kNeg32;
-    for (int i0 = 0; i0 < n; i0 += kRows) {
-      uint32_t qm[kRows];
+
+    const int S = n > 0 ? (n + R - 1) / R : 1;
+    const int W = min(S, (int)P.wmax);
+    const int C = 32 / W;                // chains in the warp
+    const int passes = (S + W - 1) / W;
+    const int c = lane / W, w = lane - c * W;
+    const int pad = S * R - n;
+
+    for (uint32_t k0 = k_lo; k0 < k_hi; k0 += (uint32_t)C) {
+      const uint32_t k = k0 + (uint32_t)c;
+      const bool has = c < C && k < k_hi;
+      const uint32_t mref = has ? P.rlen[k] : 0u;
+      // (a reference longer than the column buffer's rows, or a query that
+      // needs passes without a buffer, is not scored)
+      const bool fits = mref <= P.max_cols && (passes == 1 || buf != nullptr);
+      const int m = (fits && n > 0) ? (int)mref : 0;
+      const int M = (int)__reduce_max_sync(kFull, (unsigned)m);
+      const uint8_t* rcs = has ? P.rcodes + P.roff[k] : P.rcodes;
+      // local: the best H over the chain's cells; semi-global: the best of
+      // the last column and (on the lane of the last stripe) the last row
+      int acc = kLocal ? 0 : kNeg32;
+      for (int pass = 0; pass < passes; ++pass) {
+        const int s = pass * W + w;
+        const bool valid = m > 0 && s < S;
+        uint32_t addr[R];
 #pragma unroll
-      for (int r = 0; r < kRows; ++r) {
-        const int i = i0 + r;
-        uint32_t c = 0xffu;
-        if (i < n) {
-          uint32_t x = rc ? qc[n - 1 - i] : qc[i];
-          x = x > 4 ? 4 : x;
-          c = (rc && x < 4) ? 3 - x : x;
+        for (int r = 0; r < R; ++r) {
+          const int i = s * R + r - pad;
+          uint32_t code = 5;  // padding row
+          if (valid && i >= 0) {
+            uint32_t x = rc ? qc[n - 1 - i] : qc[i];
+            x = x > 4 ? 4 : x;
+            code = (rc && x < 4) ? 3 - x : x;
+          }
+          addr[r] = my + code * kK3Stride;
         }
-        qm[r] = c == 0xffu ? 0u : code_mask(c);
+        const uint32_t padmask = (valid && s == 0) ? ((1u << pad) - 1u) : 0u;
+        const bool from_buf = pass > 0 && w == 0;
+        const bool to_buf = pass + 1 < passes && w == W - 1;
+        int g[R], ev[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          g[r] = o;  // G of a zero border cell
+          ev[r] = kNeg32;
+        }
+        int gdc = o, gbot = o, fbot = kNeg32;
+        int best = kLocal ? 0 : kNeg32;
+        int lastrow = kNeg32, lastcol = kNeg32;
+        const int steps = M + W - 1;
+#pragma unroll 1
+        for (int t = 0; t < steps; ++t) {
+          int gt = __shfl_up_sync(kFull, gbot, 1);
+          int ft = __shfl_up_sync(kFull, fbot, 1);
+          if (w == 0) {
+            gt = o;
+            ft = kNeg32;
+          }
+          const int j = t - w;
+          if (valid && (unsigned)j < (unsigned)m) {
+            if (from_buf) {
+              const int2 b = buf[(size_t)j * C + c];
+              gt = b.x;
+              ft = b.y;
+            }
+            // this column's record: the score (s - o) of read codes 0-3
+            const int x = min((int)rcs[j], 4);
+            const int4 tw = tab[x];
+            st_shared_u32(my, (uint32_t)tw.x);
+            st_shared_u32(my + kK3Stride, (uint32_t)tw.y);
+            st_shared_u32(my + 2 * kK3Stride, (uint32_t)tw.z);
+            st_shared_u32(my + 3 * kK3Stride, (uint32_t)tw.w);
+            int gd = gdc;
+            gdc = gt;
+            int gup = gt, f = ft, hprev = 0, hlast = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int sc = (int)ld_shared_u32(addr[r]);
+              ev[r] = __viaddmax_s32(ev[r], e, g[r]);
+              f = __viaddmax_s32(f, e, gup);
+              const int h1 = __viaddmax_s32(gd, sc, ev[r]);
+              int h;
+              if constexpr (kLocal) {
+                h = __vimax3_s32(h1, f, 0);
+                if (r & 1)
+                  best = __vimax3_s32(best, hprev, h);
+                else
+                  hprev = h;
+              } else {
+                h = max(h1, f);
+              }
+              gd = g[r];
+              g[r] = (int)mad_lo((uint32_t)h, (uint32_t)P.one, (uint32_t)o);
+              gup = g[r];
+              if (r == R - 1) hlast = h;
+            }
+            gbot = g[R - 1];
+            fbot = f;
+            if (to_buf) buf[(size_t)j * C + c] = make_int2(gbot, fbot);
+            if constexpr (!kLocal) {
+              lastrow = max(lastrow, hlast);
+              if (j == m - 1) {
+                int cm = kNeg32;
+#pragma unroll
+                for (int r = 0; r < R; ++r) cm = max(cm, ((padmask >> r) & 1u) ? kNeg32 : g[r]);
+                lastcol = cm - o;
+              }
+            }
+          }
+        }
+        __syncwarp();  // the buffer's writes are seen by the next pass
+        if constexpr (kLocal) {
+          acc = max(acc, best);
+        } else {
+          acc = max(acc, lastcol);
+          if (valid && s == S - 1) acc = max(acc, lastrow);
+        }
       }
-      const int rows = min(kRows, n - i0);
-      const bool first = i0 == 0;
-      if (i0 + kRows >= n)
-        k3_stripe<kLocal, true>(rcodes, m, qm, rows, first, bnd, nthreads, P.ma, P.mi, P.o, P.e,
-                                best);
-      else
-        k3_stripe<kLocal, false>(rcodes, m, qm, rows, first, bnd, nthreads, P.ma, P.mi, P.o,
-                                 P.e, best);
+      // the chain's maximum, to its first lane
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_down_sync(kFull, acc, d);
+        if (w + d < W) acc = max(acc, v);
+      }
+      if (has && w == 0) {
+        // scalar.rs:123-125: an empty query or reference scores 0
+        const int score = !fits ? kNoScore : (m == 0 ? 0 : acc);
+        const uint32_t ref = P.ridx ? P.ridx[k] : k;
+        if (P.out) P.out[(size_t)pos * P.n_refs + ref] = score;
+        if (P.rows) P.rows[(size_t)q * P.n_refs + ref] = score;
+      }
     }
-    if (n == 0) best = 0;
-    const uint32_t ref = P.ridx[k];
-    P.out[(size_t)pos * P.n_refs + ref] = best;
-    if (P.rows) P.rows[(size_t)q * P.n_refs + ref] = best;
   }
 }
 

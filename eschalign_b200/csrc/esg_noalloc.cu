@@ -1,17 +1,23 @@
 // esg_noalloc.cu -- a scoring entry point that allocates no memory.
 //
-// Some callers cannot call cudaMalloc: code running inside a CUDA graph
-// being built by someone else, a host process whose allocator is owned by a
-// framework that forbids side allocations, or a real-time loop that must not
-// touch the driver's allocator after start-up.  esg_score_rows_noalloc
-// serves them: the caller passes device buffers for the inputs and the
-// output, and the only other memory the plain int32 kernel needs -- its
-// stripe-boundary scratch (one int2 per reference column per thread) -- is
-// the file-scope device array below, reserved when the library is loaded.
+// Some callers cannot call cudaMalloc when they need scores: a process whose
+// device memory belongs to a framework's caching allocator, which forbids
+// allocations behind its back (they fragment its pool and escape its
+// budget), or a real-time loop that must not enter the driver's allocator
+// after start-up (cudaMalloc and cudaFree can block and synchronize the
+// device).  esg_score_rows_noalloc serves them: the caller passes device
+// buffers for the inputs and the output, and the one other buffer the int32
+// kernel needs -- the column buffer that carries a reference's bottom row
+// from one pass of a long query to the next (max_ref_len int2 per warp) --
+// is the file-scope device array below.
 //
-// That array is host-side a stand-in symbol, not a device address; host code
-// gets its device address with cudaGetSymbolAddress, once per device, with
-// that device current (see scratch_on_current_device).
+// Under lazy module loading (the default since CUDA 12.2) that array is
+// reserved on a device when the module is first loaded there, which the
+// first call's cudaGetSymbolAddress triggers: that first call on a device
+// can therefore fail for want of device memory.  On the host the array's
+// name is a stand-in symbol, not a device address; the first call on each
+// device, with that device current, looks the address up and keeps it for
+// the life of the process (scratch_on_current_device).
 #include "../../include/eschalign_b200.h"
 #include "esg_kernels.cuh"
 
@@ -51,62 +57,6 @@ cudaError_t scratch_on_current_device(int2** out) {
   return cudaSuccess;
 }
 
-struct NoAllocParams {
-  const uint8_t* codes;   // queries, scored as given (forward only)
-  const uint64_t* off;
-  const uint32_t* len;
-  uint32_t n_queries;
-  const uint8_t* rcodes;  // references in the caller's order
-  const uint32_t* roff;
-  const uint32_t* rlen;
-  uint32_t n_refs;
-  int32_t* rows;          // [q * n_refs + r]
-  int2* scratch;
-  uint32_t max_cols;      // the caller's max_ref_len: the scratch is sized for it
-  int32_t ma, mi, o, e;
-};
-
-// k3_plain with the query list and reference order taken as the identity:
-// one thread per (query, reference), int32 stripes, boundary in `scratch`.
-template <bool kLocal>
-__global__ void __launch_bounds__(kK3Threads) k3_noalloc(const NoAllocParams P) {
-  const uint64_t total = (uint64_t)P.n_queries * P.n_refs;
-  const size_t nthreads = (size_t)gridDim.x * blockDim.x;
-  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int2* bnd = P.scratch + tid;
-  for (uint64_t idx = tid; idx < total; idx += nthreads) {
-    const uint32_t q = (uint32_t)(idx / P.n_refs);
-    const uint32_t k = (uint32_t)(idx % P.n_refs);
-    const int n = (int)P.len[q];
-    const uint8_t* qc = P.codes + P.off[q];
-    const int m = (int)P.rlen[k];
-    if ((uint32_t)m > P.max_cols) {
-      // longer than the caller said: the scratch has no room for its columns
-      P.rows[(size_t)q * P.n_refs + k] = INT32_MIN;
-      continue;
-    }
-    const uint8_t* rcodes = P.rcodes + P.roff[k];
-    int best = kLocal ? 0 : kNeg32;
-    for (int i0 = 0; i0 < n; i0 += kRows) {
-      uint32_t qm[kRows];
-#pragma unroll
-      for (int r = 0; r < kRows; ++r) {
-        const int i = i0 + r;
-        qm[r] = i < n ? code_mask(qc[i] > 4 ? 4u : qc[i]) : 0u;
-      }
-      const int rows = min(kRows, n - i0);
-      if (i0 + kRows >= n)
-        k3_stripe<kLocal, true>(rcodes, m, qm, rows, i0 == 0, bnd, nthreads, P.ma, P.mi, P.o,
-                                P.e, best);
-      else
-        k3_stripe<kLocal, false>(rcodes, m, qm, rows, i0 == 0, bnd, nthreads, P.ma, P.mi, P.o,
-                                 P.e, best);
-    }
-    if (n == 0 || m == 0) best = 0;  // scalar.rs:123-125
-    P.rows[(size_t)q * P.n_refs + k] = best;
-  }
-}
-
 }  // namespace
 
 extern "C" esg_status esg_score_rows_noalloc(const uint8_t* d_codes, const uint64_t* d_off,
@@ -134,31 +84,55 @@ extern "C" esg_status esg_score_rows_noalloc(const uint8_t* d_codes, const uint6
   if (max_ref_len > ESG_NOALLOC_MAX_REF_LEN) {
     esg_internal_set_error(ESG_ERR_REFERENCE_TOO_LONG,
                            "esg_score_rows_noalloc: max_ref_len exceeds ESG_NOALLOC_MAX_REF_LEN "
-                           "(8192); the static scratch holds 2^21 columns x threads");
+                           "(8192); the static column buffer holds 2^21 columns");
     return ESG_ERR_REFERENCE_TOO_LONG;
   }
   if (n_queries == 0 || n_refs == 0) return ESG_OK;
   int2* scratch = nullptr;
   cudaError_t e = scratch_on_current_device(&scratch);
   if (e != cudaSuccess) {
-    esg_internal_set_error(ESG_ERR_DRIVER, cudaGetErrorString(e));
-    return ESG_ERR_DRIVER;
+    // the first call on a device loads the module and so reserves the array
+    const esg_status st =
+        e == cudaErrorMemoryAllocation ? ESG_ERR_OUT_OF_MEMORY : ESG_ERR_DRIVER;
+    esg_internal_set_error(st, cudaGetErrorString(e));
+    return st;
   }
   int dev = 0, sms = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // threads x max_ref_len boundary cells must fit the static scratch
+  // one reference's bottom row (max_ref_len columns) per warp must fit the
+  // static array: at most kScratchInt2 / max_ref_len warps
   const size_t cols = max_ref_len ? max_ref_len : 1;
-  size_t threads = std::min<size_t>((size_t)sms * 4 * kK3Threads, kScratchInt2 / cols);
-  threads = threads / kK3Threads * kK3Threads;
-  if (threads == 0) threads = kK3Threads;  // max_ref_len <= 8192 keeps this in bounds
-  NoAllocParams P{d_codes, d_off, d_len, n_queries, d_ref_codes, d_ref_off, d_ref_len, n_refs,
-                  d_rows, scratch, (uint32_t)cols, s.match_score, s.mismatch, s.gap_open,
-                  s.gap_extend};
+  size_t blocks = std::min<size_t>((size_t)sms * 4, kScratchInt2 / (cols * kK3Warps));
+  if (blocks == 0) blocks = 1;  // max_ref_len <= 8192 keeps 64 CTAs in bounds
+  K3Params P{};
+  P.codes = d_codes;
+  P.off = d_off;
+  P.len = d_len;
+  P.n_reads = n_queries;
+  P.list = nullptr;  // query p is read p, forward
+  P.host_count = n_queries;
+  P.rcodes = d_ref_codes;
+  P.roff = d_ref_off;
+  P.rlen = d_ref_len;
+  P.ridx = nullptr;  // the caller's reference order
+  P.n_refs = n_refs;
+  P.max_cols = max_ref_len;
+  P.out = nullptr;
+  P.rows = d_rows;
+  P.wmax = 32;
+  P.refs_per_task = 32;
+  P.task_counter = nullptr;  // units taken warp-strided: no counter to clear
+  P.colbuf = scratch;
+  P.ma = s.match_score;
+  P.mi = s.mismatch;
+  P.o = s.gap_open;
+  P.e = s.gap_extend;
+  P.one = 1;
   void* args[] = {&P};
-  const void* fn = mode == ESG_MODE_LOCAL ? (const void*)k3_noalloc<true>
-                                          : (const void*)k3_noalloc<false>;
-  e = cudaLaunchKernel(fn, dim3((unsigned)(threads / kK3Threads)), dim3(kK3Threads), args, 0,
+  const void* fn = mode == ESG_MODE_LOCAL ? (const void*)k3_lanes<true>
+                                          : (const void*)k3_lanes<false>;
+  e = cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(kK3Threads), args, 0,
                        (cudaStream_t)stream);
   if (e != cudaSuccess) {
     esg_internal_set_error(ESG_ERR_DRIVER, cudaGetErrorString(e));

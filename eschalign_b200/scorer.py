@@ -33,6 +33,7 @@ RESULT_RESCORED32 = 4
 
 KERNEL_AUTO = 0
 KERNEL_PLAIN32 = 1
+KERNEL_INT32 = 2
 BOTH_STRANDS = 1
 FULL_ROWS = 2
 

@@ -52,8 +52,9 @@ typedef struct esg_scoring {
 #define ESG_MODE_SEMIGLOBAL 1
 
 /* ---- kernel choice: the A/B lever of GpuScorer::set_half2 (cuda/mod.rs:500) */
-#define ESG_KERNEL_AUTO 0    /* batched int16x2 kernel, int32 for what it cannot take */
-#define ESG_KERNEL_PLAIN32 1 /* every query on the plain one-thread-per-pair kernel  */
+#define ESG_KERNEL_AUTO 0    /* batched int16x2 kernel, int32 lanes for what it cannot take */
+#define ESG_KERNEL_PLAIN32 1 /* every query in int32, one thread per (query, reference)     */
+#define ESG_KERNEL_INT32 2   /* every query on the int32 lanes (up to 32 lanes a reference) */
 
 /* ---- batch flags */
 #define ESG_BOTH_STRANDS 1u /* also score each read's reverse complement (align.rs:2865-2872) */
@@ -169,7 +170,9 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
 void esg_scorer_free(esg_scorer* scorer);
 
 esg_status esg_scorer_info(const esg_scorer* scorer, esg_info* out);
-/* GpuScorer::set_half2 (cuda/mod.rs:500-502): ESG_KERNEL_AUTO or _PLAIN32. */
+/* GpuScorer::set_half2 (cuda/mod.rs:500-502): ESG_KERNEL_AUTO, _PLAIN32 or
+ * _INT32.  Choosing _PLAIN32 the first time makes its column buffers
+ * (32 x max_ref_len x 8 bytes per warp, at most 1 GiB). */
 esg_status esg_scorer_set_kernel(esg_scorer* scorer, int32_t kernel);
 /* Tile-shape autotuner (no counterpart in the reference, whose one kernel
  * shape is fixed): times the batched kernels on synthetic calibration
@@ -531,27 +534,35 @@ void esg_server_free(esg_server* server);
 
 /* Scoring for callers that cannot allocate.  No counterpart in the reference.
  *
- * Code that runs where cudaMalloc is off limits -- inside someone else's
- * stream capture, under a framework that owns the device allocator, in a
- * real-time loop that must not touch the allocator after start-up -- calls
- * this instead of a scorer: it allocates nothing, host or device.  The
- * caller passes device buffers: queries (codes 0..4, query q is
- * d_codes[d_off[q] .. +d_len[q]], scored as given, forward only),
+ * Some callers cannot call cudaMalloc when they need scores: a process whose
+ * device memory belongs to a framework's caching allocator, which forbids
+ * allocations behind its back (they fragment its pool and escape its
+ * budget), or a real-time loop that must not enter the driver's allocator
+ * after start-up (cudaMalloc and cudaFree can block and synchronize the
+ * device).  They call this instead of a scorer: it allocates nothing, host
+ * or device.  The caller passes device buffers: queries (codes 0..4, query
+ * q is d_codes[d_off[q] .. +d_len[q]], scored as given, forward only),
  * references (d_ref_codes[d_ref_off[r] .. +d_ref_len[r]]) and the output
  * d_rows[q * n_refs + r] (int32, the scalar oracle's score of every pair,
- * scalar.rs:120-163).  It runs the plain int32 kernel on `stream` (NULL:
- * the legacy default stream) and returns without waiting.
+ * scalar.rs:120-163).  It runs the int32 lanes kernel on `stream` (NULL: the
+ * legacy default stream) and returns without waiting.
  *
- * The kernel's scratch is a 16 MiB array reserved on every GPU that loads
- * the library, held until exit; it limits references to
- * ESG_NOALLOC_MAX_REF_LEN bases (`max_ref_len`, which must be at least
- * every d_ref_len; larger values are refused with
- * ESG_ERR_REFERENCE_TOO_LONG, and a reference longer than the stated
- * max_ref_len scores ESG_NO_SCORE).  The first call on a device looks up
- * the array's device address on that device, so make that first call
- * before any stream capture.  Every call shares the one array: calls whose
- * kernels overlap on the GPU (other streams, other threads) race and must
- * be serialized by the caller.  Nothing in the array needs to start at zero. */
+ * The kernel's column buffer (a reference's bottom row carried between the
+ * passes of a query longer than 512 bases) is a 16 MiB array held on every
+ * GPU where the library's module is loaded, until the process exits.  It
+ * limits references to ESG_NOALLOC_MAX_REF_LEN bases: `max_ref_len` above
+ * that is refused with ESG_ERR_REFERENCE_TOO_LONG, and a reference longer
+ * than the stated max_ref_len (any reference, when it is 0) scores
+ * ESG_NO_SCORE.  Under lazy module loading (the CUDA default) the module,
+ * and with it the array, is loaded on a device by the first call there,
+ * which also looks up the array's device address on that device (the
+ * device must be current) and keeps it for the life of the process: that
+ * first call can fail with ESG_ERR_OUT_OF_MEMORY, and it should come before
+ * any stream capture.  The kept address does not survive cudaDeviceReset:
+ * do not call this on a device after resetting it.  Every call shares the
+ * one array: calls whose kernels overlap on the GPU (other streams, other
+ * threads) race and must be serialized by the caller.  Nothing in the array
+ * needs to start at zero. */
 #define ESG_NOALLOC_MAX_REF_LEN 8192
 esg_status esg_score_rows_noalloc(const uint8_t* d_codes, const uint64_t* d_off,
                                   const uint32_t* d_len, uint32_t n_queries,

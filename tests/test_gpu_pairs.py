@@ -9,14 +9,15 @@ pair's ranking with the oracle, on both kernels."""
 import numpy as np
 import pytest
 
-from eschalign_b200 import KERNEL_AUTO, KERNEL_PLAIN32, GpuScorer, Mode, Scoring, adapter, synth
+from eschalign_b200 import KERNEL_AUTO, KERNEL_INT32, KERNEL_PLAIN32, GpuScorer, Mode, Scoring, adapter, synth
 from tests.helpers import pairs_fixture
 
 pytestmark = pytest.mark.gpu
 
 SG = (2, -1, -10, -1)
 NO_TIE = 0xFFFFFFFF
-CONFIGS = ((KERNEL_AUTO, 512, 64), (KERNEL_AUTO, 0, 1), (KERNEL_PLAIN32, 256, 64))
+CONFIGS = ((KERNEL_AUTO, 512, 64), (KERNEL_AUTO, 0, 1), (KERNEL_INT32, 256, 64),
+           (KERNEL_PLAIN32, 256, 64))
 
 
 def expected(O, mates, refs, scoring, local, both, min_score, cap, max_read_len=0,

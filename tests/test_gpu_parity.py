@@ -1,15 +1,16 @@
 """The CUDA path against the CPU oracle, by equality (no tolerance: integer
 scores).  Mirrors crates/eschalign/tests/gpu_parity.rs: every check runs on
-both kernels (the batched int16x2 kernel with int32 for what it cannot take,
-and the plain int32 kernel), reverse complements included, and compares
+every kernel setting (the batched int16x2 kernel with int32 lanes for what
+it cannot take, every query on the int32 lanes, and int32 one thread per
+(query, reference)), reverse complements included, and compares
 every query's full row with the scalar oracle and every read's reduced
 result (best, XS, tie count, tie list) with the oracle's selection
 (mapper.rs:444-472)."""
 import numpy as np
 import pytest
 
-from eschalign_b200 import (KERNEL_AUTO, KERNEL_PLAIN32, GpuError, GpuScorer, Mode, Scoring,
-                            encode, pack_reads, synth)
+from eschalign_b200 import (KERNEL_AUTO, KERNEL_INT32, KERNEL_PLAIN32, GpuError, GpuScorer, Mode,
+                            Scoring, encode, pack_reads, synth)
 from tests.helpers import (SCHEMES, Rng, fixture_panel, fixture_reads, golden, random_panel,
                            random_seq, reads_for)
 
@@ -37,9 +38,10 @@ def oracle_rows(O, reads, panel, scoring, local):
 
 # (kernel, 16/32-row split, panel chunks at most): 16-row stripes up to
 # 512 nt with the panel chunked or whole, every query on 32-row stripes
-# chunked or whole, the plain int32 kernel
+# chunked or whole, every query on the int32 lanes, and in int32 one thread
+# per (query, reference)
 CONFIGS = ((KERNEL_AUTO, 512, 64), (KERNEL_AUTO, 512, 1), (KERNEL_AUTO, 0, 64),
-           (KERNEL_AUTO, 0, 1), (KERNEL_PLAIN32, 256, 64))
+           (KERNEL_AUTO, 0, 1), (KERNEL_INT32, 256, 64), (KERNEL_PLAIN32, 256, 64))
 
 
 def check(O, panel, reads, scoring, mode, what, kernels=CONFIGS, tie_capacity=CAP):
@@ -241,7 +243,7 @@ def test_gpu_config1_reads_equal_avx512(oracle):
     reads = synth.reads_c1(refs)
     want, want_t = cpu_results(oracle, refs, reads, (2, -1, -10, -1), True, False)
     with GpuScorer(refs, Scoring(), Mode.LOCAL) as g:
-        for kernel in (KERNEL_AUTO, KERNEL_PLAIN32):
+        for kernel in (KERNEL_AUTO, KERNEL_INT32, KERNEL_PLAIN32):
             g.set_kernel(kernel)
             res = g.score_batch(reads.tuple())
             assert (res.results["best"] == want["best"]).all()

@@ -1,19 +1,21 @@
 """esg_score_rows_noalloc: scoring for callers that cannot allocate.
 
-Callers inside someone else's stream capture, under a framework that owns the
-device allocator, or in a loop that must not touch the allocator after
-start-up pass their own device buffers and get every (query, reference)
-score without the library allocating anything; the plain int32 kernel's
-scratch is a static device array.  Checked here against the scorer's own
-entry point (esg_score_batch with full rows) on two calls in a row, exactly:
-scores are integers.  This file is collected last on purpose."""
+A process whose device memory belongs to a framework's caching allocator,
+or a real-time loop that must not enter the driver's allocator after
+start-up, cannot let the library call cudaMalloc; it passes its own device
+buffers and gets every (query, reference) score, the int32 kernel's column
+buffer being a static device array.  Checked here through the C ABI on two
+calls in a row against the scorer's own entry point (esg_score_batch with
+full rows) and against the scalar oracle, exactly: scores are integers.
+The reads include ones longer than 512 bases, whose passes go through the
+static column buffer.  This file is collected last on purpose."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
 from eschalign_b200 import GpuScorer, Mode, Scoring, _native, encode, pack_reads
-from tests.helpers import Rng, random_panel, reads_for
+from tests.helpers import Rng, random_panel, random_seq, reads_for
 
 pytestmark = pytest.mark.gpu
 
@@ -41,7 +43,7 @@ def _noalloc(lib, torch, reads, panel, scoring, mode, max_ref_len=None):
     return st, rows.cpu().numpy()
 
 
-def test_noalloc_rows_equal_score_batch_rows_twice():
+def test_noalloc_rows_equal_score_batch_and_oracle_twice(oracle):
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -49,17 +51,23 @@ def test_noalloc_rows_equal_score_batch_rows_twice():
     rng = Rng(0x5EED_0A11)
     letters = random_panel(rng, 37, 20, 280)
     panel = [encode(s) for s in letters]
-    first = reads_for(rng, letters, 60)
-    second = reads_for(rng, letters, 90)
+    # reads past 512 bases take several passes through the column buffer
+    long_reads = [encode(letters[k] * (600 // len(letters[k]) + 1 + k % 3) +
+                         random_seq(rng, 40, 0.02)) for k in range(0, 37, 6)]
+    first = reads_for(rng, letters, 60) + long_reads[:4]
+    second = reads_for(rng, letters, 90) + long_reads[4:]
+    assert max(len(r) for r in first) > 512 and max(len(r) for r in second) > 512
     for scoring in ((2, -1, -10, -1), (3, 1, -5, -2)):
         for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+            local = mode == Mode.LOCAL
             with GpuScorer(panel, Scoring(*scoring), mode) as g:
-                for reads in (first, second):  # two calls in a row, sharing the scratch
+                for reads in (first, second):  # two calls in a row, sharing the array
                     want = g.score_batch(reads, full_rows=True).rows
                     st, got = _noalloc(lib, torch, reads, panel, scoring, mode)
                     assert st == 0, lib.esg_last_error()
                     assert got.shape == want.shape
                     assert (got == want).all(), (scoring, mode)
+                    assert (got == oracle.score_matrix(reads, panel, scoring, local)).all()
 
 
 def test_noalloc_refuses_references_past_its_scratch():
@@ -75,3 +83,7 @@ def test_noalloc_refuses_references_past_its_scratch():
     st, rows = _noalloc(lib, torch, reads, [np.zeros(100, np.uint8), np.zeros(50, np.uint8)],
                         (2, -1, -10, -1), Mode.LOCAL, max_ref_len=60)
     assert st == 0 and rows[0, 0] == -(2**31) and rows[0, 1] == 20
+    # max_ref_len 0: every reference is longer than that
+    st, rows = _noalloc(lib, torch, reads, [np.zeros(5, np.uint8)], (2, -1, -10, -1),
+                        Mode.LOCAL, max_ref_len=0)
+    assert st == 0 and rows[0, 0] == -(2**31)
