@@ -129,6 +129,13 @@ struct esg_scorer {
   const void* k2_t32 = nullptr;   // tiles of 32-row stripes
   const void* k2_long = nullptr;  // one long query, 32-row stripes, in passes
   int blocks_t16 = 0, blocks_t32 = 0, blocks_long = 0;
+  // semi-global: the same three with every cell's maximum checked against
+  // the int16 lanes' upper limit, for batches holding queries past the
+  // static bound (k2_checks)
+  const void* k2c_t16 = nullptr;
+  const void* k2c_t32 = nullptr;
+  const void* k2c_long = nullptr;
+  int blocksc_t16 = 0, blocksc_t32 = 0, blocksc_long = 0;
   // queries up to split_len bases take 16-row stripes, longer ones 32-row
   // stripes (esg_scorer_autotune measures where 32 rows start to win)
   uint32_t split_len = 256;
@@ -175,6 +182,7 @@ struct esg_batch {
   uint32_t host_list = 0;
   uint32_t redo_cap = 0;
   uint32_t n_chunks = 1;  // panel chunks per tile (k2 tasks = tiles x chunks)
+  bool sg_check = false;  // semi-global: run the checked k2 variants
   // paired batches (esg_prepare_pairs): reads 2p, 2p + 1 are pair p's mates
   bool paired = false;
   bool pair_both = false;   // rank both template strands
@@ -238,23 +246,39 @@ int64_t value_bound(uint64_t n, uint32_t max_ref_len, const esg_scoring& s) {
   return k * mm + std::abs(s.gap_open) + std::abs(s.gap_extend);
 }
 
+// Semi-global cells go negative, and the biased lanes (H - 16384) must stay
+// above the -infinity stand-in (-31500): every H is at least
+// o + (min(i, j) - 1) e (a gap from the zero border), every E and F at least
+// that + o, so 2 |o| + (min(n, L) - 1) |e| below 15000 keeps them there.
+bool sg_floor_ok(const esg_scorer* sc, uint64_t n) {
+  const int64_t k = (int64_t)std::min<uint64_t>(n, sc->max_ref_len);
+  return 2 * (int64_t)std::abs(sc->scoring.gap_open) +
+             (k - 1) * (int64_t)std::abs(sc->scoring.gap_extend) <
+         15000;
+}
+
+// Semi-global queries inside this static bound never reach H = 12000 and run
+// unchecked; past it the checked variant watches every cell's maximum and
+// flags the query for the int32 re-score when one reaches 16384.
+bool k2_checks(const esg_scorer* sc, uint64_t n) {
+  if (sc->mode != ESG_MODE_SEMIGLOBAL) return false;
+  const int64_t mm = std::max(std::abs(sc->scoring.match_score), std::abs(sc->scoring.mismatch));
+  return value_bound(n, sc->max_ref_len, sc->scoring) + mm >= 12000;
+}
+
 bool k2_takes(const esg_scorer* sc, uint64_t n) {
   if (!sc->batched_ok || n == 0) return false;
   // queries over 32 stripes of 32 rows run in passes chained through the
   // column buffer
   if ((n + 31) / 32 > (uint64_t)kMaxStripes && !sc->d_lbuf) return false;
   if ((n + 31) / 32 > 0xffffu) return false;
-  if (sc->mode == ESG_MODE_SEMIGLOBAL) {
-    // semi-global cells go negative: the biased lanes (H - 16384) must stay
-    // negative and above the -infinity stand-in
-    const int64_t mm = std::max(std::abs(sc->scoring.match_score), std::abs(sc->scoring.mismatch));
-    return value_bound(n, sc->max_ref_len, sc->scoring) + mm < 12000;
-  }
+  if (sc->mode == ESG_MODE_SEMIGLOBAL) return sg_floor_ok(sc, n);
   return true;  // local: a wrap is detected by the kernel (K2Params::sat)
 }
 
+// Queries whose k2 result may be flagged for the int32 re-score.
 bool k2_may_flag(const esg_scorer* sc, uint64_t n) {
-  if (sc->mode != ESG_MODE_LOCAL) return false;
+  if (sc->mode != ESG_MODE_LOCAL) return k2_checks(sc, n);
   const int64_t hmax = (int64_t)std::min<uint64_t>(n, sc->max_ref_len) * sc->scoring.match_score;
   return hmax >= sc->sat;
 }
@@ -268,27 +292,30 @@ T* carve(char*& at, size_t count) {
 
 size_t carve_size(size_t count, size_t elem) { return (count * elem + 255) / 256 * 256; }
 
-template <int R, bool kLong>
-const void* pick_k2(bool local, bool w, bool smem) {
-  if (local) {
-    if (w)
-      return smem ? (const void*)k2_batched<R, true, true, true, kLong>
-                  : (const void*)k2_batched<R, true, true, false, kLong>;
-    return smem ? (const void*)k2_batched<R, true, false, true, kLong>
-                : (const void*)k2_batched<R, true, false, false, kLong>;
-  }
+template <int R, bool kLong, bool kLocal, bool kCheck>
+const void* pick_k2_ws(bool w, bool smem) {
   if (w)
-    return smem ? (const void*)k2_batched<R, false, true, true, kLong>
-                : (const void*)k2_batched<R, false, true, false, kLong>;
-  return smem ? (const void*)k2_batched<R, false, false, true, kLong>
-              : (const void*)k2_batched<R, false, false, false, kLong>;
+    return smem ? (const void*)k2_batched<R, kLocal, true, true, kLong, kCheck>
+                : (const void*)k2_batched<R, kLocal, true, false, kLong, kCheck>;
+  return smem ? (const void*)k2_batched<R, kLocal, false, true, kLong, kCheck>
+              : (const void*)k2_batched<R, kLocal, false, false, kLong, kCheck>;
+}
+
+template <int R, bool kLong>
+const void* pick_k2(bool local, bool check, bool w, bool smem) {
+  if (local) return pick_k2_ws<R, kLong, true, false>(w, smem);
+  return check ? pick_k2_ws<R, kLong, false, true>(w, smem)
+               : pick_k2_ws<R, kLong, false, false>(w, smem);
 }
 
 void set_k2_fn(esg_scorer* sc) {
   const bool local = sc->mode == ESG_MODE_LOCAL;
-  sc->k2_t16 = pick_k2<16, false>(local, sc->panel_w, sc->smem_panel);
-  sc->k2_t32 = pick_k2<32, false>(local, sc->panel_w, sc->smem_panel);
-  sc->k2_long = pick_k2<32, true>(local, sc->panel_w, sc->smem_panel);
+  sc->k2_t16 = pick_k2<16, false>(local, false, sc->panel_w, sc->smem_panel);
+  sc->k2_t32 = pick_k2<32, false>(local, false, sc->panel_w, sc->smem_panel);
+  sc->k2_long = pick_k2<32, true>(local, false, sc->panel_w, sc->smem_panel);
+  sc->k2c_t16 = pick_k2<16, false>(local, !local, sc->panel_w, sc->smem_panel);
+  sc->k2c_t32 = pick_k2<32, false>(local, !local, sc->panel_w, sc->smem_panel);
+  sc->k2c_long = pick_k2<32, true>(local, !local, sc->panel_w, sc->smem_panel);
   sc->k3_fn = local ? (const void*)k3_lanes<true> : (const void*)k3_lanes<false>;
 }
 
@@ -623,7 +650,8 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
   sc->smem_panel = (size_t)sc->blob_bytes + slots <= 100 * 1024;
   set_k2_fn(sc);
   sc->k2_smem = (sc->smem_panel ? sc->blob_bytes : 0) + slots;
-  for (const void* fn : {sc->k2_t16, sc->k2_t32, sc->k2_long})
+  for (const void* fn : {sc->k2_t16, sc->k2_t32, sc->k2_long, sc->k2c_t16, sc->k2c_t32,
+                         sc->k2c_long})
     if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sc->k2_smem)) != cudaSuccess)
       return cleanup(cuda_fail(e, "cudaFuncSetAttribute(k2)"));
@@ -656,6 +684,20 @@ esg_status esg_scorer_new(int32_t device, const uint8_t* ref_codes, const uint64
   sc->blocks_t16 = std::max(1, occ16) * sc->sm_count;
   sc->blocks_t32 = std::max(1, occ32) * sc->sm_count;
   sc->blocks_long = std::max(1, occl) * sc->sm_count;
+  {
+    int c16 = 0, c32 = 0, cl = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c16, sc->k2c_t16, kK2Threads,
+                                                           sc->k2_smem)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c32, sc->k2c_t32, kK2Threads,
+                                                           sc->k2_smem)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cl, sc->k2c_long, kK2Threads,
+                                                           sc->k2_smem)) != cudaSuccess)
+      return cleanup(cuda_fail(e, "cudaOccupancy"));
+    sc->blocksc_t16 = std::max(1, c16) * sc->sm_count;
+    sc->blocksc_t32 = std::max(1, c32) * sc->sm_count;
+    // the long-query column buffer below is sized for blocks_long CTAs
+    sc->blocksc_long = std::min(std::max(1, cl) * sc->sm_count, sc->blocks_long);
+  }
   if (sc->batched_ok && max_len <= 8192) {
     sc->lbuf_cols = max_len;
     const size_t lb = (size_t)sc->blocks_long * kK2Warps * max_len * sizeof(uint2);
@@ -915,6 +957,7 @@ static esg_status prepare_impl(esg_scorer* sc, const uint8_t* const* ptrs, const
       else
         qlong.push_back({(n + 31) / 32, q});
       if (k2_may_flag(sc, n)) ++redo_cap;
+      if (k2_checks(sc, n)) b->sg_check = true;
     } else {
       route[q] = 2;
       ++n_k3;
@@ -1170,6 +1213,7 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
           1, std::min<uint64_t>((uint64_t)cap, (tasks + kK2Warps - 1) / kK2Warps));
     };
     const bool aux = n_long || n_t32;
+    const bool chk = b->sg_check;
     if (aux) {
       ESG_CUDA(cudaEventRecord(sc->fork, st));
       ESG_CUDA(cudaStreamWaitEvent(sc->aux, sc->fork, 0));
@@ -1179,7 +1223,8 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
       L.n_tasks = n_long;
       L.task_counter = b->d_counters + 3;
       void* largs[] = {&L};
-      ESG_CUDA(cudaLaunchKernel(sc->k2_long, dim3(grid(sc->blocks_long, n_long)),
+      ESG_CUDA(cudaLaunchKernel(chk ? sc->k2c_long : sc->k2_long,
+                                dim3(grid(chk ? sc->blocksc_long : sc->blocks_long, n_long)),
                                 dim3(kK2Threads), largs, sc->k2_smem, sc->aux));
       ++kernels;
     }
@@ -1189,7 +1234,9 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
       T.n_tasks = n_t32;
       T.task_counter = b->d_counters + 4;
       void* targs[] = {&T};
-      ESG_CUDA(cudaLaunchKernel(sc->k2_t32, dim3(grid(sc->blocks_t32, n_t32)), dim3(kK2Threads),
+      ESG_CUDA(cudaLaunchKernel(chk ? sc->k2c_t32 : sc->k2_t32,
+                                dim3(grid(chk ? sc->blocksc_t32 : sc->blocks_t32, n_t32)),
+                                dim3(kK2Threads),
                                 targs, sc->k2_smem, sc->aux));
       ++kernels;
     }
@@ -1199,7 +1246,9 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
       T.n_tasks = n_t16;
       T.task_counter = b->d_counters + 0;
       void* targs[] = {&T};
-      ESG_CUDA(cudaLaunchKernel(sc->k2_t16, dim3(grid(sc->blocks_t16, n_t16)), dim3(kK2Threads),
+      ESG_CUDA(cudaLaunchKernel(chk ? sc->k2c_t16 : sc->k2_t16,
+                                dim3(grid(chk ? sc->blocksc_t16 : sc->blocks_t16, n_t16)),
+                                dim3(kK2Threads),
                                 targs, sc->k2_smem, st));
       ++kernels;
     }

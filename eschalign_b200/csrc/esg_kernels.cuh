@@ -359,14 +359,14 @@ __device__ __forceinline__ uint32_t load_sel(const uint16_t* sp, int j) {
   }
 }
 
-template <int R, bool kLocal, bool kPanelW, bool kLong, bool kSmem>
+template <int R, bool kLocal, bool kPanelW, bool kLong, bool kSmem, bool kCheck>
 __device__ __forceinline__ void pair_pass(const K2Params& P, uint32_t scr, bool wild,
                                           const uint32_t (&ta)[R],
                                           const uint32_t (&tb)[kPanelW ? R : 1], int skew,
                                           bool active_lane, bool first, uint32_t padmask, int m,
                                           int jshort, const uint16_t* __restrict__ sp, int steps,
                                           const PassConst& K, uint2* buf, bool from_buf,
-                                          bool to_buf, uint32_t& v, uint32_t& lr) {
+                                          bool to_buf, uint32_t& v, uint32_t& lr, uint32_t& am) {
   const int lane = threadIdx.x & 31;
   constexpr bool kLds = sc_lds<kLocal, R>() && !kLong;
   constexpr bool kPre = sel_prefetch<kLocal>();
@@ -384,7 +384,9 @@ __device__ __forceinline__ void pair_pass(const K2Params& P, uint32_t scr, bool 
   }
   uint32_t gdc = K.g0;  // G of the row above, previous column
   uint32_t gbot = K.g0, fbot = K.neg2;
-  uint32_t best = K.bias2;                 // local: max H + B over this lane's cells
+  // local: max H + B over this lane's cells; checked semi-global: the same
+  // without the floor (the short half's taken at its own end)
+  uint32_t best = kLocal ? K.bias2 : K.neg2, s_best = K.neg2;
   uint32_t lastrow = K.neg2;               // semi-global: max H + B of row 15
   uint32_t s_col = K.neg2, s_last = K.neg2;  // semi-global short-half snapshot
   // inactive lanes of a tile sit at a skew no step reaches; only the long
@@ -441,6 +443,12 @@ __device__ __forceinline__ void pair_pass(const K2Params& P, uint32_t scr, bool 
           hprev = h;
       } else {
         h = max16x2(h1, f);
+        if constexpr (kCheck) {
+          if (r & 1)
+            best = __vimax3_s16x2(best, hprev, h);
+          else
+            hprev = h;
+        }
       }
       gd = g[r];
       g[r] = mad_lo(h, K.one, K.o32);
@@ -471,6 +479,7 @@ __device__ __forceinline__ void pair_pass(const K2Params& P, uint32_t scr, bool 
         }
         s_col = cm;
         s_last = lastrow;
+        if constexpr (kCheck) s_best = best;
       }
     }
   };
@@ -526,10 +535,13 @@ __device__ __forceinline__ void pair_pass(const K2Params& P, uint32_t scr, bool 
     const int j = t - skew;
     if ((unsigned)j < (unsigned)mlim) column(j, gt, ft);
   }
+  am = K.neg2;
   if constexpr (kLocal) {
     v = best;
     lr = 0;
   } else {
+    if constexpr (kCheck)
+      am = active_lane ? (jshort >= 0 ? (best & 0xffffu) | (s_best & 0xffff0000u) : best) : K.neg2;
     uint32_t cm = K.neg2;
 #pragma unroll
     for (int r = 0; r < R; ++r) cm = max16x2(cm, ((padmask >> r) & 1u) ? K.neg2 : g[r]);
@@ -573,11 +585,16 @@ __device__ __forceinline__ bool row_tables(const K2Params& P, const uint8_t* q, 
 }
 
 // The last lane of a query folds one reference pair's two scores into the
-// query's slot (and its rows, when asked for).
-template <bool kLocal>
+// query's slot (and its rows, when asked for).  A pair that may have left
+// the int16 lanes flags its query for the int32 re-score: in local mode a
+// best at or above P.sat; in checked semi-global mode any cell with
+// H + B >= 0 (H >= 16384), where G's IMAD may borrow wrongly (see
+// pair_pass) -- the first such cell is itself exact, its inputs being below
+// the mark, so the maximum over every cell, `am`, catches it.
+template <bool kLocal, bool kCheck>
 __device__ __forceinline__ void fold_pair(const K2Params& P, int* slot, uint32_t* sties,
                                           uint32_t cap, uint4 pm, int mB, bool rc, uint32_t qid,
-                                          uint32_t v, uint32_t lr, int bias) {
+                                          uint32_t v, uint32_t lr, uint32_t am, int bias) {
   int scA, scB;
   if constexpr (kLocal) {
     scA = lo16(v) - bias;
@@ -586,6 +603,8 @@ __device__ __forceinline__ void fold_pair(const K2Params& P, int* slot, uint32_t
   } else {
     scA = max(lo16(v) - P.o, lo16(lr)) - bias;
     scB = max(hi16(v) - P.o, hi16(lr)) - bias;
+    if constexpr (kCheck)
+      if (lo16(am) >= 0 || (mB > 0 && hi16(am) >= 0)) slot[3] |= kQRedo;
   }
   const uint32_t rbit = rc ? 1u : 0u;
   slot_add(slot, sties, cap, (pm.z << 1) | rbit, scA);
@@ -632,7 +651,7 @@ __device__ __forceinline__ void flush_query(const K2Params& P, uint32_t qid, uin
 // Stripes are aligned so the read's last row is row 15 of its last stripe;
 // the 16 S - n rows before the read's first row score 0 against every real
 // column and hold H = 0 exactly, the top border the first real row needs.
-template <int R, bool kLocal, bool kPanelW, bool kSmemPanel, bool kLong>
+template <int R, bool kLocal, bool kPanelW, bool kSmemPanel, bool kLong, bool kCheck>
 __global__ void __launch_bounds__(kK2Threads, R > 16 ? ESG_K2_R32_BLOCKS : (kPanelW ? 4 : ESG_K2_MIN_BLOCKS))
     k2_batched(const K2Params P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -706,7 +725,7 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? ESG_K2_R32_BLOCKS : (kPan
         const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);  // mA >= mB
         const int jshort = (mB > 0 && mB < mA) ? mB - 1 : -1;
         const uint16_t* sp = sels + pm.x;
-        uint32_t acc = kLocal ? K.bias2 : K.neg2, lr_last = K.neg2;
+        uint32_t acc = kLocal ? K.bias2 : K.neg2, lr_last = K.neg2, amacc = K.neg2;
         for (int pass = 0; pass < passes; ++pass) {
           const int s = pass * 32 + lane;
           const bool valid = s < S;
@@ -714,17 +733,24 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? ESG_K2_R32_BLOCKS : (kPan
           uint32_t tb[kPanelW ? R : 1];
           row_tables<R, kPanelW, false>(P, q, n, rc, valid, s, pad, ta, tb);
           const uint32_t padmask = (s == 0) ? ((1u << pad) - 1u) : 0u;
-          uint32_t v, lr;
-          pair_pass<R, kLocal, kPanelW, true, kSmemPanel>(P, 0u, false, ta, tb, lane, valid, s == 0, padmask, mA,
-                                                       jshort, sp,
-                                           mA + 31, K, lbuf, pass > 0, pass + 1 < passes, v, lr);
+          uint32_t v, lr, am;
+          pair_pass<R, kLocal, kPanelW, true, kSmemPanel, kCheck>(
+              P, 0u, false, ta, tb, lane, valid, s == 0, padmask, mA, jshort, sp, mA + 31, K,
+              lbuf, pass > 0, pass + 1 < passes, v, lr, am);
           acc = max16x2(acc, v);
+          if constexpr (kCheck) amacc = max16x2(amacc, am);
           if (pass + 1 == passes) lr_last = lr;
           __syncwarp();  // the buffer's writes are visible to the next pass
         }
 #pragma unroll
         for (int d = 16; d; d >>= 1) acc = max16x2(acc, __shfl_xor_sync(kFull, acc, d));
-        if (lane == owner) fold_pair<kLocal>(P, slot, sties, cap, pm, mB, rc, qid, acc, lr_last, bias);
+        if constexpr (kCheck) {
+#pragma unroll
+          for (int d = 16; d; d >>= 1) amacc = max16x2(amacc, __shfl_xor_sync(kFull, amacc, d));
+        }
+        if (lane == owner)
+          fold_pair<kLocal, kCheck>(P, slot, sties, cap, pm, mB, rc, qid, acc, lr_last, amacc,
+                                    bias);
       }
       if (lane == owner) flush_query(P, qid, chunk, slot, sties, cap);
       __syncwarp();
@@ -785,17 +811,21 @@ __global__ void __launch_bounds__(kK2Threads, R > 16 ? ESG_K2_R32_BLOCKS : (kPan
       const uint4 pm = pairs[p];
       const int mA = (int)(pm.y & 0xffffu), mB = (int)(pm.y >> 16);  // mA >= mB
       const int jshort = (mB > 0 && mB < mA) ? mB - 1 : -1;
-      uint32_t v, lr;
-      pair_pass<R, kLocal, kPanelW, false, kSmemPanel>(P, scr, wild, ta, tb, s, valid, first, padmask, mA, jshort,
-                                        sels + pm.x, mA + smax - 1, K, nullptr, false, false, v,
-                                        lr);
+      uint32_t v, lr, am;
+      pair_pass<R, kLocal, kPanelW, false, kSmemPanel, kCheck>(
+          P, scr, wild, ta, tb, s, valid, first, padmask, mA, jshort, sels + pm.x, mA + smax - 1,
+          K, nullptr, false, false, v, lr, am);
       // per-query maximum, to the query's last lane
 #pragma unroll
       for (int d = 1; d < 32; d <<= 1) {
         const uint32_t w = __shfl_up_sync(kFull, v, d);
         if (s >= d) v = max16x2(v, w);
+        if constexpr (kCheck) {
+          const uint32_t wa = __shfl_up_sync(kFull, am, d);
+          if (s >= d) am = max16x2(am, wa);
+        }
       }
-      if (last) fold_pair<kLocal>(P, slot, sties, cap, pm, mB, rc, qid, v, lr, bias);
+      if (last) fold_pair<kLocal, kCheck>(P, slot, sties, cap, pm, mB, rc, qid, v, lr, am, bias);
     }
 
     // --- flush the query states of this task

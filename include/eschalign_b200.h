@@ -196,8 +196,10 @@ esg_status esg_scorer_set_chunking(esg_scorer* scorer, uint32_t max_chunks);
 int32_t esg_scores_len(const esg_scorer* scorer, uint64_t len);
 /* GpuScorer::half2_scores_len (cuda/mod.rs:509-514), the fast kernel's
  * share: 1 when a query of `len` bases goes to the batched int16x2 kernel
- * (ESG_KERNEL_AUTO, inside its value bound), 0 when it goes to the int32
- * kernel. */
+ * (ESG_KERNEL_AUTO; in semi-global mode while its gap floor
+ * 2 |open| + (min(len, longest reference) - 1) |extend| stays under 15000),
+ * 0 when it goes to the int32 lanes.  A query the batched kernel takes may
+ * still be flagged there and re-scored in int32. */
 int32_t esg_batched_takes(const esg_scorer* scorer, uint64_t len);
 
 /* GpuScorer::score_batch (cuda/mod.rs:524-528): prepare + submit + finish.

@@ -220,8 +220,14 @@ def test_gpu_int16_saturation_is_rescored_in_int32(oracle):
     # the re-score requests also come through the panel-chunk merge
     assert st[(KERNEL_AUTO, 512, 64)]["panel_chunks"] > 1
     assert st[KERNEL_AUTO]["queries_batched"] == 2 * len(reads)
+    # semi-global: the checked batched kernel takes every query (the gap
+    # floor stays inside int16) and flags those whose cells pass 16384
     st = check(oracle, panel, reads, scoring, Mode.SEMIGLOBAL, "saturating semi-global")
-    assert st[KERNEL_AUTO]["queries_plain"] == 2 * len(reads)
+    assert st[KERNEL_AUTO]["queries_batched"] == 2 * len(reads)
+    assert st[KERNEL_AUTO]["queries_plain"] == 0
+    for key in ((KERNEL_AUTO, 512, 64), (KERNEL_AUTO, 512, 1), (KERNEL_AUTO, 0, 64),
+                (KERNEL_AUTO, 0, 1)):
+        assert st[key]["queries_rescored"] >= 9, key
 
 
 def test_gpu_ties_truncated_and_counted_in_full(oracle):
@@ -348,11 +354,14 @@ def test_gpu_half2_lever_and_introspection(oracle):
         slow = g.score_batch(reads, both_strands=True, full_rows=True)
         assert slow.stats["queries_plain"] == 2 * len(reads)
         assert np.array_equal(fast.rows, slow.rows)
-    # semi-global past the batched kernel's value bound goes to int32: the
-    # bound is min(read, reference) x max |match|, |mismatch| plus the gaps
+    # semi-global queries whose gap floor 2 |o| + (min(read, reference) - 1)
+    # |e| leaves the int16 lanes' range go to int32; inside it the batched
+    # kernel takes them (checked when their scores may pass int16)
     assert max(len(p) for p in panel) >= 125
-    with GpuScorer(panel, Scoring(100, -100, -27, -27), Mode.SEMIGLOBAL) as g:
+    with GpuScorer(panel, Scoring(100, -100, -27, -127), Mode.SEMIGLOBAL) as g:
         assert g.half2_scores_len(10) and not g.half2_scores_len(400)
+    with GpuScorer(panel, Scoring(100, -100, -27, -27), Mode.SEMIGLOBAL) as g:
+        assert g.half2_scores_len(10) and g.half2_scores_len(400)
 
 
 def test_gpu_panel_shards_merge_to_the_whole_panel(oracle):

@@ -76,15 +76,22 @@ def test_gpu_c3_sample_on_the_full_panel(oracle, c3_panel):
     assert_same(res.results, res.ties, want, want_t, CAP, "C3 sample")
 
 
-def test_gpu_c3_shape_saturating_scheme(oracle, c3_panel):
+@pytest.mark.parametrize("mode", [Mode.LOCAL, Mode.SEMIGLOBAL])
+def test_gpu_c3_shape_saturating_scheme(oracle, c3_panel, mode):
     """The C3 shape with a scheme whose long exact matches leave int16
-    (100,-100,-27,-27: a 500-nt match scores 50 000): flagged queries are
-    re-scored in int32 and every result equals the scalar oracle's."""
+    (100,-100,-27,-27: a 500-nt match scores 50 000): the batched kernel
+    takes the queries, flags those that may have wrapped, the int32 lanes
+    re-score them, and every result equals the scalar oracle's."""
     refs = c3_panel[:400]
     reads = synth.reads_c3(refs, n=24, seed=0x5EED_0C3F)
     scoring = (100, -100, -27, -27)
-    with GpuScorer(refs, Scoring(*scoring), Mode.LOCAL) as g:
+    with GpuScorer(refs, Scoring(*scoring), mode) as g:
         res = g.score_batch(reads.tuple(), both_strands=True)
+    if mode == Mode.LOCAL:
+        assert res.stats["queries_batched"] == 2 * len(reads)
+    else:  # reads past the semi-global gap floor's bound go to the int32 lanes
+        assert 0 < res.stats["queries_batched"] < 2 * len(reads)
     assert res.stats["queries_rescored"] > 0
-    want, want_t, _ = oracle.scalar_map_batch(reads.list(), refs, scoring, True, True, cap=CAP)
-    assert_same(res.results, res.ties, want, want_t, CAP, "C3 saturating")
+    want, want_t, _ = oracle.scalar_map_batch(reads.list(), refs, scoring, mode == Mode.LOCAL,
+                                              True, cap=CAP)
+    assert_same(res.results, res.ties, want, want_t, CAP, f"C3 saturating {mode.label}")
