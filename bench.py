@@ -614,13 +614,14 @@ def common_line(a, ctx, value, ms_per_step, workload, extra_config, e2e, rooflin
 
 # ---------------------------------------------------------------- C2
 def run_c2(a, ctx, rank):
-    from eschalign_b200 import KERNEL_AUTO, KERNEL_PLAIN32, GpuScorer, Mode, Scoring, synth
+    from eschalign_b200 import (KERNEL_AUTO, KERNEL_INT32, KERNEL_PLAIN32, GpuScorer, Mode,
+                                Scoring, synth)
     world, local_rank = ctx.world, ctx.local_rank
     refs = synth.panel_tiles()
     panel_bases = sum(len(r) for r in refs)
     if a.profile_case:
         reads = synth.reads_c2(refs, n=a.profile_case)
-        for kernel in (KERNEL_AUTO, KERNEL_PLAIN32):
+        for kernel in (KERNEL_AUTO, KERNEL_INT32, KERNEL_PLAIN32):
             g = GpuScorer(refs, Scoring(*HEADLINE[0]), Mode.parse(a.mode), device=local_rank,
                           kernel=kernel)
             if a.split >= 0:
@@ -676,17 +677,23 @@ def run_c2(a, ctx, rank):
             g2.close()
         combos[f"{mode} {','.join(map(str, scoring))}"] = round(value, 1)
         extras["gcups_by_combo"] = combos
-        # the plain one-thread-per-pair kernel on a sample of the same batch
+        # the int32 arms on a sample of the same batch: every query on the
+        # int32 lanes, and int32 one thread per (query, reference) -- the
+        # plain kernel's design; results equal the batched kernel's
         sub = reads.slice(0, min(a.plain_reads, len(reads)))
-        g.set_kernel(KERNEL_PLAIN32)
-        bp = g.submit(g.prepare(sub.tuple(), both_strands=True))
-        rp = g.finish(bp, keep=True)
-        tp = ctx.max_over_ranks(ctx.device_time(g, bp, 1, 1))
-        plain = world * rp.stats["cells"] / tp / 1e9
-        bp.free()
+        for kernel, key in ((KERNEL_INT32, "int32_lanes_gcups"), (KERNEL_PLAIN32, "plain_gcups")):
+            g.set_kernel(kernel)
+            bp = g.submit(g.prepare(sub.tuple(), both_strands=True))
+            rp = g.finish(bp, keep=True)
+            tp = ctx.max_over_ranks(ctx.device_time(g, bp, 1, 1))
+            extras[key] = world * rp.stats["cells"] / tp / 1e9
+            n_sub = len(sub)
+            parity[f"{key[:-6]}_equals_batched"] = same_results(
+                rp.results, rp.ties, first.results[:n_sub], first.ties[:n_sub])
+            bp.free()
         g.set_kernel(KERNEL_AUTO)
-        extras["plain_gcups"] = plain
-        extras["batched_over_plain"] = value / plain
+        extras["batched_over_plain"] = value / extras["plain_gcups"]
+        extras["batched_over_int32_lanes"] = value / extras["int32_lanes_gcups"]
         extras["plain_sample"] = f"first {len(sub)} reads, both strands"
         extras["traceback"] = traceback_stage(g, refs, sub, scoring, mode == "local",
                                               a.no_cpu_baseline or rank != 0 or world != 1)
@@ -695,12 +702,14 @@ def run_c2(a, ctx, rank):
         arms = reference_gpu_arms(refs, sub, scoring, mode == "local", local_rank)
         if arms:
             arms["batched_over_ref_half2"] = value / arms["half2_gcups"]
+            # the reference's own one-thread-per-pair int kernel
+            arms["batched_over_ref_int"] = value / arms["int_gcups"]
             extras["reference_gpu_kernels"] = arms
 
     chunks = [reads.slice(k, k + a.chunk) for k in range(0, len(reads), a.chunk)]
     te, n_pass, h2d, d2h = feeder(
         ctx, chunks, lambda c: g.prepare(c.tuple(), both_strands=True), g.submit,
-        lambda b: g.finish(b).stats, max(1, min(2, a.steps)))
+        lambda b: g.finish(b).stats, max(1, a.steps))
     e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "reads_per_s": world * len(reads) * n_pass / te, "chunk_reads": a.chunk,
