@@ -183,6 +183,7 @@ SIGNATURES = {
     "esg_batch_free": (None, [C.c_void_p]),
     "esg_batch_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(EsgBatchStats)]),
     "esg_relaunch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "esg_scorer_set_graphs": (C.c_int32, [C.c_void_p, C.c_int32]),
     "esg_batch_read_results": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, _u32p]),
     "esg_pair_adapters": (C.c_int32, [_u8p, _u64p, _u32p, C.c_uint32,
                                       C.POINTER(EsgAdapterConfig), _u32p, _u32p]),

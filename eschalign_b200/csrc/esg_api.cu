@@ -165,6 +165,11 @@ struct esg_scorer {
   const void* k3_fn = nullptr;
   PinnedPool pinned;
   esg_info info{};
+  // CUDA graphs of batches' launch sequences: one instantiated graph per
+  // sequence shape (which kernels a batch launches), updated in place with
+  // each batch's parameters before it is launched
+  bool use_graphs = true;
+  std::vector<std::pair<uint32_t, cudaGraphExec_t>> graph_execs;
 };
 
 struct esg_batch {
@@ -227,6 +232,8 @@ struct esg_batch {
   int4* d_pairs = nullptr;
   uint32_t* d_pties = nullptr;
   cudaEvent_t done = nullptr;
+  cudaGraph_t graph = nullptr;  // this batch's launch sequence, captured at submit
+  uint32_t graph_key = 0;       // its shape
   bool submitted = false;
   esg_scorer* owner = nullptr;
   esg_batch_stats stats{};
@@ -234,6 +241,7 @@ struct esg_batch {
 
 extern "C" {
 static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t st);
+static esg_status launch_work(esg_scorer* sc, esg_batch* b, cudaStream_t st);
 }
 
 namespace {
@@ -769,6 +777,7 @@ void esg_scorer_free(esg_scorer* sc) {
   }
   if (sc->fork) cudaEventDestroy(sc->fork);
   if (sc->join) cudaEventDestroy(sc->join);
+  for (auto& ge : sc->graph_execs) cudaGraphExecDestroy(ge.second);
   if (sc->pool) cudaMemPoolDestroy(sc->pool);
   if (sc->own_stream && sc->stream) cudaStreamDestroy(sc->stream);
   delete sc;
@@ -1370,6 +1379,71 @@ static esg_status launch_device_work(esg_scorer* sc, esg_batch* b, cudaStream_t 
   return ESG_OK;
 }
 
+// The shape of a batch's launch sequence: which of its kernels run.  Batches
+// of one shape differ only in kernel parameters and sizes, which an
+// instantiated graph takes by update.
+static uint32_t work_key(const esg_scorer* sc, const esg_batch* b) {
+  const uint32_t nc = b->n_chunks;
+  const bool k3 = b->host_list + b->redo_cap > 0;
+  return (b->n_long ? 1u : 0u) | (b->n_t32 ? 2u : 0u) | (b->n_t16 ? 4u : 0u) |
+         ((b->n_tasks && nc > 1) ? 8u : 0u) | (k3 ? 16u : 0u) | (b->n_reads ? 32u : 0u) |
+         ((b->paired && b->n_pairs) ? 64u : 0u) | (b->sg_check ? 128u : 0u) |
+         (b->kernel == ESG_KERNEL_PLAIN32 ? 256u : 0u) | (sc->mode == ESG_MODE_LOCAL ? 512u : 0u);
+}
+
+// The batch's device work as one CUDA graph launch on `st`: the launch
+// sequence (counter reset, the three k2 groups on two streams joined by
+// events, chunk merge, k3 / k4, k5, k6) is captured from the scorer's
+// stream once per batch, and the scorer's instantiated graph of that shape
+// is updated with the batch's parameters and launched.  Work already in
+// flight from an earlier launch of the same graph keeps its own parameters.
+// A stream that is itself being captured by the caller, or the legacy
+// default stream (which cannot be captured), gets the launches directly.
+static esg_status launch_work(esg_scorer* sc, esg_batch* b, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (!sc->use_graphs || !sc->stream || cudaStreamIsCapturing(st, &cs) != cudaSuccess ||
+      cs != cudaStreamCaptureStatusNone ||
+      cudaStreamIsCapturing(sc->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return launch_device_work(sc, b, st);
+  if (!b->graph) {
+    ESG_CUDA(cudaStreamBeginCapture(sc->stream, cudaStreamCaptureModeThreadLocal));
+    const esg_status ls = launch_device_work(sc, b, sc->stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(sc->stream, &g);
+    if (ls != ESG_OK || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      if (ls != ESG_OK) return ls;
+      // the capture was refused: this scorer launches one by one from now on
+      sc->use_graphs = false;
+      return launch_device_work(sc, b, st);
+    }
+    b->graph = g;
+    b->graph_key = work_key(sc, b);
+  }
+  cudaGraphExec_t exec = nullptr;
+  for (auto& ge : sc->graph_execs) {
+    if (ge.first != b->graph_key) continue;
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(ge.second, b->graph, &info) == cudaSuccess) {
+      exec = ge.second;
+    } else {
+      cudaGetLastError();
+      cudaGraphExecDestroy(ge.second);
+      ge.second = nullptr;
+      ESG_CUDA(cudaGraphInstantiate(&ge.second, b->graph, 0));
+      exec = ge.second;
+    }
+    break;
+  }
+  if (!exec) {
+    ESG_CUDA(cudaGraphInstantiate(&exec, b->graph, 0));
+    sc->graph_execs.emplace_back(b->graph_key, exec);
+  }
+  ESG_CUDA(cudaGraphLaunch(exec, st));
+  return ESG_OK;
+}
+
 esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   g_err.clear();
   if (!sc || !b || b->owner != sc) return fail(ESG_ERR_BAD_ARGUMENT, "batch/scorer mismatch");
@@ -1410,7 +1484,7 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   // for the first seven buffers
   ESG_CUDA(cudaMemcpyAsync(b->d_codes, b->in_buf.p, b->in_bytes, cudaMemcpyHostToDevice, st));
   b->stats.h2d_bytes = b->in_bytes;
-  esg_status s = launch_device_work(sc, b, st);
+  esg_status s = launch_work(sc, b, st);
   if (s != ESG_OK) return s;
   // downloads into pinned staging
   const size_t out_bytes = carve_size(nr, 16) + carve_size(nr * sc->cap, 4) +
@@ -1451,7 +1525,14 @@ esg_status esg_relaunch(esg_scorer* sc, esg_batch* b, void* stream) {
     return fail(ESG_ERR_BAD_ARGUMENT, "relaunch needs a submitted batch of this scorer");
   ESG_CUDA(cudaSetDevice(sc->device));
   cudaStream_t st = stream ? (cudaStream_t)stream : sc->stream;
-  return launch_device_work(sc, b, st);
+  return launch_work(sc, b, st);
+}
+
+esg_status esg_scorer_set_graphs(esg_scorer* sc, int32_t enabled) {
+  g_err.clear();
+  if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");
+  sc->use_graphs = enabled != 0;
+  return ESG_OK;
 }
 
 esg_status esg_batch_read_results(esg_scorer* sc, esg_batch* b, esg_read_result* results,
@@ -1503,6 +1584,7 @@ void esg_batch_free(esg_batch* b) {
       cudaEventDestroy(b->done);
     }
     if (b->d_mem) cudaFreeAsync(b->d_mem, sc->stream);
+    if (b->graph) cudaGraphDestroy(b->graph);
     sc->pinned.put(b->in_buf.p, b->in_buf.cap);
     sc->pinned.put(b->out_buf.p, b->out_buf.cap);
   }

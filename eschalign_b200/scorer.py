@@ -419,6 +419,11 @@ class GpuScorer:
     def set_split(self, split_len: int):
         _check(self._lib, self._lib.esg_scorer_set_split(self._h, int(split_len)))
 
+    def set_graphs(self, enabled: bool):
+        """Launch each batch's device work as one CUDA graph (default) or
+        kernel by kernel; results are the same."""
+        _check(self._lib, self._lib.esg_scorer_set_graphs(self._h, int(bool(enabled))))
+
     def set_chunking(self, max_chunks: int):
         """Cap the panel chunks per tile (1: every task walks the whole panel)."""
         _check(self._lib, self._lib.esg_scorer_set_chunking(self._h, int(max_chunks)))

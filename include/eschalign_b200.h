@@ -234,6 +234,16 @@ esg_status esg_batch_stats_get(const esg_batch* batch, esg_batch_stats* out);
  * scorer's) with its inputs already resident, no copies.  For measuring the
  * kernels alone; the batch's results are overwritten with identical ones. */
 esg_status esg_relaunch(esg_scorer* scorer, esg_batch* batch, void* stream);
+/* A batch's device work (counter reset, the batched kernel's three task
+ * groups on two streams, the chunk merge, the int32 path, the per-read
+ * merge, the pair ranking) is captured once as a CUDA graph at esg_submit
+ * and launched as one graph, by esg_submit and esg_relaunch; the scorer
+ * keeps one instantiated graph per launch-sequence shape and updates it
+ * with each batch's parameters.  No counterpart in the reference, which
+ * launches its kernels one by one (cuda/mod.rs:581-699).  enabled = 0
+ * launches the kernels one by one instead; results are the same.  A
+ * scorer whose stream the caller is capturing launches one by one. */
+esg_status esg_scorer_set_graphs(esg_scorer* scorer, int32_t enabled);
 /* Copy a submitted batch's per-read results and ties as they stand in device
  * memory now -- after esg_relaunch, the last launch's -- into the caller's
  * buffers (ties may be NULL), after the device has finished its work.  No

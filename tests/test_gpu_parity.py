@@ -387,3 +387,36 @@ def test_gpu_panel_shards_merge_to_the_whole_panel(oracle):
     for f in ("best", "suboptimal", "n_tied", "flags"):
         assert np.array_equal(got_r[f], want.results[f]), f
     assert np.array_equal(got_t, want.ties)
+
+
+def test_gpu_graph_launches_equal_direct_launches(oracle):
+    """A batch's device work launched as one CUDA graph (the default) and
+    kernel by kernel give the same results; relaunching a submitted batch
+    through its graph leaves them unchanged; batches of other shapes in
+    between (long reads, a chunked small batch) update or add graphs without
+    disturbing the others."""
+    refs = synth.panel_tiles()
+    reads = synth.reads_c2(refs, n=5000)
+    small = synth.reads_c2(refs, n=40, seed=99)
+    rng = Rng(0x5EED_0A12)
+    longs = [encode(random_seq(rng, 1500 + 100 * k, 0.0)) for k in range(3)]
+    for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+        with GpuScorer(refs, Scoring(), mode) as g:
+            got = [g.score_batch(x, both_strands=True)
+                   for x in (reads.tuple(), longs, small.tuple(), reads.tuple())]
+            g.set_graphs(False)
+            want = [g.score_batch(x, both_strands=True)
+                    for x in (reads.tuple(), longs, small.tuple(), reads.tuple())]
+            for a, b in zip(got, want):
+                assert (a.results == b.results).all() and (a.ties == b.ties).all()
+            assert got[1].stats["queries_batched"] == 2 * len(longs)
+            assert got[2].stats["panel_chunks"] > 1
+            g.set_graphs(True)
+            pb = g.submit(g.prepare(reads.tuple(), both_strands=True))
+            first = g.finish(pb, keep=True)
+            g.score_batch(small.tuple(), both_strands=True)  # another shape in between
+            g.relaunch(pb)
+            res, ties = g.read_results(pb)
+            pb.free()
+            assert (res == first.results).all() and (ties == first.ties).all()
+            assert (first.results == want[0].results).all()
