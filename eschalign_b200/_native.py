@@ -94,7 +94,14 @@ class EsgInfo(C.Structure):
 class EsgTuneReport(C.Structure):
     _fields_ = [("n_lengths", C.c_uint32), ("lengths", C.c_uint32 * 8),
                 ("ms_rows16", C.c_float * 8), ("ms_rows32", C.c_float * 8),
-                ("split_len", C.c_uint32)]
+                ("split_len", C.c_uint32), ("ms_int32", C.c_float * 8),
+                ("int32_from", C.c_uint32),
+                ("n_ctas16", C.c_uint32), ("cand_ctas16", C.c_uint32 * 4),
+                ("ms_ctas16", C.c_float * 4), ("ctas16", C.c_uint32),
+                ("n_ctas32", C.c_uint32), ("cand_ctas32", C.c_uint32 * 4),
+                ("ms_ctas32", C.c_float * 4), ("ctas32", C.c_uint32),
+                ("n_chunk_targets", C.c_uint32), ("chunk_targets", C.c_uint32 * 8),
+                ("ms_chunks", C.c_float * 8), ("chunk_target", C.c_uint32)]
 
 
 class EsgBatchStats(C.Structure):

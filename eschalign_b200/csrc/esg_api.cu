@@ -140,6 +140,12 @@ struct esg_scorer {
   // stripes (esg_scorer_autotune measures where 32 rows start to win)
   uint32_t split_len = 256;
   bool tuned = false;
+  // queries of this length and longer go to the int32 lanes instead of the
+  // batched kernel (0: none; set by the autotuner where the batched kernel
+  // would flag most of them)
+  uint32_t int32_from = 0;
+  // panel chunking aims for this many tasks per resident warp
+  uint32_t chunk_target = 8;
   uint32_t max_chunks = 64;  // panel chunks per tile at most (1: never chunk)
   cudaStream_t aux = nullptr;          // second stream: the long-query kernel
   // batches' device memory: a pool of this scorer's own that keeps what
@@ -806,7 +812,8 @@ esg_status esg_scorer_set_kernel(esg_scorer* sc, int32_t kernel) {
 int32_t esg_scores_len(const esg_scorer* sc, uint64_t len) { return sc && len > 0; }
 
 int32_t esg_batched_takes(const esg_scorer* sc, uint64_t len) {
-  return sc && sc->kernel == ESG_KERNEL_AUTO && k2_takes(sc, len);
+  return sc && sc->kernel == ESG_KERNEL_AUTO && !(sc->int32_from && len >= sc->int32_from) &&
+         k2_takes(sc, len);
 }
 
 esg_status esg_scorer_set_chunking(esg_scorer* sc, uint32_t max_chunks) {
@@ -825,77 +832,140 @@ esg_status esg_scorer_set_split(esg_scorer* sc, uint32_t split_len) {
   return ESG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Calibration batch of the autotuner: n reads of L +- 25 % bases, nine in
+// ten cut from the panel's references with 8 % substitutions (shorter
+// references padded with random bases) and one in ten random, so the batch
+// packs, scores and flags as reads of this panel do.
+struct Calib {
+  std::vector<uint8_t> codes;
+  std::vector<uint64_t> off;
+  std::vector<uint32_t> len;
+  uint32_t n = 0;
+};
+
+void calib_reads(const esg_scorer* sc, uint32_t L, uint32_t n, uint64_t& x, Calib& c) {
+  auto next = [&x]() {  // xorshift64*
+    x ^= x >> 12;
+    x ^= x << 25;
+    x ^= x >> 27;
+    return x * 0x2545F4914F6CDD1Dull;
+  };
+  c.n = n;
+  c.off.assign(n, 0);
+  c.len.assign(n, 0);
+  c.codes.clear();
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t len = L - L / 4 + (uint32_t)(next() % (L / 2 + 1));
+    c.off[k] = c.codes.size();
+    c.len[k] = len;
+    const bool derived = next() % 10 != 0;
+    const uint32_t r = (uint32_t)(next() % sc->n_refs);
+    const uint32_t m = sc->len_of[r];
+    const uint32_t start = m > len ? (uint32_t)(next() % (m - len + 1)) : 0u;
+    for (uint32_t i = 0; i < len; ++i) {
+      uint8_t b = (uint8_t)(next() >> 62);
+      if (derived && start + i < m && next() % 100 >= 8) b = sc->h_codes[sc->h_off[r] + start + i];
+      c.codes.push_back(b);
+    }
+  }
+}
+
+}  // namespace
+
+// Device time (ms) of a calibration batch's work under the scorer's current
+// settings: prepared and submitted once, then launched twice more, timed.
+static esg_status time_calib(esg_scorer* sc, const Calib& c, cudaEvent_t e0, cudaEvent_t e1,
+                             float* ms) {
+  esg_batch* b = nullptr;
+  esg_status st =
+      esg_prepare(sc, c.codes.data(), c.off.data(), c.len.data(), c.n, ESG_BOTH_STRANDS, &b);
+  if (st == ESG_OK) st = esg_submit(sc, b);
+  if (st == ESG_OK) st = esg_finish(sc, b, nullptr, nullptr, nullptr);
+  if (st == ESG_OK) {
+    cudaEventRecord(e0, sc->stream);
+    for (int i = 0; i < 2 && st == ESG_OK; ++i) st = launch_work(sc, b, sc->stream);
+    cudaEventRecord(e1, sc->stream);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    *ms /= 2;
+  }
+  esg_batch_free(b);
+  return st;
+}
+
+extern "C" {
+
 esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
   g_err.clear();
   if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");
   esg_tune_report rep{};
+  rep.chunk_target = sc->chunk_target;
+  rep.ctas16 = sc->blocks_t16 / std::max(1, sc->sm_count);
+  rep.ctas32 = sc->blocks_t32 / std::max(1, sc->sm_count);
   if (!sc->batched_ok || sc->kernel != ESG_KERNEL_AUTO) {
     rep.split_len = sc->split_len;
+    rep.int32_from = sc->int32_from;
     if (out) *out = rep;
     return ESG_OK;
   }
   ESG_CUDA(cudaSetDevice(sc->device));
   static const uint32_t kLens[] = {48, 80, 112, 160, 224, 320, 448};
   const uint32_t n_lens = sizeof(kLens) / sizeof(kLens[0]);
-  const uint32_t keep = sc->split_len;
-  uint64_t x = 0x9e3779b97f4a7c15ull;  // xorshift64* calibration reads
+  const uint32_t keep_split = sc->split_len, keep_from = sc->int32_from;
+  const int keep16 = sc->blocks_t16, keep32 = sc->blocks_t32;
+  const uint32_t keep_target = sc->chunk_target;
+  auto restore = [&]() {
+    sc->split_len = keep_split;
+    sc->int32_from = keep_from;
+    sc->kernel = ESG_KERNEL_AUTO;
+    sc->blocks_t16 = keep16;
+    sc->blocks_t32 = keep32;
+    sc->chunk_target = keep_target;
+  };
+  uint64_t x = 0x9e3779b97f4a7c15ull;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   ESG_CUDA(cudaEventCreate(&e0));
   ESG_CUDA(cudaEventCreate(&e1));
   esg_status st = ESG_OK;
+  Calib c;
+  // about 2e10 cells per batch (a few ms of device time), both strands
+  auto reads_for = [&](uint32_t L) {
+    const uint64_t want = (uint64_t)(2.0e10 / (2.0 * L * (double)sc->panel_bases));
+    return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 64), 200000);
+  };
+  sc->int32_from = 0;
+  // 1. per read length: 16-row stripes, 32-row stripes, the int32 lanes
   for (uint32_t li = 0; li < n_lens && st == ESG_OK; ++li) {
     const uint32_t L = kLens[li];
-    // about 2e10 cells per batch (a few ms of device time), both strands
-    const uint64_t want = (uint64_t)(2.0e10 / (2.0 * L * (double)sc->panel_bases));
-    const uint32_t n = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 512), 200000);
-    // lengths spread over L +- 25 %, as a real batch has, so the tiles pack
-    // as they would in use
-    auto next = [&x]() {
-      x ^= x >> 12;
-      x ^= x << 25;
-      x ^= x >> 27;
-      return x * 0x2545F4914F6CDD1Dull;
-    };
-    std::vector<uint64_t> off(n);
-    std::vector<uint32_t> len(n);
-    uint64_t total = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-      len[k] = L - L / 4 + (uint32_t)(next() % (L / 2 + 1));
-      off[k] = total;
-      total += len[k];
-    }
-    std::vector<uint8_t> codes(total);
-    for (auto& c : codes) c = (uint8_t)(next() >> 62);
-    float ms[2] = {0, 0};
-    for (int cfg = 0; cfg < 2 && st == ESG_OK; ++cfg) {
+    calib_reads(sc, L, reads_for(L), x, c);
+    float ms[3] = {0, 0, 0};
+    for (int cfg = 0; cfg < 3 && st == ESG_OK; ++cfg) {
       sc->split_len = cfg == 0 ? 512u : 0u;
-      esg_batch* b = nullptr;
-      st = esg_prepare(sc, codes.data(), off.data(), len.data(), n, ESG_BOTH_STRANDS, &b);
-      if (st == ESG_OK) st = esg_submit(sc, b);
-      if (st == ESG_OK) st = esg_finish(sc, b, nullptr, nullptr, nullptr);
-      if (st == ESG_OK) {
-        cudaEventRecord(e0, sc->stream);
-        for (int rep_i = 0; rep_i < 2 && st == ESG_OK; ++rep_i) st = launch_device_work(sc, b, sc->stream);
-        cudaEventRecord(e1, sc->stream);
-        cudaEventSynchronize(e1);
-        cudaEventElapsedTime(&ms[cfg], e0, e1);
-        ms[cfg] /= 2;
-      }
-      esg_batch_free(b);
+      sc->kernel = cfg == 2 ? ESG_KERNEL_INT32 : ESG_KERNEL_AUTO;
+      st = time_calib(sc, c, e0, e1, &ms[cfg]);
     }
+    sc->kernel = ESG_KERNEL_AUTO;
     rep.lengths[li] = L;
     rep.ms_rows16[li] = ms[0];
     rep.ms_rows32[li] = ms[1];
+    rep.ms_int32[li] = ms[2];
     rep.n_lengths = li + 1;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   if (st != ESG_OK) {
-    sc->split_len = keep;
+    restore();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return st;
   }
   // 16-row stripes up to the last length where they are at least as fast,
-  // counting from the shortest; 32-row stripes from the first length they win
+  // counting from the shortest; 32-row stripes from the first length they
+  // win.  The int32 lanes from the length where they win at it and every
+  // longer length (a scheme whose long queries mostly flag, to be scored
+  // twice by the batched kernel), else never.
   uint32_t split = 0;
   for (uint32_t li = 0; li < rep.n_lengths; ++li) {
     if (rep.ms_rows16[li] <= rep.ms_rows32[li])
@@ -904,11 +974,79 @@ esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
       break;
   }
   if (split == kLens[n_lens - 1]) split = 512;
+  uint32_t from = 0;
+  for (int li = (int)rep.n_lengths - 1; li >= 0; --li) {
+    if (rep.ms_int32[li] < std::min(rep.ms_rows16[li], rep.ms_rows32[li]))
+      from = rep.lengths[li];
+    else
+      break;
+  }
+  // 2. resident CTAs per SM of the 16-row tiles (112-nt reads) and the
+  //    32-row tiles (448-nt reads): the occupancy limit and one or two fewer
+  for (int which = 0; which < 2 && st == ESG_OK; ++which) {
+    const uint32_t L = which == 0 ? 112u : 448u;
+    calib_reads(sc, L, reads_for(L), x, c);
+    sc->split_len = which == 0 ? 512u : 0u;
+    int& blocks = which == 0 ? sc->blocks_t16 : sc->blocks_t32;
+    const int occ = (which == 0 ? keep16 : keep32) / std::max(1, sc->sm_count);
+    uint32_t* cand = which == 0 ? rep.cand_ctas16 : rep.cand_ctas32;
+    float* tms = which == 0 ? rep.ms_ctas16 : rep.ms_ctas32;
+    uint32_t& n_c = which == 0 ? rep.n_ctas16 : rep.n_ctas32;
+    float best = 0;
+    int pick = occ;
+    for (int k = occ; k >= std::max(1, occ - 2) && st == ESG_OK; --k) {
+      blocks = k * sc->sm_count;
+      float ms = 0;
+      st = time_calib(sc, c, e0, e1, &ms);
+      cand[n_c] = (uint32_t)k;
+      tms[n_c] = ms;
+      ++n_c;
+      if (k == occ || ms < best) {
+        best = ms;
+        pick = k;
+      }
+    }
+    blocks = pick * sc->sm_count;
+    (which == 0 ? rep.ctas16 : rep.ctas32) = (uint32_t)pick;
+  }
   sc->split_len = split;
+  // 3. panel chunking: a batch of about one read per resident warp (too few
+  //    tiles to fill the GPU), chunked to aim for 1-16 tasks per resident warp
+  if (st == ESG_OK) {
+    calib_reads(sc, 112, (uint32_t)std::max(64, sc->blocks_t16 * kK2Warps), x, c);
+    static const uint32_t kTargets[] = {1, 2, 4, 8, 16};
+    float best = 0;
+    uint32_t pick = keep_target;
+    for (uint32_t t : kTargets) {
+      if (st != ESG_OK) break;
+      sc->chunk_target = t;
+      float ms = 0;
+      st = time_calib(sc, c, e0, e1, &ms);
+      rep.chunk_targets[rep.n_chunk_targets] = t;
+      rep.ms_chunks[rep.n_chunk_targets] = ms;
+      ++rep.n_chunk_targets;
+      if (rep.n_chunk_targets == 1 || ms < best) {
+        best = ms;
+        pick = t;
+      }
+    }
+    sc->chunk_target = pick;
+    rep.chunk_target = pick;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != ESG_OK) {
+    restore();
+    return st;
+  }
+  sc->split_len = split;
+  sc->int32_from = from;
   sc->tuned = true;
   sc->info.split_len = split;
   sc->info.tuned = 1;
+  sc->info.batched_blocks = sc->blocks_t16;
   rep.split_len = split;
+  rep.int32_from = from;
   if (out) *out = rep;
   return ESG_OK;
 }
@@ -958,7 +1096,8 @@ static esg_status prepare_impl(esg_scorer* sc, const uint8_t* const* ptrs, const
       continue;
     }
     cells += (uint64_t)n * sc->panel_bases;
-    if (b->kernel == ESG_KERNEL_AUTO && k2_takes(sc, n)) {
+    const bool lanes32 = sc->int32_from && n >= sc->int32_from;
+    if (b->kernel == ESG_KERNEL_AUTO && !lanes32 && k2_takes(sc, n)) {
       if (n <= split)
         q16.push_back({(n + 15) / 16, q});
       else if (n <= 32 * kMaxStripes)
@@ -992,7 +1131,8 @@ static esg_status prepare_impl(esg_scorer* sc, const uint8_t* const* ptrs, const
   // the per-chunk query states are merged afterwards
   {
     const uint64_t tiles = b->n_tasks;
-    const uint64_t target = 8ull * (uint64_t)std::max(sc->blocks_t16, 1) * kK2Warps;
+    const uint64_t target =
+        (uint64_t)sc->chunk_target * (uint64_t)std::max(sc->blocks_t16, 1) * kK2Warps;
     uint32_t nc = 1;
     if (tiles && tiles < target) nc = (uint32_t)((target + tiles - 1) / tiles);
     nc = std::min<uint32_t>(nc, std::max<uint32_t>(1, sc->n_pairs / 4));

@@ -408,13 +408,26 @@ class GpuScorer:
         return bool(self._lib.esg_batched_takes(self._h, int(n)))
 
     def autotune(self) -> dict:
-        """Measure the 16/32-row stripe split on this panel (esg_scorer_autotune)."""
+        """Measure the tile shape on this panel (esg_scorer_autotune): the
+        16/32-row stripe split, the length from which the int32 lanes take
+        over, resident CTAs per SM, the panel-chunk target."""
         rep = _native.EsgTuneReport()
         _check(self._lib, self._lib.esg_scorer_autotune(self._h, C.byref(rep)))
         n = rep.n_lengths
+
+        def ms(a, k):
+            return [round(v, 3) for v in a[:k]]
+
         return {"split_len": rep.split_len, "lengths": list(rep.lengths[:n]),
-                "ms_rows16": [round(v, 3) for v in rep.ms_rows16[:n]],
-                "ms_rows32": [round(v, 3) for v in rep.ms_rows32[:n]]}
+                "ms_rows16": ms(rep.ms_rows16, n), "ms_rows32": ms(rep.ms_rows32, n),
+                "ms_int32": ms(rep.ms_int32, n), "int32_from": rep.int32_from,
+                "ctas16": {"tried": list(rep.cand_ctas16[:rep.n_ctas16]),
+                           "ms": ms(rep.ms_ctas16, rep.n_ctas16), "chosen": rep.ctas16},
+                "ctas32": {"tried": list(rep.cand_ctas32[:rep.n_ctas32]),
+                           "ms": ms(rep.ms_ctas32, rep.n_ctas32), "chosen": rep.ctas32},
+                "chunk_target": {"tried": list(rep.chunk_targets[:rep.n_chunk_targets]),
+                                 "ms": ms(rep.ms_chunks, rep.n_chunk_targets),
+                                 "chosen": rep.chunk_target}}
 
     def set_split(self, split_len: int):
         _check(self._lib, self._lib.esg_scorer_set_split(self._h, int(split_len)))

@@ -106,15 +106,29 @@ typedef struct esg_info {
     int32_t tuned;            /* split_len was measured by esg_scorer_autotune   */
 } esg_info;
 
-/* What esg_scorer_autotune measured: device time of the batched kernels on
- * calibration batches of each read length, with 16-row and 32-row stripes. */
+/* What esg_scorer_autotune measured (device time of calibration batches
+ * cut from this panel) and chose.  Scores do not depend on any choice. */
 #define ESG_TUNE_MAX_LENGTHS 8
 typedef struct esg_tune_report {
     uint32_t n_lengths;
-    uint32_t lengths[ESG_TUNE_MAX_LENGTHS];
-    float ms_rows16[ESG_TUNE_MAX_LENGTHS];
-    float ms_rows32[ESG_TUNE_MAX_LENGTHS];
-    uint32_t split_len;
+    uint32_t lengths[ESG_TUNE_MAX_LENGTHS];   /* read lengths (each batch +-25 %)      */
+    float ms_rows16[ESG_TUNE_MAX_LENGTHS];    /* batched kernel, 16-row stripes        */
+    float ms_rows32[ESG_TUNE_MAX_LENGTHS];    /* batched kernel, 32-row stripes        */
+    uint32_t split_len;                       /* chosen: 16-row stripes up to this     */
+    float ms_int32[ESG_TUNE_MAX_LENGTHS];     /* every query on the int32 lanes        */
+    uint32_t int32_from;                      /* chosen: int32 lanes from this length (0: never) */
+    uint32_t n_ctas16;                        /* resident CTAs per SM tried, 16-row tiles */
+    uint32_t cand_ctas16[4];
+    float ms_ctas16[4];
+    uint32_t ctas16;                          /* chosen                                 */
+    uint32_t n_ctas32;                        /* the same for 32-row tiles              */
+    uint32_t cand_ctas32[4];
+    float ms_ctas32[4];
+    uint32_t ctas32;
+    uint32_t n_chunk_targets;                 /* panel-chunk targets tried (tasks per resident warp) */
+    uint32_t chunk_targets[8];
+    float ms_chunks[8];
+    uint32_t chunk_target;                    /* chosen                                 */
 } esg_tune_report;
 
 typedef struct esg_batch_stats {
@@ -175,10 +189,15 @@ esg_status esg_scorer_info(const esg_scorer* scorer, esg_info* out);
  * (32 x max_ref_len x 8 bytes per warp, at most 1 GiB). */
 esg_status esg_scorer_set_kernel(esg_scorer* scorer, int32_t kernel);
 /* Tile-shape autotuner (no counterpart in the reference, whose one kernel
- * shape is fixed): times the batched kernels on synthetic calibration
- * batches of read lengths 48..448 (each +-25 %) against this panel, with 16-row and
- * 32-row stripes per lane, and sets the length up to which 16-row stripes
- * are used.  Scores do not depend on the choice.  `out` may be NULL. */
+ * shape is fixed, cuda/mod.rs:238-301).  On calibration batches cut from
+ * this panel (read lengths 48..448, each +-25 %) it times the batched kernel
+ * with 16-row and with 32-row stripes and every query on the int32 lanes,
+ * and sets the length up to which 16-row stripes are used and the length
+ * from which queries go to the int32 lanes (where the batched kernel would
+ * flag most of them); then the resident CTAs per SM of the 16- and 32-row
+ * tiles (the occupancy limit and one or two fewer) and the panel-chunk
+ * target for batches too small to fill the GPU.  Scores do not depend on
+ * the choices.  `out` may be NULL. */
 esg_status esg_scorer_autotune(esg_scorer* scorer, esg_tune_report* out);
 /* Set the 16/32-row split by hand (0: every query on 32-row stripes). */
 esg_status esg_scorer_set_split(esg_scorer* scorer, uint32_t split_len);

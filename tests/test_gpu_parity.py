@@ -326,8 +326,13 @@ def test_gpu_autotune_measures_and_keeps_results(oracle):
     with GpuScorer(refs, Scoring(), Mode.LOCAL) as g:
         before = g.score_batch(reads.tuple(), both_strands=True)
         rep = g.autotune()
-        assert len(rep["lengths"]) == 7 and all(t > 0 for t in rep["ms_rows16"] + rep["ms_rows32"])
+        assert len(rep["lengths"]) == 7 and all(
+            t > 0 for t in rep["ms_rows16"] + rep["ms_rows32"] + rep["ms_int32"])
         assert rep["split_len"] in (0, 48, 80, 112, 160, 224, 320, 512)
+        # int16x2 lanes beat int32 lanes on this scheme at every length
+        assert rep["int32_from"] == 0
+        for knob in ("ctas16", "ctas32", "chunk_target"):
+            assert rep[knob]["chosen"] in rep[knob]["tried"] and all(t > 0 for t in rep[knob]["ms"])
         info = g.info()
         assert info["tuned"] == 1 and info["split_len"] == rep["split_len"]
         after = g.score_batch(reads.tuple(), both_strands=True)
@@ -420,3 +425,26 @@ def test_gpu_graph_launches_equal_direct_launches(oracle):
             pb.free()
             assert (res == first.results).all() and (ties == first.ties).all()
             assert (first.results == want[0].results).all()
+
+
+def test_gpu_autotune_sends_flagging_lengths_to_int32_lanes(oracle):
+    """With a scheme whose long reads leave int16 (100,-100,-27,-27 on a
+    panel of ~500-nt references) the batched kernel would flag most long
+    queries and score them twice: the autotuner measures the int32 lanes
+    faster there and routes those lengths to them; results stay exact."""
+    rng = Rng(0x5EED_0A13)
+    letters = random_panel(rng, 60, 480, 40)
+    panel = [encode(s) for s in letters]
+    reads = [encode(letters[k][5:60 + 9 * k]) for k in range(50)]
+    reads += [encode(random_seq(rng, 50 + 8 * k, 0.0)) for k in range(10)]
+    scoring = (100, -100, -27, -27)
+    with GpuScorer(panel, Scoring(*scoring), Mode.LOCAL) as g:
+        rep = g.autotune()
+        assert rep["int32_from"] > 0, rep
+        res = g.score_batch(reads, both_strands=True, full_rows=True)
+        assert res.stats["queries_plain"] > 0 and res.stats["queries_batched"] > 0
+    want_rows = oracle_rows(oracle, reads, panel, scoring, True)
+    assert (res.rows == want_rows).all()
+    want, want_t, _ = oracle.scalar_map_batch(reads, panel, scoring, True, True, cap=CAP)
+    for f in ("best", "suboptimal", "n_tied"):
+        assert (res.results[f] == want[f]).all(), f
