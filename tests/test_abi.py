@@ -106,3 +106,39 @@ def test_mapping_entry_points_refuse_bad_arguments_on_any_host():
     assert lib.esg_mapping_pairs(None, ctypes.byref(n32)) is None and n32.value == 0
     assert lib.esg_mapping_pair_hits(None, ctypes.byref(n64)) is None
     lib.esg_mapping_free(None)
+
+
+# ctypes mirror -> the header's struct name
+_STRUCTS = {"EsgScoring": "esg_scoring", "EsgOptions": "esg_options", "EsgInfo": "esg_info",
+            "EsgTuneReport": "esg_tune_report", "EsgBatchStats": "esg_batch_stats",
+            "EsgAdapterConfig": "esg_adapter_config", "EsgAlignJob": "esg_align_job",
+            "EsgAlignment": "esg_alignment", "EsgMapOptions": "esg_map_options",
+            "EsgPairMapOptions": "esg_pair_map_options", "EsgServerOptions": "esg_server_options",
+            "EsgRequestTiming": "esg_request_timing", "EsgServerStats": "esg_server_stats"}
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every ctypes mirror has the size and field offsets the C compiler
+    gives the header's struct (a drifted mirror would read garbage)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', f'#include "{HEADER}"',
+             "int main(void) {"]
+    for py, c in _STRUCTS.items():
+        lines.append(f'printf("{py} size %zu\\n", sizeof({c}));')
+        for fname, _ in getattr(_native, py)._fields_:
+            lines.append(f'printf("{py} {fname} %zu\\n", offsetof({c}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "abi.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "abi"
+    subprocess.run([cc, "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    for line in out.splitlines():
+        py, what, val = line.split()
+        cls = getattr(_native, py)
+        got = ctypes.sizeof(cls) if what == "size" else getattr(cls, what).offset
+        assert got == int(val), (py, what, got, val)
