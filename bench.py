@@ -521,6 +521,13 @@ class Ctx:
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
+    def sum_over_ranks(self, x):
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
     def device_time(self, scorer, batch, steps, warmup, sampler=None):
         torch, stream = self.torch, self.stream
         for _ in range(warmup):
@@ -631,7 +638,14 @@ def run_c2(a, ctx, rank):
                               "stats": r.stats}), flush=True)
             g.close()
         return
-    reads = synth.reads_c2(refs, n=a.reads)  # weak scaling: every rank scores the full batch
+    # weak scaling: the job is a.reads reads per GPU, cut into this rank's
+    # slice the way the library shards a batch (replicas.shard: contiguous,
+    # balanced by cells); one GPU scores the whole a.reads
+    if world > 1:
+        from eschalign_b200 import replicas
+        reads, _ = replicas.shard(synth.reads_c2(refs, n=a.reads * world), rank, world)
+    else:
+        reads = synth.reads_c2(refs, n=a.reads)
     extras = {}
     scoring, mode = HEADLINE
     g = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank,
@@ -646,7 +660,9 @@ def run_c2(a, ctx, rank):
     t = ctx.device_time(g, batch, a.steps, a.warmup, sampler)
     clocks = sampler.summary()
     t_max = ctx.max_over_ranks(t)
-    value = world * cells * a.steps / t_max / 1e9
+    job_cells = ctx.sum_over_ranks(cells)  # every rank's slice
+    job_reads = ctx.sum_over_ranks(len(reads))
+    value = job_cells * a.steps / t_max / 1e9
     # the timed launches' results (the last one's, in device memory) against
     # the submit's, every read
     timed_res, timed_ties = g.read_results(batch)
@@ -710,9 +726,9 @@ def run_c2(a, ctx, rank):
     te, n_pass, h2d, d2h = feeder(
         ctx, chunks, lambda c: g.prepare(c.tuple(), both_strands=True), g.submit,
         lambda b: g.finish(b).stats, max(1, a.steps))
-    e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
+    e2e = {"value": job_cells * n_pass / te / 1e9, "unit": "GCUPS",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "reads_per_s": world * len(reads) * n_pass / te, "chunk_reads": a.chunk,
+           "reads_per_s": job_reads * n_pass / te, "chunk_reads": a.chunk,
            "host_seconds_per_pass": feeder.last_split}
     g.close()
 
@@ -733,10 +749,11 @@ def run_c2(a, ctx, rank):
             a, ctx, value, 1e3 * t_max / a.steps,
             "C2: 1M reads (lognormal median 110 nt) x 164-ref panel (70-180 nt), both "
             "strands, local 2,-1,-10,-1, best + XS + 8 ties per read",
-            {"reads": a.reads, "refs": len(refs), "panel_bases": panel_bases,
-             "cells_per_step": cells},
+            {"reads": int(job_reads), "refs": len(refs), "panel_bases": panel_bases,
+             "cells_per_step": int(job_cells),
+             "sharding": "replicas.shard: contiguous slices balanced by cells"},
             e2e, roofline, clocks, st["kernels"] * a.steps)
-        line["reads_per_s"] = world * len(reads) * a.steps / t_max
+        line["reads_per_s"] = job_reads * a.steps / t_max
         line["kernel_info"] = {k: info[k] for k in (
             "regs_batched", "regs_plain", "local_bytes_batched", "batched_blocks",
             "panel_bytes", "sm_count", "split_len")}
