@@ -111,7 +111,7 @@ def args_parse():
     ap.add_argument("--c3-reads", type=int, default=4000, help="c3: reads per step")
     ap.add_argument("--rates", default="10,30,100,300,1000,2000",
                     help="c5: Poisson arrival rates swept (requests/s)")
-    ap.add_argument("--requests", type=int, default=200, help="c5: requests per rate")
+    ap.add_argument("--requests", type=int, default=1000, help="c5: requests per rate")
     ap.add_argument("--split", type=int, default=-1,
                     help="16/32-row split in nt, set instead of autotuning (for runs under a "
                          "profiler, whose serialised launches would skew the autotuner)")
@@ -973,16 +973,20 @@ def run_c5(a, ctx, rank):
     clocks = None
     with Server(scorers) as sv:
         for ri, rate in enumerate(rates):
-            rr = np.random.default_rng([0x5EED_0C05, ri])
+            # the same requests (sizes, panels, modes, strands, reads) at
+            # every rate, so rates differ only in arrival times; the
+            # arrivals of each rate are its own Poisson draw
+            rr = np.random.default_rng(0x5EED_0C05)
             n_req = a.requests
             sizes = np.floor(np.exp(rr.uniform(0, np.log(50_000), n_req))).astype(np.int64)
             slots = rr.integers(0, 4, n_req)
             both = rr.random(n_req) < 0.5
-            gaps = rr.exponential(1.0 / rate, n_req)
+            starts = [int(rr.integers(0, pool_n - sizes[k] + 1)) for k in range(n_req)]
+            gaps = np.random.default_rng([0x5EED_0C05, ri]).exponential(1.0 / rate, n_req)
             reqs = []
             for k in range(n_req):
                 pk = specs[slots[k]][0]
-                start = int(rr.integers(0, pool_n - sizes[k] + 1))
+                start = starts[k]
                 reqs.append((int(slots[k]), pools[pk].slice(start, start + int(sizes[k])),
                              bool(both[k])))
             cells = sum(int(r[1].bases()) * (2 if r[2] else 1) * pbases[specs[r[0]][0]]
@@ -1017,6 +1021,10 @@ def run_c5(a, ctx, rank):
             else:
                 sampler.summary()
             lat = np.array([results[k][1].total_ms for k in range(n_req)])
+            small = sizes <= 1000
+
+            def pct(x, q):
+                return round(float(np.percentile(x, q)), 2) if x.size else None
             queued = np.array([results[k][1].queued_ms for k in range(n_req)])
             bsz = np.array([results[k][1].batch_requests for k in range(n_req)])
             span = t_end - t0
@@ -1027,6 +1035,11 @@ def run_c5(a, ctx, rank):
                 "p50_ms": round(float(np.percentile(lat, 50)), 2),
                 "p99_ms": round(float(np.percentile(lat, 99)), 2),
                 "p999_ms": round(float(np.percentile(lat, 99.9)), 2),
+                "small_le_1000_reads": {"requests": int(small.sum()),
+                                        "p50_ms": pct(lat[small], 50),
+                                        "p99_ms": pct(lat[small], 99)},
+                "large": {"requests": int((~small).sum()), "p50_ms": pct(lat[~small], 50),
+                          "p99_ms": pct(lat[~small], 99)},
                 "mean_queued_ms": round(float(queued.mean()), 2),
                 "mean_requests_per_batch": round(float(bsz.mean()), 2),
                 "seconds": round(span, 2),
