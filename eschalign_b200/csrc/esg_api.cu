@@ -932,9 +932,12 @@ esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
   ESG_CUDA(cudaEventCreate(&e1));
   esg_status st = ESG_OK;
   Calib c;
-  // about 2e10 cells per batch (a few ms of device time), both strands
+  // about 2e11 cells per batch (~40 ms of device time), both strands: on a
+  // small panel enough tiles to keep every resident warp busy without panel
+  // chunks, the regime of a real batch (smaller batches measured the chunked
+  // regime, where 16- and 32-row stripes time alike, and chose badly)
   auto reads_for = [&](uint32_t L) {
-    const uint64_t want = (uint64_t)(2.0e10 / (2.0 * L * (double)sc->panel_bases));
+    const uint64_t want = (uint64_t)(2.0e11 / (2.0 * L * (double)sc->panel_bases));
     return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 64), 200000);
   };
   sc->int32_from = 0;
@@ -961,14 +964,14 @@ esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
     cudaEventDestroy(e1);
     return st;
   }
-  // 16-row stripes up to the last length where they are at least as fast,
-  // counting from the shortest; 32-row stripes from the first length they
-  // win.  The int32 lanes from the length where they win at it and every
-  // longer length (a scheme whose long queries mostly flag, to be scored
-  // twice by the batched kernel), else never.
+  // 16-row stripes up to the last length where they are as fast within 2 %
+  // (timing noise), counting from the shortest; 32-row stripes from the
+  // first length they win by more.  The int32 lanes from the length where
+  // they win at it and every longer length (a scheme whose long queries
+  // mostly flag, to be scored twice by the batched kernel), else never.
   uint32_t split = 0;
   for (uint32_t li = 0; li < rep.n_lengths; ++li) {
-    if (rep.ms_rows16[li] <= rep.ms_rows32[li])
+    if (rep.ms_rows16[li] <= 1.02f * rep.ms_rows32[li])
       split = rep.lengths[li];
     else
       break;
