@@ -184,6 +184,12 @@ struct esg_batch {
   uint32_t n_q = 0;
   int kernel = ESG_KERNEL_AUTO;
   uint64_t total_bases = 0;
+  // upload: reads packed at 2 bits a base, each read starting on a byte
+  // (its offset a multiple of 4 bases); positions of bases that are not
+  // A/C/G/T travel as a list and become the wildcard code on the device
+  uint64_t padded_bases = 0;  // sum of lengths rounded up to 4
+  uint64_t code_words = 0;    // 32-bit packed words (16 bases each) unpacked
+  std::vector<uint64_t> exceptions;
   // host plan
   uint32_t n_tasks = 0;
   uint32_t n_long = 0;   // tasks are [n_long long | n_t32 tiles | n_t16 tiles]
@@ -202,7 +208,7 @@ struct esg_batch {
   std::vector<uint32_t> adapters;  // adapter bases removed, per mate
   // pinned staging (inputs, then outputs)
   Pinned in_buf, out_buf;
-  uint8_t* h_codes = nullptr;
+  uint8_t* h_packed = nullptr;
   uint64_t* h_off = nullptr;
   uint32_t* h_len = nullptr;
   uint32_t* h_order = nullptr;
@@ -219,7 +225,9 @@ struct esg_batch {
   // device
   void* d_mem = nullptr;
   size_t d_bytes = 0;
-  uint8_t* d_codes = nullptr;
+  uint8_t* d_codes = nullptr;   // one byte a base, unpacked on the device
+  uint8_t* d_packed = nullptr;  // the upload
+  uint64_t* d_exc = nullptr;
   uint64_t* d_off = nullptr;
   uint32_t* d_len = nullptr;
   uint32_t* d_order = nullptr;
@@ -1057,6 +1065,61 @@ esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
 // ---------------------------------------------------------------- prepare
 }  // extern "C"
 
+// Read codes packed at 2 bits a base into `out` (base i of a byte in bits
+// 2i..2i+1); a code above 3 (the wildcard, or any other byte) packs as 0 and
+// its stream position base + i goes to `exc`.  Eight bases at a time: the
+// shifts gather the low two bits of eight bytes into 16 bits.
+static void pack_read(const uint8_t* src, uint32_t n, uint8_t* out, uint64_t base,
+                      std::vector<uint64_t>& exc) {
+  uint32_t i = 0;
+  for (; i + 8 <= n; i += 8) {
+    uint64_t v;
+    memcpy(&v, src + i, 8);
+    if (v & 0xFCFCFCFCFCFCFCFCull) {
+      for (uint32_t j = 0; j < 8; ++j)
+        if (src[i + j] > 3) exc.push_back(base + i + j);
+      v &= 0x0303030303030303ull;
+      for (uint32_t j = 0; j < 8; ++j)
+        if (src[i + j] > 3) v &= ~(0xffull << (8 * j));
+    }
+    uint64_t x = (v | (v >> 6)) & 0x000F000F000F000Full;
+    x = (x | (x >> 12)) & 0x000000FF000000FFull;
+    x = x | (x >> 24);
+    out[i / 4] = (uint8_t)x;
+    out[i / 4 + 1] = (uint8_t)(x >> 8);
+  }
+  for (; i < n; i += 4) {
+    uint8_t byte = 0;
+    for (uint32_t j = 0; j < 4 && i + j < n; ++j) {
+      uint8_t c = src[i + j];
+      if (c > 3) {
+        exc.push_back(base + i + j);
+        c = 0;
+      }
+      byte |= (uint8_t)(c << (2 * j));
+    }
+    out[i / 4] = byte;
+  }
+}
+
+// The packing esg_prepare does, for the host-side tests: reads k at
+// out + pos_k / 4 with pos_k the sum of the earlier lengths rounded up to 4;
+// returns the packed bytes, exceptions to `exc` (up to exc_cap), their count
+// to *n_exc.
+extern "C" uint64_t esg_internal_pack_reads(const uint8_t* codes, const uint64_t* off,
+                                            const uint32_t* len, uint32_t n, uint8_t* out,
+                                            uint64_t* exc, uint64_t exc_cap, uint64_t* n_exc) {
+  std::vector<uint64_t> e;
+  uint64_t pos = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    if (len[k]) pack_read(codes + off[k], len[k], out + pos / 4, pos, e);
+    pos += ((uint64_t)len[k] + 3) & ~(uint64_t)3;
+  }
+  for (uint64_t i = 0; i < e.size() && i < exc_cap; ++i) exc[i] = e[i];
+  *n_exc = e.size();
+  return pos / 4;
+}
+
 // The planning half of esg_prepare.  Read k is `ptrs[k]` when `ptrs` is
 // given (reads gathered from several requests), else codes + off[k].
 static esg_status prepare_impl(esg_scorer* sc, const uint8_t* const* ptrs, const uint8_t* codes,
@@ -1143,8 +1206,12 @@ static esg_status prepare_impl(esg_scorer* sc, const uint8_t* const* ptrs, const
     b->n_chunks = std::max<uint32_t>(nc, 1);
   }
 
-  // --- pinned staging for the inputs
-  const size_t sz_codes = carve_size(total ? total : 1, 1);
+  // --- pinned staging for the inputs (reads packed at 2 bits a base)
+  uint64_t padded = 0;
+  for (uint32_t k = 0; k < n_reads; ++k) padded += ((uint64_t)len[k] + 3) & ~(uint64_t)3;
+  b->padded_bases = padded;
+  b->code_words = (padded + 15) / 16;
+  const size_t sz_codes = carve_size(b->code_words ? b->code_words * 4 : 1, 1);
   const size_t sz_off = carve_size(n_reads ? n_reads : 1, 8);
   const size_t sz_len = carve_size(n_reads ? n_reads : 1, 4);
   const size_t sz_order = carve_size(b->n_order ? b->n_order : 1, 4);
@@ -1158,7 +1225,7 @@ static esg_status prepare_impl(esg_scorer* sc, const uint8_t* const* ptrs, const
     return fail(ESG_ERR_OUT_OF_MEMORY, "pinned host memory (%zu bytes)", (size_t)b->in_bytes);
   }
   char* at = (char*)b->in_buf.p;
-  b->h_codes = carve<uint8_t>(at, total ? total : 1);
+  b->h_packed = carve<uint8_t>(at, b->code_words ? b->code_words * 4 : 1);
   b->h_off = carve<uint64_t>(at, n_reads ? n_reads : 1);
   b->h_len = carve<uint32_t>(at, n_reads ? n_reads : 1);
   b->h_order = carve<uint32_t>(at, b->n_order ? b->n_order : 1);
@@ -1185,9 +1252,12 @@ static esg_status prepare_impl(esg_scorer* sc, const uint8_t* const* ptrs, const
   for (uint32_t k = 0; k < n_reads; ++k) {
     b->h_off[k] = pos;
     b->h_len[k] = len[k];
-    if (len[k]) memcpy(b->h_codes + pos, ptrs ? ptrs[k] : codes + off[k], len[k]);
-    pos += len[k];
+    if (len[k]) pack_read(ptrs ? ptrs[k] : codes + off[k], len[k], b->h_packed + pos / 4, pos,
+                          b->exceptions);
+    pos += ((uint64_t)len[k] + 3) & ~(uint64_t)3;
   }
+  // the packed tail up to the last whole word unpacks to padding
+  memset(b->h_packed + pos / 4, 0, b->code_words * 4 - pos / 4);
   // order[] and tasks[] laid out [long | 32-row tiles | 16-row tiles];
   // tasks[t] = {start in order[], count | stripes << 16}
   {
@@ -1287,7 +1357,9 @@ static size_t batch_device_bytes(const esg_scorer* sc, const esg_batch* b) {
   const uint32_t nlist = b->host_list + b->redo_cap;
   const size_t nr = b->n_reads ? b->n_reads : 1, nq = b->n_q ? b->n_q : 1;
   const size_t sizes[] = {
-      carve_size(b->total_bases ? b->total_bases : 1, 1),
+      carve_size(b->code_words ? b->code_words * 16 : 1, 1),
+      carve_size(b->code_words ? b->code_words * 4 : 1, 1),
+      carve_size(b->exceptions.empty() ? 1 : b->exceptions.size(), 8),
       carve_size(nr, 8),
       carve_size(nr, 4),
       carve_size(b->n_order ? b->n_order : 1, 4),
@@ -1603,7 +1675,9 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
   ESG_CUDA(cudaMallocFromPoolAsync(&b->d_mem, total, sc->pool, st));
   b->d_bytes = total;
   char* at = (char*)b->d_mem;
-  b->d_codes = carve<uint8_t>(at, b->total_bases ? b->total_bases : 1);
+  b->d_codes = carve<uint8_t>(at, b->code_words ? b->code_words * 16 : 1);
+  b->d_exc = carve<uint64_t>(at, b->exceptions.empty() ? 1 : b->exceptions.size());
+  b->d_packed = carve<uint8_t>(at, b->code_words ? b->code_words * 4 : 1);
   b->d_off = carve<uint64_t>(at, nr);
   b->d_len = carve<uint32_t>(at, nr);
   b->d_order = carve<uint32_t>(at, b->n_order ? b->n_order : 1);
@@ -1624,9 +1698,28 @@ esg_status esg_submit(esg_scorer* sc, esg_batch* b) {
     b->d_part_ties = carve<uint32_t>(at, nq * b->n_chunks * sc->cap);
   }
   // uploads: the pinned staging is one contiguous block laid out the same way
-  // for the first seven buffers
-  ESG_CUDA(cudaMemcpyAsync(b->d_codes, b->in_buf.p, b->in_bytes, cudaMemcpyHostToDevice, st));
+  // as the device buffers from d_packed on (packed reads, offsets, lengths,
+  // the plan); then the reads are unpacked to a byte a base
+  ESG_CUDA(cudaMemcpyAsync(b->d_packed, b->in_buf.p, b->in_bytes, cudaMemcpyHostToDevice, st));
   b->stats.h2d_bytes = b->in_bytes;
+  if (!b->exceptions.empty()) {
+    ESG_CUDA(cudaMemcpyAsync(b->d_exc, b->exceptions.data(), b->exceptions.size() * 8,
+                             cudaMemcpyHostToDevice, st));
+    b->stats.h2d_bytes += b->exceptions.size() * 8;
+  }
+  if (b->code_words) {
+    const int ublocks = (int)std::min<uint64_t>(
+        (uint64_t)sc->sm_count * 8, (b->code_words + 255) / 256);
+    k0_unpack<<<ublocks, 256, 0, st>>>(reinterpret_cast<const uint32_t*>(b->d_packed),
+                                       b->code_words, reinterpret_cast<uint4*>(b->d_codes));
+    ESG_CUDA(cudaGetLastError());
+    if (!b->exceptions.empty()) {
+      const int eblocks = (int)std::min<uint64_t>(
+          (uint64_t)sc->sm_count * 4, (b->exceptions.size() + 255) / 256);
+      k0_exceptions<<<eblocks, 256, 0, st>>>(b->d_exc, b->exceptions.size(), b->d_codes);
+      ESG_CUDA(cudaGetLastError());
+    }
+  }
   esg_status s = launch_work(sc, b, st);
   if (s != ESG_OK) return s;
   // downloads into pinned staging

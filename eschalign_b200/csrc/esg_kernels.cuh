@@ -1197,6 +1197,34 @@ static __global__ void __launch_bounds__(256) k4_rows(const K4Params P) {
   }
 }
 
+// ---------------------------------------------------------------- k0
+// Reads travel host to device packed at 2 bits a base (base i of a byte in
+// bits 2i..2i+1, each read starting on a byte); these two kernels run once
+// after the upload.  k0_unpack writes one byte a base: each thread takes a
+// 32-bit word (16 bases) and stores 16 bytes.  k0_exceptions then sets the
+// listed positions -- read bases that were not A/C/G/T -- to the wildcard
+// code 4.
+__device__ __forceinline__ uint32_t spread4(uint32_t b) {
+  return (b & 3u) | ((b >> 2) & 3u) << 8 | ((b >> 4) & 3u) << 16 | ((b >> 6) & 3u) << 24;
+}
+
+static __global__ void __launch_bounds__(256) k0_unpack(const uint32_t* __restrict__ packed,
+                                                        uint64_t n_words, uint4* __restrict__ codes) {
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n_words;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = packed[w];
+    codes[w] = make_uint4(spread4(p & 0xffu), spread4((p >> 8) & 0xffu), spread4((p >> 16) & 0xffu),
+                          spread4(p >> 24));
+  }
+}
+
+static __global__ void __launch_bounds__(256) k0_exceptions(const uint64_t* __restrict__ at,
+                                                            uint64_t n, uint8_t* __restrict__ codes) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    codes[at[i]] = 4;
+}
+
 // ---------------------------------------------------------------- k5
 struct K5Params {
   const uint32_t* len;

@@ -148,3 +148,42 @@ def test_mapping_results_decode_without_a_device():
     p1 = pm.pair_mapping(1)
     assert not p1["proper"] and p1["mates"][0]["hits"][0]["cigar"] == "4M"
     assert p1["mates"][1]["best_score"] is None
+
+
+def test_reads_pack_at_two_bits_and_unpack_to_their_codes():
+    """The upload format: reads packed at 2 bits a base (each read on a byte,
+    base i of a byte in bits 2i..2i+1), bases that are not A/C/G/T listed by
+    position.  Unpacked the way the device does it (k0_unpack, then the
+    listed positions set to 4), every read is its codes again, wildcards and
+    odd bytes as the wildcard code."""
+    import ctypes as C
+
+    import numpy as np
+
+    from eschalign_b200 import _native, pack_reads
+    lib = _native.load()
+    fn = lib.esg_internal_pack_reads
+    fn.restype = C.c_uint64
+    rng = np.random.default_rng(5)
+    reads = []
+    for n in [0, 1, 3, 4, 5, 7, 8, 9, 15, 16, 17, 31, 100, 257] + list(rng.integers(1, 400, 60)):
+        r = rng.integers(0, 4, int(n)).astype(np.uint8)
+        if n and rng.random() < 0.4:
+            r[rng.integers(0, n, max(1, int(n) // 20))] = rng.choice([4, 4, 5, 200])
+        reads.append(r)
+    codes, off, lens = pack_reads(reads)
+    padded = int(((lens.astype(np.int64) + 3) // 4 * 4).sum())
+    out = np.zeros(padded // 4 + 16, np.uint8)
+    exc = np.zeros(int((codes > 3).sum()) + 1, np.uint64)
+    n_exc = C.c_uint64(0)
+    nbytes = fn(codes.ctypes.data, off.ctypes.data, lens.ctypes.data, len(reads),
+                out.ctypes.data, exc.ctypes.data, exc.size, C.byref(n_exc))
+    assert nbytes == padded // 4 and n_exc.value == int((codes > 3).sum())
+    # the device's unpack: byte b -> bases b & 3, b >> 2 & 3, ...
+    unpacked = np.stack([(out >> (2 * i)) & 3 for i in range(4)], 1).reshape(-1)
+    unpacked[exc[:n_exc.value].astype(np.int64)] = 4
+    pos = 0
+    for r in reads:
+        got = unpacked[pos:pos + r.size]
+        assert np.array_equal(got, np.minimum(r, 4)), r
+        pos += (r.size + 3) // 4 * 4
