@@ -112,6 +112,8 @@ def args_parse():
     ap.add_argument("--rates", default="10,30,100,300,1000,2000",
                     help="c5: Poisson arrival rates swept (requests/s)")
     ap.add_argument("--requests", type=int, default=1000, help="c5: requests per rate")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch each batch's kernels one by one instead of as one CUDA graph")
     ap.add_argument("--split", type=int, default=-1,
                     help="16/32-row split in nt, set instead of autotuning (for runs under a "
                          "profiler, whose serialised launches would skew the autotuner)")
@@ -600,6 +602,8 @@ def feeder(ctx, chunks, prepare, submit, finish, steps):
 
 def tune(g, a):
     """The autotuner's report, or the pinned split (--split)."""
+    if a.no_graphs:
+        g.set_graphs(False)
     if a.split >= 0:
         g.set_split(a.split)
         return {"split_len": a.split, "pinned": True}

@@ -427,11 +427,12 @@ def test_gpu_graph_launches_equal_direct_launches(oracle):
             assert (first.results == want[0].results).all()
 
 
-def test_gpu_autotune_sends_flagging_lengths_to_int32_lanes(oracle):
+def test_gpu_autotune_lane_type_follows_its_measurements(oracle):
     """With a scheme whose long reads leave int16 (100,-100,-27,-27 on a
-    panel of ~500-nt references) the batched kernel would flag most long
-    queries and score them twice: the autotuner measures the int32 lanes
-    faster there and routes those lengths to them; results stay exact."""
+    panel of ~500-nt references) the batched kernel flags long queries for a
+    second, int32 pass; the autotuner times that against every query on the
+    int32 lanes and routes to the int32 lanes exactly the lengths where they
+    win at that length and every longer one.  Results stay exact either way."""
     rng = Rng(0x5EED_0A13)
     letters = random_panel(rng, 60, 480, 40)
     panel = [encode(s) for s in letters]
@@ -440,9 +441,16 @@ def test_gpu_autotune_sends_flagging_lengths_to_int32_lanes(oracle):
     scoring = (100, -100, -27, -27)
     with GpuScorer(panel, Scoring(*scoring), Mode.LOCAL) as g:
         rep = g.autotune()
-        assert rep["int32_from"] > 0, rep
+        best_k2 = [min(a, b) for a, b in zip(rep["ms_rows16"], rep["ms_rows32"])]
+        wins = [i32 < k2 for i32, k2 in zip(rep["ms_int32"], best_k2)]
+        if rep["int32_from"]:
+            at = rep["lengths"].index(rep["int32_from"])
+            assert all(wins[at:]) and (at == 0 or not wins[at - 1])
+        else:
+            assert not wins[-1]
         res = g.score_batch(reads, both_strands=True, full_rows=True)
-        assert res.stats["queries_plain"] > 0 and res.stats["queries_batched"] > 0
+        n_int32 = sum(2 for r in reads if rep["int32_from"] and len(r) >= rep["int32_from"])
+        assert res.stats["queries_plain"] == n_int32
     want_rows = oracle_rows(oracle, reads, panel, scoring, True)
     assert (res.rows == want_rows).all()
     want, want_t, _ = oracle.scalar_map_batch(reads, panel, scoring, True, True, cap=CAP)
