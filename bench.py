@@ -600,14 +600,15 @@ def feeder(ctx, chunks, prepare, submit, finish, steps):
     return ctx.max_over_ranks(sum(times)), len(times), h2d, d2h
 
 
-def tune(g, a):
-    """The autotuner's report, or the pinned split (--split)."""
+def tune(g, a, lengths=None):
+    """The autotuner's report (on the workload's length histogram when a
+    sample of its read lengths is given), or the pinned split (--split)."""
     if a.no_graphs:
         g.set_graphs(False)
     if a.split >= 0:
         g.set_split(a.split)
         return {"split_len": a.split, "pinned": True}
-    return g.autotune()
+    return g.autotune(lengths)
 
 
 def common_line(a, ctx, value, ms_per_step, workload, extra_config, e2e, roofline, clocks,
@@ -654,7 +655,7 @@ def run_c2(a, ctx, rank):
     scoring, mode = HEADLINE
     g = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank,
                   stream=ctx.stream.cuda_stream)
-    tune_rep = tune(g, a)  # tile shape for this panel, before any timing
+    tune_rep = tune(g, a, reads.lens[:20000])  # tile shape for this panel, before any timing
     info = g.info()
     batch = g.submit(g.prepare(reads.tuple(), both_strands=True))
     first = g.finish(batch, keep=True)
@@ -688,7 +689,7 @@ def run_c2(a, ctx, rank):
         for sc_, md in COMBOS[1:]:
             g2 = GpuScorer(refs, Scoring(*sc_), Mode.parse(md), device=local_rank,
                            stream=ctx.stream.cuda_stream)
-            tune(g2, a)
+            tune(g2, a, reads.lens[:20000])
             b2 = g2.submit(g2.prepare(reads.tuple(), both_strands=True))
             r2 = g2.finish(b2, keep=True)
             t2 = ctx.max_over_ranks(ctx.device_time(g2, b2, 1, 1))
@@ -781,7 +782,7 @@ def run_c1(a, ctx, rank):
     reads = synth.reads_c1(refs)
     g = GpuScorer(refs, Scoring(*scoring), Mode.LOCAL, device=local_rank,
                   stream=ctx.stream.cuda_stream)
-    tune_rep = tune(g, a)
+    tune_rep = tune(g, a, reads.lens)
     batch = g.submit(g.prepare(reads.tuple()))
     st = g.finish(batch, keep=True).stats
     cells = st["cells"]
@@ -841,7 +842,7 @@ def run_c4(a, ctx, rank):
     cfg = adapter.config()
     g = GpuScorer(refs, Scoring(*C4_SCORING), Mode.SEMIGLOBAL, device=local_rank,
                   stream=ctx.stream.cuda_stream)
-    tune_rep = tune(g, a)
+    tune_rep = tune(g, a, pairs.lens[:40000])
     batch = g.submit(g.prepare_pairs(pairs.tuple(), adapters=cfg, both_strands=True))
     st = g.finish_pairs(batch, keep=True).stats
     cells = st["cells"]
@@ -904,7 +905,7 @@ def run_c3(a, ctx, rank):
     reads = synth.reads_c3(refs, n=a.c3_reads)
     g = GpuScorer(refs, Scoring(*C3_SCORING), Mode.LOCAL, device=local_rank,
                   stream=ctx.stream.cuda_stream)
-    tune_rep = tune(g, a)
+    tune_rep = tune(g, a, reads.lens)
     info = g.info()
     batch = g.submit(g.prepare(reads.tuple(), both_strands=True))
     st = g.finish(batch, keep=True).stats
@@ -969,7 +970,7 @@ def run_c5(a, ctx, rank):
     tunes = {}
     for pk, md in specs:
         g = GpuScorer(panels[pk], Scoring(*scoring), md, device=local_rank)
-        tunes[f"{pk} {md.label}"] = tune(g, a)["split_len"]
+        tunes[f"{pk} {md.label}"] = tune(g, a, pools[pk].lens[:20000])["split_len"]
         scorers.append(g)
     rates = [float(x) for x in a.rates.split(",") if x]
     per_rate = []

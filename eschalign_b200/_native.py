@@ -101,7 +101,9 @@ class EsgTuneReport(C.Structure):
                 ("n_ctas32", C.c_uint32), ("cand_ctas32", C.c_uint32 * 4),
                 ("ms_ctas32", C.c_float * 4), ("ctas32", C.c_uint32),
                 ("n_chunk_targets", C.c_uint32), ("chunk_targets", C.c_uint32 * 8),
-                ("ms_chunks", C.c_float * 8), ("chunk_target", C.c_uint32)]
+                ("ms_chunks", C.c_float * 8), ("chunk_target", C.c_uint32),
+                ("n_splits", C.c_uint32), ("splits", C.c_uint32 * 8),
+                ("ms_splits", C.c_float * 8)]
 
 
 class EsgBatchStats(C.Structure):
@@ -179,6 +181,8 @@ SIGNATURES = {
     "esg_scores_len": (C.c_int32, [C.c_void_p, C.c_uint64]),
     "esg_batched_takes": (C.c_int32, [C.c_void_p, C.c_uint64]),
     "esg_scorer_autotune": (C.c_int32, [C.c_void_p, C.POINTER(EsgTuneReport)]),
+    "esg_scorer_autotune_lengths": (C.c_int32, [C.c_void_p, _u32p, C.c_uint32,
+                                                C.POINTER(EsgTuneReport)]),
     "esg_scorer_set_split": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "esg_scorer_set_chunking": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "esg_score_batch": (C.c_int32, [C.c_void_p, _u8p, _u64p, _u32p, C.c_uint32, C.c_uint32,

@@ -855,7 +855,9 @@ struct Calib {
   uint32_t n = 0;
 };
 
-void calib_reads(const esg_scorer* sc, uint32_t L, uint32_t n, uint64_t& x, Calib& c) {
+// Read lengths: L +- 25 %, or (hist non-empty) drawn from the sample `hist`.
+void calib_reads(const esg_scorer* sc, uint32_t L, uint32_t n, uint64_t& x, Calib& c,
+                 const std::vector<uint32_t>& hist = {}) {
   auto next = [&x]() {  // xorshift64*
     x ^= x >> 12;
     x ^= x << 25;
@@ -867,7 +869,8 @@ void calib_reads(const esg_scorer* sc, uint32_t L, uint32_t n, uint64_t& x, Cali
   c.len.assign(n, 0);
   c.codes.clear();
   for (uint32_t k = 0; k < n; ++k) {
-    const uint32_t len = L - L / 4 + (uint32_t)(next() % (L / 2 + 1));
+    const uint32_t len = hist.empty() ? L - L / 4 + (uint32_t)(next() % (L / 2 + 1))
+                                      : std::max<uint32_t>(1, hist[next() % hist.size()]);
     c.off[k] = c.codes.size();
     c.len[k] = len;
     const bool derived = next() % 10 != 0;
@@ -905,9 +908,8 @@ static esg_status time_calib(esg_scorer* sc, const Calib& c, cudaEvent_t e0, cud
   return st;
 }
 
-extern "C" {
-
-esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
+static esg_status autotune_impl(esg_scorer* sc, const std::vector<uint32_t>& hist,
+                                esg_tune_report* out) {
   g_err.clear();
   if (!sc) return fail(ESG_ERR_BAD_ARGUMENT, "NULL scorer");
   esg_tune_report rep{};
@@ -992,6 +994,33 @@ esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
     else
       break;
   }
+  // 1b. with a sample of the workload's read lengths: every candidate split
+  //     timed on one batch drawn from that histogram, the fastest kept (of
+  //     equal times, within 1 %, the larger split: 16-row tiles carry less
+  //     skew per pair)
+  if (!hist.empty()) {
+    uint64_t bases = 0;
+    for (uint32_t v : hist) bases += v;
+    const double mean = std::max(1.0, (double)bases / (double)hist.size());
+    const uint64_t want = (uint64_t)(2.0e11 / (2.0 * mean * (double)sc->panel_bases));
+    calib_reads(sc, 0, (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 64), 400000), x, c,
+                hist);
+    static const uint32_t kSplits[] = {0, 48, 80, 112, 160, 224, 320, 512};
+    float best = 0;
+    for (uint32_t cand : kSplits) {
+      if (st != ESG_OK) break;
+      sc->split_len = cand;
+      float ms = 0;
+      st = time_calib(sc, c, e0, e1, &ms);
+      rep.splits[rep.n_splits] = cand;
+      rep.ms_splits[rep.n_splits] = ms;
+      ++rep.n_splits;
+      if (rep.n_splits == 1 || ms <= 1.01f * best) {
+        if (rep.n_splits == 1 || ms < best) best = ms;
+        split = cand;
+      }
+    }
+  }
   // 2. resident CTAs per SM of the 16-row tiles (112-nt reads) and the
   //    32-row tiles (448-nt reads): the occupancy limit and one or two fewer
   for (int which = 0; which < 2 && st == ESG_OK; ++which) {
@@ -1060,6 +1089,23 @@ esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
   rep.int32_from = from;
   if (out) *out = rep;
   return ESG_OK;
+}
+
+extern "C" {
+
+esg_status esg_scorer_autotune(esg_scorer* sc, esg_tune_report* out) {
+  return autotune_impl(sc, {}, out);
+}
+
+esg_status esg_scorer_autotune_lengths(esg_scorer* sc, const uint32_t* lens, uint32_t n,
+                                       esg_tune_report* out) {
+  g_err.clear();
+  if (!sc || (n && !lens)) return fail(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  std::vector<uint32_t> hist;
+  hist.reserve(n);
+  for (uint32_t k = 0; k < n; ++k)
+    if (lens[k]) hist.push_back(lens[k]);
+  return autotune_impl(sc, hist, out);
 }
 
 // ---------------------------------------------------------------- prepare

@@ -407,12 +407,19 @@ class GpuScorer:
         kernel (else the int32 kernel)."""
         return bool(self._lib.esg_batched_takes(self._h, int(n)))
 
-    def autotune(self) -> dict:
+    def autotune(self, lengths=None) -> dict:
         """Measure the tile shape on this panel (esg_scorer_autotune): the
         16/32-row stripe split, the length from which the int32 lanes take
-        over, resident CTAs per SM, the panel-chunk target."""
+        over, resident CTAs per SM, the panel-chunk target.  With `lengths`
+        (a sample of the workload's read lengths) the split is chosen on a
+        batch of that length histogram (esg_scorer_autotune_lengths)."""
         rep = _native.EsgTuneReport()
-        _check(self._lib, self._lib.esg_scorer_autotune(self._h, C.byref(rep)))
+        if lengths is None:
+            _check(self._lib, self._lib.esg_scorer_autotune(self._h, C.byref(rep)))
+        else:
+            lens = np.ascontiguousarray(lengths, dtype=np.uint32)
+            _check(self._lib, self._lib.esg_scorer_autotune_lengths(
+                self._h, _ptr(lens, C.c_uint32), int(lens.size), C.byref(rep)))
         n = rep.n_lengths
 
         def ms(a, k):
@@ -427,7 +434,9 @@ class GpuScorer:
                            "ms": ms(rep.ms_ctas32, rep.n_ctas32), "chosen": rep.ctas32},
                 "chunk_target": {"tried": list(rep.chunk_targets[:rep.n_chunk_targets]),
                                  "ms": ms(rep.ms_chunks, rep.n_chunk_targets),
-                                 "chosen": rep.chunk_target}}
+                                 "chosen": rep.chunk_target},
+                "split_on_histogram": {"tried": list(rep.splits[:rep.n_splits]),
+                                       "ms": ms(rep.ms_splits, rep.n_splits)}}
 
     def set_split(self, split_len: int):
         _check(self._lib, self._lib.esg_scorer_set_split(self._h, int(split_len)))

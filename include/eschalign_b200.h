@@ -129,6 +129,9 @@ typedef struct esg_tune_report {
     uint32_t chunk_targets[8];
     float ms_chunks[8];
     uint32_t chunk_target;                    /* chosen                                 */
+    uint32_t n_splits;                        /* esg_scorer_autotune_lengths: 16/32 splits tried */
+    uint32_t splits[8];                       /* on one batch of the given length histogram */
+    float ms_splits[8];
 } esg_tune_report;
 
 typedef struct esg_batch_stats {
@@ -199,6 +202,14 @@ esg_status esg_scorer_set_kernel(esg_scorer* scorer, int32_t kernel);
  * target for batches too small to fill the GPU.  Scores do not depend on
  * the choices.  `out` may be NULL. */
 esg_status esg_scorer_autotune(esg_scorer* scorer, esg_tune_report* out);
+/* The same, for a workload whose read lengths are sampled in `lens` (n of
+ * them; zeros ignored): the 16/32-row split is then chosen on one
+ * calibration batch drawn from that length histogram, every candidate split
+ * (0, 48, ..., 512) timed on it, the fastest kept (the per-length
+ * measurements still set the int32 lanes' length).  No counterpart in the
+ * reference. */
+esg_status esg_scorer_autotune_lengths(esg_scorer* scorer, const uint32_t* lens, uint32_t n,
+                                       esg_tune_report* out);
 /* Set the 16/32-row split by hand (0: every query on 32-row stripes). */
 esg_status esg_scorer_set_split(esg_scorer* scorer, uint32_t split_len);
 

@@ -333,6 +333,12 @@ def test_gpu_autotune_measures_and_keeps_results(oracle):
         assert rep["int32_from"] == 0
         for knob in ("ctas16", "ctas32", "chunk_target"):
             assert rep[knob]["chosen"] in rep[knob]["tried"] and all(t > 0 for t in rep[knob]["ms"])
+        # on the workload's length histogram: every split timed on one batch
+        rep = g.autotune(reads.lens)
+        hs = rep["split_on_histogram"]
+        assert len(hs["tried"]) == 8 and rep["split_len"] in hs["tried"]
+        best = min(hs["ms"])
+        assert hs["ms"][hs["tried"].index(rep["split_len"])] <= 1.01 * best
         info = g.info()
         assert info["tuned"] == 1 and info["split_len"] == rep["split_len"]
         after = g.score_batch(reads.tuple(), both_strands=True)
