@@ -1008,8 +1008,7 @@ __global__ void __launch_bounds__(kK3Threads, 4) k3_lanes(const K3Params P) {
     }
     if (unit >= n_units) break;
     const uint32_t pos = (uint32_t)(unit / tpq);
-    const uint32_t k_lo = (uint32_t)(unit - (unsigned long long)pos * tpq) * P.refs_per_task;
-    const uint32_t k_hi = min(k_lo + P.refs_per_task, P.n_refs);
+    const uint32_t u = (uint32_t)(unit - (unsigned long long)pos * tpq);
     const uint32_t q = P.list ? P.list[pos] : pos;
     const bool rc = q >= P.n_reads;
     const uint32_t rd = rc ? q - P.n_reads : q;
@@ -1022,6 +1021,11 @@ __global__ void __launch_bounds__(kK3Threads, 4) k3_lanes(const K3Params P) {
     const int passes = (S + W - 1) / W;
     const int c = lane / W, w = lane - c * W;
     const int pad = S * R - n;
+    // this unit's references: its share of the query's groups of C (whole
+    // groups, so only the query's very last group can be short)
+    const uint32_t groups = (P.n_refs + (uint32_t)C - 1) / (uint32_t)C;
+    const uint32_t k_lo = (uint32_t)((uint64_t)u * groups / tpq) * (uint32_t)C;
+    const uint32_t k_hi = min((uint32_t)((uint64_t)(u + 1) * groups / tpq) * (uint32_t)C, P.n_refs);
 
     for (uint32_t k0 = k_lo; k0 < k_hi; k0 += (uint32_t)C) {
       const uint32_t k = k0 + (uint32_t)c;
