@@ -1002,8 +1002,10 @@ static esg_status autotune_impl(esg_scorer* sc, const std::vector<uint32_t>& his
     uint64_t bases = 0;
     for (uint32_t v : hist) bases += v;
     const double mean = std::max(1.0, (double)bases / (double)hist.size());
-    const uint64_t want = (uint64_t)(2.0e11 / (2.0 * mean * (double)sc->panel_bases));
-    calib_reads(sc, 0, (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 64), 400000), x, c,
+    // about 1e12 cells (~0.2 s a launch): the splits differ by a percent or
+    // two on a whole batch, less than the noise of a 40-ms one
+    const uint64_t want = (uint64_t)(1.0e12 / (2.0 * mean * (double)sc->panel_bases));
+    calib_reads(sc, 0, (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 64), 500000), x, c,
                 hist);
     static const uint32_t kSplits[] = {0, 48, 80, 112, 160, 224, 320, 512};
     float best = 0;

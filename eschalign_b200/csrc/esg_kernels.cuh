@@ -230,11 +230,14 @@ struct K2Params {
 };
 
 // Bounded wait on an mbarrier phase (a TMA bulk copy's completion).  Gives
-// up after ~2^26 polls, setting an error bit the host reads (when `err` is
-// given).
+// up after 2^26 polls, setting an error bit the host reads.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_t* err) {
   const uint32_t addr = (uint32_t)__cvta_generic_to_shared(bar);
-  for (uint32_t it = 0; it < (1u << 26); ++it) {
+  // 2^26 polls; past them the thread that issued the copies (thread 0)
+  // keeps polling up to 2^24 more so that its copies in flight land before
+  // the CTA's shared memory is released
+  const uint32_t limit = (1u << 26) + (threadIdx.x == 0 ? (1u << 24) : 0u);
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -243,9 +246,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_
         : "=r"(done)
         : "r"(addr), "r"(phase)
         : "memory");
-    if (done) return true;
+    if (done) {
+      if (it < (1u << 26)) return true;
+      break;  // landed only in thread 0's extra polls: still a timeout
+    }
   }
-  if (err) atomicOr(err, kErrPanelWait);
+  atomicOr(err, kErrPanelWait);
   return false;
 }
 
@@ -279,13 +285,7 @@ __device__ __forceinline__ bool stage_panel(void* smem, const void* gsrc, uint32
   // One decision for the whole CTA: a thread that gave up and one that saw
   // the phase flip must not part ways (the survivors' warp-wide shuffles
   // would then run with exited lanes).
-  const bool all_ok = __syncthreads_and(ok) != 0;
-  if (!all_ok && threadIdx.x == 0) {
-    // give the copies in flight one more bounded wait before the CTA's
-    // shared memory is released
-    mbar_wait(bar, 0, nullptr);
-  }
-  return all_ok;
+  return __syncthreads_and(ok) != 0;
 }
 
 // One systolic pass of a warp over the columns of one reference pair.
