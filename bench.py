@@ -842,7 +842,9 @@ def run_c4(a, ctx, rank):
     cfg = adapter.config()
     g = GpuScorer(refs, Scoring(*C4_SCORING), Mode.SEMIGLOBAL, device=local_rank,
                   stream=ctx.stream.cuda_stream)
-    tune_rep = tune(g, a, pairs.lens[:40000])
+    # the lengths the scorer sees: mates after adapter trimming
+    _, trimmed = adapter.pair_adapters(pairs.slice(0, 40_000).tuple(), cfg)
+    tune_rep = tune(g, a, trimmed)
     batch = g.submit(g.prepare_pairs(pairs.tuple(), adapters=cfg, both_strands=True))
     st = g.finish_pairs(batch, keep=True).stats
     cells = st["cells"]
