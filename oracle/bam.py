@@ -1,0 +1,242 @@
+"""Test infrastructure: a CPU restatement of the reference CLI's BAM output
+for unpaired reads -- the records it writes for each read's mapping and their
+encoding -- used as the checker of the library's BAM writer.  Nothing under
+eschalign_b200/ imports it.
+
+Restated from crates/eschalign-cli/src/align.rs:
+* read_batches (align.rs:604-660): secondary and supplementary input records
+  are skipped; a record aligned to the reverse strand is refused;
+* process_chunk (align.rs:1504-1602): a read over --max-read-len is not
+  scored and is written as an unmapped read;
+* build_records (align.rs:1084-1200), OWNED_TAGS (align.rs:346-352),
+  int_value (align.rs:1001-1015), sam_cigar / clipped_span
+  (align.rs:1017-1052), xa_entry (align.rs:1054-1069): the output record of a
+  read and, with --secondary, one record per further hit;
+* the coordinate sort (align.rs:2406-2450): stable on (reference, position,
+  reverse flag), unmapped last;
+* the reverse complement of letters (crates/eschalign/src/alphabet.rs:69-80).
+
+The record buffer the CLI edits (noodles-sam's RecordBuf data) removes a tag
+by moving its last tag into the freed slot; the new tags go to the end.  The
+encoding is the BAM layout of the SAM specification (section 4.2) with its
+reg2bin.  Pinned on the reference's own golden digests (unpaired_golden.tsv:
+record count and FNV-1a 64 of the uncompressed record stream, as
+crates/eschalign-cli/tests/align_unpaired.rs:37-62 computes them) for six
+flag sets.
+"""
+from __future__ import annotations
+
+import gzip
+import struct
+
+SEQ_CODES = b"=ACMGRSVTWYHKDBN"
+CIGAR_CODES = {"M": 0, "I": 1, "D": 2, "N": 3, "S": 4, "H": 5, "P": 6, "=": 7, "X": 8}
+OWNED_TAGS = (b"NM", b"MD", b"AS", b"XS", b"XA")  # align.rs:346-352
+FLAG_REVERSE, FLAG_UNMAPPED, FLAG_SECONDARY = 0x10, 0x4, 0x100
+FLAG_QC_FAIL, FLAG_DUPLICATE, FLAG_SUPPLEMENTARY = 0x200, 0x400, 0x800
+_AUX_SIZE = {b"A": 1, b"c": 1, b"C": 1, b"s": 2, b"S": 2, b"i": 4, b"I": 4, b"f": 4}
+
+
+def split_aux(b: bytes):
+    """[(tag, encoded field bytes)] of a BAM record's auxiliary data."""
+    out, i = [], 0
+    while i < len(b):
+        tag, t = b[i:i + 2], b[i + 2:i + 3]
+        j = i + 3
+        if t in _AUX_SIZE:
+            j += _AUX_SIZE[t]
+        elif t in (b"Z", b"H"):
+            j = b.index(b"\0", j) + 1
+        elif t == b"B":
+            n = struct.unpack("<I", b[j + 1:j + 5])[0]
+            j += 5 + n * _AUX_SIZE[b[j:j + 1]]
+        else:
+            raise ValueError(f"unknown aux type {t!r}")
+        out.append((tag, b[i:j]))
+        i = j
+    return out
+
+
+def read_bam(data: bytes):
+    """(header text, [(name, length)], records) of a BGZF-compressed BAM;
+    a record is a dict of its flag, name, sequence letters, qualities and
+    (tag, field bytes) auxiliary list."""
+    raw = gzip.decompress(data)
+    if raw[:4] != b"BAM\1":
+        raise ValueError("not a BAM file")
+    lt = struct.unpack("<I", raw[4:8])[0]
+    text = raw[8:8 + lt]
+    o = 8 + lt
+    n_ref = struct.unpack("<I", raw[o:o + 4])[0]
+    o += 4
+    refs = []
+    for _ in range(n_ref):
+        ln = struct.unpack("<I", raw[o:o + 4])[0]
+        name = raw[o + 4:o + 4 + ln - 1]
+        refs.append((name, struct.unpack("<I", raw[o + 4 + ln:o + 8 + ln])[0]))
+        o += 8 + ln
+    recs = []
+    while o < len(raw):
+        bs = struct.unpack("<I", raw[o:o + 4])[0]
+        r = raw[o + 4:o + 4 + bs]
+        o += 4 + bs
+        (_, _, lrn, _, _, ncig, flag, lseq, _, _, _) = struct.unpack("<iiBBHHHIiii", r[:32])
+        p = 32
+        name = r[p:p + lrn - 1]
+        p += lrn + 4 * ncig
+        sb = r[p:p + (lseq + 1) // 2]
+        p += (lseq + 1) // 2
+        seq = bytes(SEQ_CODES[(sb[k // 2] >> (0 if k % 2 else 4)) & 0xF] for k in range(lseq))
+        qual = r[p:p + lseq]
+        p += lseq
+        recs.append({"flag": flag, "name": name, "seq": seq, "qual": qual,
+                     "aux": split_aux(r[p:])})
+    return text, refs, recs
+
+
+def input_reads(recs):
+    """read_batches (align.rs:604-660): the primary records, in order."""
+    out = []
+    for r in recs:
+        if r["flag"] & (FLAG_SECONDARY | FLAG_SUPPLEMENTARY):
+            continue
+        if not r["flag"] & FLAG_UNMAPPED and r["flag"] & FLAG_REVERSE:
+            raise ValueError("input record aligned to the reverse strand")
+        out.append(r)
+    return out
+
+
+def reg2bin(beg: int, end: int) -> int:
+    """The SAM specification's bin of [beg, end) (0-based, end exclusive)."""
+    end -= 1
+    for shift, base in ((14, 4681), (17, 585), (20, 73), (23, 9), (26, 1)):
+        if beg >> shift == end >> shift:
+            return base + (beg >> shift)
+    return 0
+
+
+def int_field(tag: bytes, v: int) -> bytes:
+    """int_value (align.rs:1001-1015): the smallest of u8, i8, u16, i16, u32,
+    else i32."""
+    for code, fmt, lo, hi in ((b"C", "<B", 0, 255), (b"c", "<b", -128, 127),
+                              (b"S", "<H", 0, 65535), (b"s", "<h", -32768, 32767),
+                              (b"I", "<I", 0, 2**32 - 1)):
+        if lo <= v <= hi:
+            return tag + code + struct.pack(fmt, v)
+    return tag + b"i" + struct.pack("<i", v)
+
+
+def str_field(tag: bytes, s: str) -> bytes:
+    return tag + b"Z" + s.encode() + b"\0"
+
+
+def encode_record(refid, pos, mapq, cigar, flag, name, seq, qual, aux) -> bytes:
+    """One BAM record (block_size included); cigar is [(length, op)], pos
+    0-based or -1, aux the encoded fields in order."""
+    span = sum(n for n, op in cigar if op in "MDN=X")
+    b = 4680 if pos < 0 else reg2bin(pos, pos + span)
+    nm = (name if name else b"*") + b"\0"
+    body = struct.pack("<iiBBHHHIiii", refid, pos, len(nm), mapq, b, len(cigar), flag, len(seq),
+                       -1, -1, 0)
+    body += nm + b"".join(struct.pack("<I", n << 4 | CIGAR_CODES[op]) for n, op in cigar)
+    sb = bytearray((len(seq) + 1) // 2)
+    for k, ch in enumerate(seq):
+        c = SEQ_CODES.find(bytes([ch]).upper())
+        sb[k // 2] |= (c if c >= 0 else 15) << (0 if k % 2 else 4)
+    body += bytes(sb) + (qual if len(qual) == len(seq) else b"\xff" * len(seq)) + b"".join(aux)
+    return struct.pack("<I", len(body)) + body
+
+
+def revcomp_letters(s: bytes) -> bytes:
+    """alphabet::reverse_complement (alphabet.rs:69-80)."""
+    m = {ord("A"): b"T", ord("C"): b"G", ord("G"): b"C", ord("T"): b"A", ord("U"): b"A"}
+    return b"".join(m.get(c, b"N") for c in bytes(s).upper()[::-1])
+
+
+def _cigar_ops(s: str):
+    out, n = [], ""
+    for ch in s:
+        if ch.isdigit():
+            n += ch
+        else:
+            out.append((int(n), ch))
+            n = ""
+    return out
+
+
+def _without_owned(aux):
+    """RecordBuf data with OWNED_TAGS removed: each removal moves the last
+    tag into the freed slot."""
+    aux = list(aux)
+    for t in OWNED_TAGS:
+        for i, (tag, _) in enumerate(aux):
+            if tag == t:
+                last = aux.pop()
+                if i < len(aux):
+                    aux[i] = last
+                break
+    return aux
+
+
+def build_records(rec, m, ref_names, secondary=False):
+    """build_records (align.rs:1084-1200) for one read and its mapping (the
+    oracle's map_reads form: best_score, n_tied, suboptimal, hits)."""
+    kept = rec["flag"] & (FLAG_QC_FAIL | FLAG_DUPLICATE)
+    aux = _without_owned(rec["aux"])
+    hits = m["hits"]
+    if not hits:
+        return [encode_record(-1, -1, 0, [], kept | FLAG_UNMAPPED, rec["name"], rec["seq"],
+                              rec["qual"], [f for _, f in aux])]
+    n = len(rec["seq"])
+
+    def sam_cigar(h):  # sam_cigar / clipped_span (align.rs:1017-1052)
+        c = [(h["query_start"], "S")] if h["query_start"] > 0 else []
+        c += _cigar_ops(h["cigar"])
+        if n > h["query_end"]:
+            c.append((n - h["query_end"], "S"))
+        return c
+
+    p = hits[0]
+    seq, qual, flag = rec["seq"], rec["qual"], kept
+    if p["reverse"]:
+        flag |= FLAG_REVERSE
+        seq, qual = revcomp_letters(seq), qual[::-1]
+    fields = [f for _, f in aux]
+    fields += [int_field(b"NM", p["nm"]), str_field(b"MD", p["md"]),
+               int_field(b"AS", m["best_score"])]
+    if m["suboptimal"] is not None:
+        fields.append(int_field(b"XS", m["suboptimal"]))
+    if len(hits) > 1:  # xa_entry (align.rs:1054-1069)
+        xa = "".join(f"{ref_names[h['reference']]},{'-' if h['reverse'] else '+'}"
+                     f"{h['ref_start'] + 1},{''.join(f'{k}{op}' for k, op in sam_cigar(h))},"
+                     f"{h['nm']};" for h in hits[1:])
+        fields.append(str_field(b"XA", xa))
+    out = [encode_record(p["reference"], p["ref_start"], 60 if m["n_tied"] == 1 else 0,
+                         sam_cigar(p), flag, rec["name"], seq, qual, fields)]
+    if secondary:
+        rg = [f for t, f in rec["aux"] if t == b"RG"]
+        for h in hits[1:]:
+            d = [int_field(b"NM", h["nm"]), str_field(b"MD", h["md"]),
+                 int_field(b"AS", m["best_score"])] + rg
+            out.append(encode_record(h["reference"], h["ref_start"], 0, sam_cigar(h),
+                                     FLAG_SECONDARY | kept | (FLAG_REVERSE if h["reverse"] else 0),
+                                     rec["name"], b"", b"", d))
+    return out
+
+
+def coordinate_order(records):
+    """The coordinate sort (align.rs:2406-2450): stable on (reference,
+    position, reverse), unmapped last."""
+    def key(r):
+        tid, pos = struct.unpack("<ii", r[4:12])
+        flag = struct.unpack("<H", r[18:20])[0]
+        return (tid if tid >= 0 else 1 << 40, pos, bool(flag & FLAG_REVERSE))
+    return sorted(records, key=key)
+
+
+def fnv1a64(b: bytes) -> int:
+    """The digest of crates/eschalign-cli/tests/align_unpaired.rs:37-62."""
+    h = 0xCBF29CE484222325
+    for x in b:
+        h = ((h ^ x) * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return h

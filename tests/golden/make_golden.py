@@ -23,8 +23,15 @@ It reads, as data:
   samtools calmd wrote for 21 CIGARs over reference ``N``, IUPAC, lower case
   and ``U`` (the reference's ``gen_calmd_golden.py``, checked by its
   ``tests/sam_fields.rs``);
+* ``crates/eschalign-cli/tests/fixtures/trna_mappings_padded.bam`` and
+  ``unpaired_golden.tsv`` -- the 60-record input BAM the reference's
+  ``tests/align_unpaired.rs`` aligns against ``trna_reference.fa`` under six
+  flag sets, and for each the record count and FNV-1a 64 digest of the
+  uncompressed output record stream its binary wrote;
 
-and writes the subset this project tests against into ``tests/golden/``:
+and writes the subset this project tests against into ``tests/golden/``
+(the input BAM's bytes unchanged as ``unpaired_input.bam``, the digests as
+``unpaired_golden.json``):
 ``align_golden_scores.json`` (query, reference, mode, scheme, score and the
 parasail end coordinates), the two panels as ``panel_trna*.json`` (name +
 letters, file order) and the paired fixture as ``pairs_fixture.json`` (panel
@@ -108,6 +115,29 @@ def main(ref_root):
                    "reference": cm["reference"]["seq"],
                    "records": [{k: r[k] for k in ("name", "pos", "cigar", "seq", "md", "nm")}
                                for r in cm["records"]]}, fh, indent=0)
+    fix = os.path.join(ref_root, "crates/eschalign-cli/tests/fixtures")
+    with open(os.path.join(fix, "trna_mappings_padded.bam"), "rb") as fh:
+        bam = fh.read()
+    with open(os.path.join(here, "unpaired_input.bam"), "wb") as fh:
+        fh.write(bam)
+    rows = {}
+    with open(os.path.join(fix, "unpaired_golden.tsv")) as fh:
+        for line in fh:
+            if line.strip():
+                label, n, digest = line.split()
+                rows[label] = {"records": int(n), "fnv1a64": digest}
+    with open(os.path.join(here, "unpaired_golden.json"), "w") as fh:
+        json.dump({"about": "records and FNV-1a 64 digest of the uncompressed BAM record "
+                            "stream (header skipped) the reference CLI wrote for "
+                            "unpaired_input.bam against the trna panel, per flag set "
+                            "(reference fixture unpaired_golden.tsv, test align_unpaired.rs)",
+                   "flags": {"default": [], "semiglobal_both_secondary":
+                             ["--mode", "semiglobal", "--strand", "both", "--secondary"],
+                             "sort_coordinate": ["--sort", "coordinate"],
+                             "min_score_max_ties": ["--min-score", "60", "--max-ties", "1"],
+                             "scoring_bwa": ["--scoring", "1,-1,-2,-1", "--strand", "both"],
+                             "max_read_len": ["--max-read-len", "60"]},
+                   "digests": rows}, fh, indent=1)
     print(f"{len(cases)} golden scores, {len(out['fixture_reads'])} fixture reads, "
           f"{len(pairs)} fixture pairs, {len(cm['records'])} calmd records")
 
