@@ -38,6 +38,8 @@ def _compile(src, out: str, verbose: bool) -> None:
     srcs = [src] if isinstance(src, str) else list(src)
     cmd = [nvcc(), *ARCH_FLAGS, *NVCC_FLAGS, *(os.path.join(CSRC, f) for f in srcs), "-o",
            out + ".tmp"]
+    if "esg_bam.cu" in srcs:
+        cmd.append("-lz")
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)
@@ -49,7 +51,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     probe csrc/esg_probe.cu into libesg_probe.so (sm_100a, ahead of time)."""
     newest = max(os.path.getmtime(s) for s in sources())
     for src, out in ((("esg_api.cu", "esg_server.cu", "esg_trace.cu", "esg_map.cu",
-                        "esg_noalloc.cu"), LIB_PATH),
+                        "esg_bam.cu", "esg_noalloc.cu"), LIB_PATH),
                      ("esg_probe.cu", PROBE_PATH)):
         if force or not os.path.exists(out) or os.path.getmtime(out) < newest:
             _compile(src, out, verbose)
@@ -143,6 +145,10 @@ class EsgPairMapOptions(C.Structure):
                 ("max_insert", C.c_uint32), ("both_strands", C.c_uint32)]
 
 
+class EsgBamOptions(C.Structure):
+    _fields_ = [("secondary", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class EsgServerOptions(C.Structure):
     _fields_ = [("max_batch_reads", C.c_uint32), ("max_inflight", C.c_uint32),
                 ("memory_budget", C.c_uint64), ("memory_headroom", C.c_uint64),
@@ -224,6 +230,9 @@ SIGNATURES = {
     "esg_mapping_ops": (C.c_void_p, [C.c_void_p, _u64p]),
     "esg_mapping_md": (C.c_void_p, [C.c_void_p, _u64p]),
     "esg_mapping_free": (None, [C.c_void_p]),
+    "esg_mapping_from_arrays": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, _u32p,
+                                            C.c_uint64, C.c_char_p, C.c_uint64,
+                                            C.POINTER(C.c_void_p)]),
     "esg_server_new": (C.c_int32, [C.POINTER(EsgServerOptions), C.POINTER(C.c_void_p)]),
     "esg_server_add_scorer": (C.c_int32, [C.c_void_p, C.c_void_p, _u32p]),
     "esg_server_submit": (C.c_int32, [C.c_void_p, C.c_uint32, _u8p, _u64p, _u32p, C.c_uint32,
@@ -232,6 +241,23 @@ SIGNATURES = {
                                     C.POINTER(EsgRequestTiming)]),
     "esg_server_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(EsgServerStats)]),
     "esg_server_free": (None, [C.c_void_p]),
+    "esg_bam_open": (C.c_int32, [C.c_char_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "esg_bam_header_text": (C.c_void_p, [C.c_void_p, _u64p]),
+    "esg_bam_read_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "esg_bam_batch_reads": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_void_p), _u32p]),
+    "esg_bam_batch_free": (None, [C.c_void_p]),
+    "esg_bam_close": (None, [C.c_void_p]),
+    "esg_bam_encode": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(EsgBamOptions),
+                                   C.POINTER(C.c_char_p), C.c_uint32, C.c_uint32,
+                                   C.POINTER(C.c_void_p)]),
+    "esg_bam_records_bytes": (C.c_void_p, [C.c_void_p, _u64p, _u32p]),
+    "esg_bam_records_free": (None, [C.c_void_p]),
+    "esg_bam_writer_open": (C.c_int32, [C.c_char_p, C.c_char_p, C.POINTER(C.c_char_p), _u32p,
+                                        C.c_uint32, C.c_int32, C.c_uint32,
+                                        C.POINTER(C.c_void_p)]),
+    "esg_bam_writer_push": (C.c_int32, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    "esg_bam_writer_close": (C.c_int32, [C.c_void_p]),
     "esg_score_rows_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_uint32, C.POINTER(EsgScoring), C.c_int32,

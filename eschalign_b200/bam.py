@@ -1,0 +1,240 @@
+"""BAM input and output around the mapping stage (esg_bam_*), and the CLI's
+unpaired pipeline over them.
+
+The reference's `eschalign` binary reads a BAM in batches (read_batches,
+crates/eschalign-cli/src/align.rs:604-660), maps them
+(Aligner::map_reads_scored), turns each read's mapping into its output
+records (build_records, align.rs:1084-1200) and writes them in input order or
+coordinate order (write_in_order, align.rs:2345-2400; the sort, 2406-2450).
+`align_bam` does the same with the library: batches from `BamReader`,
+`GpuScorer.map_reads` on the device, `encode` and `BamWriter` on host threads.
+The records are the reference CLI's byte for byte.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native
+from .scorer import HIT_DTYPE, MAPPING_DTYPE, Mappings, _check, _ptr
+
+
+def _lib():
+    return _native.load()
+
+
+class BamBatch:
+    """A batch of primary input records and their reads as alphabet codes
+    (reads over the reader's max_read_len have length 0: left unmapped)."""
+
+    def __init__(self, h):
+        self._h = h
+        lib = _lib()
+        codes, off, lens = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        n = C.c_uint32()
+        _check(lib, lib.esg_bam_batch_reads(h, C.byref(codes), C.byref(off), C.byref(lens),
+                                            C.byref(n)))
+        self.n = n.value
+        if self.n:
+            self.lens = np.ctypeslib.as_array((C.c_uint32 * self.n).from_address(lens.value)).copy()
+            self.off = np.ctypeslib.as_array((C.c_uint64 * self.n).from_address(off.value)).copy()
+            total = int(self.lens.sum(dtype=np.uint64))
+            self.codes = (np.ctypeslib.as_array((C.c_uint8 * total).from_address(codes.value)).copy()
+                          if total else np.zeros(1, np.uint8))
+        else:
+            self.lens = np.zeros(0, np.uint32)
+            self.off = np.zeros(0, np.uint64)
+            self.codes = np.zeros(1, np.uint8)
+
+    def __len__(self):
+        return self.n
+
+    def reads(self):
+        """(codes, off, lens) for GpuScorer.map_reads."""
+        return self.codes, self.off, self.lens
+
+    def free(self):
+        if self._h:
+            _lib().esg_bam_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class BamReader:
+    """esg_bam_open: a BGZF BAM's header and its primary records in batches."""
+
+    def __init__(self, path: str, threads: int = 0):
+        self._lib = _lib()
+        h = C.c_void_p()
+        _check(self._lib, self._lib.esg_bam_open(path.encode(), threads, C.byref(h)))
+        self._h = h
+        n = C.c_uint64()
+        p = self._lib.esg_bam_header_text(h, C.byref(n))
+        self.header_text = C.string_at(p, n.value) if n.value else b""
+
+    def batches(self, max_reads: int = 50_000, max_read_len: int = 1000):
+        while True:
+            b = C.c_void_p()
+            _check(self._lib, self._lib.esg_bam_read_batch(self._h, max_reads, max_read_len,
+                                                           C.byref(b)))
+            batch = BamBatch(b)
+            if not len(batch):
+                batch.free()
+                return
+            yield batch
+
+    def close(self):
+        if self._h:
+            self._lib.esg_bam_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BamRecords:
+    """Encoded output records (esg_bam_encode): the uncompressed BAM record
+    stream of a batch, in read order."""
+
+    def __init__(self, h):
+        self._h = h
+        lib = _lib()
+        nb, nr = C.c_uint64(), C.c_uint32()
+        p = lib.esg_bam_records_bytes(h, C.byref(nb), C.byref(nr))
+        self.n_records = nr.value
+        self.nbytes = nb.value
+        self._p = p
+
+    def bytes(self) -> bytes:
+        return C.string_at(self._p, self.nbytes) if self.nbytes else b""
+
+    def free(self):
+        if self._h:
+            _lib().esg_bam_records_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _names(ref_names):
+    names = [n.encode() if isinstance(n, str) else bytes(n) for n in ref_names]
+    return (C.c_char_p * max(len(names), 1))(*names), len(names)
+
+
+def mapping_handle(m: Mappings):
+    """An esg_mapping (esg_mapping_from_arrays) holding `m`'s arrays; free it
+    with esg_mapping_free."""
+    lib = _lib()
+    reads = np.ascontiguousarray(m.reads, dtype=MAPPING_DTYPE)
+    hits = np.ascontiguousarray(m.hits, dtype=HIT_DTYPE)
+    ops = np.ascontiguousarray(m.ops, dtype=np.uint32)
+    md = bytes(m.md_bytes)
+    h = C.c_void_p()
+    _check(lib, lib.esg_mapping_from_arrays(reads.ctypes.data, reads.size, hits.ctypes.data,
+                                            hits.size, _ptr(ops, C.c_uint32), ops.size, md,
+                                            len(md), C.byref(h)))
+    return h
+
+
+def encode(batch: BamBatch, mapping, ref_names, secondary: bool = False,
+           threads: int = 0) -> BamRecords:
+    """build_records (align.rs:1084-1200) for every read of `batch` from its
+    mapping (a Mappings, or an esg_mapping handle)."""
+    lib = _lib()
+    own = isinstance(mapping, Mappings)
+    h = mapping_handle(mapping) if own else mapping
+    names, n = _names(ref_names)
+    opts = _native.EsgBamOptions(int(bool(secondary)), 0)
+    out = C.c_void_p()
+    try:
+        _check(lib, lib.esg_bam_encode(batch._h, h, C.byref(opts), names, n, threads,
+                                       C.byref(out)))
+    finally:
+        if own:
+            lib.esg_mapping_free(h)
+    return BamRecords(out)
+
+
+class BamWriter:
+    """esg_bam_writer_*: header, then pushed chunks in sequence order (or in
+    coordinate order at close), BGZF-compressed on host threads."""
+
+    def __init__(self, path: str, header_text: bytes, ref_names, ref_lens,
+                 sort_coordinate: bool = False, threads: int = 0):
+        self._lib = _lib()
+        names, n = _names(ref_names)
+        lens = np.ascontiguousarray(ref_lens, dtype=np.uint32)
+        h = C.c_void_p()
+        _check(self._lib, self._lib.esg_bam_writer_open(
+            path.encode(), header_text, names, _ptr(lens, C.c_uint32), n,
+            int(bool(sort_coordinate)), threads, C.byref(h)))
+        self._h = h
+
+    def push(self, seq: int, records: BamRecords):
+        _check(self._lib, self._lib.esg_bam_writer_push(self._h, seq, records._h))
+
+    def close(self):
+        if self._h:
+            h, self._h = self._h, None
+            _check(self._lib, self._lib.esg_bam_writer_close(h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def header_text(ref_names, ref_lens, sort_coordinate: bool = False) -> bytes:
+    """@HD (SO as the CLI writes it) and an @SQ line per reference."""
+    so = "coordinate" if sort_coordinate else "unsorted"
+    lines = [f"@HD\tVN:1.6\tSO:{so}"]
+    for n, ln in zip(ref_names, ref_lens):
+        lines.append(f"@SQ\tSN:{n if isinstance(n, str) else n.decode()}\tLN:{int(ln)}")
+    lines.append("@PG\tID:eschalign-b200\tPN:eschalign-b200")
+    return ("\n".join(lines) + "\n").encode()
+
+
+def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
+              min_score: int = 0, max_ties: int | None = None, both_strands: bool = False,
+              secondary: bool = False, sort_coordinate: bool = False,
+              max_read_len: int = 1000, batch_size: int = 50_000, threads: int = 0) -> dict:
+    """The CLI's unpaired run (align.rs:1822-2250, the --device gpu path) over
+    a scorer: every batch of `in_path` mapped on the device (map_reads_scored
+    with min_score / max_ties / both strands), its records built and written
+    to `out_path` in order (or coordinate order).  Returns counts."""
+    ref_lens = [len(r) for r in ref_letters]
+    out = {"reads": 0, "records": 0, "batches": 0}
+    with BamReader(in_path, threads) as rd, \
+            BamWriter(out_path, header_text(ref_names, ref_lens, sort_coordinate), ref_names,
+                      ref_lens, sort_coordinate, threads) as wr:
+        for seq, batch in enumerate(rd.batches(batch_size, max_read_len)):
+            m = scorer.map_reads(batch.reads(), min_score=min_score, max_ties=max_ties,
+                                 both_strands=both_strands, ref_letters=ref_letters)
+            rec = encode(batch, m, ref_names, secondary, threads)
+            wr.push(seq, rec)
+            out["reads"] += len(batch)
+            out["records"] += rec.n_records
+            out["batches"] += 1
+            rec.free()
+            batch.free()
+    return out

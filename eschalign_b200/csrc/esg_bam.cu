@@ -1,0 +1,793 @@
+// esg_bam.cu -- BAM input and output around the mapping stage (host code).
+//
+// The CLI's I/O stage for unpaired reads (crates/eschalign-cli/src/align.rs):
+//   * reading: read_batches (align.rs:604-660) -- primary records of a BGZF
+//     BAM in batches; secondary and supplementary records skipped; a record
+//     aligned to the reverse strand refused;
+//   * the output records of a read's mapping: build_records
+//     (align.rs:1084-1200) with OWNED_TAGS (346-352), int_value (1001-1015),
+//     sam_cigar / clipped_span (1017-1052), xa_entry (1054-1069); a read over
+//     --max-read-len is written unmapped (process_chunk, 1504-1602);
+//   * writing: write_in_order (align.rs:2345-2400) -- chunks in sequence
+//     order -- or the coordinate sort (2406-2450): stable on (reference,
+//     position, reverse), unmapped last; BGZF blocks with the end marker.
+//
+// The records are built directly in the BAM layout of the SAM specification
+// (section 4.2).  Input tags the CLI does not own are kept byte for byte; the
+// owned ones are removed the way its record buffer removes a tag -- the last
+// tag moves into the freed slot -- and the new ones appended.  Sequences stay
+// in the 4-bit BAM encoding throughout (a reverse hit's read is complemented
+// in that encoding).  BGZF blocks are inflated and deflated with zlib on
+// several host threads.
+#include "../../include/eschalign_b200.h"
+
+#include <zlib.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+
+extern "C" void esg_internal_set_error(esg_status st, const char* msg);
+
+namespace {
+
+esg_status berr(esg_status st, const std::string& msg) {
+  esg_internal_set_error(st, msg.c_str());
+  return st;
+}
+
+uint32_t u32_at(const uint8_t* p) {
+  uint32_t v;
+  memcpy(&v, p, 4);
+  return v;
+}
+int32_t i32_at(const uint8_t* p) {
+  int32_t v;
+  memcpy(&v, p, 4);
+  return v;
+}
+uint16_t u16_at(const uint8_t* p) {
+  uint16_t v;
+  memcpy(&v, p, 2);
+  return v;
+}
+void put32(std::vector<uint8_t>& o, uint32_t v) {
+  const size_t n = o.size();
+  o.resize(n + 4);
+  memcpy(o.data() + n, &v, 4);
+}
+void put16(std::vector<uint8_t>& o, uint16_t v) {
+  const size_t n = o.size();
+  o.resize(n + 2);
+  memcpy(o.data() + n, &v, 2);
+}
+
+uint32_t threads_or(uint32_t t) {
+  if (t) return t;
+  return std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+}
+
+template <typename F>
+void parallel_for(size_t n, uint32_t threads, F&& f) {
+  const uint32_t t = (uint32_t)std::min<size_t>(threads, std::max<size_t>(n, 1));
+  if (t <= 1) {
+    for (size_t i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::vector<std::thread> th;
+  for (uint32_t k = 0; k < t; ++k)
+    th.emplace_back([&]() {
+      for (size_t i; (i = next.fetch_add(1)) < n;) f(i);
+    });
+  for (auto& x : th) x.join();
+}
+
+// ---------------------------------------------------------------- BGZF
+constexpr size_t kBgzfMaxIn = 0xff00;  // uncompressed bytes per written block
+const uint8_t kBgzfEof[28] = {0x1f, 0x8b, 8, 4, 0, 0, 0, 0, 0, 0xff, 6, 0, 0x42, 0x43,
+                              2,    0,    0x1b, 0, 3, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+
+// Inflate BGZF blocks [first, first + n) of `data` (offsets in `starts`)
+// into `out`, in order, in parallel.
+esg_status inflate_blocks(const std::vector<uint8_t>& data, const std::vector<size_t>& starts,
+                          size_t first, size_t n, uint32_t threads, std::vector<uint8_t>& out) {
+  std::vector<std::vector<uint8_t>> parts(n);
+  std::atomic<int> bad{0};
+  parallel_for(n, threads, [&](size_t i) {
+    const size_t s = starts[first + i], e = starts[first + i + 1];
+    const uint8_t* b = data.data() + s;
+    const uint16_t xlen = u16_at(b + 10);
+    const size_t cstart = 12 + xlen, clen = (e - s) - cstart - 8;
+    const uint32_t isize = u32_at(b + (e - s) - 4);
+    parts[i].resize(isize);
+    if (!isize) return;
+    z_stream z{};
+    if (inflateInit2(&z, -15) != Z_OK) {
+      bad = 1;
+      return;
+    }
+    z.next_in = const_cast<Bytef*>(b + cstart);
+    z.avail_in = (uInt)clen;
+    z.next_out = parts[i].data();
+    z.avail_out = isize;
+    const int rc = inflate(&z, Z_FINISH);
+    inflateEnd(&z);
+    if (rc != Z_STREAM_END || z.avail_out != 0 ||
+        crc32(0L, parts[i].data(), isize) != u32_at(b + (e - s) - 8))
+      bad = 1;
+  });
+  if (bad) return berr(ESG_ERR_BAD_ARGUMENT, "corrupt BGZF block");
+  for (auto& p : parts) out.insert(out.end(), p.begin(), p.end());
+  return ESG_OK;
+}
+
+// One BGZF block holding `n` bytes of `src`.
+void deflate_block(const uint8_t* src, size_t n, int level, std::vector<uint8_t>& out) {
+  z_stream z{};
+  deflateInit2(&z, level, Z_DEFLATED, -15, 8, Z_DEFAULT_STRATEGY);
+  std::vector<uint8_t> c(deflateBound(&z, (uLong)n) + 32);
+  z.next_in = const_cast<Bytef*>(src);
+  z.avail_in = (uInt)n;
+  z.next_out = c.data();
+  z.avail_out = (uInt)c.size();
+  deflate(&z, Z_FINISH);
+  const size_t clen = c.size() - z.avail_out;
+  deflateEnd(&z);
+  const uint8_t head[18] = {0x1f, 0x8b, 8, 4, 0, 0, 0, 0, 0, 0xff, 6, 0, 0x42, 0x43, 2, 0, 0, 0};
+  out.assign(head, head + 18);
+  const uint16_t bsize = (uint16_t)(18 + clen + 8 - 1);
+  memcpy(out.data() + 16, &bsize, 2);
+  out.insert(out.end(), c.data(), c.data() + clen);
+  put32(out, (uint32_t)crc32(0L, src, (uInt)n));
+  put32(out, (uint32_t)n);
+}
+
+// ---------------------------------------------------------------- records
+// BAM's 4-bit base codes: complement (A<->T, C<->G; anything else N, as the
+// reference's letter complement makes it) and to the alphabet's codes 0-4.
+const uint8_t kComp4[16] = {15, 8, 4, 15, 2, 15, 15, 15, 1, 15, 15, 15, 15, 15, 15, 15};
+const uint8_t kCode4[16] = {4, 0, 1, 4, 2, 4, 4, 4, 3, 4, 4, 4, 4, 4, 4, 4};
+
+struct InRec {  // one input record, `rec` pointing past its block_size
+  const uint8_t* rec;
+  uint32_t size;
+  uint32_t name_len;  // l_read_name (with the NUL)
+  uint32_t n_cigar, l_seq;
+  uint16_t flag;
+  uint32_t aux_off;   // offset of the auxiliary data in rec
+  uint32_t seq_off;
+};
+
+bool parse_rec(const uint8_t* r, uint32_t size, InRec& x) {
+  if (size < 32) return false;
+  x.rec = r;
+  x.size = size;
+  x.name_len = r[8];
+  x.n_cigar = u16_at(r + 12);
+  x.flag = u16_at(r + 14);
+  x.l_seq = u32_at(r + 16);
+  x.seq_off = 32 + x.name_len + 4 * x.n_cigar;
+  x.aux_off = x.seq_off + (x.l_seq + 1) / 2 + x.l_seq;
+  return x.aux_off <= size;
+}
+
+// (offset, length) of each auxiliary field of a record
+bool split_aux(const uint8_t* a, uint32_t n, std::vector<std::pair<uint32_t, uint32_t>>& out) {
+  out.clear();
+  uint32_t i = 0;
+  auto size_of = [](uint8_t t) -> int {
+    switch (t) {
+      case 'A': case 'c': case 'C': return 1;
+      case 's': case 'S': return 2;
+      case 'i': case 'I': case 'f': return 4;
+      default: return -1;
+    }
+  };
+  while (i < n) {
+    if (i + 3 > n) return false;
+    const uint8_t t = a[i + 2];
+    uint32_t j = i + 3;
+    if (size_of(t) > 0) {
+      j += size_of(t);
+    } else if (t == 'Z' || t == 'H') {
+      while (j < n && a[j]) ++j;
+      ++j;
+    } else if (t == 'B') {
+      if (j + 5 > n || size_of(a[j]) <= 0) return false;
+      j += 5 + u32_at(a + j + 1) * (uint32_t)size_of(a[j]);
+    } else {
+      return false;
+    }
+    if (j > n) return false;
+    out.push_back({i, j - i});
+    i = j;
+  }
+  return true;
+}
+
+void int_field(std::vector<uint8_t>& o, const char tag[2], int64_t v) {
+  o.push_back((uint8_t)tag[0]);
+  o.push_back((uint8_t)tag[1]);
+  if (v >= 0 && v <= 255) {
+    o.push_back('C');
+    o.push_back((uint8_t)v);
+  } else if (v >= -128 && v <= 127) {
+    o.push_back('c');
+    o.push_back((uint8_t)(int8_t)v);
+  } else if (v >= 0 && v <= 65535) {
+    o.push_back('S');
+    put16(o, (uint16_t)v);
+  } else if (v >= -32768 && v <= 32767) {
+    o.push_back('s');
+    put16(o, (uint16_t)(int16_t)v);
+  } else if (v >= 0 && v <= 0xffffffffll) {
+    o.push_back('I');
+    put32(o, (uint32_t)v);
+  } else {
+    o.push_back('i');
+    put32(o, (uint32_t)(int32_t)v);
+  }
+}
+
+void str_field(std::vector<uint8_t>& o, const char tag[2], const char* s, size_t n) {
+  o.push_back((uint8_t)tag[0]);
+  o.push_back((uint8_t)tag[1]);
+  o.push_back('Z');
+  o.insert(o.end(), s, s + n);
+  o.push_back(0);
+}
+
+uint16_t reg2bin(int64_t beg, int64_t end) {
+  --end;
+  if (beg >> 14 == end >> 14) return (uint16_t)(((1 << 15) - 1) / 7 + (beg >> 14));
+  if (beg >> 17 == end >> 17) return (uint16_t)(((1 << 12) - 1) / 7 + (beg >> 17));
+  if (beg >> 20 == end >> 20) return (uint16_t)(((1 << 9) - 1) / 7 + (beg >> 20));
+  if (beg >> 23 == end >> 23) return (uint16_t)(((1 << 6) - 1) / 7 + (beg >> 23));
+  if (beg >> 26 == end >> 26) return (uint16_t)(((1 << 3) - 1) / 7 + (beg >> 26));
+  return 0;
+}
+
+// A hit's SAM CIGAR words: soft clips around the aligned span.
+void sam_cigar(const esg_hit& h, const uint32_t* ops, uint32_t read_len, std::vector<uint32_t>& c) {
+  c.clear();
+  const esg_alignment& a = h.alignment;
+  if (a.query_start > 0) c.push_back(a.query_start << 4 | 4u);
+  for (uint32_t k = 0; k < a.n_ops; ++k) c.push_back(ops[a.ops_offset + k]);
+  if (read_len > a.query_end) c.push_back((read_len - a.query_end) << 4 | 4u);
+}
+
+// One record in the BAM layout.  seq4: 4-bit codes, one per byte.
+void encode_record(std::vector<uint8_t>& o, int32_t ref, int32_t pos, uint8_t mapq,
+                   const std::vector<uint32_t>& cigar, uint16_t flag, const uint8_t* name,
+                   uint32_t name_len, const uint8_t* seq4, uint32_t l_seq, const uint8_t* qual,
+                   bool have_qual, const std::vector<uint8_t>& aux) {
+  const size_t at = o.size();
+  put32(o, 0);  // block_size, set below
+  put32(o, (uint32_t)ref);
+  put32(o, (uint32_t)pos);
+  uint32_t span = 0;
+  for (uint32_t w : cigar) {
+    const uint32_t op = w & 0xfu;
+    if (op == 0 || op == 2 || op == 3 || op == 7 || op == 8) span += w >> 4;
+  }
+  const uint16_t bin = pos < 0 ? 4680 : reg2bin(pos, (int64_t)pos + span);
+  const uint8_t* nm = name_len > 1 ? name : (const uint8_t*)"*";
+  const uint32_t nl = name_len > 1 ? name_len : 2;
+  o.push_back((uint8_t)nl);
+  o.push_back(mapq);
+  put16(o, bin);
+  put16(o, (uint16_t)cigar.size());
+  put16(o, flag);
+  put32(o, l_seq);
+  put32(o, 0xffffffffu);
+  put32(o, 0xffffffffu);
+  put32(o, 0);
+  o.insert(o.end(), nm, nm + nl - 1);
+  o.push_back(0);
+  for (uint32_t w : cigar) put32(o, w);
+  for (uint32_t k = 0; k < l_seq; k += 2)
+    o.push_back((uint8_t)(seq4[k] << 4 | (k + 1 < l_seq ? seq4[k + 1] : 0)));
+  if (have_qual)
+    o.insert(o.end(), qual, qual + l_seq);
+  else
+    o.insert(o.end(), l_seq, 0xff);
+  o.insert(o.end(), aux.begin(), aux.end());
+  const uint32_t bs = (uint32_t)(o.size() - at - 4);
+  memcpy(o.data() + at, &bs, 4);
+}
+
+}  // namespace
+
+// ===================================================================== reader
+struct esg_bam_reader {
+  FILE* f = nullptr;
+  uint32_t threads = 1;
+  std::vector<uint8_t> text;
+  std::vector<std::string> ref_names;
+  std::vector<uint32_t> ref_lens;
+  std::vector<uint8_t> buf;  // inflated bytes not yet consumed
+  size_t pos = 0;            // consumed prefix of buf
+  bool eof = false;
+  uint64_t skipped = 0;      // secondary / supplementary records
+};
+
+struct esg_bam_batch {
+  std::vector<uint8_t> bytes;  // the batch's records, each without block_size
+  std::vector<InRec> recs;
+  std::vector<uint8_t> codes;  // alphabet codes of every read, concatenated
+  std::vector<uint64_t> off;
+  std::vector<uint32_t> len;
+  std::vector<uint32_t> full_len;  // lengths before --max-read-len
+};
+
+struct esg_bam_records {
+  std::vector<uint8_t> bytes;
+  uint32_t n_records = 0;
+  uint32_t n_unmapped = 0;
+};
+
+// Inflate more blocks into r->buf: up to `want` more blocks, read from the
+// file in one go and inflated in parallel.
+static esg_status fill(esg_bam_reader* r, size_t want) {
+  if (r->eof) return ESG_OK;
+  if (r->pos > (1u << 24)) {  // drop the consumed prefix now and then
+    r->buf.erase(r->buf.begin(), r->buf.begin() + (long)r->pos);
+    r->pos = 0;
+  }
+  std::vector<uint8_t> data;
+  std::vector<size_t> starts{0};
+  for (size_t k = 0; k < want; ++k) {
+    uint8_t head[18];
+    const size_t got = fread(head, 1, 18, r->f);
+    if (got == 0) {
+      r->eof = true;
+      break;
+    }
+    if (got != 18 || head[0] != 0x1f || head[1] != 0x8b || !(head[3] & 4))
+      return berr(ESG_ERR_BAD_ARGUMENT, "not a BGZF file");
+    const uint16_t xlen = u16_at(head + 10);
+    if (xlen != 6 || head[12] != 'B' || head[13] != 'C')
+      return berr(ESG_ERR_BAD_ARGUMENT, "BGZF block without its size field");
+    const uint32_t bsize = (uint32_t)u16_at(head + 16) + 1;
+    const size_t s = data.size();
+    data.resize(s + bsize);
+    memcpy(data.data() + s, head, 18);
+    if (fread(data.data() + s + 18, 1, bsize - 18, r->f) != bsize - 18)
+      return berr(ESG_ERR_BAD_ARGUMENT, "truncated BGZF block");
+    starts.push_back(data.size());
+  }
+  if (starts.size() > 1)
+    return inflate_blocks(data, starts, 0, starts.size() - 1, r->threads, r->buf);
+  return ESG_OK;
+}
+
+// At least n unconsumed bytes in r->buf (false at the end of the file).
+static esg_status need(esg_bam_reader* r, size_t n, bool* ok) {
+  while (r->buf.size() - r->pos < n && !r->eof) {
+    const esg_status st = fill(r, (size_t)r->threads * 8);
+    if (st != ESG_OK) return st;
+  }
+  *ok = r->buf.size() - r->pos >= n;
+  return ESG_OK;
+}
+
+extern "C" {
+
+esg_status esg_bam_open(const char* path, uint32_t threads, esg_bam_reader** out) {
+  if (!path || !out) return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  auto* r = new esg_bam_reader();
+  r->threads = threads_or(threads);
+  r->f = fopen(path, "rb");
+  if (!r->f) {
+    delete r;
+    return berr(ESG_ERR_BAD_ARGUMENT, std::string("cannot open ") + path);
+  }
+  bool ok = false;
+  esg_status st = need(r, 8, &ok);
+  auto fail = [&](esg_status s, const char* m) {
+    esg_bam_close(r);
+    return st != ESG_OK ? st : berr(s, m);
+  };
+  if (st != ESG_OK || !ok || memcmp(r->buf.data(), "BAM\1", 4) != 0)
+    return fail(ESG_ERR_BAD_ARGUMENT, "not a BAM file");
+  const uint32_t lt = u32_at(r->buf.data() + 4);
+  if ((st = need(r, 12 + (size_t)lt, &ok)) != ESG_OK || !ok)
+    return fail(ESG_ERR_BAD_ARGUMENT, "truncated BAM header");
+  r->text.assign(r->buf.begin() + 8, r->buf.begin() + 8 + lt);
+  r->pos = 8 + lt;
+  const uint32_t n_ref = u32_at(r->buf.data() + r->pos);
+  r->pos += 4;
+  for (uint32_t k = 0; k < n_ref; ++k) {
+    if ((st = need(r, 4, &ok)) != ESG_OK || !ok) return fail(ESG_ERR_BAD_ARGUMENT, "truncated");
+    const uint32_t ln = u32_at(r->buf.data() + r->pos);
+    if ((st = need(r, 8 + (size_t)ln, &ok)) != ESG_OK || !ok)
+      return fail(ESG_ERR_BAD_ARGUMENT, "truncated BAM references");
+    const char* nm = (const char*)r->buf.data() + r->pos + 4;
+    r->ref_names.emplace_back(nm, ln ? ln - 1 : 0);
+    r->ref_lens.push_back(u32_at(r->buf.data() + r->pos + 4 + ln));
+    r->pos += 8 + ln;
+  }
+  *out = r;
+  return ESG_OK;
+}
+
+const char* esg_bam_header_text(const esg_bam_reader* r, uint64_t* len) {
+  if (!r) return nullptr;
+  if (len) *len = r->text.size();
+  return (const char*)r->text.data();
+}
+
+esg_status esg_bam_read_batch(esg_bam_reader* r, uint32_t max_reads, uint32_t max_read_len,
+                              esg_bam_batch** out) {
+  if (!r || !out || !max_reads) return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument or batch of 0");
+  *out = nullptr;
+  auto* b = new esg_bam_batch();
+  std::vector<uint64_t> rec_off;
+  while (b->recs.size() < max_reads) {
+    bool ok = false;
+    esg_status st = need(r, 4, &ok);
+    if (st != ESG_OK) {
+      delete b;
+      return st;
+    }
+    if (!ok) break;
+    const uint32_t bs = u32_at(r->buf.data() + r->pos);
+    if ((st = need(r, 4 + (size_t)bs, &ok)) != ESG_OK || !ok) {
+      delete b;
+      return st != ESG_OK ? st : berr(ESG_ERR_BAD_ARGUMENT, "truncated BAM record");
+    }
+    const uint8_t* rec = r->buf.data() + r->pos + 4;
+    InRec x{};
+    if (!parse_rec(rec, bs, x)) {
+      delete b;
+      return berr(ESG_ERR_BAD_ARGUMENT, "malformed BAM record");
+    }
+    r->pos += 4 + bs;
+    if (x.flag & (0x100 | 0x800)) {  // secondary, supplementary
+      ++r->skipped;
+      continue;
+    }
+    if (!(x.flag & 0x4) && (x.flag & 0x10)) {
+      delete b;
+      return berr(ESG_ERR_BAD_ARGUMENT,
+                  "input record aligned to the reverse strand: unaligned reads (or forward-"
+                  "strand alignments, whose SEQ is the read as sequenced) are taken");
+    }
+    rec_off.push_back(b->bytes.size());
+    b->bytes.insert(b->bytes.end(), rec, rec + bs);
+    b->recs.push_back(x);
+  }
+  // the records now live in b->bytes; the reads' codes for the mapping stage
+  uint64_t total = 0;
+  for (size_t k = 0; k < b->recs.size(); ++k) {
+    InRec& x = b->recs[k];
+    x.rec = b->bytes.data() + rec_off[k];
+    const bool over = max_read_len && x.l_seq > max_read_len;
+    b->full_len.push_back(x.l_seq);
+    b->len.push_back(over ? 0u : x.l_seq);
+    b->off.push_back(total);
+    total += b->len.back();
+  }
+  b->codes.resize(total);
+  for (size_t k = 0; k < b->recs.size(); ++k) {
+    const InRec& x = b->recs[k];
+    const uint8_t* s = x.rec + x.seq_off;
+    uint8_t* d = b->codes.data() + b->off[k];
+    for (uint32_t i = 0; i < b->len[k]; ++i) d[i] = kCode4[(s[i / 2] >> ((i & 1) ? 0 : 4)) & 0xf];
+  }
+  *out = b;
+  return ESG_OK;
+}
+
+esg_status esg_bam_batch_reads(const esg_bam_batch* b, const uint8_t** codes,
+                               const uint64_t** off, const uint32_t** len, uint32_t* n_reads) {
+  if (!b || !codes || !off || !len || !n_reads) return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  *codes = b->codes.data();
+  *off = b->off.data();
+  *len = b->len.data();
+  *n_reads = (uint32_t)b->recs.size();
+  return ESG_OK;
+}
+
+void esg_bam_batch_free(esg_bam_batch* b) { delete b; }
+
+void esg_bam_close(esg_bam_reader* r) {
+  if (!r) return;
+  if (r->f) fclose(r->f);
+  delete r;
+}
+
+// ===================================================================== records
+esg_status esg_bam_encode(const esg_bam_batch* b, const esg_mapping* m,
+                          const esg_bam_options* opt, const char* const* ref_names,
+                          uint32_t n_refs, uint32_t threads, esg_bam_records** out) {
+  if (!b || !m || !opt || !out || (n_refs && !ref_names))
+    return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  uint32_t n_maps = 0;
+  uint64_t n_hits = 0, n_ops = 0, n_md = 0;
+  const esg_read_mapping* maps = esg_mapping_reads(m, &n_maps);
+  const esg_hit* hits = esg_mapping_hits(m, &n_hits);
+  const uint32_t* ops = esg_mapping_ops(m, &n_ops);
+  const char* md = esg_mapping_md(m, &n_md);
+  if (n_maps != b->recs.size())
+    return berr(ESG_ERR_BAD_ARGUMENT, "the mapping is not of this batch's reads");
+  const size_t n = b->recs.size();
+  for (size_t k = 0; k < n; ++k)
+    for (uint32_t h = 0; h < maps[k].n_hits; ++h)
+      if (hits[maps[k].first_hit + h].reference >= n_refs)
+        return berr(ESG_ERR_BAD_ARGUMENT, "a hit's reference is past ref_names");
+  std::vector<std::vector<uint8_t>> enc(n);
+  std::vector<uint32_t> count(n, 0), unmapped(n, 0);
+  std::atomic<int> bad{0};
+  parallel_for((n + 63) / 64, threads_or(threads), [&](size_t chunk) {
+    std::vector<std::pair<uint32_t, uint32_t>> fields;
+    std::vector<uint32_t> cigar;
+    std::vector<uint8_t> aux, seq4;
+    for (size_t k = chunk * 64; k < std::min(n, chunk * 64 + 64); ++k) {
+      const InRec& x = b->recs[k];
+      const esg_read_mapping& rm = maps[k];
+      std::vector<uint8_t>& o = enc[k];
+      const uint8_t* a = x.rec + x.aux_off;
+      if (!split_aux(a, x.size - x.aux_off, fields)) {
+        bad = 1;
+        return;
+      }
+      // the owned tags removed, each by moving the last field into its slot
+      static const char kOwned[5][2] = {{'N', 'M'}, {'M', 'D'}, {'A', 'S'}, {'X', 'S'}, {'X', 'A'}};
+      for (const auto& t : kOwned) {
+        for (size_t i = 0; i < fields.size(); ++i) {
+          if (a[fields[i].first] == (uint8_t)t[0] && a[fields[i].first + 1] == (uint8_t)t[1]) {
+            fields[i] = fields.back();
+            fields.pop_back();
+            break;
+          }
+        }
+      }
+      aux.clear();
+      for (const auto& fld : fields) aux.insert(aux.end(), a + fld.first, a + fld.first + fld.second);
+      const uint16_t kept = x.flag & (0x200 | 0x400);
+      const uint8_t* name = x.rec + 32;
+      const uint8_t* s = x.rec + x.seq_off;
+      const uint8_t* q = s + (x.l_seq + 1) / 2;
+      const bool have_qual = x.l_seq == 0 || q[0] != 0xff;
+      seq4.resize(x.l_seq);
+      for (uint32_t i = 0; i < x.l_seq; ++i) seq4[i] = (s[i / 2] >> ((i & 1) ? 0 : 4)) & 0xf;
+      cigar.clear();
+      // a read over max_read_len was not scored: unmapped (process_chunk,
+      // align.rs:1504-1602)
+      if (!rm.n_hits || b->len[k] != b->full_len[k]) {
+        encode_record(o, -1, -1, 0, cigar, kept | 0x4, name, x.name_len, seq4.data(), x.l_seq, q,
+                      have_qual, aux);
+        count[k] = 1;
+        unmapped[k] = 1;
+        continue;
+      }
+      const esg_hit& p = hits[rm.first_hit];
+      uint16_t flag = kept;
+      std::vector<uint8_t> qual(q, q + x.l_seq);
+      if (p.reverse) {
+        flag |= 0x10;
+        std::reverse(seq4.begin(), seq4.end());
+        for (auto& c : seq4) c = kComp4[c];
+        std::reverse(qual.begin(), qual.end());
+      }
+      int_field(aux, "NM", p.nm);
+      str_field(aux, "MD", md + p.md_offset, p.md_len);
+      int_field(aux, "AS", rm.best_score);
+      if (rm.flags & ESG_MAPPING_HAS_SUBOPTIMAL) int_field(aux, "XS", rm.suboptimal);
+      if (rm.n_hits > 1) {
+        std::string xa;
+        for (uint32_t h = 1; h < rm.n_hits; ++h) {
+          const esg_hit& e = hits[rm.first_hit + h];
+          xa += ref_names[e.reference];
+          xa += e.reverse ? ",-" : ",+";
+          xa += std::to_string(e.alignment.ref_start + 1);
+          xa += ',';
+          sam_cigar(e, ops, x.l_seq, cigar);
+          for (uint32_t w : cigar) {
+            xa += std::to_string(w >> 4);
+            xa += "MIDNSHP=X"[w & 0xfu];
+          }
+          xa += ',';
+          xa += std::to_string(e.nm);
+          xa += ';';
+        }
+        str_field(aux, "XA", xa.data(), xa.size());
+      }
+      sam_cigar(p, ops, x.l_seq, cigar);
+      encode_record(o, (int32_t)p.reference, (int32_t)p.alignment.ref_start,
+                    rm.n_tied == 1 ? 60 : 0, cigar, flag, name, x.name_len, seq4.data(), x.l_seq,
+                    qual.data(), have_qual, aux);
+      count[k] = 1;
+      if (opt->secondary) {
+        // the read group of the input record, if any
+        std::vector<uint8_t> rg;
+        {
+          std::vector<std::pair<uint32_t, uint32_t>> all;
+          split_aux(a, x.size - x.aux_off, all);
+          for (const auto& fld : all)
+            if (a[fld.first] == 'R' && a[fld.first + 1] == 'G')
+              rg.assign(a + fld.first, a + fld.first + fld.second);
+        }
+        for (uint32_t h = 1; h < rm.n_hits; ++h) {
+          const esg_hit& e = hits[rm.first_hit + h];
+          std::vector<uint8_t> d;
+          int_field(d, "NM", e.nm);
+          str_field(d, "MD", md + e.md_offset, e.md_len);
+          int_field(d, "AS", rm.best_score);
+          d.insert(d.end(), rg.begin(), rg.end());
+          sam_cigar(e, ops, x.l_seq, cigar);
+          encode_record(o, (int32_t)e.reference, (int32_t)e.alignment.ref_start, 0, cigar,
+                        (uint16_t)(0x100 | kept | (e.reverse ? 0x10 : 0)), name, x.name_len,
+                        nullptr, 0, nullptr, true, d);
+          ++count[k];
+        }
+      }
+    }
+  });
+  if (bad) return berr(ESG_ERR_BAD_ARGUMENT, "malformed auxiliary data in an input record");
+  auto* r = new esg_bam_records();
+  size_t total = 0;
+  for (auto& e : enc) total += e.size();
+  r->bytes.reserve(total);
+  for (size_t k = 0; k < n; ++k) {
+    r->bytes.insert(r->bytes.end(), enc[k].begin(), enc[k].end());
+    r->n_records += count[k];
+    r->n_unmapped += unmapped[k];
+  }
+  *out = r;
+  return ESG_OK;
+}
+
+const uint8_t* esg_bam_records_bytes(const esg_bam_records* r, uint64_t* n_bytes,
+                                     uint32_t* n_records) {
+  if (!r) return nullptr;
+  if (n_bytes) *n_bytes = r->bytes.size();
+  if (n_records) *n_records = r->n_records;
+  return r->bytes.data();
+}
+
+void esg_bam_records_free(esg_bam_records* r) { delete r; }
+
+}  // extern "C"
+
+// ===================================================================== writer
+struct esg_bam_writer {
+  FILE* f = nullptr;
+  uint32_t threads = 1;
+  int level = 6;
+  bool sort = false;
+  std::vector<uint8_t> pending;  // uncompressed bytes not yet in a block
+  std::map<uint64_t, std::vector<uint8_t>> waiting;  // chunks ahead of `next`
+  uint64_t next = 0;
+  std::vector<std::vector<uint8_t>> buckets;  // coordinate sort: per reference, + unmapped
+  bool failed = false;
+};
+
+// Compress every whole block of w->pending (all of it with `flush`) and
+// write them in order.
+static esg_status drain(esg_bam_writer* w, bool flush) {
+  const size_t whole = flush ? w->pending.size() : w->pending.size() / kBgzfMaxIn * kBgzfMaxIn;
+  if (!whole) return ESG_OK;
+  const size_t nb = (whole + kBgzfMaxIn - 1) / kBgzfMaxIn;
+  std::vector<std::vector<uint8_t>> blocks(nb);
+  parallel_for(nb, w->threads, [&](size_t i) {
+    const size_t s = i * kBgzfMaxIn;
+    deflate_block(w->pending.data() + s, std::min(kBgzfMaxIn, whole - s), w->level, blocks[i]);
+  });
+  for (auto& bl : blocks)
+    if (fwrite(bl.data(), 1, bl.size(), w->f) != bl.size()) {
+      w->failed = true;
+      return berr(ESG_ERR_DRIVER, "writing the BAM file failed");
+    }
+  w->pending.erase(w->pending.begin(), w->pending.begin() + (long)whole);
+  return ESG_OK;
+}
+
+static void put_records(esg_bam_writer* w, const uint8_t* p, size_t n) {
+  if (!w->sort) {
+    w->pending.insert(w->pending.end(), p, p + n);
+    return;
+  }
+  for (size_t at = 0; at + 4 <= n;) {
+    const uint32_t bs = u32_at(p + at);
+    const int32_t tid = i32_at(p + at + 4);
+    const size_t b = (tid >= 0 && (size_t)tid < w->buckets.size() - 1) ? (size_t)tid
+                                                                          : w->buckets.size() - 1;
+    w->buckets[b].insert(w->buckets[b].end(), p + at, p + at + 4 + bs);
+    at += 4 + bs;
+  }
+}
+
+extern "C" {
+
+esg_status esg_bam_writer_open(const char* path, const char* header_text,
+                               const char* const* ref_names, const uint32_t* ref_lens,
+                               uint32_t n_refs, int32_t sort_coordinate, uint32_t threads,
+                               esg_bam_writer** out) {
+  if (!path || !out || (n_refs && (!ref_names || !ref_lens)))
+    return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  auto* w = new esg_bam_writer();
+  w->threads = threads_or(threads);
+  w->sort = sort_coordinate != 0;
+  w->buckets.resize((size_t)n_refs + 1);
+  w->f = fopen(path, "wb");
+  if (!w->f) {
+    delete w;
+    return berr(ESG_ERR_BAD_ARGUMENT, std::string("cannot create ") + path);
+  }
+  const size_t lt = header_text ? strlen(header_text) : 0;
+  std::vector<uint8_t>& h = w->pending;
+  h.insert(h.end(), {'B', 'A', 'M', 1});
+  put32(h, (uint32_t)lt);
+  h.insert(h.end(), header_text, header_text + lt);
+  put32(h, n_refs);
+  for (uint32_t k = 0; k < n_refs; ++k) {
+    const size_t ln = strlen(ref_names[k]) + 1;
+    put32(h, (uint32_t)ln);
+    h.insert(h.end(), ref_names[k], ref_names[k] + ln);
+    put32(h, ref_lens[k]);
+  }
+  *out = w;
+  return ESG_OK;
+}
+
+esg_status esg_bam_writer_push(esg_bam_writer* w, uint64_t seq, const esg_bam_records* r) {
+  if (!w || !r) return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  if (w->failed) return berr(ESG_ERR_DRIVER, "the writer failed earlier");
+  if (seq < w->next || w->waiting.count(seq))
+    return berr(ESG_ERR_BAD_ARGUMENT, "chunk sequence number already written");
+  w->waiting[seq] = r->bytes;
+  for (auto it = w->waiting.find(w->next); it != w->waiting.end(); it = w->waiting.find(w->next)) {
+    put_records(w, it->second.data(), it->second.size());
+    w->waiting.erase(it);
+    ++w->next;
+  }
+  return drain(w, false);
+}
+
+esg_status esg_bam_writer_close(esg_bam_writer* w) {
+  if (!w) return berr(ESG_ERR_BAD_ARGUMENT, "NULL writer");
+  esg_status st = ESG_OK;
+  if (!w->waiting.empty()) st = berr(ESG_ERR_BAD_ARGUMENT, "chunks missing before the last pushed");
+  if (st == ESG_OK && w->sort) {
+    // per reference, stable on (position, reverse): records are pushed in
+    // input order, so ties keep it
+    for (size_t bkt = 0; bkt < w->buckets.size() && st == ESG_OK; ++bkt) {
+      std::vector<uint8_t>& v = w->buckets[bkt];
+      std::vector<std::pair<uint64_t, size_t>> keyed;
+      for (size_t at = 0; at + 4 <= v.size(); at += 4 + u32_at(v.data() + at)) {
+        const bool unmapped = bkt == w->buckets.size() - 1;
+        const uint64_t pos = unmapped ? 0 : (uint64_t)(uint32_t)i32_at(v.data() + at + 8);
+        const uint64_t rev = (u16_at(v.data() + at + 18) & 0x10) ? 1 : 0;
+        keyed.push_back({pos << 1 | rev, at});
+      }
+      std::stable_sort(keyed.begin(), keyed.end(),
+                       [](const std::pair<uint64_t, size_t>& a,
+                          const std::pair<uint64_t, size_t>& b) { return a.first < b.first; });
+      for (const auto& kv : keyed) {
+        const uint32_t bs = u32_at(v.data() + kv.second);
+        w->pending.insert(w->pending.end(), v.data() + kv.second, v.data() + kv.second + 4 + bs);
+      }
+      std::vector<uint8_t>().swap(v);
+      st = drain(w, false);
+    }
+  }
+  if (st == ESG_OK) st = drain(w, true);
+  if (st == ESG_OK && fwrite(kBgzfEof, 1, sizeof kBgzfEof, w->f) != sizeof kBgzfEof)
+    st = berr(ESG_ERR_DRIVER, "writing the BAM file failed");
+  if (fclose(w->f) != 0 && st == ESG_OK) st = berr(ESG_ERR_DRIVER, "closing the BAM file failed");
+  delete w;
+  return st;
+}
+
+}  // extern "C"

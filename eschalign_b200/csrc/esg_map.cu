@@ -763,6 +763,31 @@ const esg_pair_hit* esg_mapping_pair_hits(const esg_mapping* m, uint64_t* n) {
   return m ? m->pair_hits.data() : nullptr;
 }
 
+esg_status esg_mapping_from_arrays(const esg_read_mapping* reads, uint32_t n_reads,
+                                   const esg_hit* hits, uint64_t n_hits, const uint32_t* ops,
+                                   uint64_t n_ops, const char* md, uint64_t n_md,
+                                   esg_mapping** out) {
+  if (!out || (n_reads && !reads) || (n_hits && !hits) || (n_ops && !ops) || (n_md && !md))
+    return merr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  for (uint32_t k = 0; k < n_reads; ++k)
+    if (reads[k].first_hit > n_hits || reads[k].n_hits > n_hits - reads[k].first_hit)
+      return merr(ESG_ERR_BAD_ARGUMENT, "read %u's hits run past the hit array", k);
+  for (uint64_t h = 0; h < n_hits; ++h)
+    if (hits[h].alignment.ops_offset > n_ops ||
+        hits[h].alignment.n_ops > n_ops - hits[h].alignment.ops_offset ||
+        hits[h].md_offset > n_md || hits[h].md_len > n_md - hits[h].md_offset)
+      return merr(ESG_ERR_BAD_ARGUMENT, "hit %llu's ops or MD run past their arrays",
+                  (unsigned long long)h);
+  auto* m = new esg_mapping();
+  m->reads.assign(reads, reads + n_reads);
+  m->hits.assign(hits, hits + n_hits);
+  m->ops.assign(ops, ops + n_ops);
+  m->md.assign(md, md + n_md);
+  *out = m;
+  return ESG_OK;
+}
+
 const esg_read_mapping* esg_mapping_reads(const esg_mapping* m, uint32_t* n) {
   if (n) *n = m ? (uint32_t)m->reads.size() : 0u;
   return m ? m->reads.data() : nullptr;

@@ -507,6 +507,13 @@ const esg_hit* esg_mapping_hits(const esg_mapping* mapping, uint64_t* n);
 const uint32_t* esg_mapping_ops(const esg_mapping* mapping, uint64_t* n);
 const char* esg_mapping_md(const esg_mapping* mapping, uint64_t* n);
 void esg_mapping_free(esg_mapping* mapping);
+/* A mapping made from the caller's arrays (copied; the same layout the
+ * accessors above return), for reads mapped elsewhere that go to
+ * esg_bam_encode.  No counterpart in the reference. */
+esg_status esg_mapping_from_arrays(const esg_read_mapping* reads, uint32_t n_reads,
+                                   const esg_hit* hits, uint64_t n_hits, const uint32_t* ops,
+                                   uint64_t n_ops, const char* md, uint64_t n_md,
+                                   esg_mapping** out);
 
 /* ---- serving: a request queue over resident scorers.  No counterpart in
  * the reference, which scores batches of one stream of reads and has no
@@ -573,6 +580,68 @@ esg_status esg_server_stats_get(esg_server* server, esg_server_stats* out);
  * Call it once no other thread is inside esg_server_submit / _wait;
  * requests nobody waited for are dropped. */
 void esg_server_free(esg_server* server);
+
+/* ---- BAM input and output around the mapping stage (host code, zlib).
+ *
+ * The CLI's I/O stage for unpaired reads (crates/eschalign-cli/src/align.rs):
+ * read_batches (604-660), the records of a read's mapping (build_records,
+ * 1084-1200; process_chunk's --max-read-len rule, 1504-1602), and the
+ * ordered or coordinate-sorted writer (write_in_order, 2345-2400; the sort,
+ * 2406-2450).  A batch's reads go to esg_map_reads as they come
+ * (esg_bam_batch_reads); its mapping comes back to esg_bam_encode, whose
+ * records are byte for byte the reference CLI's: input tags kept, NM / MD /
+ * AS / XS / XA replaced, MAPQ 60 for a unique best and 0 otherwise, the
+ * primary hit's CIGAR with soft clips, XA for the other taken ties, and with
+ * `secondary` one record per further tie. */
+typedef struct esg_bam_reader esg_bam_reader;
+typedef struct esg_bam_batch esg_bam_batch;
+typedef struct esg_bam_records esg_bam_records;
+typedef struct esg_bam_writer esg_bam_writer;
+typedef struct esg_bam_options {
+    uint32_t secondary; /* --secondary: one SECONDARY record per further taken tie */
+    uint32_t reserved;  /* 0 */
+} esg_bam_options;
+
+/* Open a BGZF-compressed BAM and read its header (threads: inflating
+ * threads, 0 = the host's cores). */
+esg_status esg_bam_open(const char* path, uint32_t threads, esg_bam_reader** out);
+const char* esg_bam_header_text(const esg_bam_reader* reader, uint64_t* len);
+/* The next primary records, at most max_reads (secondary and supplementary
+ * ones skipped; a record aligned to the reverse strand is refused with
+ * ESG_ERR_BAD_ARGUMENT).  A batch of 0 reads means the end of the file.
+ * Reads over max_read_len (0 = no limit) get length 0 in
+ * esg_bam_batch_reads, so the mapping stage leaves them unmapped. */
+esg_status esg_bam_read_batch(esg_bam_reader* reader, uint32_t max_reads, uint32_t max_read_len,
+                              esg_bam_batch** out);
+/* The batch's reads as alphabet codes (0..3 = A,C,G,T; 4 = any other base),
+ * for esg_map_reads; owned by the batch. */
+esg_status esg_bam_batch_reads(const esg_bam_batch* batch, const uint8_t** codes,
+                               const uint64_t** off, const uint32_t** len, uint32_t* n_reads);
+void esg_bam_batch_free(esg_bam_batch* batch);
+void esg_bam_close(esg_bam_reader* reader);
+/* The output records of a batch from its mapping (esg_map_reads over
+ * esg_bam_batch_reads, with the panel's letters for MD), encoded in the BAM
+ * layout, in read order; ref_names in panel order. */
+esg_status esg_bam_encode(const esg_bam_batch* batch, const esg_mapping* mapping,
+                          const esg_bam_options* options, const char* const* ref_names,
+                          uint32_t n_refs, uint32_t threads, esg_bam_records** out);
+const uint8_t* esg_bam_records_bytes(const esg_bam_records* records, uint64_t* n_bytes,
+                                     uint32_t* n_records);
+void esg_bam_records_free(esg_bam_records* records);
+/* A BGZF BAM writer: header, then the records of the chunks pushed, in the
+ * order of their sequence numbers 0, 1, ... whatever order they arrive in;
+ * with sort_coordinate, in coordinate order at close (reference, position,
+ * reverse after forward, then input order; unmapped last).  Blocks are
+ * deflated on `threads` host threads (0 = the host's cores). */
+esg_status esg_bam_writer_open(const char* path, const char* header_text,
+                               const char* const* ref_names, const uint32_t* ref_lens,
+                               uint32_t n_refs, int32_t sort_coordinate, uint32_t threads,
+                               esg_bam_writer** out);
+esg_status esg_bam_writer_push(esg_bam_writer* writer, uint64_t seq,
+                               const esg_bam_records* records);
+/* Writes what is left (the sorted records), the end-of-file block, and
+ * frees the writer. */
+esg_status esg_bam_writer_close(esg_bam_writer* writer);
 
 /* Scoring for callers that cannot allocate.  No counterpart in the reference.
  *

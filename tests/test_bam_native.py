@@ -1,0 +1,193 @@
+"""The library's BAM stage (esg_bam_*) against the reference CLI's golden
+record streams, on the CPU.
+
+The reader parses the reference's 60-record fixture; the encoder builds each
+read's records from its mapping (here the oracle's mappings, handed over with
+esg_mapping_from_arrays, so no GPU is needed) and must give the record count
+and FNV-1a 64 digest the reference CLI gave for each of its six flag sets
+(crates/eschalign-cli/tests/align_unpaired.rs:37-62).  The writer's BGZF file
+must decompress to the same stream, in input or coordinate order."""
+import gzip
+import os
+import struct
+
+import numpy as np
+import pytest
+
+from eschalign_b200 import bam as EB
+from eschalign_b200.scorer import (HIT_DTYPE, MAPPING_DTYPE, MAPPING_HAS_BEST,
+                                   MAPPING_HAS_SUBOPTIMAL, Mappings)
+from tests.helpers import GOLDEN
+from tests.test_bam_golden import flag_set, golden_digests, input_records, trna_panel
+
+FIXTURE = os.path.join(GOLDEN, "unpaired_input.bam")
+_OPS = "MIDNSHP=X"
+
+
+def mappings_from_oracle(ms) -> Mappings:
+    """The oracle's map_reads dicts as esg_map_reads' arrays."""
+    reads = np.zeros(len(ms), MAPPING_DTYPE)
+    hits, ops, md = [], [], bytearray()
+    for k, m in enumerate(ms):
+        r = reads[k]
+        r["first_hit"] = len(hits)
+        r["n_hits"] = len(m["hits"])
+        r["n_tied"] = m["n_tied"]
+        if m["best_score"] is not None:
+            r["best_score"] = m["best_score"]
+            r["flags"] |= MAPPING_HAS_BEST
+        if m["suboptimal"] is not None:
+            r["suboptimal"] = m["suboptimal"]
+            r["flags"] |= MAPPING_HAS_SUBOPTIMAL
+        for h in m["hits"]:
+            e = np.zeros((), HIT_DTYPE)
+            for f in ("reference", "reverse", "score", "query_start", "query_end", "ref_start",
+                      "ref_end", "nm"):
+                e[f] = int(h[f])
+            words, n = [], ""
+            for ch in h["cigar"]:
+                if ch.isdigit():
+                    n += ch
+                else:
+                    words.append(int(n) << 4 | _OPS.index(ch))
+                    n = ""
+            e["ops_offset"], e["n_ops"] = len(ops), len(words)
+            ops += words
+            e["md_offset"], e["md_len"] = len(md), len(h["md"])
+            md += h["md"].encode()
+            hits.append(e)
+    return Mappings(reads, np.array(hits, HIT_DTYPE), np.array(ops, np.uint32), bytes(md))
+
+
+def oracle_mappings(oracle, recs, o):
+    names, refs = trna_panel()
+    keep = [k for k, r in enumerate(recs)
+            if not (o["max_read_len"] and len(r["seq"]) > o["max_read_len"])]
+    ms = oracle.map_reads([recs[k]["seq"] for k in keep], refs, o["scoring"], o["local"],
+                          min_score=o["min_score"], max_ties=o["max_ties"],
+                          both_strands=o["both"])
+    out = [{"best_score": None, "n_tied": 0, "suboptimal": None, "hits": []} for _ in recs]
+    for k, m in zip(keep, ms):
+        out[k] = m
+    return out
+
+
+def record_stream(path):
+    """The uncompressed records of a BAM file, header skipped."""
+    raw = gzip.decompress(open(path, "rb").read())
+    lt = struct.unpack("<I", raw[4:8])[0]
+    o = 8 + lt
+    n_ref = struct.unpack("<I", raw[o:o + 4])[0]
+    o += 4
+    for _ in range(n_ref):
+        o += 8 + struct.unpack("<I", raw[o:o + 4])[0]
+    return raw[o:]
+
+
+def test_reader_gives_the_primary_records_as_codes():
+    from eschalign_b200 import encode
+    recs = input_records()
+    with EB.BamReader(FIXTURE, threads=2) as rd:
+        assert rd.header_text.startswith(b"@")
+        batches = list(rd.batches(max_reads=17, max_read_len=1000))
+    assert [len(b) for b in batches] == [17, 17, 17, len(recs) - 51]
+    got = []
+    for b in batches:
+        codes, off, lens = b.reads()
+        got += [codes[int(off[k]):int(off[k]) + int(lens[k])].tolist() for k in range(len(b))]
+    assert got == [encode(r["seq"]).tolist() for r in recs]
+
+
+def test_reader_leaves_long_reads_unscored():
+    recs = input_records()
+    with EB.BamReader(FIXTURE) as rd:
+        (b,) = list(rd.batches(max_reads=1000, max_read_len=40))
+    assert b.lens.tolist() == [0 if len(r["seq"]) > 40 else len(r["seq"]) for r in recs]
+
+
+@pytest.mark.parametrize("label", sorted(golden_digests()))
+def test_encoder_reproduces_the_reference_record_stream(oracle, label):
+    from oracle import bam as B
+    want = golden_digests()[label]
+    o = flag_set(label)
+    names, _ = trna_panel()
+    recs = input_records()
+    maps = mappings_from_oracle(oracle_mappings(oracle, recs, o))
+    with EB.BamReader(FIXTURE) as rd:
+        (b,) = list(rd.batches(max_reads=1000, max_read_len=o["max_read_len"]))
+    rec = EB.encode(b, maps, names, secondary=o["secondary"], threads=3)
+    stream = rec.bytes()
+    if o["sort"]:
+        parts, at = [], 0
+        while at < len(stream):
+            n = 4 + struct.unpack("<I", stream[at:at + 4])[0]
+            parts.append(stream[at:at + n])
+            at += n
+        stream = b"".join(B.coordinate_order(parts))
+    assert rec.n_records == want["records"]
+    assert format(B.fnv1a64(stream), "016x") == want["fnv1a64"]
+
+
+@pytest.mark.parametrize("label", ["default", "sort_coordinate", "semiglobal_both_secondary"])
+def test_writer_file_holds_the_reference_record_stream(oracle, tmp_path, label):
+    """Chunks pushed out of order; the file is BGZF with the end marker and
+    decompresses to the golden stream (coordinate-sorted by the writer)."""
+    from oracle import bam as B
+    want = golden_digests()[label]
+    o = flag_set(label)
+    names, refs = trna_panel()
+    recs = input_records()
+    ms = oracle_mappings(oracle, recs, o)
+    path = str(tmp_path / "out.bam")
+    hdr = EB.header_text(names, [len(r) for r in refs], o["sort"])
+    chunks = []
+    with EB.BamReader(FIXTURE) as rd:
+        for seq, b in enumerate(rd.batches(max_reads=7, max_read_len=o["max_read_len"])):
+            lo = seq * 7
+            chunks.append(EB.encode(b, mappings_from_oracle(ms[lo:lo + len(b)]), names,
+                                    secondary=o["secondary"]))
+    with EB.BamWriter(path, hdr, names, [len(r) for r in refs], o["sort"], threads=2) as wr:
+        for seq in [2, 0, 1] + list(range(3, len(chunks))):
+            wr.push(seq, chunks[seq])
+    data = open(path, "rb").read()
+    assert data[-28:] == bytes.fromhex("1f8b08040000000000ff0600424302001b0003000000000000000000")
+    text, refs_out, out_recs = B.read_bam(data)
+    assert text == hdr and [n.decode() for n, _ in refs_out] == names
+    assert len(out_recs) == want["records"]
+    assert format(B.fnv1a64(record_stream(path)), "016x") == want["fnv1a64"]
+
+
+def test_writer_refuses_a_repeated_chunk(tmp_path):
+    names, refs = trna_panel()
+    with EB.BamReader(FIXTURE) as rd:
+        (b,) = list(rd.batches(max_reads=1000))
+    empty = {"best_score": None, "n_tied": 0, "suboptimal": None, "hits": []}
+    rec = EB.encode(b, mappings_from_oracle([empty] * len(b)), names)
+    wr = EB.BamWriter(str(tmp_path / "x.bam"), b"", names, [len(r) for r in refs])
+    wr.push(0, rec)
+    with pytest.raises(RuntimeError):
+        wr.push(0, rec)
+    wr.close()
+    assert len(record_stream(str(tmp_path / "x.bam"))) == rec.nbytes
+
+
+def test_encoder_refuses_a_mapping_of_other_reads():
+    names, _ = trna_panel()
+    with EB.BamReader(FIXTURE) as rd:
+        (b,) = list(rd.batches(max_reads=1000))
+    empty = {"best_score": None, "n_tied": 0, "suboptimal": None, "hits": []}
+    with pytest.raises(RuntimeError):
+        EB.encode(b, mappings_from_oracle([empty] * (len(b) - 1)), names)
+
+
+def test_mapping_from_arrays_checks_its_offsets():
+    m = mappings_from_oracle([{"best_score": 5, "n_tied": 1, "suboptimal": None, "hits": [
+        {"reference": 0, "reverse": False, "score": 5, "query_start": 0, "query_end": 3,
+         "ref_start": 0, "ref_end": 3, "cigar": "3M", "md": "3", "nm": 0}]}])
+    m.hits["md_len"] = 2 ** 32 - 1
+    with pytest.raises(RuntimeError):
+        EB.mapping_handle(m)
+    m.hits["md_len"] = 1
+    m.reads["first_hit"] = 2 ** 64 - 1
+    with pytest.raises(RuntimeError):
+        EB.mapping_handle(m)

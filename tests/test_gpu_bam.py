@@ -1,0 +1,32 @@
+"""The CLI's unpaired run end to end on the CUDA path: the reference's fixture
+BAM read by esg_bam_read_batch, mapped by esg_map_reads on the device, its
+records built by esg_bam_encode and written by esg_bam_writer must hold the
+record stream the reference CLI wrote -- record count and FNV-1a 64 digest
+(crates/eschalign-cli/tests/align_unpaired.rs:37-62) -- for each of its six
+flag sets."""
+import pytest
+
+from eschalign_b200 import GpuScorer, Mode, Scoring, encode
+from eschalign_b200 import bam as EB
+from tests.test_bam_golden import flag_set, golden_digests, trna_panel
+from tests.test_bam_native import FIXTURE, record_stream
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("batch_size", [1000, 13])
+@pytest.mark.parametrize("label", sorted(golden_digests()))
+def test_align_bam_writes_the_reference_record_stream(tmp_path, label, batch_size):
+    from oracle import bam as B
+    want = golden_digests()[label]
+    o = flag_set(label)
+    names, refs = trna_panel()
+    mode = Mode.LOCAL if o["local"] else Mode.SEMIGLOBAL
+    path = str(tmp_path / "out.bam")
+    with GpuScorer([encode(r) for r in refs], Scoring(*o["scoring"]), mode) as g:
+        n = EB.align_bam(g, FIXTURE, path, names, refs, min_score=o["min_score"],
+                         max_ties=o["max_ties"], both_strands=o["both"],
+                         secondary=o["secondary"], sort_coordinate=o["sort"],
+                         max_read_len=o["max_read_len"], batch_size=batch_size, threads=4)
+    assert n["records"] == want["records"]
+    assert format(B.fnv1a64(record_stream(path)), "016x") == want["fnv1a64"]
