@@ -346,6 +346,99 @@ def map_stage(g, refs, reads, scoring, local, skip_cpu):
     return out
 
 
+def unmapped_bam(path, reads, seed=11):
+    """`reads` as an unaligned BAM, the CLI's usual input: flag 4, names
+    r0000000.., Phred qualities 2-40, an RG:Z tag; BGZF at level 1.  Built
+    with array operations (a loop over a million records takes seconds)."""
+    import zlib
+    from concurrent.futures import ThreadPoolExecutor
+    rng = np.random.default_rng(seed)
+    n = len(reads)
+    lens = reads.lens.astype(np.int64)
+    plen = (lens + 1) // 2
+    aux = np.frombuffer(b"RGZgrp1\0", np.uint8)
+    size = 32 + 9 + plen + lens + aux.size            # block_size
+    start = np.zeros(n + 1, np.int64)
+    np.cumsum(size + 4, out=start[1:])
+    buf = np.zeros(int(start[-1]), np.uint8)
+    hdr = np.zeros(n, np.dtype([("bs", "<u4"), ("ref", "<i4"), ("pos", "<i4"), ("lrn", "u1"),
+                                ("mapq", "u1"), ("bin", "<u2"), ("ncig", "<u2"), ("flag", "<u2"),
+                                ("lseq", "<u4"), ("nref", "<i4"), ("npos", "<i4"),
+                                ("tlen", "<i4")]))
+    hdr["bs"], hdr["ref"], hdr["pos"], hdr["lrn"] = size, -1, -1, 9
+    hdr["bin"], hdr["flag"], hdr["lseq"], hdr["nref"], hdr["npos"] = 4680, 4, lens, -1, -1
+    buf[(start[:-1, None] + np.arange(36)).ravel()] = hdr.view(np.uint8)
+    k = np.arange(n)
+    name = np.zeros((n, 9), np.uint8)
+    name[:, 0] = ord("r")
+    for d in range(7):
+        name[:, 7 - d] = ord("0") + (k // 10 ** d) % 10
+    buf[(start[:-1, None] + 36 + np.arange(9)).ravel()] = name.ravel()
+    # 4-bit sequence: each read padded to an even length, then paired
+    code4 = np.array([1, 2, 4, 8, 15], np.uint8)[np.minimum(reads.codes[:int(lens.sum())], 4)]
+    poff = np.zeros(n + 1, np.int64)
+    np.cumsum(2 * plen, out=poff[1:])
+    pad = np.zeros(int(poff[-1]), np.uint8)
+    roff = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=roff[1:])
+    pad[np.repeat(poff[:-1] - roff[:-1], lens) + np.arange(int(roff[-1]))] = code4
+    packed = pad[0::2] << 4 | pad[1::2]
+    pk = np.zeros(n + 1, np.int64)
+    np.cumsum(plen, out=pk[1:])
+    seq_at = start[:-1] + 45
+    buf[np.repeat(seq_at - pk[:-1], plen) + np.arange(int(pk[-1]))] = packed
+    qual_at = seq_at + plen
+    buf[np.repeat(qual_at - roff[:-1], lens) + np.arange(int(roff[-1]))] = \
+        rng.integers(2, 41, int(roff[-1]), dtype=np.uint8)
+    aux_at = qual_at + lens
+    buf[(aux_at[:, None] + np.arange(aux.size)).ravel()] = np.tile(aux, n)
+    text = b"@HD\tVN:1.6\tSO:unsorted\n@RG\tID:grp1\tSM:s\n"
+    head = b"BAM\1" + len(text).to_bytes(4, "little") + text + (0).to_bytes(4, "little")
+    raw = memoryview(np.concatenate([np.frombuffer(head, np.uint8), buf]))
+
+    def block(i):
+        src = raw[i:i + 0xff00]
+        c = zlib.compressobj(1, zlib.DEFLATED, -15)
+        body = c.compress(src) + c.flush()
+        return (b"\x1f\x8b\x08\x04\0\0\0\0\0\xff\x06\0BC\x02\0" +
+                (len(body) + 25).to_bytes(2, "little") + body +
+                zlib.crc32(src).to_bytes(4, "little") + len(src).to_bytes(4, "little"))
+    with ThreadPoolExecutor(os.cpu_count() or 4) as pool, open(path, "wb") as fh:
+        for b in pool.map(block, range(0, len(raw), 0xff00)):
+            fh.write(b)
+        fh.write(bytes.fromhex("1f8b08040000000000ff0600424302001b0003000000000000000000"))
+    return len(raw)
+
+
+def bam_stage(g, refs, reads, batch_size=50_000):
+    """The CLI's unpaired run through the library (bam.align_bam): an
+    unaligned BAM of the workload's reads read, mapped on the device (every
+    tie traced, MD / NM from the panel's letters), its records built and
+    written as BGZF; wall time, input order, default batch size 50 000."""
+    from eschalign_b200 import bam as EB
+    names = [f"ref{k}" for k in range(len(refs))]
+    letters = [bytes(b"ACGTN"[int(c)] for c in r) for r in refs]
+    with tempfile.TemporaryDirectory() as tmp:
+        src, dst = os.path.join(tmp, "in.bam"), os.path.join(tmp, "out.bam")
+        raw = unmapped_bam(src, reads)
+        in_bytes = os.path.getsize(src)
+        warm = os.path.join(tmp, "warm.bam")
+        unmapped_bam(warm, reads.slice(0, 2000))
+        EB.align_bam(g, warm, dst, names, letters, both_strands=True, batch_size=1000)
+        st = {}
+        t0 = time.perf_counter()
+        n = EB.align_bam(g, src, dst, names, letters, both_strands=True,
+                         batch_size=batch_size, max_read_len=1000, stats=st)
+        dt = time.perf_counter() - t0
+        out_bytes = os.path.getsize(dst)
+    return {"reads": n["reads"], "records": n["records"], "seconds": round(dt, 3),
+            "reads_per_s": n["reads"] / dt, "batch_reads": batch_size,
+            "input_bgzf_bytes": in_bytes, "input_raw_bytes": raw, "output_bgzf_bytes": out_bytes,
+            "stage_seconds": {k: round(v, 3) for k, v in st.items()},
+            "options": "both strands, min_score 0, every tie traced, MD/NM from letters, "
+                       "input order; map on one thread overlapped with read/encode/write"}
+
+
 def map_pairs_stage(g, refs, pairs, scoring, local, skip_cpu, n=100_000):
     """The whole paired mapping stage: adapters trimmed by the library
     (esg_pair_adapters), then esg_map_pairs (pair.rs:157-390: the device
@@ -720,6 +813,7 @@ def run_c2(a, ctx, rank):
                                               a.no_cpu_baseline or rank != 0 or world != 1)
         extras["map"] = map_stage(g, refs, reads, scoring, mode == "local",
                                   a.no_cpu_baseline or rank != 0 or world != 1)
+        extras["bam"] = bam_stage(g, refs, reads)
         arms = reference_gpu_arms(refs, sub, scoring, mode == "local", local_rank)
         if arms:
             arms["batched_over_ref_half2"] = value / arms["half2_gcups"]

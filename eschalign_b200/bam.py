@@ -13,6 +13,9 @@ The records are the reference CLI's byte for byte.
 from __future__ import annotations
 
 import ctypes as C
+import time
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -200,8 +203,14 @@ class BamWriter:
     def __enter__(self):
         return self
 
-    def __exit__(self, *exc):
-        self.close()
+    def __exit__(self, exc_type, *exc):
+        if exc_type is None:
+            self.close()
+            return
+        try:  # the error in flight is the one to report
+            self.close()
+        except Exception:
+            pass
 
 
 def header_text(ref_names, ref_lens, sort_coordinate: bool = False) -> bytes:
@@ -217,24 +226,77 @@ def header_text(ref_names, ref_lens, sort_coordinate: bool = False) -> bytes:
 def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
               min_score: int = 0, max_ties: int | None = None, both_strands: bool = False,
               secondary: bool = False, sort_coordinate: bool = False,
-              max_read_len: int = 1000, batch_size: int = 50_000, threads: int = 0) -> dict:
+              max_read_len: int = 1000, batch_size: int = 50_000, threads: int = 0,
+              stats: dict | None = None, depth: int = 2) -> dict:
     """The CLI's unpaired run (align.rs:1822-2250, the --device gpu path) over
     a scorer: every batch of `in_path` mapped on the device (map_reads_scored
     with min_score / max_ties / both strands), its records built and written
-    to `out_path` in order (or coordinate order).  Returns counts."""
+    to `out_path` in input order (or coordinate order).  Returns counts.
+
+    Three stages run on their own threads, as the CLI's reader, GPU feeder
+    and workers do (align.rs:2078-2250): reading batch k + 1, mapping batch k
+    on the device, building and writing the records of batch k - 1; at most
+    `depth` batches wait between the stages.  `stats`, if given, receives the
+    seconds each stage spent (read, map, encode, write; they overlap, so they
+    add up to more than the wall time)."""
     ref_lens = [len(r) for r in ref_letters]
     out = {"reads": 0, "records": 0, "batches": 0}
+    st = stats if stats is not None else {}
+    for k in ("read", "map", "encode", "write"):
+        st.setdefault(k, 0.0)
+
+    def mapped(batch):
+        t0 = time.perf_counter()
+        m = scorer.map_reads(batch.reads(), min_score=min_score, max_ties=max_ties,
+                             both_strands=both_strands, ref_letters=ref_letters)
+        st["map"] += time.perf_counter() - t0
+        return batch, m
+
     with BamReader(in_path, threads) as rd, \
             BamWriter(out_path, header_text(ref_names, ref_lens, sort_coordinate), ref_names,
-                      ref_lens, sort_coordinate, threads) as wr:
-        for seq, batch in enumerate(rd.batches(batch_size, max_read_len)):
-            m = scorer.map_reads(batch.reads(), min_score=min_score, max_ties=max_ties,
-                                 both_strands=both_strands, ref_letters=ref_letters)
+                      ref_lens, sort_coordinate, threads) as wr, \
+            ThreadPoolExecutor(1) as rpool, ThreadPoolExecutor(1) as mpool, \
+            ThreadPoolExecutor(1) as opool:
+        it = rd.batches(batch_size, max_read_len)
+
+        def read_next():
+            t0 = time.perf_counter()
+            b = next(it, None)
+            st["read"] += time.perf_counter() - t0
+            return b
+
+        def emit(seq, mfut):
+            batch, m = mfut.result()
+            t0 = time.perf_counter()
             rec = encode(batch, m, ref_names, secondary, threads)
+            t1 = time.perf_counter()
             wr.push(seq, rec)
+            st["encode"] += t1 - t0
+            st["write"] += time.perf_counter() - t1
             out["reads"] += len(batch)
             out["records"] += rec.n_records
             out["batches"] += 1
             rec.free()
             batch.free()
+
+        inflight = deque()
+        try:
+            nxt, seq = rpool.submit(read_next), 0
+            while True:
+                batch = nxt.result()
+                if batch is None:
+                    break
+                nxt = rpool.submit(read_next)
+                inflight.append(opool.submit(emit, seq, mpool.submit(mapped, batch)))
+                seq += 1
+                while len(inflight) > max(depth, 1):
+                    inflight.popleft().result()
+            while inflight:
+                inflight.popleft().result()
+        except BaseException:
+            for p in (rpool, mpool, opool):
+                p.shutdown(wait=True, cancel_futures=True)
+            raise
+        t0 = time.perf_counter()
+    st["write"] += time.perf_counter() - t0  # the writer's close: its last blocks (or the sort)
     return out

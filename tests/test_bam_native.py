@@ -191,3 +191,43 @@ def test_mapping_from_arrays_checks_its_offsets():
     m.reads["first_hit"] = 2 ** 64 - 1
     with pytest.raises(RuntimeError):
         EB.mapping_handle(m)
+
+
+class OracleScorer:
+    """A stand-in for GpuScorer.map_reads that maps with the oracle, so the
+    pipeline of align_bam runs on the CPU."""
+
+    def __init__(self, oracle, refs, scoring, local):
+        self.oracle, self.refs, self.scoring, self.local = oracle, refs, scoring, local
+        self.calls = 0
+
+    def map_reads(self, reads, min_score=0, max_ties=None, both_strands=False, ref_letters=None):
+        codes, off, lens = reads
+        letters = [bytes(b"ACGTN"[int(c)] for c in codes[int(o):int(o) + int(n)])
+                   for o, n in zip(off, lens)]
+        self.calls += 1
+        ms = self.oracle.map_reads(letters, self.refs, self.scoring, self.local,
+                                   min_score=min_score, max_ties=max_ties,
+                                   both_strands=both_strands)
+        return mappings_from_oracle(ms)
+
+
+@pytest.mark.parametrize("label", sorted(golden_digests()))
+def test_align_bam_pipeline_writes_the_reference_record_stream(oracle, tmp_path, label):
+    """align_bam's overlapped read / map / encode / write, in batches of 13,
+    with the oracle's mappings: the golden stream, input order kept."""
+    from oracle import bam as B
+    want = golden_digests()[label]
+    o = flag_set(label)
+    names, refs = trna_panel()
+    sc = OracleScorer(oracle, refs, o["scoring"], o["local"])
+    path = str(tmp_path / "out.bam")
+    st = {}
+    n = EB.align_bam(sc, FIXTURE, path, names, refs, min_score=o["min_score"],
+                     max_ties=o["max_ties"], both_strands=o["both"], secondary=o["secondary"],
+                     sort_coordinate=o["sort"], max_read_len=o["max_read_len"], batch_size=13,
+                     threads=3, stats=st)
+    assert n["batches"] == sc.calls == 5 and n["reads"] == 60
+    assert n["records"] == want["records"]
+    assert format(B.fnv1a64(record_stream(path)), "016x") == want["fnv1a64"]
+    assert set(st) == {"read", "map", "encode", "write"}
