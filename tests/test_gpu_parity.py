@@ -90,6 +90,21 @@ def test_gpu_scores_equal_scalar_random_panel(oracle):
             assert st[(KERNEL_AUTO, 512, 1)]["panel_chunks"] == 1
 
 
+def test_gpu_gap_open_cheaper_than_extend(oracle):
+    """Schemes whose gap open costs less than an extension (|o| < |e|; valid
+    for the reference, scoring.rs:70-100), where a gap of one base can beat
+    the extension of an open one: short and long (multi-pass) reads, both
+    modes, every kernel setting."""
+    rng = Rng(0x5EED_0101 + 3)
+    letters = random_panel(rng, 37, 20, 280)
+    panel = [encode(s) for s in letters]
+    reads = reads_for(rng, letters, 40)
+    reads += [encode(random_seq(rng, 1100 + 150 * k, 0.01)) for k in range(3)]
+    for scoring in ((2, -3, -1, -5), (1, -1, 0, -2), (3, -2, -2, -4)):
+        for mode in (Mode.LOCAL, Mode.SEMIGLOBAL):
+            check(oracle, panel, reads, scoring, mode, "open below extend")
+
+
 def test_gpu_scores_equal_scalar_wide_panel(oracle):
     """gpu_parity.rs:234-247: 300 references up to 620 nt -- too big for the
     shared-memory panel, so the batched kernel reads it through L2."""
