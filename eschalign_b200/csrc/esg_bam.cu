@@ -3,7 +3,9 @@
 // The CLI's I/O stage for unpaired reads (crates/eschalign-cli/src/align.rs):
 //   * reading: read_batches (align.rs:604-660) -- primary records of a BGZF
 //     BAM in batches; secondary and supplementary records skipped; a record
-//     aligned to the reverse strand refused;
+//     aligned to the reverse strand refused; or the records of a FASTA or
+//     FASTQ file, plain or gzip (sniff, FastxReader, fastx_to_record:
+//     align.rs:385-563), each taken as an unmapped record;
 //   * the output records of a read's mapping: build_records
 //     (align.rs:1084-1200) with OWNED_TAGS (346-352), int_value (1001-1015),
 //     sam_cigar / clipped_span (1017-1052), xa_entry (1054-1069); a read over
@@ -24,7 +26,9 @@
 #include <zlib.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
+#include <cctype>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -315,6 +319,15 @@ struct esg_bam_reader {
   size_t pos = 0;            // consumed prefix of buf
   bool eof = false;
   uint64_t skipped = 0;      // secondary / supplementary records
+  // FASTA / FASTQ input (plain or gzip, read through zlib's gz reader)
+  int format = 0;            // 0 BAM, 1 FASTA, 2 FASTQ
+  gzFile gz = nullptr;
+  std::vector<char> lbuf;    // bytes read and not yet split into lines
+  size_t lpos = 0, lend = 0;
+  bool leof = false;
+  uint64_t line_no = 0;
+  std::string pending;       // a FASTA header met while ending the previous record
+  bool has_pending = false;
 };
 
 struct esg_bam_batch {
@@ -377,6 +390,152 @@ static esg_status need(esg_bam_reader* r, size_t n, bool* ok) {
   return ESG_OK;
 }
 
+// ------------------------------------------------------------ FASTA / FASTQ
+// The CLI's FastxReader (align.rs:436-537), normalise_seq and fastx_to_record
+// (align.rs:539-563): multi-line FASTA, four-line FASTQ; a record's name is
+// its header up to the first ASCII whitespace; FASTQ qualities are Phred + 33
+// (saturating at 0); sequences upper-cased, U read as T, anything outside the
+// BAM alphabet as N.  Each record becomes an unmapped BAM record, so the
+// encoder treats every input alike.
+
+// Rust's u8::is_ascii_whitespace: space, \t, \n, \x0C, \r.
+bool ascii_ws(uint8_t c) { return c == ' ' || c == '\t' || c == '\n' || c == 0x0c || c == '\r'; }
+
+// Next line without its terminator (trailing \n and \r dropped); false at
+// the end of the input.
+static esg_status next_line(esg_bam_reader* r, std::string& line, bool* got) {
+  line.clear();
+  *got = false;
+  for (;;) {
+    if (r->lpos == r->lend) {
+      if (r->leof) break;
+      const int n = gzread(r->gz, r->lbuf.data(), (unsigned)r->lbuf.size());
+      if (n < 0) return berr(ESG_ERR_BAD_ARGUMENT, "reading the input failed (corrupt gzip?)");
+      r->lpos = 0;
+      r->lend = (size_t)n;
+      if (n == 0) {
+        r->leof = true;
+        break;
+      }
+    }
+    const char* b = r->lbuf.data() + r->lpos;
+    const char* nl = (const char*)memchr(b, '\n', r->lend - r->lpos);
+    const size_t take = nl ? (size_t)(nl - b) : r->lend - r->lpos;
+    line.append(b, take);
+    *got = true;
+    r->lpos += take;
+    if (nl) {
+      ++r->lpos;
+      break;
+    }
+  }
+  if (*got) {
+    ++r->line_no;
+    while (!line.empty() && (line.back() == '\n' || line.back() == '\r')) line.pop_back();
+  }
+  return ESG_OK;
+}
+
+// Append one FASTX record to `bytes` as an unmapped BAM record (without its
+// block_size); false in *got at the end of the input.
+static esg_status next_fastx(esg_bam_reader* r, std::vector<uint8_t>& bytes, bool* got) {
+  static const std::array<uint8_t, 256> to4 = [] {
+    const char* letters = "=ACMGRSVTWYHKDBN";
+    std::array<uint8_t, 256> t{};
+    t.fill(15);
+    for (int k = 0; k < 16; ++k) {
+      t[(uint8_t)letters[k]] = (uint8_t)k;
+      t[(uint8_t)tolower(letters[k])] = (uint8_t)k;
+    }
+    t['U'] = t['u'] = 8;  // U as T
+    return t;
+  }();
+  *got = false;
+  std::string header, seq, qual, line;
+  bool have = false;
+  esg_status st;
+  const bool fastq = r->format == 2;
+  if (!fastq && r->has_pending) {
+    header.swap(r->pending);
+    r->has_pending = false;
+    have = true;
+  }
+  while (!have) {
+    if ((st = next_line(r, line, &have)) != ESG_OK) return st;
+    if (!have) return ESG_OK;  // end of input
+    if (line.empty()) have = false;
+    else header.swap(line);
+  }
+  const char mark = fastq ? '@' : '>';
+  if (header[0] != mark) {
+    char m[96];
+    snprintf(m, sizeof m, "%s line %llu: expected '%c'", fastq ? "FASTQ" : "FASTA",
+             (unsigned long long)r->line_no, mark);
+    return berr(ESG_ERR_BAD_ARGUMENT, m);
+  }
+  size_t ne = 1;
+  while (ne < header.size() && !ascii_ws((uint8_t)header[ne])) ++ne;
+  const std::string name = header.substr(1, ne - 1);
+  if (name.size() > 254) return berr(ESG_ERR_BAD_ARGUMENT, "read name longer than 254 bytes");
+  bool qual_given = false;
+  if (fastq) {
+    if ((st = next_line(r, seq, &have)) != ESG_OK) return st;
+    if (!have) return berr(ESG_ERR_BAD_ARGUMENT, "FASTQ truncated after header");
+    if ((st = next_line(r, line, &have)) != ESG_OK) return st;
+    if (!have || line.empty() || line[0] != '+') {
+      char m[64];
+      snprintf(m, sizeof m, "FASTQ line %llu: expected '+'", (unsigned long long)r->line_no);
+      return berr(ESG_ERR_BAD_ARGUMENT, m);
+    }
+    if ((st = next_line(r, qual, &have)) != ESG_OK) return st;
+    if (!have) return berr(ESG_ERR_BAD_ARGUMENT, "FASTQ truncated before quality");
+    if (qual.size() != seq.size()) {
+      char m[128];
+      snprintf(m, sizeof m, "FASTQ line %llu: %zu quality values for %zu bases",
+               (unsigned long long)r->line_no, qual.size(), seq.size());
+      return berr(ESG_ERR_BAD_ARGUMENT, m);
+    }
+    qual_given = true;
+  } else {
+    for (;;) {
+      if ((st = next_line(r, line, &have)) != ESG_OK) return st;
+      if (!have) break;
+      if (!line.empty() && line[0] == '>') {
+        r->pending.swap(line);
+        r->has_pending = true;
+        break;
+      }
+      for (char c : line)
+        if (!ascii_ws((uint8_t)c)) seq.push_back(c);
+    }
+  }
+  if (seq.size() > 0xffffffffull) return berr(ESG_ERR_BAD_ARGUMENT, "read too long");
+  const uint32_t l = (uint32_t)seq.size(), nl = (uint32_t)name.size() + 1;
+  put32(bytes, 0xffffffffu);  // reference: none
+  put32(bytes, 0xffffffffu);  // position: none
+  bytes.push_back((uint8_t)nl);
+  bytes.push_back(255);       // mapping quality: missing
+  put16(bytes, 4680);
+  put16(bytes, 0);            // no CIGAR
+  put16(bytes, 0x4);          // unmapped
+  put32(bytes, l);
+  put32(bytes, 0xffffffffu);
+  put32(bytes, 0xffffffffu);
+  put32(bytes, 0);
+  bytes.insert(bytes.end(), name.begin(), name.end());
+  bytes.push_back(0);
+  for (uint32_t k = 0; k < l; k += 2)
+    bytes.push_back((uint8_t)(to4[(uint8_t)seq[k]] << 4 |
+                              (k + 1 < l ? to4[(uint8_t)seq[k + 1]] : 0)));
+  if (qual_given) {
+    for (char q : qual) bytes.push_back((uint8_t)q >= 33 ? (uint8_t)((uint8_t)q - 33) : 0);
+  } else {
+    bytes.insert(bytes.end(), l, 0xff);
+  }
+  *got = true;
+  return ESG_OK;
+}
+
 extern "C" {
 
 esg_status esg_bam_open(const char* path, uint32_t threads, esg_bam_reader** out) {
@@ -388,6 +547,47 @@ esg_status esg_bam_open(const char* path, uint32_t threads, esg_bam_reader** out
   if (!r->f) {
     delete r;
     return berr(ESG_ERR_BAD_ARGUMENT, std::string("cannot open ") + path);
+  }
+  {
+    // sniff (align.rs:385-414): BGZF whose payload starts with BAM\1, or a
+    // FASTA / FASTQ, plain or gzip, by its first non-blank character
+    uint8_t magic[2] = {0, 0};
+    const bool gzip = fread(magic, 1, 2, r->f) == 2 && magic[0] == 0x1f && magic[1] == 0x8b;
+    rewind(r->f);
+    gzFile g = gzopen(path, "rb");
+    if (!g) {
+      esg_bam_close(r);
+      return berr(ESG_ERR_BAD_ARGUMENT, std::string("cannot open ") + path);
+    }
+    std::vector<char> head(1 << 16);
+    const int n = gzread(g, head.data(), (unsigned)head.size());
+    gzclose(g);
+    if (n >= 4 && memcmp(head.data(), "BAM\1", 4) == 0) {
+      if (!gzip) {
+        esg_bam_close(r);
+        return berr(ESG_ERR_BAD_ARGUMENT, std::string(path) + ": uncompressed BAM is not supported");
+      }
+    } else {
+      int k = 0;
+      while (k < n && ascii_ws((uint8_t)head[k])) ++k;
+      if (k == n || (head[k] != '>' && head[k] != '@')) {
+        esg_bam_close(r);
+        return berr(ESG_ERR_BAD_ARGUMENT,
+                    std::string(path) + ": not a BAM, FASTA or FASTQ file (plain or gzip)");
+      }
+      r->format = head[k] == '>' ? 1 : 2;
+      fclose(r->f);
+      r->f = nullptr;
+      r->gz = gzopen(path, "rb");
+      if (!r->gz) {
+        esg_bam_close(r);
+        return berr(ESG_ERR_BAD_ARGUMENT, std::string("cannot open ") + path);
+      }
+      gzbuffer(r->gz, 1u << 20);
+      r->lbuf.resize(1u << 20);
+      *out = r;
+      return ESG_OK;
+    }
   }
   bool ok = false;
   esg_status st = need(r, 8, &ok);
@@ -430,7 +630,22 @@ esg_status esg_bam_read_batch(esg_bam_reader* r, uint32_t max_reads, uint32_t ma
   *out = nullptr;
   auto* b = new esg_bam_batch();
   std::vector<uint64_t> rec_off;
-  while (b->recs.size() < max_reads) {
+  while (r->format != 0 && b->recs.size() < max_reads) {
+    const size_t at = b->bytes.size();
+    bool got = false;
+    const esg_status st = next_fastx(r, b->bytes, &got);
+    if (st != ESG_OK) {
+      delete b;
+      return st;
+    }
+    if (!got) break;
+    InRec x{};
+    parse_rec(b->bytes.data() + at, (uint32_t)(b->bytes.size() - at), x);
+    x.rec = nullptr;  // set once b->bytes stops growing
+    rec_off.push_back(at);
+    b->recs.push_back(x);
+  }
+  while (r->format == 0 && b->recs.size() < max_reads) {
     bool ok = false;
     esg_status st = need(r, 4, &ok);
     if (st != ESG_OK) {
@@ -501,6 +716,7 @@ void esg_bam_batch_free(esg_bam_batch* b) { delete b; }
 void esg_bam_close(esg_bam_reader* r) {
   if (!r) return;
   if (r->f) fclose(r->f);
+  if (r->gz) gzclose(r->gz);
   delete r;
 }
 

@@ -602,13 +602,19 @@ typedef struct esg_bam_options {
     uint32_t reserved;  /* 0 */
 } esg_bam_options;
 
-/* Open a BGZF-compressed BAM and read its header (threads: inflating
- * threads, 0 = the host's cores). */
+/* Open the CLI's unpaired input (align.rs:385-414): a BGZF-compressed BAM
+ * (header read; threads: inflating threads, 0 = the host's cores), or a
+ * FASTA or FASTQ file, plain or gzip, told apart by content.  FASTX records
+ * come in as unmapped records with no header (align.rs:436-563: the name up
+ * to the first blank, sequences upper-cased with U as T and other letters
+ * outside the BAM alphabet as N, FASTQ qualities Phred + 33, FASTA ones
+ * missing).  An uncompressed BAM is refused, as the CLI refuses it. */
 esg_status esg_bam_open(const char* path, uint32_t threads, esg_bam_reader** out);
 const char* esg_bam_header_text(const esg_bam_reader* reader, uint64_t* len);
 /* The next primary records, at most max_reads (secondary and supplementary
  * ones skipped; a record aligned to the reverse strand is refused with
- * ESG_ERR_BAD_ARGUMENT).  A batch of 0 reads means the end of the file.
+ * ESG_ERR_BAD_ARGUMENT, as is a malformed FASTA / FASTQ record).  A batch of
+ * 0 reads means the end of the file.
  * Reads over max_read_len (0 = no limit) get length 0 in
  * esg_bam_batch_reads, so the mapping stage leaves them unmapped. */
 esg_status esg_bam_read_batch(esg_bam_reader* reader, uint32_t max_reads, uint32_t max_read_len,

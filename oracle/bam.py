@@ -14,7 +14,9 @@ Restated from crates/eschalign-cli/src/align.rs:
   read and, with --secondary, one record per further hit;
 * the coordinate sort (align.rs:2406-2450): stable on (reference, position,
   reverse flag), unmapped last;
-* the reverse complement of letters (crates/eschalign/src/alphabet.rs:69-80).
+* the reverse complement of letters (crates/eschalign/src/alphabet.rs:69-80);
+* FASTA / FASTQ input: sniff, FastxReader, normalise_seq and fastx_to_record
+  (align.rs:385-563).
 
 The record buffer the CLI edits (noodles-sam's RecordBuf data) removes a tag
 by moving its last tag into the freed slot; the new tags go to the end.  The
@@ -104,6 +106,84 @@ def input_reads(recs):
             raise ValueError("input record aligned to the reverse strand")
         out.append(r)
     return out
+
+
+_ASCII_WS = b" \t\n\x0c\r"  # Rust's u8::is_ascii_whitespace
+
+
+def sniff(data: bytes) -> str:
+    """sniff (align.rs:385-414): "bam", "fasta" or "fastq"."""
+    gz = data[:2] == b"\x1f\x8b"
+    payload = gzip.decompress(data) if gz else data
+    if payload[:4] == b"BAM\1":
+        if not gz:
+            raise ValueError("uncompressed BAM is not supported")
+        return "bam"
+    first = payload.lstrip(_ASCII_WS)[:1]
+    if first == b">":
+        return "fasta"
+    if first == b"@":
+        return "fastq"
+    raise ValueError("not a BAM, FASTA or FASTQ file (plain or gzip)")
+
+
+def normalise_seq(seq: bytes) -> bytes:
+    """normalise_seq (align.rs:539-549): upper case, U as T, anything outside
+    the BAM alphabet as N."""
+    out = bytearray()
+    for b in seq.upper():
+        out.append(ord("T") if b == ord("U") else (b if b in SEQ_CODES else ord("N")))
+    return bytes(out)
+
+
+def read_fastx(data: bytes):
+    """FastxReader::next_record (align.rs:436-537) over a whole FASTA / FASTQ
+    file (plain or gzip), each record as fastx_to_record (align.rs:551-563)
+    makes it: an unmapped record in read_bam's form (no tags; FASTQ
+    qualities Phred + 33 saturating at 0, FASTA ones missing)."""
+    fastq = sniff(data) == "fastq"
+    text = gzip.decompress(data) if data[:2] == b"\x1f\x8b" else data
+    lines = text.split(b"\n")
+    if lines and lines[-1] == b"":
+        lines.pop()  # the terminator of the last line
+    lines = [ln.rstrip(b"\r\n") for ln in lines]
+
+    def name_of(h):
+        for k, b in enumerate(h):
+            if b in _ASCII_WS:
+                return h[:k]
+        return h
+    out, i = [], 0
+    while True:
+        while i < len(lines) and lines[i] == b"":
+            i += 1
+        if i == len(lines):
+            return out
+        h = lines[i]
+        i += 1
+        if h[:1] != (b"@" if fastq else b">"):
+            raise ValueError(f"line {i}: expected {'@' if fastq else '>'}")
+        name = name_of(h[1:])
+        if fastq:
+            if i >= len(lines):
+                raise ValueError("FASTQ truncated after header")
+            if i + 1 >= len(lines) or lines[i + 1][:1] != b"+":
+                raise ValueError("FASTQ: expected '+'")
+            if i + 2 >= len(lines):
+                raise ValueError("FASTQ truncated before quality")
+            seq, qual = lines[i], lines[i + 2]
+            if len(qual) != len(seq):
+                raise ValueError("FASTQ: quality and sequence lengths differ")
+            i += 3
+            q = bytes(max(c - 33, 0) for c in qual)
+        else:
+            seq = bytearray()
+            while i < len(lines) and lines[i][:1] != b">":
+                seq += bytes(b for b in lines[i] if b not in _ASCII_WS)
+                i += 1
+            seq, q = bytes(seq), b""
+        out.append({"flag": FLAG_UNMAPPED, "name": name, "seq": normalise_seq(seq),
+                    "qual": q, "aux": []})
 
 
 def reg2bin(beg: int, end: int) -> int:

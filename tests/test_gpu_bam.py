@@ -30,3 +30,34 @@ def test_align_bam_writes_the_reference_record_stream(tmp_path, label, batch_siz
                          max_read_len=o["max_read_len"], batch_size=batch_size, threads=4)
     assert n["records"] == want["records"]
     assert format(B.fnv1a64(record_stream(path)), "016x") == want["fnv1a64"]
+
+
+@pytest.mark.parametrize("label", ["default", "semiglobal_both_secondary", "sort_coordinate"])
+def test_align_bam_fastq_gz_input(oracle, tmp_path, label):
+    """The fixture's reads as gzip FASTQ through the same run: the records
+    the oracle builds for the FASTQ records (read_fastx + build_records, in
+    coordinate order when sorting)."""
+    import gzip
+
+    from oracle import bam as B
+    from tests.test_bam_fastx import fastq_of
+    from tests.test_bam_golden import input_records
+    o = flag_set(label)
+    names, refs = trna_panel()
+    text = gzip.compress(fastq_of(input_records()))
+    src, dst = str(tmp_path / "reads.fq.gz"), str(tmp_path / "out.bam")
+    open(src, "wb").write(text)
+    recs = B.read_fastx(text)
+    ms = oracle.map_reads([r["seq"] for r in recs], refs, o["scoring"], o["local"],
+                          min_score=o["min_score"], max_ties=o["max_ties"],
+                          both_strands=o["both"])
+    want = [x for r, m in zip(recs, ms) for x in B.build_records(r, m, names, o["secondary"])]
+    if o["sort"]:
+        want = B.coordinate_order(want)
+    mode = Mode.LOCAL if o["local"] else Mode.SEMIGLOBAL
+    with GpuScorer([encode(r) for r in refs], Scoring(*o["scoring"]), mode) as g:
+        n = EB.align_bam(g, src, dst, names, refs, min_score=o["min_score"],
+                         max_ties=o["max_ties"], both_strands=o["both"],
+                         secondary=o["secondary"], sort_coordinate=o["sort"], batch_size=11)
+    assert n["reads"] == len(recs) and n["records"] == len(want)
+    assert record_stream(dst) == b"".join(want)
