@@ -268,3 +268,21 @@ def test_map_pairs_large_batch_equals_small_ones():
                                min_score=40, both_strands=True)
             for p in range(len(part)):
                 assert whole.pair_mapping(p0 + p) == part.pair_mapping(p), p0 + p
+
+
+def test_map_mid_sized_call_equals_small_ones():
+    """50 000 C2 reads (the CLI's batch size) in one call equal five calls
+    of 10 000, array for array."""
+    refs = synth.panel_tiles()
+    data = synth.reads_c2(refs, n=50_000, seed=0x5EED_0908)
+    with GpuScorer(refs, Scoring(*SCHEME), Mode.LOCAL) as g:
+        whole = g.map_reads(data.tuple(), both_strands=True)
+        parts = [g.map_reads(data.slice(k, k + 10_000).tuple(), both_strands=True)
+                 for k in range(0, 50_000, 10_000)]
+    for f in ("best_score", "suboptimal", "n_tied", "flags", "n_hits"):
+        assert (whole.reads[f] == np.concatenate([p.reads[f] for p in parts])).all(), f
+    for f in ("reference", "reverse", "score", "query_start", "query_end", "ref_start",
+              "ref_end", "n_ops", "nm", "md_len"):
+        assert (whole.hits[f] == np.concatenate([p.hits[f] for p in parts])).all(), f
+    assert (whole.ops == np.concatenate([p.ops for p in parts])).all()
+    assert whole.md_bytes == b"".join(p.md_bytes for p in parts)
