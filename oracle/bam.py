@@ -16,7 +16,11 @@ Restated from crates/eschalign-cli/src/align.rs:
   reverse flag), unmapped last;
 * the reverse complement of letters (crates/eschalign/src/alphabet.rs:69-80);
 * FASTA / FASTQ input: sniff, FastxReader, normalise_seq and fastx_to_record
-  (align.rs:385-563).
+  (align.rs:385-563);
+* paired runs: PairSource::next_pair and mate_stem (align.rs:700-870), the
+  mate placements of process_pair_chunk (align.rs:1683-1713),
+  build_pair_records with clipped_span / sam_cigar_ad / template_length
+  (align.rs:1021-1051, 1203-1425).
 
 The record buffer the CLI edits (noodles-sam's RecordBuf data) removes a tag
 by moving its last tag into the freed slot; the new tags go to the end.  The
@@ -210,14 +214,21 @@ def str_field(tag: bytes, s: str) -> bytes:
     return tag + b"Z" + s.encode() + b"\0"
 
 
-def encode_record(refid, pos, mapq, cigar, flag, name, seq, qual, aux) -> bytes:
+def encode_record(refid, pos, mapq, cigar, flag, name, seq, qual, aux, mate_ref=-1, mate_pos=-1,
+                  tlen=0) -> bytes:
     """One BAM record (block_size included); cigar is [(length, op)], pos
-    0-based or -1, aux the encoded fields in order."""
+    0-based or -1, aux the encoded fields in order.  The bin is noodles'
+    (the writer of the CLI): the region [pos, pos + span - 1], so a record
+    with a position and no CIGAR (an unmapped mate placed at its partner's
+    position) takes the bin of [pos, pos - 1], and none (4680) at pos 0."""
     span = sum(n for n, op in cigar if op in "MDN=X")
-    b = 4680 if pos < 0 else reg2bin(pos, pos + span)
+    if pos < 0 or (span == 0 and pos == 0):
+        b = 4680
+    else:
+        b = reg2bin(pos, pos + span)
     nm = (name if name else b"*") + b"\0"
     body = struct.pack("<iiBBHHHIiii", refid, pos, len(nm), mapq, b, len(cigar), flag, len(seq),
-                       -1, -1, 0)
+                       mate_ref, mate_pos, tlen)
     body += nm + b"".join(struct.pack("<I", n << 4 | CIGAR_CODES[op]) for n, op in cigar)
     sb = bytearray((len(seq) + 1) // 2)
     for k, ch in enumerate(seq):
@@ -244,11 +255,11 @@ def _cigar_ops(s: str):
     return out
 
 
-def _without_owned(aux):
-    """RecordBuf data with OWNED_TAGS removed: each removal moves the last
-    tag into the freed slot."""
+def _without_owned(aux, tags=OWNED_TAGS):
+    """RecordBuf data with `tags` removed, in that order: each removal moves
+    the last tag into the freed slot."""
     aux = list(aux)
-    for t in OWNED_TAGS:
+    for t in tags:
         for i, (tag, _) in enumerate(aux):
             if tag == t:
                 last = aux.pop()
@@ -301,6 +312,222 @@ def build_records(rec, m, ref_names, secondary=False):
             out.append(encode_record(h["reference"], h["ref_start"], 0, sam_cigar(h),
                                      FLAG_SECONDARY | kept | (FLAG_REVERSE if h["reverse"] else 0),
                                      rec["name"], b"", b"", d))
+    return out
+
+
+# ---------------------------------------------------------------- pairs
+FLAG_PAIRED, FLAG_PROPER, FLAG_MATE_UNMAPPED = 0x1, 0x2, 0x8
+FLAG_MATE_REVERSE, FLAG_FIRST, FLAG_LAST = 0x20, 0x40, 0x80
+PAIR_OWNED_TAGS = OWNED_TAGS + (b"MC", b"ad")  # align.rs:1203-1206, 1262
+
+
+def mate_stem(name: bytes) -> bytes:
+    """mate_stem (align.rs:700-706): the name without a trailing /1 or /2."""
+    return name[:-2] if len(name) >= 2 and name[-2:] in (b"/1", b"/2") else name
+
+
+def _renamed(rec, name):
+    r = dict(rec)
+    r["name"] = name
+    return r
+
+
+def read_pairs(data1: bytes, data2: bytes | None = None):
+    """PairSource::next_pair (align.rs:759-870): [(mate 1, mate 2)] of two
+    FASTA / FASTQ files, one interleaved FASTX file, or a paired BAM (mates
+    adjacent, 0x1 with one of 0x40 / 0x80), each mate named by the pair's
+    stem (process_pair_chunk, align.rs:1631-1639).  Errors raise ValueError
+    naming the read."""
+    out = []
+    if data2 is not None:
+        a, b = read_fastx(data1), read_fastx(data2)
+        for k in range(max(len(a), len(b))):
+            if k >= len(b):
+                raise ValueError(f"read {a[k]['name'].decode()} has no mate")
+            if k >= len(a):
+                raise ValueError(f"read {b[k]['name'].decode()} has no mate")
+            if mate_stem(a[k]["name"]) != mate_stem(b[k]["name"]):
+                raise ValueError(f"mate names differ: {a[k]['name'].decode()} but "
+                                 f"{b[k]['name'].decode()}")
+            stem = mate_stem(a[k]["name"])
+            out.append((_renamed(a[k], stem), _renamed(b[k], stem)))
+        return out
+    if sniff(data1) != "bam":
+        recs = read_fastx(data1)
+        for k in range(0, len(recs), 2):
+            if k + 1 >= len(recs):
+                raise ValueError(f"read {recs[k]['name'].decode()} has no mate")
+            x, y = recs[k], recs[k + 1]
+            if mate_stem(x["name"]) != mate_stem(y["name"]):
+                raise ValueError(f"read {x['name'].decode()} has no mate: the next record is "
+                                 f"{y['name'].decode()}")
+            stem = mate_stem(x["name"])
+            out.append((_renamed(x, stem), _renamed(y, stem)))
+        return out
+    _, _, recs = read_bam(data1)
+    recs = input_reads(recs)
+    for k in range(0, len(recs), 2):
+        x = recs[k]
+        fx = x["flag"]
+        if not fx & FLAG_PAIRED or bool(fx & FLAG_FIRST) == bool(fx & FLAG_LAST):
+            raise ValueError(f"read {x['name'].decode()}: not a mate")
+        if k + 1 >= len(recs):
+            raise ValueError(f"read {x['name'].decode()} has no mate")
+        y = recs[k + 1]
+        fy = y["flag"]
+        if mate_stem(x["name"]) != mate_stem(y["name"]):
+            raise ValueError(f"read {x['name'].decode()} has no mate: the next record is "
+                             f"{y['name'].decode()}")
+        if (not fy & FLAG_PAIRED or bool(fy & FLAG_FIRST) == bool(fy & FLAG_LAST)
+                or bool(fy & FLAG_FIRST) == bool(fx & FLAG_FIRST)):
+            raise ValueError(f"read {mate_stem(x['name']).decode()}: not mate 1 and mate 2")
+        stem = mate_stem(x["name"])
+        m1, m2 = (x, y) if fx & FLAG_FIRST else (y, x)
+        out.append((_renamed(m1, stem), _renamed(m2, stem)))
+    return out
+
+
+def clipped_span(h, ad):
+    """clipped_span (align.rs:1021-1029): the aligned part within the whole
+    SEQ, the adapter being the 3' end (the start of a reverse hit's SEQ)."""
+    shift = ad if h["reverse"] else 0
+    return h["query_start"] + shift, h["query_end"] + shift
+
+
+def sam_cigar_ad(h, full, ad):
+    """sam_cigar_ad (align.rs:1031-1051) as [(length, op)]."""
+    qs, qe = clipped_span(h, ad)
+    c = [(qs, "S")] if qs > 0 else []
+    c += _cigar_ops(h["cigar"])
+    if full > qe:
+        c.append((full - qe, "S"))
+    return c
+
+
+def _cigar_text(c):
+    return "".join(f"{n}{op}" for n, op in c)
+
+
+def template_length(h, partner, first):
+    """template_length (align.rs:1225-1236)."""
+    n = max(h["ref_end"], partner["ref_end"]) - min(h["ref_start"], partner["ref_start"])
+    left = h["ref_start"] < partner["ref_start"] or (h["ref_start"] == partner["ref_start"]
+                                                     and first)
+    return n if left else -n
+
+
+def pair_placements(pm):
+    """process_pair_chunk's MatePlacement per mate (align.rs:1683-1713) from
+    the oracle's map_pairs form; returns (placements, proper)."""
+    if pm["proper"]:
+        hits = pm["hits"]
+        return [{"primary": hits[0]["mates"][m],
+                 "others": [h["mates"][m] for h in hits[1:]],
+                 "partners": [h["mates"][1 - m] for h in hits[1:]],
+                 "score": hits[0]["mates"][m]["score"], "xs": pm["suboptimal"][m],
+                 "unique": pm["n_tied"] == 1} for m in range(2)], True
+    ms = pm["mates"]
+    out = []
+    for m in range(2):
+        me, other = ms[m], ms[1 - m]
+        others = me["hits"][1:]
+        out.append({"primary": me["hits"][0] if me["hits"] else None, "others": others,
+                    "partners": [other["hits"][0] if other["hits"] else None] * len(others),
+                    "score": me["best_score"] if me["best_score"] is not None else 0,
+                    "xs": me["suboptimal"], "unique": me["n_tied"] == 1})
+    return out, False
+
+
+def build_pair_records(recs, pm, ad, ref_names, secondary=False):
+    """build_pair_records (align.rs:1238-1425) for one pair: [mate 1, mate 2,
+    then with `secondary` a pair of 0x100 records per further tie-set
+    member]; `ad` is [mate 1, mate 2] adapter bases, or None when adapters
+    were not searched (no `ad` tag)."""
+    place, proper = pair_placements(pm)
+    full = [len(recs[0]["seq"]), len(recs[1]["seq"])]
+    adn = ad if ad is not None else [0, 0]
+    seg = [FLAG_FIRST, FLAG_LAST]
+    st = []
+    for m in range(2):
+        r = recs[m]
+        kept = r["flag"] & (FLAG_QC_FAIL | FLAG_DUPLICATE)
+        fields = [f for _, f in _without_owned(r["aux"], PAIR_OWNED_TAGS)]
+        d = {"kept": kept, "flag": kept | FLAG_PAIRED | seg[m], "ref": -1, "pos": -1, "mapq": 0,
+             "cigar": [], "seq": r["seq"], "qual": r["qual"], "fields": fields,
+             "mate_ref": -1, "mate_pos": -1, "tlen": 0}
+        h = place[m]["primary"]
+        if h is None:
+            d["flag"] |= FLAG_UNMAPPED
+        else:
+            if h["reverse"]:
+                d["flag"] |= FLAG_REVERSE
+                d["seq"], d["qual"] = revcomp_letters(r["seq"]), r["qual"][::-1]
+            d["ref"], d["pos"] = h["reference"], h["ref_start"]
+            d["mapq"] = 60 if place[m]["unique"] else 0
+            d["cigar"] = sam_cigar_ad(h, full[m], adn[m])
+            fields += [int_field(b"NM", h["nm"]), str_field(b"MD", h["md"]),
+                       int_field(b"AS", place[m]["score"])]
+            if place[m]["xs"] is not None:
+                fields.append(int_field(b"XS", place[m]["xs"]))
+            if place[m]["others"]:
+                fields.append(str_field(b"XA", "".join(
+                    f"{ref_names[o['reference']]},{'-' if o['reverse'] else '+'}"
+                    f"{o['ref_start'] + 1},{_cigar_text(sam_cigar_ad(o, full[m], adn[m]))},"
+                    f"{o['nm']};" for o in place[m]["others"])))
+        if ad is not None:
+            fields.append(int_field(b"ad", ad[m]))
+        st.append(d)
+    for m in range(2):
+        o = 1 - m
+        h, oh, d = place[m]["primary"], place[o]["primary"], st[m]
+        if h is not None and oh is not None:
+            if oh["reverse"]:
+                d["flag"] |= FLAG_MATE_REVERSE
+            if proper:
+                d["flag"] |= FLAG_PROPER
+            d["mate_ref"], d["mate_pos"] = oh["reference"], oh["ref_start"]
+            d["fields"].append(str_field(b"MC", _cigar_text(sam_cigar_ad(oh, full[o], adn[o]))))
+            if h["reference"] == oh["reference"]:
+                d["tlen"] = template_length(h, oh, m == 0)
+        elif h is not None:
+            d["flag"] |= FLAG_MATE_UNMAPPED
+            d["mate_ref"], d["mate_pos"] = h["reference"], h["ref_start"]
+        elif oh is not None:
+            if oh["reverse"]:
+                d["flag"] |= FLAG_MATE_REVERSE
+            d["ref"], d["pos"] = oh["reference"], oh["ref_start"]
+            d["mate_ref"], d["mate_pos"] = oh["reference"], oh["ref_start"]
+        else:
+            d["flag"] |= FLAG_MATE_UNMAPPED
+    out = [encode_record(d["ref"], d["pos"], d["mapq"], d["cigar"], d["flag"], recs[m]["name"],
+                         d["seq"], d["qual"], d["fields"], d["mate_ref"], d["mate_pos"], d["tlen"])
+           for m, d in enumerate(st)]
+    if secondary:
+        for k in range(max(len(place[0]["others"]), len(place[1]["others"]))):
+            for m in range(2):
+                if k >= len(place[m]["others"]):
+                    continue
+                h, ph = place[m]["others"][k], place[m]["partners"][k]
+                f = FLAG_SECONDARY | FLAG_PAIRED | seg[m] | st[m]["kept"]
+                if h["reverse"]:
+                    f |= FLAG_REVERSE
+                fields = [int_field(b"NM", h["nm"]), str_field(b"MD", h["md"]),
+                          int_field(b"AS", h["score"])]
+                fields += [fl for t, fl in recs[m]["aux"] if t == b"RG"][:1]
+                mref, mpos, tlen = h["reference"], h["ref_start"], 0
+                if ph is not None:
+                    if ph["reverse"]:
+                        f |= FLAG_MATE_REVERSE
+                    mref, mpos = ph["reference"], ph["ref_start"]
+                    if proper:
+                        f |= FLAG_PROPER
+                        if ph["reference"] == h["reference"]:
+                            tlen = template_length(h, ph, m == 0)
+                else:
+                    f |= FLAG_MATE_UNMAPPED
+                out.append(encode_record(h["reference"], h["ref_start"], 0,
+                                         sam_cigar_ad(h, full[m], adn[m]), f, recs[m]["name"],
+                                         b"", b"", fields, mref, mpos, tlen))
     return out
 
 

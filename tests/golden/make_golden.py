@@ -100,8 +100,10 @@ def main(ref_root):
     for fq in ("pairs_R1.fq", "pairs_R2.fq"):
         with open(os.path.join(pdir, fq)) as fh:
             lines = fh.read().splitlines()
-        mates.append([(lines[i][1:], lines[i + 1]) for i in range(0, len(lines), 4)])
-    pairs = [{"name": a[0], "r1": a[1], "r2": b[1]} for a, b in zip(*mates)]
+        mates.append([(lines[i][1:], lines[i + 1], lines[i + 3])
+                      for i in range(0, len(lines), 4)])
+    pairs = [{"name": a[0], "r1": a[1], "r2": b[1], "q1": a[2], "q2": b[2]}
+             for a, b in zip(*mates)]
     panel = read_fasta(os.path.join(pdir, "pairs_panel.fa"))
     with open(os.path.join(here, "pairs_fixture.json"), "w") as fh:
         json.dump({"source": "pairs/pairs_panel.fa, pairs_R1.fq, pairs_R2.fq",
