@@ -233,6 +233,8 @@ SIGNATURES = {
     "esg_mapping_from_arrays": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, _u32p,
                                             C.c_uint64, C.c_char_p, C.c_uint64,
                                             C.POINTER(C.c_void_p)]),
+    "esg_mapping_set_pairs": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                          C.c_uint64]),
     "esg_server_new": (C.c_int32, [C.POINTER(EsgServerOptions), C.POINTER(C.c_void_p)]),
     "esg_server_add_scorer": (C.c_int32, [C.c_void_p, C.c_void_p, _u32p]),
     "esg_server_submit": (C.c_int32, [C.c_void_p, C.c_uint32, _u8p, _u64p, _u32p, C.c_uint32,
@@ -244,6 +246,9 @@ SIGNATURES = {
     "esg_bam_open": (C.c_int32, [C.c_char_p, C.c_uint32, C.POINTER(C.c_void_p)]),
     "esg_bam_header_text": (C.c_void_p, [C.c_void_p, _u64p]),
     "esg_bam_read_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "esg_bam_open_pairs": (C.c_int32, [C.c_char_p, C.c_char_p, C.c_uint32,
+                                       C.POINTER(C.c_void_p)]),
+    "esg_bam_read_pair_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
     "esg_bam_batch_reads": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                         C.POINTER(C.c_void_p), _u32p]),
     "esg_bam_batch_free": (None, [C.c_void_p]),
@@ -251,6 +256,9 @@ SIGNATURES = {
     "esg_bam_encode": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(EsgBamOptions),
                                    C.POINTER(C.c_char_p), C.c_uint32, C.c_uint32,
                                    C.POINTER(C.c_void_p)]),
+    "esg_bam_encode_pairs": (C.c_int32, [C.c_void_p, C.c_void_p, _u32p, C.POINTER(EsgBamOptions),
+                                         C.POINTER(C.c_char_p), C.c_uint32, C.c_uint32,
+                                         C.POINTER(C.c_void_p)]),
     "esg_bam_records_bytes": (C.c_void_p, [C.c_void_p, _u64p, _u32p]),
     "esg_bam_records_free": (None, [C.c_void_p]),
     "esg_bam_writer_open": (C.c_int32, [C.c_char_p, C.c_char_p, C.POINTER(C.c_char_p), _u32p,

@@ -20,7 +20,8 @@ from concurrent.futures import ThreadPoolExecutor
 import numpy as np
 
 from . import _native
-from .scorer import HIT_DTYPE, MAPPING_DTYPE, Mappings, _check, _ptr
+from .scorer import (HIT_DTYPE, MAPPING_DTYPE, PAIR_HIT_DTYPE, PAIR_MAPPING_DTYPE,
+                     GpuError, Mappings, _check, _ptr)
 
 
 def _lib():
@@ -110,6 +111,34 @@ class BamReader:
             pass
 
 
+class PairReader(BamReader):
+    """esg_bam_open_pairs: read pairs from two mate files, or from one
+    interleaved FASTX / paired BAM file (path2 None), in batches of pairs
+    (records 2p and 2p + 1)."""
+
+    def __init__(self, path1: str, path2: str | None = None, threads: int = 0):
+        self._lib = _lib()
+        h = C.c_void_p()
+        _check(self._lib, self._lib.esg_bam_open_pairs(path1.encode(),
+                                                       path2.encode() if path2 else None,
+                                                       threads, C.byref(h)))
+        self._h = h
+        n = C.c_uint64()
+        p = self._lib.esg_bam_header_text(h, C.byref(n))
+        self.header_text = C.string_at(p, n.value) if n.value else b""
+
+    def batches(self, max_pairs: int = 25_000, max_read_len: int = 0):
+        while True:
+            b = C.c_void_p()
+            _check(self._lib, self._lib.esg_bam_read_pair_batch(self._h, max_pairs,
+                                                                C.byref(b)))
+            batch = BamBatch(b)
+            if not len(batch):
+                batch.free()
+                return
+            yield batch
+
+
 class BamRecords:
     """Encoded output records (esg_bam_encode): the uncompressed BAM record
     stream of a batch, in read order."""
@@ -155,6 +184,15 @@ def mapping_handle(m: Mappings):
     _check(lib, lib.esg_mapping_from_arrays(reads.ctypes.data, reads.size, hits.ctypes.data,
                                             hits.size, _ptr(ops, C.c_uint32), ops.size, md,
                                             len(md), C.byref(h)))
+    if m.pairs is not None:
+        pairs = np.ascontiguousarray(m.pairs, dtype=PAIR_MAPPING_DTYPE)
+        phits = np.ascontiguousarray(m.pair_hits, dtype=PAIR_HIT_DTYPE)
+        st = lib.esg_mapping_set_pairs(h, pairs.ctypes.data, pairs.size, phits.ctypes.data,
+                                       phits.size)
+        if st:
+            err = lib.esg_last_error().decode(errors="replace")
+            lib.esg_mapping_free(h)
+            raise GpuError(st, err)
     return h
 
 
@@ -171,6 +209,29 @@ def encode(batch: BamBatch, mapping, ref_names, secondary: bool = False,
     try:
         _check(lib, lib.esg_bam_encode(batch._h, h, C.byref(opts), names, n, threads,
                                        C.byref(out)))
+    finally:
+        if own:
+            lib.esg_mapping_free(h)
+    return BamRecords(out)
+
+
+def encode_pairs(batch: BamBatch, mapping, ref_names, adapter_bases=None,
+                 secondary: bool = False, threads: int = 0) -> BamRecords:
+    """build_pair_records (align.rs:1238-1425) for every pair of `batch`
+    from its paired mapping (a Mappings with pairs, or an esg_mapping
+    handle); adapter_bases per mate (esg_pair_adapters), or None when
+    adapters were not searched."""
+    lib = _lib()
+    own = isinstance(mapping, Mappings)
+    h = mapping_handle(mapping) if own else mapping
+    names, n = _names(ref_names)
+    opts = _native.EsgBamOptions(int(bool(secondary)), 0)
+    ads = None if adapter_bases is None else np.ascontiguousarray(adapter_bases, dtype=np.uint32)
+    out = C.c_void_p()
+    try:
+        _check(lib, lib.esg_bam_encode_pairs(batch._h, h, None if ads is None else
+                                             _ptr(ads, C.c_uint32), C.byref(opts), names, n,
+                                             threads, C.byref(out)))
     finally:
         if own:
             lib.esg_mapping_free(h)
@@ -223,23 +284,12 @@ def header_text(ref_names, ref_lens, sort_coordinate: bool = False) -> bytes:
     return ("\n".join(lines) + "\n").encode()
 
 
-def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
-              min_score: int = 0, max_ties: int | None = None, both_strands: bool = False,
-              secondary: bool = False, sort_coordinate: bool = False,
-              max_read_len: int = 1000, batch_size: int = 50_000, threads: int = 0,
-              stats: dict | None = None, depth: int = 2) -> dict:
-    """The CLI's unpaired run (align.rs:1822-2250, the --device gpu path) over
-    a scorer: every batch of `in_path` mapped on the device (map_reads_scored
-    with min_score / max_ties / both strands), its records built and written
-    to `out_path` in input order (or coordinate order).  Returns counts.
-
-    Three stages run on their own threads, as the CLI's reader, GPU feeder
-    and workers do (align.rs:2078-2250): reading batch k + 1, mapping batch k
-    on the device, building and writing the records of batch k - 1; at most
-    `depth` batches wait between the stages.  `stats`, if given, receives the
-    seconds each stage spent (read, map, encode, write; they overlap, so they
-    add up to more than the wall time)."""
-    ref_lens = [len(r) for r in ref_letters]
+def _run(reader, batches, map_batch, encode_batch, out_path, ref_names, ref_lens,
+         sort_coordinate, threads, stats, depth):
+    """Read, map and encode/write on three threads (the CLI's reader, GPU
+    feeder and workers, align.rs:2078-2335): reading batch k + 1, mapping
+    batch k, building and writing the records of batch k - 1, at most
+    `depth` batches waiting between the stages."""
     out = {"reads": 0, "records": 0, "batches": 0}
     st = stats if stats is not None else {}
     for k in ("read", "map", "encode", "write"):
@@ -247,28 +297,24 @@ def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
 
     def mapped(batch):
         t0 = time.perf_counter()
-        m = scorer.map_reads(batch.reads(), min_score=min_score, max_ties=max_ties,
-                             both_strands=both_strands, ref_letters=ref_letters)
+        m = map_batch(batch)
         st["map"] += time.perf_counter() - t0
         return batch, m
 
-    with BamReader(in_path, threads) as rd, \
-            BamWriter(out_path, header_text(ref_names, ref_lens, sort_coordinate), ref_names,
-                      ref_lens, sort_coordinate, threads) as wr, \
+    with reader, BamWriter(out_path, header_text(ref_names, ref_lens, sort_coordinate),
+                           ref_names, ref_lens, sort_coordinate, threads) as wr, \
             ThreadPoolExecutor(1) as rpool, ThreadPoolExecutor(1) as mpool, \
             ThreadPoolExecutor(1) as opool:
-        it = rd.batches(batch_size, max_read_len)
-
         def read_next():
             t0 = time.perf_counter()
-            b = next(it, None)
+            b = next(batches, None)
             st["read"] += time.perf_counter() - t0
             return b
 
         def emit(seq, mfut):
             batch, m = mfut.result()
             t0 = time.perf_counter()
-            rec = encode(batch, m, ref_names, secondary, threads)
+            rec = encode_batch(batch, m)
             t1 = time.perf_counter()
             wr.push(seq, rec)
             st["encode"] += t1 - t0
@@ -300,3 +346,69 @@ def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
         t0 = time.perf_counter()
     st["write"] += time.perf_counter() - t0  # the writer's close: its last blocks (or the sort)
     return out
+
+
+def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
+              min_score: int = 0, max_ties: int | None = None, both_strands: bool = False,
+              secondary: bool = False, sort_coordinate: bool = False,
+              max_read_len: int = 1000, batch_size: int = 50_000, threads: int = 0,
+              stats: dict | None = None, depth: int = 2) -> dict:
+    """The CLI's unpaired run (align.rs:1822-2250, the --device gpu path) over
+    a scorer: every batch of `in_path` (BAM, FASTA or FASTQ) mapped on the
+    device (map_reads_scored with min_score / max_ties / both strands), its
+    records built and written to `out_path` in input order (or coordinate
+    order).  Returns counts.  Reading, mapping and encoding/writing overlap
+    on three threads; `stats`, if given, receives the seconds each stage
+    spent (read, map, encode, write; they overlap, so they add up to more
+    than the wall time)."""
+    rd = BamReader(in_path, threads)
+    return _run(rd, rd.batches(batch_size, max_read_len),
+                lambda b: scorer.map_reads(b.reads(), min_score=min_score, max_ties=max_ties,
+                                           both_strands=both_strands, ref_letters=ref_letters),
+                lambda b, m: encode(b, m, ref_names, secondary, threads),
+                out_path, ref_names, [len(r) for r in ref_letters], sort_coordinate, threads,
+                stats, depth)
+
+
+DEFAULT_ADAPTERS = "truseq"
+
+
+def align_pairs_bam(scorer, path1: str, path2: str | None, out_path: str, ref_names, ref_letters,
+                    min_score: int = 0, max_ties: int | None = None, max_insert: int = 500,
+                    both_strands: bool = False, secondary: bool = False,
+                    sort_coordinate: bool = False, max_read_len: int = 1000,
+                    adapters=DEFAULT_ADAPTERS, batch_size: int = 50_000, threads: int = 0,
+                    stats: dict | None = None, depth: int = 2) -> dict:
+    """The CLI's paired run (align.rs:1613-1750 over run, 1822-2250): pairs
+    from two mate files, or one interleaved / paired-BAM file (path2 None),
+    each mate trimmed of its 3' adapter (pair_adapters; `adapters` an
+    adapter.config() dict, the TruSeq default, or None for
+    --no-adapter-trim), the pairs mapped on the device (map_pairs_scored),
+    their records built (build_pair_records) and written in input or
+    coordinate order.  batch_size counts records, two per pair, as the
+    CLI's --batch-size does."""
+    from . import adapter as A
+    if adapters == DEFAULT_ADAPTERS:
+        adapters = A.config()
+    cfg = None if adapters is None else dict(adapters, max_read_len=int(max_read_len))
+    rd = PairReader(path1, path2, threads)
+    state = {}
+
+    def map_batch(b):
+        codes, off, lens = b.reads()
+        if cfg is not None:
+            ads, aligned = A.pair_adapters((codes, off, lens), cfg)
+        else:
+            ads = None
+            aligned = np.where((lens > max_read_len) if max_read_len else False, 0,
+                               lens).astype(np.uint32)
+        state[id(b)] = ads
+        return scorer.map_pairs((codes, off, aligned), min_score=min_score, max_ties=max_ties,
+                                max_insert=max_insert, both_strands=both_strands,
+                                ref_letters=ref_letters)
+
+    def encode_batch(b, m):
+        return encode_pairs(b, m, ref_names, state.pop(id(b)), secondary, threads)
+
+    return _run(rd, rd.batches((batch_size + 1) // 2), map_batch, encode_batch, out_path,
+                ref_names, [len(r) for r in ref_letters], sort_coordinate, threads, stats, depth)

@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -257,20 +258,36 @@ uint16_t reg2bin(int64_t beg, int64_t end) {
   return 0;
 }
 
-// A hit's SAM CIGAR words: soft clips around the aligned span.
-void sam_cigar(const esg_hit& h, const uint32_t* ops, uint32_t read_len, std::vector<uint32_t>& c) {
+// A hit's SAM CIGAR words: soft clips around the aligned span
+// (sam_cigar_ad / clipped_span, align.rs:1021-1051).  `ad`: 3' adapter bases
+// left out of the alignment, the start of a reverse hit's SEQ.
+void sam_cigar(const esg_hit& h, const uint32_t* ops, uint32_t read_len, std::vector<uint32_t>& c,
+               uint32_t ad = 0) {
   c.clear();
   const esg_alignment& a = h.alignment;
-  if (a.query_start > 0) c.push_back(a.query_start << 4 | 4u);
+  const uint32_t shift = h.reverse ? ad : 0;
+  const uint32_t qs = a.query_start + shift, qe = a.query_end + shift;
+  if (qs > 0) c.push_back(qs << 4 | 4u);
   for (uint32_t k = 0; k < a.n_ops; ++k) c.push_back(ops[a.ops_offset + k]);
-  if (read_len > a.query_end) c.push_back((read_len - a.query_end) << 4 | 4u);
+  if (read_len > qe) c.push_back((read_len - qe) << 4 | 4u);
 }
 
-// One record in the BAM layout.  seq4: 4-bit codes, one per byte.
+void cigar_text(const std::vector<uint32_t>& c, std::string& s) {
+  for (uint32_t w : c) {
+    s += std::to_string(w >> 4);
+    s += "MIDNSHP=X"[w & 0xfu];
+  }
+}
+
+// One record in the BAM layout.  seq4: 4-bit codes, one per byte.  The bin
+// is the one noodles' writer (the CLI's) gives: the region [pos, pos + span
+// - 1], so a record placed at a position with no CIGAR (an unmapped mate at
+// its partner's place) takes [pos, pos - 1]'s bin, and none at position 0.
 void encode_record(std::vector<uint8_t>& o, int32_t ref, int32_t pos, uint8_t mapq,
                    const std::vector<uint32_t>& cigar, uint16_t flag, const uint8_t* name,
                    uint32_t name_len, const uint8_t* seq4, uint32_t l_seq, const uint8_t* qual,
-                   bool have_qual, const std::vector<uint8_t>& aux) {
+                   bool have_qual, const std::vector<uint8_t>& aux, int32_t mate_ref = -1,
+                   int32_t mate_pos = -1, int32_t tlen = 0) {
   const size_t at = o.size();
   put32(o, 0);  // block_size, set below
   put32(o, (uint32_t)ref);
@@ -280,7 +297,8 @@ void encode_record(std::vector<uint8_t>& o, int32_t ref, int32_t pos, uint8_t ma
     const uint32_t op = w & 0xfu;
     if (op == 0 || op == 2 || op == 3 || op == 7 || op == 8) span += w >> 4;
   }
-  const uint16_t bin = pos < 0 ? 4680 : reg2bin(pos, (int64_t)pos + span);
+  const uint16_t bin =
+      (pos < 0 || (span == 0 && pos == 0)) ? 4680 : reg2bin(pos, (int64_t)pos + span);
   const uint8_t* nm = name_len > 1 ? name : (const uint8_t*)"*";
   const uint32_t nl = name_len > 1 ? name_len : 2;
   o.push_back((uint8_t)nl);
@@ -289,9 +307,9 @@ void encode_record(std::vector<uint8_t>& o, int32_t ref, int32_t pos, uint8_t ma
   put16(o, (uint16_t)cigar.size());
   put16(o, flag);
   put32(o, l_seq);
-  put32(o, 0xffffffffu);
-  put32(o, 0xffffffffu);
-  put32(o, 0);
+  put32(o, (uint32_t)mate_ref);
+  put32(o, (uint32_t)mate_pos);
+  put32(o, (uint32_t)tlen);
   o.insert(o.end(), nm, nm + nl - 1);
   o.push_back(0);
   for (uint32_t w : cigar) put32(o, w);
@@ -328,6 +346,9 @@ struct esg_bam_reader {
   uint64_t line_no = 0;
   std::string pending;       // a FASTA header met while ending the previous record
   bool has_pending = false;
+  // paired input: mate 2's file when the mates come in two files
+  bool paired = false;
+  esg_bam_reader* mate2 = nullptr;
 };
 
 struct esg_bam_batch {
@@ -536,6 +557,141 @@ static esg_status next_fastx(esg_bam_reader* r, std::vector<uint8_t>& bytes, boo
   return ESG_OK;
 }
 
+// The next primary input record, appended to `bytes` without its
+// block_size: a BAM's next record that is neither secondary nor
+// supplementary (one aligned to the reverse strand is refused), or the next
+// FASTX record.  false in *got at the end of the input.
+static esg_status next_record(esg_bam_reader* r, std::vector<uint8_t>& bytes, bool* got) {
+  *got = false;
+  if (r->format != 0) return next_fastx(r, bytes, got);
+  for (;;) {
+    bool ok = false;
+    esg_status st = need(r, 4, &ok);
+    if (st != ESG_OK) return st;
+    if (!ok) return ESG_OK;
+    const uint32_t bs = u32_at(r->buf.data() + r->pos);
+    if ((st = need(r, 4 + (size_t)bs, &ok)) != ESG_OK) return st;
+    if (!ok) return berr(ESG_ERR_BAD_ARGUMENT, "truncated BAM record");
+    const uint8_t* rec = r->buf.data() + r->pos + 4;
+    InRec x{};
+    if (!parse_rec(rec, bs, x)) return berr(ESG_ERR_BAD_ARGUMENT, "malformed BAM record");
+    r->pos += 4 + bs;
+    if (x.flag & (0x100 | 0x800)) {  // secondary, supplementary
+      ++r->skipped;
+      continue;
+    }
+    if (!(x.flag & 0x4) && (x.flag & 0x10))
+      return berr(ESG_ERR_BAD_ARGUMENT,
+                  "input record aligned to the reverse strand: unaligned reads (or forward-"
+                  "strand alignments, whose SEQ is the read as sequenced) are taken");
+    bytes.insert(bytes.end(), rec, rec + bs);
+    *got = true;
+    return ESG_OK;
+  }
+}
+
+// A record's name (without its NUL).
+static std::string rec_name(const std::vector<uint8_t>& rec) {
+  const uint32_t l = rec[8];
+  return l > 1 ? std::string((const char*)rec.data() + 32, l - 1) : std::string();
+}
+
+// mate_stem (align.rs:700-706): the name without a trailing /1 or /2.
+static std::string mate_stem(const std::string& n) {
+  if (n.size() >= 2 && n[n.size() - 2] == '/' && (n.back() == '1' || n.back() == '2'))
+    return n.substr(0, n.size() - 2);
+  return n;
+}
+
+// The record with its name replaced.
+static void rename_rec(std::vector<uint8_t>& rec, const std::string& name) {
+  const uint32_t l = rec[8];
+  std::vector<uint8_t> o(rec.begin(), rec.begin() + 32);
+  o[8] = (uint8_t)(name.size() + 1);
+  o.insert(o.end(), name.begin(), name.end());
+  o.push_back(0);
+  o.insert(o.end(), rec.begin() + 32 + l, rec.end());
+  rec.swap(o);
+}
+
+// PairSource::next_pair (align.rs:759-870): the next pair as mate 1, mate 2
+// records, both named by the pair's stem (process_pair_chunk,
+// align.rs:1631-1639); an orphan mate or a name mismatch is an error
+// naming the read.
+static esg_status next_pair(esg_bam_reader* r, std::vector<uint8_t>& a, std::vector<uint8_t>& b,
+                            bool* got) {
+  a.clear();
+  b.clear();
+  *got = false;
+  bool ga = false, gb = false;
+  esg_status st;
+  if ((st = next_record(r, a, &ga)) != ESG_OK) return st;
+  if (r->mate2) {  // two files, record k of each
+    if ((st = next_record(r->mate2, b, &gb)) != ESG_OK) return st;
+    if (!ga && !gb) return ESG_OK;
+    if (ga != gb)
+      return berr(ESG_ERR_BAD_ARGUMENT, "read " + rec_name(ga ? a : b) + " has no mate: " +
+                                            (ga ? "the mate 2 file" : "the mate 1 file") +
+                                            " ends before the other");
+    if (mate_stem(rec_name(a)) != mate_stem(rec_name(b)))
+      return berr(ESG_ERR_BAD_ARGUMENT, "mate names differ: " + rec_name(a) + " in the mate 1 "
+                                        "file but " + rec_name(b) + " in the mate 2 file");
+  } else {
+    if (!ga) return ESG_OK;
+    if (r->format == 0) {
+      const uint16_t fa = u16_at(a.data() + 14);
+      if (!(fa & 0x1) || !(fa & 0x40) == !(fa & 0x80))
+        return berr(ESG_ERR_BAD_ARGUMENT,
+                    "read " + rec_name(a) + ": not a mate (paired input needs 0x1 with exactly "
+                    "one of 0x40 / 0x80 on every record)");
+    }
+    if ((st = next_record(r, b, &gb)) != ESG_OK) return st;
+    if (!gb) return berr(ESG_ERR_BAD_ARGUMENT, "read " + rec_name(a) + " has no mate: the "
+                                                "input ends after it");
+    if (mate_stem(rec_name(a)) != mate_stem(rec_name(b)))
+      return berr(ESG_ERR_BAD_ARGUMENT, "read " + rec_name(a) + " has no mate: the next record "
+                                        "is " + rec_name(b) + " (mates must be adjacent)");
+    if (r->format == 0) {
+      const uint16_t fa = u16_at(a.data() + 14), fb = u16_at(b.data() + 14);
+      if (!(fb & 0x1) || !(fb & 0x40) == !(fb & 0x80) || !(fb & 0x40) == !(fa & 0x40))
+        return berr(ESG_ERR_BAD_ARGUMENT, "read " + mate_stem(rec_name(a)) +
+                                              ": the two records are not mate 1 and mate 2");
+      if (!(fa & 0x40)) a.swap(b);
+    }
+  }
+  const std::string stem = mate_stem(rec_name(a));
+  if (stem.size() + 1 != a[8] || memcmp(a.data() + 32, stem.data(), stem.size()) != 0)
+    rename_rec(a, stem);
+  if (stem.size() + 1 != b[8] || memcmp(b.data() + 32, stem.data(), stem.size()) != 0)
+    rename_rec(b, stem);
+  *got = true;
+  return ESG_OK;
+}
+
+// Index a batch's records (bytes complete) and take their reads as
+// alphabet codes; a read over max_read_len (0: no limit) gets length 0.
+static void finish_batch(esg_bam_batch* b, const std::vector<uint64_t>& rec_off,
+                         uint32_t max_read_len) {
+  uint64_t total = 0;
+  for (size_t k = 0; k < b->recs.size(); ++k) {
+    const uint64_t end = k + 1 < rec_off.size() ? rec_off[k + 1] : b->bytes.size();
+    InRec& x = b->recs[k];
+    parse_rec(b->bytes.data() + rec_off[k], (uint32_t)(end - rec_off[k]), x);
+    const bool over = max_read_len && x.l_seq > max_read_len;
+    b->full_len.push_back(x.l_seq);
+    b->len.push_back(over ? 0u : x.l_seq);
+    b->off.push_back(total);
+    total += b->len.back();
+  }
+  b->codes.resize(total);
+  for (size_t k = 0; k < b->recs.size(); ++k) {
+    const InRec& x = b->recs[k];
+    const uint8_t* s = x.rec + x.seq_off;
+    uint8_t* d = b->codes.data() + b->off[k];
+    for (uint32_t i = 0; i < b->len[k]; ++i) d[i] = kCode4[(s[i / 2] >> ((i & 1) ? 0 : 4)) & 0xf];
+  }
+}
+
 extern "C" {
 
 esg_status esg_bam_open(const char* path, uint32_t threads, esg_bam_reader** out) {
@@ -627,77 +783,45 @@ const char* esg_bam_header_text(const esg_bam_reader* r, uint64_t* len) {
 esg_status esg_bam_read_batch(esg_bam_reader* r, uint32_t max_reads, uint32_t max_read_len,
                               esg_bam_batch** out) {
   if (!r || !out || !max_reads) return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument or batch of 0");
+  if (r->paired) return berr(ESG_ERR_BAD_ARGUMENT, "a paired reader: use esg_bam_read_pair_batch");
   *out = nullptr;
-  auto* b = new esg_bam_batch();
+  std::unique_ptr<esg_bam_batch> b(new esg_bam_batch());
   std::vector<uint64_t> rec_off;
-  while (r->format != 0 && b->recs.size() < max_reads) {
+  while (b->recs.size() < max_reads) {
     const size_t at = b->bytes.size();
     bool got = false;
-    const esg_status st = next_fastx(r, b->bytes, &got);
-    if (st != ESG_OK) {
-      delete b;
-      return st;
-    }
+    const esg_status st = next_record(r, b->bytes, &got);
+    if (st != ESG_OK) return st;
     if (!got) break;
-    InRec x{};
-    parse_rec(b->bytes.data() + at, (uint32_t)(b->bytes.size() - at), x);
-    x.rec = nullptr;  // set once b->bytes stops growing
     rec_off.push_back(at);
-    b->recs.push_back(x);
+    b->recs.push_back(InRec{});
   }
-  while (r->format == 0 && b->recs.size() < max_reads) {
-    bool ok = false;
-    esg_status st = need(r, 4, &ok);
-    if (st != ESG_OK) {
-      delete b;
-      return st;
-    }
-    if (!ok) break;
-    const uint32_t bs = u32_at(r->buf.data() + r->pos);
-    if ((st = need(r, 4 + (size_t)bs, &ok)) != ESG_OK || !ok) {
-      delete b;
-      return st != ESG_OK ? st : berr(ESG_ERR_BAD_ARGUMENT, "truncated BAM record");
-    }
-    const uint8_t* rec = r->buf.data() + r->pos + 4;
-    InRec x{};
-    if (!parse_rec(rec, bs, x)) {
-      delete b;
-      return berr(ESG_ERR_BAD_ARGUMENT, "malformed BAM record");
-    }
-    r->pos += 4 + bs;
-    if (x.flag & (0x100 | 0x800)) {  // secondary, supplementary
-      ++r->skipped;
-      continue;
-    }
-    if (!(x.flag & 0x4) && (x.flag & 0x10)) {
-      delete b;
-      return berr(ESG_ERR_BAD_ARGUMENT,
-                  "input record aligned to the reverse strand: unaligned reads (or forward-"
-                  "strand alignments, whose SEQ is the read as sequenced) are taken");
-    }
+  finish_batch(b.get(), rec_off, max_read_len);
+  *out = b.release();
+  return ESG_OK;
+}
+
+esg_status esg_bam_read_pair_batch(esg_bam_reader* r, uint32_t max_pairs, esg_bam_batch** out) {
+  if (!r || !out || !max_pairs) return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument or batch of 0");
+  if (!r->paired) return berr(ESG_ERR_BAD_ARGUMENT, "not a paired reader (esg_bam_open_pairs)");
+  *out = nullptr;
+  std::unique_ptr<esg_bam_batch> b(new esg_bam_batch());
+  std::vector<uint64_t> rec_off;
+  std::vector<uint8_t> ra, rb;
+  while (b->recs.size() < 2 * (size_t)max_pairs) {
+    bool got = false;
+    const esg_status st = next_pair(r, ra, rb, &got);
+    if (st != ESG_OK) return st;
+    if (!got) break;
     rec_off.push_back(b->bytes.size());
-    b->bytes.insert(b->bytes.end(), rec, rec + bs);
-    b->recs.push_back(x);
+    b->bytes.insert(b->bytes.end(), ra.begin(), ra.end());
+    rec_off.push_back(b->bytes.size());
+    b->bytes.insert(b->bytes.end(), rb.begin(), rb.end());
+    b->recs.push_back(InRec{});
+    b->recs.push_back(InRec{});
   }
-  // the records now live in b->bytes; the reads' codes for the mapping stage
-  uint64_t total = 0;
-  for (size_t k = 0; k < b->recs.size(); ++k) {
-    InRec& x = b->recs[k];
-    x.rec = b->bytes.data() + rec_off[k];
-    const bool over = max_read_len && x.l_seq > max_read_len;
-    b->full_len.push_back(x.l_seq);
-    b->len.push_back(over ? 0u : x.l_seq);
-    b->off.push_back(total);
-    total += b->len.back();
-  }
-  b->codes.resize(total);
-  for (size_t k = 0; k < b->recs.size(); ++k) {
-    const InRec& x = b->recs[k];
-    const uint8_t* s = x.rec + x.seq_off;
-    uint8_t* d = b->codes.data() + b->off[k];
-    for (uint32_t i = 0; i < b->len[k]; ++i) d[i] = kCode4[(s[i / 2] >> ((i & 1) ? 0 : 4)) & 0xf];
-  }
-  *out = b;
+  finish_batch(b.get(), rec_off, 0);
+  *out = b.release();
   return ESG_OK;
 }
 
@@ -717,7 +841,31 @@ void esg_bam_close(esg_bam_reader* r) {
   if (!r) return;
   if (r->f) fclose(r->f);
   if (r->gz) gzclose(r->gz);
+  esg_bam_close(r->mate2);
   delete r;
+}
+
+esg_status esg_bam_open_pairs(const char* path1, const char* path2, uint32_t threads,
+                              esg_bam_reader** out) {
+  if (!path1 || !out) return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  esg_bam_reader* r = nullptr;
+  esg_status st = esg_bam_open(path1, threads, &r);
+  if (st != ESG_OK) return st;
+  r->paired = true;
+  if (path2) {
+    if ((st = esg_bam_open(path2, threads, &r->mate2)) != ESG_OK) {
+      esg_bam_close(r);
+      return st;
+    }
+    if (r->format == 0 || r->mate2->format == 0) {
+      esg_bam_close(r);
+      return berr(ESG_ERR_BAD_ARGUMENT, "mates in two files are FASTA / FASTQ; a paired BAM "
+                                        "holds both mates in one file");
+    }
+  }
+  *out = r;
+  return ESG_OK;
 }
 
 // ===================================================================== records
@@ -808,10 +956,7 @@ esg_status esg_bam_encode(const esg_bam_batch* b, const esg_mapping* m,
           xa += std::to_string(e.alignment.ref_start + 1);
           xa += ',';
           sam_cigar(e, ops, x.l_seq, cigar);
-          for (uint32_t w : cigar) {
-            xa += std::to_string(w >> 4);
-            xa += "MIDNSHP=X"[w & 0xfu];
-          }
+          cigar_text(cigar, xa);
           xa += ',';
           xa += std::to_string(e.nm);
           xa += ';';
@@ -830,8 +975,10 @@ esg_status esg_bam_encode(const esg_bam_batch* b, const esg_mapping* m,
           std::vector<std::pair<uint32_t, uint32_t>> all;
           split_aux(a, x.size - x.aux_off, all);
           for (const auto& fld : all)
-            if (a[fld.first] == 'R' && a[fld.first + 1] == 'G')
+            if (a[fld.first] == 'R' && a[fld.first + 1] == 'G') {
               rg.assign(a + fld.first, a + fld.first + fld.second);
+              break;
+            }
         }
         for (uint32_t h = 1; h < rm.n_hits; ++h) {
           const esg_hit& e = hits[rm.first_hit + h];
@@ -858,6 +1005,251 @@ esg_status esg_bam_encode(const esg_bam_batch* b, const esg_mapping* m,
     r->bytes.insert(r->bytes.end(), enc[k].begin(), enc[k].end());
     r->n_records += count[k];
     r->n_unmapped += unmapped[k];
+  }
+  *out = r;
+  return ESG_OK;
+}
+
+esg_status esg_bam_encode_pairs(const esg_bam_batch* b, const esg_mapping* m,
+                                const uint32_t* adapter_bases, const esg_bam_options* opt,
+                                const char* const* ref_names, uint32_t n_refs, uint32_t threads,
+                                esg_bam_records** out) {
+  if (!b || !m || !opt || !out || (n_refs && !ref_names))
+    return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  uint32_t n_pairs = 0, n_maps = 0;
+  uint64_t n_phits = 0, n_hits = 0, n_ops = 0, n_md = 0;
+  const esg_pair_mapping* pairs = esg_mapping_pairs(m, &n_pairs);
+  const esg_pair_hit* phits = esg_mapping_pair_hits(m, &n_phits);
+  const esg_read_mapping* maps = esg_mapping_reads(m, &n_maps);
+  const esg_hit* hits = esg_mapping_hits(m, &n_hits);
+  const uint32_t* ops = esg_mapping_ops(m, &n_ops);
+  const char* md = esg_mapping_md(m, &n_md);
+  const size_t n = b->recs.size();
+  if (n % 2 || (size_t)n_pairs * 2 != n || n_maps != n)
+    return berr(ESG_ERR_BAD_ARGUMENT, "the mapping is not of this batch's pairs");
+  // every hit's reference named
+  for (uint64_t h = 0; h < n_hits; ++h)
+    if (hits[h].reference >= n_refs)
+      return berr(ESG_ERR_BAD_ARGUMENT, "a hit's reference is past ref_names");
+  for (uint64_t h = 0; h < n_phits; ++h)
+    if (phits[h].mates[0].reference >= n_refs || phits[h].mates[1].reference >= n_refs)
+      return berr(ESG_ERR_BAD_ARGUMENT, "a hit's reference is past ref_names");
+  const size_t np = n / 2;
+  std::vector<std::vector<uint8_t>> enc(np);
+  std::vector<uint32_t> count(np, 0);
+  std::atomic<int> bad{0};
+  static const char kOwned[7][2] = {{'N', 'M'}, {'M', 'D'}, {'A', 'S'}, {'X', 'S'},
+                                    {'X', 'A'}, {'M', 'C'}, {'a', 'd'}};
+  parallel_for((np + 31) / 32, threads_or(threads), [&](size_t chunk) {
+    struct Place {
+      const esg_hit* primary = nullptr;
+      std::vector<const esg_hit*> others, partners;
+      int32_t score = 0;
+      bool has_xs = false;
+      int32_t xs = 0;
+      bool unique = false;
+    };
+    struct Mate {
+      uint16_t kept = 0, flag = 0;
+      int32_t ref = -1, pos = -1, mate_ref = -1, mate_pos = -1, tlen = 0;
+      uint8_t mapq = 0;
+      std::vector<uint32_t> cigar;
+      std::vector<uint8_t> seq4, qual, aux, rg;
+      bool have_qual = true;
+    };
+    std::vector<std::pair<uint32_t, uint32_t>> fields;
+    std::vector<uint32_t> cig;
+    for (size_t p = chunk * 32; p < std::min(np, chunk * 32 + 32); ++p) {
+      const esg_pair_mapping& pm = pairs[p];
+      const bool proper = pm.flags & ESG_PAIR_PROPER;
+      Place pl[2];
+      if (proper) {
+        const esg_pair_hit* ph = phits + pm.first_hit;
+        for (int k = 0; k < 2; ++k) {
+          pl[k].primary = &ph[0].mates[k];
+          for (uint32_t t = 1; t < pm.n_hits; ++t) {
+            pl[k].others.push_back(&ph[t].mates[k]);
+            pl[k].partners.push_back(&ph[t].mates[1 - k]);
+          }
+          pl[k].score = ph[0].mates[k].alignment.score;
+          pl[k].has_xs = pm.flags & (k == 0 ? ESG_PAIR_HAS_XS1 : ESG_PAIR_HAS_XS2);
+          pl[k].xs = pm.suboptimal[k];
+          pl[k].unique = pm.n_tied == 1;
+        }
+      } else {
+        for (int k = 0; k < 2; ++k) {
+          const esg_read_mapping& me = maps[2 * p + k];
+          const esg_read_mapping& other = maps[2 * p + 1 - k];
+          const esg_hit* partner = other.n_hits ? &hits[other.first_hit] : nullptr;
+          pl[k].primary = me.n_hits ? &hits[me.first_hit] : nullptr;
+          for (uint32_t t = 1; t < me.n_hits; ++t) {
+            pl[k].others.push_back(&hits[me.first_hit + t]);
+            pl[k].partners.push_back(partner);
+          }
+          pl[k].score = (me.flags & ESG_MAPPING_HAS_BEST) ? me.best_score : 0;
+          pl[k].has_xs = me.flags & ESG_MAPPING_HAS_SUBOPTIMAL;
+          pl[k].xs = me.suboptimal;
+          pl[k].unique = me.n_tied == 1;
+        }
+      }
+      Mate mt[2];
+      uint32_t full[2], ad[2];
+      for (int k = 0; k < 2; ++k) {
+        const InRec& x = b->recs[2 * p + k];
+        full[k] = x.l_seq;
+        ad[k] = adapter_bases ? adapter_bases[2 * p + k] : 0u;
+        const uint8_t* a = x.rec + x.aux_off;
+        if (!split_aux(a, x.size - x.aux_off, fields)) {
+          bad = 1;
+          return;
+        }
+        for (const auto& fl : fields)
+          if (a[fl.first] == 'R' && a[fl.first + 1] == 'G') {
+            mt[k].rg.assign(a + fl.first, a + fl.first + fl.second);
+            break;
+          }
+        for (const auto& t : kOwned)
+          for (size_t i = 0; i < fields.size(); ++i)
+            if (a[fields[i].first] == (uint8_t)t[0] && a[fields[i].first + 1] == (uint8_t)t[1]) {
+              fields[i] = fields.back();
+              fields.pop_back();
+              break;
+            }
+        Mate& q = mt[k];
+        for (const auto& fl : fields) q.aux.insert(q.aux.end(), a + fl.first, a + fl.first + fl.second);
+        q.kept = x.flag & (0x200 | 0x400);
+        q.flag = q.kept | 0x1 | (k == 0 ? 0x40 : 0x80);
+        const uint8_t* sq = x.rec + x.seq_off;
+        const uint8_t* ql = sq + (x.l_seq + 1) / 2;
+        q.have_qual = x.l_seq == 0 || ql[0] != 0xff;
+        q.seq4.resize(x.l_seq);
+        for (uint32_t i = 0; i < x.l_seq; ++i) q.seq4[i] = (sq[i / 2] >> ((i & 1) ? 0 : 4)) & 0xf;
+        q.qual.assign(ql, ql + x.l_seq);
+        const esg_hit* h = pl[k].primary;
+        if (!h) {
+          q.flag |= 0x4;
+        } else {
+          if (h->reverse) {
+            q.flag |= 0x10;
+            std::reverse(q.seq4.begin(), q.seq4.end());
+            for (auto& c : q.seq4) c = kComp4[c];
+            std::reverse(q.qual.begin(), q.qual.end());
+          }
+          q.ref = (int32_t)h->reference;
+          q.pos = (int32_t)h->alignment.ref_start;
+          q.mapq = pl[k].unique ? 60 : 0;
+          sam_cigar(*h, ops, full[k], q.cigar, ad[k]);
+          int_field(q.aux, "NM", h->nm);
+          str_field(q.aux, "MD", md + h->md_offset, h->md_len);
+          int_field(q.aux, "AS", pl[k].score);
+          if (pl[k].has_xs) int_field(q.aux, "XS", pl[k].xs);
+          if (!pl[k].others.empty()) {
+            std::string xa;
+            for (const esg_hit* e : pl[k].others) {
+              xa += ref_names[e->reference];
+              xa += e->reverse ? ",-" : ",+";
+              xa += std::to_string(e->alignment.ref_start + 1);
+              xa += ',';
+              sam_cigar(*e, ops, full[k], cig, ad[k]);
+              cigar_text(cig, xa);
+              xa += ',';
+              xa += std::to_string(e->nm);
+              xa += ';';
+            }
+            str_field(q.aux, "XA", xa.data(), xa.size());
+          }
+        }
+        if (adapter_bases) int_field(q.aux, "ad", ad[k]);
+      }
+      // template_length (align.rs:1225-1236)
+      auto tlen_of = [](const esg_hit& h, const esg_hit& o, bool first) {
+        const uint32_t e = std::max(h.alignment.ref_end, o.alignment.ref_end);
+        const uint32_t s0 = std::min(h.alignment.ref_start, o.alignment.ref_start);
+        const int64_t len = std::min<int64_t>((int64_t)e - s0, INT32_MAX);
+        const bool left = h.alignment.ref_start < o.alignment.ref_start ||
+                          (h.alignment.ref_start == o.alignment.ref_start && first);
+        return (int32_t)(left ? len : -len);
+      };
+      for (int k = 0; k < 2; ++k) {
+        Mate& q = mt[k];
+        const esg_hit* h = pl[k].primary;
+        const esg_hit* oh = pl[1 - k].primary;
+        if (h && oh) {
+          if (oh->reverse) q.flag |= 0x20;
+          if (proper) q.flag |= 0x2;
+          q.mate_ref = (int32_t)oh->reference;
+          q.mate_pos = (int32_t)oh->alignment.ref_start;
+          std::string mc;
+          sam_cigar(*oh, ops, full[1 - k], cig, ad[1 - k]);
+          cigar_text(cig, mc);
+          str_field(q.aux, "MC", mc.data(), mc.size());
+          if (h->reference == oh->reference) q.tlen = tlen_of(*h, *oh, k == 0);
+        } else if (h) {
+          q.flag |= 0x8;
+          q.mate_ref = (int32_t)h->reference;
+          q.mate_pos = (int32_t)h->alignment.ref_start;
+        } else if (oh) {
+          // an unmapped mate sits at its partner's place, as samtools writes it
+          if (oh->reverse) q.flag |= 0x20;
+          q.ref = q.mate_ref = (int32_t)oh->reference;
+          q.pos = q.mate_pos = (int32_t)oh->alignment.ref_start;
+        } else {
+          q.flag |= 0x8;
+        }
+      }
+      std::vector<uint8_t>& o = enc[p];
+      for (int k = 0; k < 2; ++k) {
+        const InRec& x = b->recs[2 * p + k];
+        const Mate& q = mt[k];
+        encode_record(o, q.ref, q.pos, q.mapq, q.cigar, q.flag, x.rec + 32, x.name_len,
+                      q.seq4.data(), x.l_seq, q.qual.data(), q.have_qual, q.aux, q.mate_ref,
+                      q.mate_pos, q.tlen);
+      }
+      count[p] = 2;
+      if (opt->secondary) {
+        const size_t nt = std::max(pl[0].others.size(), pl[1].others.size());
+        for (size_t t = 0; t < nt; ++t)
+          for (int k = 0; k < 2; ++k) {
+            if (t >= pl[k].others.size()) continue;
+            const esg_hit& h = *pl[k].others[t];
+            const esg_hit* ph = pl[k].partners[t];
+            uint16_t f = 0x100 | 0x1 | (k == 0 ? 0x40 : 0x80) | mt[k].kept;
+            if (h.reverse) f |= 0x10;
+            std::vector<uint8_t> d;
+            int_field(d, "NM", h.nm);
+            str_field(d, "MD", md + h.md_offset, h.md_len);
+            int_field(d, "AS", h.alignment.score);
+            d.insert(d.end(), mt[k].rg.begin(), mt[k].rg.end());
+            int32_t mref = (int32_t)h.reference, mpos = (int32_t)h.alignment.ref_start, tl = 0;
+            if (ph) {
+              if (ph->reverse) f |= 0x20;
+              mref = (int32_t)ph->reference;
+              mpos = (int32_t)ph->alignment.ref_start;
+              if (proper) {
+                f |= 0x2;
+                if (ph->reference == h.reference) tl = tlen_of(h, *ph, k == 0);
+              }
+            } else {
+              f |= 0x8;
+            }
+            sam_cigar(h, ops, full[k], cig, ad[k]);
+            const InRec& x = b->recs[2 * p + k];
+            encode_record(o, (int32_t)h.reference, (int32_t)h.alignment.ref_start, 0, cig, f,
+                          x.rec + 32, x.name_len, nullptr, 0, nullptr, true, d, mref, mpos, tl);
+            ++count[p];
+          }
+      }
+    }
+  });
+  if (bad) return berr(ESG_ERR_BAD_ARGUMENT, "malformed auxiliary data in an input record");
+  auto* r = new esg_bam_records();
+  size_t total = 0;
+  for (auto& e : enc) total += e.size();
+  r->bytes.reserve(total);
+  for (size_t p = 0; p < np; ++p) {
+    r->bytes.insert(r->bytes.end(), enc[p].begin(), enc[p].end());
+    r->n_records += count[p];
   }
   *out = r;
   return ESG_OK;

@@ -788,6 +788,27 @@ esg_status esg_mapping_from_arrays(const esg_read_mapping* reads, uint32_t n_rea
   return ESG_OK;
 }
 
+esg_status esg_mapping_set_pairs(esg_mapping* m, const esg_pair_mapping* pairs, uint32_t n_pairs,
+                                 const esg_pair_hit* pair_hits, uint64_t n_pair_hits) {
+  if (!m || (n_pairs && !pairs) || (n_pair_hits && !pair_hits))
+    return merr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  if (m->reads.size() != 2 * (size_t)n_pairs)
+    return merr(ESG_ERR_BAD_ARGUMENT, "a paired mapping holds two read entries per pair");
+  for (uint32_t p = 0; p < n_pairs; ++p)
+    if (pairs[p].first_hit > n_pair_hits || pairs[p].n_hits > n_pair_hits - pairs[p].first_hit)
+      return merr(ESG_ERR_BAD_ARGUMENT, "pair %u's hits run past the pair-hit array", p);
+  const uint64_t n_ops = m->ops.size(), n_md = m->md.size();
+  for (uint64_t h = 0; h < n_pair_hits; ++h)
+    for (const esg_hit& e : pair_hits[h].mates)
+      if (e.alignment.ops_offset > n_ops || e.alignment.n_ops > n_ops - e.alignment.ops_offset ||
+          e.md_offset > n_md || e.md_len > n_md - e.md_offset)
+        return merr(ESG_ERR_BAD_ARGUMENT, "pair hit %llu's ops or MD run past their arrays",
+                    (unsigned long long)h);
+  m->pairs.assign(pairs, pairs + n_pairs);
+  m->pair_hits.assign(pair_hits, pair_hits + n_pair_hits);
+  return ESG_OK;
+}
+
 const esg_read_mapping* esg_mapping_reads(const esg_mapping* m, uint32_t* n) {
   if (n) *n = m ? (uint32_t)m->reads.size() : 0u;
   return m ? m->reads.data() : nullptr;

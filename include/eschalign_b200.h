@@ -514,6 +514,12 @@ esg_status esg_mapping_from_arrays(const esg_read_mapping* reads, uint32_t n_rea
                                    const esg_hit* hits, uint64_t n_hits, const uint32_t* ops,
                                    uint64_t n_ops, const char* md, uint64_t n_md,
                                    esg_mapping** out);
+/* Give a mapping made by esg_mapping_from_arrays the paired arrays of
+ * esg_map_pairs' output (two read entries per pair; offsets checked), for
+ * esg_bam_encode_pairs. */
+esg_status esg_mapping_set_pairs(esg_mapping* mapping, const esg_pair_mapping* pairs,
+                                 uint32_t n_pairs, const esg_pair_hit* pair_hits,
+                                 uint64_t n_pair_hits);
 
 /* ---- serving: a request queue over resident scorers.  No counterpart in
  * the reference, which scores batches of one stream of reads and has no
@@ -611,6 +617,20 @@ typedef struct esg_bam_options {
  * missing).  An uncompressed BAM is refused, as the CLI refuses it. */
 esg_status esg_bam_open(const char* path, uint32_t threads, esg_bam_reader** out);
 const char* esg_bam_header_text(const esg_bam_reader* reader, uint64_t* len);
+/* Open the CLI's paired input (PairSource, align.rs:674-870): mate 1 and
+ * mate 2 FASTA / FASTQ files (path2 given; record k of each is a pair), or
+ * one file holding both mates (path2 NULL): an interleaved FASTA / FASTQ or
+ * a BAM whose mates are adjacent records flagged 0x1 with one of 0x40 /
+ * 0x80.  Mates share the pair's name, a trailing /1 or /2 dropped. */
+esg_status esg_bam_open_pairs(const char* path1, const char* path2, uint32_t threads,
+                              esg_bam_reader** out);
+/* The next pairs of a paired reader, at most max_pairs: records 2p (mate 1)
+ * and 2p + 1 (mate 2), their reads at full length in esg_bam_batch_reads
+ * (esg_pair_adapters trims them, and leaves mates over --max-read-len out).
+ * An orphan mate, mates whose names differ or a BAM record that is not a
+ * mate is ESG_ERR_BAD_ARGUMENT naming the read.  0 pairs: the end. */
+esg_status esg_bam_read_pair_batch(esg_bam_reader* reader, uint32_t max_pairs,
+                                   esg_bam_batch** out);
 /* The next primary records, at most max_reads (secondary and supplementary
  * ones skipped; a record aligned to the reverse strand is refused with
  * ESG_ERR_BAD_ARGUMENT, as is a malformed FASTA / FASTQ record).  A batch of
@@ -631,6 +651,18 @@ void esg_bam_close(esg_bam_reader* reader);
 esg_status esg_bam_encode(const esg_bam_batch* batch, const esg_mapping* mapping,
                           const esg_bam_options* options, const char* const* ref_names,
                           uint32_t n_refs, uint32_t threads, esg_bam_records** out);
+/* The records of a batch of pairs from esg_map_pairs over its trimmed
+ * mates (build_pair_records, align.rs:1238-1425, with process_pair_chunk's
+ * placements, 1683-1713): mate 1, mate 2, then with `secondary` a pair of
+ * 0x100 records per further tie-set member.  Flags 0x1 / 0x2 / 0x8 / 0x20 /
+ * 0x40 / 0x80, mate reference and position, TLEN, MC, and each mate's
+ * adapter bases soft-clipped at its 3' end and counted in `ad`
+ * (adapter_bases[2n] from esg_pair_adapters; NULL under --no-adapter-trim:
+ * no `ad` tag). */
+esg_status esg_bam_encode_pairs(const esg_bam_batch* batch, const esg_mapping* mapping,
+                                const uint32_t* adapter_bases, const esg_bam_options* options,
+                                const char* const* ref_names, uint32_t n_refs, uint32_t threads,
+                                esg_bam_records** out);
 const uint8_t* esg_bam_records_bytes(const esg_bam_records* records, uint64_t* n_bytes,
                                      uint32_t* n_records);
 void esg_bam_records_free(esg_bam_records* records);

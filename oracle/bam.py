@@ -305,7 +305,7 @@ def build_records(rec, m, ref_names, secondary=False):
     out = [encode_record(p["reference"], p["ref_start"], 60 if m["n_tied"] == 1 else 0,
                          sam_cigar(p), flag, rec["name"], seq, qual, fields)]
     if secondary:
-        rg = [f for t, f in rec["aux"] if t == b"RG"]
+        rg = [f for t, f in rec["aux"] if t == b"RG"][:1]  # the first, as Data::get finds it
         for h in hits[1:]:
             d = [int_field(b"NM", h["nm"]), str_field(b"MD", h["md"]),
                  int_field(b"AS", m["best_score"])] + rg
