@@ -439,6 +439,73 @@ def bam_stage(g, refs, reads, batch_size=50_000):
                        "input order; map on one thread overlapped with read/encode/write"}
 
 
+def fastq_files(path1, path2, pairs, seed=12):
+    """Mates 2p and 2p + 1 of `pairs` as two FASTQ files (names p0000000..,
+    Phred qualities 2-40), the CLI's usual paired input.  Built with array
+    operations."""
+    rng = np.random.default_rng(seed)
+    letters = np.frombuffer(b"ACGTN", np.uint8)
+    for m, path in ((0, path1), (1, path2)):
+        idx = np.arange(m, len(pairs), 2)
+        lens = pairs.lens[idx].astype(np.int64)
+        offs = pairs.off[idx].astype(np.int64)
+        n = idx.size
+        size = 10 + lens + 3 + lens + 1         # @name\n seq \n+\n qual \n
+        start = np.zeros(n + 1, np.int64)
+        np.cumsum(size, out=start[1:])
+        buf = np.full(int(start[-1]), ord("\n"), np.uint8)
+        k = np.arange(n)
+        head = np.zeros((n, 9), np.uint8)
+        head[:, 0] = ord("@")
+        head[:, 1] = ord("p")
+        for d in range(7):
+            head[:, 8 - d] = ord("0") + (k // 10 ** d) % 10
+        buf[(start[:-1, None] + np.arange(9)).ravel()] = head.ravel()
+        total = int(lens.sum())
+        src = np.repeat(offs, lens) + (np.arange(total) - np.repeat(np.cumsum(lens) - lens, lens))
+        seq_at = start[:-1] + 10
+        rel = np.arange(total) - np.repeat(np.cumsum(lens) - lens, lens)
+        buf[np.repeat(seq_at, lens) + rel] = letters[np.minimum(pairs.codes[src], 4)]
+        plus_at = seq_at + lens
+        buf[plus_at + 1] = ord("+")
+        buf[np.repeat(plus_at + 3, lens) + rel] = rng.integers(35, 74, total, dtype=np.uint8)
+        with open(path, "wb") as fh:
+            fh.write(memoryview(buf))
+
+
+def bam_pairs_stage(g, refs, pairs, n=500_000, batch_size=50_000):
+    """The CLI's paired run through the library (bam.align_pairs_bam): the
+    first n pairs as two FASTQ files, each mate trimmed of its adapter,
+    mapped on the device (map_pairs_scored: every tie traced, MD / NM from
+    the panel's letters), its records built and written as BGZF; wall time,
+    input order, default batch size 50 000 records."""
+    from eschalign_b200 import bam as EB
+    names = [f"ref{k}" for k in range(len(refs))]
+    letters = [bytes(b"ACGTN"[int(c)] for c in r) for r in refs]
+    sub = pairs.slice(0, 2 * min(n, len(pairs) // 2))
+    with tempfile.TemporaryDirectory() as tmp:
+        p1, p2 = os.path.join(tmp, "r1.fq"), os.path.join(tmp, "r2.fq")
+        w1, w2 = os.path.join(tmp, "w1.fq"), os.path.join(tmp, "w2.fq")
+        dst = os.path.join(tmp, "out.bam")
+        fastq_files(p1, p2, sub)
+        fastq_files(w1, w2, sub.slice(0, 2000))
+        EB.align_pairs_bam(g, w1, w2, dst, names, letters, min_score=40, batch_size=1000)
+        st = {}
+        t0 = time.perf_counter()
+        r = EB.align_pairs_bam(g, p1, p2, dst, names, letters, min_score=40,
+                               batch_size=batch_size, stats=st)
+        dt = time.perf_counter() - t0
+        out_bytes = os.path.getsize(dst)
+        in_bytes = os.path.getsize(p1) + os.path.getsize(p2)
+    return {"pairs": r["reads"] // 2, "records": r["records"], "seconds": round(dt, 3),
+            "pairs_per_s": r["reads"] / 2 / dt, "batch_records": batch_size,
+            "input_fastq_bytes": in_bytes, "output_bgzf_bytes": out_bytes,
+            "stage_seconds": {k: round(v, 3) for k, v in st.items()},
+            "options": "semi-global, --min-score 40, max insert 500, forward template strand, "
+                       "TruSeq adapters trimmed, every tie traced, MD/NM from letters, "
+                       "input order"}
+
+
 def map_pairs_stage(g, refs, pairs, scoring, local, skip_cpu, n=100_000):
     """The whole paired mapping stage: adapters trimmed by the library
     (esg_pair_adapters), then esg_map_pairs (pair.rs:157-390: the device
@@ -950,10 +1017,11 @@ def run_c4(a, ctx, rank):
     peak = int_peak(local_rank)
     roofline = roofline_of(peak, cells * a.steps / t, "semiglobal", None)
     batch.free()
-    map_pairs = None
+    map_pairs = bam_pairs = None
     if not a.no_extras:
         map_pairs = map_pairs_stage(g, refs, pairs, C4_SCORING, False,
                                     a.no_cpu_baseline or rank != 0 or world != 1)
+        bam_pairs = bam_pairs_stage(g, refs, pairs)
     step_pairs = a.pair_chunk
     chunks = [pairs.slice(2 * k, 2 * (k + step_pairs)) for k in range(0, n_pairs, step_pairs)]
     te, n_pass, h2d, d2h = feeder(
@@ -989,6 +1057,8 @@ def run_c4(a, ctx, rank):
             line["cpu_baseline"] = cpu
         if map_pairs:
             line["map_pairs"] = map_pairs
+        if bam_pairs:
+            line["bam_pairs"] = bam_pairs
         print(json.dumps(line), flush=True)
 
 

@@ -61,3 +61,40 @@ def test_align_bam_fastq_gz_input(oracle, tmp_path, label):
                          secondary=o["secondary"], sort_coordinate=o["sort"], batch_size=11)
     assert n["reads"] == len(recs) and n["records"] == len(want)
     assert record_stream(dst) == b"".join(want)
+
+
+PAIR_CASES = [{}, {"secondary": True, "both": True}, {"max_insert": 120},
+              {"trim": False, "local": True}, {"sort": True, "secondary": True}]
+
+
+@pytest.mark.parametrize("extra", PAIR_CASES, ids=[str(c) for c in PAIR_CASES])
+def test_align_pairs_bam_equals_the_oracle(oracle, tmp_path, extra):
+    """The CLI's paired run on the CUDA path (align_pairs_bam: the mate
+    files read, trimmed by esg_pair_adapters, mapped by esg_map_pairs,
+    encoded and written) holds the records of the oracle's restatement,
+    which pins what align_paired.rs asserts; batches of 3 pairs."""
+    from oracle import bam as B
+    from tests.test_bam_pairs import fastq_texts, fixture, opts, run_oracle
+    extra = dict(extra)
+    sort = extra.pop("sort", False)
+    o = opts(**extra)
+    refs, _ = fixture()
+    names = [r["name"] for r in refs]
+    letters = [r["seq"].encode() for r in refs]
+    r1, r2 = fastq_texts()
+    p1, p2, dst = str(tmp_path / "r1.fq"), str(tmp_path / "r2.fq"), str(tmp_path / "o.bam")
+    open(p1, "wb").write(r1)
+    open(p2, "wb").write(r2)
+    want = run_oracle(oracle, o, r1, r2)
+    if sort:
+        want = B.coordinate_order(want)
+    mode = Mode.LOCAL if o["local"] else Mode.SEMIGLOBAL
+    with GpuScorer([encode(r) for r in letters], Scoring(*o["scoring"]), mode) as g:
+        n = EB.align_pairs_bam(g, p1, p2, dst, names, letters, min_score=o["min_score"],
+                               max_ties=o["max_ties"], max_insert=o["max_insert"],
+                               both_strands=o["both"], secondary=o["secondary"],
+                               sort_coordinate=sort,
+                               adapters=EB.DEFAULT_ADAPTERS if o["trim"] else None,
+                               batch_size=6)
+    assert n["reads"] == 18 and n["records"] == len(want)
+    assert record_stream(dst) == b"".join(want)
