@@ -249,6 +249,8 @@ SIGNATURES = {
     "esg_bam_open_pairs": (C.c_int32, [C.c_char_p, C.c_char_p, C.c_uint32,
                                        C.POINTER(C.c_void_p)]),
     "esg_bam_read_pair_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "esg_bam_set_read_ids": (C.c_int32, [C.c_void_p, C.c_char_p]),
+    "esg_bam_reader_counts": (C.c_int32, [C.c_void_p, _u64p, _u64p]),
     "esg_bam_batch_reads": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                         C.POINTER(C.c_void_p), _u32p]),
     "esg_bam_batch_free": (None, [C.c_void_p]),

@@ -73,14 +73,30 @@ class BamBatch:
 class BamReader:
     """esg_bam_open: a BGZF BAM's header and its primary records in batches."""
 
-    def __init__(self, path: str, threads: int = 0):
+    def __init__(self, path: str, threads: int = 0, read_ids: str | None = None):
         self._lib = _lib()
         h = C.c_void_p()
         _check(self._lib, self._lib.esg_bam_open(path.encode(), threads, C.byref(h)))
         self._h = h
+        self._after_open(read_ids)
+
+    def _after_open(self, read_ids):
+        if read_ids is not None:
+            st = self._lib.esg_bam_set_read_ids(self._h, read_ids.encode())
+            if st:
+                err = self._lib.esg_last_error().decode(errors="replace")
+                self.close()
+                raise GpuError(st, err)
         n = C.c_uint64()
-        p = self._lib.esg_bam_header_text(h, C.byref(n))
+        p = self._lib.esg_bam_header_text(self._h, C.byref(n))
         self.header_text = C.string_at(p, n.value) if n.value else b""
+
+    def counts(self) -> dict:
+        """Secondary / supplementary input records skipped, and reads left
+        out by read_ids (two per pair)."""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(self._lib, self._lib.esg_bam_reader_counts(self._h, C.byref(a), C.byref(b)))
+        return {"not_primary": a.value, "filtered": b.value}
 
     def batches(self, max_reads: int = 50_000, max_read_len: int = 1000):
         while True:
@@ -116,16 +132,15 @@ class PairReader(BamReader):
     interleaved FASTX / paired BAM file (path2 None), in batches of pairs
     (records 2p and 2p + 1)."""
 
-    def __init__(self, path1: str, path2: str | None = None, threads: int = 0):
+    def __init__(self, path1: str, path2: str | None = None, threads: int = 0,
+                 read_ids: str | None = None):
         self._lib = _lib()
         h = C.c_void_p()
         _check(self._lib, self._lib.esg_bam_open_pairs(path1.encode(),
                                                        path2.encode() if path2 else None,
                                                        threads, C.byref(h)))
         self._h = h
-        n = C.c_uint64()
-        p = self._lib.esg_bam_header_text(h, C.byref(n))
-        self.header_text = C.string_at(p, n.value) if n.value else b""
+        self._after_open(read_ids)
 
     def batches(self, max_pairs: int = 25_000, max_read_len: int = 0):
         while True:
@@ -352,7 +367,7 @@ def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
               min_score: int = 0, max_ties: int | None = None, both_strands: bool = False,
               secondary: bool = False, sort_coordinate: bool = False,
               max_read_len: int = 1000, batch_size: int = 50_000, threads: int = 0,
-              stats: dict | None = None, depth: int = 2) -> dict:
+              stats: dict | None = None, depth: int = 2, read_ids: str | None = None) -> dict:
     """The CLI's unpaired run (align.rs:1822-2250, the --device gpu path) over
     a scorer: every batch of `in_path` (BAM, FASTA or FASTQ) mapped on the
     device (map_reads_scored with min_score / max_ties / both strands), its
@@ -360,8 +375,8 @@ def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
     order).  Returns counts.  Reading, mapping and encoding/writing overlap
     on three threads; `stats`, if given, receives the seconds each stage
     spent (read, map, encode, write; they overlap, so they add up to more
-    than the wall time)."""
-    rd = BamReader(in_path, threads)
+    than the wall time).  read_ids: --read-ids, a file of the names kept."""
+    rd = BamReader(in_path, threads, read_ids)
     return _run(rd, rd.batches(batch_size, max_read_len),
                 lambda b: scorer.map_reads(b.reads(), min_score=min_score, max_ties=max_ties,
                                            both_strands=both_strands, ref_letters=ref_letters),
@@ -378,7 +393,8 @@ def align_pairs_bam(scorer, path1: str, path2: str | None, out_path: str, ref_na
                     both_strands: bool = False, secondary: bool = False,
                     sort_coordinate: bool = False, max_read_len: int = 1000,
                     adapters=DEFAULT_ADAPTERS, batch_size: int = 50_000, threads: int = 0,
-                    stats: dict | None = None, depth: int = 2) -> dict:
+                    stats: dict | None = None, depth: int = 2,
+                    read_ids: str | None = None) -> dict:
     """The CLI's paired run (align.rs:1613-1750 over run, 1822-2250): pairs
     from two mate files, or one interleaved / paired-BAM file (path2 None),
     each mate trimmed of its 3' adapter (pair_adapters; `adapters` an
@@ -386,12 +402,12 @@ def align_pairs_bam(scorer, path1: str, path2: str | None, out_path: str, ref_na
     --no-adapter-trim), the pairs mapped on the device (map_pairs_scored),
     their records built (build_pair_records) and written in input or
     coordinate order.  batch_size counts records, two per pair, as the
-    CLI's --batch-size does."""
+    CLI's --batch-size does; read_ids (--read-ids) selects pairs by name."""
     from . import adapter as A
     if adapters == DEFAULT_ADAPTERS:
         adapters = A.config()
     cfg = None if adapters is None else dict(adapters, max_read_len=int(max_read_len))
-    rd = PairReader(path1, path2, threads)
+    rd = PairReader(path1, path2, threads, read_ids)
     state = {}
 
     def map_batch(b):

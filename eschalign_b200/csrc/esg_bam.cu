@@ -35,6 +35,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <unordered_set>
 #include <vector>
 
 extern "C" void esg_internal_set_error(esg_status st, const char* msg);
@@ -349,6 +350,10 @@ struct esg_bam_reader {
   // paired input: mate 2's file when the mates come in two files
   bool paired = false;
   esg_bam_reader* mate2 = nullptr;
+  // --read-ids: the canonical names kept (empty set: no filter)
+  std::unordered_set<std::string> wanted;
+  bool filter = false;
+  uint64_t filtered = 0;
 };
 
 struct esg_bam_batch {
@@ -668,6 +673,52 @@ static esg_status next_pair(esg_bam_reader* r, std::vector<uint8_t>& a, std::vec
   return ESG_OK;
 }
 
+// canonical_read_name (align.rs:572-583): a name that parses as a UUID --
+// the forms the uuid crate's parse_str takes (32 hex digits, 8-4-4-4-12,
+// {8-4-4-4-12}, urn:uuid:8-4-4-4-12; uuid_util.rs:10-30) -- as its dashed
+// lower-case string, any other name as it is.
+static std::string canonical_read_name(const std::string& n) {
+  auto hex = [](char c) { return isxdigit((unsigned char)c) != 0; };
+  auto hyphenated = [&](const std::string& t, std::string& h) {
+    if (t.size() != 36) return false;
+    for (size_t i = 0; i < 36; ++i) {
+      if (i == 8 || i == 13 || i == 18 || i == 23) {
+        if (t[i] != '-') return false;
+      } else if (!hex(t[i])) {
+        return false;
+      } else {
+        h.push_back(t[i]);
+      }
+    }
+    return true;
+  };
+  std::string h;
+  bool ok = false;
+  if (n.size() == 32 && std::all_of(n.begin(), n.end(), hex)) {
+    h = n;
+    ok = true;
+  } else if (n.size() == 36) {
+    ok = hyphenated(n, h);
+  } else if (n.size() == 38 && n.front() == '{' && n.back() == '}') {
+    ok = hyphenated(n.substr(1, 36), h);
+  } else if (n.size() == 45 && n.compare(0, 9, "urn:uuid:") == 0) {
+    ok = hyphenated(n.substr(9), h);
+  }
+  if (!ok) return n;
+  for (char& c : h) c = (char)tolower((unsigned char)c);
+  return h.substr(0, 8) + "-" + h.substr(8, 4) + "-" + h.substr(12, 4) + "-" + h.substr(16, 4) +
+         "-" + h.substr(20, 12);
+}
+
+// Whether --read-ids keeps a read of this name ("*" in a BAM: no name, not
+// kept), counting the reads it drops.
+static bool kept(esg_bam_reader* r, const std::string& name, bool bam, uint64_t n) {
+  if (!r->filter) return true;
+  if (!(bam && name == "*") && r->wanted.count(canonical_read_name(name))) return true;
+  r->filtered += n;
+  return false;
+}
+
 // Index a batch's records (bytes complete) and take their reads as
 // alphabet codes; a read over max_read_len (0: no limit) gets length 0.
 static void finish_batch(esg_bam_batch* b, const std::vector<uint64_t>& rec_off,
@@ -793,6 +844,14 @@ esg_status esg_bam_read_batch(esg_bam_reader* r, uint32_t max_reads, uint32_t ma
     const esg_status st = next_record(r, b->bytes, &got);
     if (st != ESG_OK) return st;
     if (!got) break;
+    if (r->filter) {
+      const uint32_t l = b->bytes[at + 8];
+      const std::string name(l > 1 ? (const char*)b->bytes.data() + at + 32 : "", l > 1 ? l - 1 : 0);
+      if (!kept(r, name, r->format == 0, 1)) {
+        b->bytes.resize(at);
+        continue;
+      }
+    }
     rec_off.push_back(at);
     b->recs.push_back(InRec{});
   }
@@ -813,6 +872,7 @@ esg_status esg_bam_read_pair_batch(esg_bam_reader* r, uint32_t max_pairs, esg_ba
     const esg_status st = next_pair(r, ra, rb, &got);
     if (st != ESG_OK) return st;
     if (!got) break;
+    if (!kept(r, rec_name(ra), false, 2)) continue;
     rec_off.push_back(b->bytes.size());
     b->bytes.insert(b->bytes.end(), ra.begin(), ra.end());
     rec_off.push_back(b->bytes.size());
@@ -843,6 +903,45 @@ void esg_bam_close(esg_bam_reader* r) {
   if (r->gz) gzclose(r->gz);
   esg_bam_close(r->mate2);
   delete r;
+}
+
+esg_status esg_bam_set_read_ids(esg_bam_reader* r, const char* path) {
+  if (!r || !path) return berr(ESG_ERR_BAD_ARGUMENT, "NULL argument");
+  // load_read_ids (align.rs:585-601): a name per line, its first word; blank
+  // lines and lines starting '#' skipped
+  gzFile g = gzopen(path, "rb");
+  if (!g) return berr(ESG_ERR_BAD_ARGUMENT, std::string("cannot open ") + path);
+  std::string text;
+  std::vector<char> chunk(1 << 16);
+  for (int n; (n = gzread(g, chunk.data(), (unsigned)chunk.size())) > 0;) text.append(chunk.data(), n);
+  gzclose(g);
+  std::unordered_set<std::string> ids;
+  size_t at = 0;
+  while (at <= text.size()) {
+    size_t e = text.find('\n', at);
+    if (e == std::string::npos) e = text.size();
+    size_t a = at, z = e;
+    while (a < z && ascii_ws((uint8_t)text[a])) ++a;
+    while (z > a && ascii_ws((uint8_t)text[z - 1])) --z;
+    if (z > a && text[a] != '#') {
+      size_t w = a;
+      while (w < z && !ascii_ws((uint8_t)text[w])) ++w;
+      ids.insert(canonical_read_name(text.substr(a, w - a)));
+    }
+    at = e + 1;
+  }
+  if (ids.empty()) return berr(ESG_ERR_BAD_ARGUMENT, std::string("no read names in ") + path);
+  r->wanted.swap(ids);
+  r->filter = true;
+  return ESG_OK;
+}
+
+esg_status esg_bam_reader_counts(const esg_bam_reader* r, uint64_t* not_primary,
+                                 uint64_t* filtered) {
+  if (!r) return berr(ESG_ERR_BAD_ARGUMENT, "NULL reader");
+  if (not_primary) *not_primary = r->skipped + (r->mate2 ? r->mate2->skipped : 0);
+  if (filtered) *filtered = r->filtered;
+  return ESG_OK;
 }
 
 esg_status esg_bam_open_pairs(const char* path1, const char* path2, uint32_t threads,

@@ -631,6 +631,17 @@ esg_status esg_bam_open_pairs(const char* path1, const char* path2, uint32_t thr
  * mate is ESG_ERR_BAD_ARGUMENT naming the read.  0 pairs: the end. */
 esg_status esg_bam_read_pair_batch(esg_bam_reader* reader, uint32_t max_pairs,
                                    esg_bam_batch** out);
+/* --read-ids (load_read_ids, canonical_read_name: align.rs:572-601): keep
+ * only the reads (or pairs, by the pair's name) named in the file at
+ * `path`, one name per line (its first word; blank lines and lines starting
+ * '#' skipped).  A name that is a UUID -- dashed, 32 hex digits, braced or
+ * urn:uuid: -- matches any spelling of it.  A file with no name is
+ * ESG_ERR_BAD_ARGUMENT. */
+esg_status esg_bam_set_read_ids(esg_bam_reader* reader, const char* path);
+/* What the reader dropped so far: secondary / supplementary input records,
+ * and reads not in --read-ids (two per pair). */
+esg_status esg_bam_reader_counts(const esg_bam_reader* reader, uint64_t* not_primary,
+                                 uint64_t* filtered);
 /* The next primary records, at most max_reads (secondary and supplementary
  * ones skipped; a record aligned to the reverse strand is refused with
  * ESG_ERR_BAD_ARGUMENT, as is a malformed FASTA / FASTQ record).  A batch of

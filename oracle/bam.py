@@ -321,6 +321,43 @@ FLAG_MATE_REVERSE, FLAG_FIRST, FLAG_LAST = 0x20, 0x40, 0x80
 PAIR_OWNED_TAGS = OWNED_TAGS + (b"MC", b"ad")  # align.rs:1203-1206, 1262
 
 
+def canonical_read_name(name: bytes) -> bytes:
+    """canonical_read_name (align.rs:572-583) with parse_uuid_flexible
+    (uuid_util.rs:10-30): a UUID name, in any spelling the uuid crate parses
+    (32 hex digits, dashed, braced, urn:uuid:), as its dashed lower-case
+    form; any other name as it is."""
+    import re
+    s = name.decode("latin-1")
+    m = (re.fullmatch(r"[0-9a-fA-F]{32}", s)
+         or re.fullmatch(r"(?:\{|urn:uuid:)?([0-9a-fA-F]{8})-([0-9a-fA-F]{4})-([0-9a-fA-F]{4})-"
+                         r"([0-9a-fA-F]{4})-([0-9a-fA-F]{12})\}?", s))
+    if not m or (s.startswith("{") != s.endswith("}")) or (s.startswith("urn:") and
+                                                         s.endswith("}")):
+        return name
+    h = "".join(m.groups()) if m.groups() else s
+    h = h.lower()
+    return f"{h[:8]}-{h[8:12]}-{h[12:16]}-{h[16:20]}-{h[20:]}".encode()
+
+
+def load_read_ids(text: bytes):
+    """load_read_ids (align.rs:585-601): the canonical names of an ID list."""
+    ids = set()
+    for line in text.split(b"\n"):
+        line = line.strip(_ASCII_WS)
+        if line and not line.startswith(b"#"):
+            ids.add(canonical_read_name(line.split()[0]))
+    if not ids:
+        raise ValueError("no read names")
+    return ids
+
+
+def select_reads(recs, wanted):
+    """read_batches' --read-ids filter (align.rs:611-621): a record without
+    a name ('*') is not kept."""
+    return [r for r in recs
+            if r["name"] != b"*" and canonical_read_name(r["name"]) in wanted]
+
+
 def mate_stem(name: bytes) -> bytes:
     """mate_stem (align.rs:700-706): the name without a trailing /1 or /2."""
     return name[:-2] if len(name) >= 2 and name[-2:] in (b"/1", b"/2") else name
@@ -332,7 +369,16 @@ def _renamed(rec, name):
     return r
 
 
-def read_pairs(data1: bytes, data2: bytes | None = None):
+def read_pairs(data1: bytes, data2: bytes | None = None, wanted=None):
+    """read_pair_batches (align.rs:875-905): the pairs of _read_pairs, with
+    --read-ids (`wanted`, canonical names) selecting by the pair's name."""
+    pairs = _read_pairs(data1, data2)
+    if wanted is None:
+        return pairs
+    return [(a, b) for a, b in pairs if canonical_read_name(a["name"]) in wanted]
+
+
+def _read_pairs(data1: bytes, data2: bytes | None = None):
     """PairSource::next_pair (align.rs:759-870): [(mate 1, mate 2)] of two
     FASTA / FASTQ files, one interleaved FASTX file, or a paired BAM (mates
     adjacent, 0x1 with one of 0x40 / 0x80), each mate named by the pair's
