@@ -414,7 +414,8 @@ def bam_stage(g, refs, reads, batch_size=50_000):
     """The CLI's unpaired run through the library (bam.align_bam): an
     unaligned BAM of the workload's reads read, mapped on the device (every
     tie traced, MD / NM from the panel's letters), its records built and
-    written as BGZF; wall time, input order, default batch size 50 000."""
+    written as BGZF; wall time, input order, default batch size 50 000;
+    `g` one scorer or several (one mapping thread each)."""
     from eschalign_b200 import bam as EB
     names = [f"ref{k}" for k in range(len(refs))]
     letters = [bytes(b"ACGTN"[int(c)] for c in r) for r in refs]
@@ -435,8 +436,10 @@ def bam_stage(g, refs, reads, batch_size=50_000):
             "reads_per_s": n["reads"] / dt, "batch_reads": batch_size,
             "input_bgzf_bytes": in_bytes, "input_raw_bytes": raw, "output_bgzf_bytes": out_bytes,
             "stage_seconds": {k: round(v, 3) for k, v in st.items()},
+            "scorers": len(g) if isinstance(g, (list, tuple)) else 1,
             "options": "both strands, min_score 0, every tie traced, MD/NM from letters, "
-                       "input order; map on one thread overlapped with read/encode/write"}
+                       "input order; read, map (one thread per scorer) and encode/write "
+                       "overlapped"}
 
 
 def fastq_files(path1, path2, pairs, seed=12):
@@ -498,6 +501,7 @@ def bam_pairs_stage(g, refs, pairs, n=500_000, batch_size=50_000):
         out_bytes = os.path.getsize(dst)
         in_bytes = os.path.getsize(p1) + os.path.getsize(p2)
     return {"pairs": r["reads"] // 2, "records": r["records"], "seconds": round(dt, 3),
+            "scorers": len(g) if isinstance(g, (list, tuple)) else 1,
             "pairs_per_s": r["reads"] / 2 / dt, "batch_records": batch_size,
             "input_fastq_bytes": in_bytes, "output_bgzf_bytes": out_bytes,
             "stage_seconds": {k: round(v, 3) for k, v in st.items()},
@@ -880,7 +884,12 @@ def run_c2(a, ctx, rank):
                                               a.no_cpu_baseline or rank != 0 or world != 1)
         extras["map"] = map_stage(g, refs, reads, scoring, mode == "local",
                                   a.no_cpu_baseline or rank != 0 or world != 1)
-        extras["bam"] = bam_stage(g, refs, reads)
+        # a second scorer over the same panel: one maps while the other's
+        # host share of the mapping runs
+        g2 = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank)
+        g2.set_split(info["split_len"])
+        extras["bam"] = bam_stage([g, g2], refs, reads)
+        g2.close()
         arms = reference_gpu_arms(refs, sub, scoring, mode == "local", local_rank)
         if arms:
             arms["batched_over_ref_half2"] = value / arms["half2_gcups"]
@@ -1021,7 +1030,10 @@ def run_c4(a, ctx, rank):
     if not a.no_extras:
         map_pairs = map_pairs_stage(g, refs, pairs, C4_SCORING, False,
                                     a.no_cpu_baseline or rank != 0 or world != 1)
-        bam_pairs = bam_pairs_stage(g, refs, pairs)
+        g2 = GpuScorer(refs, Scoring(*C4_SCORING), Mode.SEMIGLOBAL, device=local_rank)
+        g2.set_split(g.info()["split_len"])
+        bam_pairs = bam_pairs_stage([g, g2], refs, pairs)
+        g2.close()
     step_pairs = a.pair_chunk
     chunks = [pairs.slice(2 * k, 2 * (k + step_pairs)) for k in range(0, n_pairs, step_pairs)]
     te, n_pass, h2d, d2h = feeder(

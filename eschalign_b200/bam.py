@@ -13,6 +13,8 @@ The records are the reference CLI's byte for byte.
 from __future__ import annotations
 
 import ctypes as C
+import queue
+import threading
 import time
 from collections import deque
 from concurrent.futures import ThreadPoolExecutor
@@ -299,26 +301,43 @@ def header_text(ref_names, ref_lens, sort_coordinate: bool = False) -> bytes:
     return ("\n".join(lines) + "\n").encode()
 
 
-def _run(reader, batches, map_batch, encode_batch, out_path, ref_names, ref_lens,
+def _scorers(scorer):
+    """One scorer, or several over the same panel and scoring."""
+    return list(scorer) if isinstance(scorer, (list, tuple)) else [scorer]
+
+
+def _run(reader, batches, scorers, map_batch, encode_batch, out_path, ref_names, ref_lens,
          sort_coordinate, threads, stats, depth):
-    """Read, map and encode/write on three threads (the CLI's reader, GPU
+    """Read, map and encode/write on their own threads (the CLI's reader, GPU
     feeder and workers, align.rs:2078-2335): reading batch k + 1, mapping
     batch k, building and writing the records of batch k - 1, at most
-    `depth` batches waiting between the stages."""
+    `depth` batches waiting between the stages.  With several scorers, one
+    mapping thread per scorer: one thread's host share of the mapping
+    (packing, tie lists, MD / NM, assembly) overlaps another's scoring on
+    the device."""
     out = {"reads": 0, "records": 0, "batches": 0}
     st = stats if stats is not None else {}
     for k in ("read", "map", "encode", "write"):
         st.setdefault(k, 0.0)
+    free = queue.SimpleQueue()
+    for sc in scorers:
+        free.put(sc)
+    lock = threading.Lock()
 
     def mapped(batch):
         t0 = time.perf_counter()
-        m = map_batch(batch)
-        st["map"] += time.perf_counter() - t0
+        sc = free.get()
+        try:
+            m = map_batch(sc, batch)
+        finally:
+            free.put(sc)
+        with lock:
+            st["map"] += time.perf_counter() - t0
         return batch, m
 
     with reader, BamWriter(out_path, header_text(ref_names, ref_lens, sort_coordinate),
                            ref_names, ref_lens, sort_coordinate, threads) as wr, \
-            ThreadPoolExecutor(1) as rpool, ThreadPoolExecutor(1) as mpool, \
+            ThreadPoolExecutor(1) as rpool, ThreadPoolExecutor(len(scorers)) as mpool, \
             ThreadPoolExecutor(1) as opool:
         def read_next():
             t0 = time.perf_counter()
@@ -350,7 +369,7 @@ def _run(reader, batches, map_batch, encode_batch, out_path, ref_names, ref_lens
                 nxt = rpool.submit(read_next)
                 inflight.append(opool.submit(emit, seq, mpool.submit(mapped, batch)))
                 seq += 1
-                while len(inflight) > max(depth, 1):
+                while len(inflight) > max(depth, len(scorers)):
                     inflight.popleft().result()
             while inflight:
                 inflight.popleft().result()
@@ -375,10 +394,13 @@ def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
     order).  Returns counts.  Reading, mapping and encoding/writing overlap
     on three threads; `stats`, if given, receives the seconds each stage
     spent (read, map, encode, write; they overlap, so they add up to more
-    than the wall time).  read_ids: --read-ids, a file of the names kept."""
+    than the wall time).  read_ids: --read-ids, a file of the names kept.
+    `scorer` may be a list of scorers over the same panel and scoring: each
+    maps on its own thread, so the device scores one batch while the host
+    finishes another (the records do not depend on it)."""
     rd = BamReader(in_path, threads, read_ids)
-    return _run(rd, rd.batches(batch_size, max_read_len),
-                lambda b: scorer.map_reads(b.reads(), min_score=min_score, max_ties=max_ties,
+    return _run(rd, rd.batches(batch_size, max_read_len), _scorers(scorer),
+                lambda sc, b: sc.map_reads(b.reads(), min_score=min_score, max_ties=max_ties,
                                            both_strands=both_strands, ref_letters=ref_letters),
                 lambda b, m: encode(b, m, ref_names, secondary, threads),
                 out_path, ref_names, [len(r) for r in ref_letters], sort_coordinate, threads,
@@ -402,7 +424,8 @@ def align_pairs_bam(scorer, path1: str, path2: str | None, out_path: str, ref_na
     --no-adapter-trim), the pairs mapped on the device (map_pairs_scored),
     their records built (build_pair_records) and written in input or
     coordinate order.  batch_size counts records, two per pair, as the
-    CLI's --batch-size does; read_ids (--read-ids) selects pairs by name."""
+    CLI's --batch-size does; read_ids (--read-ids) selects pairs by name.
+    `scorer` may be a list of scorers, as for align_bam."""
     from . import adapter as A
     if adapters == DEFAULT_ADAPTERS:
         adapters = A.config()
@@ -410,7 +433,7 @@ def align_pairs_bam(scorer, path1: str, path2: str | None, out_path: str, ref_na
     rd = PairReader(path1, path2, threads, read_ids)
     state = {}
 
-    def map_batch(b):
+    def map_batch(sc, b):
         codes, off, lens = b.reads()
         if cfg is not None:
             ads, aligned = A.pair_adapters((codes, off, lens), cfg)
@@ -419,12 +442,13 @@ def align_pairs_bam(scorer, path1: str, path2: str | None, out_path: str, ref_na
             aligned = np.where((lens > max_read_len) if max_read_len else False, 0,
                                lens).astype(np.uint32)
         state[id(b)] = ads
-        return scorer.map_pairs((codes, off, aligned), min_score=min_score, max_ties=max_ties,
+        return sc.map_pairs((codes, off, aligned), min_score=min_score, max_ties=max_ties,
                                 max_insert=max_insert, both_strands=both_strands,
                                 ref_letters=ref_letters)
 
     def encode_batch(b, m):
         return encode_pairs(b, m, ref_names, state.pop(id(b)), secondary, threads)
 
-    return _run(rd, rd.batches((batch_size + 1) // 2), map_batch, encode_batch, out_path,
+    return _run(rd, rd.batches((batch_size + 1) // 2), _scorers(scorer), map_batch,
+                encode_batch, out_path,
                 ref_names, [len(r) for r in ref_letters], sort_coordinate, threads, stats, depth)

@@ -212,22 +212,25 @@ class OracleScorer:
         return mappings_from_oracle(ms)
 
 
+@pytest.mark.parametrize("n_scorers", [1, 2])
 @pytest.mark.parametrize("label", sorted(golden_digests()))
-def test_align_bam_pipeline_writes_the_reference_record_stream(oracle, tmp_path, label):
+def test_align_bam_pipeline_writes_the_reference_record_stream(oracle, tmp_path, label,
+                                                               n_scorers):
     """align_bam's overlapped read / map / encode / write, in batches of 13,
     with the oracle's mappings: the golden stream, input order kept."""
     from oracle import bam as B
     want = golden_digests()[label]
     o = flag_set(label)
     names, refs = trna_panel()
-    sc = OracleScorer(oracle, refs, o["scoring"], o["local"])
+    scs = [OracleScorer(oracle, refs, o["scoring"], o["local"]) for _ in range(n_scorers)]
     path = str(tmp_path / "out.bam")
     st = {}
-    n = EB.align_bam(sc, FIXTURE, path, names, refs, min_score=o["min_score"],
+    n = EB.align_bam(scs if n_scorers > 1 else scs[0], FIXTURE, path, names, refs,
+                     min_score=o["min_score"],
                      max_ties=o["max_ties"], both_strands=o["both"], secondary=o["secondary"],
                      sort_coordinate=o["sort"], max_read_len=o["max_read_len"], batch_size=13,
                      threads=3, stats=st)
-    assert n["batches"] == sc.calls == 5 and n["reads"] == 60
+    assert n["batches"] == sum(sc.calls for sc in scs) == 5 and n["reads"] == 60
     assert n["records"] == want["records"]
     assert format(B.fnv1a64(record_stream(path)), "016x") == want["fnv1a64"]
     assert set(st) == {"read", "map", "encode", "write"}
