@@ -103,6 +103,11 @@ def args_parse():
     ap.add_argument("--profile-case", type=int, default=0, metavar="READS",
                     help="score READS reads of the workload once per kernel and exit "
                          "(a small target for ncu)")
+    ap.add_argument("--bam-case", type=int, default=0, metavar="READS",
+                    help="run the unpaired BAM stage alone on READS reads of the workload, "
+                         "print its figures and exit (a target for ncu)")
+    ap.add_argument("--bam-scorers", type=int, default=2,
+                    help="--bam-case: scorers mapping at once, one thread each")
     ap.add_argument("--mode", default="local", choices=["local", "semiglobal"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--pairs", type=int, default=2_000_000, help="c4: read pairs")
@@ -795,6 +800,16 @@ def run_c2(a, ctx, rank):
     world, local_rank = ctx.world, ctx.local_rank
     refs = synth.panel_tiles()
     panel_bases = sum(len(r) for r in refs)
+    if a.bam_case:
+        reads = synth.reads_c2(refs, n=a.bam_case)
+        gs = [GpuScorer(refs, Scoring(*HEADLINE[0]), Mode.parse(a.mode), device=local_rank)
+              for _ in range(max(1, a.bam_scorers))]
+        for g in gs:
+            g.set_split(a.split if a.split >= 0 else 512)
+        print(json.dumps({"bam_case": a.bam_case, **bam_stage(gs, refs, reads)}), flush=True)
+        for g in gs:
+            g.close()
+        return
     if a.profile_case:
         reads = synth.reads_c2(refs, n=a.profile_case)
         for kernel in (KERNEL_AUTO, KERNEL_INT32, KERNEL_PLAIN32):
