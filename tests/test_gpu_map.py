@@ -286,3 +286,29 @@ def test_map_mid_sized_call_equals_small_ones():
         assert (whole.hits[f] == np.concatenate([p.hits[f] for p in parts])).all(), f
     assert (whole.ops == np.concatenate([p.ops for p in parts])).all()
     assert whole.md_bytes == b"".join(p.md_bytes for p in parts)
+
+
+def test_map_two_scorers_on_two_threads():
+    """align_bam's several mapping threads: two scorers over one panel, each
+    mapping on its own thread at once, give what one thread gives, call for
+    call."""
+    from concurrent.futures import ThreadPoolExecutor
+    refs = synth.panel_tiles()
+    data = synth.reads_c2(refs, n=20_000, seed=0x5EED_0909)
+    letters = [code_letters(r) for r in refs]
+    chunks = [data.slice(k, k + 1000) for k in range(0, 20_000, 1000)]
+    gs = [GpuScorer(refs, Scoring(*SCHEME), Mode.LOCAL) for _ in range(2)]
+    try:
+        want = [gs[0].map_reads(c.tuple(), both_strands=True, ref_letters=letters)
+                for c in chunks]
+        for _ in range(2):
+            with ThreadPoolExecutor(2) as ex:
+                got = list(ex.map(lambda k: gs[k % 2].map_reads(
+                    chunks[k].tuple(), both_strands=True, ref_letters=letters),
+                    range(len(chunks))))
+            for g, w in zip(got, want):
+                assert np.array_equal(g.reads, w.reads) and np.array_equal(g.hits, w.hits)
+                assert np.array_equal(g.ops, w.ops) and g.md_bytes == w.md_bytes
+    finally:
+        for g in gs:
+            g.close()
