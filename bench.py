@@ -722,11 +722,12 @@ class Ctx:
         return total
 
 
-def feeder(ctx, chunks, prepare, submit, finish, steps):
-    """prepare / submit / finish over host chunks, like the GPU feeder thread
-    of crates/eschalign-cli/src/align.rs:2801-2917, with two batches in
-    flight: chunk k + 1 is prepared and queued before chunk k is waited for,
-    so the device never drains between chunks.  Returns (seconds of the
+def feeder(ctx, run, steps):
+    """The end-to-end passes through the library's GPU feeder
+    (GpuScorer.score_batches / score_pair_batches, the CLI's score_batches,
+    crates/eschalign-cli/src/align.rs:2801-2917): run(timing) yields each
+    chunk's result, chunk k + 1 prepared and queued before chunk k is waited
+    for, so the device never drains between chunks.  Returns (seconds of the
     timed passes, passes, h2d bytes, d2h bytes per pass); the host time split
     is left in feeder.last_split.  The first pass warms the pinned pool and
     the allocator and is not timed."""
@@ -736,29 +737,11 @@ def feeder(ctx, chunks, prepare, submit, finish, steps):
     for it in range(steps + 1):
         ctx.barrier()
         t0 = pc()
-        inflight = []
         h2d = d2h = 0
-        split = {"prepare_s": 0.0, "submit_s": 0.0, "finish_s": 0.0}
-
-        def done(b):
-            nonlocal h2d, d2h
-            a = pc()
-            st = finish(b)
-            split["finish_s"] += pc() - a
-            h2d += st["h2d_bytes"]
-            d2h += st["d2h_bytes"]
-
-        for c in chunks:
-            a = pc()
-            prepared = prepare(c)
-            b = pc()
-            inflight.append(submit(prepared))
-            split["prepare_s"] += b - a
-            split["submit_s"] += pc() - b
-            if len(inflight) > 1:
-                done(inflight.pop(0))
-        while inflight:
-            done(inflight.pop(0))
+        split = {}
+        for res in run(split):
+            h2d += res.stats["h2d_bytes"]
+            d2h += res.stats["d2h_bytes"]
         ctx.torch.cuda.synchronize()
         dt = pc() - t0
         if it > 0:
@@ -914,8 +897,8 @@ def run_c2(a, ctx, rank):
 
     chunks = [reads.slice(k, k + a.chunk) for k in range(0, len(reads), a.chunk)]
     te, n_pass, h2d, d2h = feeder(
-        ctx, chunks, lambda c: g.prepare(c.tuple(), both_strands=True), g.submit,
-        lambda b: g.finish(b).stats, max(1, a.steps))
+        ctx, lambda tm: g.score_batches((c.tuple() for c in chunks), both_strands=True,
+                                        timing=tm), max(1, a.steps))
     e2e = {"value": job_cells * n_pass / te / 1e9, "unit": "GCUPS",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "reads_per_s": job_reads * n_pass / te, "chunk_reads": a.chunk,
@@ -979,8 +962,8 @@ def run_c1(a, ctx, rank):
     peak = int_peak(local_rank)
     roofline = roofline_of(peak, cells * a.steps / t, "local", None)
     batch.free()
-    te, n_pass, h2d, d2h = feeder(ctx, [reads], lambda c: g.prepare(c.tuple()), g.submit,
-                                  lambda b: g.finish(b).stats, max(3, a.steps))
+    te, n_pass, h2d, d2h = feeder(ctx, lambda tm: g.score_batches([reads.tuple()], timing=tm),
+                                  max(3, a.steps))
     e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "reads_per_s": world * len(reads) * n_pass / te}
@@ -1052,8 +1035,9 @@ def run_c4(a, ctx, rank):
     step_pairs = a.pair_chunk
     chunks = [pairs.slice(2 * k, 2 * (k + step_pairs)) for k in range(0, n_pairs, step_pairs)]
     te, n_pass, h2d, d2h = feeder(
-        ctx, chunks, lambda c: g.prepare_pairs(c.tuple(), adapters=cfg, both_strands=True),
-        g.submit, lambda b: g.finish_pairs(b).stats, max(1, min(2, a.steps)))
+        ctx, lambda tm: g.score_pair_batches((c.tuple() for c in chunks), adapters=cfg,
+                                             both_strands=True, timing=tm),
+        max(1, min(2, a.steps)))
     e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "pairs_per_s": world * n_pairs * n_pass / te, "chunk_pairs": step_pairs,
@@ -1112,8 +1096,7 @@ def run_c3(a, ctx, rank):
     roofline = roofline_of(peak, cells * a.steps / t, "local", None)
     batch.free()
     te, n_pass, h2d, d2h = feeder(
-        ctx, [reads], lambda c: g.prepare(c.tuple(), both_strands=True), g.submit,
-        lambda b: g.finish(b).stats, 1)
+        ctx, lambda tm: g.score_batches([reads.tuple()], both_strands=True, timing=tm), 1)
     e2e = {"value": world * cells * n_pass / te / 1e9, "unit": "GCUPS",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
     g.close()

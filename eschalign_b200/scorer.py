@@ -18,6 +18,7 @@ asked for.  Every read is scored on the GPU -- there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import time
 from dataclasses import dataclass
 
 import numpy as np
@@ -505,6 +506,60 @@ class GpuScorer:
     def score_batch(self, reads, both_strands: bool = False, full_rows: bool = False) -> BatchResult:
         """cuda/mod.rs:524-528."""
         return self.finish(self.submit(self.prepare(reads, both_strands, full_rows)))
+
+    def score_batches(self, batches, both_strands: bool = False, full_rows: bool = False,
+                      timing: dict | None = None):
+        """The CLI's GPU feeder (score_batches, align.rs:2801-2917) over this
+        scorer: every item of `batches` (reads as `prepare` takes them) is
+        prepared and queued while the one before it runs on the device, so
+        the device does not drain between batches; yields each batch's
+        result, in order.  `timing`, if given, accumulates the host seconds
+        spent preparing, submitting and waiting to finish."""
+        return self._feed(batches, lambda r: self.prepare(r, both_strands, full_rows),
+                          self.finish, timing)
+
+    def score_pair_batches(self, batches, adapters=None, min_score: int = 0,
+                           both_strands: bool = True, full_rows: bool = False,
+                           timing: dict | None = None):
+        """score_batches for read pairs (the feeder's paired branch,
+        align.rs:2844-2872): each item's mates trimmed and scored as
+        `prepare_pairs` does; yields each batch's PairBatchResult."""
+        return self._feed(batches,
+                          lambda r: self.prepare_pairs(r, adapters, min_score, both_strands,
+                                                       full_rows),
+                          self.finish_pairs, timing)
+
+    def _feed(self, batches, prepare, finish, timing):
+        t = timing if timing is not None else {}
+        for k in ("prepare_s", "submit_s", "finish_s"):
+            t.setdefault(k, 0.0)
+        pc = time.perf_counter
+        in_flight = None
+        try:
+            for reads in batches:
+                a = pc()
+                nxt = prepare(reads)
+                b = pc()
+                self.submit(nxt)
+                t["prepare_s"] += b - a
+                t["submit_s"] += pc() - b
+                if in_flight is not None:
+                    done, in_flight = in_flight, nxt
+                    a = pc()
+                    res = finish(done)
+                    t["finish_s"] += pc() - a
+                    yield res
+                else:
+                    in_flight = nxt
+            if in_flight is not None:
+                done, in_flight = in_flight, None
+                a = pc()
+                res = finish(done)
+                t["finish_s"] += pc() - a
+                yield res
+        finally:
+            if in_flight is not None:  # abandoned: wait for it, drop it
+                finish(in_flight)
 
     # -- traceback of winners (scalar.rs:182-364)
     def align(self, reads, jobs) -> "Alignments":

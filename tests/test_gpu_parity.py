@@ -477,3 +477,26 @@ def test_gpu_autotune_lane_type_follows_its_measurements(oracle):
     want, want_t, _ = oracle.scalar_map_batch(reads, panel, scoring, True, True, cap=CAP)
     for f in ("best", "suboptimal", "n_tied"):
         assert (res.results[f] == want[f]).all(), f
+
+
+def test_gpu_feeder_equals_single_batches():
+    """GpuScorer.score_batches (the CLI's GPU feeder, two batches in flight)
+    gives each chunk what score_batch gives it alone, in order; and the
+    paired feeder what prepare_pairs / finish_pairs give."""
+    from eschalign_b200 import adapter
+    refs = synth.panel_tiles()
+    reads = synth.reads_c2(refs, n=12_000, seed=0x5EED_0911)
+    chunks = [reads.slice(k, k + 2500) for k in range(0, 12_000, 2500)]
+    with GpuScorer(refs, Scoring(), Mode.LOCAL) as g:
+        got = list(g.score_batches((c.tuple() for c in chunks), both_strands=True))
+        for c, r in zip(chunks, got):
+            w = g.score_batch(c.tuple(), both_strands=True)
+            assert np.array_equal(r.results, w.results) and np.array_equal(r.ties, w.ties)
+    pairs, _ = synth.pairs_c4(refs, n=6000)
+    pch = [pairs.slice(2 * k, 2 * (k + 1500)) for k in range(0, 6000, 1500)]
+    cfg = adapter.config()
+    with GpuScorer(refs, Scoring(), Mode.SEMIGLOBAL) as g:
+        got = list(g.score_pair_batches((c.tuple() for c in pch), adapters=cfg))
+        for c, r in zip(pch, got):
+            w = g.finish_pairs(g.submit(g.prepare_pairs(c.tuple(), adapters=cfg)))
+            assert np.array_equal(r.pairs, w.pairs) and np.array_equal(r.pair_ties, w.pair_ties)
