@@ -13,7 +13,8 @@
  * matches everything), exactly what GpuScorer::score_batch takes
  * (cuda/mod.rs:524).  Plain pointers and sizes only; the library owns all
  * device memory; a scorer is used by one thread at a time, like GpuScorer
- * (`&mut self`, cuda/mod.rs:326-327).
+ * (`&mut self`, cuda/mod.rs:326-327), while different scorers, each on its
+ * own stream, may be used from different threads at once.
  */
 #ifndef ESCHALIGN_B200_H
 #define ESCHALIGN_B200_H
