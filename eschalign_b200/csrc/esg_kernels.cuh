@@ -255,8 +255,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_
   return false;
 }
 
-// Stage the panel blob into shared memory with TMA bulk copies (no
-// multicast): one thread arms an mbarrier with the byte count and issues
+// Stage the panel blob into shared memory with TMA bulk copies, each CTA
+// its own: one thread arms an mbarrier with the byte count and issues
 // cp.async.bulk in chunks; every thread waits on the phase.
 __device__ __forceinline__ bool stage_panel(void* smem, const void* gsrc, uint32_t bytes,
                                             uint64_t* bar, uint32_t* err) {
