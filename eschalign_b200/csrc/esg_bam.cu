@@ -347,6 +347,7 @@ struct esg_bam_reader {
   uint64_t line_no = 0;
   std::string pending;       // a FASTA header met while ending the previous record
   bool has_pending = false;
+  std::string s_header, s_seq, s_qual, s_line;  // next_fastx's scratch
   // paired input: mate 2's file when the mates come in two files
   bool paired = false;
   esg_bam_reader* mate2 = nullptr;
@@ -477,7 +478,14 @@ static esg_status next_fastx(esg_bam_reader* r, std::vector<uint8_t>& bytes, boo
     return t;
   }();
   *got = false;
-  std::string header, seq, qual, line;
+  // the reader's scratch strings keep their capacity from record to record
+  std::string& header = r->s_header;
+  std::string& seq = r->s_seq;
+  std::string& qual = r->s_qual;
+  std::string& line = r->s_line;
+  header.clear();
+  seq.clear();
+  qual.clear();
   bool have = false;
   esg_status st;
   const bool fastq = r->format == 2;
@@ -550,13 +558,16 @@ static esg_status next_fastx(esg_bam_reader* r, std::vector<uint8_t>& bytes, boo
   put32(bytes, 0);
   bytes.insert(bytes.end(), name.begin(), name.end());
   bytes.push_back(0);
-  for (uint32_t k = 0; k < l; k += 2)
-    bytes.push_back((uint8_t)(to4[(uint8_t)seq[k]] << 4 |
-                              (k + 1 < l ? to4[(uint8_t)seq[k + 1]] : 0)));
+  const size_t at = bytes.size();
+  bytes.resize(at + (l + 1) / 2 + l);
+  uint8_t* d = bytes.data() + at;
+  const uint8_t* sq = (const uint8_t*)seq.data();
+  for (uint32_t k = 0; k < l; k += 2) *d++ = (uint8_t)(to4[sq[k]] << 4 | (k + 1 < l ? to4[sq[k + 1]] : 0));
   if (qual_given) {
-    for (char q : qual) bytes.push_back((uint8_t)q >= 33 ? (uint8_t)((uint8_t)q - 33) : 0);
+    const uint8_t* qq = (const uint8_t*)qual.data();
+    for (uint32_t k = 0; k < l; ++k) d[k] = qq[k] >= 33 ? (uint8_t)(qq[k] - 33) : 0;
   } else {
-    bytes.insert(bytes.end(), l, 0xff);
+    memset(d, 0xff, l);
   }
   *got = true;
   return ESG_OK;
