@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _native
 from .scorer import (HIT_DTYPE, MAPPING_DTYPE, PAIR_HIT_DTYPE, PAIR_MAPPING_DTYPE,
-                     GpuError, Mappings, _check, _ptr)
+                     GpuError, MappingHandle, Mappings, _check, _ptr)
 
 
 def _lib():
@@ -213,13 +213,18 @@ def mapping_handle(m: Mappings):
     return h
 
 
+def _handle_of(mapping):
+    """The esg_mapping pointer of a MappingHandle (or a raw handle as is)."""
+    return mapping._h if isinstance(mapping, MappingHandle) else mapping
+
+
 def encode(batch: BamBatch, mapping, ref_names, secondary: bool = False,
            threads: int = 0) -> BamRecords:
     """build_records (align.rs:1084-1200) for every read of `batch` from its
     mapping (a Mappings, or an esg_mapping handle)."""
     lib = _lib()
     own = isinstance(mapping, Mappings)
-    h = mapping_handle(mapping) if own else mapping
+    h = mapping_handle(mapping) if own else _handle_of(mapping)
     names, n = _names(ref_names)
     opts = _native.EsgBamOptions(int(bool(secondary)), 0)
     out = C.c_void_p()
@@ -240,7 +245,7 @@ def encode_pairs(batch: BamBatch, mapping, ref_names, adapter_bases=None,
     adapters were not searched."""
     lib = _lib()
     own = isinstance(mapping, Mappings)
-    h = mapping_handle(mapping) if own else mapping
+    h = mapping_handle(mapping) if own else _handle_of(mapping)
     names, n = _names(ref_names)
     opts = _native.EsgBamOptions(int(bool(secondary)), 0)
     ads = None if adapter_bases is None else np.ascontiguousarray(adapter_bases, dtype=np.uint32)
@@ -349,6 +354,8 @@ def _run(reader, batches, scorers, map_batch, encode_batch, out_path, ref_names,
             batch, m = mfut.result()
             t0 = time.perf_counter()
             rec = encode_batch(batch, m)
+            if isinstance(m, MappingHandle):
+                m.free()
             t1 = time.perf_counter()
             wr.push(seq, rec)
             st["encode"] += t1 - t0
@@ -401,7 +408,8 @@ def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
     rd = BamReader(in_path, threads, read_ids)
     return _run(rd, rd.batches(batch_size, max_read_len), _scorers(scorer),
                 lambda sc, b: sc.map_reads(b.reads(), min_score=min_score, max_ties=max_ties,
-                                           both_strands=both_strands, ref_letters=ref_letters),
+                                           both_strands=both_strands, ref_letters=ref_letters,
+                                           raw=True),
                 lambda b, m: encode(b, m, ref_names, secondary, threads),
                 out_path, ref_names, [len(r) for r in ref_letters], sort_coordinate, threads,
                 stats, depth)
@@ -443,8 +451,8 @@ def align_pairs_bam(scorer, path1: str, path2: str | None, out_path: str, ref_na
                                lens).astype(np.uint32)
         state[id(b)] = ads
         return sc.map_pairs((codes, off, aligned), min_score=min_score, max_ties=max_ties,
-                                max_insert=max_insert, both_strands=both_strands,
-                                ref_letters=ref_letters)
+                            max_insert=max_insert, both_strands=both_strands,
+                            ref_letters=ref_letters, raw=True)
 
     def encode_batch(b, m):
         return encode_pairs(b, m, ref_names, state.pop(id(b)), secondary, threads)

@@ -69,12 +69,15 @@ void md_nm(const uint8_t* q, uint32_t n, bool reverse, const uint8_t* r, const u
   md.clear();
   nm = 0;
   uint32_t run = 0, i = a.query_start, j = a.ref_start;
-  char num[16];
   auto letter = [&](uint32_t jj) { return rl ? upper(rl[jj]) : kLetter[r[jj] > 4 ? 4 : r[jj]]; };
-  auto flush = [&]() {
-    const int w = snprintf(num, sizeof num, "%u", run);
-    md.append(num, (size_t)w);
-    run = 0;
+  auto flush = [&]() {  // the run of matches in decimal
+    char digits[10];
+    int w = 0;
+    do {
+      digits[w++] = (char)('0' + run % 10);
+      run /= 10;
+    } while (run);
+    while (w) md.push_back(digits[--w]);
   };
   for (uint32_t k = 0; k < a.n_ops; ++k) {
     const uint32_t op = ops[k] & 0xfu, len = ops[k] >> 4;

@@ -590,11 +590,14 @@ class GpuScorer:
 
     # -- mapping (mapper.rs:400-552)
     def map_reads(self, reads, min_score: int = 0, max_ties: int | None = None,
-                  both_strands: bool = False, ref_letters=None) -> "Mappings":
+                  both_strands: bool = False, ref_letters=None, raw: bool = False):
         """Aligner::map_reads_scored over this scorer: per read the best, XS,
         tie count and the traced hits (primary first) with MD and NM.
         `ref_letters`: the panel's letters (a list of str/bytes, panel order)
-        for MD; without them MD spells the panel's codes as A/C/G/T/N."""
+        for MD; without them MD spells the panel's codes as A/C/G/T/N.
+        Returns Mappings, or with `raw` the library's mapping itself
+        (MappingHandle), for a consumer in the library such as the BAM
+        encoder, with no copy."""
         codes, off, lens = self._inputs(reads)
         lp, lo, keep = self._letters(ref_letters)
         opts = _native.EsgMapOptions(int(min_score),
@@ -606,6 +609,8 @@ class GpuScorer:
         _check(self._lib, self._lib.esg_map_reads(self._h, _ptr(codes, C.c_uint8),
                                                   _ptr(off, C.c_uint64), _ptr(lens, C.c_uint32),
                                                   lens.size, C.byref(opts), lp, lo, C.byref(h)))
+        if raw:
+            return MappingHandle(self._lib, h)
         try:
             return Mappings._copy(self._lib, h)
         finally:
@@ -613,11 +618,11 @@ class GpuScorer:
 
     def map_pairs(self, mates, min_score: int = 0, max_ties: int | None = None,
                   max_insert: int = 500, both_strands: bool = False,
-                  ref_letters=None) -> "Mappings":
+                  ref_letters=None, raw: bool = False):
         """Aligner::map_pairs_scored (pair.rs:157-390) over this scorer:
         mates 2p and 2p + 1 are pair p (adapters already trimmed).  Per pair
         Proper (score, tie count, per-mate XS, pair hits) or Separate (each
-        mate as map_reads maps it on both strands)."""
+        mate as map_reads maps it on both strands).  `raw` as for map_reads."""
         codes, off, lens = self._inputs(mates)
         if lens.size % 2:
             raise ValueError("mates come in pairs")
@@ -634,6 +639,8 @@ class GpuScorer:
                                                   _ptr(off, C.c_uint64), _ptr(lens, C.c_uint32),
                                                   lens.size // 2, C.byref(opts), lp, lo,
                                                   C.byref(h)))
+        if raw:
+            return MappingHandle(self._lib, h)
         try:
             return Mappings._copy(self._lib, h, paired=True)
         finally:
@@ -765,6 +772,29 @@ PAIR_PROPER = 1
 PAIR_HAS_XS = (2, 4)
 
 
+class MappingHandle:
+    """An esg_mapping the library owns (map_reads / map_pairs with raw=True),
+    freed with free() or when collected; mappings() copies it out."""
+
+    def __init__(self, lib, h):
+        self._lib = lib
+        self._h = h
+
+    def mappings(self, paired: bool = False) -> "Mappings":
+        return Mappings._copy(self._lib, self._h, paired)
+
+    def free(self):
+        if self._h:
+            self._lib.esg_mapping_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 class Mappings:
     """esg_map_reads' output: per read a MAPPING_DTYPE record, its hits
     (HIT_DTYPE) and their CIGAR words and MD strings."""
@@ -785,7 +815,7 @@ class Mappings:
             if not n.value:
                 return np.zeros(0, dtype=dtype)
             buf = (ct * (n.value * dtype.itemsize // C.sizeof(ct))).from_address(p)
-            return np.frombuffer(bytes(buf), dtype=dtype).copy()
+            return np.frombuffer(buf, dtype=dtype).copy()
         reads = arr(lib.esg_mapping_reads, C.c_uint8, MAPPING_DTYPE, C.c_uint32)
         hits = arr(lib.esg_mapping_hits, C.c_uint8, HIT_DTYPE, C.c_uint64)
         ops = arr(lib.esg_mapping_ops, C.c_uint8, np.dtype("<u4"), C.c_uint64)

@@ -201,7 +201,8 @@ class OracleScorer:
         self.oracle, self.refs, self.scoring, self.local = oracle, refs, scoring, local
         self.calls = 0
 
-    def map_reads(self, reads, min_score=0, max_ties=None, both_strands=False, ref_letters=None):
+    def map_reads(self, reads, min_score=0, max_ties=None, both_strands=False, ref_letters=None,
+                  raw=False):
         codes, off, lens = reads
         letters = [bytes(b"ACGTN"[int(c)] for c in codes[int(o):int(o) + int(n)])
                    for o, n in zip(off, lens)]
