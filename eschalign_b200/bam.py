@@ -1,14 +1,16 @@
 """BAM input and output around the mapping stage (esg_bam_*), and the CLI's
-unpaired pipeline over them.
+unpaired and paired runs over them.
 
-The reference's `eschalign` binary reads a BAM in batches (read_batches,
-crates/eschalign-cli/src/align.rs:604-660), maps them
+The reference's `eschalign` binary reads a BAM, FASTA or FASTQ in batches
+(read_batches, crates/eschalign-cli/src/align.rs:604-660), maps them
 (Aligner::map_reads_scored), turns each read's mapping into its output
 records (build_records, align.rs:1084-1200) and writes them in input order or
-coordinate order (write_in_order, align.rs:2345-2400; the sort, 2406-2450).
-`align_bam` does the same with the library: batches from `BamReader`,
-`GpuScorer.map_reads` on the device, `encode` and `BamWriter` on host threads.
-The records are the reference CLI's byte for byte.
+coordinate order (write_in_order, align.rs:2345-2400; the sort, 2406-2450);
+read pairs go through map_pairs_scored and build_pair_records
+(align.rs:1203-1425, 1613-1750).  `align_bam` and `align_pairs_bam` do the
+same with the library: batches from `BamReader` / `PairReader`, the mapping
+stage on the device, `encode` / `encode_pairs` and `BamWriter` on host
+threads.  The records are the reference CLI's byte for byte.
 """
 from __future__ import annotations
 

@@ -1,15 +1,19 @@
 // esg_bam.cu -- BAM input and output around the mapping stage (host code).
 //
-// The CLI's I/O stage for unpaired reads (crates/eschalign-cli/src/align.rs):
+// The CLI's I/O stage (crates/eschalign-cli/src/align.rs):
 //   * reading: read_batches (align.rs:604-660) -- primary records of a BGZF
 //     BAM in batches; secondary and supplementary records skipped; a record
 //     aligned to the reverse strand refused; or the records of a FASTA or
 //     FASTQ file, plain or gzip (sniff, FastxReader, fastx_to_record:
-//     align.rs:385-563), each taken as an unmapped record;
+//     align.rs:385-563), each taken as an unmapped record; --read-ids
+//     (align.rs:572-621); read pairs from two mate files, an interleaved
+//     file or a paired BAM (PairSource, align.rs:674-905);
 //   * the output records of a read's mapping: build_records
 //     (align.rs:1084-1200) with OWNED_TAGS (346-352), int_value (1001-1015),
 //     sam_cigar / clipped_span (1017-1052), xa_entry (1054-1069); a read over
-//     --max-read-len is written unmapped (process_chunk, 1504-1602);
+//     --max-read-len is written unmapped (process_chunk, 1504-1602); a
+//     pair's records: build_pair_records (align.rs:1203-1425) with
+//     process_pair_chunk's mate placements (1683-1713);
 //   * writing: write_in_order (align.rs:2345-2400) -- chunks in sequence
 //     order -- or the coordinate sort (2406-2450): stable on (reference,
 //     position, reverse), unmapped last; BGZF blocks with the end marker.
