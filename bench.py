@@ -882,12 +882,13 @@ def run_c2(a, ctx, rank):
                                               a.no_cpu_baseline or rank != 0 or world != 1)
         extras["map"] = map_stage(g, refs, reads, scoring, mode == "local",
                                   a.no_cpu_baseline or rank != 0 or world != 1)
-        # a second scorer over the same panel: one maps while the other's
-        # host share of the mapping runs
-        g2 = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank)
-        g2.set_split(info["split_len"])
-        extras["bam"] = bam_stage([g, g2], refs, reads)
-        g2.close()
+        if world == 1:
+            # the BAM run, a single-GPU figure: a second scorer over the same
+            # panel maps while the other's host share of the mapping runs
+            g2 = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank)
+            g2.set_split(info["split_len"])
+            extras["bam"] = bam_stage([g, g2], refs, reads)
+            g2.close()
         arms = reference_gpu_arms(refs, sub, scoring, mode == "local", local_rank)
         if arms:
             arms["batched_over_ref_half2"] = value / arms["half2_gcups"]
@@ -1028,10 +1029,11 @@ def run_c4(a, ctx, rank):
     if not a.no_extras:
         map_pairs = map_pairs_stage(g, refs, pairs, C4_SCORING, False,
                                     a.no_cpu_baseline or rank != 0 or world != 1)
-        g2 = GpuScorer(refs, Scoring(*C4_SCORING), Mode.SEMIGLOBAL, device=local_rank)
-        g2.set_split(g.info()["split_len"])
-        bam_pairs = bam_pairs_stage([g, g2], refs, pairs)
-        g2.close()
+        if world == 1:
+            g2 = GpuScorer(refs, Scoring(*C4_SCORING), Mode.SEMIGLOBAL, device=local_rank)
+            g2.set_split(g.info()["split_len"])
+            bam_pairs = bam_pairs_stage([g, g2], refs, pairs)
+            g2.close()
     step_pairs = a.pair_chunk
     chunks = [pairs.slice(2 * k, 2 * (k + step_pairs)) for k in range(0, n_pairs, step_pairs)]
     te, n_pass, h2d, d2h = feeder(
