@@ -182,9 +182,13 @@ bool parse_rec(const uint8_t* r, uint32_t size, InRec& x) {
   x.n_cigar = u16_at(r + 12);
   x.flag = u16_at(r + 14);
   x.l_seq = u32_at(r + 16);
-  x.seq_off = 32 + x.name_len + 4 * x.n_cigar;
-  x.aux_off = x.seq_off + (x.l_seq + 1) / 2 + x.l_seq;
-  return x.aux_off <= size;
+  // in 64 bits: a corrupt l_seq must not wrap the bound below
+  const uint64_t seq_off = 32ull + x.name_len + 4ull * x.n_cigar;
+  const uint64_t aux_off = seq_off + (x.l_seq + 1ull) / 2 + x.l_seq;
+  if (aux_off > size) return false;
+  x.seq_off = (uint32_t)seq_off;
+  x.aux_off = (uint32_t)aux_off;
+  return true;
 }
 
 // (offset, length) of each auxiliary field of a record
@@ -200,9 +204,9 @@ bool split_aux(const uint8_t* a, uint32_t n, std::vector<std::pair<uint32_t, uin
     }
   };
   while (i < n) {
-    if (i + 3 > n) return false;
+    if ((uint64_t)i + 3 > n) return false;
     const uint8_t t = a[i + 2];
-    uint32_t j = i + 3;
+    uint64_t j = i + 3ull;  // 64 bits: a corrupt array length must not wrap
     if (size_of(t) > 0) {
       j += size_of(t);
     } else if (t == 'Z' || t == 'H') {
@@ -210,13 +214,13 @@ bool split_aux(const uint8_t* a, uint32_t n, std::vector<std::pair<uint32_t, uin
       ++j;
     } else if (t == 'B') {
       if (j + 5 > n || size_of(a[j]) <= 0) return false;
-      j += 5 + u32_at(a + j + 1) * (uint32_t)size_of(a[j]);
+      j += 5 + (uint64_t)u32_at(a + j + 1) * (uint64_t)size_of(a[j]);
     } else {
       return false;
     }
     if (j > n) return false;
-    out.push_back({i, j - i});
-    i = j;
+    out.push_back({i, (uint32_t)(j - i)});
+    i = (uint32_t)j;
   }
   return true;
 }

@@ -235,3 +235,29 @@ def test_align_bam_pipeline_writes_the_reference_record_stream(oracle, tmp_path,
     assert n["records"] == want["records"]
     assert format(B.fnv1a64(record_stream(path)), "016x") == want["fnv1a64"]
     assert set(st) == {"read", "map", "encode", "write"}
+
+
+def test_corrupt_records_are_errors(tmp_path):
+    """A record whose sequence length runs past its block, or whose B-array
+    count runs past its tags, is an error status, not a read past the
+    buffer."""
+    import struct
+    from oracle import bam as B
+    from tests.test_bam_pairs import bgzf
+    good = B.encode_record(-1, -1, 0, [], 4, b"r1", b"ACGT", b"IIII", [])
+    bad_len = good[:20] + struct.pack("<I", 0xFFFFFFF0) + good[24:]
+    p = tmp_path / "bad_len.bam"
+    p.write_bytes(bgzf(b"BAM\1" + bytes(8) + bad_len))
+    with pytest.raises(RuntimeError, match="malformed BAM record"):
+        with EB.BamReader(str(p)) as rd:
+            list(rd.batches(10, 0))
+    arr = b"ZZBc" + struct.pack("<I", 0xFFFFFFF0) + b"\x01"
+    bad_aux = B.encode_record(-1, -1, 0, [], 4, b"r2", b"ACGT", b"IIII", [arr])
+    p = tmp_path / "bad_aux.bam"
+    p.write_bytes(bgzf(b"BAM\1" + bytes(8) + bad_aux))
+    names, _ = trna_panel()
+    with EB.BamReader(str(p)) as rd:
+        (b,) = list(rd.batches(10, 0))
+        with pytest.raises(RuntimeError, match="malformed auxiliary"):
+            EB.encode(b, mappings_from_oracle([{"best_score": None, "n_tied": 0,
+                                                "suboptimal": None, "hits": []}]), names)
