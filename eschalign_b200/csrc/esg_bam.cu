@@ -115,6 +115,10 @@ esg_status inflate_blocks(const std::vector<uint8_t>& data, const std::vector<si
     const uint16_t xlen = u16_at(b + 10);
     const size_t cstart = 12 + xlen, clen = (e - s) - cstart - 8;
     const uint32_t isize = u32_at(b + (e - s) - 4);
+    if (isize > 65536) {  // a BGZF block holds at most 64 KiB
+      bad = 1;
+      return;
+    }
     parts[i].resize(isize);
     if (!isize) return;
     z_stream z{};
@@ -403,6 +407,7 @@ static esg_status fill(esg_bam_reader* r, size_t want) {
     if (xlen != 6 || head[12] != 'B' || head[13] != 'C')
       return berr(ESG_ERR_BAD_ARGUMENT, "BGZF block without its size field");
     const uint32_t bsize = (uint32_t)u16_at(head + 16) + 1;
+    if (bsize < 26) return berr(ESG_ERR_BAD_ARGUMENT, "corrupt BGZF block size");
     const size_t s = data.size();
     data.resize(s + bsize);
     memcpy(data.data() + s, head, 18);

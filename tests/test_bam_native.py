@@ -261,3 +261,24 @@ def test_corrupt_records_are_errors(tmp_path):
         with pytest.raises(RuntimeError, match="malformed auxiliary"):
             EB.encode(b, mappings_from_oracle([{"best_score": None, "n_tied": 0,
                                                 "suboptimal": None, "hits": []}]), names)
+
+
+def test_corrupt_bgzf_is_an_error(tmp_path):
+    """A BGZF block whose size field is too small, or whose stated inflated
+    size is over 64 KiB, is an error status."""
+    import struct
+    from tests.test_bam_pairs import bgzf
+    data = bytearray(bgzf(b"BAM\1" + bytes(8)))
+    small = bytearray(data)
+    small[16:18] = struct.pack("<H", 10)
+    p = tmp_path / "small.bam"
+    p.write_bytes(bytes(small))
+    with pytest.raises(RuntimeError, match="BGZF"):
+        EB.BamReader(str(p))
+    bsize = struct.unpack("<H", data[16:18])[0] + 1
+    big = bytearray(data)
+    big[bsize - 4:bsize] = struct.pack("<I", 1 << 20)
+    p = tmp_path / "big.bam"
+    p.write_bytes(bytes(big))
+    with pytest.raises(RuntimeError, match="BGZF|not a BAM"):
+        EB.BamReader(str(p))
