@@ -95,3 +95,45 @@ def test_gpu_c3_shape_saturating_scheme(oracle, c3_panel, mode):
     want, want_t, _ = oracle.scalar_map_batch(reads.list(), refs, scoring, mode == Mode.LOCAL,
                                               True, cap=CAP)
     assert_same(res.results, res.ties, want, want_t, CAP, f"C3 saturating {mode.label}")
+
+
+def test_bam_run_at_scale_equals_the_oracle(c2, tmp_path):
+    """The unpaired BAM run on 100 000 C2 reads (an unaligned BAM in, both
+    strands, every tie traced, MD from the panel's letters, two scorers)
+    against the oracle's: the CPU mapping stage (AVX-512 scores and ties,
+    scalar traceback, MD / NM, all in C) and its restatement of the CLI's
+    record building -- the output record stream byte for byte."""
+    from eschalign_b200 import bam as EB
+    from oracle import bam as B
+    from oracle import oracle as O
+    from tests.test_bam_pairs import bgzf
+    refs, reads = c2
+    sub = reads.slice(0, 100_000)
+    names = [f"ref{k}" for k in range(len(refs))]
+    letters = [bytes(b"ACGTN"[int(c)] for c in r) for r in refs]
+    rng = np.random.default_rng(5)
+    recs = []
+    for k in range(len(sub)):
+        seq = bytes(b"ACGTN"[int(c)] for c in sub.read(k))
+        qual = rng.integers(2, 41, len(seq), dtype=np.uint8).tobytes()
+        recs.append(B.encode_record(-1, -1, 0, [], 4, b"r%06d" % k, seq, qual,
+                                    [B.str_field(b"RG", "grp1")]))
+    src, dst = str(tmp_path / "in.bam"), str(tmp_path / "out.bam")
+    with open(src, "wb") as fh:
+        fh.write(bgzf(b"BAM\1" + bytes(8) + b"".join(recs)))
+    gs = [GpuScorer(refs, Scoring(2, -1, -10, -1), Mode.LOCAL) for _ in range(2)]
+    try:
+        n = EB.align_bam(gs, src, dst, names, letters, both_strands=True, secondary=True)
+    finally:
+        for g in gs:
+            g.close()
+    from tests.test_bam_native import record_stream
+    got = record_stream(dst)
+    res, jobs, al, ops, mds, nm, _ = O.cpu_map_reads(
+        *sub.tuple(), refs, (2, -1, -10, -1), True, both_strands=True,
+        ref_letters=letters)
+    maps = O.cpu_mappings(res, jobs, al, ops, mds, nm)
+    _, _, inputs = B.read_bam(open(src, "rb").read())
+    want = b"".join(x for r, m in zip(inputs, maps) for x in B.build_records(r, m, names, True))
+    assert n["reads"] == len(sub)
+    assert got == want
