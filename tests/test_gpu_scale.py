@@ -137,3 +137,51 @@ def test_bam_run_at_scale_equals_the_oracle(c2, tmp_path):
     want = b"".join(x for r, m in zip(inputs, maps) for x in B.build_records(r, m, names, True))
     assert n["reads"] == len(sub)
     assert got == want
+
+
+def test_paired_bam_run_at_scale_equals_the_oracle(tmp_path):
+    """The paired BAM run on 20 000 C4 pairs (two FASTQ files, TruSeq
+    adapters trimmed, semi-global, --min-score 40, two scorers) against the
+    oracle's: its pair reader and adapter search, its C-composed paired
+    mapping stage and its restatement of build_pair_records -- the output
+    record stream byte for byte."""
+    from eschalign_b200 import bam as EB
+    from oracle import bam as B
+    from oracle import oracle as O
+    from tests.test_bam_native import record_stream
+    refs = synth.panel_tiles()
+    pairs, _ = synth.pairs_c4(refs, n=20_000, seed=0x5EED_0912)
+    names = [f"ref{k}" for k in range(len(refs))]
+    letters = [bytes(b"ACGTN"[int(c)] for c in r) for r in refs]
+    rng = np.random.default_rng(6)
+    texts = [[], []]
+    for p in range(len(pairs) // 2):
+        for m in range(2):
+            seq = bytes(b"ACGTN"[int(c)] for c in pairs.read(2 * p + m)).decode()
+            q = "".join(chr(33 + int(x)) for x in rng.integers(2, 41, len(seq)))
+            texts[m].append(f"@p{p}\n{seq}\n+\n{q}\n")
+    t1, t2 = "".join(texts[0]).encode(), "".join(texts[1]).encode()
+    p1, p2, dst = str(tmp_path / "r1.fq"), str(tmp_path / "r2.fq"), str(tmp_path / "o.bam")
+    open(p1, "wb").write(t1)
+    open(p2, "wb").write(t2)
+    scoring = (2, -1, -10, -1)
+    gs = [GpuScorer(refs, Scoring(*scoring), Mode.SEMIGLOBAL) for _ in range(2)]
+    try:
+        n = EB.align_pairs_bam(gs, p1, p2, dst, names, letters, min_score=40, secondary=True)
+    finally:
+        for g in gs:
+            g.close()
+    got = record_stream(dst)
+    recs = B.read_pairs(t1, t2)
+    ads, mates = [], []
+    for a, b in recs:
+        ad = O.pair_adapters(a["seq"], b["seq"], max_read_len=1000)
+        ads.append(ad)
+        mates += [a["seq"][:len(a["seq"]) - ad[0]], b["seq"][:len(b["seq"]) - ad[1]]]
+    from eschalign_b200 import pack_reads, encode
+    codes, off, lens = pack_reads([encode(m) for m in mates])
+    pms, _ = O.cpu_map_pairs(codes, off, lens, refs, scoring, False, min_score=40,
+                             ref_letters=letters)
+    want = b"".join(x for (a, b), pm, ad in zip(recs, pms, ads)
+                    for x in B.build_pair_records([a, b], pm, ad, names, True))
+    assert n["reads"] == len(pairs) and got == want
