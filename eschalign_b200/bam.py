@@ -146,7 +146,10 @@ class PairReader(BamReader):
         self._h = h
         self._after_open(read_ids)
 
-    def batches(self, max_pairs: int = 25_000, max_read_len: int = 0):
+    def batches(self, max_pairs: int = 25_000):
+        """Batches of at most max_pairs pairs, mates at full length (the
+        adapter search, esg_pair_adapters, trims them and leaves mates over
+        --max-read-len out)."""
         while True:
             b = C.c_void_p()
             _check(self._lib, self._lib.esg_bam_read_pair_batch(self._h, max_pairs,
