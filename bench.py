@@ -415,12 +415,116 @@ def unmapped_bam(path, reads, seed=11):
     return len(raw)
 
 
-def bam_stage(g, refs, reads, batch_size=50_000):
+class CpuMapper:
+    """The CPU path's mapping stage for the BAM run's CPU arm: map_reads as
+    the reference's CPU path runs it (the oracle's cpu_map_reads: AVX-512
+    scores and ties, scalar traceback, MD / NM, in C on every thread), its
+    mappings handed to the library's BAM encoder."""
+
+    def __init__(self, refs, scoring, local):
+        from oracle import oracle as O
+        self.O, self.refs, self.scoring, self.local = O, refs, scoring, local
+        self.prof = O.Profile(refs, scoring)
+
+    def map_reads(self, reads, min_score=0, max_ties=None, both_strands=False,
+                  ref_letters=None, raw=False):
+        O = self.O
+        res, jobs, al, ops, mds, nm, _ = O.cpu_map_reads(
+            *reads, self.refs, self.scoring, self.local, min_score=min_score,
+            max_ties=max_ties, both_strands=both_strands, ref_letters=ref_letters,
+            profile=self.prof)
+        ms = O.cpu_mappings(res, jobs, al, ops, mds, nm)
+        return _mappings_of(ms)
+
+
+def _hit_of(h, words, md):
+    """One map_reads-form hit dict as a HIT_DTYPE record, its CIGAR words
+    and MD appended to `words` and `md`."""
+    from eschalign_b200.scorer import HIT_DTYPE
+    e = np.zeros((), HIT_DTYPE)
+    for f in ("reference", "reverse", "score", "query_start", "query_end", "ref_start",
+              "ref_end", "nm"):
+        e[f] = int(h[f])
+    w, num = [], ""
+    for ch in h["cigar"]:
+        if ch.isdigit():
+            num += ch
+        else:
+            w.append(int(num) << 4 | "MIDNSHP=X".index(ch))
+            num = ""
+    e["ops_offset"], e["n_ops"] = len(words), len(w)
+    words += w
+    e["md_offset"], e["md_len"] = len(md), len(h["md"])
+    md += h["md"].encode()
+    return e
+
+
+def _read_entry(r, m, hits, words, md):
+    r["first_hit"], r["n_hits"], r["n_tied"] = len(hits), len(m["hits"]), m["n_tied"]
+    if m["best_score"] is not None:
+        r["best_score"], r["flags"] = m["best_score"], 1
+    if m["suboptimal"] is not None:
+        r["suboptimal"], r["flags"] = m["suboptimal"], r["flags"] | 2
+    hits += [_hit_of(h, words, md) for h in m["hits"]]
+
+
+def _mappings_of(ms, pms=None):
+    """The oracle's per-read (or, with pms, per-pair) dicts as the arrays
+    esg_map_reads / esg_map_pairs return."""
+    from eschalign_b200.scorer import (HIT_DTYPE, MAPPING_DTYPE, PAIR_HIT_DTYPE,
+                                       PAIR_MAPPING_DTYPE, Mappings)
+    hits, words, md = [], [], bytearray()
+    if pms is None:
+        out = np.zeros(len(ms), MAPPING_DTYPE)
+        for k, m in enumerate(ms):
+            _read_entry(out[k], m, hits, words, md)
+        return Mappings(out, np.array(hits, HIT_DTYPE), np.array(words, np.uint32), bytes(md))
+    out = np.zeros(2 * len(pms), MAPPING_DTYPE)
+    pairs = np.zeros(len(pms), PAIR_MAPPING_DTYPE)
+    phits = []
+    for p, pm in enumerate(pms):
+        if not pm["proper"]:
+            for m in range(2):
+                _read_entry(out[2 * p + m], pm["mates"][m], hits, words, md)
+            continue
+        pr = pairs[p]
+        sub = pm["suboptimal"]
+        pr["flags"] = 1 | (2 if sub[0] is not None else 0) | (4 if sub[1] is not None else 0)
+        pr["score"], pr["n_tied"], pr["n_hits"] = pm["score"], pm["n_tied"], len(pm["hits"])
+        pr["suboptimal"] = [x if x is not None else 0 for x in sub]
+        pr["first_hit"] = len(phits)
+        for h in pm["hits"]:
+            e = np.zeros((), PAIR_HIT_DTYPE)
+            e["reference"], e["reverse"], e["insert"] = h["reference"], h["reverse"], h["insert"]
+            e["mates"][0] = _hit_of(h["mates"][0], words, md)
+            e["mates"][1] = _hit_of(h["mates"][1], words, md)
+            phits.append(e)
+    return Mappings(out, np.array(hits, HIT_DTYPE), np.array(words, np.uint32), bytes(md),
+                    pairs, np.array(phits, PAIR_HIT_DTYPE))
+
+
+class CpuPairMapper(CpuMapper):
+    """map_pairs on the host cores for the paired BAM run's CPU arm (the
+    oracle's cpu_map_pairs: AVX-512 ranking, scalar traceback, pair
+    constraints, MD / NM, in C on every thread)."""
+
+    def map_pairs(self, mates, min_score=0, max_ties=None, max_insert=500, both_strands=False,
+                  ref_letters=None, raw=False):
+        pms, _ = self.O.cpu_map_pairs(*mates, self.refs, self.scoring, self.local,
+                                      min_score=min_score, max_ties=max_ties,
+                                      max_insert=max_insert, both_strands=both_strands,
+                                      ref_letters=ref_letters, profile=self.prof)
+        return _mappings_of(None, pms)
+
+
+def bam_stage(g, refs, reads, batch_size=50_000, cpu_reads=0, scoring=HEADLINE[0]):
     """The CLI's unpaired run through the library (bam.align_bam): an
     unaligned BAM of the workload's reads read, mapped on the device (every
     tie traced, MD / NM from the panel's letters), its records built and
     written as BGZF; wall time, input order, default batch size 50 000;
-    `g` one scorer or several (one mapping thread each)."""
+    `g` one scorer or several (one mapping thread each).  With cpu_reads,
+    the CPU path on the first cpu_reads reads beside it: the same run with
+    the mapping stage on the host cores (CpuMapper), the BAM I/O the same."""
     from eschalign_b200 import bam as EB
     names = [f"ref{k}" for k in range(len(refs))]
     letters = [bytes(b"ACGTN"[int(c)] for c in r) for r in refs]
@@ -437,14 +541,31 @@ def bam_stage(g, refs, reads, batch_size=50_000):
                          batch_size=batch_size, max_read_len=1000, stats=st)
         dt = time.perf_counter() - t0
         out_bytes = os.path.getsize(dst)
-    return {"reads": n["reads"], "records": n["records"], "seconds": round(dt, 3),
-            "reads_per_s": n["reads"] / dt, "batch_reads": batch_size,
+        cpu = None
+        if cpu_reads:
+            small = os.path.join(tmp, "cpu.bam")
+            unmapped_bam(small, reads.slice(0, cpu_reads))
+            mapper = CpuMapper(refs, scoring, True)
+            t0 = time.perf_counter()
+            nc = EB.align_bam(mapper, small, dst, names, letters, both_strands=True,
+                              batch_size=batch_size, max_read_len=1000)
+            dc = time.perf_counter() - t0
+            cpu = {"reads_per_s": nc["reads"] / dc, "kind": "port",
+                   "cores": os.cpu_count(),
+                   "sample": f"first {nc['reads']} reads: the same BAM run with the mapping "
+                             "stage on the host cores (AVX-512 scores and ties, scalar "
+                             "traceback, MD / NM, in C on all threads)"}
+    out = {"reads": n["reads"], "records": n["records"], "seconds": round(dt, 3),
+           "reads_per_s": n["reads"] / dt, "batch_reads": batch_size,
             "input_bgzf_bytes": in_bytes, "input_raw_bytes": raw, "output_bgzf_bytes": out_bytes,
             "stage_seconds": {k: round(v, 3) for k, v in st.items()},
-            "scorers": len(g) if isinstance(g, (list, tuple)) else 1,
-            "options": "both strands, min_score 0, every tie traced, MD/NM from letters, "
-                       "input order; read, map (one thread per scorer) and encode/write "
-                       "overlapped"}
+           "scorers": len(g) if isinstance(g, (list, tuple)) else 1,
+           "options": "both strands, min_score 0, every tie traced, MD/NM from letters, "
+                      "input order; read, map (one thread per scorer) and encode/write "
+                      "overlapped"}
+    if cpu:
+        out["cpu"] = cpu
+    return out
 
 
 def fastq_files(path1, path2, pairs, seed=12):
@@ -481,7 +602,7 @@ def fastq_files(path1, path2, pairs, seed=12):
             fh.write(memoryview(buf))
 
 
-def bam_pairs_stage(g, refs, pairs, n=500_000, batch_size=50_000):
+def bam_pairs_stage(g, refs, pairs, n=500_000, batch_size=50_000, cpu_pairs=0):
     """The CLI's paired run through the library (bam.align_pairs_bam): the
     first n pairs as two FASTQ files, each mate trimmed of its adapter,
     mapped on the device (map_pairs_scored: every tie traced, MD / NM from
@@ -505,14 +626,30 @@ def bam_pairs_stage(g, refs, pairs, n=500_000, batch_size=50_000):
         dt = time.perf_counter() - t0
         out_bytes = os.path.getsize(dst)
         in_bytes = os.path.getsize(p1) + os.path.getsize(p2)
-    return {"pairs": r["reads"] // 2, "records": r["records"], "seconds": round(dt, 3),
-            "scorers": len(g) if isinstance(g, (list, tuple)) else 1,
-            "pairs_per_s": r["reads"] / 2 / dt, "batch_records": batch_size,
-            "input_fastq_bytes": in_bytes, "output_bgzf_bytes": out_bytes,
-            "stage_seconds": {k: round(v, 3) for k, v in st.items()},
-            "options": "semi-global, --min-score 40, max insert 500, forward template strand, "
-                       "TruSeq adapters trimmed, every tie traced, MD/NM from letters, "
-                       "input order"}
+        cpu = None
+        if cpu_pairs:
+            c1, c2 = os.path.join(tmp, "c1.fq"), os.path.join(tmp, "c2.fq")
+            fastq_files(c1, c2, sub.slice(0, 2 * cpu_pairs))
+            mapper = CpuPairMapper(refs, C4_SCORING, False)
+            t0 = time.perf_counter()
+            rc = EB.align_pairs_bam(mapper, c1, c2, dst, names, letters, min_score=40,
+                                    batch_size=batch_size)
+            dc = time.perf_counter() - t0
+            cpu = {"pairs_per_s": rc["reads"] / 2 / dc, "kind": "port", "cores": os.cpu_count(),
+                   "sample": f"first {rc['reads'] // 2} pairs: the same paired BAM run with "
+                             "the paired mapping stage on the host cores (AVX-512 ranking, "
+                             "scalar traceback, MD / NM, in C on all threads)"}
+    out = {"pairs": r["reads"] // 2, "records": r["records"], "seconds": round(dt, 3),
+           "scorers": len(g) if isinstance(g, (list, tuple)) else 1,
+           "pairs_per_s": r["reads"] / 2 / dt, "batch_records": batch_size,
+           "input_fastq_bytes": in_bytes, "output_bgzf_bytes": out_bytes,
+           "stage_seconds": {k: round(v, 3) for k, v in st.items()},
+           "options": "semi-global, --min-score 40, max insert 500, forward template strand, "
+                      "TruSeq adapters trimmed, every tie traced, MD/NM from letters, "
+                      "input order"}
+    if cpu:
+        out["cpu"] = cpu
+    return out
 
 
 def map_pairs_stage(g, refs, pairs, scoring, local, skip_cpu, n=100_000):
@@ -887,7 +1024,8 @@ def run_c2(a, ctx, rank):
             # panel maps while the other's host share of the mapping runs
             g2 = GpuScorer(refs, Scoring(*scoring), Mode.parse(mode), device=local_rank)
             g2.set_split(info["split_len"])
-            extras["bam"] = bam_stage([g, g2], refs, reads)
+            extras["bam"] = bam_stage([g, g2], refs, reads,
+                                      cpu_reads=0 if a.no_cpu_baseline else 40_000)
             g2.close()
         arms = reference_gpu_arms(refs, sub, scoring, mode == "local", local_rank)
         if arms:
@@ -1032,7 +1170,8 @@ def run_c4(a, ctx, rank):
         if world == 1:
             g2 = GpuScorer(refs, Scoring(*C4_SCORING), Mode.SEMIGLOBAL, device=local_rank)
             g2.set_split(g.info()["split_len"])
-            bam_pairs = bam_pairs_stage([g, g2], refs, pairs)
+            bam_pairs = bam_pairs_stage([g, g2], refs, pairs,
+                                        cpu_pairs=0 if a.no_cpu_baseline else 20_000)
             g2.close()
     step_pairs = a.pair_chunk
     chunks = [pairs.slice(2 * k, 2 * (k + step_pairs)) for k in range(0, n_pairs, step_pairs)]
