@@ -301,13 +301,34 @@ class BamWriter:
             pass
 
 
-def header_text(ref_names, ref_lens, sort_coordinate: bool = False) -> bytes:
-    """@HD (SO as the CLI writes it) and an @SQ line per reference."""
+def header_text(ref_names, ref_lens, sort_coordinate: bool = False,
+                input_text: bytes = b"") -> bytes:
+    """The output header as the CLI builds it (build_header,
+    align.rs:1780-1808): @HD VN:1.6 with the sort order, an @SQ line per
+    panel reference, the input's read groups, programs and comments, and a
+    @PG line of its own chained (PP) after the input's last program."""
     so = "coordinate" if sort_coordinate else "unsorted"
     lines = [f"@HD\tVN:1.6\tSO:{so}"]
     for n, ln in zip(ref_names, ref_lens):
         lines.append(f"@SQ\tSN:{n if isinstance(n, str) else n.decode()}\tLN:{int(ln)}")
-    lines.append("@PG\tID:eschalign-b200\tPN:eschalign-b200")
+    kept = {"@RG": [], "@PG": [], "@CO": []}
+    for line in input_text.decode(errors="replace").splitlines():
+        if line[:3] in kept:
+            kept[line[:3]].append(line)
+    ids, parents = [], set()
+    for line in kept["@PG"]:
+        f = dict(x.split(":", 1) for x in line.split("\t")[1:] if ":" in x)
+        if "ID" in f:
+            ids.append(f["ID"])
+        if "PP" in f:
+            parents.add(f["PP"])
+    pid, k = "eschalign-b200", 0
+    while pid in ids:
+        k += 1
+        pid = f"eschalign-b200.{k}"
+    leaves = [x for x in ids if x not in parents]
+    pg = f"@PG\tID:{pid}\tPN:eschalign-b200" + (f"\tPP:{leaves[-1]}" if leaves else "")
+    lines += kept["@RG"] + kept["@PG"] + [pg] + kept["@CO"]
     return ("\n".join(lines) + "\n").encode()
 
 
@@ -345,7 +366,8 @@ def _run(reader, batches, scorers, map_batch, encode_batch, out_path, ref_names,
             st["map"] += time.perf_counter() - t0
         return batch, m
 
-    with reader, BamWriter(out_path, header_text(ref_names, ref_lens, sort_coordinate),
+    with reader, BamWriter(out_path, header_text(ref_names, ref_lens, sort_coordinate,
+                                                 reader.header_text),
                            ref_names, ref_lens, sort_coordinate, threads) as wr, \
             ThreadPoolExecutor(1) as rpool, ThreadPoolExecutor(len(scorers)) as mpool, \
             ThreadPoolExecutor(1) as opool:

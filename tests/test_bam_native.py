@@ -282,3 +282,28 @@ def test_corrupt_bgzf_is_an_error(tmp_path):
     p.write_bytes(bytes(big))
     with pytest.raises(RuntimeError, match="BGZF|not a BAM"):
         EB.BamReader(str(p))
+
+
+def test_output_header_carries_the_inputs_programs(oracle, tmp_path):
+    """build_header (align.rs:1780-1808): @HD 1.6 with the sort order, the
+    panel's @SQ lines, the input's @RG / @PG / @CO lines, and a @PG of its
+    own after the input's last program."""
+    from oracle import bam as B
+    names, refs = trna_panel()
+    with EB.BamReader(FIXTURE) as rd:
+        text_in = rd.header_text
+    h = EB.header_text(names, [len(r) for r in refs], True,
+                       text_in + b"@RG\tID:grp1\tSM:s\n@CO\ta comment\n").decode().splitlines()
+    assert h[0] == "@HD\tVN:1.6\tSO:coordinate"
+    assert [x.split("\t")[1][3:] for x in h[1:1 + len(names)]] == names
+    rest = h[1 + len(names):]
+    assert rest[0] == "@RG\tID:grp1\tSM:s"
+    assert [x for x in rest if x.startswith("@PG")][:3] == \
+        [x for x in text_in.decode().splitlines() if x.startswith("@PG")]
+    assert rest[-2] == "@PG\tID:eschalign-b200\tPN:eschalign-b200\tPP:samtools.1"
+    assert rest[-1] == "@CO\ta comment"
+    sc = OracleScorer(oracle, refs, (2, -1, -10, -1), True)
+    out = str(tmp_path / "o.bam")
+    EB.align_bam(sc, FIXTURE, out, names, refs)
+    text_out, _, _ = B.read_bam(open(out, "rb").read())
+    assert b"PP:samtools.1" in text_out and b"ID:bwa" in text_out
