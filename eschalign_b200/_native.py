@@ -262,6 +262,7 @@ SIGNATURES = {
                                          C.POINTER(C.c_char_p), C.c_uint32, C.c_uint32,
                                          C.POINTER(C.c_void_p)]),
     "esg_bam_records_bytes": (C.c_void_p, [C.c_void_p, _u64p, _u32p]),
+    "esg_bam_records_outcomes": (C.c_int32, [C.c_void_p, _u64p, _u64p, _u64p]),
     "esg_bam_records_free": (None, [C.c_void_p]),
     "esg_bam_writer_open": (C.c_int32, [C.c_char_p, C.c_char_p, C.POINTER(C.c_char_p), _u32p,
                                         C.c_uint32, C.c_int32, C.c_uint32,

@@ -177,6 +177,13 @@ class BamRecords:
     def bytes(self) -> bytes:
         return C.string_at(self._p, self.nbytes) if self.nbytes else b""
 
+    def outcomes(self) -> dict:
+        """How the batch's reads (mates) went: unique best, tied, unmapped."""
+        u, t, m = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        lib = _lib()
+        _check(lib, lib.esg_bam_records_outcomes(self._h, C.byref(u), C.byref(t), C.byref(m)))
+        return {"unique": u.value, "tied": t.value, "unmapped": m.value}
+
     def free(self):
         if self._h:
             _lib().esg_bam_records_free(self._h)
@@ -346,7 +353,7 @@ def _run(reader, batches, scorers, map_batch, encode_batch, out_path, ref_names,
     mapping thread per scorer: one thread's host share of the mapping
     (packing, tie lists, MD / NM, assembly) overlaps another's scoring on
     the device."""
-    out = {"reads": 0, "records": 0, "batches": 0}
+    out = {"reads": 0, "records": 0, "batches": 0, "unique": 0, "tied": 0, "unmapped": 0}
     st = stats if stats is not None else {}
     for k in ("read", "map", "encode", "write"):
         st.setdefault(k, 0.0)
@@ -390,6 +397,8 @@ def _run(reader, batches, scorers, map_batch, encode_batch, out_path, ref_names,
             out["reads"] += len(batch)
             out["records"] += rec.n_records
             out["batches"] += 1
+            for k, v in rec.outcomes().items():
+                out[k] += v
             rec.free()
             batch.free()
 

@@ -381,7 +381,8 @@ struct esg_bam_batch {
 struct esg_bam_records {
   std::vector<uint8_t> bytes;
   uint32_t n_records = 0;
-  uint32_t n_unmapped = 0;
+  // how each read went, the CLI's Outcome (align.rs:1077-1082)
+  uint64_t n_unique = 0, n_tied = 0, n_unmapped = 0;
 };
 
 // Inflate more blocks into r->buf: up to `want` more blocks, read from the
@@ -1012,7 +1013,7 @@ esg_status esg_bam_encode(const esg_bam_batch* b, const esg_mapping* m,
       if (hits[maps[k].first_hit + h].reference >= n_refs)
         return berr(ESG_ERR_BAD_ARGUMENT, "a hit's reference is past ref_names");
   std::vector<std::vector<uint8_t>> enc(n);
-  std::vector<uint32_t> count(n, 0), unmapped(n, 0);
+  std::vector<uint32_t> count(n, 0), unmapped(n, 0), unique(n, 0);
   std::atomic<int> bad{0};
   parallel_for((n + 63) / 64, threads_or(threads), [&](size_t chunk) {
     std::vector<std::pair<uint32_t, uint32_t>> fields;
@@ -1091,6 +1092,7 @@ esg_status esg_bam_encode(const esg_bam_batch* b, const esg_mapping* m,
                     rm.n_tied == 1 ? 60 : 0, cigar, flag, name, x.name_len, seq4.data(), x.l_seq,
                     qual.data(), have_qual, aux);
       count[k] = 1;
+      unique[k] = rm.n_tied == 1;
       if (opt->secondary) {
         // the read group of the input record, if any
         std::vector<uint8_t> rg;
@@ -1128,6 +1130,8 @@ esg_status esg_bam_encode(const esg_bam_batch* b, const esg_mapping* m,
     r->bytes.insert(r->bytes.end(), enc[k].begin(), enc[k].end());
     r->n_records += count[k];
     r->n_unmapped += unmapped[k];
+    r->n_unique += unique[k];
+    r->n_tied += !unmapped[k] && !unique[k];
   }
   *out = r;
   return ESG_OK;
@@ -1161,6 +1165,7 @@ esg_status esg_bam_encode_pairs(const esg_bam_batch* b, const esg_mapping* m,
   const size_t np = n / 2;
   std::vector<std::vector<uint8_t>> enc(np);
   std::vector<uint32_t> count(np, 0);
+  std::vector<uint8_t> outcome(n, 0);  // per mate: 0 unmapped, 1 unique, 2 tied
   std::atomic<int> bad{0};
   static const char kOwned[7][2] = {{'N', 'M'}, {'M', 'D'}, {'A', 'S'}, {'X', 'S'},
                                     {'X', 'A'}, {'M', 'C'}, {'a', 'd'}};
@@ -1322,6 +1327,8 @@ esg_status esg_bam_encode_pairs(const esg_bam_batch* b, const esg_mapping* m,
         }
       }
       std::vector<uint8_t>& o = enc[p];
+      for (int k = 0; k < 2; ++k)
+        outcome[2 * p + k] = !pl[k].primary ? 0 : (pl[k].unique ? 1 : 2);
       for (int k = 0; k < 2; ++k) {
         const InRec& x = b->recs[2 * p + k];
         const Mate& q = mt[k];
@@ -1374,6 +1381,11 @@ esg_status esg_bam_encode_pairs(const esg_bam_batch* b, const esg_mapping* m,
     r->bytes.insert(r->bytes.end(), enc[p].begin(), enc[p].end());
     r->n_records += count[p];
   }
+  for (uint8_t oc : outcome) {
+    r->n_unmapped += oc == 0;
+    r->n_unique += oc == 1;
+    r->n_tied += oc == 2;
+  }
   *out = r;
   return ESG_OK;
 }
@@ -1384,6 +1396,15 @@ const uint8_t* esg_bam_records_bytes(const esg_bam_records* r, uint64_t* n_bytes
   if (n_bytes) *n_bytes = r->bytes.size();
   if (n_records) *n_records = r->n_records;
   return r->bytes.data();
+}
+
+esg_status esg_bam_records_outcomes(const esg_bam_records* r, uint64_t* unique, uint64_t* tied,
+                                    uint64_t* unmapped) {
+  if (!r) return berr(ESG_ERR_BAD_ARGUMENT, "NULL records");
+  if (unique) *unique = r->n_unique;
+  if (tied) *tied = r->n_tied;
+  if (unmapped) *unmapped = r->n_unmapped;
+  return ESG_OK;
 }
 
 void esg_bam_records_free(esg_bam_records* r) { delete r; }

@@ -677,6 +677,10 @@ esg_status esg_bam_encode_pairs(const esg_bam_batch* batch, const esg_mapping* m
                                 esg_bam_records** out);
 const uint8_t* esg_bam_records_bytes(const esg_bam_records* records, uint64_t* n_bytes,
                                      uint32_t* n_records);
+/* How the batch's reads (mates, for pairs) went, the CLI's run summary
+ * (Outcome, align.rs:1077-1082, 2360-2372): a unique best, a tie, unmapped. */
+esg_status esg_bam_records_outcomes(const esg_bam_records* records, uint64_t* unique,
+                                    uint64_t* tied, uint64_t* unmapped);
 void esg_bam_records_free(esg_bam_records* records);
 /* A BGZF BAM writer: header, then the records of the chunks pushed, in the
  * order of their sequence numbers 0, 1, ... whatever order they arrive in;

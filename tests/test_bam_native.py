@@ -235,6 +235,12 @@ def test_align_bam_pipeline_writes_the_reference_record_stream(oracle, tmp_path,
     assert n["records"] == want["records"]
     assert format(B.fnv1a64(record_stream(path)), "016x") == want["fnv1a64"]
     assert set(st) == {"read", "map", "encode", "write"}
+    # the run summary (Outcome, align.rs:1077-1082): from the oracle's mappings
+    ms = oracle_mappings(oracle, input_records(), o)
+    assert (n["unique"], n["tied"], n["unmapped"]) == (
+        sum(1 for m in ms if m["hits"] and m["n_tied"] == 1),
+        sum(1 for m in ms if m["hits"] and m["n_tied"] > 1),
+        sum(1 for m in ms if not m["hits"]))
 
 
 def test_corrupt_records_are_errors(tmp_path):

@@ -145,6 +145,39 @@ def test_paired_records_equal_the_oracle(oracle, tmp_path, extra):
     assert library_records(oracle, o, p1, p2) == want
 
 
+def test_paired_outcomes(oracle, tmp_path):
+    """The run summary per mate (Outcome, align.rs:1420-1423): the oracle's
+    placements give each mate unique, tied or unmapped."""
+    from oracle import bam as B
+    o = opts(both=True)
+    r1, r2 = fastq_texts()
+    p1, p2 = str(tmp_path / "r1.fq"), str(tmp_path / "r2.fq")
+    open(p1, "wb").write(r1)
+    open(p2, "wb").write(r2)
+    refs, _ = fixture()
+    names = [r["name"] for r in refs]
+    got = {"unique": 0, "tied": 0, "unmapped": 0}
+    want = dict(got)
+    with EB.PairReader(p1, p2) as rd:
+        for b in rd.batches(100):
+            codes, off, lens = b.reads()
+            ads, _ = A.pair_adapters((codes, off, lens), A.config())
+            letters = [bytes(b"ACGTN"[int(c)] for c in codes[int(off[k]):int(off[k] + lens[k])])
+                       for k in range(len(lens))]
+            pms = oracle_pms(oracle, o, [(letters[2 * i], letters[2 * i + 1])
+                                         for i in range(len(lens) // 2)],
+                             [(int(ads[2 * i]), int(ads[2 * i + 1]))
+                              for i in range(len(lens) // 2)])
+            rec = EB.encode_pairs(b, pair_mappings_from_oracle(pms), names, ads)
+            for k, v in rec.outcomes().items():
+                got[k] += v
+            for pm in pms:
+                for pl in B.pair_placements(pm)[0]:
+                    want["unmapped" if pl["primary"] is None else
+                         ("unique" if pl["unique"] else "tied")] += 1
+    assert got == want and sum(got.values()) == 18
+
+
 @pytest.mark.parametrize("form", ["interleaved", "ubam", "gz_suffixed"])
 def test_paired_input_forms(oracle, tmp_path, form):
     """align_paired.rs:462-505 through the library's readers: interleaved
