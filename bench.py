@@ -328,12 +328,18 @@ def map_stage(g, refs, reads, scoring, local, skip_cpu):
     MD / NM, all in C on every thread) on a bounded sample."""
     g.map_reads(reads.slice(0, 1000).tuple(), both_strands=True)  # warm-up
     t0 = time.perf_counter()
-    m = g.map_reads(reads.tuple(), both_strands=True)
+    h = g.map_reads(reads.tuple(), both_strands=True, raw=True)
     dt = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    m = h.mappings()  # the arrays copied out to Python, as the Python binding returns them
+    dt_copy = time.perf_counter() - t1
+    h.free()
     mapped = int((m.reads["n_hits"] > 0).sum())
     out = {"reads": len(reads), "seconds": round(dt, 4), "reads_per_s": len(reads) / dt,
+           "reads_per_s_with_python_copy": len(reads) / (dt + dt_copy),
            "mapped": mapped, "hits": int(m.hits.size),
-           "options": "both strands, min_score 0, every tie traced, MD/NM without letters"}
+           "options": "both strands, min_score 0, every tie traced, MD/NM without letters; "
+                      "the mapping as the C ABI returns it (esg_map_reads)"}
     if not skip_cpu:
         from oracle import oracle as O
         n = min(len(reads), 40_000)
@@ -669,18 +675,25 @@ def map_pairs_stage(g, refs, pairs, scoring, local, skip_cpu, n=100_000):
         part = sub.slice(2 * k0, 2 * k1)
         _, aligned = adapter.pair_adapters(part.tuple())
         c, o, _ = part.tuple()
-        return g.map_pairs((c, o, aligned), min_score=40, max_insert=500, both_strands=True)
+        return g.map_pairs((c, o, aligned), min_score=40, max_insert=500, both_strands=True,
+                           raw=True)
 
-    run(0, 1000)  # warm-up
+    run(0, 1000).free()  # warm-up
     t0 = time.perf_counter()
-    m = run(0, len(sub) // 2)
+    h = run(0, len(sub) // 2)
     dt = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    m = h.mappings(paired=True)  # copied out to Python, as the Python binding returns it
+    dt_copy = time.perf_counter() - t1
+    h.free()
     n_pairs = len(sub) // 2
     proper = int((m.pairs["flags"] & 1).sum())
     out = {"pairs": n_pairs, "seconds": round(dt, 4), "pairs_per_s": n_pairs / dt,
+           "pairs_per_s_with_python_copy": n_pairs / (dt + dt_copy),
            "proper": proper, "pair_hits": int(m.pair_hits.size),
            "options": "trim + map: min_score 40, max_insert 500, both template strands, "
-                      "every tie traced, MD/NM without letters"}
+                      "every tie traced, MD/NM without letters; the mapping as the C ABI "
+                      "returns it (esg_map_pairs)"}
     if not skip_cpu:
         from oracle import oracle as O
         k = min(n_pairs, 20_000)
