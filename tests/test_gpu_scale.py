@@ -121,12 +121,16 @@ def test_bam_run_at_scale_equals_the_oracle(c2, tmp_path):
     src, dst = str(tmp_path / "in.bam"), str(tmp_path / "out.bam")
     with open(src, "wb") as fh:
         fh.write(bgzf(b"BAM\1" + bytes(8) + b"".join(recs)))
+    srt = str(tmp_path / "sorted.bam")
     gs = [GpuScorer(refs, Scoring(2, -1, -10, -1), Mode.LOCAL) for _ in range(2)]
     try:
         n = EB.align_bam(gs, src, dst, names, letters, both_strands=True, secondary=True)
+        EB.align_bam(gs, src, srt, names, letters, both_strands=True, secondary=True,
+                     sort_coordinate=True)
     finally:
         for g in gs:
             g.close()
+    from tests.test_bam_fastx import split_records
     from tests.test_bam_native import record_stream
     got = record_stream(dst)
     res, jobs, al, ops, mds, nm, _ = O.cpu_map_reads(
@@ -137,6 +141,8 @@ def test_bam_run_at_scale_equals_the_oracle(c2, tmp_path):
     want = b"".join(x for r, m in zip(inputs, maps) for x in B.build_records(r, m, names, True))
     assert n["reads"] == len(sub)
     assert got == want
+    # and coordinate-sorted: the CLI's stable sort (align.rs:2406-2450)
+    assert record_stream(srt) == b"".join(B.coordinate_order(split_records(want)))
 
 
 def test_paired_bam_run_at_scale_equals_the_oracle(tmp_path):
