@@ -117,6 +117,8 @@ def args_parse():
     ap.add_argument("--rates", default="10,30,100,300,1000,2000",
                     help="c5: Poisson arrival rates swept (requests/s)")
     ap.add_argument("--requests", type=int, default=1000, help="c5: requests per rate")
+    ap.add_argument("--max-batch-cells", type=int, default=0,
+                    help="c5: DP cells per server batch at most (0: the server's default)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch each batch's kernels one by one instead of as one CUDA graph")
     ap.add_argument("--split", type=int, default=-1,
@@ -1306,7 +1308,7 @@ def run_c5(a, ctx, rank):
     per_rate = []
     verify = []
     clocks = None
-    with Server(scorers) as sv:
+    with Server(scorers, max_batch_cells=a.max_batch_cells) as sv:
         for ri, rate in enumerate(rates):
             # the same requests (sizes, panels, modes, strands, reads) at
             # every rate, so rates differ only in arrival times; the
@@ -1416,7 +1418,8 @@ def run_c5(a, ctx, rank):
             "C5: serving, Poisson arrivals at " + a.rates + " req/s, requests of log-uniform "
             "1-50 000 C2-length reads for panel A (164 x 70-180 nt) or B (2000 x 300 nt), "
             "local or semi-global 2,-1,-10,-1, forward or both strands, through esg_server",
-            {"requests_per_rate": a.requests, "panels": {k: len(v) for k, v in panels.items()}},
+            {"requests_per_rate": a.requests, "panels": {k: len(v) for k, v in panels.items()},
+             "max_batch_cells": a.max_batch_cells or "server default (1.5e11)"},
             {"value": best["gcups"], "unit": "GCUPS", "h2d_bytes_per_step": best["h2d_bytes"],
              "d2h_bytes_per_step": best["d2h_bytes"],
              "note": "serving is end to end: host requests in, results out"},
