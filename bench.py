@@ -549,6 +549,15 @@ def bam_stage(g, refs, reads, batch_size=50_000, cpu_reads=0, scoring=HEADLINE[0
                          batch_size=batch_size, max_read_len=1000, stats=st)
         dt = time.perf_counter() - t0
         out_bytes = os.path.getsize(dst)
+        # the same run with the blocks deflated on the host threads (zlib 6)
+        sh = {}
+        t0 = time.perf_counter()
+        EB.align_bam(g, src, dst, names, letters, both_strands=True, batch_size=batch_size,
+                     max_read_len=1000, stats=sh, deflate_on_device=False)
+        dh = time.perf_counter() - t0
+        host = {"reads_per_s": n["reads"] / dh, "seconds": round(dh, 3),
+                "output_bgzf_bytes": os.path.getsize(dst),
+                "stage_seconds": {k: round(v, 3) for k, v in sh.items()}}
         cpu = None
         if cpu_reads:
             small = os.path.join(tmp, "cpu.bam")
@@ -570,7 +579,8 @@ def bam_stage(g, refs, reads, batch_size=50_000, cpu_reads=0, scoring=HEADLINE[0
            "scorers": len(g) if isinstance(g, (list, tuple)) else 1,
            "options": "both strands, min_score 0, every tie traced, MD/NM from letters, "
                       "input order; read, map (one thread per scorer) and encode/write "
-                      "overlapped"}
+                      "overlapped; output blocks deflated on the device",
+           "host_deflate": host}
     if cpu:
         out["cpu"] = cpu
     return out
@@ -634,6 +644,14 @@ def bam_pairs_stage(g, refs, pairs, n=500_000, batch_size=50_000, cpu_pairs=0):
         dt = time.perf_counter() - t0
         out_bytes = os.path.getsize(dst)
         in_bytes = os.path.getsize(p1) + os.path.getsize(p2)
+        sh = {}
+        t0 = time.perf_counter()
+        EB.align_pairs_bam(g, p1, p2, dst, names, letters, min_score=40,
+                           batch_size=batch_size, stats=sh, deflate_on_device=False)
+        dh = time.perf_counter() - t0
+        host = {"pairs_per_s": r["reads"] / 2 / dh, "seconds": round(dh, 3),
+                "output_bgzf_bytes": os.path.getsize(dst),
+                "stage_seconds": {k: round(v, 3) for k, v in sh.items()}}
         cpu = None
         if cpu_pairs:
             c1, c2 = os.path.join(tmp, "c1.fq"), os.path.join(tmp, "c2.fq")
@@ -654,7 +672,8 @@ def bam_pairs_stage(g, refs, pairs, n=500_000, batch_size=50_000, cpu_pairs=0):
            "stage_seconds": {k: round(v, 3) for k, v in st.items()},
            "options": "semi-global, --min-score 40, max insert 500, forward template strand, "
                       "TruSeq adapters trimmed, every tie traced, MD/NM from letters, "
-                      "input order"}
+                      "input order; output blocks deflated on the device",
+           "host_deflate": host}
     if cpu:
         out["cpu"] = cpu
     return out

@@ -269,6 +269,10 @@ SIGNATURES = {
                                         C.POINTER(C.c_void_p)]),
     "esg_bam_writer_push": (C.c_int32, [C.c_void_p, C.c_uint64, C.c_void_p]),
     "esg_bam_writer_close": (C.c_int32, [C.c_void_p]),
+    "esg_bam_writer_use_device": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "esg_bam_writer_blocks": (C.c_int32, [C.c_void_p, _u64p, _u64p]),
+    "esg_bgzf_deflate_host": (C.c_uint32, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "esg_bgzf_code_lengths": (C.c_int32, [_u32p, C.c_uint32, C.c_uint32, C.c_void_p]),
     "esg_score_rows_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_uint32, C.POINTER(EsgScoring), C.c_int32,

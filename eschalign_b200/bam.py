@@ -274,10 +274,11 @@ def encode_pairs(batch: BamBatch, mapping, ref_names, adapter_bases=None,
 
 class BamWriter:
     """esg_bam_writer_*: header, then pushed chunks in sequence order (or in
-    coordinate order at close), BGZF-compressed on host threads."""
+    coordinate order at close), BGZF-compressed on host threads, or on
+    `device` (esg_bam_writer_use_device: one warp per block)."""
 
     def __init__(self, path: str, header_text: bytes, ref_names, ref_lens,
-                 sort_coordinate: bool = False, threads: int = 0):
+                 sort_coordinate: bool = False, threads: int = 0, device: int | None = None):
         self._lib = _lib()
         names, n = _names(ref_names)
         lens = np.ascontiguousarray(ref_lens, dtype=np.uint32)
@@ -286,6 +287,20 @@ class BamWriter:
             path.encode(), header_text, names, _ptr(lens, C.c_uint32), n,
             int(bool(sort_coordinate)), threads, C.byref(h)))
         self._h = h
+        self.device = device
+        if device is not None:
+            try:
+                _check(self._lib, self._lib.esg_bam_writer_use_device(h, int(device)))
+            except Exception:
+                self._lib.esg_bam_writer_close(h)
+                self._h = None
+                raise
+
+    def blocks(self) -> tuple:
+        """(blocks the device compressed so far, of them stored)."""
+        b, s = C.c_uint64(), C.c_uint64()
+        _check(self._lib, self._lib.esg_bam_writer_blocks(self._h, C.byref(b), C.byref(s)))
+        return b.value, s.value
 
     def push(self, seq: int, records: BamRecords):
         _check(self._lib, self._lib.esg_bam_writer_push(self._h, seq, records._h))
@@ -344,8 +359,17 @@ def _scorers(scorer):
     return list(scorer) if isinstance(scorer, (list, tuple)) else [scorer]
 
 
+def _deflate_device(scorers, deflate_on_device):
+    """The device the writer compresses on: the first scorer's, when it has
+    one and deflate_on_device is set."""
+    if not deflate_on_device:
+        return None
+    dev = getattr(scorers[0], "device", None)
+    return dev if isinstance(dev, int) else None
+
+
 def _run(reader, batches, scorers, map_batch, encode_batch, out_path, ref_names, ref_lens,
-         sort_coordinate, threads, stats, depth):
+         sort_coordinate, threads, stats, depth, deflate_device=None):
     """Read, map and encode/write on their own threads (the CLI's reader, GPU
     feeder and workers, align.rs:2078-2335): reading batch k + 1, mapping
     batch k, building and writing the records of batch k - 1, at most
@@ -375,7 +399,8 @@ def _run(reader, batches, scorers, map_batch, encode_batch, out_path, ref_names,
 
     with reader, BamWriter(out_path, header_text(ref_names, ref_lens, sort_coordinate,
                                                  reader.header_text),
-                           ref_names, ref_lens, sort_coordinate, threads) as wr, \
+                           ref_names, ref_lens, sort_coordinate, threads,
+                           deflate_device) as wr, \
             ThreadPoolExecutor(1) as rpool, ThreadPoolExecutor(len(scorers)) as mpool, \
             ThreadPoolExecutor(1) as opool:
         def read_next():
@@ -429,7 +454,8 @@ def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
               min_score: int = 0, max_ties: int | None = None, both_strands: bool = False,
               secondary: bool = False, sort_coordinate: bool = False,
               max_read_len: int = 1000, batch_size: int = 50_000, threads: int = 0,
-              stats: dict | None = None, depth: int = 2, read_ids: str | None = None) -> dict:
+              stats: dict | None = None, depth: int = 2, read_ids: str | None = None,
+              deflate_on_device: bool = True) -> dict:
     """The CLI's unpaired run (align.rs:1822-2250, the --device gpu path) over
     a scorer: every batch of `in_path` (BAM, FASTA or FASTQ) mapped on the
     device (map_reads_scored with min_score / max_ties / both strands), its
@@ -440,15 +466,18 @@ def align_bam(scorer, in_path: str, out_path: str, ref_names, ref_letters,
     than the wall time).  read_ids: --read-ids, a file of the names kept.
     `scorer` may be a list of scorers over the same panel and scoring: each
     maps on its own thread, so the device scores one batch while the host
-    finishes another (the records do not depend on it)."""
+    finishes another (the records do not depend on it).  With
+    deflate_on_device, the output's BGZF blocks are compressed on the
+    scorer's device (BamWriter's `device`); the records are the same."""
     rd = BamReader(in_path, threads, read_ids)
-    return _run(rd, rd.batches(batch_size, max_read_len), _scorers(scorer),
+    scs = _scorers(scorer)
+    return _run(rd, rd.batches(batch_size, max_read_len), scs,
                 lambda sc, b: sc.map_reads(b.reads(), min_score=min_score, max_ties=max_ties,
                                            both_strands=both_strands, ref_letters=ref_letters,
                                            raw=True),
                 lambda b, m: encode(b, m, ref_names, secondary, threads),
                 out_path, ref_names, [len(r) for r in ref_letters], sort_coordinate, threads,
-                stats, depth)
+                stats, depth, _deflate_device(scs, deflate_on_device))
 
 
 DEFAULT_ADAPTERS = "truseq"
@@ -460,7 +489,7 @@ def align_pairs_bam(scorer, path1: str, path2: str | None, out_path: str, ref_na
                     sort_coordinate: bool = False, max_read_len: int = 1000,
                     adapters=DEFAULT_ADAPTERS, batch_size: int = 50_000, threads: int = 0,
                     stats: dict | None = None, depth: int = 2,
-                    read_ids: str | None = None) -> dict:
+                    read_ids: str | None = None, deflate_on_device: bool = True) -> dict:
     """The CLI's paired run (align.rs:1613-1750 over run, 1822-2250): pairs
     from two mate files, or one interleaved / paired-BAM file (path2 None),
     each mate trimmed of its 3' adapter (pair_adapters; `adapters` an
@@ -493,6 +522,8 @@ def align_pairs_bam(scorer, path1: str, path2: str | None, out_path: str, ref_na
     def encode_batch(b, m):
         return encode_pairs(b, m, ref_names, state.pop(id(b)), secondary, threads)
 
-    return _run(rd, rd.batches((batch_size + 1) // 2), _scorers(scorer), map_batch,
+    scs = _scorers(scorer)
+    return _run(rd, rd.batches((batch_size + 1) // 2), scs, map_batch,
                 encode_batch, out_path,
-                ref_names, [len(r) for r in ref_letters], sort_coordinate, threads, stats, depth)
+                ref_names, [len(r) for r in ref_letters], sort_coordinate, threads, stats, depth,
+                _deflate_device(scs, deflate_on_device))

@@ -27,6 +27,7 @@
 // several host threads.
 #include "../../include/eschalign_b200.h"
 
+#include <cuda_runtime.h>
 #include <zlib.h>
 
 #include <algorithm>
@@ -41,6 +42,8 @@
 #include <thread>
 #include <unordered_set>
 #include <vector>
+
+#include "esg_deflate.cuh"
 
 extern "C" void esg_internal_set_error(esg_status st, const char* msg);
 
@@ -141,6 +144,28 @@ esg_status inflate_blocks(const std::vector<uint8_t>& data, const std::vector<si
   return ESG_OK;
 }
 
+// A BGZF member: header, the DEFLATE data cdata[0, clen), the CRC32 and
+// length of the `n` bytes it holds.
+void bgzf_member(const uint8_t* cdata, size_t clen, uint32_t crc, size_t n,
+                 std::vector<uint8_t>& out) {
+  const uint8_t head[18] = {0x1f, 0x8b, 8, 4, 0, 0, 0, 0, 0, 0xff, 6, 0, 0x42, 0x43, 2, 0, 0, 0};
+  out.assign(head, head + 18);
+  const uint16_t bsize = (uint16_t)(18 + clen + 8 - 1);
+  memcpy(out.data() + 16, &bsize, 2);
+  out.insert(out.end(), cdata, cdata + clen);
+  put32(out, crc);
+  put32(out, (uint32_t)n);
+}
+
+// One stored DEFLATE block (BFINAL, BTYPE 00, LEN, NLEN, the bytes) as a
+// BGZF member.
+void stored_member(const uint8_t* src, size_t n, uint32_t crc, std::vector<uint8_t>& out) {
+  std::vector<uint8_t> c = {1, (uint8_t)(n & 0xff), (uint8_t)(n >> 8), (uint8_t)(~n & 0xff),
+                            (uint8_t)((~n >> 8) & 0xff)};
+  c.insert(c.end(), src, src + n);
+  bgzf_member(c.data(), c.size(), crc, n, out);
+}
+
 // One BGZF block holding `n` bytes of `src`.
 void deflate_block(const uint8_t* src, size_t n, int level, std::vector<uint8_t>& out) {
   z_stream z{};
@@ -153,13 +178,7 @@ void deflate_block(const uint8_t* src, size_t n, int level, std::vector<uint8_t>
   deflate(&z, Z_FINISH);
   const size_t clen = c.size() - z.avail_out;
   deflateEnd(&z);
-  const uint8_t head[18] = {0x1f, 0x8b, 8, 4, 0, 0, 0, 0, 0, 0xff, 6, 0, 0x42, 0x43, 2, 0, 0, 0};
-  out.assign(head, head + 18);
-  const uint16_t bsize = (uint16_t)(18 + clen + 8 - 1);
-  memcpy(out.data() + 16, &bsize, 2);
-  out.insert(out.end(), c.data(), c.data() + clen);
-  put32(out, (uint32_t)crc32(0L, src, (uInt)n));
-  put32(out, (uint32_t)n);
+  bgzf_member(c.data(), clen, (uint32_t)crc32(0L, src, (uInt)n), n, out);
 }
 
 // ---------------------------------------------------------------- records
@@ -1412,6 +1431,28 @@ void esg_bam_records_free(esg_bam_records* r) { delete r; }
 }  // extern "C"
 
 // ===================================================================== writer
+// Blocks deflated on a device (esg_deflate.cuh): one job in flight.  A job
+// is the whole blocks of one drain: uploaded, compressed by k_bgzf_deflate
+// on a stream of the highest priority, and copied back; the next drain (or
+// the close) writes them, so the device's work overlaps the host's next
+// chunk.  Each block's CRC32 is computed on the host while the device
+// compresses.
+struct DeviceDeflate {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  uint8_t* d_in = nullptr;
+  uint32_t* d_tok = nullptr;
+  uint32_t* d_out = nullptr;
+  uint32_t* d_len = nullptr;
+  uint8_t* h_out = nullptr;  // pinned
+  uint32_t* h_len = nullptr;  // pinned
+  size_t cap = 0;             // blocks the buffers hold
+  size_t nb = 0;              // blocks of the job in flight (0: none)
+  size_t bytes = 0;           // its input bytes
+  std::vector<uint32_t> crc;
+  uint64_t blocks = 0, stored = 0;  // blocks written, of them stored
+};
+
 struct esg_bam_writer {
   FILE* f = nullptr;
   uint32_t threads = 1;
@@ -1422,12 +1463,137 @@ struct esg_bam_writer {
   uint64_t next = 0;
   std::vector<std::vector<uint8_t>> buckets;  // coordinate sort: per reference, + unmapped
   bool failed = false;
+  std::unique_ptr<DeviceDeflate> dev;
 };
+
+static esg_status cuda_fail(esg_bam_writer* w, cudaError_t e, const char* what) {
+  w->failed = true;
+  return berr(ESG_ERR_DRIVER, std::string("device deflate: ") + what + ": " +
+                                  cudaGetErrorString(e));
+}
+
+static void device_free(DeviceDeflate& D) {
+  if (D.device < 0) return;
+  cudaSetDevice(D.device);
+  if (D.stream) cudaStreamSynchronize(D.stream);
+  cudaFree(D.d_in);
+  cudaFree(D.d_tok);
+  cudaFree(D.d_out);
+  cudaFree(D.d_len);
+  cudaFreeHost(D.h_out);
+  cudaFreeHost(D.h_len);
+  if (D.stream) cudaStreamDestroy(D.stream);
+  D = DeviceDeflate{};
+}
+
+// Write the blocks of the job in flight.
+static esg_status device_finish(esg_bam_writer* w) {
+  DeviceDeflate& D = *w->dev;
+  if (!D.nb) return ESG_OK;
+  cudaError_t e = cudaSetDevice(D.device);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(D.stream);
+  if (e != cudaSuccess) return cuda_fail(w, e, "compressing");
+  namespace dz = esg_deflate;
+  std::vector<uint8_t> member, raw;
+  for (size_t i = 0; i < D.nb; ++i) {
+    const size_t n = std::min<size_t>(kBgzfMaxIn, D.bytes - i * kBgzfMaxIn);
+    const uint32_t clen = D.h_len[i];
+    if (clen == dz::kStored) {  // incompressible: the input, from the device
+      raw.resize(n);
+      e = cudaMemcpyAsync(raw.data(), D.d_in + i * kBgzfMaxIn, n, cudaMemcpyDeviceToHost,
+                          D.stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(D.stream);
+      if (e != cudaSuccess) return cuda_fail(w, e, "reading a stored block back");
+      stored_member(raw.data(), n, D.crc[i], member);
+      ++D.stored;
+    } else {
+      if (clen > n + 5) {
+        w->failed = true;
+        return berr(ESG_ERR_DRIVER, "device deflate: block length out of range");
+      }
+      bgzf_member(D.h_out + i * dz::kSlotBytes, clen, D.crc[i], n, member);
+    }
+    if (fwrite(member.data(), 1, member.size(), w->f) != member.size()) {
+      w->failed = true;
+      return berr(ESG_ERR_DRIVER, "writing the BAM file failed");
+    }
+  }
+  D.blocks += D.nb;
+  D.nb = 0;
+  return ESG_OK;
+}
+
+// Start a job on w->pending[0, whole).
+static esg_status device_start(esg_bam_writer* w, size_t whole) {
+  DeviceDeflate& D = *w->dev;
+  namespace dz = esg_deflate;
+  const size_t nb = (whole + kBgzfMaxIn - 1) / kBgzfMaxIn;
+  cudaError_t e = cudaSetDevice(D.device);
+  if (e != cudaSuccess) return cuda_fail(w, e, "selecting the device");
+  if (!D.stream) {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    e = cudaStreamCreateWithPriority(&D.stream, cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(dz::k_bgzf_deflate, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(dz::BlockState));
+    if (e != cudaSuccess) return cuda_fail(w, e, "creating the stream");
+  }
+  if (nb > D.cap) {
+    cudaFree(D.d_in);
+    cudaFree(D.d_tok);
+    cudaFree(D.d_out);
+    cudaFree(D.d_len);
+    cudaFreeHost(D.h_out);
+    cudaFreeHost(D.h_len);
+    D.d_in = nullptr;
+    D.d_tok = D.d_out = D.d_len = D.h_len = nullptr;
+    D.h_out = nullptr;
+    D.cap = 0;
+    const size_t cap = std::max<size_t>(nb, 64);
+    e = cudaMalloc(&D.d_in, cap * kBgzfMaxIn);
+    if (e == cudaSuccess) e = cudaMalloc(&D.d_tok, cap * dz::kTokensPerBlock * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&D.d_out, cap * dz::kSlotBytes);
+    if (e == cudaSuccess) e = cudaMalloc(&D.d_len, cap * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaHostAlloc(&D.h_out, cap * dz::kSlotBytes, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(&D.h_len, cap * sizeof(uint32_t), cudaHostAllocDefault);
+    if (e != cudaSuccess) return cuda_fail(w, e, "allocating buffers");
+    D.cap = cap;
+  }
+  e = cudaMemcpyAsync(D.d_in, w->pending.data(), whole, cudaMemcpyHostToDevice, D.stream);
+  if (e != cudaSuccess) return cuda_fail(w, e, "uploading");
+  dz::k_bgzf_deflate<<<(unsigned)nb, dz::kLanes, sizeof(dz::BlockState), D.stream>>>(
+      D.d_in, whole, D.d_tok, D.d_out, D.d_len);
+  e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(D.h_len, D.d_len, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                        D.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(D.h_out, D.d_out, nb * dz::kSlotBytes, cudaMemcpyDeviceToHost, D.stream);
+  if (e != cudaSuccess) return cuda_fail(w, e, "launching");
+  D.crc.assign(nb, 0);
+  parallel_for(nb, w->threads, [&](size_t i) {
+    const size_t n = std::min<size_t>(kBgzfMaxIn, whole - i * kBgzfMaxIn);
+    D.crc[i] = (uint32_t)crc32(0L, w->pending.data() + i * kBgzfMaxIn, (uInt)n);
+  });
+  D.nb = nb;
+  D.bytes = whole;
+  return ESG_OK;
+}
 
 // Compress every whole block of w->pending (all of it with `flush`) and
 // write them in order.
 static esg_status drain(esg_bam_writer* w, bool flush) {
   const size_t whole = flush ? w->pending.size() : w->pending.size() / kBgzfMaxIn * kBgzfMaxIn;
+  if (w->dev) {
+    esg_status st = device_finish(w);
+    if (st == ESG_OK && whole) {
+      st = device_start(w, whole);
+      if (st == ESG_OK) w->pending.erase(w->pending.begin(), w->pending.begin() + (long)whole);
+    }
+    if (st == ESG_OK && flush) st = device_finish(w);
+    return st;
+  }
   if (!whole) return ESG_OK;
   const size_t nb = (whole + kBgzfMaxIn - 1) / kBgzfMaxIn;
   std::vector<std::vector<uint8_t>> blocks(nb);
@@ -1538,8 +1704,71 @@ esg_status esg_bam_writer_close(esg_bam_writer* w) {
   if (st == ESG_OK && fwrite(kBgzfEof, 1, sizeof kBgzfEof, w->f) != sizeof kBgzfEof)
     st = berr(ESG_ERR_DRIVER, "writing the BAM file failed");
   if (fclose(w->f) != 0 && st == ESG_OK) st = berr(ESG_ERR_DRIVER, "closing the BAM file failed");
+  if (w->dev) device_free(*w->dev);
   delete w;
   return st;
+}
+
+esg_status esg_bam_writer_use_device(esg_bam_writer* w, int32_t device) {
+  if (!w) return berr(ESG_ERR_BAD_ARGUMENT, "NULL writer");
+  if (w->failed) return berr(ESG_ERR_DRIVER, "the writer failed earlier");
+  if (device < 0) {  // back to the host threads
+    if (w->dev) {
+      const esg_status st = device_finish(w);
+      device_free(*w->dev);
+      w->dev.reset();
+      return st;
+    }
+    return ESG_OK;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device >= count)
+    return berr(ESG_ERR_BAD_ARGUMENT, "esg_bam_writer_use_device: no such device");
+  if (w->dev && w->dev->device != device) {
+    const esg_status st = device_finish(w);
+    if (st != ESG_OK) return st;
+    device_free(*w->dev);
+    w->dev.reset();
+  }
+  if (!w->dev) {
+    w->dev.reset(new DeviceDeflate);
+    w->dev->device = device;
+  }
+  return ESG_OK;
+}
+
+esg_status esg_bam_writer_blocks(const esg_bam_writer* w, uint64_t* blocks,
+                                 uint64_t* stored) {
+  if (!w) return berr(ESG_ERR_BAD_ARGUMENT, "NULL writer");
+  if (blocks) *blocks = w->dev ? w->dev->blocks : 0;
+  if (stored) *stored = w->dev ? w->dev->stored : 0;
+  return ESG_OK;
+}
+
+// The device deflate's steps run on the host, lane by lane: one block of at
+// most 0xff00 bytes into `out` (65536 bytes, 4-byte aligned).  Returns the
+// DEFLATE length, 0xffffffff for "store it", 0 on a bad argument.  A check
+// of the steps for tests; the writer never calls it.
+uint32_t esg_bgzf_deflate_host(const uint8_t* src, uint32_t n, uint8_t* out) {
+  namespace dz = esg_deflate;
+  if (!src || !out || n == 0 || n > dz::kBlockIn) return 0;
+  std::unique_ptr<dz::BlockState> S(new dz::BlockState);
+  std::vector<uint32_t> tok(dz::kTokensPerBlock);
+  return dz::deflate_block_host(src, n, out, *S, tok.data());
+}
+
+// The compressor's code lengths on the host: freq[0, n) (n <= 288) to
+// lengths of at most `limit` (1..15) bits.  Returns 0, or -1 on a bad
+// argument.  A check of the step for tests.
+int32_t esg_bgzf_code_lengths(const uint32_t* freq, uint32_t n, uint32_t limit, uint8_t* len) {
+  namespace dz = esg_deflate;
+  if (!freq || !len || n < 2 || n > dz::kMaxSyms || limit < 1 || limit > 15) return -1;
+  uint64_t m = 0;
+  for (uint32_t i = 0; i < n; ++i) m += freq[i] != 0;
+  if (m > (1ull << limit)) return -1;  // more symbols than codes of that length
+  std::unique_ptr<dz::BlockState> S(new dz::BlockState);
+  dz::huffman_lengths(freq, n, limit, len, *S);
+  return 0;
 }
 
 }  // extern "C"

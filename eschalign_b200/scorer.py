@@ -306,6 +306,7 @@ class GpuScorer:
         self.scoring = scoring
         self.mode = Mode(mode)
         self.cap = int(tie_capacity)
+        self.device = int(device)
         codes, off, lens = panel.packed()
         self._panel_arrays = (codes, off, lens)
         self._kernel = int(kernel)

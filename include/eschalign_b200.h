@@ -696,6 +696,30 @@ esg_status esg_bam_writer_push(esg_bam_writer* writer, uint64_t seq,
 /* Writes what is left (the sorted records), the end-of-file block, and
  * frees the writer. */
 esg_status esg_bam_writer_close(esg_bam_writer* writer);
+/* Deflate the writer's blocks on `device` from now on (a negative device:
+ * on the host threads again).  No counterpart in the reference, whose writer
+ * deflates on host threads (noodles' MultithreadedWriter, align.rs:2066).
+ * One warp per 0xff00-byte block: greedy LZ77 over 2040-byte stripes, one
+ * dynamic-Huffman DEFLATE block per BGZF block, an incompressible block
+ * stored; the file is a valid BGZF BAM whose records are those of the host
+ * writer (its compressed bytes differ).  Each push uploads its whole blocks
+ * and returns while the device compresses them; they are written at the
+ * next push or at close.  Uses about 270 KiB of device memory per block of
+ * the largest push, and the device's CUDA stream of greatest priority. */
+esg_status esg_bam_writer_use_device(esg_bam_writer* writer, int32_t device);
+/* Blocks written by the device so far, and how many of them stored. */
+esg_status esg_bam_writer_blocks(const esg_bam_writer* writer, uint64_t* blocks,
+                                 uint64_t* stored);
+/* The device compressor's steps run on the host, lane by lane, on one block
+ * (1 <= n <= 0xff00 bytes) into `out` (65536 bytes, 4-byte aligned): the
+ * length of the raw DEFLATE stream, 0xffffffff when the block is to be
+ * stored, 0 on a bad argument.  For checking the steps without a device;
+ * the writer does not call it. */
+uint32_t esg_bgzf_deflate_host(const uint8_t* src, uint32_t n, uint8_t* out);
+/* The compressor's Huffman code lengths on the host: freq[0, n) (2 <= n <=
+ * 288) to lengths of at most `limit` (1..15) bits, every symbol with a
+ * frequency coded and the code complete.  0, or -1 on a bad argument. */
+int32_t esg_bgzf_code_lengths(const uint32_t* freq, uint32_t n, uint32_t limit, uint8_t* len);
 
 /* Scoring for callers that cannot allocate.  No counterpart in the reference.
  *
