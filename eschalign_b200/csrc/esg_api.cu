@@ -1269,8 +1269,9 @@ static esg_status prepare_impl(esg_scorer* sc, const uint8_t* const* ptrs, const
   b->in_bytes = sz_codes + sz_off + sz_len + sz_order + sz_tasks + sz_list + sz_chunks;
   b->in_buf.p = sc->pinned.get(b->in_bytes, &b->in_buf.cap);
   if (!b->in_buf.p) {
+    const size_t want = b->in_bytes;
     delete b;
-    return fail(ESG_ERR_OUT_OF_MEMORY, "pinned host memory (%zu bytes)", (size_t)b->in_bytes);
+    return fail(ESG_ERR_OUT_OF_MEMORY, "pinned host memory (%zu bytes)", want);
   }
   char* at = (char*)b->in_buf.p;
   b->h_packed = carve<uint8_t>(at, b->code_words ? b->code_words * 4 : 1);
