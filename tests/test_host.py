@@ -164,6 +164,8 @@ def test_reads_pack_at_two_bits_and_unpack_to_their_codes():
     lib = _native.load()
     fn = lib.esg_internal_pack_reads
     fn.restype = C.c_uint64
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                   C.c_uint64, C.POINTER(C.c_uint64)]
     rng = np.random.default_rng(5)
     reads = []
     for n in [0, 1, 3, 4, 5, 7, 8, 9, 15, 16, 17, 31, 100, 257] + list(rng.integers(1, 400, 60)):
