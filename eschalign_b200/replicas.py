@@ -1,4 +1,5 @@
-"""Replicated panels, reads sharded across GPUs (one process per GPU).
+"""Replicated panels, reads sharded across GPUs (one process per GPU, or
+several devices in one process: score_on_devices).
 
 Reads are independent, so the path shards with no collective on the data
 path: every rank holds its own copy of the panel and scores a contiguous
@@ -36,6 +37,32 @@ def shard(packed, rank: int, world: int):
     off = (packed.off[lo:hi] - start).astype(np.uint64)
     codes = packed.codes[start:stop] if stop > start else np.zeros(1, np.uint8)
     return Packed(codes, off, lens), lo
+
+
+def score_on_devices(scorers, reads, both_strands: bool = False):
+    """The same sharding inside one process: `scorers` are GpuScorers over
+    one panel, scoring and mode, one per device (or several on one device);
+    `reads` a synth.Packed batch or a (codes, off, lens) tuple.  Each scorer
+    takes the cell-balanced slice shard() gives its index and scores it on a
+    thread of its own (the library's calls release the interpreter lock, so
+    the devices run at once).  Returns (results, ties) in read order, equal
+    to one scorer's score_batch over the whole batch, and the slices'
+    BatchResults.  No collective: the slices meet in host memory."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from .synth import Packed
+    scorers = list(scorers)
+    if not scorers:
+        raise ValueError("score_on_devices needs at least one scorer")
+    if not hasattr(reads, "lens"):
+        reads = Packed(*reads)
+    world = len(scorers)
+    parts = [shard(reads, r, world)[0] for r in range(world)]
+    with ThreadPoolExecutor(world) as pool:
+        done = list(pool.map(lambda sp: sp[0].score_batch(sp[1].tuple(), both_strands=both_strands),
+                             zip(scorers, parts)))
+    return (np.concatenate([d.results for d in done]),
+            np.concatenate([d.ties for d in done])), done
 
 
 def gather(results: np.ndarray, ties: np.ndarray, rank: int, world: int, group=None):
