@@ -766,6 +766,27 @@ const esg_pair_hit* esg_mapping_pair_hits(const esg_mapping* m, uint64_t* n) {
   return m ? m->pair_hits.data() : nullptr;
 }
 
+// What is wrong with a caller's hit, or NULL: the strand is 0 or 1, each
+// start is at most its end, and the CIGAR words (BAM ops M..X) consume
+// exactly [query_start, query_end) of the read and [ref_start, ref_end) of
+// the reference, as every traced hit does.  Its ops must already be known
+// to lie inside `ops`.
+static const char* hit_inconsistency(const esg_hit& h, const uint32_t* ops) {
+  const esg_alignment& a = h.alignment;
+  if (h.reverse > 1) return "its strand is not 0 or 1";
+  if (a.query_start > a.query_end || a.ref_start > a.ref_end) return "a start is past its end";
+  uint64_t q = 0, r = 0;
+  for (uint32_t k = 0; k < a.n_ops; ++k) {
+    const uint32_t w = ops[a.ops_offset + k], op = w & 0xfu, n = w >> 4;
+    if (op > 8) return "a CIGAR op is past X";
+    if (op == 0 || op == 1 || op == 4 || op == 7 || op == 8) q += n;  // M I S = X
+    if (op == 0 || op == 2 || op == 3 || op == 7 || op == 8) r += n;  // M D N = X
+  }
+  if (q != (uint64_t)(a.query_end - a.query_start) || r != (uint64_t)(a.ref_end - a.ref_start))
+    return "its CIGAR does not span its coordinates";
+  return nullptr;
+}
+
 esg_status esg_mapping_from_arrays(const esg_read_mapping* reads, uint32_t n_reads,
                                    const esg_hit* hits, uint64_t n_hits, const uint32_t* ops,
                                    uint64_t n_ops, const char* md, uint64_t n_md,
@@ -782,6 +803,9 @@ esg_status esg_mapping_from_arrays(const esg_read_mapping* reads, uint32_t n_rea
         hits[h].md_offset > n_md || hits[h].md_len > n_md - hits[h].md_offset)
       return merr(ESG_ERR_BAD_ARGUMENT, "hit %llu's ops or MD run past their arrays",
                   (unsigned long long)h);
+  for (uint64_t h = 0; h < n_hits; ++h)
+    if (const char* why = hit_inconsistency(hits[h], ops))
+      return merr(ESG_ERR_BAD_ARGUMENT, "hit %llu: %s", (unsigned long long)h, why);
   auto* m = new esg_mapping();
   m->reads.assign(reads, reads + n_reads);
   m->hits.assign(hits, hits + n_hits);
@@ -807,6 +831,11 @@ esg_status esg_mapping_set_pairs(esg_mapping* m, const esg_pair_mapping* pairs, 
           e.md_offset > n_md || e.md_len > n_md - e.md_offset)
         return merr(ESG_ERR_BAD_ARGUMENT, "pair hit %llu's ops or MD run past their arrays",
                     (unsigned long long)h);
+  for (uint64_t h = 0; h < n_pair_hits; ++h)
+    for (const esg_hit& e : pair_hits[h].mates)
+      if (const char* why = hit_inconsistency(e, m->ops.data()))
+        return merr(ESG_ERR_BAD_ARGUMENT, "pair hit %llu, a mate: %s", (unsigned long long)h,
+                    why);
   m->pairs.assign(pairs, pairs + n_pairs);
   m->pair_hits.assign(pair_hits, pair_hits + n_pair_hits);
   return ESG_OK;

@@ -510,14 +510,19 @@ const char* esg_mapping_md(const esg_mapping* mapping, uint64_t* n);
 void esg_mapping_free(esg_mapping* mapping);
 /* A mapping made from the caller's arrays (copied; the same layout the
  * accessors above return), for reads mapped elsewhere that go to
- * esg_bam_encode.  No counterpart in the reference. */
+ * esg_bam_encode.  Offsets are checked against the arrays, and each hit
+ * must be one a traceback gives: strand 0 or 1, each start at most its end,
+ * CIGAR words of the BAM ops M..X whose read- and reference-consuming
+ * lengths span [query_start, query_end) and [ref_start, ref_end); anything
+ * else is ESG_ERR_BAD_ARGUMENT naming the hit.  No counterpart in the
+ * reference. */
 esg_status esg_mapping_from_arrays(const esg_read_mapping* reads, uint32_t n_reads,
                                    const esg_hit* hits, uint64_t n_hits, const uint32_t* ops,
                                    uint64_t n_ops, const char* md, uint64_t n_md,
                                    esg_mapping** out);
 /* Give a mapping made by esg_mapping_from_arrays the paired arrays of
- * esg_map_pairs' output (two read entries per pair; offsets checked), for
- * esg_bam_encode_pairs. */
+ * esg_map_pairs' output (two read entries per pair; offsets and each mate's
+ * hit checked as above), for esg_bam_encode_pairs. */
 esg_status esg_mapping_set_pairs(esg_mapping* mapping, const esg_pair_mapping* pairs,
                                  uint32_t n_pairs, const esg_pair_hit* pair_hits,
                                  uint64_t n_pair_hits);

@@ -193,6 +193,33 @@ def test_mapping_from_arrays_checks_its_offsets():
         EB.mapping_handle(m)
 
 
+@pytest.mark.parametrize("field,value,why", [
+    ("reverse", 2, "strand"), ("query_end", 3, "CIGAR does not span"),
+    ("ref_end", 6, "CIGAR does not span"), ("query_start", 5, "start is past its end")])
+def test_mapping_from_arrays_checks_each_hit(field, value, why):
+    """A caller's hit must be one a traceback could give: strand 0 / 1,
+    starts before ends, CIGAR words spanning its read and reference
+    coordinates; anything else is refused before the encoder sees it."""
+    from eschalign_b200 import _native
+    # 2M1D1I1M: 4 read bases (0..4) and 4 reference bases (1..5)
+    hit = {"reference": 0, "reverse": False, "score": 5, "query_start": 0, "query_end": 4,
+           "ref_start": 1, "ref_end": 5, "cigar": "2M1D1I1M", "md": "2^A1", "nm": 2}
+
+    def mapping():
+        return mappings_from_oracle([{"best_score": 5, "n_tied": 1, "suboptimal": None,
+                                      "hits": [dict(hit)]}])
+
+    _native.load().esg_mapping_free(EB.mapping_handle(mapping()))  # consistent: taken
+    m = mapping()
+    m.hits[field] = value
+    with pytest.raises(RuntimeError, match=why):
+        EB.mapping_handle(m)
+    m = mapping()
+    m.ops[0] = (2 << 4) | 9  # no BAM op 9
+    with pytest.raises(RuntimeError, match="past X"):
+        EB.mapping_handle(m)
+
+
 class OracleScorer:
     """A stand-in for GpuScorer.map_reads that maps with the oracle, so the
     pipeline of align_bam runs on the CPU."""
