@@ -1181,6 +1181,10 @@ esg_status esg_bam_encode_pairs(const esg_bam_batch* b, const esg_mapping* m,
   for (uint64_t h = 0; h < n_phits; ++h)
     if (phits[h].mates[0].reference >= n_refs || phits[h].mates[1].reference >= n_refs)
       return berr(ESG_ERR_BAD_ARGUMENT, "a hit's reference is past ref_names");
+  // a Proper pair is placed by its primary pair hit
+  for (uint32_t p = 0; p < n_pairs; ++p)
+    if ((pairs[p].flags & ESG_PAIR_PROPER) && pairs[p].n_hits == 0)
+      return berr(ESG_ERR_BAD_ARGUMENT, "a proper pair has no pair hit");
   const size_t np = n / 2;
   std::vector<std::vector<uint8_t>> enc(np);
   std::vector<uint32_t> count(np, 0);

@@ -824,6 +824,9 @@ esg_status esg_mapping_set_pairs(esg_mapping* m, const esg_pair_mapping* pairs, 
   for (uint32_t p = 0; p < n_pairs; ++p)
     if (pairs[p].first_hit > n_pair_hits || pairs[p].n_hits > n_pair_hits - pairs[p].first_hit)
       return merr(ESG_ERR_BAD_ARGUMENT, "pair %u's hits run past the pair-hit array", p);
+  for (uint32_t p = 0; p < n_pairs; ++p)
+    if ((pairs[p].flags & ESG_PAIR_PROPER) && pairs[p].n_hits == 0)
+      return merr(ESG_ERR_BAD_ARGUMENT, "pair %u is proper but has no pair hit", p);
   const uint64_t n_ops = m->ops.size(), n_md = m->md.size();
   for (uint64_t h = 0; h < n_pair_hits; ++h)
     for (const esg_hit& e : pair_hits[h].mates)

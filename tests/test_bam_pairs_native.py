@@ -270,3 +270,14 @@ def test_paired_writer_sorts_mates_consistently(oracle, tmp_path):
                               for i in range(len(lens) // 2)])
             wr.push(seq, EB.encode_pairs(b, pair_mappings_from_oracle(pms), names, ads, True))
     assert record_stream(out) == b"".join(B.coordinate_order(recs))
+
+
+def test_proper_pair_without_a_pair_hit_is_refused():
+    """A caller's paired mapping whose Proper pair lists no pair hit has
+    nothing to place the mates by: esg_mapping_set_pairs refuses it."""
+    from eschalign_b200 import bam as EB
+    pm = {"proper": True, "score": 10, "n_tied": 1, "suboptimal": [None, None], "hits": []}
+    m = pair_mappings_from_oracle([pm])
+    m.pair_hits = np.zeros(0, m.pair_hits.dtype)
+    with pytest.raises(RuntimeError, match="proper but has no pair hit"):
+        EB.mapping_handle(m)
