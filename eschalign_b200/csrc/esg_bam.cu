@@ -1031,6 +1031,12 @@ esg_status esg_bam_encode(const esg_bam_batch* b, const esg_mapping* m,
     for (uint32_t h = 0; h < maps[k].n_hits; ++h)
       if (hits[maps[k].first_hit + h].reference >= n_refs)
         return berr(ESG_ERR_BAD_ARGUMENT, "a hit's reference is past ref_names");
+  // a scored read's hits lie inside it (a traced hit always does)
+  for (size_t k = 0; k < n; ++k)
+    if (b->len[k] == b->full_len[k])
+      for (uint32_t h = 0; h < maps[k].n_hits; ++h)
+        if (hits[maps[k].first_hit + h].alignment.query_end > b->recs[k].l_seq)
+          return berr(ESG_ERR_BAD_ARGUMENT, "a hit runs past the end of its read");
   std::vector<std::vector<uint8_t>> enc(n);
   std::vector<uint32_t> count(n, 0), unmapped(n, 0), unique(n, 0);
   std::atomic<int> bad{0};
@@ -1185,6 +1191,25 @@ esg_status esg_bam_encode_pairs(const esg_bam_batch* b, const esg_mapping* m,
   for (uint32_t p = 0; p < n_pairs; ++p)
     if ((pairs[p].flags & ESG_PAIR_PROPER) && pairs[p].n_hits == 0)
       return berr(ESG_ERR_BAD_ARGUMENT, "a proper pair has no pair hit");
+  // every mate's hit lies inside the mate, its 3' adapter bases around it
+  // (a traced hit always does)
+  auto outside = [&](const esg_hit& h, size_t mate) {
+    const uint32_t shift = (h.reverse && adapter_bases) ? adapter_bases[mate] : 0u;
+    return (uint64_t)h.alignment.query_end + shift > b->recs[mate].l_seq;
+  };
+  for (uint32_t p = 0; p < n_pairs; ++p) {
+    for (uint32_t q = 0; q < 2; ++q) {
+      const esg_read_mapping& me = maps[2 * (size_t)p + q];
+      for (uint32_t h = 0; h < me.n_hits; ++h)
+        if (outside(hits[me.first_hit + h], 2 * (size_t)p + q))
+          return berr(ESG_ERR_BAD_ARGUMENT, "a hit runs past the end of its mate");
+    }
+    if (pairs[p].flags & ESG_PAIR_PROPER)
+      for (uint32_t t = 0; t < pairs[p].n_hits; ++t)
+        for (uint32_t q = 0; q < 2; ++q)
+          if (outside(phits[pairs[p].first_hit + t].mates[q], 2 * (size_t)p + q))
+            return berr(ESG_ERR_BAD_ARGUMENT, "a pair hit runs past the end of its mate");
+  }
   const size_t np = n / 2;
   std::vector<std::vector<uint8_t>> enc(np);
   std::vector<uint32_t> count(np, 0);

@@ -664,7 +664,9 @@ void esg_bam_batch_free(esg_bam_batch* batch);
 void esg_bam_close(esg_bam_reader* reader);
 /* The output records of a batch from its mapping (esg_map_reads over
  * esg_bam_batch_reads, with the panel's letters for MD), encoded in the BAM
- * layout, in read order; ref_names in panel order. */
+ * layout, in read order; ref_names in panel order.  A hit whose reference
+ * is past ref_names, or whose read coordinates run past its read, is
+ * ESG_ERR_BAD_ARGUMENT. */
 esg_status esg_bam_encode(const esg_bam_batch* batch, const esg_mapping* mapping,
                           const esg_bam_options* options, const char* const* ref_names,
                           uint32_t n_refs, uint32_t threads, esg_bam_records** out);
@@ -675,7 +677,8 @@ esg_status esg_bam_encode(const esg_bam_batch* batch, const esg_mapping* mapping
  * 0x40 / 0x80, mate reference and position, TLEN, MC, and each mate's
  * adapter bases soft-clipped at its 3' end and counted in `ad`
  * (adapter_bases[2n] from esg_pair_adapters; NULL under --no-adapter-trim:
- * no `ad` tag). */
+ * no `ad` tag).  A Proper pair with no pair hit, or a hit running past its
+ * mate (with the mate's adapter bases), is ESG_ERR_BAD_ARGUMENT. */
 esg_status esg_bam_encode_pairs(const esg_bam_batch* batch, const esg_mapping* mapping,
                                 const uint32_t* adapter_bases, const esg_bam_options* options,
                                 const char* const* ref_names, uint32_t n_refs, uint32_t threads,

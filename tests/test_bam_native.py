@@ -340,3 +340,24 @@ def test_output_header_carries_the_inputs_programs(oracle, tmp_path):
     EB.align_bam(sc, FIXTURE, out, names, refs)
     text_out, _, _ = B.read_bam(open(out, "rb").read())
     assert b"PP:samtools.1" in text_out and b"ID:bwa" in text_out
+
+
+def test_encoder_refuses_a_hit_past_its_read(oracle):
+    """A hit whose CIGAR is consistent but whose read coordinates run past
+    the read (no traceback gives one) is refused by the encoder instead of
+    becoming a record whose CIGAR and sequence disagree."""
+    from eschalign_b200 import bam as EB
+    o = flag_set("default")
+    names, refs = trna_panel()
+    ms = oracle_mappings(oracle, input_records(), o)
+    with EB.BamReader(FIXTURE) as rd:
+        b = next(iter(rd.batches(max_reads=7, max_read_len=o["max_read_len"])))
+    m = mappings_from_oracle(ms[:len(b)])
+    EB.encode(b, m, names)  # as traced: taken
+    k = int(np.nonzero(m.reads["n_hits"])[0][0])
+    h = int(m.reads["first_hit"][k])
+    shift = int(b.reads()[2][k])  # the read's length
+    m.hits["query_start"][h] += shift
+    m.hits["query_end"][h] += shift
+    with pytest.raises(RuntimeError, match="past the end of its read"):
+        EB.encode(b, m, names)
